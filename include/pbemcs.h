@@ -1,0 +1,217 @@
+/*
+ * pbemcs.h — C-ABI of the B200 PIC-MCC step library (libpbemcs.so).
+ *
+ * The entry points replace the numeric kernels and the per-timestep loop of the
+ * PY-BEMCS reference, Python/physics_engine.py (cited as file:line below).  A Python
+ * host binds them with ctypes (thruster_cx_code_b200/_lib.py); the signatures use plain
+ * pointers, sizes and scalars only.
+ *
+ * Conventions
+ *   - Every function returns 0 (PB_OK) or a PB_ERR_* code; pb_last_error() gives text.
+ *   - Array arguments of the kernel-level functions are DEVICE pointers (any CUDA
+ *     allocation, e.g. a torch tensor's data_ptr()); `stream` is a cudaStream_t or NULL.
+ *   - Fields are row-major (ny, nx) with x fastest, as NumPy's [iy, ix]; particles are
+ *     1-D structure-of-arrays.  Positions are in mm, velocities in m/s.
+ *   - Host helpers (pb_host_*) run on the CPU and need no GPU.
+ */
+#ifndef PBEMCS_H
+#define PBEMCS_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PB_OK = 0,
+  PB_ERR_CUDA = 1,        /* a CUDA call failed (message in pb_last_error) */
+  PB_ERR_ARG = 2,         /* invalid argument */
+  PB_ERR_CAPACITY = 3,    /* particle storage or a per-step list would overflow */
+  PB_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  PB_ERR_NOCONV = 5,      /* the field solve did not reach its tolerance */
+  PB_ERR_STATE = 6        /* call out of order (e.g. step before a domain is set) */
+};
+
+/* error flags reported by the device in pb_step_report.errflags */
+enum {
+  PB_EF_CAPACITY_ION = 1 << 0, PB_EF_CAPACITY_ELE = 1 << 1, PB_EF_SEE_OVERFLOW = 1 << 2,
+  PB_EF_ANGLE_OVERFLOW = 1 << 3, PB_EF_SPIN_TIMEOUT = 1 << 4, PB_EF_NAN_SUBSTEP = 1 << 5,
+  PB_EF_SUBSTEP_CAP = 1 << 6, PB_EF_POISSON_NOCONV = 1 << 7, PB_EF_ID_OVERFLOW = 1 << 8
+};
+
+int32_t pb_version(void);
+const char* pb_last_error(void);
+
+/* ---------------------------------------------------------------- kernel level */
+
+/* NGP charge deposition: rho[iy, ix] += charge_density for every particle, with
+ * ix = clip(rint(x/dx), 1, nx-2), iy likewise; bit-identical to the sequential float32
+ * np.add.at of accumulate_rho_cpu (physics_engine.py:178-185; Taichi form :38-60).
+ * Uses a temporary count array from the stream-ordered allocator. */
+int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy,
+                          int32_t nx, int32_t ny, double charge_density, void* stream);
+
+/* Bilinear E/B gather + 2D3V Boris + drift (x += vx dt 1000), in place; bit-identical
+ * to push_particles_boris_cpu (physics_engine.py:188-254; Taichi form :63-144). */
+int32_t pb_push_particles_boris(float* x, float* y, float* vx, float* vy, float* vz, const float* Ex,
+                                const float* Ey, const float* Bx, const float* By, const float* Bz,
+                                int32_t num_p, double dx, double dy, int32_t nx, int32_t ny, double dt,
+                                double q_m, void* stream);
+
+/* One explicit conduction sweep with the Taichi kernel's edge handling
+ * (thermal_conduction_taichi, physics_engine.py:147-171). */
+int32_t pb_thermal_conduction(const float* T, float* T_new, const int32_t* mask, int32_t nx, int32_t ny,
+                              double Fo_x, double Fo_y, void* stream);
+
+/* compute_particle_substeps (physics_engine.py:928-966): out_host[0] = n_sub,
+ * out_host[1] = ds_max [m], out_host[2] = ds_lim [m]; synchronises the stream. */
+int32_t pb_compute_particle_substeps(const float* x, const float* y, const float* vx, const float* vy,
+                                     const float* vz, int32_t n, const float* Ex, const float* Ey, int32_t nx,
+                                     int32_t ny, double dx, double dy, double qm, double dt, double frac,
+                                     double* out_host, void* stream);
+
+/* _segment_hits_grid (physics_engine.py:1880-1901) with samples = 8; hit_ix/hit_iy int64. */
+int32_t pb_segment_hits_grid(const uint8_t* isBound, int32_t nx, int32_t ny, double dx, double dy,
+                             const float* x0, const float* y0, const float* x1, const float* y1, int32_t n,
+                             uint8_t* hit, int64_t* hit_ix, int64_t* hit_iy, void* stream);
+
+/* ---------------------------------------------------------------- simulation instance */
+typedef struct pb_sim pb_sim;
+
+/* Scalars of one timestep, computed by the host in IEEE double exactly as the reference
+ * does (physics_engine.py:969-1784); float32 thresholds are cast on the device. */
+typedef struct pb_step_params {
+  int32_t iteration;       /* self.iteration after the increment */
+  int32_t do_poisson;      /* iteration % 2 == 0 */
+  int32_t picard_iters;    /* 5 */
+  int32_t thermal_on;      /* sim_mode in (Thermal, Both) */
+  int32_t erosion_on;      /* sim_mode in (Erosion, Both) */
+  int32_t sort_now;        /* re-sort particles by cell after this step */
+  /* injection */
+  int32_t inject_on;
+  int32_t geometry;        /* 0 half_hole, 1 one_hole, 2 two_holes, 3 no grids */
+  double lam, ylo, yhi, x_inj, v_bohm, v_spread;
+  double span[4];          /* two_holes band limits (cast to float32) */
+  int32_t rf_on;
+  int32_t neut_n;
+  double rf_num_float, rf_ylo, rf_yhi, v_e_src;
+  double neut_r, neut_x, v_e_th;
+  /* deposit and field solve */
+  double charge_density;   /* q * macro_weight / V_cell */
+  double coeff, qn0_neg, V_plasma, Te_up, omega_keep, omega_new;
+  double hx, two_hx, hy, two_hy, two_hy_per;
+  /* grid spacing [mm] (Python floats, cast to float32 where NumPy does) */
+  double dx, dy;
+  /* push */
+  double dt, qm_ion, qm_e, ds_lim, dt2;
+  /* geometry thresholds */
+  double x_entry, x_exit, x_plume, Lx, Ly;
+  /* tallies */
+  double half_m_ion, macro_w, C_cell, thermal_accel, q, Y_coeff, E_th, thresh;
+  /* CEX */
+  double rT, n0a, neut_vth;
+  /* SEE */
+  double v_see_th;
+  /* thermal */
+  double cooling_factor, T4_300, Fo_x, Fo_y;
+  int32_t sweeps;
+  /* RF co-extraction (V_fixed on one grid = Vdc + v_rf before injection) */
+  int32_t rf_grid;         /* -1: off */
+  double v_rf;
+  /* saddle sample indices (flat), -1 unused */
+  int32_t n_saddle;
+  int32_t saddle_idx[8];
+} pb_step_params;
+
+typedef struct pb_step_report {
+  int32_t num_p, num_e;
+  int32_t n_sub_ion, n_sub_e;
+  double ds_ion, ds_e;
+  int32_t injected, rf_injected, neut_injected, see_spawned;
+  uint64_t entered, crossed, exited_any, lost_to_grid, hits, cex_collisions, cex_ties;
+  double exit_sums[9];     /* sum vx, |v|, E_eV, |v| primary, n primary, |v| cex, n cex, vx^2, |v|^2 */
+  double theta95;          /* NaN when 5 or fewer ions crossed */
+  double min_pot;
+  double grid_sums[32];    /* per grid: sum T, cell count */
+  int32_t broken;          /* cells broken by sputtering this step */
+  int32_t pad0;
+  uint64_t ppc_active, ppc_low, ppc_min;
+  double poisson_stats[4]; /* outer, inner iterations (cumulative), last relative residual, solves */
+  uint32_t errflags;
+  int32_t pad1;
+} pb_step_report;
+
+int32_t pb_sim_create(pb_sim** out, int32_t device);
+int32_t pb_sim_destroy(pb_sim* s);
+int32_t pb_sim_set_seed(pb_sim* s, uint64_t seed);
+
+/* Field solver controls: FP64 relative residual target, FP32 inner reduction, loop caps,
+ * smoothing sweeps per level and the largest coarsest-level size. */
+int32_t pb_sim_set_solver(pb_sim* s, double tol, double tol_inner, int32_t max_outer, int32_t max_inner,
+                          int32_t nu, int32_t max_coarse);
+
+/* Upload the domain of build_domain (physics_engine.py:629-847): node masks, Dirichlet
+ * values, electrode masks (bit g of gridmask = grid g), plus the state arrays to keep.
+ * Host pointers.  Builds the node classes of build_sparse_matrix (:525-552) and the
+ * multigrid hierarchy.  keep_state != 0 keeps particles and damage. */
+int32_t pb_sim_set_domain(pb_sim* s, int32_t ny, int32_t nx, int32_t periodic, const uint8_t* isBound,
+                          const double* V_fixed, const uint16_t* gridmask, int32_t ngrids, const double* V,
+                          const float* Tmap, const double* damage, const double* eroded, int32_t keep_state);
+
+/* User cross-section (lookup_user_cs, physics_engine.py:475-484): the cubic B-spline of
+ * the log-log table (SciPy UnivariateSpline knots t[nt], coefficients c[nt-4]) and the
+ * clip range [lo, hi] in log10 eV; which = 0 charge exchange ('CX'), 1 secondary
+ * emission ('SEE'); nt = 0 removes it. */
+int32_t pb_sim_set_spline(pb_sim* s, int32_t which, int32_t nt, const double* t, const double* c, double lo,
+                          double hi);
+
+/* Rebuild node classes and the multigrid hierarchy from the device isBound (after cells
+ * broke by sputtering; build_sparse_matrix, physics_engine.py:1448). */
+int32_t pb_sim_rebuild_operator(pb_sim* s);
+
+/* Replace one species' particles (species 0 ions, 1 electrons); host arrays; cex may be
+ * NULL for electrons. */
+int32_t pb_sim_set_particles(pb_sim* s, int32_t species, int32_t n, const float* x, const float* y,
+                             const float* vx, const float* vy, const float* vz, const uint8_t* cex,
+                             const uint32_t* id, uint32_t next_id);
+int32_t pb_sim_get_particles(pb_sim* s, int32_t species, int32_t n, float* x, float* y, float* vx, float* vy,
+                             float* vz, uint8_t* cex, uint32_t* id);
+int32_t pb_sim_counts(pb_sim* s, int32_t* num_p, int32_t* num_e, uint32_t* next_ion_id, uint32_t* next_e_id);
+int32_t pb_sim_reserve(pb_sim* s, int32_t species, int32_t capacity);
+
+/* Field arrays: 0 V (f64), 1 Ex, 2 Ey, 3 rho, 4 Tmap (f32), 5 damage (f64), 6 isBound (u8),
+ * 7 V_fixed (f64), 8 ppc (i32), 9 accum_ppc (f64), 10 eroded (f64), 11 Vnew (f64),
+ * 12 node class (u8). */
+int32_t pb_sim_field_ptr(pb_sim* s, int32_t which, void** dptr);
+int32_t pb_sim_get_field(pb_sim* s, int32_t which, void* host, int64_t nbytes);
+int32_t pb_sim_set_field(pb_sim* s, int32_t which, const void* host, int64_t nbytes);
+/* particle arrays of the current buffer: 0 x, 1 y, 2 vx, 3 vy, 4 vz, 5 cex, 6 id */
+int32_t pb_sim_particle_ptr(pb_sim* s, int32_t species, int32_t which, void** dptr);
+
+/* recalc_poisson(iterations) (physics_engine.py:850-884) on the current rho. */
+int32_t pb_sim_poisson(pb_sim* s, int32_t iterations, const pb_step_params* p, double* stats4_host);
+
+/* One timestep (physics_engine.py:969-1784); report may be NULL (no host sync). */
+int32_t pb_sim_step(pb_sim* s, const pb_step_params* p, pb_step_report* report);
+/* Steps without a host synchronisation; params[k] for k < nsteps; reports optional. */
+int32_t pb_sim_run(pb_sim* s, const pb_step_params* params, int32_t nsteps, pb_step_report* reports);
+int32_t pb_sim_synchronize(pb_sim* s);
+void* pb_sim_stream(pb_sim* s);
+
+/* Device time (ms) of the last pb_sim_run / pb_sim_step in out[0]; with profiling on,
+ * out[1..6] = summed phase times (inject+deposit, field solve, sub-step reduction, ion
+ * step kernel, sputter break + electron step + SEE, thermal/diagnostics/sort), out[7] =
+ * steps profiled, out[8] = kernels enqueued by that call. */
+int32_t pb_sim_timing(pb_sim* s, double* out_host9);
+int32_t pb_sim_set_profiling(pb_sim* s, int32_t on);
+
+/* ---------------------------------------------------------------- host helpers */
+float pb_host_seq_add_f32(float s, float c, uint32_t n);
+double pb_host_philox_uniform(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j);
+double pb_host_philox_normal(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j);
+float pb_host_percentile95(const float* sorted, int32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

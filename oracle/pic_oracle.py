@@ -125,6 +125,24 @@ def thermal_sweeps(T, isBound, Fo_x, Fo_y, sweeps=10):
     return T
 
 
+def thermal_taichi_sweep(T, mask, Fo_x, Fo_y):
+    """One sweep of thermal_conduction_taichi (``physics_engine.py:147-171``): every masked
+    cell (edges included), a neighbour is used when it is inside the domain and masked,
+    ``T_new = max(T + dT, 300)`` in float32 (Taichi default_fp f32, Fo as f32); unmasked
+    cells are copied.  Restated from the source (Taichi cannot run here)."""
+    T = np.asarray(T, dtype=np.float32)
+    ny, nx = T.shape
+    m = np.asarray(mask).astype(bool)
+    fx, fy = np.float32(Fo_x), np.float32(Fo_y)
+    Tl = T.copy(); Tl[:, 1:] = np.where(m[:, :-1], T[:, :-1], T[:, 1:])
+    Tr = T.copy(); Tr[:, :-1] = np.where(m[:, 1:], T[:, 1:], T[:, :-1])
+    Td = T.copy(); Td[1:, :] = np.where(m[:-1, :], T[:-1, :], T[1:, :])
+    Tu = T.copy(); Tu[:-1, :] = np.where(m[1:, :], T[1:, :], T[:-1, :])
+    c2 = np.float32(2.0) * T
+    dT = fx * ((Tl - c2) + Tr) + fy * ((Td - c2) + Tu)
+    return np.where(m, np.maximum(T + dT, np.float32(300.0)), T).astype(np.float32)
+
+
 def segment_hits(isBound, dx, dy, nx, ny, x0, y0, x1, y1, samples=8):
     """Path absorption test, ``physics_engine.py:1880-1901``: 8 samples along the
     straight segment, cell = clip(rint(s/d), 0, n-1); first hit cell recorded."""
@@ -289,7 +307,7 @@ class ReplayDraws:
     def see_u(self, ion_ids, step):
         return self._take("rand", len(ion_ids))
 
-    def see_v(self, n, e_ids, step):
+    def see_v(self, n, parent_ids, step):
         return self._normals3(n)
 
     def cex_u(self, ion_ids, step):
@@ -344,8 +362,9 @@ class PhiloxDraws:
     def see_u(self, ion_ids, step):
         return _px.uniforms(self.seed, ion_ids, _px.SITE_SEE_SPAWN, step, 1)[0]
 
-    def see_v(self, n, e_ids, step):
-        g = _px.normals(self.seed, e_ids, _px.SITE_SEE_V, step, 3)
+    def see_v(self, n, parent_ids, step):
+        # keyed by the parent ion, so the draw does not depend on spawn order
+        g = _px.normals(self.seed, parent_ids, _px.SITE_SEE_V, step, 3)
         return g[0], g[1], g[2]
 
     def cex_u(self, ion_ids, step):
@@ -812,7 +831,7 @@ class OracleSimulator:
                 sy = (p_y[hot][spawn] - p_vy[hot][spawn] * self.dt * 1000.0 / 1.5).astype(fp)
                 v_see_th = np.sqrt(2.0 * self.q * 2.0 / self.m_e)
                 eids = self.new_e_ids(num_see)
-                gx, gy, gz = draws.see_v(num_see, eids, it)
+                gx, gy, gz = draws.see_v(num_see, p_ids[hot][spawn], it)
                 self._add_electrons(sx, sy, (gx * v_see_th).astype(fp), (gy * v_see_th).astype(fp),
                                     (gz * v_see_th).astype(fp), eids)
 

@@ -1,0 +1,246 @@
+// Shared device helpers for the PIC-MCC kernels (sm_100a).
+//
+// Arithmetic here reproduces NumPy 2 semantics on x86-64 exactly where the reference
+// path (Python/physics_engine.py) depends on it:
+//   * float32 -> integer casts (ndarray.astype) give INT_MIN for NaN / out of range;
+//   * np.round is round-half-to-even (rintf);
+//   * every expression is written with explicit __f*_rn / __d*_rn intrinsics so that no
+//     multiply-add is contracted (NumPy evaluates each ufunc separately);
+//   * seq_add_f32() gives the exact result of n sequential float32 additions of one
+//     value, which is what np.add.at produces when every particle adds the same charge.
+#pragma once
+#include <cstdint>
+#include <climits>
+#include <cuda_runtime.h>
+
+#define PB_HD __host__ __device__ __forceinline__
+
+// error flags (PB_EF_*) come from the public header
+#include "pbemcs.h"
+
+// ---------------------------------------------------------------- draw sites
+// Must equal oracle/philox.py.
+enum pb_site : uint32_t {
+  SITE_ION_COUNT = 1, SITE_ION_Y = 2, SITE_ION_V = 3, SITE_RF_COUNT = 4, SITE_RF_Y = 5,
+  SITE_RF_V = 6, SITE_NEUT_Y = 7, SITE_NEUT_V = 8, SITE_SEE_SPAWN = 9, SITE_SEE_V = 10,
+  SITE_CEX_U = 11, SITE_CEX_FM = 12, SITE_ION_HOLE = 13, SITE_PRELOAD = 14,
+};
+
+// ---------------------------------------------------------------- NumPy casts
+PB_HD int np_f2i32(float v) {
+  return (v >= -2147483648.0f && v < 2147483648.0f) ? (int)v : INT_MIN;
+}
+PB_HD long long np_f2i64(float v) {
+  return (v >= -9223372036854775808.0f && v < 9223372036854775808.0f) ? (long long)v : LLONG_MIN;
+}
+PB_HD int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+PB_HD long long clampll(long long v, long long lo, long long hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// cell index of np.clip(np.round(s / d).astype(int), lo, hi)   (float32 division)
+__device__ __forceinline__ int cell_round(float s, float d, int lo, int hi) {
+  float q = __fdiv_rn(s, d);
+  return (int)clampll(np_f2i64(rintf(q)), lo, hi);
+}
+// same with an int32 cast (accumulate_rho uses astype(np.int32))
+__device__ __forceinline__ int cell_round32(float s, float d, int lo, int hi) {
+  float q = __fdiv_rn(s, d);
+  return clampi(np_f2i32(rintf(q)), lo, hi);
+}
+
+// np.maximum / np.minimum propagate NaN (fmaxf does not)
+__device__ __forceinline__ float np_maxf(float a, float b) { return (a != a || b != b) ? __int_as_float(0x7fc00000) : (a >= b ? a : b); }
+__device__ __forceinline__ double np_maxd(double a, double b) { return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000ll) : (a >= b ? a : b); }
+
+// np.mod for float32 with a positive divisor: fmod, then shift into [0, b)
+__device__ __forceinline__ float np_modf_pos(float a, float b) {
+  float m = fmodf(a, b);
+  if (m != 0.0f) {
+    if ((b < 0.0f) != (m < 0.0f)) m = __fadd_rn(m, b);
+  } else {
+    m = copysignf(0.0f, b);
+  }
+  return m;
+}
+
+// ---------------------------------------------------------------- Philox4x32-10
+struct u32x4 { uint32_t x, y, z, w; };
+
+PB_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c.x;
+    uint64_t p1 = (uint64_t)0xCD9E8D57u * c.z;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+    uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    u32x4 n;
+    n.x = hi1 ^ c.y ^ k0;
+    n.y = lo1;
+    n.z = hi0 ^ c.w ^ k1;
+    n.w = lo0;
+    c = n;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  return c;
+}
+
+PB_HD double u53(uint32_t a, uint32_t b) {
+  return ((double)(a >> 5) * 67108864.0 + (double)(b >> 6)) * (1.0 / 9007199254740992.0);
+}
+
+// counter = (pid lo, pid hi16 | site << 16, step, block); key = seed
+PB_HD u32x4 philox_block(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t block) {
+  u32x4 c;
+  c.x = (uint32_t)pid;
+  c.y = (uint32_t)((pid >> 32) & 0xFFFFu) | (site << 16);
+  c.z = step;
+  c.w = block;
+  return philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+// j-th uniform double of (seed, pid, site, step)
+PB_HD double philox_uniform(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j) {
+  u32x4 r = philox_block(seed, pid, site, step, j >> 1);
+  return (j & 1) ? u53(r.z, r.w) : u53(r.x, r.y);
+}
+
+// ---------------------------------------------------------------- Box-Muller
+// ln and cos from series in plain IEEE double, identical operation order to the oracle
+// (oracle/philox.py: bm_log, bm_cos2pi).  Fused multiply-add is never used.
+#ifdef __CUDA_ARCH__
+#define DMUL(a, b) __dmul_rn((a), (b))
+#define DADD(a, b) __dadd_rn((a), (b))
+#define DSUB(a, b) __dsub_rn((a), (b))
+#define DDIV(a, b) __ddiv_rn((a), (b))
+#else
+#define DMUL(a, b) ((a) * (b))
+#define DADD(a, b) ((a) + (b))
+#define DSUB(a, b) ((a) - (b))
+#define DDIV(a, b) ((a) / (b))
+#endif
+
+PB_HD double bm_log(double x) {
+  int e;
+  double m = frexp(x, &e);
+  if (m < 0.7071067811865476) { m = DMUL(m, 2.0); e -= 1; }
+  double s = DDIV(DSUB(m, 1.0), DADD(m, 1.0));
+  double s2 = DMUL(s, s);
+  double acc = 1.0 / 27.0;
+  for (int k = 25; k >= 1; k -= 2) acc = DADD(DMUL(acc, s2), 1.0 / (double)k);
+  return DADD(DMUL(DMUL(s, acc), 2.0), DMUL((double)e, 0.6931471805599453));
+}
+
+PB_HD double bm_cos2pi(double u) {
+  double w = DMUL(u, 8.0);
+  double kf = floor(w);
+  double f = DSUB(w, kf);
+  int k = ((int)kf) & 7;
+  if (k & 1) f = DSUB(1.0, f);
+  double r = DMUL(f, 0.7853981633974483);
+  double r2 = DMUL(r, r);
+  double c = 1.0, s = 1.0;
+  for (int n = 22; n >= 2; n -= 2) c = DSUB(1.0, DMUL(DDIV(r2, (double)(n * (n - 1))), c));
+  for (int n = 23; n >= 3; n -= 2) s = DSUB(1.0, DMUL(DDIV(r2, (double)(n * (n - 1))), s));
+  s = DMUL(r, s);
+  bool use_sin = (k == 1) | (k == 2) | (k == 5) | (k == 6);
+  double v = use_sin ? s : c;
+  bool neg = (k == 2) | (k == 3) | (k == 4) | (k == 5);
+  return neg ? -v : v;
+}
+
+// j-th standard normal of (seed, pid, site, step): uniforms 2j, 2j+1
+PB_HD double philox_normal(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j) {
+  u32x4 r = philox_block(seed, pid, site, step, j);
+  double u1 = u53(r.x, r.y), u2 = u53(r.z, r.w);
+  double rad = sqrt(DMUL(-2.0, bm_log(DSUB(1.0, u1))));
+  return DMUL(rad, bm_cos2pi(u2));
+}
+
+// ---------------------------------------------------------------- sequential float32 sums
+// Exact result of:  for (i < n) s = RN32(s + c);
+// Within one binade of the running sum (and away from zero) every addition moves s by
+// the same number of ulps, so whole runs are applied at once; transitions between
+// binades, sign changes and stagnation are taken one real addition at a time.
+PB_HD float f32_add_rn(float a, float b) {
+#ifdef __CUDA_ARCH__
+  return __fadd_rn(a, b);
+#else
+  volatile float r = a + b;
+  return r;
+#endif
+}
+
+PB_HD bool f32_signbit(float v) {
+#ifdef __CUDA_ARCH__
+  return (__float_as_uint(v) >> 31) != 0u;
+#else
+  union { float f; uint32_t u; } a; a.f = v; return (a.u >> 31) != 0u;
+#endif
+}
+
+PB_HD float seq_add_f32(float s, float c, uint32_t n) {
+  uint32_t guard = 0;
+  while (n > 0) {
+    float t = f32_add_rn(s, c);
+    --n;
+    if (t == s && !(t == 0.0f && f32_signbit(t) != f32_signbit(s))) return t;  // stagnation
+    float prev = s;
+    s = t;
+    if (!(s == s) || n == 0) return s;
+    if (++guard > 4096) {  // safety net: finish the remainder one addition at a time
+      while (n > 0) { s = f32_add_rn(s, c); --n; }
+      return s;
+    }
+    // try a jump: source and result in the same binade, same sign, normal range
+    uint32_t bp, bs, bc;
+#ifdef __CUDA_ARCH__
+    bp = __float_as_uint(prev); bs = __float_as_uint(s); bc = __float_as_uint(c);
+#else
+    { union { float f; uint32_t u; } a1, a2, a3; a1.f = prev; a2.f = s; a3.f = c; bp = a1.u; bs = a2.u; bc = a3.u; }
+#endif
+    uint32_t ep = (bp >> 23) & 0xFF, es = (bs >> 23) & 0xFF, ec = (bc >> 23) & 0xFF;
+    if (ep != es || (bp >> 31) != (bs >> 31) || es == 0 || es >= 254 || ec == 255) continue;
+    // units of ulp(s) = 2^(es-150);  S = significand of |s| in [2^23, 2^24)
+    int32_t S = (int32_t)((bs & 0x7FFFFF) | 0x800000);
+    bool up = ((bs >> 31) == (bc >> 31));  // |s| grows when c has the sign of s
+    // |c| / ulp as q + f, exactly: |c| = Mc 2^(ec-150) (normal) or Mc 2^-149 (subnormal)
+    uint32_t Mc = (ec == 0) ? (bc & 0x7FFFFF) : ((bc & 0x7FFFFF) | 0x800000);
+    int shift = (ec == 0 ? 1 : (int)ec) - (int)es;  // |c| = Mc * 2^shift ulps
+    int64_t q;
+    int frac_cmp;  // -1: f < 1/2, 0: f == 1/2, 1: f > 1/2
+    if (shift >= 0) {
+      if (shift > 30) continue;
+      q = (int64_t)Mc << shift;
+      frac_cmp = -1;
+    } else {
+      int sh = -shift;
+      if (sh > 40) { q = 0; frac_cmp = -1; }
+      else {
+        q = (int64_t)(Mc >> sh);
+        uint64_t rem = (uint64_t)Mc & ((1ull << sh) - 1ull);
+        uint64_t half = 1ull << (sh - 1);
+        frac_cmp = rem < half ? -1 : (rem == half ? 0 : 1);
+      }
+    }
+    int64_t D;  // steady increment in ulps (S stays even after a tie)
+    if (frac_cmp < 0) D = q;
+    else if (frac_cmp > 0) D = q + 1;
+    else D = (q & 1) ? q + 1 : q;
+    if (D == 0) continue;
+    if (frac_cmp == 0 && (S & 1)) continue;  // parity not yet settled
+    int64_t room;
+    if (up) room = ((int64_t)0xFFFFFF - S) / D - 1;     // keep S + m D + D <= 2^24 - 1
+    else room = (S - (int64_t)0x800000 - 1) / D - 1;    // keep S - m D - D >= 2^23
+    if (room <= 0) continue;
+    int64_t m = room < (int64_t)n ? room : (int64_t)n;
+    int64_t S2 = up ? S + m * D : S - m * D;
+    uint32_t nb = (bs & 0xFF800000u) | ((uint32_t)S2 & 0x7FFFFFu);
+#ifdef __CUDA_ARCH__
+    s = __uint_as_float(nb);
+#else
+    { union { float f; uint32_t u; } a4; a4.u = nb; s = a4.f; }
+#endif
+    n -= (uint32_t)m;
+  }
+  return s;
+}

@@ -1,0 +1,101 @@
+// Device-side argument structures shared by the kernel translation units and the runtime.
+#pragma once
+#include "pb_common.cuh"
+
+namespace pb {
+
+// One species' structure-of-arrays particle store (one of two ping-pong buffers).
+struct Soa {
+  float *x, *y, *vx, *vy, *vz;
+  uint8_t *cex;  // ions only, nullptr for electrons
+  uint32_t *id;
+};
+
+// Cubic B-spline in (log10 E -> log10 value) form, the SciPy UnivariateSpline of a
+// cross-section table (t: knots, c: coefficients, k = 3), clipped to [lo, hi].
+struct Spline {
+  const double *t, *c;
+  int nt;      // number of knots
+  double lo, hi;
+  int enabled;
+};
+
+// Everything the ion step kernel reads besides the particles.
+struct IonStepArgs {
+  Soa src, dst;
+  const int *num_src;
+  int *num_dst;
+  // fields
+  const float *Ex, *Ey, *Bx, *By, *Bz;
+  int has_B;
+  const uint8_t *isBound;
+  int nx, ny;
+  float dxf, dyf;
+  // push
+  double dt, qm, ds_lim;
+  const double *ds_max;   // device: max predicted displacement (n_sub)
+  int *n_sub_out;
+  int periodic;
+  float Lyf, Lxf;
+  // thresholds (float32 casts of Python floats, as NumPy compares)
+  float x_entry, x_exit, x_plume;
+  // tallies
+  int thermal_on, erosion_on;
+  float *Tmap;
+  double *damage;
+  float k_half_m;   // f32(0.5*m_ion)
+  float mw_f;       // f32(macro_weight)
+  float ccell_f;    // f32(C_cell)
+  float accel_f;    // f32(thermal_accel)
+  float q_f;        // f32(q)
+  float Y_f, Eth_f; // f32(Y_coeff), f32(E_th)
+  float dt_f;       // f32(dt) (SEE spawn offset)
+  Spline see_spline;
+  // SEE spawn records
+  uint64_t *see_key;   // (parent id << 32) | record index
+  float *see_xy;       // x, y per record
+  int *see_count;
+  int see_cap;
+  // exit diagnostics
+  float *angles;
+  int *angle_count;
+  int angle_cap;
+  double *exit_sums;     // [sum vx, sum |v|, sum E, sum |v| prim, n prim, sum |v| cex, n cex, sum vx^2, sum |v|^2]
+  unsigned long long *counters;  // [entered, crossed, exited_any, lost_to_grid, hits, cex_collisions, cex_ties]
+  // CEX
+  float rT_f;          // f32(Ly*1e-3)
+  double n0a;          // n0 * a_corr
+  double neut_vth;
+  Spline cx_spline;
+  uint64_t seed;
+  uint32_t step;
+  // counts for diagnostics / next deposit
+  int *ppc;            // int32 (ny, nx) current PPC map (trunc cells)
+  int *cnt;            // int32 (ny, nx) deposit counts for the next step (round cells)
+  // single-pass compaction
+  unsigned long long *tile_status;
+  int *tile_counter;
+  uint32_t *errflags;
+};
+
+struct EleStepArgs {
+  Soa src, dst;
+  const int *num_src;
+  int *num_dst;
+  const float *Ex, *Ey, *Bx, *By, *Bz;
+  int has_B;
+  const uint8_t *isBound;
+  int nx, ny;
+  float dxf, dyf;
+  double dt, qm, ds_lim;
+  const double *ds_max;
+  int *n_sub_out;
+  int periodic;
+  float Lyf, Lxf;
+  int *cnt;
+  unsigned long long *tile_status;
+  int *tile_counter;
+  uint32_t *errflags;
+};
+
+}  // namespace pb

@@ -1,0 +1,229 @@
+// Host-side construction of the multigrid hierarchy for the field solver.
+//
+// Level 0 is the fine grid with the node classes of build_sparse_matrix
+// (Python/physics_engine.py:525-552): Dirichlet (bound), Neumann copy rows (right
+// column, and top/bottom rows when y is not periodic), free otherwise.  Coarse levels
+// use bilinear prolongation P (coarse node (I,J) <-> fine (2I,2J); y wraps when the
+// fine level is periodic with even size) and Galerkin operators A_c = P^T A P stored
+// as 9-point stencils (y periodic on every level when the domain is).  Coarse nodes
+// centred on Dirichlet fine nodes, and coarse nodes no active fine node interpolates
+// from, are inactive.  Coarsening stops at <= max_coarse active nodes; that level is
+// solved with a dense inverse computed here by Cholesky factorisation.
+#pragma once
+#include <cmath>
+#include <cstdint>
+#include <stdexcept>
+#include <vector>
+
+namespace pb {
+namespace mghost {
+
+struct Level {
+  int ny = 0, nx = 0, per = 0, wrapP = 0, ncolors = 2;
+  std::vector<uint8_t> act;   // active nodes (level 0: free nodes)
+  std::vector<float> st;      // 9 * N stencil (coarse levels)
+};
+
+struct Hierarchy {
+  std::vector<Level> lev;
+  std::vector<int> cidx;      // coarsest active nodes
+  std::vector<float> cinvT;   // coarsest inverse, transposed
+};
+
+inline std::vector<uint8_t> node_classes(int ny, int nx, int periodic, const uint8_t* isBound) {
+  // 0 free, 1 Dirichlet, 2 Neumann
+  std::vector<uint8_t> c((size_t)ny * nx, 0);
+  for (int y = 0; y < ny; ++y)
+    for (int x = 0; x < nx; ++x) {
+      size_t i = (size_t)y * nx + x;
+      if (isBound[i]) { c[i] = 1; continue; }
+      if (x == nx - 1) { c[i] = 2; continue; }
+      if (!periodic && (y == 0 || y == ny - 1)) c[i] = 2;
+    }
+  return c;
+}
+
+// neighbour of (y, x) by (dy, dx) with optional y wrap; -1 outside
+inline long nb(int ny, int nx, int per, int y, int x, int dy, int dx) {
+  int yy = y + dy, xx = x + dx;
+  if (per) { if (yy < 0) yy += ny; else if (yy >= ny) yy -= ny; }
+  if (yy < 0 || yy >= ny || xx < 0 || xx >= nx) return -1;
+  return (long)yy * nx + xx;
+}
+
+struct Entry { long j; double v; };
+
+// row of the operator of level l (only active columns)
+inline void row_of(const Level& L, int level, const std::vector<uint8_t>& cls0, long i, std::vector<Entry>& out) {
+  out.clear();
+  int y = (int)(i / L.nx), x = (int)(i % L.nx);
+  if (level == 0) {
+    static const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
+    int nneu = 0;
+    for (int k = 0; k < 4; ++k) {
+      long j = nb(L.ny, L.nx, L.per, y, x, DY[k], DX[k]);
+      uint8_t c = j < 0 ? 2 : cls0[j];
+      if (c == 0) out.push_back({j, -1.0});
+      else if (c == 2) ++nneu;
+    }
+    out.push_back({i, (double)(4 - nneu)});
+    return;
+  }
+  size_t N = (size_t)L.ny * L.nx;
+  for (int k = 0; k < 9; ++k) {
+    float v = L.st[k * N + i];
+    if (v == 0.0f) continue;
+    long j = nb(L.ny, L.nx, L.per, y, x, k / 3 - 1, k % 3 - 1);
+    if (j >= 0 && L.act[j]) out.push_back({j, (double)v});
+  }
+}
+
+// prolongation weights of fine node (y, x) from the coarse level: up to 4 (c, w)
+inline int p_row(int nyf, int nxf, int wrap, int nyc, int nxc, int y, int x, long* c, double* w) {
+  int I0 = y >> 1, a = y & 1, J0 = x >> 1, b = x & 1;
+  int n = 0;
+  for (int da = 0; da <= a; ++da) {
+    int I = I0 + da;
+    if (I >= nyc) { if (wrap) I -= nyc; else continue; }
+    double wy = a ? 0.5 : 1.0;
+    for (int db = 0; db <= b; ++db) {
+      int J = J0 + db;
+      if (J >= nxc) continue;
+      double wx = b ? 0.5 : 1.0;
+      c[n] = (long)I * nxc + J;
+      w[n] = wy * wx;
+      ++n;
+    }
+  }
+  (void)nyf; (void)nxf;
+  return n;
+}
+
+inline int colors_for(const Level& L, int level) {
+  if (level == 0) return 2;
+  return (L.per && (L.ny & 1)) ? 6 : 4;
+}
+
+inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>& cls0, int max_coarse) {
+  Hierarchy H;
+  Level L0;
+  L0.ny = ny; L0.nx = nx; L0.per = periodic; L0.wrapP = 0; L0.ncolors = 2;
+  L0.act.resize((size_t)ny * nx);
+  for (size_t i = 0; i < L0.act.size(); ++i) L0.act[i] = cls0[i] == 0;
+  H.lev.push_back(L0);
+  std::vector<Entry> row;
+  while (true) {
+    Level& F = H.lev.back();
+    int level = (int)H.lev.size() - 1;
+    size_t nact = 0;
+    for (uint8_t a : F.act) nact += a;
+    int nyc = F.per ? (F.ny + 1) / 2 : F.ny / 2 + 1;
+    int nxc = F.nx / 2 + 1;
+    if ((long)nact <= max_coarse || F.ny < 4 || F.nx < 4 || (F.per && nyc < 3) || H.lev.size() >= 15) break;
+    int wrap = F.per && (F.ny % 2 == 0);
+    Level C;
+    C.ny = nyc; C.nx = nxc; C.per = F.per; C.wrapP = wrap;
+    size_t Nc = (size_t)nyc * nxc, Nf = (size_t)F.ny * F.nx;
+    C.act.assign(Nc, 0);
+    long pc[4]; double pw[4];
+    for (size_t f = 0; f < Nf; ++f) {
+      if (!F.act[f]) continue;
+      int n = p_row(F.ny, F.nx, wrap, nyc, nxc, (int)(f / F.nx), (int)(f % F.nx), pc, pw);
+      for (int k = 0; k < n; ++k) C.act[pc[k]] = 1;
+    }
+    if (level == 0)
+      for (size_t c = 0; c < Nc; ++c) {
+        int I = (int)(c / nxc), J = (int)(c % nxc);
+        int yf = 2 * I, xf = 2 * J;
+        if (yf < F.ny && xf < F.nx && cls0[(size_t)yf * F.nx + xf] == 1) C.act[c] = 0;
+      }
+    // Galerkin product, accumulated in double then stored as float stencils
+    std::vector<double> st(9 * Nc, 0.0);
+    long qc[4]; double qw[4];
+    bool ok = true;
+    for (size_t f = 0; f < Nf && ok; ++f) {
+      if (!F.act[f]) continue;
+      int n = p_row(F.ny, F.nx, wrap, nyc, nxc, (int)(f / F.nx), (int)(f % F.nx), pc, pw);
+      row_of(F, level, cls0, (long)f, row);
+      for (const Entry& e : row) {
+        int m = p_row(F.ny, F.nx, wrap, nyc, nxc, (int)(e.j / F.nx), (int)(e.j % F.nx), qc, qw);
+        for (int a = 0; a < n; ++a) {
+          if (!C.act[pc[a]]) continue;
+          int I = (int)(pc[a] / nxc), J = (int)(pc[a] % nxc);
+          for (int b = 0; b < m; ++b) {
+            if (!C.act[qc[b]]) continue;
+            int I2 = (int)(qc[b] / nxc), J2 = (int)(qc[b] % nxc);
+            int dI = I2 - I, dJ = J2 - J;
+            if (C.per) { if (dI > nyc / 2) dI -= nyc; else if (dI < -(nyc / 2)) dI += nyc; }
+            if (dI < -1 || dI > 1 || dJ < -1 || dJ > 1) { ok = false; break; }
+            st[(size_t)((dI + 1) * 3 + (dJ + 1)) * Nc + pc[a]] += pw[a] * e.v * qw[b];
+          }
+          if (!ok) break;
+        }
+        if (!ok) break;
+      }
+    }
+    if (!ok) break;  // coupling outside the 9-point pattern: keep the current level as coarsest
+    C.st.resize(9 * Nc);
+    for (size_t k = 0; k < 9 * Nc; ++k) C.st[k] = (float)st[k];
+    for (size_t c = 0; c < Nc; ++c)
+      if (C.act[c] && !(C.st[4 * Nc + c] > 0.0f)) C.act[c] = 0;
+    C.ncolors = colors_for(C, (int)H.lev.size());
+    H.lev.push_back(std::move(C));
+  }
+  // dense inverse of the coarsest operator (Cholesky, then L^-T L^-1)
+  Level& Lc = H.lev.back();
+  int level = (int)H.lev.size() - 1;
+  size_t N = (size_t)Lc.ny * Lc.nx;
+  std::vector<long> pos(N, -1);
+  for (size_t i = 0; i < N; ++i)
+    if (Lc.act[i]) { pos[i] = (long)H.cidx.size(); H.cidx.push_back((int)i); }
+  int n = (int)H.cidx.size();
+  if (n > 1024) throw std::runtime_error("coarsest level too large for the dense solve");
+  std::vector<double> A((size_t)n * n, 0.0);
+  for (int r = 0; r < n; ++r) {
+    row_of(Lc, level, cls0, H.cidx[r], row);
+    for (const Entry& e : row)
+      if (pos[e.j] >= 0) A[(size_t)r * n + pos[e.j]] += e.v;
+  }
+  // symmetrise (round-off) and factor
+  for (int r = 0; r < n; ++r)
+    for (int c = r + 1; c < n; ++c) {
+      double v = 0.5 * (A[(size_t)r * n + c] + A[(size_t)c * n + r]);
+      A[(size_t)r * n + c] = A[(size_t)c * n + r] = v;
+    }
+  std::vector<double> Lm((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    double s = A[(size_t)j * n + j];
+    for (int k = 0; k < j; ++k) s -= Lm[(size_t)j * n + k] * Lm[(size_t)j * n + k];
+    if (!(s > 0.0)) throw std::runtime_error("coarsest operator is not positive definite");
+    double d = std::sqrt(s);
+    Lm[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double t = A[(size_t)i * n + j];
+      for (int k = 0; k < j; ++k) t -= Lm[(size_t)i * n + k] * Lm[(size_t)j * n + k];
+      Lm[(size_t)i * n + j] = t / d;
+    }
+  }
+  // inverse columns: solve L L^T x = e_c
+  std::vector<double> inv((size_t)n * n, 0.0), yv(n);
+  for (int c = 0; c < n; ++c) {
+    for (int i = 0; i < n; ++i) {
+      double t = (i == c) ? 1.0 : 0.0;
+      for (int k = 0; k < i; ++k) t -= Lm[(size_t)i * n + k] * yv[k];
+      yv[i] = t / Lm[(size_t)i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+      double t = yv[i];
+      for (int k = i + 1; k < n; ++k) t -= Lm[(size_t)k * n + i] * inv[(size_t)k * n + c];
+      inv[(size_t)i * n + c] = t / Lm[(size_t)i * n + i];
+    }
+  }
+  H.cinvT.resize((size_t)n * n);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) H.cinvT[(size_t)c * n + r] = (float)inv[(size_t)r * n + c];
+  return H;
+}
+
+}  // namespace mghost
+}  // namespace pb

@@ -1,0 +1,600 @@
+// Particle kernels of the PIC-MCC step for sm_100a.
+//
+//  * boris_push_one      bilinear E (and B) gather + 2D3V Boris + drift, in the exact
+//                        operation order and precision of push_particles_boris_cpu
+//                        (Python/physics_engine.py:188-254): float32 cell indices,
+//                        float64 weights and velocity update, float32 drift in mm.
+//  * k_push_boris        one push over caller arrays (module-level function signature).
+//  * k_count_cells       NGP cell counts clip(rint(x/dx), 1, n-2), warp-aggregated.
+//  * k_rho_finalize      rho from counts: the exact float32 result of the reference's
+//                        sequential np.add.at (ions, then electrons).
+//  * k_substep_reduce    max predicted displacement of compute_particle_substeps (:928-966).
+//  * k_segment_hits      8-sample path absorption test (_segment_hits_grid, :1880-1901).
+//  * k_ion_step          the fused ion timestep: n_sub pushes, periodic wrap, final-cell and
+//                        path hits, impact heating, SEE spawn records, sputter damage, exit
+//                        diagnostics, stable compaction (single pass, decoupled look-back),
+//                        CEX collision, PPC and next-step deposit counts (:1166-1739).
+//  * k_ele_step          the fused electron timestep: pushes, wrap, purge (:1534-1561).
+#include "pb_kernels.cuh"
+
+namespace pb {
+
+constexpr int NT = 256;    // threads per block of the step kernels
+constexpr int IPT = 4;     // particles per thread (one float4 of each array)
+constexpr int TILE = NT * IPT;
+constexpr long long SPIN_LIMIT = 1ll << 22;  // polls of a predecessor tile (~1-2 s) before giving up
+
+// ------------------------------------------------------------------ field gather + push
+__device__ __forceinline__ double gather4(const float* __restrict__ F, size_t r0, size_t r1, int ix0, int ix1,
+                                          double w00, double w10, double w01, double w11) {
+  double a = DMUL((double)__ldg(F + r0 + ix0), w00);
+  double b = DMUL((double)__ldg(F + r0 + ix1), w10);
+  double c = DMUL((double)__ldg(F + r1 + ix0), w01);
+  double d = DMUL((double)__ldg(F + r1 + ix1), w11);
+  return DADD(DADD(DADD(a, b), c), d);
+}
+
+__device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, float& vy, float& vz,
+                                               const float* __restrict__ Ex, const float* __restrict__ Ey,
+                                               const float* __restrict__ Bx, const float* __restrict__ By,
+                                               const float* __restrict__ Bz, bool hasB, int nx, int ny,
+                                               float dxf, float dyf, double h, float dtf) {
+  float ixf = __fdiv_rn(x, dxf);
+  float iyf = __fdiv_rn(y, dyf);
+  int ix0 = clampi(np_f2i32(floorf(ixf)), 0, nx - 2);
+  int iy0 = clampi(np_f2i32(floorf(iyf)), 0, ny - 2);
+  double fx = DSUB((double)ixf, (double)ix0);
+  double fy = DSUB((double)iyf, (double)iy0);
+  int ix1 = min(ix0 + 1, nx - 1);
+  int iy1 = min(iy0 + 1, ny - 1);
+  double gx = DSUB(1.0, fx), gy = DSUB(1.0, fy);
+  double w00 = DMUL(gx, gy), w10 = DMUL(fx, gy), w01 = DMUL(gx, fy), w11 = DMUL(fx, fy);
+  size_t r0 = (size_t)iy0 * nx, r1 = (size_t)iy1 * nx;
+  double ex = gather4(Ex, r0, r1, ix0, ix1, w00, w10, w01, w11);
+  double ey = gather4(Ey, r0, r1, ix0, ix1, w00, w10, w01, w11);
+  double bx = 0.0, by = 0.0, bz = 0.0;
+  if (hasB) {
+    bx = gather4(Bx, r0, r1, ix0, ix1, w00, w10, w01, w11);
+    by = gather4(By, r0, r1, ix0, ix1, w00, w10, w01, w11);
+    bz = gather4(Bz, r0, r1, ix0, ix1, w00, w10, w01, w11);
+  }
+  double vmx = DADD((double)vx, DMUL(h, ex));
+  double vmy = DADD((double)vy, DMUL(h, ey));
+  double vmz = (double)vz;
+  double tx = DMUL(h, bx), ty = DMUL(h, by), tz = DMUL(h, bz);
+  double t2 = DADD(DADD(DMUL(tx, tx), DMUL(ty, ty)), DMUL(tz, tz));
+  double den = DADD(1.0, t2);
+  double sx = DDIV(DMUL(2.0, tx), den), sy = DDIV(DMUL(2.0, ty), den), sz = DDIV(DMUL(2.0, tz), den);
+  double vpx = DADD(vmx, DSUB(DMUL(vmy, tz), DMUL(vmz, ty)));
+  double vpy = DADD(vmy, DSUB(DMUL(vmz, tx), DMUL(vmx, tz)));
+  double vpz = DADD(vmz, DSUB(DMUL(vmx, ty), DMUL(vmy, tx)));
+  double wx = DADD(vmx, DSUB(DMUL(vpy, sz), DMUL(vpz, sy)));
+  double wy = DADD(vmy, DSUB(DMUL(vpz, sx), DMUL(vpx, sz)));
+  double wz = DADD(vmz, DSUB(DMUL(vpx, sy), DMUL(vpy, sx)));
+  vx = __double2float_rn(DADD(wx, DMUL(h, ex)));
+  vy = __double2float_rn(DADD(wy, DMUL(h, ey)));
+  vz = __double2float_rn(wz);
+  x = __fadd_rn(x, __fmul_rn(__fmul_rn(vx, dtf), 1000.0f));
+  y = __fadd_rn(y, __fmul_rn(__fmul_rn(vy, dtf), 1000.0f));
+}
+
+// n_sub from the reduced displacement: max(1, ceil(ds_max / max(ds_lim, 1e-30)))
+__device__ __forceinline__ int substep_count(double ds_max, double ds_lim, uint32_t* errflags) {
+  double lim = ds_lim > 1e-30 ? ds_lim : 1e-30;
+  double q = ceil(DDIV(ds_max, lim));
+  if (!(q == q)) { if (errflags) atomicOr(errflags, PB_EF_NAN_SUBSTEP); return 1; }
+  if (q > 65536.0) { if (errflags) atomicOr(errflags, PB_EF_SUBSTEP_CAP); return 65536; }
+  int n = (int)q;
+  return n < 1 ? 1 : n;
+}
+
+// ------------------------------------------------------------------ standalone push
+__global__ void k_push_boris(float* x, float* y, float* vx, float* vy, float* vz, const float* Ex,
+                             const float* Ey, const float* Bx, const float* By, const float* Bz, int n,
+                             int nx, int ny, float dxf, float dyf, double h, float dtf) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float a = x[i], b = y[i], c = vx[i], d = vy[i], e = vz[i];
+    boris_push_one(a, b, c, d, e, Ex, Ey, Bx, By, Bz, true, nx, ny, dxf, dyf, h, dtf);
+    x[i] = a; y[i] = b; vx[i] = c; vy[i] = d; vz[i] = e;
+  }
+}
+
+// ------------------------------------------------------------------ NGP counting
+__device__ __forceinline__ void warp_count_add(int* cnt, int cell, bool valid) {
+  unsigned act = __activemask();
+  unsigned key = valid ? (unsigned)cell : 0xFFFFFFFFu;
+  unsigned peers = __match_any_sync(act, key);
+  int leader = __ffs(peers) - 1;
+  if (valid && (int)(threadIdx.x & 31) == leader) atomicAdd(cnt + cell, __popc(peers));
+}
+
+__device__ __forceinline__ int deposit_cell(float x, float y, float dxf, float dyf, int nx, int ny) {
+  int ix = cell_round32(x, dxf, 1, nx - 2);
+  int iy = cell_round32(y, dyf, 1, ny - 2);
+  return iy * nx + ix;
+}
+
+__global__ void k_count_cells(const float* __restrict__ x, const float* __restrict__ y, const int* n_dev, int n_host,
+                              int start, int* cnt, int nx, int ny, float dxf, float dyf) {
+  int n = n_dev ? *n_dev : n_host;
+  int base = blockIdx.x * blockDim.x;
+  for (int i0 = base; i0 < n - start; i0 += gridDim.x * blockDim.x) {
+    int i = i0 + threadIdx.x + start;
+    bool v = i < n;
+    int c = v ? deposit_cell(x[i], y[i], dxf, dyf, nx, ny) : 0;
+    warp_count_add(cnt, c, v);
+  }
+}
+
+// rho = seq(seq(rho0, +c, k_ion), -c, k_ele); counts are cleared for reuse
+__global__ void k_rho_finalize(float* rho, int* cnt_i, int* cnt_e, int G, float cd, int accumulate) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G; i += gridDim.x * blockDim.x) {
+    float s = accumulate ? rho[i] : 0.0f;
+    int ki = cnt_i ? cnt_i[i] : 0;
+    int ke = cnt_e ? cnt_e[i] : 0;
+    if (ki) s = seq_add_f32(s, cd, (uint32_t)ki);
+    if (ke) s = seq_add_f32(s, -cd, (uint32_t)ke);
+    rho[i] = s;
+    if (cnt_i) cnt_i[i] = 0;
+    if (cnt_e) cnt_e[i] = 0;
+  }
+}
+
+// ------------------------------------------------------------------ substep reduction
+__device__ __forceinline__ double gather_sub(const float* __restrict__ F, size_t r0, size_t r1, long long ix0,
+                                             long long ix1, double fx, double fy) {
+  double gx = DSUB(1.0, fx), gy = DSUB(1.0, fy);
+  double a = DMUL(DMUL((double)__ldg(F + r0 + ix0), gx), gy);
+  double b = DMUL(DMUL((double)__ldg(F + r0 + ix1), fx), gy);
+  double c = DMUL(DMUL((double)__ldg(F + r1 + ix0), gx), fy);
+  double d = DMUL(DMUL((double)__ldg(F + r1 + ix1), fx), fy);
+  return DADD(DADD(DADD(a, b), c), d);
+}
+
+__device__ __forceinline__ double predicted_ds(float x, float y, float vx, float vy, float vz,
+                                               const float* Ex, const float* Ey, int nx, int ny, float dxf,
+                                               float dyf, double qm, float dtf, double dt2) {
+  float ixf = __fdiv_rn(x, dxf), iyf = __fdiv_rn(y, dyf);
+  long long ix0 = clampll(np_f2i64(floorf(ixf)), 0, nx - 2);
+  long long iy0 = clampll(np_f2i64(floorf(iyf)), 0, ny - 2);
+  double fx = DSUB((double)ixf, (double)ix0), fy = DSUB((double)iyf, (double)iy0);
+  size_t r0 = (size_t)iy0 * nx, r1 = (size_t)(iy0 + 1) * nx;
+  double ex = gather_sub(Ex, r0, r1, ix0, ix0 + 1, fx, fy);
+  double ey = gather_sub(Ey, r0, r1, ix0, ix0 + 1, fx, fy);
+  double ax = DMUL(qm, ex), ay = DMUL(qm, ey);
+  double a_mag = sqrt(DADD(DMUL(ax, ax), DMUL(ay, ay)));
+  float v_mag = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+  return DADD((double)__fmul_rn(v_mag, dtf), DMUL(DMUL(0.5, a_mag), dt2));
+}
+
+__global__ void k_substep_reduce(const float* __restrict__ x, const float* __restrict__ y,
+                                 const float* __restrict__ vx, const float* __restrict__ vy,
+                                 const float* __restrict__ vz, const int* n_dev, int n_host, const float* Ex,
+                                 const float* Ey, int nx, int ny, float dxf, float dyf, double qm, float dtf,
+                                 double dt2, unsigned long long* ds_max_bits) {
+  int n = n_dev ? *n_dev : n_host;
+  unsigned long long m = 0ull;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double ds = predicted_ds(x[i], y[i], vx[i], vy[i], vz[i], Ex, Ey, nx, ny, dxf, dyf, qm, dtf, dt2);
+    unsigned long long b = (unsigned long long)__double_as_longlong(ds);
+    m = b > m ? b : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long v = __shfl_down_sync(0xFFFFFFFFu, m, o);
+    m = v > m ? v : m;
+  }
+  __shared__ unsigned long long sm[32];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0ull;
+    for (int o = 16; o > 0; o >>= 1) {
+      unsigned long long v = __shfl_down_sync(0xFFFFFFFFu, m, o);
+      m = v > m ? v : m;
+    }
+    if (threadIdx.x == 0 && m) atomicMax(ds_max_bits, m);
+  }
+}
+
+// n_sub for the host-facing report: read ds_max, write n_sub
+__global__ void k_substep_finish(const double* ds_max, double ds_lim, int* n_sub_out, uint32_t* errflags) {
+  *n_sub_out = substep_count(*ds_max, ds_lim, errflags);
+}
+
+// ------------------------------------------------------------------ path absorption
+struct SegHit { bool hit; int ix, iy; };
+
+__device__ __forceinline__ SegHit segment_hit(const uint8_t* __restrict__ isBound, int nx, int ny, float dxf,
+                                              float dyf, float x0, float y0, float x1, float y1) {
+  SegHit r;
+  r.hit = false;
+  r.ix = cell_round(x1, dxf, 0, nx - 1);
+  r.iy = cell_round(y1, dyf, 0, ny - 1);
+  float ddx = __fsub_rn(x1, x0), ddy = __fsub_rn(y1, y0);
+#pragma unroll
+  for (int i = 1; i <= 8; ++i) {
+    float f = (float)i * 0.125f;
+    float xi = __fadd_rn(x0, __fmul_rn(ddx, f));
+    float yi = __fadd_rn(y0, __fmul_rn(ddy, f));
+    int cx = cell_round(xi, dxf, 0, nx - 1);
+    int cy = cell_round(yi, dyf, 0, ny - 1);
+    if (!r.hit && __ldg(isBound + (size_t)cy * nx + cx)) { r.hit = true; r.ix = cx; r.iy = cy; }
+  }
+  return r;
+}
+
+__global__ void k_segment_hits(const uint8_t* isBound, int nx, int ny, float dxf, float dyf, const float* x0,
+                               const float* y0, const float* x1, const float* y1, int n, uint8_t* hit,
+                               int64_t* hix, int64_t* hiy) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    SegHit s = segment_hit(isBound, nx, ny, dxf, dyf, x0[i], y0[i], x1[i], y1[i]);
+    hit[i] = s.hit;
+    hix[i] = s.ix;
+    hiy[i] = s.iy;
+  }
+}
+
+// ------------------------------------------------------------------ cross-section splines
+// de Boor evaluation of a cubic B-spline (FITPACK splev convention, knots t[0..nt-1],
+// coefficients c[0..nt-5]); x is clipped into the base interval.
+__device__ double spline_eval(const Spline& s, double x) {
+  const int k = 3;
+  int n = s.nt;
+  int l = k;
+  while (l < n - k - 2 && x >= s.t[l + 1]) ++l;
+  double d[4];
+  for (int j = 0; j <= k; ++j) d[j] = s.c[j + l - k];
+  for (int r = 1; r <= k; ++r)
+    for (int j = k; j >= r; --j) {
+      double tl = s.t[j + l - k], tr = s.t[j + 1 + l - r];
+      double alpha = (x - tl) / (tr - tl);
+      d[j] = (1.0 - alpha) * d[j - 1] + alpha * d[j];
+    }
+  return d[k];
+}
+
+// 10 ** spline(clip(log10(max(E, 1e-30)), lo, hi))  (lookup_user_cs, physics_engine.py:475-484)
+__device__ __forceinline__ double user_cs(const Spline& s, float E) {
+  float le = log10f(np_maxf(E, 1e-30f));
+  double l = (double)le;
+  l = l < s.lo ? s.lo : (l > s.hi ? s.hi : l);
+  return pow(10.0, spline_eval(s, l));
+}
+
+// ------------------------------------------------------------------ tile scan / look-back
+constexpr unsigned long long FLAG_AGG = 1ull << 62, FLAG_PRE = 2ull << 62, VAL_MASK = (1ull << 62) - 1;
+
+// Exclusive prefix of tile `tile` given its aggregate (decoupled look-back, warp-parallel).
+// Called by warp 0; returns the prefix in every lane.  Waits are bounded.
+__device__ long long lookback_warp(unsigned long long* status, int tile, int agg, uint32_t* errflags) {
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) atomicExch(status, FLAG_PRE | (unsigned long long)agg);
+    return 0;
+  }
+  if (lane == 0) atomicExch(status + tile, FLAG_AGG | (unsigned long long)agg);
+  long long excl = 0;
+  int t = tile - 1;
+  while (true) {
+    int tt = t - lane;
+    unsigned long long v = FLAG_PRE;  // before tile 0: an inclusive prefix of 0
+    if (tt >= 0) {
+      long long spin = 0;
+      do {
+        v = *((volatile unsigned long long*)(status + tt));
+      } while ((v >> 62) == 0 && ++spin < SPIN_LIMIT);
+      if ((v >> 62) == 0) { atomicOr(errflags, PB_EF_SPIN_TIMEOUT); v = FLAG_PRE; }
+    }
+    unsigned pre = __ballot_sync(0xFFFFFFFFu, (v >> 62) == 2);
+    int stop = pre ? __ffs(pre) - 1 : 31;  // nearest lane holding an inclusive prefix
+    long long val = (lane <= stop) ? (long long)(v & VAL_MASK) : 0;
+    for (int o = 16; o > 0; o >>= 1) val += __shfl_down_sync(0xFFFFFFFFu, val, o);
+    val = __shfl_sync(0xFFFFFFFFu, val, 0);
+    excl += val;
+    if (pre) break;
+    t -= 32;
+  }
+  if (lane == 0) atomicExch(status + tile, FLAG_PRE | (unsigned long long)(excl + agg));
+  return excl;
+}
+
+// Block-wide exclusive scan of keep flags staged in shared memory (index order), plus
+// the global base via look-back.  Fills rank[] and returns the number kept in the tile.
+template <int NTHR, int TILE_SZ>
+__device__ __forceinline__ int tile_compact_ranks(const uint8_t* keep, int* rank, int tile, int t0, int n,
+                                                  unsigned long long* status, int* num_dst, long long& base,
+                                                  uint32_t* errflags) {
+  constexpr int PER = TILE_SZ / NTHR;
+  __shared__ int sm[NTHR / 32];
+  __shared__ long long sbase;
+  __shared__ int stotal;
+  int k0 = threadIdx.x * PER;
+  int c = 0;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) c += keep[k0 + q];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int inc = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) sm[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < NTHR / 32 ? sm[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xFFFFFFFFu, v, o);
+      if (lane >= o) v += t;
+    }
+    if (lane < NTHR / 32) sm[lane] = v;
+    int total = __shfl_sync(0xFFFFFFFFu, v, NTHR / 32 - 1);
+    long long b = lookback_warp(status, tile, total, errflags);
+    if (lane == 0) {
+      sbase = b;
+      stotal = total;
+      if (t0 + TILE_SZ >= n) *num_dst = (int)(b + total);
+    }
+  }
+  __syncthreads();
+  int ex = (w ? sm[w - 1] : 0) + inc - c;
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    rank[k0 + q] = ex;
+    ex += keep[k0 + q];
+  }
+  base = sbase;
+  int tot = stotal;
+  __syncthreads();
+  return tot;
+}
+
+// ------------------------------------------------------------------ fused ion step
+// Tile of TILE particles: item k of the tile is particle t0 + k; thread t handles
+// k = t, t + NT, ... (coalesced loads), results are staged in shared memory, ranked by a
+// block scan in index order and written compacted (stable) at the global offset.
+struct IonStage {
+  float x[TILE], y[TILE], vx[TILE], vy[TILE], vz[TILE];
+  uint32_t id[TILE];
+  int rank[TILE];
+  uint8_t cex[TILE], keep[TILE];
+};
+
+__global__ void __launch_bounds__(NT) k_ion_step(IonStepArgs a) {
+  __shared__ IonStage st;
+  __shared__ int sm_tile;
+  const int n = *a.num_src;
+  const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
+  const double dt_sub = DDIV(a.dt, (double)n_sub);
+  const double h = DMUL(DMUL(0.5, a.qm), dt_sub);
+  const float dtf = __double2float_rn(dt_sub);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.n_sub_out = n_sub;
+  const float pi_f = 3.14159265358979323846f;
+  unsigned long long cnt[7] = {0, 0, 0, 0, 0, 0, 0};
+  double sums[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+
+  while (true) {
+    if (threadIdx.x == 0) sm_tile = atomicAdd(a.tile_counter, 1);
+    __syncthreads();
+    const int tile = sm_tile;
+    const int t0 = tile * TILE;
+    if (t0 >= n) break;
+#pragma unroll 1
+    for (int k = threadIdx.x; k < TILE; k += NT) {
+      const int i = t0 + k;
+      uint8_t kp = 0;
+      if (i < n) {
+        float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
+        uint8_t cx = a.src.cex[i];
+        const uint32_t pid = a.src.id[i];
+        const float x0 = x, y0 = y;
+        for (int s = 0; s < n_sub; ++s)
+          boris_push_one(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.has_B, a.nx, a.ny, a.dxf, a.dyf, h, dtf);
+        if (a.periodic) y = np_modf_pos(y, a.Lyf);
+        // entered the optics (:1316-1324)
+        if (x0 < a.x_entry && x >= a.x_entry && vx > 0.0f) cnt[0]++;
+        // final-cell and path hits (:1326-1336)
+        int icx = cell_round(x, a.dxf, 0, a.nx - 1), icy = cell_round(y, a.dyf, 0, a.ny - 1);
+        bool hit_final = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
+        SegHit sh = segment_hit(a.isBound, a.nx, a.ny, a.dxf, a.dyf, x0, y0, x, y);
+        bool hit = hit_final || sh.hit;
+        int imx = sh.hit ? sh.ix : icx, imy = sh.hit ? sh.iy : icy;
+        bool oob = (x < 0.0f) || (x > a.x_plume) || (x != x);
+        if (!a.periodic) oob = oob || (y < 0.0f) || (y > a.Lyf);
+        if (hit) cnt[4]++;
+        if (hit && !oob) cnt[3]++;
+        // heating, SEE, sputtering for hits beyond x = 0.25 mm (:1359-1449)
+        if (hit && x > 0.25f) {
+          float v2 = __fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz));
+          size_t cell = (size_t)imy * a.nx + imx;
+          if (a.thermal_on) {
+            float Ej = __fmul_rn(__fmul_rn(a.k_half_m, v2), a.mw_f);
+            float dT = __fmul_rn(__fdiv_rn(Ej, a.ccell_f), a.accel_f);
+            atomicAdd(a.Tmap + cell, dT);
+          }
+          float E_eV = __fdiv_rn(__fmul_rn(a.k_half_m, v2), a.q_f);
+          double gamma;
+          if (a.see_spline.enabled) {
+            double g = user_cs(a.see_spline, E_eV);
+            gamma = g < 0.0 ? 0.0 : (g > 1.0 ? 1.0 : g);
+          } else {
+            float g = __fadd_rn(0.05f, __fmul_rn(1e-4f, E_eV));
+            g = (g != g) ? g : (g < 0.0f ? 0.0f : (g > 1.0f ? 1.0f : g));
+            gamma = (double)g;
+          }
+          double u = philox_uniform(a.seed, pid, SITE_SEE_SPAWN, a.step, 0);
+          if (u < gamma) {
+            int r = atomicAdd(a.see_count, 1);
+            if (r < a.see_cap) {
+              float off_x = __fdiv_rn(__fmul_rn(__fmul_rn(vx, a.dt_f), 1000.0f), 1.5f);
+              float off_y = __fdiv_rn(__fmul_rn(__fmul_rn(vy, a.dt_f), 1000.0f), 1.5f);
+              a.see_xy[2 * r] = __fsub_rn(x, off_x);
+              a.see_xy[2 * r + 1] = __fsub_rn(y, off_y);
+              a.see_key[r] = ((uint64_t)pid << 32) | (uint32_t)r;
+            } else {
+              atomicOr(a.errflags, PB_EF_SEE_OVERFLOW);
+            }
+          }
+          if (a.erosion_on && E_eV > a.Eth_f) {
+            float dmg = __fmul_rn(__fmul_rn(a.Y_f, __fsub_rn(E_eV, a.Eth_f)), a.mw_f);
+            atomicAdd(a.damage + cell, (double)dmg);
+          }
+        }
+        // exit plane diagnostics (:1451-1494), pre-collision velocities and flag
+        bool crossed = (x0 <= a.x_exit) && (x > a.x_exit) && (vx > 0.0f);
+        if ((x > a.x_exit) && (vx > 0.0f)) cnt[2]++;
+        if (crossed) {
+          cnt[1]++;
+          float ve = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+          float Ee = __fdiv_rn(__fmul_rn(a.k_half_m, __fmul_rn(ve, ve)), a.q_f);
+          sums[0] += vx; sums[1] += ve; sums[2] += Ee;
+          sums[7] += (double)vx * vx; sums[8] += (double)ve * ve;
+          if (cx) { sums[5] += ve; sums[6] += 1.0; } else { sums[3] += ve; sums[4] += 1.0; }
+          int r = atomicAdd(a.angle_count, 1);
+          float ang = __fdiv_rn(__fmul_rn(fabsf(atan2f(vy, vx)), 180.0f), pi_f);
+          if (r < a.angle_cap) a.angles[r] = ang; else atomicOr(a.errflags, PB_EF_ANGLE_OVERFLOW);
+        }
+        bool alive = !(hit || oob);
+        kp = alive && ((x <= a.x_plume) || (vx < 0.0f));
+        if (kp) {
+          // CEX null-collision MCC on primaries (:1682-1739)
+          if (!cx && x >= 1.0f && x <= a.Lxf) {
+            float z_m = __fmul_rn(__fsub_rn(x, 1.0f), 1e-3f);
+            z_m = z_m >= 0.0f ? z_m : 0.0f;
+            float r_m = __fmul_rn(y, 1e-3f);
+            float zr = __fadd_rn(z_m, a.rT_f);
+            float R = sqrtf(__fadd_rn(__fmul_rn(r_m, r_m), __fmul_rn(zr, zr)));
+            float th = atan2f(r_m, zr);
+            float Rm = np_maxf(R, 1e-12f);
+            float q1 = __fdiv_rn(a.rT_f, Rm);
+            float geo = __fsub_rn(1.0f, __fdiv_rn(1.0f, sqrtf(__fadd_rn(1.0f, __fmul_rn(q1, q1)))));
+            double nl = DMUL(DMUL(a.n0a, (double)geo), (double)cosf(th));
+            nl = np_maxd(nl, 0.0);
+            float vm = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
+            float g = np_maxf(vm, 1.0f);
+            double sigma;
+            if (a.cx_spline.enabled) {
+              float Ec = __fdiv_rn(__fmul_rn(a.k_half_m, __fmul_rn(g, g)), a.q_f);
+              sigma = user_cs(a.cx_spline, Ec);
+            } else {
+              float t = __fadd_rn(__fmul_rn(-0.8821f, logf(g)), 15.1262f);
+              sigma = (double)__fmul_rn(__fmul_rn(t, t), 1e-20f);
+            }
+            double prob = DSUB(1.0, exp(DMUL(DMUL(DMUL(-nl, sigma), (double)g), a.dt)));
+            double u = philox_uniform(a.seed, pid, SITE_CEX_U, a.step, 0);
+            if (fabs(u - prob) <= fabs(prob) * 8.9e-16 + 1e-300) cnt[6]++;
+            if (u < prob) {
+              cnt[5]++;
+              u32x4 r0 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 0);
+              u32x4 r1 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 1);
+              u32x4 r2 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 2);
+              u32x4 r3 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 3);
+              u32x4 r4 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 4);
+              double fmx = DMUL(2.0, DSUB(DADD(DADD(u53(r0.x, r0.y), u53(r0.z, r0.w)), u53(r1.x, r1.y)), 1.5));
+              double fmy = DMUL(2.0, DSUB(DADD(DADD(u53(r1.z, r1.w), u53(r2.x, r2.y)), u53(r2.z, r2.w)), 1.5));
+              double fmz = DMUL(2.0, DSUB(DADD(DADD(u53(r3.x, r3.y), u53(r3.z, r3.w)), u53(r4.x, r4.y)), 1.5));
+              vx = __double2float_rn(DMUL(a.neut_vth, fmx));
+              vy = __double2float_rn(DMUL(a.neut_vth, fmy));
+              vz = __double2float_rn(DMUL(a.neut_vth, fmz));
+              cx = 1;
+            }
+          }
+          // PPC map with truncated cells (:1749-1757)
+          long long tx = clampll(np_f2i64(truncf(__fdiv_rn(x, a.dxf))), 0, a.nx - 1);
+          long long ty = clampll(np_f2i64(truncf(__fdiv_rn(y, a.dyf))), 0, a.ny - 1);
+          atomicAdd(a.ppc + ty * a.nx + tx, 1);
+        }
+        st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
+        st.cex[k] = cx; st.id[k] = pid;
+      }
+      st.keep[k] = kp;
+      // next-step deposit counts (warp-aggregated: consecutive lanes, near-sorted cells)
+      int c = kp ? deposit_cell(st.x[k], st.y[k], a.dxf, a.dyf, a.nx, a.ny) : 0;
+      warp_count_add(a.cnt, c, kp != 0);
+    }
+    __syncthreads();
+    long long base;
+    tile_compact_ranks<NT, TILE>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
+    for (int k = threadIdx.x; k < TILE; k += NT) {
+      if (!st.keep[k]) continue;
+      long long pos = base + st.rank[k];
+      a.dst.x[pos] = st.x[k]; a.dst.y[pos] = st.y[k];
+      a.dst.vx[pos] = st.vx[k]; a.dst.vy[pos] = st.vy[k]; a.dst.vz[pos] = st.vz[k];
+      a.dst.cex[pos] = st.cex[k]; a.dst.id[pos] = st.id[k];
+    }
+    __syncthreads();
+  }
+  // flush per-thread tallies
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    unsigned long long v = cnt[j];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(a.counters + j, v);
+  }
+#pragma unroll
+  for (int j = 0; j < 9; ++j) {
+    double v = sums[j];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(a.exit_sums + j, v);
+  }
+}
+
+// ------------------------------------------------------------------ fused electron step
+struct EleStage {
+  float x[TILE], y[TILE], vx[TILE], vy[TILE], vz[TILE];
+  uint32_t id[TILE];
+  int rank[TILE];
+  uint8_t keep[TILE];
+};
+
+__global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
+  __shared__ EleStage st;
+  __shared__ int sm_tile;
+  const int n = *a.num_src;
+  const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
+  const double dt_sub = DDIV(a.dt, (double)n_sub);
+  const double h = DMUL(DMUL(0.5, a.qm), dt_sub);
+  const float dtf = __double2float_rn(dt_sub);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.n_sub_out = n_sub;
+  while (true) {
+    if (threadIdx.x == 0) sm_tile = atomicAdd(a.tile_counter, 1);
+    __syncthreads();
+    const int tile = sm_tile;
+    const int t0 = tile * TILE;
+    if (t0 >= n) break;
+#pragma unroll 1
+    for (int k = threadIdx.x; k < TILE; k += NT) {
+      const int i = t0 + k;
+      uint8_t kp = 0;
+      if (i < n) {
+        float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
+        for (int s = 0; s < n_sub; ++s)
+          boris_push_one(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.has_B, a.nx, a.ny, a.dxf, a.dyf, h, dtf);
+        if (a.periodic) y = np_modf_pos(y, a.Lyf);
+        int icx = cell_round(x, a.dxf, 0, a.nx - 1), icy = cell_round(y, a.dyf, 0, a.ny - 1);
+        bool dead = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
+        dead = dead || (x < 0.0f) || (x > a.Lxf) || (y < 0.0f) || (y > a.Lyf) || (x != x);
+        kp = !dead;
+        st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
+        st.id[k] = a.src.id[i];
+      }
+      st.keep[k] = kp;
+      int c = kp ? deposit_cell(st.x[k], st.y[k], a.dxf, a.dyf, a.nx, a.ny) : 0;
+      warp_count_add(a.cnt, c, kp != 0);
+    }
+    __syncthreads();
+    long long base;
+    tile_compact_ranks<NT, TILE>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
+    for (int k = threadIdx.x; k < TILE; k += NT) {
+      if (!st.keep[k]) continue;
+      long long pos = base + st.rank[k];
+      a.dst.x[pos] = st.x[k]; a.dst.y[pos] = st.y[k];
+      a.dst.vx[pos] = st.vx[k]; a.dst.vy[pos] = st.vy[k]; a.dst.vz[pos] = st.vz[k];
+      a.dst.id[pos] = st.id[k];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace pb

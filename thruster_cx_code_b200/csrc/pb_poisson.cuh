@@ -1,0 +1,60 @@
+// Poisson solver data layout (device pointers) shared by the kernel and the host builder.
+#pragma once
+#include <cstdint>
+
+namespace pb {
+
+constexpr int MG_MAX_LEVELS = 16;
+enum NodeClass : uint8_t { NC_FREE = 0, NC_DIR = 1, NC_NEU = 2 };
+
+struct MgLevel {
+  int ny, nx;
+  int per;        // y is periodic on this level's operator
+  int wrapP;      // prolongation from the next coarser level wraps in y
+  int ncolors;    // smoother colours (2 on level 0, 4 or 6 on coarse levels)
+  const uint8_t* act;     // active (unknown) nodes; level 0: class array instead
+  const float* st;        // 9-point stencil, st[k * N + i], k = (dI+1)*3 + (dJ+1); null on level 0
+  float *r, *z;           // right-hand side and correction on this level
+};
+
+struct PoissonArgs {
+  // fine grid
+  int ny, nx, periodic;
+  const uint8_t* cls;     // NodeClass per node (level 0)
+  const double* Vfixed;
+  const float* rho;
+  double* V;              // Picard state (all nodes)
+  double* x;              // linear-solve solution (Vnew), warm start across solves
+  double* f;              // reduced right-hand side
+  double* dirsum;         // sum of Dirichlet neighbour values
+  float *r32, *z32, *p32, *q32, *e32;
+  float *Ex, *Ey;
+  // physics scalars (host double precision, as the reference computes them)
+  double coeff;           // (dx*1e-3)^2 / eps0
+  double qn0_neg;         // -q * n0
+  double V_plasma, Te_up;
+  double omega_keep, omega_new;   // 1 - omega, omega
+  // np.gradient spacings: hx = dx*1e-3, two_hx = 2.*hx, ...; two_hy_per = (2.0*dy)*1e-3
+  double hx, two_hx, hy, two_hy, two_hy_per;
+  int iterations;         // Picard iterations
+  int compute_field;      // write Ex, Ey at the end
+  // solver control
+  double tol;             // relative FP64 residual target ||f - A x|| / ||f||
+  double tol_inner;       // relative residual reduction of each FP32 MG-PCG solve
+  int max_outer, max_inner;
+  int nu;                 // smoothing sweeps per level
+  // hierarchy
+  int nlevels;            // including level 0 and the coarsest
+  int first_small;        // first level handled by a single block
+  MgLevel lev[MG_MAX_LEVELS];
+  int nc;                 // coarsest active count
+  const int* cidx;        // coarsest active node indices
+  const float* cinvT;     // coarsest inverse, transposed (nc x nc)
+  // reductions and barrier
+  double* partials;       // 4 * gridDim doubles
+  unsigned int* bar;      // [count, generation]
+  uint32_t* errflags;
+  double* stats;          // [outer its, inner its, final rel residual, solves] accumulated
+};
+
+}  // namespace pb

@@ -1,0 +1,1083 @@
+// libpbemcs runtime: device state of one simulation instance, the timestep sequence and
+// the C-ABI (include/pbemcs.h).  Unity build: the kernel sources are included here.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pbemcs.h"
+#include "pb_particles.cu"
+#include "pb_poisson.cu"
+#include "pb_misc.cu"
+#include "pb_mg_host.hpp"
+
+namespace pb {
+
+static thread_local std::string g_err;
+
+static int32_t fail(int32_t code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return fail(PB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T>
+static cudaError_t dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  return cudaMalloc((void**)p, n * sizeof(T));
+}
+template <typename T>
+static void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+struct Species {
+  Soa buf[2] = {};
+  int cur = 0;
+  int cap = 0;
+  bool ion = false;
+};
+
+struct DevLevel {
+  int ny = 0, nx = 0, per = 0, wrapP = 0, ncolors = 2;
+  uint8_t* act = nullptr;
+  float* st = nullptr;
+  float* r = nullptr;
+  float* z = nullptr;
+};
+
+struct Sim {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  // grid
+  int ny = 0, nx = 0, periodic = 0, ngrids = 0;
+  double *V = nullptr, *Vnew = nullptr, *Vfixed = nullptr, *Vdc = nullptr, *damage = nullptr, *eroded = nullptr;
+  double *accum_ppc = nullptr, *f = nullptr, *dirsum = nullptr;
+  float *Ex = nullptr, *Ey = nullptr, *rho = nullptr, *Tmap = nullptr;
+  float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *e32 = nullptr;
+  uint8_t *isBound = nullptr, *cls = nullptr;
+  uint16_t* gridmask = nullptr;
+  int *ppc = nullptr, *cnt_i = nullptr, *cnt_e = nullptr;
+  // multigrid
+  std::vector<DevLevel> lev;
+  int first_small = 1;
+  int nc = 0;
+  int* cidx = nullptr;
+  float* cinvT = nullptr;
+  double* partials = nullptr;
+  unsigned int* bar = nullptr;
+  double* pstats = nullptr;
+  int pgrid = 0;
+  // particles
+  Species sp[2];
+  int* counts = nullptr;         // [ion buf0, ion buf1, ele buf0, ele buf1]
+  uint32_t* next_ids = nullptr;  // [ion, electron]
+  // per-step scratch
+  unsigned long long* tile_status = nullptr;
+  int* tile_counter = nullptr;   // [ion, ele]
+  size_t tile_cap = 0;
+  uint64_t* see_key = nullptr;
+  float* see_xy = nullptr;
+  int see_cap = 0;
+  int* see_count = nullptr;
+  float* angles = nullptr;
+  uint64_t* angle_scratch = nullptr;
+  int angle_cap = 0;
+  int* angle_count = nullptr;
+  unsigned long long* ds_bits = nullptr;  // [ion, ele]
+  int* n_sub = nullptr;                    // [ion, ele]
+  int* inj = nullptr;                      // 7 ints
+  int* see_spawned = nullptr;
+  // sort
+  uint32_t *skey[2] = {nullptr, nullptr}, *sval[2] = {nullptr, nullptr}, *shist = nullptr;
+  size_t sort_cap = 0, hist_cap = 0;
+  // report
+  pb_step_report* rep_dev = nullptr;
+  pb_step_report* rep_host = nullptr;
+  // settings
+  double tol = 1e-10, tol_inner = 1e-5;
+  int max_outer = 8, max_inner = 40, nu = 1, max_coarse = 256;
+  uint64_t seed = 0;
+  bool counts_valid = false;
+  bool domain_set = false;
+  int host_num[2] = {0, 0};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  // optional per-phase timing: events at 7 marks per step, reused across runs
+  int profiling = 0;
+  std::vector<cudaEvent_t> marks;
+  size_t mark_used = 0;
+  long long launches = 0;   // kernels enqueued by the last pb_sim_run / pb_sim_step
+  double sp_dx = 1.0, sp_dy = 1.0;   // grid spacing of the last step (cell keys of the sort)
+};
+
+// ------------------------------------------------------------------ helpers
+static int grid_for(const Sim* s, long n, int bs, int per_sm = 8) {
+  long g = (n + bs - 1) / bs;
+  long cap = (long)s->num_sms * per_sm;
+  if (g > cap) g = cap;
+  return (int)std::max(1L, g);
+}
+
+static int32_t alloc_species(Sim* s, int k, int cap, int keep_n) {
+  Species& S = s->sp[k];
+  if (cap <= S.cap) return PB_OK;
+  cap = ((cap + 1023) / 1024) * 1024;
+  for (int b = 0; b < 2; ++b) {
+    Soa nb{};
+    CK(dalloc(&nb.x, cap)); CK(dalloc(&nb.y, cap)); CK(dalloc(&nb.vx, cap));
+    CK(dalloc(&nb.vy, cap)); CK(dalloc(&nb.vz, cap)); CK(dalloc(&nb.id, cap));
+    if (S.ion) CK(dalloc(&nb.cex, cap));
+    Soa& ob = S.buf[b];
+    if (ob.x && keep_n > 0 && b == S.cur) {
+      size_t n4 = (size_t)keep_n * 4;
+      CK(cudaMemcpyAsync(nb.x, ob.x, n4, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(nb.y, ob.y, n4, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(nb.vx, ob.vx, n4, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(nb.vy, ob.vy, n4, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(nb.vz, ob.vz, n4, cudaMemcpyDeviceToDevice, s->stream));
+      CK(cudaMemcpyAsync(nb.id, ob.id, n4, cudaMemcpyDeviceToDevice, s->stream));
+      if (S.ion) CK(cudaMemcpyAsync(nb.cex, ob.cex, keep_n, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    CK(cudaStreamSynchronize(s->stream));
+    dfree(ob.x); dfree(ob.y); dfree(ob.vx); dfree(ob.vy); dfree(ob.vz); dfree(ob.id); dfree(ob.cex);
+    ob = nb;
+  }
+  S.cap = cap;
+  // per-step scratch sized by the largest species
+  size_t tiles = (size_t)std::max(s->sp[0].cap, s->sp[1].cap) / TILE + 2;
+  if (tiles > s->tile_cap) {
+    dfree(s->tile_status);
+    CK(dalloc(&s->tile_status, 2 * tiles));
+    s->tile_cap = tiles;
+  }
+  size_t scap = (size_t)std::max(s->sp[0].cap, s->sp[1].cap);
+  if (scap > s->sort_cap) {
+    for (int b = 0; b < 2; ++b) { dfree(s->skey[b]); dfree(s->sval[b]); CK(dalloc(&s->skey[b], scap)); CK(dalloc(&s->sval[b], scap)); }
+    s->sort_cap = scap;
+    size_t hc = (size_t)RADIX * (scap / SORT_TILE + 1);
+    dfree(s->shist);
+    CK(dalloc(&s->shist, hc));
+    s->hist_cap = hc;
+  }
+  return PB_OK;
+}
+
+static int32_t read_counts(Sim* s) {
+  int h[4];
+  CK(cudaMemcpyAsync(h, s->counts, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  s->host_num[0] = h[s->sp[0].cur];
+  s->host_num[1] = h[2 + s->sp[1].cur];
+  return PB_OK;
+}
+
+// keep room for one more step: injections, neutralizer, SEE spawns
+static int32_t ensure_room(Sim* s, const pb_step_params* p, int steps) {
+  long inj_max = 0;
+  if (p->inject_on) inj_max = (long)(p->lam + 40.0 * std::sqrt(std::max(p->lam, 0.0)) + 100.0);
+  long e_max = (long)p->neut_n + (p->rf_on ? (long)p->rf_num_float + 1 : 0);
+  long need_p = s->host_num[0] + (long)steps * inj_max;
+  long need_e = s->host_num[1] + (long)steps * (e_max + std::min<long>(s->see_cap, s->host_num[0] + 1024));
+  int32_t rc;
+  if (need_p > s->sp[0].cap) {
+    if ((rc = read_counts(s))) return rc;
+    need_p = s->host_num[0] + (long)steps * inj_max;
+    if (need_p > s->sp[0].cap && (rc = alloc_species(s, 0, (int)(need_p + need_p / 4 + 4096), s->host_num[0]))) return rc;
+  }
+  if (need_e > s->sp[1].cap) {
+    if ((rc = read_counts(s))) return rc;
+    need_e = s->host_num[1] + (long)steps * (e_max + std::min<long>(s->see_cap, s->host_num[0] + 1024));
+    if (need_e > s->sp[1].cap && (rc = alloc_species(s, 1, (int)(need_e + need_e / 4 + 4096), s->host_num[1]))) return rc;
+  }
+  return PB_OK;
+}
+
+static void free_levels(Sim* s) {
+  for (size_t l = 0; l < s->lev.size(); ++l) {
+    if (l > 0) { dfree(s->lev[l].act); dfree(s->lev[l].st); dfree(s->lev[l].r); dfree(s->lev[l].z); }
+  }
+  s->lev.clear();
+  dfree(s->cidx);
+  dfree(s->cinvT);
+}
+
+// node classes from isBound (host copy) and the multigrid hierarchy
+static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
+  std::vector<uint8_t> cls = mghost::node_classes(s->ny, s->nx, s->periodic, isBound_host);
+  CK(cudaMemcpyAsync(s->cls, cls.data(), cls.size(), cudaMemcpyHostToDevice, s->stream));
+  mghost::Hierarchy H;
+  try {
+    H = mghost::build(s->ny, s->nx, s->periodic, cls, s->max_coarse);
+  } catch (const std::exception& e) {
+    return fail(PB_ERR_ARG, std::string("multigrid build: ") + e.what());
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  free_levels(s);
+  s->lev.resize(H.lev.size());
+  s->first_small = (int)H.lev.size() - 1;
+  for (size_t l = 0; l < H.lev.size(); ++l) {
+    const auto& L = H.lev[l];
+    DevLevel& D = s->lev[l];
+    D.ny = L.ny; D.nx = L.nx; D.per = L.per; D.wrapP = L.wrapP; D.ncolors = L.ncolors;
+    size_t N = (size_t)L.ny * L.nx;
+    if (l == 0) {
+      D.act = s->cls; D.st = nullptr; D.r = s->r32; D.z = s->z32;
+    } else {
+      CK(dalloc(&D.act, N)); CK(dalloc(&D.st, 9 * N)); CK(dalloc(&D.r, N)); CK(dalloc(&D.z, N));
+      CK(cudaMemcpy(D.act, L.act.data(), N, cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(D.st, L.st.data(), 9 * N * sizeof(float), cudaMemcpyHostToDevice));
+      CK(cudaMemset(D.r, 0, N * sizeof(float)));
+      CK(cudaMemset(D.z, 0, N * sizeof(float)));
+      if ((int)l < s->first_small && N <= 6000) s->first_small = (int)l;
+    }
+  }
+  if (s->first_small < 1) s->first_small = 1;
+  s->nc = (int)H.cidx.size();
+  CK(dalloc(&s->cidx, s->nc));
+  CK(dalloc(&s->cinvT, (size_t)s->nc * s->nc));
+  CK(cudaMemcpy(s->cidx, H.cidx.data(), s->nc * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->cinvT, H.cinvT.data(), (size_t)s->nc * s->nc * sizeof(float), cudaMemcpyHostToDevice));
+  return PB_OK;
+}
+
+static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p) {
+  PoissonArgs a{};
+  a.ny = s->ny; a.nx = s->nx; a.periodic = s->periodic;
+  a.cls = s->cls; a.Vfixed = s->Vfixed; a.rho = s->rho; a.V = s->V; a.x = s->Vnew; a.f = s->f; a.dirsum = s->dirsum;
+  a.r32 = s->r32; a.z32 = s->z32; a.p32 = s->p32; a.q32 = s->q32; a.e32 = s->e32;
+  a.Ex = s->Ex; a.Ey = s->Ey;
+  a.coeff = p->coeff; a.qn0_neg = p->qn0_neg; a.V_plasma = p->V_plasma; a.Te_up = p->Te_up;
+  a.omega_keep = p->omega_keep; a.omega_new = p->omega_new;
+  a.hx = p->hx; a.two_hx = p->two_hx; a.hy = p->hy; a.two_hy = p->two_hy; a.two_hy_per = p->two_hy_per;
+  a.iterations = iterations; a.compute_field = 1;
+  a.tol = s->tol; a.tol_inner = s->tol_inner; a.max_outer = s->max_outer; a.max_inner = s->max_inner; a.nu = s->nu;
+  a.nlevels = (int)s->lev.size(); a.first_small = s->first_small;
+  for (size_t l = 0; l < s->lev.size() && l < (size_t)MG_MAX_LEVELS; ++l) {
+    const DevLevel& D = s->lev[l];
+    a.lev[l].ny = D.ny; a.lev[l].nx = D.nx; a.lev[l].per = D.per; a.lev[l].wrapP = D.wrapP;
+    a.lev[l].ncolors = D.ncolors; a.lev[l].act = D.act; a.lev[l].st = D.st; a.lev[l].r = D.r; a.lev[l].z = D.z;
+  }
+  a.nc = s->nc; a.cidx = s->cidx; a.cinvT = s->cinvT;
+  a.partials = s->partials; a.bar = s->bar;
+  a.errflags = &s->rep_dev->errflags;
+  a.stats = s->pstats;
+  return a;
+}
+
+static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
+  if (iterations <= 0) return PB_OK;
+  PoissonArgs a = poisson_args(s, iterations, p);
+  CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), s->stream));
+  void* args[] = {&a};
+  CK(cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, 0, s->stream));
+  ++s->launches;
+  return PB_OK;
+}
+
+// RF: V_fixed on grid g = Vdc + v_rf
+__global__ void k_rf_update(double* Vfixed, const double* Vdc, const uint16_t* gridmask, int N, int g, double v_rf) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+    if (gridmask[i] & (1u << g)) Vfixed[i] = Vdc[i] + v_rf;
+}
+
+__global__ void k_report(pb_step_report* r, const int* counts, int ci, int ce, const int* n_sub,
+                         const unsigned long long* ds_bits, const int* inj, const int* see_spawned, const double* V,
+                         int n_saddle, const int* saddle_idx8, const double* pstats, int rf_on) {
+  r->num_p = counts[ci];
+  r->num_e = counts[2 + ce];
+  r->n_sub_ion = n_sub[0];
+  r->n_sub_e = n_sub[1];
+  r->ds_ion = __longlong_as_double((long long)ds_bits[0]);
+  r->ds_e = __longlong_as_double((long long)ds_bits[1]);
+  r->injected = inj[0];
+  r->rf_injected = inj[1];
+  r->neut_injected = inj[2];
+  r->see_spawned = *see_spawned;
+  double mp = 0.0;
+  for (int k = 0; k < n_saddle; ++k) {
+    double v = V[saddle_idx8[k]];
+    mp = (k == 0 || v < mp) ? v : mp;
+  }
+  r->min_pot = mp;
+  for (int k = 0; k < 4; ++k) r->poisson_stats[k] = pstats[k];
+  (void)rf_on;
+}
+
+struct SaddleIdx { int v[8]; };
+__global__ void k_report_saddle(pb_step_report* r, const double* V, int n, SaddleIdx idx) {
+  double mp = 0.0;
+  for (int k = 0; k < n; ++k) {
+    double v = V[idx.v[k]];
+    mp = (k == 0 || v < mp) ? v : mp;
+  }
+  r->min_pot = mp;
+}
+
+}  // namespace pb
+
+using namespace pb;
+
+struct SplineStore {
+  double* t = nullptr;
+  double* c = nullptr;
+  int nt = 0;
+  double lo = 0.0, hi = 0.0;
+};
+
+struct pb_sim {
+  Sim s;
+  SplineStore cx, see;
+};
+
+static Spline spline_of(const SplineStore& st) {
+  Spline sp{};
+  sp.t = st.t; sp.c = st.c; sp.nt = st.nt; sp.lo = st.lo; sp.hi = st.hi; sp.enabled = st.nt > 0;
+  return sp;
+}
+
+static int32_t sort_species(Sim* s, int k, int ncell_bits) {
+  Species& S = s->sp[k];
+  cudaStream_t st = s->stream;
+  int* n_src = s->counts + 2 * k + S.cur;
+  int* n_dst = s->counts + 2 * k + (1 - S.cur);
+  int cap = S.cap;
+  int ntiles = (cap + SORT_TILE - 1) / SORT_TILE;
+  const Soa& src = S.buf[S.cur];
+  k_sort_keys<<<grid_for(s, cap, 256), 256, 0, st>>>(src.x, src.y, n_src, s->nx, s->ny, (float)s->sp_dx,
+                                                     (float)s->sp_dy, s->skey[0], s->sval[0]);
+  ++s->launches;
+  int a = 0;
+  for (int shift = 0; shift < ncell_bits; shift += RADIX_BITS) {
+    k_sort_hist<<<ntiles, SORT_NT, 0, st>>>(s->skey[a], n_src, shift, s->shist, ntiles);
+    ++s->launches;
+    k_sort_scan<<<1, 1024, 0, st>>>(s->shist, RADIX * ntiles);
+    ++s->launches;
+    k_sort_scatter<<<ntiles, SORT_NT, 0, st>>>(s->skey[a], s->sval[a], n_src, shift, s->shist, ntiles,
+                                                s->skey[1 - a], s->sval[1 - a]);
+    ++s->launches;
+    a = 1 - a;
+  }
+  k_sort_gather<<<grid_for(s, cap, 256), 256, 0, st>>>(src, S.buf[1 - S.cur], s->sval[a], n_src);
+  ++s->launches;
+  k_copy_int<<<1, 1, 0, st>>>(n_src, n_dst);
+  ++s->launches;
+  S.cur ^= 1;
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+static int32_t check_flags(Sim* s, uint32_t f) {
+  if (f & PB_EF_SPIN_TIMEOUT) return fail(PB_ERR_TIMEOUT, "a bounded device wait timed out");
+  if (f & (PB_EF_CAPACITY_ION | PB_EF_CAPACITY_ELE | PB_EF_SEE_OVERFLOW | PB_EF_ANGLE_OVERFLOW | PB_EF_ID_OVERFLOW))
+    return fail(PB_ERR_CAPACITY, "particle storage or a per-step list overflowed (flags " + std::to_string(f) + ")");
+  if (f & (PB_EF_NAN_SUBSTEP | PB_EF_SUBSTEP_CAP)) return fail(PB_ERR_ARG, "sub-step count is NaN or above 65536");
+  if (f & PB_EF_POISSON_NOCONV) return fail(PB_ERR_NOCONV, "field solve did not reach its tolerance");
+  return PB_OK;
+}
+
+// one timestep, enqueued on the instance stream (physics_engine.py:969-1784)
+// record a phase mark (profiling only); marks k..k+6 of one step bracket its six phases
+static void mark(Sim* s) {
+  if (!s->profiling) return;
+  if (s->mark_used >= s->marks.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    s->marks.push_back(e);
+  }
+  cudaEventRecord(s->marks[s->mark_used++], s->stream);
+}
+
+static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
+  Sim* s = &h->s;
+  mark(s);
+  cudaStream_t st = s->stream;
+  const int N = s->ny * s->nx;
+  Species& I = s->sp[0];
+  Species& E = s->sp[1];
+  const float dxf = (float)p->dx, dyf = (float)p->dy;
+  s->sp_dx = p->dx;
+  s->sp_dy = p->dy;
+  int* ni_src = s->counts + I.cur;
+  int* ni_dst = s->counts + (1 - I.cur);
+  int* ne_src = s->counts + 2 + E.cur;
+  int* ne_dst = s->counts + 2 + (1 - E.cur);
+  pb_step_report* rep = s->rep_dev;
+  uint32_t* ef = &rep->errflags;
+
+  // per-step resets
+  CK(cudaMemsetAsync(rep, 0, sizeof(pb_step_report), st));
+  CK(cudaMemsetAsync(&rep->ppc_min, 0xFF, sizeof(uint64_t), st));
+  CK(cudaMemsetAsync(s->ppc, 0, (size_t)N * sizeof(int), st));
+  CK(cudaMemsetAsync(s->angle_count, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(s->see_count, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(s->see_spawned, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(s->ds_bits, 0, 2 * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(s->tile_counter, 0, 2 * sizeof(int), st));
+  CK(cudaMemsetAsync(s->tile_status, 0, 2 * s->tile_cap * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(ni_dst, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(ne_dst, 0, sizeof(int), st));
+  CK(cudaMemsetAsync(s->inj, 0, 7 * sizeof(int), st));
+
+  if (!s->counts_valid) {
+    CK(cudaMemsetAsync(s->cnt_i, 0, (size_t)N * sizeof(int), st));
+    CK(cudaMemsetAsync(s->cnt_e, 0, (size_t)N * sizeof(int), st));
+    k_count_cells<<<grid_for(s, I.cap, 256), 256, 0, st>>>(I.buf[I.cur].x, I.buf[I.cur].y, ni_src, 0, 0, s->cnt_i,
+                                                           s->nx, s->ny, dxf, dyf);
+    ++s->launches;
+    k_count_cells<<<grid_for(s, E.cap, 256), 256, 0, st>>>(E.buf[E.cur].x, E.buf[E.cur].y, ne_src, 0, 0, s->cnt_e,
+                                                           s->nx, s->ny, dxf, dyf);
+    ++s->launches;
+    s->counts_valid = true;
+  }
+
+  // RF co-extraction: V_fixed on one grid, then recalc_poisson(2) (:984-991)
+  int32_t rc;
+  if (p->rf_grid >= 0) {
+    k_rf_update<<<grid_for(s, N, 256), 256, 0, st>>>(s->Vfixed, s->Vdc, s->gridmask, N, p->rf_grid, p->v_rf);
+    ++s->launches;
+    if ((rc = launch_poisson(s, 2, p))) return rc;
+  }
+
+  // A. injection (:996-1099)
+  InjectArgs ia{};
+  ia.ion_on = p->inject_on; ia.lam = p->lam; ia.geometry = p->geometry; ia.ylo = p->ylo; ia.yhi = p->yhi;
+  for (int k = 0; k < 4; ++k) ia.span[k] = (float)p->span[k];
+  ia.x_inj = (float)p->x_inj; ia.v_bohm = p->v_bohm; ia.v_spread = p->v_spread;
+  ia.rf_on = p->rf_on; ia.rf_num_float = p->rf_num_float; ia.rf_ylo = p->rf_ylo; ia.rf_yhi = p->rf_yhi;
+  ia.v_e_src = p->v_e_src;
+  ia.neut_n = p->neut_n; ia.neut_r = p->neut_r; ia.v_e_th = p->v_e_th; ia.neut_x = (float)p->neut_x;
+  ia.seed = s->seed; ia.step = (uint32_t)p->iteration;
+  ia.num_p = ni_src; ia.num_e = ne_src; ia.cap_p = I.cap; ia.cap_e = E.cap;
+  ia.next_ion_id = s->next_ids; ia.next_e_id = s->next_ids + 1;
+  ia.inj = s->inj;
+  ia.ions = I.buf[I.cur]; ia.eles = E.buf[E.cur];
+  ia.cnt_i = s->cnt_i; ia.cnt_e = s->cnt_e;
+  ia.nx = s->nx; ia.ny = s->ny; ia.dxf = dxf; ia.dyf = dyf; ia.errflags = ef;
+  k_inject_prep<<<1, 1, 0, st>>>(ia);
+  ++s->launches;
+  {
+    long mx = std::max<long>({(long)(p->lam + 40.0 * std::sqrt(std::max(p->lam, 0.0)) + 100.0),
+                              (long)p->neut_n, (long)p->rf_num_float + 1, 1L});
+    k_inject_gen<<<dim3(grid_for(s, mx, 128, 2), 3), 128, 0, st>>>(ia);
+    ++s->launches;
+  }
+
+  // B. deposit (counts -> exact float32 sums) and the Picard field solve (:1104-1161)
+  k_rho_finalize<<<grid_for(s, N, 256), 256, 0, st>>>(s->rho, s->cnt_i, s->cnt_e, N, (float)p->charge_density, 0);
+  ++s->launches;
+  mark(s);
+  if (p->do_poisson && (rc = launch_poisson(s, p->picard_iters, p))) return rc;
+  mark(s);
+
+  // C. sub-step counts (:1177-1209)
+  const float dtf = (float)p->dt;
+  k_substep_reduce<<<grid_for(s, I.cap, 256), 256, 0, st>>>(I.buf[I.cur].x, I.buf[I.cur].y, I.buf[I.cur].vx,
+      I.buf[I.cur].vy, I.buf[I.cur].vz, ni_src, 0, s->Ex, s->Ey, s->nx, s->ny, dxf, dyf, p->qm_ion, dtf, p->dt2,
+      s->ds_bits);
+  ++s->launches;
+  k_substep_reduce<<<grid_for(s, E.cap, 256), 256, 0, st>>>(E.buf[E.cur].x, E.buf[E.cur].y, E.buf[E.cur].vx,
+      E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->nx, s->ny, dxf, dyf, p->qm_e, dtf, p->dt2,
+      s->ds_bits + 1);
+  ++s->launches;
+  k_substep_finish<<<1, 1, 0, st>>>((const double*)s->ds_bits, p->ds_lim, s->n_sub, ef);
+  ++s->launches;
+  k_substep_finish<<<1, 1, 0, st>>>((const double*)(s->ds_bits + 1), p->ds_lim, s->n_sub + 1, ef);
+  ++s->launches;
+  mark(s);
+
+  // ions: push, hits, tallies, exit diagnostics, compaction, CEX, PPC (:1211-1739)
+  IonStepArgs a{};
+  a.src = I.buf[I.cur]; a.dst = I.buf[1 - I.cur]; a.num_src = ni_src; a.num_dst = ni_dst;
+  a.Ex = s->Ex; a.Ey = s->Ey; a.Bx = a.By = a.Bz = nullptr; a.has_B = 0;
+  a.isBound = s->isBound; a.nx = s->nx; a.ny = s->ny; a.dxf = dxf; a.dyf = dyf;
+  a.dt = p->dt; a.qm = p->qm_ion; a.ds_lim = p->ds_lim; a.ds_max = (const double*)s->ds_bits; a.n_sub_out = s->n_sub;
+  a.periodic = s->periodic; a.Lyf = (float)p->Ly; a.Lxf = (float)p->Lx;
+  a.x_entry = (float)p->x_entry; a.x_exit = (float)p->x_exit; a.x_plume = (float)p->x_plume;
+  a.thermal_on = p->thermal_on; a.erosion_on = p->erosion_on;
+  a.Tmap = s->Tmap; a.damage = s->damage;
+  a.k_half_m = (float)p->half_m_ion; a.mw_f = (float)p->macro_w; a.ccell_f = (float)p->C_cell;
+  a.accel_f = (float)p->thermal_accel; a.q_f = (float)p->q; a.Y_f = (float)p->Y_coeff; a.Eth_f = (float)p->E_th;
+  a.dt_f = dtf;
+  a.see_spline = spline_of(h->see);
+  a.see_key = s->see_key; a.see_xy = s->see_xy; a.see_count = s->see_count; a.see_cap = s->see_cap;
+  a.angles = s->angles; a.angle_count = s->angle_count; a.angle_cap = s->angle_cap;
+  a.exit_sums = rep->exit_sums; a.counters = (unsigned long long*)&rep->entered;
+  a.rT_f = (float)p->rT; a.n0a = p->n0a; a.neut_vth = p->neut_vth; a.cx_spline = spline_of(h->cx);
+  a.seed = s->seed; a.step = (uint32_t)p->iteration;
+  a.ppc = s->ppc; a.cnt = s->cnt_i;
+  a.tile_status = s->tile_status; a.tile_counter = s->tile_counter; a.errflags = ef;
+  k_ion_step<<<grid_for(s, I.cap, TILE, 8), NT, 0, st>>>(a);
+  ++s->launches;
+  mark(s);
+
+  // sputter cell break (:1443-1449) before the electron purge, which sees the new mask
+  if (p->erosion_on) {
+    k_erosion_break<<<grid_for(s, N, 256), 256, 0, st>>>(s->damage, s->isBound, s->cls, s->eroded, s->ny, s->nx,
+                                                         s->periodic, p->thresh, p->dy, &rep->broken);
+    ++s->launches;
+  }
+
+  // electrons: push and purge (:1248-1293, 1534-1561)
+  EleStepArgs b{};
+  b.src = E.buf[E.cur]; b.dst = E.buf[1 - E.cur]; b.num_src = ne_src; b.num_dst = ne_dst;
+  b.Ex = s->Ex; b.Ey = s->Ey; b.Bx = b.By = b.Bz = nullptr; b.has_B = 0;
+  b.isBound = s->isBound; b.nx = s->nx; b.ny = s->ny; b.dxf = dxf; b.dyf = dyf;
+  b.dt = p->dt; b.qm = p->qm_e; b.ds_lim = p->ds_lim; b.ds_max = (const double*)(s->ds_bits + 1);
+  b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
+  b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
+  b.errflags = ef;
+  k_ele_step<<<grid_for(s, E.cap, TILE, 8), NT, 0, st>>>(b);
+  ++s->launches;
+
+  // SEE electrons, appended after the surviving electrons (:1390-1417)
+  SeeArgs sa{};
+  sa.see_key = s->see_key; sa.see_xy = s->see_xy; sa.see_count = s->see_count; sa.see_cap = s->see_cap;
+  sa.see_spawned = s->see_spawned; sa.seed = s->seed; sa.step = (uint32_t)p->iteration; sa.v_see_th = p->v_see_th;
+  sa.eles = E.buf[1 - E.cur]; sa.num_e = ne_dst; sa.cap_e = E.cap; sa.next_e_id = s->next_ids + 1;
+  sa.isBound = s->isBound; sa.nx = s->nx; sa.ny = s->ny; sa.dxf = dxf; sa.dyf = dyf;
+  sa.Lxf = (float)p->Lx; sa.Lyf = (float)p->Ly; sa.cnt_e = s->cnt_e; sa.errflags = ef;
+  k_see_finish<<<1, 1024, 0, st>>>(sa);
+  ++s->launches;
+  mark(s);
+  I.cur ^= 1;
+  E.cur ^= 1;
+
+  // F. thermal (:1566-1620)
+  if (p->thermal_on) {
+    k_thermal<<<dim3((s->nx + TT - 1) / TT, (s->ny + TT - 1) / TT), 256, 0, st>>>(
+        s->Tmap, s->isBound, s->ny, s->nx, (float)p->cooling_factor, (float)p->T4_300, (float)p->Fo_x,
+        (float)p->Fo_y, p->sweeps);
+    ++s->launches;
+  }
+  if (s->ngrids > 0) {
+    k_grid_sums<<<grid_for(s, N, 256), 256, 0, st>>>(s->Tmap, s->gridmask, N, std::min(s->ngrids, 16), rep->grid_sums);
+    ++s->launches;
+  }
+
+  // exit divergence, saddle potential, PPC map (:1482-1488, 1655-1676, 1741-1767)
+  k_theta95<<<1, 1024, 0, st>>>(s->angles, s->angle_count, s->angle_cap, s->angle_scratch, &rep->theta95);
+  ++s->launches;
+  k_report<<<1, 1, 0, st>>>(rep, s->counts, I.cur, E.cur, s->n_sub, s->ds_bits, s->inj, s->see_spawned, s->V,
+                            0, nullptr, s->pstats, 0);
+  ++s->launches;
+  SaddleIdx sidx{};
+  for (int k = 0; k < 8; ++k) sidx.v[k] = p->saddle_idx[k];
+  if (p->n_saddle > 0) {
+    k_report_saddle<<<1, 1, 0, st>>>(rep, s->V, p->n_saddle, sidx);
+    ++s->launches;
+  }
+  k_ppc_stats<<<grid_for(s, N, 256), 256, 0, st>>>(s->ppc, s->accum_ppc, N, (unsigned long long*)&rep->ppc_active);
+  ++s->launches;
+
+  // periodic re-sort by cell (north-star (a)); the permutation equals a stable argsort
+  if (p->sort_now) {
+    int bits = 1;
+    while ((1L << bits) < (long)N) ++bits;
+    if ((rc = sort_species(s, 0, bits))) return rc;
+    if ((rc = sort_species(s, 1, bits))) return rc;
+  }
+  mark(s);
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+static int32_t finish_report(Sim* s, pb_step_report* out) {
+  CK(cudaMemcpyAsync(s->rep_host, s->rep_dev, sizeof(pb_step_report), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  *out = *s->rep_host;
+  s->host_num[0] = out->num_p;
+  s->host_num[1] = out->num_e;
+  return check_flags(s, out->errflags);
+}
+
+// ------------------------------------------------------------------ C-ABI
+extern "C" {
+
+int32_t pb_version(void) { return 10000; }
+const char* pb_last_error(void) { return g_err.c_str(); }
+
+int32_t pb_sim_create(pb_sim** out, int32_t device) {
+  if (!out) return fail(PB_ERR_ARG, "null output");
+  pb_sim* h = new pb_sim();
+  Sim* s = &h->s;
+  s->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_poisson, PT, 0));
+  s->pgrid = s->num_sms * std::max(1, std::min(occ, 2));
+  CK(dalloc(&s->partials, 4 * (size_t)s->pgrid));
+  CK(dalloc(&s->bar, 2));
+  CK(dalloc(&s->pstats, 4));
+  CK(cudaMemset(s->pstats, 0, 4 * sizeof(double)));
+  CK(dalloc(&s->counts, 4));
+  CK(cudaMemset(s->counts, 0, 4 * sizeof(int)));
+  CK(dalloc(&s->next_ids, 2));
+  CK(cudaMemset(s->next_ids, 0, 2 * sizeof(uint32_t)));
+  CK(dalloc(&s->tile_counter, 2));
+  CK(dalloc(&s->ds_bits, 2));
+  CK(dalloc(&s->n_sub, 2));
+  CK(dalloc(&s->inj, 7));
+  CK(dalloc(&s->see_count, 1));
+  CK(dalloc(&s->see_spawned, 1));
+  CK(dalloc(&s->angle_count, 1));
+  s->see_cap = 1 << 16;
+  s->angle_cap = 1 << 16;
+  CK(dalloc(&s->see_key, 2 * (size_t)s->see_cap));
+  CK(dalloc(&s->see_xy, 2 * (size_t)s->see_cap));
+  CK(dalloc(&s->angles, (size_t)s->angle_cap));
+  CK(dalloc(&s->angle_scratch, 2 * (size_t)s->angle_cap));
+  CK(dalloc(&s->rep_dev, 1));
+  CK(cudaMemset(s->rep_dev, 0, sizeof(pb_step_report)));
+  CK(cudaMallocHost((void**)&s->rep_host, sizeof(pb_step_report)));
+  s->sp[0].ion = true;
+  s->sp[1].ion = false;
+  CK(cudaEventCreate(&s->ev0));
+  CK(cudaEventCreate(&s->ev1));
+  int32_t rc;
+  if ((rc = alloc_species(s, 0, 4096, 0)) || (rc = alloc_species(s, 1, 4096, 0))) return rc;
+  *out = h;
+  return PB_OK;
+}
+
+int32_t pb_sim_destroy(pb_sim* h) {
+  if (!h) return PB_OK;
+  Sim* s = &h->s;
+  cudaSetDevice(s->device);
+  cudaStreamSynchronize(s->stream);
+  free_levels(s);
+  double* d[] = {s->V, s->Vnew, s->Vfixed, s->Vdc, s->damage, s->eroded, s->accum_ppc, s->f, s->dirsum, s->partials, s->pstats};
+  for (double* q : d) if (q) cudaFree(q);
+  float* fl[] = {s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->see_xy, s->angles};
+  for (float* q : fl) if (q) cudaFree(q);
+  void* v[] = {s->isBound, s->cls, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->bar, s->counts, s->next_ids,
+               s->tile_status, s->tile_counter, s->see_key, s->see_count, s->angle_scratch, s->angle_count,
+               s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1], s->sval[0], s->sval[1],
+               s->shist, s->rep_dev, h->cx.t, h->cx.c, h->see.t, h->see.c};
+  for (void* q : v) if (q) cudaFree(q);
+  for (int k = 0; k < 2; ++k)
+    for (int b = 0; b < 2; ++b) {
+      Soa& o = s->sp[k].buf[b];
+      dfree(o.x); dfree(o.y); dfree(o.vx); dfree(o.vy); dfree(o.vz); dfree(o.id); dfree(o.cex);
+    }
+  if (s->rep_host) cudaFreeHost(s->rep_host);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  delete h;
+  return PB_OK;
+}
+
+int32_t pb_sim_set_seed(pb_sim* h, uint64_t seed) { h->s.seed = seed; return PB_OK; }
+
+int32_t pb_sim_set_solver(pb_sim* h, double tol, double tol_inner, int32_t max_outer, int32_t max_inner, int32_t nu,
+                          int32_t max_coarse) {
+  Sim* s = &h->s;
+  if (!(tol > 0) || !(tol_inner > 0) || max_outer < 1 || max_inner < 1 || nu < 1 || max_coarse < 4 || max_coarse > 1024)
+    return fail(PB_ERR_ARG, "pb_sim_set_solver: invalid value");
+  s->tol = tol; s->tol_inner = tol_inner; s->max_outer = max_outer; s->max_inner = max_inner; s->nu = nu;
+  s->max_coarse = max_coarse;
+  return PB_OK;
+}
+
+int32_t pb_sim_set_spline(pb_sim* h, int32_t which, int32_t nt, const double* t, const double* c, double lo, double hi) {
+  if (which != 0 && which != 1) return fail(PB_ERR_ARG, "spline: which must be 0 (CX) or 1 (SEE)");
+  SplineStore& S = which == 0 ? h->cx : h->see;
+  dfree(S.t);
+  dfree(S.c);
+  S.nt = 0;
+  if (nt <= 0) return PB_OK;
+  if (nt < 8) return fail(PB_ERR_ARG, "spline: a cubic spline needs at least 8 knots");
+  CK(dalloc(&S.t, nt));
+  CK(dalloc(&S.c, nt));
+  CK(cudaMemcpy(S.t, t, nt * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(S.c, c, (nt - 4) * sizeof(double), cudaMemcpyHostToDevice));
+  S.nt = nt; S.lo = lo; S.hi = hi;
+  return PB_OK;
+}
+
+int32_t pb_sim_set_domain(pb_sim* h, int32_t ny, int32_t nx, int32_t periodic, const uint8_t* isBound,
+                          const double* V_fixed, const uint16_t* gridmask, int32_t ngrids, const double* V,
+                          const float* Tmap, const double* damage, const double* eroded, int32_t keep_state) {
+  Sim* s = &h->s;
+  if (ny < 3 || nx < 3 || !isBound || !V_fixed) return fail(PB_ERR_ARG, "pb_sim_set_domain: bad grid");
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize(s->stream));
+  size_t N = (size_t)ny * nx;
+  bool realloc = (ny != s->ny || nx != s->nx);
+  if (realloc) {
+    if (keep_state && s->domain_set) return fail(PB_ERR_ARG, "pb_sim_set_domain: keep_state with a new grid size");
+    double** dd[] = {&s->V, &s->Vnew, &s->Vfixed, &s->Vdc, &s->damage, &s->eroded, &s->accum_ppc, &s->f, &s->dirsum};
+    for (double** q : dd) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(double))); }
+    float** ff[] = {&s->Ex, &s->Ey, &s->rho, &s->Tmap, &s->r32, &s->z32, &s->p32, &s->q32, &s->e32};
+    for (float** q : ff) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(float))); }
+    dfree(s->isBound); CK(dalloc(&s->isBound, N));
+    dfree(s->cls); CK(dalloc(&s->cls, N));
+    dfree(s->gridmask); CK(dalloc(&s->gridmask, N));
+    int** ii[] = {&s->ppc, &s->cnt_i, &s->cnt_e};
+    for (int** q : ii) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(int))); }
+    s->ny = ny; s->nx = nx;
+  }
+  s->periodic = periodic ? 1 : 0;
+  s->ngrids = std::min<int>(ngrids, 16);
+  CK(cudaMemcpy(s->isBound, isBound, N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->Vfixed, V_fixed, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->Vdc, V_fixed, N * sizeof(double), cudaMemcpyHostToDevice));
+  if (gridmask) CK(cudaMemcpy(s->gridmask, gridmask, N * sizeof(uint16_t), cudaMemcpyHostToDevice));
+  else CK(cudaMemset(s->gridmask, 0, N * sizeof(uint16_t)));
+  if (V) { CK(cudaMemcpy(s->V, V, N * sizeof(double), cudaMemcpyHostToDevice)); CK(cudaMemcpy(s->Vnew, V, N * sizeof(double), cudaMemcpyHostToDevice)); }
+  if (Tmap) CK(cudaMemcpy(s->Tmap, Tmap, N * sizeof(float), cudaMemcpyHostToDevice));
+  if (damage) CK(cudaMemcpy(s->damage, damage, N * sizeof(double), cudaMemcpyHostToDevice));
+  if (eroded) CK(cudaMemcpy(s->eroded, eroded, N * sizeof(double), cudaMemcpyHostToDevice));
+  if (!keep_state) {
+    // reset_arrays (physics_engine.py:424-438): a fresh build starts from empty maps
+    CK(cudaMemset(s->accum_ppc, 0, N * sizeof(double)));
+    CK(cudaMemset(s->rho, 0, N * sizeof(float)));
+    if (!damage) CK(cudaMemset(s->damage, 0, N * sizeof(double)));
+    if (!eroded) CK(cudaMemset(s->eroded, 0, N * sizeof(double)));
+    CK(cudaMemset(s->ppc, 0, N * sizeof(int)));
+    CK(cudaMemset(s->Ex, 0, N * sizeof(float)));
+    CK(cudaMemset(s->Ey, 0, N * sizeof(float)));
+    if (!V) { CK(cudaMemset(s->V, 0, N * sizeof(double))); CK(cudaMemset(s->Vnew, 0, N * sizeof(double))); }
+  }
+  int32_t rc = build_operator(s, isBound);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  s->domain_set = true;
+  s->counts_valid = false;
+  return PB_OK;
+}
+
+int32_t pb_sim_rebuild_operator(pb_sim* h) {
+  Sim* s = &h->s;
+  if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_rebuild_operator: no domain");
+  std::vector<uint8_t> ib((size_t)s->ny * s->nx);
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaMemcpy(ib.data(), s->isBound, ib.size(), cudaMemcpyDeviceToHost));
+  int32_t rc = build_operator(s, ib.data());
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  return PB_OK;
+}
+
+int32_t pb_sim_reserve(pb_sim* h, int32_t species, int32_t capacity) {
+  Sim* s = &h->s;
+  if (species < 0 || species > 1 || capacity < 0) return fail(PB_ERR_ARG, "pb_sim_reserve");
+  int32_t rc = read_counts(s);
+  if (rc) return rc;
+  return alloc_species(s, species, capacity, s->host_num[species]);
+}
+
+int32_t pb_sim_set_particles(pb_sim* h, int32_t species, int32_t n, const float* x, const float* y, const float* vx,
+                             const float* vy, const float* vz, const uint8_t* cex, const uint32_t* id,
+                             uint32_t next_id) {
+  Sim* s = &h->s;
+  if (species < 0 || species > 1 || n < 0) return fail(PB_ERR_ARG, "pb_sim_set_particles");
+  int32_t rc;
+  if ((rc = alloc_species(s, species, std::max(n + n / 4 + 4096, 4096), 0))) return rc;
+  Species& S = s->sp[species];
+  Soa& b = S.buf[S.cur];
+  size_t n4 = (size_t)n * 4;
+  if (n > 0) {
+    CK(cudaMemcpy(b.x, x, n4, cudaMemcpyHostToDevice)); CK(cudaMemcpy(b.y, y, n4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.vx, vx, n4, cudaMemcpyHostToDevice)); CK(cudaMemcpy(b.vy, vy, n4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b.vz, vz, n4, cudaMemcpyHostToDevice)); CK(cudaMemcpy(b.id, id, n4, cudaMemcpyHostToDevice));
+    if (S.ion) {
+      if (cex) CK(cudaMemcpy(b.cex, cex, n, cudaMemcpyHostToDevice));
+      else CK(cudaMemset(b.cex, 0, n));
+    }
+  }
+  CK(cudaMemcpy(s->counts + 2 * species + S.cur, &n, sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->next_ids + species, &next_id, sizeof(uint32_t), cudaMemcpyHostToDevice));
+  s->host_num[species] = n;
+  s->counts_valid = false;
+  return PB_OK;
+}
+
+int32_t pb_sim_get_particles(pb_sim* h, int32_t species, int32_t n, float* x, float* y, float* vx, float* vy, float* vz,
+                             uint8_t* cex, uint32_t* id) {
+  Sim* s = &h->s;
+  if (species < 0 || species > 1 || n < 0 || n > s->sp[species].cap) return fail(PB_ERR_ARG, "pb_sim_get_particles");
+  CK(cudaStreamSynchronize(s->stream));
+  Species& S = s->sp[species];
+  const Soa& b = S.buf[S.cur];
+  size_t n4 = (size_t)n * 4;
+  if (n == 0) return PB_OK;
+  if (x) CK(cudaMemcpy(x, b.x, n4, cudaMemcpyDeviceToHost));
+  if (y) CK(cudaMemcpy(y, b.y, n4, cudaMemcpyDeviceToHost));
+  if (vx) CK(cudaMemcpy(vx, b.vx, n4, cudaMemcpyDeviceToHost));
+  if (vy) CK(cudaMemcpy(vy, b.vy, n4, cudaMemcpyDeviceToHost));
+  if (vz) CK(cudaMemcpy(vz, b.vz, n4, cudaMemcpyDeviceToHost));
+  if (id) CK(cudaMemcpy(id, b.id, n4, cudaMemcpyDeviceToHost));
+  if (cex && S.ion) CK(cudaMemcpy(cex, b.cex, n, cudaMemcpyDeviceToHost));
+  return PB_OK;
+}
+
+int32_t pb_sim_counts(pb_sim* h, int32_t* num_p, int32_t* num_e, uint32_t* next_ion_id, uint32_t* next_e_id) {
+  Sim* s = &h->s;
+  int32_t rc = read_counts(s);
+  if (rc) return rc;
+  uint32_t ids[2];
+  CK(cudaMemcpy(ids, s->next_ids, sizeof(ids), cudaMemcpyDeviceToHost));
+  if (num_p) *num_p = s->host_num[0];
+  if (num_e) *num_e = s->host_num[1];
+  if (next_ion_id) *next_ion_id = ids[0];
+  if (next_e_id) *next_e_id = ids[1];
+  return PB_OK;
+}
+
+static void* field_of(Sim* s, int which, size_t* esize) {
+  switch (which) {
+    case 0: *esize = 8; return s->V;
+    case 1: *esize = 4; return s->Ex;
+    case 2: *esize = 4; return s->Ey;
+    case 3: *esize = 4; return s->rho;
+    case 4: *esize = 4; return s->Tmap;
+    case 5: *esize = 8; return s->damage;
+    case 6: *esize = 1; return s->isBound;
+    case 7: *esize = 8; return s->Vfixed;
+    case 8: *esize = 4; return s->ppc;
+    case 9: *esize = 8; return s->accum_ppc;
+    case 10: *esize = 8; return s->eroded;
+    case 11: *esize = 8; return s->Vnew;
+    case 12: *esize = 1; return s->cls;
+    default: *esize = 0; return nullptr;
+  }
+}
+
+int32_t pb_sim_field_ptr(pb_sim* h, int32_t which, void** dptr) {
+  size_t es;
+  void* p = field_of(&h->s, which, &es);
+  if (!p) return fail(PB_ERR_ARG, "pb_sim_field_ptr: unknown field");
+  *dptr = p;
+  return PB_OK;
+}
+
+int32_t pb_sim_get_field(pb_sim* h, int32_t which, void* host, int64_t nbytes) {
+  Sim* s = &h->s;
+  size_t es;
+  void* p = field_of(s, which, &es);
+  if (!p || (size_t)nbytes != es * (size_t)s->ny * s->nx) return fail(PB_ERR_ARG, "pb_sim_get_field: size");
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaMemcpy(host, p, nbytes, cudaMemcpyDeviceToHost));
+  return PB_OK;
+}
+
+int32_t pb_sim_set_field(pb_sim* h, int32_t which, const void* host, int64_t nbytes) {
+  Sim* s = &h->s;
+  size_t es;
+  void* p = field_of(s, which, &es);
+  if (!p || (size_t)nbytes != es * (size_t)s->ny * s->nx) return fail(PB_ERR_ARG, "pb_sim_set_field: size");
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaMemcpy(p, host, nbytes, cudaMemcpyHostToDevice));
+  if (which == 7) CK(cudaMemcpy(s->Vdc, host, nbytes, cudaMemcpyHostToDevice));
+  return PB_OK;
+}
+
+int32_t pb_sim_particle_ptr(pb_sim* h, int32_t species, int32_t which, void** dptr) {
+  Sim* s = &h->s;
+  if (species < 0 || species > 1) return fail(PB_ERR_ARG, "species");
+  const Soa& b = s->sp[species].buf[s->sp[species].cur];
+  void* p[] = {b.x, b.y, b.vx, b.vy, b.vz, b.cex, b.id};
+  if (which < 0 || which > 6 || !p[which]) return fail(PB_ERR_ARG, "which");
+  *dptr = p[which];
+  return PB_OK;
+}
+
+int32_t pb_sim_poisson(pb_sim* h, int32_t iterations, const pb_step_params* p, double* stats4_host) {
+  Sim* s = &h->s;
+  if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_poisson: no domain");
+  CK(cudaMemsetAsync(&s->rep_dev->errflags, 0, sizeof(uint32_t), s->stream));
+  int32_t rc = launch_poisson(s, iterations, p);
+  if (rc) return rc;
+  uint32_t f = 0;
+  CK(cudaMemcpyAsync(&f, &s->rep_dev->errflags, sizeof(f), cudaMemcpyDeviceToHost, s->stream));
+  if (stats4_host) CK(cudaMemcpyAsync(stats4_host, s->pstats, 4 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return check_flags(s, f);
+}
+
+int32_t pb_sim_step(pb_sim* h, const pb_step_params* p, pb_step_report* report) {
+  Sim* s = &h->s;
+  if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_step: no domain");
+  int32_t rc;
+  if ((rc = ensure_room(s, p, 1))) return rc;
+  s->mark_used = 0;
+  s->launches = 0;
+  CK(cudaEventRecord(s->ev0, s->stream));
+  if ((rc = enqueue_step(h, p))) return rc;
+  CK(cudaEventRecord(s->ev1, s->stream));
+  if (report) {
+    if ((rc = finish_report(s, report))) return rc;
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    s->last_ms = ms;
+  }
+  return PB_OK;
+}
+
+int32_t pb_sim_run(pb_sim* h, const pb_step_params* params, int32_t nsteps, pb_step_report* reports) {
+  Sim* s = &h->s;
+  if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_run: no domain");
+  int32_t rc;
+  if (nsteps <= 0) return PB_OK;
+  if ((rc = ensure_room(s, &params[0], nsteps))) return rc;
+  s->mark_used = 0;
+  s->launches = 0;
+  CK(cudaEventRecord(s->ev0, s->stream));
+  for (int k = 0; k < nsteps; ++k) {
+    if ((rc = enqueue_step(h, &params[k]))) return rc;
+    if (reports) {
+      CK(cudaMemcpyAsync(&reports[k], s->rep_dev, sizeof(pb_step_report), cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  CK(cudaEventRecord(s->ev1, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+  s->last_ms = ms;
+  if ((rc = read_counts(s))) return rc;
+  if (reports)
+    for (int k = 0; k < nsteps; ++k)
+      if ((rc = check_flags(s, reports[k].errflags))) return rc;
+  return PB_OK;
+}
+
+int32_t pb_sim_synchronize(pb_sim* h) {
+  CK(cudaStreamSynchronize(h->s.stream));
+  return PB_OK;
+}
+
+void* pb_sim_stream(pb_sim* h) { return (void*)h->s.stream; }
+
+int32_t pb_sim_timing(pb_sim* h, double* out) {
+  Sim* s = &h->s;
+  for (int k = 0; k < 9; ++k) out[k] = 0.0;
+  out[0] = s->last_ms;
+  out[8] = (double)s->launches;
+  if (s->profiling && s->mark_used >= 7) {
+    CK(cudaStreamSynchronize(s->stream));
+    size_t steps = s->mark_used / 7;
+    for (size_t t = 0; t < steps; ++t)
+      for (int k = 0; k < 6; ++k) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, s->marks[t * 7 + k], s->marks[t * 7 + k + 1]));
+        out[1 + k] += ms;
+      }
+    out[7] = (double)steps;
+  }
+  return PB_OK;
+}
+
+int32_t pb_sim_set_profiling(pb_sim* h, int32_t on) {
+  h->s.profiling = on ? 1 : 0;
+  h->s.mark_used = 0;
+  return PB_OK;
+}
+
+// ------------------------------------------------------------------ kernel-level entry points
+int32_t pb_push_particles_boris(float* x, float* y, float* vx, float* vy, float* vz, const float* Ex, const float* Ey,
+                                const float* Bx, const float* By, const float* Bz, int32_t num_p, double dx, double dy,
+                                int32_t nx, int32_t ny, double dt, double q_m, void* stream) {
+  if (num_p <= 0) return PB_OK;
+  if (nx < 2 || ny < 2) return fail(PB_ERR_ARG, "push: grid must be at least 2 x 2");
+  double h = (0.5 * q_m) * dt;
+  int bs = 256;
+  int g = (int)std::min<long>((num_p + bs - 1) / bs, 148L * 16);
+  k_push_boris<<<g, bs, 0, (cudaStream_t)stream>>>(x, y, vx, vy, vz, Ex, Ey, Bx, By, Bz, num_p, nx, ny, (float)dx,
+                                                   (float)dy, h, (float)dt);
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy, int32_t nx,
+                          int32_t ny, double charge_density, void* stream) {
+  if (num_p <= 0) return PB_OK;
+  if (nx < 3 || ny < 3) return fail(PB_ERR_ARG, "accumulate_rho: grid must be at least 3 x 3");
+  cudaStream_t st = (cudaStream_t)stream;
+  int G = nx * ny;
+  int* cnt = nullptr;
+  CK(cudaMallocAsync((void**)&cnt, (size_t)G * sizeof(int), st));
+  CK(cudaMemsetAsync(cnt, 0, (size_t)G * sizeof(int), st));
+  int g = (int)std::min<long>((num_p + 255) / 256, 148L * 16);
+  k_count_cells<<<g, 256, 0, st>>>(x, y, nullptr, num_p, 0, cnt, nx, ny, (float)dx, (float)dy);
+  k_rho_finalize<<<(int)std::min<long>((G + 255) / 256, 148L * 16), 256, 0, st>>>(rho, cnt, nullptr, G,
+                                                                                  (float)charge_density, 1);
+  CK(cudaFreeAsync(cnt, st));
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+int32_t pb_thermal_conduction(const float* T, float* T_new, const int32_t* mask, int32_t nx, int32_t ny, double Fo_x,
+                              double Fo_y, void* stream) {
+  if (nx < 1 || ny < 1) return fail(PB_ERR_ARG, "thermal_conduction: empty grid");
+  int G = nx * ny;
+  k_thermal_taichi<<<(int)std::min<long>((G + 255) / 256, 148L * 16), 256, 0, (cudaStream_t)stream>>>(
+      T, T_new, mask, nx, ny, (float)Fo_x, (float)Fo_y);
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+int32_t pb_compute_particle_substeps(const float* x, const float* y, const float* vx, const float* vy, const float* vz,
+                                     int32_t n, const float* Ex, const float* Ey, int32_t nx, int32_t ny, double dx,
+                                     double dy, double qm, double dt, double frac, double* out_host, void* stream) {
+  double ds_lim = frac * std::min(dx, dy) * 1e-3;
+  if (n <= 0) { out_host[0] = 1; out_host[1] = 0.0; out_host[2] = ds_lim; return PB_OK; }
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* bits = nullptr;
+  CK(cudaMallocAsync((void**)&bits, sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), st));
+  int g = (int)std::min<long>((n + 255) / 256, 148L * 16);
+  k_substep_reduce<<<g, 256, 0, st>>>(x, y, vx, vy, vz, nullptr, n, Ex, Ey, nx, ny, (float)dx, (float)dy, qm, (float)dt,
+                                      dt * dt, bits);
+  unsigned long long hb = 0;
+  CK(cudaMemcpyAsync(&hb, bits, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  CK(cudaFreeAsync(bits, st));
+  CK(cudaStreamSynchronize(st));
+  double ds_max;
+  std::memcpy(&ds_max, &hb, sizeof(double));
+  double q = std::ceil(ds_max / std::max(ds_lim, 1e-30));
+  out_host[0] = std::max(1.0, q);
+  out_host[1] = ds_max;
+  out_host[2] = ds_lim;
+  return PB_OK;
+}
+
+int32_t pb_segment_hits_grid(const uint8_t* isBound, int32_t nx, int32_t ny, double dx, double dy, const float* x0,
+                             const float* y0, const float* x1, const float* y1, int32_t n, uint8_t* hit,
+                             int64_t* hit_ix, int64_t* hit_iy, void* stream) {
+  if (n <= 0) return PB_OK;
+  int g = (int)std::min<long>((n + 255) / 256, 148L * 16);
+  k_segment_hits<<<g, 256, 0, (cudaStream_t)stream>>>(isBound, nx, ny, (float)dx, (float)dy, x0, y0, x1, y1, n, hit,
+                                                       hit_ix, hit_iy);
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+// ------------------------------------------------------------------ host helpers
+float pb_host_seq_add_f32(float s, float c, uint32_t n) { return seq_add_f32(s, c, n); }
+double pb_host_philox_uniform(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j) {
+  return philox_uniform(seed, pid, site, step, j);
+}
+double pb_host_philox_normal(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j) {
+  return philox_normal(seed, pid, site, step, j);
+}
+float pb_host_percentile95(const float* sorted, int32_t n) {
+  if (n <= 0) return NAN;
+  return percentile95_sorted(sorted, n);
+}
+
+}  // extern "C"

@@ -1,0 +1,883 @@
+"""GPU drop-in for PY-BEMCS ``physics_engine`` (the per-timestep PIC-MCC loop).
+
+``DigitalTwinSimulator`` keeps the reference class's constructor, attributes, methods and
+return values (``Python/physics_engine.py:309-1963``): ``build_domain(params,
+preserve_state)``, ``step(params) -> (remeshed, min_pot, current_div, T_grids,
+trans_last_frame)``, ``recalc_poisson``, ``compute_particle_substeps``,
+``_segment_hits_grid``, ``set_material``, ``lookup_user_cs``, ``_add_ions`` /
+``_add_electrons`` and the diagnostics.  The state lives on the GPU inside libpbemcs (one
+instance per object); every step runs as hand-written sm_100a kernels.  Host arrays such
+as ``p_x``, ``V`` or ``Tmap`` are mirrors that download on access; a mirror that the caller
+assigns or modifies in place is uploaded before the next device operation.
+
+Random draws come from a keyed Philox4x32-10 stream (seed, draw site, particle id, step)
+instead of NumPy's global MT19937; ``seed`` selects the stream.
+
+The module-level ``accumulate_rho``, ``push_particles_boris`` and ``thermal_conduction``
+take torch CUDA tensors (or anything with ``data_ptr()``) and mirror the reference's
+kernel-level functions (``:38-171``, ``:178-254``).
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from .domain import build_domain_geometry, compute_debye_upstream_gap  # noqa: F401
+
+_NP_FP = np.float32
+
+MATERIAL_PRESETS = {
+    'Molybdenum': {'k': 138.0, 'rho': 10280.0, 'cp': 250.0, 'emissivity': 0.80, 'alpha': 4.8e-6,
+                   'E_mod': 329e9, 'Y_coeff': 1.05e-4, 'E_th': 30.0},
+    'Steel (SS316)': {'k': 16.3, 'rho': 8000.0, 'cp': 500.0, 'emissivity': 0.60, 'alpha': 16.0e-6,
+                      'E_mod': 193e9, 'Y_coeff': 2.8e-4, 'E_th': 25.0},
+    'Titanium': {'k': 21.9, 'rho': 4507.0, 'cp': 520.0, 'emissivity': 0.50, 'alpha': 8.6e-6,
+                 'E_mod': 116e9, 'Y_coeff': 1.8e-4, 'E_th': 20.0},
+    'Graphite': {'k': 120.0, 'rho': 2200.0, 'cp': 710.0, 'emissivity': 0.85, 'alpha': 3.0e-6,
+                 'E_mod': 11e9, 'Y_coeff': 3.5e-4, 'E_th': 15.0},
+}
+
+# field ids of pb_sim_get_field / pb_sim_set_field
+_FIELDS = {"V": (0, np.float64), "Ex": (1, np.float32), "Ey": (2, np.float32), "rho": (3, np.float32),
+           "Tmap": (4, np.float32), "damage_map": (5, np.float64), "isBound": (6, np.bool_),
+           "V_fixed": (7, np.float64), "current_ppc_map": (8, np.int32), "accum_ppc_map": (9, np.float64),
+           "eroded_depth": (10, np.float64)}
+_PARTICLES = {"p_x": (0, 0), "p_y": (0, 1), "p_vx": (0, 2), "p_vy": (0, 3), "p_vz": (0, 4), "p_isCEX": (0, 5),
+              "p_id": (0, 6), "e_x": (1, 0), "e_y": (1, 1), "e_vx": (1, 2), "e_vy": (1, 3), "e_vz": (1, 4),
+              "e_id": (1, 6)}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class _Mirror:
+    """Host copy of a device array with change detection for uploads."""
+    __slots__ = ("host", "snap", "valid", "touched")
+
+    def __init__(self):
+        self.host = None
+        self.snap = None
+        self.valid = False
+        self.touched = False
+
+
+class DigitalTwinSimulator:
+    """B200 implementation of the reference ``DigitalTwinSimulator``.
+
+    Extra keyword arguments: ``device`` (CUDA ordinal), ``seed`` (Philox stream),
+    ``sort_every`` (re-sort particles by cell every N steps, 0 = never), ``verbose``
+    (print the reference's sub-step and PPC warnings), ``solver`` (dict of field-solver
+    controls: tol, tol_inner, max_outer, max_inner, nu, max_coarse).
+    """
+
+    def __init__(self, device=0, seed=0, sort_every=20, verbose=False, solver=None):
+        lib = _lib.load()
+        self._libh = lib
+        h = C.c_void_p()
+        _lib.check(lib.pb_sim_create(C.byref(h), int(device)), "pb_sim_create")
+        self._h = h
+        self.device = int(device)
+        self.seed = int(seed)
+        lib.pb_sim_set_seed(h, C.c_uint64(self.seed))
+        self.sort_every = int(sort_every)
+        self.verbose = bool(verbose)
+        s = dict(tol=1e-10, tol_inner=1e-5, max_outer=8, max_inner=40, nu=1, max_coarse=256)
+        s.update(solver or {})
+        self.solver = s
+        _lib.check(lib.pb_sim_set_solver(h, s["tol"], s["tol_inner"], s["max_outer"], s["max_inner"], s["nu"],
+                                         s["max_coarse"]), "pb_sim_set_solver")
+        object.__setattr__(self, "_mirrors", {k: _Mirror() for k in list(_FIELDS) + list(_PARTICLES)})
+        # constants and defaults of the reference constructor (physics_engine.py:310-401)
+        self.dt = 5e-10
+        self.injection_stop_time = None
+        self.injection_enabled = True
+        self.q = 1.602e-19
+        self.m_XE = 131.293 * 1.6605e-27
+        self.m_ion = self.m_XE
+        self.Z_ion = 1
+        self.q_ion = self.q
+        self.kB = 1.380649e-23
+        self.eps0 = 8.854e-12
+        self.m_e = self.m_XE / 100.0
+        self.user_cs = {}
+        self.MATERIAL_PRESETS = MATERIAL_PRESETS
+        mat = MATERIAL_PRESETS['Molybdenum']
+        self._apply_material(mat)
+        self.macro_weight = 3e5
+        self.sb_sigma = 5.67e-8
+        self.thermal_accel = 1e7
+        self.injected_ions = 0.0
+        self.injected_ions_step = 0.0
+        self.transmitted_ions = 0.0
+        self.transmitted_ions_step = 0.0
+        self.transmitted3_step = 0.0
+        self.entered_optics = 0.0
+        self.entered_optics_step = 0.0
+        self.lost_to_grid_step = 0.0
+        self.Lx = 3
+        self.Ly = 3
+        self.dx = 0.02
+        self.dy = 0.02
+        self.nx = int(self.Lx / self.dx) + 1
+        self.ny = int(self.Ly / self.dy) + 1
+        self.dx = self.Lx / (self.nx - 1)
+        self.dy = self.Ly / (self.ny - 1)
+        self._recompute_cell_constants()
+        self.T_grids = []
+        self.mask_grids = []
+        self.V_dc = None
+        self.iteration = 0
+        self.laplacian_lu = None
+        self._domain_built = False
+        self.exit_vx_mean = np.nan
+        self.exit_v_mean = np.nan
+        self.exit_vx_std = np.nan
+        self.exit_v_std = np.nan
+        self.exit_energy_mean_eV = np.nan
+        self.exit_v_mean_primary = np.nan
+        self.exit_v_mean_cex = np.nan
+        self.exit_count_step = 0
+        self.total_active_cells = 0
+        self.low_ppc_cells = 0
+        self.ppc_steps_count = 0
+        self.energy_history_t, self.energy_history_ke_i, self.energy_history_ke_e = [], [], []
+        self.energy_history_fe, self.energy_history_tot = [], []
+        self._prev_total_energy = None
+        self.energy_warning_threshold = 0.05
+        self.num_p = 0
+        self.num_e = 0
+        self.max_p = 100000
+        self.max_e = 100000
+        self.next_ion_id = 0
+        self.next_e_id = 0
+        self.last_report = None
+        self.n_sub_ion = 1
+        self.n_sub_e = 1
+        self._cs_uploaded = None
+
+    # ------------------------------------------------------------------ mirrors
+    def __getattr__(self, name):
+        mirrors = object.__getattribute__(self, "_mirrors")
+        if name in mirrors:
+            return self._mirror_get(name)
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        mirrors = self.__dict__.get("_mirrors")
+        if mirrors is not None and name in mirrors:
+            m = mirrors[name]
+            if name in _FIELDS and self.__dict__.get("_domain_built"):
+                m.host = np.ascontiguousarray(np.asarray(value), dtype=_FIELDS[name][1]).reshape(self.ny, self.nx).copy()
+                m.snap = None
+                m.valid = True
+                m.touched = True
+                return
+            if name in _FIELDS:
+                # before the first build the reference keeps plain host arrays
+                m.host = np.asarray(value)
+                m.snap = None
+                m.valid = True
+                m.touched = False
+                return
+            raise AttributeError(f"{name} is read-only on the GPU simulator; use _add_ions/_add_electrons")
+        object.__setattr__(self, name, value)
+
+    def _mirror_get(self, name):
+        m = self._mirrors[name]
+        if not m.valid:
+            if name in _FIELDS:
+                if not self._domain_built:
+                    return m.host
+                fid, dt = _FIELDS[name]
+                raw = np.empty((self.ny, self.nx), dtype=np.uint8 if dt is np.bool_ else dt)
+                _lib.check(self._libh.pb_sim_get_field(self._h, fid, _ptr(raw), raw.nbytes), "get_field")
+                m.host = raw.astype(bool) if dt is np.bool_ else raw
+            else:
+                sp, which = _PARTICLES[name]
+                n = self.num_p if sp == 0 else self.num_e
+                arr = self._download_particles(sp, n)[which]
+                m.host = arr
+            m.snap = m.host.copy()
+            m.valid = True
+        if name in _FIELDS and self._domain_built:
+            m.touched = True
+        return m.host
+
+    def _invalidate(self):
+        for m in self._mirrors.values():
+            m.valid = False
+            m.touched = False
+            m.snap = None
+
+    def _flush(self):
+        """Upload field mirrors the caller changed (assignment or in-place)."""
+        for name, (fid, dt) in _FIELDS.items():
+            m = self._mirrors[name]
+            if not (m.valid and m.touched):
+                continue
+            if m.snap is not None and np.array_equal(m.host, m.snap):
+                m.touched = False
+                continue
+            raw = np.ascontiguousarray(m.host, dtype=np.uint8 if dt is np.bool_ else dt)
+            _lib.check(self._libh.pb_sim_set_field(self._h, fid, _ptr(raw), raw.nbytes), "set_field")
+            m.snap = m.host.copy()
+            m.touched = False
+            if name == "isBound":
+                _lib.check(self._libh.pb_sim_rebuild_operator(self._h), "rebuild_operator")
+
+    def _download_particles(self, sp, n):
+        x, y, vx, vy, vz = (np.empty(n, np.float32) for _ in range(5))
+        ids = np.empty(n, np.uint32)
+        cex = np.empty(n, np.uint8) if sp == 0 else None
+        _lib.check(self._libh.pb_sim_get_particles(self._h, sp, n, _ptr(x), _ptr(y), _ptr(vx), _ptr(vy), _ptr(vz),
+                                                   _ptr(cex), _ptr(ids)), "get_particles")
+        return [x, y, vx, vy, vz, (cex.astype(bool) if cex is not None else None), ids]
+
+    def close(self):
+        h = self.__dict__.get("_h")
+        if h is not None and h.value:
+            self._libh.pb_sim_destroy(h)
+            object.__setattr__(self, "_h", C.c_void_p())
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------ state
+    def reset_arrays(self):
+        """``physics_engine.py:404-448``: empty particle sets, zero fields."""
+        self.max_p = 100000
+        self.max_e = 100000
+        self.num_p = 0
+        self.num_e = 0
+        self.iteration = 0
+        self.next_ion_id = 0
+        self.next_e_id = 0
+        self.ppc_steps_count = 0
+        if self.__dict__.get("_h") is not None and self._h.value:
+            z = np.zeros(0, np.float32)
+            for sp in (0, 1):
+                _lib.check(self._libh.pb_sim_set_particles(self._h, sp, 0, _ptr(z), _ptr(z), _ptr(z), _ptr(z),
+                                                           _ptr(z), None, None, 0), "set_particles")
+        self._invalidate()
+        self.energy_history_t, self.energy_history_ke_i, self.energy_history_ke_e = [], [], []
+        self.energy_history_fe, self.energy_history_tot = [], []
+        self._prev_total_energy = None
+
+    def _apply_material(self, mat):
+        self.mat_k = mat['k']
+        self.mat_rho = mat['rho']
+        self.mat_cp = mat['cp']
+        self.emissivity = mat['emissivity']
+        self.alpha_thermal = mat['alpha']
+        self.E_modulus = mat['E_mod']
+        self.sputter_Y_coeff = mat['Y_coeff']
+        self.sputter_E_th = mat['E_th']
+
+    def _recompute_cell_constants(self):
+        """``physics_engine.py:450-452`` (refreshed only here and in set_material, as in
+        the reference)."""
+        self.C_cell = self.mat_rho * (self.dx * 1e-3) * (self.dy * 1e-3) * 1e-3 * self.mat_cp
+        self.A_cell = 2 * (self.dx * 1e-3) * 1e-3
+
+    def set_material(self, name=None, props=None):
+        """``physics_engine.py:454-473``."""
+        if name and name in MATERIAL_PRESETS:
+            mat = MATERIAL_PRESETS[name]
+        elif props:
+            mat = props
+        else:
+            return
+        self._apply_material(mat)
+        self._recompute_cell_constants()
+
+    def lookup_user_cs(self, cs_type_prefix, energy_eV):
+        """Host evaluation of a user table (``physics_engine.py:475-484``); the device uses
+        the same spline's knots and coefficients."""
+        for label, ds in self.user_cs.items():
+            if label.startswith(cs_type_prefix) and ds.get('spline') is not None:
+                log_e = np.log10(np.maximum(energy_eV, 1e-30))
+                e_min = np.log10(max(ds['energy'][0], 1e-30))
+                e_max = np.log10(ds['energy'][-1])
+                return 10.0 ** ds['spline'](np.clip(log_e, e_min, e_max))
+        return None
+
+    def _upload_user_cs(self):
+        key = tuple(sorted((k, id(v.get('spline'))) for k, v in self.user_cs.items()))
+        if key == self._cs_uploaded:
+            return
+        for which, prefix in ((0, 'CX'), (1, 'SEE')):
+            tab = None
+            for label, ds in self.user_cs.items():
+                if label.startswith(prefix) and ds.get('spline') is not None:
+                    tab = ds
+                    break
+            if tab is None:
+                _lib.check(self._libh.pb_sim_set_spline(self._h, which, 0, None, None, 0.0, 0.0), "set_spline")
+                continue
+            t, c, k = tab['spline']._eval_args
+            if k != 3:
+                raise ValueError("user cross-section splines must be cubic (k = 3)")
+            t = np.ascontiguousarray(t, np.float64)
+            c = np.ascontiguousarray(c, np.float64)
+            lo = float(np.log10(max(tab['energy'][0], 1e-30)))
+            hi = float(np.log10(tab['energy'][-1]))
+            _lib.check(self._libh.pb_sim_set_spline(self._h, which, len(t), t.ctypes.data_as(C.POINTER(C.c_double)),
+                                                    c.ctypes.data_as(C.POINTER(C.c_double)), lo, hi), "set_spline")
+        self._cs_uploaded = key
+
+    def _add_particles(self, sp, x, y, vx, vy, vz, is_cex=None):
+        n_new = len(x)
+        n_old = self.num_p if sp == 0 else self.num_e
+        old = self._download_particles(sp, n_old)
+        nid0 = self.next_ion_id if sp == 0 else self.next_e_id
+        cat = [np.concatenate([old[k], np.asarray(v, dtype=np.float32)]) for k, v in
+               zip(range(5), (x, y, vx, vy, vz))]
+        ids = np.concatenate([old[6], np.arange(nid0, nid0 + n_new, dtype=np.uint32)])
+        cex = None
+        if sp == 0:
+            cex = np.concatenate([old[5].astype(np.uint8),
+                                  np.asarray(is_cex if is_cex is not None else np.zeros(n_new), dtype=bool).astype(np.uint8)])
+        n = n_old + n_new
+        _lib.check(self._libh.pb_sim_set_particles(self._h, sp, n, *[_ptr(np.ascontiguousarray(a)) for a in cat],
+                                                   _ptr(cex), _ptr(ids), nid0 + n_new), "set_particles")
+        if sp == 0:
+            self.num_p = n
+            self.next_ion_id = nid0 + n_new
+            self.max_p = max(self.max_p, n)
+        else:
+            self.num_e = n
+            self.next_e_id = nid0 + n_new
+            self.max_e = max(self.max_e, n)
+        self._invalidate()
+
+    def _add_ions(self, x, y, vx, vy, vz, is_cex):
+        """``physics_engine.py:486-504``."""
+        self._add_particles(0, x, y, vx, vy, vz, is_cex)
+
+    def _add_electrons(self, x, y, vx, vy, vz):
+        """``physics_engine.py:506-522``."""
+        self._add_particles(1, x, y, vx, vy, vz)
+
+    def set_particles(self, species, x, y, vx, vy, vz, is_cex=None, ids=None):
+        """Replace a species wholesale (species 'ions' or 'electrons')."""
+        sp = 0 if species in (0, 'ions', 'ion') else 1
+        n = len(x)
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (x, y, vx, vy, vz)]
+        ids = np.arange(n, dtype=np.uint32) if ids is None else np.ascontiguousarray(ids, dtype=np.uint32)
+        cex = None
+        if sp == 0:
+            cex = np.ascontiguousarray(np.zeros(n, bool) if is_cex is None else is_cex, dtype=np.uint8)
+        nxt = int(ids.max()) + 1 if n else 0
+        _lib.check(self._libh.pb_sim_set_particles(self._h, sp, n, *[_ptr(a) for a in arrs], _ptr(cex), _ptr(ids),
+                                                   nxt), "set_particles")
+        if sp == 0:
+            self.num_p, self.next_ion_id = n, nxt
+        else:
+            self.num_e, self.next_e_id = n, nxt
+        self._invalidate()
+
+    # ------------------------------------------------------------------ domain
+    def _gridmask(self):
+        gm = np.zeros((self.ny, self.nx), np.uint16)
+        for g, m in enumerate(self.mask_grids[:16]):
+            gm[m] |= np.uint16(1 << g)
+        return gm
+
+    def _upload_domain(self, keep_state):
+        isB = np.ascontiguousarray(self._host_isBound, dtype=np.uint8)
+        Vf = np.ascontiguousarray(self._host_V_fixed, dtype=np.float64)
+        gm = self._gridmask()
+        Vh = np.ascontiguousarray(self._host_V, dtype=np.float64) if self._host_V is not None else None
+        Th = np.ascontiguousarray(self._host_T, dtype=np.float32) if self._host_T is not None else None
+        _lib.check(self._libh.pb_sim_set_domain(self._h, self.ny, self.nx, int(bool(self.periodic_y)), _ptr(isB),
+                                                _ptr(Vf), _ptr(gm), len(self.mask_grids), _ptr(Vh), _ptr(Th), None,
+                                                None, int(keep_state)), "set_domain")
+
+    def build_domain(self, params, preserve_state=False):
+        """``physics_engine.py:629-847``: host geometry, device upload, initial Picard."""
+        self._flush()
+        geo = _GeometryState(self, preserve_state)
+        build_domain_geometry(geo, params, preserve_state, _NP_FP)
+        for k in ("Lx", "Ly", "nx", "ny", "dx", "dy", "xpts", "ypts", "X", "Y", "geometry", "periodic_y",
+                  "recommended_upstream_gap_mm", "upstream_gap_mm", "injection_stop_time", "injection_enabled",
+                  "macro_weight", "mask_grids", "T_grids", "grid_deflections", "hole_centers", "grid_x_starts",
+                  "grid_x_ends", "Vdc"):
+            if hasattr(geo, k):
+                object.__setattr__(self, k, getattr(geo, k))
+        if not preserve_state:
+            for k in ("iteration", "injected_ions", "injected_ions_step", "transmitted_ions", "transmitted_ions_step",
+                      "entered_optics", "entered_optics_step"):
+                object.__setattr__(self, k, getattr(geo, k))
+            self.reset_arrays()
+        self._host_isBound = geo.isBound
+        self._host_V_fixed = geo.V_fixed
+        self._host_V = geo.V if preserve_state else np.zeros((self.ny, self.nx))
+        self._host_T = geo.Tmap
+        self._upload_domain(keep_state=preserve_state)
+        self._domain_built = True
+        self.laplacian_lu = True
+        self._invalidate()
+        self._upload_user_cs()
+        self.recalc_poisson(iterations=30 if not preserve_state else 10, params=params)
+
+    def build_sparse_matrix(self):
+        """``physics_engine.py:525-608``: rebuild the field operator from isBound."""
+        self._flush()
+        _lib.check(self._libh.pb_sim_rebuild_operator(self._h), "rebuild_operator")
+
+    # ------------------------------------------------------------------ parameters
+    def _poisson_params(self, P, params):
+        params = params or {}
+        grids = params.get('grids', [{'V': 1000}])
+        P.coeff = (self.dx * 1e-3) ** 2 / self.eps0
+        P.V_plasma = grids[0]['V'] + params.get('V_plasma_offset', 20.0)
+        P.Te_up = params.get('Te_up', 3.0)
+        n0 = params.get('n0_plasma', 1e17)
+        P.qn0_neg = -self.q * n0
+        omega = 0.2
+        P.omega_keep = 1 - omega
+        P.omega_new = omega
+        P.hx = self.dx * 1e-3
+        P.two_hx = 2. * P.hx
+        P.hy = self.dy * 1e-3
+        P.two_hy = 2. * P.hy
+        P.two_hy_per = 2.0 * self.dy * 1e-3
+        P.dx = self.dx
+        P.dy = self.dy
+
+    def recalc_poisson(self, iterations=5, params=None):
+        """``physics_engine.py:850-884`` on the device."""
+        if not self.laplacian_lu:
+            return
+        self._flush()
+        P = _lib.StepParams()
+        self._poisson_params(P, params)
+        stats = (C.c_double * 4)()
+        _lib.check(self._libh.pb_sim_poisson(self._h, int(iterations), C.byref(P), stats), "recalc_poisson")
+        self.poisson_stats = list(stats)
+        self._invalidate()
+
+    def step_params(self, params):
+        """The pb_step_params of the next step (advances nothing).  Mirrors the scalar
+        arithmetic of ``step`` (physics_engine.py:969-1739) in IEEE double."""
+        P = _lib.StepParams()
+        it = self.iteration + 1
+        sim_mode = params.get('sim_mode', 'Both')
+        t_current = it * self.dt
+        grids = params.get('grids', [])
+        P.iteration = it
+        P.do_poisson = int(it % 2 == 0)
+        P.picard_iters = 5
+        P.thermal_on = int(sim_mode in ('Thermal', 'Both'))
+        P.erosion_on = int(sim_mode in ('Erosion', 'Both'))
+        P.sort_now = int(self.sort_every > 0 and it % self.sort_every == 0)
+        P.rf_grid = -1
+        if params.get('rf_enable') and grids:
+            rf_idx = params.get('rf_grid_idx', 0)
+            if rf_idx < len(grids):
+                f_hz = params.get('rf_freq', 13.56) * 1e6
+                P.rf_grid = rf_idx
+                P.v_rf = params.get('rf_amp', 100.0) * np.sin(2.0 * np.pi * f_hz * t_current)
+        n0 = params.get('n0_plasma', 1e17)
+        Te_up = params.get('Te_up', 3.0)
+        Ti = params.get('Ti', 0.1)
+        v_bohm = np.sqrt(self.q_ion * Te_up / self.m_ion)
+        injection_area = self.Ly * 1e-3 * 0.005
+        charge_per_macro = self.q_ion * self.macro_weight
+        if self.injection_enabled and (self.injection_stop_time is None or t_current <= self.injection_stop_time):
+            P.inject_on = 1
+            bohm_factor = 1.0 if params.get('entire_bulk_plasma', False) else 0.61
+            I_ion = self.q_ion * bohm_factor * n0 * v_bohm * injection_area
+            P.lam = (I_ion * self.dt) / charge_per_macro
+            geometry = getattr(self, 'geometry', 'half_hole')
+            if grids:
+                screen_r = grids[0]['r']
+                pitch_inj = params.get('pitch_mm', 0.0)
+                if geometry == 'two_holes':
+                    P.geometry = 2
+                    span = np.array([[max(self.dy, 0.5 * screen_r), min(2.5 * screen_r, self.Ly - self.dy)],
+                                     [max(self.dy, 0.5 * screen_r + pitch_inj),
+                                      min(2.5 * screen_r + pitch_inj, self.Ly - self.dy)]], dtype=np.float32)
+                    for k, v in enumerate(span.ravel()):
+                        P.span[k] = float(v)
+                elif geometry == 'one_hole':
+                    P.geometry = 1
+                    P.ylo, P.yhi = max(self.dy, 0.5 * screen_r), min(2.5 * screen_r, self.Ly - self.dy)
+                else:
+                    P.geometry = 0
+                    P.ylo, P.yhi = 0.0, min(screen_r, self.Ly - self.dy)
+            else:
+                P.geometry = 3
+                P.ylo, P.yhi = self.dy, self.Ly - self.dy
+            P.x_inj = self.dx * 1.5
+            P.v_bohm = v_bohm
+            P.v_spread = np.sqrt(self.q_ion * Ti / self.m_ion)
+            if params.get('rf_enable'):
+                P.rf_on = 1
+                v_e_th_source = np.sqrt(2.0 * self.q * Te_up / self.m_e)
+                I_e = self.q * 0.25 * n0 * v_e_th_source * injection_area
+                P.rf_num_float = (I_e * self.dt) / charge_per_macro
+                y_margin = max(self.dy, 1e-9)
+                P.rf_ylo = y_margin
+                P.rf_yhi = max(y_margin, self.Ly - y_margin)
+                P.v_e_src = v_e_th_source
+        num_e_neut = int(params.get('neut_rate', 30))
+        P.neut_n = max(num_e_neut, 0)
+        P.neut_x = float(np.clip(params.get('neut_x', self.Lx - 0.5), self.dx, self.Lx - self.dx))
+        P.neut_r = float(np.clip(params.get('neut_r', self.Ly), self.dy, self.Ly))
+        P.v_e_th = np.sqrt(2.0 * self.q * params.get('Te', 5.0) / self.m_e)
+        cell_vol = (self.dx * 1e-3) * (self.dy * 1e-3) * 1e-3
+        P.charge_density = self.q * self.macro_weight / cell_vol
+        self._poisson_params(P, params)
+        P.dt = self.dt
+        P.qm_ion = self.q_ion / self.m_ion
+        P.qm_e = -self.q / self.m_e
+        P.ds_lim = 0.25 * min(self.dx, self.dy) * 1e-3
+        P.dt2 = self.dt ** 2
+        if grids and hasattr(self, "grid_x_starts") and len(self.grid_x_starts) == len(grids):
+            P.x_entry = self.grid_x_starts[0]
+            P.x_exit = self.grid_x_ends[-1]
+            P.x_plume = self.grid_x_ends[-1] + grids[-1]["gap"]
+        else:
+            P.x_entry, P.x_exit, P.x_plume = 0.5, 3.0, 3.0
+        P.Lx = self.Lx
+        P.Ly = self.Ly
+        P.half_m_ion = 0.5 * self.m_ion
+        P.macro_w = self.macro_weight
+        P.C_cell = self.C_cell
+        P.thermal_accel = self.thermal_accel
+        P.q = self.q
+        P.Y_coeff = self.sputter_Y_coeff
+        P.E_th = self.sputter_E_th
+        P.thresh = params.get('Thresh', 1e5)
+        P.rT = self.Ly * 1e-3
+        a_corr = 1.0 / (1.0 - 1.0 / np.sqrt(2.0))
+        P.n0a = params.get('n0', 1e20) * a_corr
+        P.neut_vth = np.sqrt(2.0 * self.kB * params.get('Tn', 300.0) / self.m_ion)
+        P.v_see_th = np.sqrt(2.0 * self.q * 2.0 / self.m_e)
+        P.cooling_factor = (self.emissivity * self.sb_sigma * self.A_cell * self.dt * self.thermal_accel) / self.C_cell
+        P.T4_300 = 300.0 ** 4
+        alpha_diff = self.mat_k / (self.mat_rho * self.mat_cp)
+        dt_thermal = self.dt * self.thermal_accel
+        Fo_x = alpha_diff * dt_thermal / (self.dx * 1e-3) ** 2
+        Fo_y = alpha_diff * dt_thermal / (self.dy * 1e-3) ** 2
+        if Fo_x > 0.2 or Fo_y > 0.2:
+            scale = 0.2 / max(Fo_x, Fo_y)
+            Fo_x *= scale
+            Fo_y *= scale
+        P.Fo_x, P.Fo_y = Fo_x, Fo_y
+        P.sweeps = 10
+        idx = self._saddle_indices(grids)
+        P.n_saddle = len(idx)
+        for k, v in enumerate(idx[:8]):
+            P.saddle_idx[k] = v
+        return P
+
+    def _saddle_indices(self, grids):
+        """Flat indices of the mid-hole potential samples (physics_engine.py:1655-1676)."""
+        hole_centers = getattr(self, 'hole_centers', [0.0])
+        if len(grids) >= 2:
+            x_grid_mm = 0.5 * (self.grid_x_starts[1] + self.grid_x_ends[1])
+        elif len(grids) == 1:
+            x_grid_mm = 0.5 * (self.grid_x_starts[0] + self.grid_x_ends[0])
+        else:
+            x_grid_mm = self.Lx * 0.5
+        x_idx = int(np.clip(round(x_grid_mm / self.dx), 0, self.nx - 1))
+        if hole_centers:
+            return [int(np.clip(round(yc / self.dy), 0, self.ny - 1)) * self.nx + x_idx for yc in hole_centers]
+        return [(self.ny // 2) * self.nx + x_idx]
+
+    # ------------------------------------------------------------------ the timestep
+    def step(self, params):
+        """One timestep (``physics_engine.py:969-1784``) on the GPU; returns
+        ``(remeshed, min_pot, current_div, T_grids, trans_last_frame)``."""
+        if not self.laplacian_lu:
+            return False, np.nan, np.nan, self.T_grids, 0.0
+        self._flush()
+        self._upload_user_cs()
+        P = self.step_params(params)
+        rep = _lib.StepReport()
+        _lib.check(self._libh.pb_sim_step(self._h, C.byref(P), C.byref(rep)), "step")
+        self.iteration += 1
+        self._invalidate()
+        return self._apply_report(rep, params)
+
+    def _apply_report(self, rep, params):
+        sim_mode = params.get('sim_mode', 'Both')
+        grids = params.get('grids', [])
+        self.last_report = rep
+        self.num_p, self.num_e = rep.num_p, rep.num_e
+        self.max_p = max(self.max_p, self.num_p)
+        self.max_e = max(self.max_e, self.num_e)
+        self.n_sub_ion, self.n_sub_e = rep.n_sub_ion, rep.n_sub_e
+        self.next_ion_id += rep.injected
+        self.next_e_id += rep.rf_injected + rep.neut_injected + rep.see_spawned
+        if self.verbose:
+            lim = 0.25 * min(self.dx, self.dy) * 1e-3
+            if rep.n_sub_ion > 1:
+                print(f"[Warning] Ion displacement criterion violated at iter {self.iteration}: predicted ds_max = "
+                      f"{rep.ds_ion:.3e} m, allowed = {lim:.3e} m, required substeps = {rep.n_sub_ion}")
+            if rep.n_sub_e > 1:
+                print(f"[Warning] Electron displacement criterion violated at iter {self.iteration}: predicted "
+                      f"ds_max = {rep.ds_e:.3e} m, allowed = {lim:.3e} m, required substeps = {rep.n_sub_e}")
+        self.injected_ions_step = float(rep.injected)
+        self.injected_ions += float(rep.injected)
+        self.entered_optics_step = float(rep.entered)
+        self.entered_optics += float(rep.entered)
+        self.prev_entered = self.entered_optics_step
+        self.transmitted_ions_step = 0.0
+        self.transmitted3_step = 0.0
+        if rep.exited_any > 0:
+            self.transmitted_ions_step = float(rep.crossed)
+            self.transmitted_ions += float(rep.crossed)
+            self.transmitted3_step = float(rep.crossed)
+        self.lost_to_grid_step = float(rep.lost_to_grid)
+        s = rep.exit_sums
+        n = rep.crossed
+        if n > 0:
+            self.exit_vx_mean = s[0] / n
+            self.exit_v_mean = s[1] / n
+            self.exit_energy_mean_eV = s[2] / n
+            self.exit_vx_std = math.sqrt(max(s[7] / n - (s[0] / n) ** 2, 0.0))
+            self.exit_v_std = math.sqrt(max(s[8] / n - (s[1] / n) ** 2, 0.0))
+            self.exit_count_step = int(n)
+            self.exit_v_mean_primary = s[3] / s[4] if s[4] > 0 else np.nan
+            self.exit_v_mean_cex = s[5] / s[6] if s[6] > 0 else np.nan
+        else:
+            self.exit_vx_mean = self.exit_v_mean = self.exit_vx_std = self.exit_v_std = np.nan
+            self.exit_energy_mean_eV = self.exit_v_mean_primary = self.exit_v_mean_cex = np.nan
+            self.exit_count_step = 0
+        current_div = float(rep.theta95) if n > 5 else np.nan
+        remeshed = False
+        if rep.broken > 0:
+            _lib.check(self._libh.pb_sim_rebuild_operator(self._h), "rebuild_operator")
+            remeshed = True
+        min_pot = np.float64(rep.min_pot)
+        if sim_mode in ('Thermal', 'Both'):
+            for i, mask in enumerate(self.mask_grids[:16]):
+                cnt = rep.grid_sums[2 * i + 1]
+                if cnt > 0:
+                    self.T_grids[i] = np.float32(rep.grid_sums[2 * i] / cnt)
+            if self._thermal_bow(params, grids):
+                self.build_domain(params, preserve_state=True)
+                remeshed = True
+                V = self.V
+                min_pot = min(V.ravel()[i] for i in self._saddle_indices(grids))
+        trans_last_frame = self.transmitted3_step / self.entered_optics_step if self.entered_optics_step > 0 else 0.0
+        self.total_active_cells = int(rep.ppc_active)
+        self.low_ppc_cells = int(rep.ppc_low)
+        self.ppc_steps_count += 1
+        if self.verbose and self.low_ppc_cells > 0:
+            pct = self.low_ppc_cells / self.total_active_cells * 100.0 if self.total_active_cells else 0.0
+            print(f"Warning: {self.low_ppc_cells} active cells have fewer than 3 macroparticles.")
+            print(f"Total active cells: {self.total_active_cells}")
+            print(f"Percentage of low PPC cells (< 3): {pct:.2f}%")
+            print(f"Lowest non-zero PPC found: {rep.ppc_min}")
+        return remeshed, min_pot, current_div, self.T_grids, trans_last_frame
+
+    def _thermal_bow(self, params, grids):
+        """Cantilever deflection check (physics_engine.py:1617-1643); True -> remesh."""
+        needs = False
+        geometry = getattr(self, 'geometry', 'half_hole')
+        for i, grid in enumerate(grids):
+            dT = self.T_grids[i] - 300.0
+            if geometry == 'two_holes':
+                dc = params.get("discharge_chamber")
+                pitch_val = params.get("pitch_mm", dc.get("pitch_mm", 3.0) if isinstance(dc, dict) else 3.0)
+                L_cant_mm = max(0.2, pitch_val - 2.0 * grid['r'])
+            elif geometry == 'one_hole':
+                L_cant_mm = max(0.2, 0.5 * (self.Ly - 2.0 * grid['r']))
+            else:
+                L_cant_mm = max(0.2, self.Ly - grid['r'])
+            L_cant_m = L_cant_mm * 1e-3
+            t_m = grid['t'] * 1e-3
+            if t_m > 0 and L_cant_m > 0:
+                new_defl = (self.alpha_thermal * dT * L_cant_m ** 2 / (2.0 * t_m)) * 1e3
+            else:
+                new_defl = 0.0
+            if abs(new_defl - self.grid_deflections[i]) > 0.005:
+                self.grid_deflections[i] = new_defl
+                needs = True
+        return needs
+
+    # ------------------------------------------------------------------ kernels on host arrays
+    def compute_particle_substeps(self, x, y, vx, vy, vz, qm, dt, frac=0.25):
+        """``physics_engine.py:928-966`` evaluated by the device kernel."""
+        import torch
+        self._flush()
+        n = len(x)
+        if n == 0:
+            return 1, 0.0, frac * min(self.dx, self.dy) * 1e-3
+        dev = torch.device("cuda", self.device)
+        t = [torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev) for a in (x, y, vx, vy, vz)]
+        Ex = torch.as_tensor(np.ascontiguousarray(self.Ex), device=dev)
+        Ey = torch.as_tensor(np.ascontiguousarray(self.Ey), device=dev)
+        out = (C.c_double * 3)()
+        _lib.check(self._libh.pb_compute_particle_substeps(*[a.data_ptr() for a in t], n, Ex.data_ptr(), Ey.data_ptr(),
+                                                           self.nx, self.ny, self.dx, self.dy, qm, dt, frac, out,
+                                                           torch.cuda.current_stream(dev).cuda_stream),
+                   "compute_particle_substeps")
+        return int(out[0]), float(out[1]), float(out[2])
+
+    def _segment_hits_grid(self, x0, y0, x1, y1, samples=8):
+        """``physics_engine.py:1880-1901`` evaluated by the device kernel (samples = 8)."""
+        import torch
+        if samples != 8:
+            raise ValueError("the device path tests 8 samples per segment, as the reference step does")
+        dev = torch.device("cuda", self.device)
+        n = len(x0)
+        t = [torch.as_tensor(np.ascontiguousarray(a, dtype=np.float32), device=dev) for a in (x0, y0, x1, y1)]
+        isb = torch.as_tensor(np.ascontiguousarray(self.isBound, dtype=np.uint8), device=dev)
+        hit = torch.empty(n, dtype=torch.uint8, device=dev)
+        hx = torch.empty(n, dtype=torch.int64, device=dev)
+        hy = torch.empty(n, dtype=torch.int64, device=dev)
+        _lib.check(self._libh.pb_segment_hits_grid(isb.data_ptr(), self.nx, self.ny, self.dx, self.dy,
+                                                   *[a.data_ptr() for a in t], n, hit.data_ptr(), hx.data_ptr(),
+                                                   hy.data_ptr(), torch.cuda.current_stream(dev).cuda_stream),
+                   "segment_hits")
+        return hit.bool().cpu().numpy(), hx.cpu().numpy(), hy.cpu().numpy()
+
+    # ------------------------------------------------------------------ diagnostics (:1786-1963)
+    def reset_ppc_accumulator(self):
+        self.accum_ppc_map = np.zeros((self.ny, self.nx))
+        self.ppc_steps_count = 0
+
+    def get_avg_ppc_map(self):
+        if self.ppc_steps_count > 0:
+            return self.accum_ppc_map / float(self.ppc_steps_count)
+        return self.current_ppc_map.astype(np.float64)
+
+    def get_total_energy(self):
+        t_now = self.iteration * self.dt
+        ke_i = float(np.sum(self.p_vx ** 2 + self.p_vy ** 2 + self.p_vz ** 2)) * 0.5 * self.m_ion * self.macro_weight \
+            if self.num_p > 0 else 0.0
+        ke_e = float(np.sum(self.e_vx ** 2 + self.e_vy ** 2 + self.e_vz ** 2)) * 0.5 * self.m_e * self.macro_weight \
+            if self.num_e > 0 else 0.0
+        cell_area = (self.dx * 1e-3) * (self.dy * 1e-3)
+        e_field = float(np.sum(self.Ex ** 2 + self.Ey ** 2)) * 0.5 * self.eps0 * cell_area
+        total = ke_i + ke_e + e_field
+        if self._prev_total_energy is not None and self._prev_total_energy > 0.0:
+            rel = abs(total - self._prev_total_energy) / self._prev_total_energy
+            if rel > self.energy_warning_threshold:
+                print(f"[Energy Warning] iter={self.iteration}: total energy changed by {rel*100:.1f}% in one step "
+                      f"(prev={self._prev_total_energy:.4e} J, now={total:.4e} J). "
+                      f"KE_i={ke_i:.3e} J, KE_e={ke_e:.3e} J, E_field={e_field:.3e} J")
+        self._prev_total_energy = total
+        self.energy_history_t.append(t_now)
+        self.energy_history_ke_i.append(ke_i)
+        self.energy_history_ke_e.append(ke_e)
+        self.energy_history_fe.append(e_field)
+        self.energy_history_tot.append(total)
+        return dict(t_s=t_now, ke_ions_J=ke_i, ke_elec_J=ke_e, field_J=e_field, total_J=total)
+
+    def get_third_grid_transparency_frame(self):
+        if self.entered_optics_step <= 0.0:
+            return 0.0
+        return self.transmitted3_step / self.entered_optics_step
+
+    def get_transparency(self):
+        if self.entered_optics <= 0.0:
+            return 0.0
+        return self.transmitted_ions / self.entered_optics
+
+    def has_active_particles(self):
+        return (self.num_p > 0) or (self.num_e > 0)
+
+    def get_groove_profile(self, grid_idx, thresh=None, accumulate_subcell=True, face='upstream'):
+        if grid_idx < 0 or grid_idx >= len(self.mask_grids):
+            return np.array([]), np.array([])
+        mask = self.mask_grids[grid_idx]
+        if not np.any(mask):
+            return np.array([]), np.array([])
+        depth = self.eroded_depth
+        if accumulate_subcell and thresh and thresh > 0:
+            depth = depth + (self.damage_map / thresh) * self.dy
+        y_mm = np.arange(self.ny) * self.dy
+        per_y = np.zeros(self.ny, dtype=np.float64)
+        has_any = mask.any(axis=1)
+        if face == 'any':
+            cols = np.any(mask, axis=0)
+            if not np.any(cols):
+                return np.array([]), np.array([])
+            per_y[has_any] = depth[has_any][:, cols].max(axis=1)
+        elif face == 'upstream':
+            first_idx = np.argmax(mask, axis=1)
+            per_y[has_any] = depth[np.where(has_any)[0], first_idx[has_any]]
+        elif face == 'downstream':
+            last_idx = self.nx - 1 - np.argmax(mask[:, ::-1], axis=1)
+            per_y[has_any] = depth[np.where(has_any)[0], last_idx[has_any]]
+        else:
+            raise ValueError(f"face must be 'upstream','downstream', or 'any' (got {face!r})")
+        return y_mm, per_y * 1000.0
+
+    def get_particle_kinematics(self):
+        t_current = self.iteration * self.dt
+        if self.num_p > 0:
+            vx, vy, vz = self.p_vx, self.p_vy, self.p_vz
+            e = (0.5 * self.m_ion * (vx ** 2 + vy ** 2 + vz ** 2)) / self.q
+            ions = np.column_stack((np.full(self.num_p, t_current), self.p_x, self.p_y, vx, vy, vz, e,
+                                    self.p_isCEX.astype(int)))
+        else:
+            ions = np.empty((0, 8))
+        if self.num_e > 0:
+            vx, vy, vz = self.e_vx, self.e_vy, self.e_vz
+            e = (0.5 * self.m_e * (vx ** 2 + vy ** 2 + vz ** 2)) / self.q
+            ex = self.e_x
+            elecs = np.column_stack((np.full(self.num_e, t_current), ex, self.e_y, vx, vy, vz, e,
+                                     np.where(ex <= 4.0, 2, 3)))
+        else:
+            elecs = np.empty((0, 8))
+        return np.vstack((ions, elecs))
+
+
+class _GeometryState:
+    """Attribute bag handed to the host geometry builder (reads the simulator's current
+    spacing, constants and temperature map; collects the new geometry)."""
+
+    def __init__(self, sim, preserve_state):
+        for k in ("dx", "dy", "dt", "eps0", "q", "q_ion", "m_ion", "m_e", "Lx", "Ly"):
+            setattr(self, k, getattr(sim, k))
+        if hasattr(sim, "grid_deflections"):
+            self.grid_deflections = list(sim.grid_deflections)
+        if preserve_state and sim._domain_built:
+            self.Tmap = np.array(sim.Tmap)
+            self.V = np.array(sim.V)
+        else:
+            self.Tmap = np.full((1, 1), 300.0, dtype=np.float32)
+
+    def reset_arrays(self):
+        pass
+
+
+# ---------------------------------------------------------------------- module-level kernels
+def _stream_of(t):
+    import torch
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def accumulate_rho(x, y, rho, num_p, dx, dy, nx, ny, charge_density):
+    """GPU ``accumulate_rho`` (physics_engine.py:38-60, 178-185) on CUDA tensors; rho is
+    updated in place with the exact float32 result of the sequential deposit."""
+    _lib.check(_lib.load().pb_accumulate_rho(x.data_ptr(), y.data_ptr(), rho.data_ptr(), int(num_p), float(dx),
+                                             float(dy), int(nx), int(ny), float(charge_density), _stream_of(rho)),
+               "accumulate_rho")
+
+
+def push_particles_boris(x, y, vx, vy, vz, Ex, Ey, Bx, By, Bz, num_p, dx, dy, nx, ny, dt, q_m):
+    """GPU ``push_particles_boris`` (physics_engine.py:63-144, 188-254) on CUDA tensors."""
+    _lib.check(_lib.load().pb_push_particles_boris(x.data_ptr(), y.data_ptr(), vx.data_ptr(), vy.data_ptr(),
+                                                   vz.data_ptr(), Ex.data_ptr(), Ey.data_ptr(), Bx.data_ptr(),
+                                                   By.data_ptr(), Bz.data_ptr(), int(num_p), float(dx), float(dy),
+                                                   int(nx), int(ny), float(dt), float(q_m), _stream_of(x)),
+               "push_particles_boris")
+
+
+def thermal_conduction(T, T_new, mask, nx, ny, Fo_x, Fo_y):
+    """GPU ``thermal_conduction`` (Taichi kernel semantics, physics_engine.py:147-171)."""
+    _lib.check(_lib.load().pb_thermal_conduction(T.data_ptr(), T_new.data_ptr(), mask.data_ptr(), int(nx), int(ny),
+                                                 float(Fo_x), float(Fo_y), _stream_of(T)), "thermal_conduction")

@@ -1,0 +1,93 @@
+"""Named aperture workloads (params dicts in the reference's config.json vocabulary).
+
+``single_aperture_2grid``: 2-grid screen/accel optics at 25 um spacing (65 x 284 nodes,
+the geometry of the reference's own CPU-runnable case), 100k macro-particles.
+
+``large_aperture_3grid``: 3-grid screen +1000 V / accel -250 V / decel 0 V, each 0.5 mm
+thick, 6.25 um spacing chosen so the derived domain is exactly 257 x 1025 nodes
+(256 x 1024 cells), 8M FP32 macro-particles (6M Xe+ and 2M electrons at mass ratio
+1/400), CEX cross-section 7e-19 E^-0.1 m^2 as a log-log table over 1-1000 eV, sputtering on.
+
+Particles are pre-loaded from a seeded NumPy generator: positions uniform over the
+non-electrode cells, ion velocities N(v_Bohm, v_th), electron velocities thermal.
+"""
+import numpy as np
+
+Q = 1.602e-19
+M_XE = 131.293 * 1.6605e-27
+
+
+def cx_table_power_law(a=7e-19, p=-0.1, e_lo=1.0, e_hi=1000.0, n=16):
+    e = np.logspace(np.log10(e_lo), np.log10(e_hi), n)
+    return np.stack([e, a * e ** p], axis=1)
+
+
+def cx_store(table):
+    from scipy.interpolate import UnivariateSpline
+    t = np.asarray(table, dtype=np.float64)
+    return {"CX": {"energy": t[:, 0], "cs": t[:, 1], "type": "CX",
+                   "spline": UnivariateSpline(np.log10(t[:, 0]), np.log10(t[:, 1]), s=0.0, k=3)}}
+
+
+WORKLOADS = {
+    "single_aperture_2grid": dict(
+        dx=0.025, dy=0.025, dt=1e-10, m_e_ratio=100.0, n_ions=80000, n_e=20000, cx=None,
+        params=dict(grids=[dict(V=1000.0, t=0.38, gap=1.0, r=0.95, cham=0.0),
+                           dict(V=-200.0, t=1.0, gap=1.0, r=0.55, cham=0.0)],
+                    pitch_mm=3.75, Te_up=5.0, n0_plasma=1e17, Ti=0.1, Tn=300.0, n0=1e18,
+                    sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9)),
+    "large_aperture_3grid": dict(
+        dx=0.00625, dy=0.00625, dt=2.5e-11, m_e_ratio=400.0, n_ions=6_000_000, n_e=2_000_000,
+        cx=cx_table_power_law(),
+        params=dict(grids=[dict(V=1000.0, t=0.5, gap=0.5, r=0.8, cham=0.0),
+                           dict(V=-250.0, t=0.5, gap=0.5, r=0.5, cham=0.0),
+                           dict(V=0.0, t=0.5, gap=0.5, r=0.7, cham=0.0)],
+                    pitch_mm=4.0, upstream_gap_mm=0.4, Te_up=5.0, n0_plasma=1e17, Ti=0.1, Tn=300.0,
+                    n0=1e18, sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9)),
+}
+
+
+def configure(sim, name, n_scale=1.0):
+    """Apply a workload's spacing, species and cross-section to a simulator (either the
+    GPU one or the oracle) before build_domain; returns the params dict."""
+    w = WORKLOADS[name]
+    sim.dx, sim.dy, sim.dt = w["dx"], w["dy"], w["dt"]
+    sim.m_ion = M_XE
+    sim.m_e = M_XE / w["m_e_ratio"]
+    if w["cx"] is not None:
+        sim.user_cs = cx_store(w["cx"])
+    return dict(w["params"])
+
+
+def preload(isBound, dx, dy, Lx, Ly, n_ions, n_e, v_bohm, v_th_i, v_th_e, seed=0):
+    """Seeded initial particles over the non-electrode cells (float32 SoA)."""
+    rs = np.random.RandomState(seed)
+    ny, nx = isBound.shape
+
+    def positions(n):
+        xs, ys, got = [], [], 0
+        while got < n:
+            m = max(2 * (n - got), 1024)
+            x = rs.uniform(1.5 * dx, Lx - dx, m)
+            y = rs.uniform(0.0, Ly, m)
+            ok = ~isBound[np.clip(np.round(y / dy).astype(np.int64), 0, ny - 1),
+                          np.clip(np.round(x / dx).astype(np.int64), 0, nx - 1)]
+            xs.append(x[ok]); ys.append(y[ok]); got += int(ok.sum())
+        return np.concatenate(xs)[:n].astype(np.float32), np.concatenate(ys)[:n].astype(np.float32)
+
+    xi, yi = positions(n_ions)
+    ions = (xi, yi, (v_bohm + v_th_i * rs.randn(n_ions)).astype(np.float32),
+            (v_th_i * rs.randn(n_ions)).astype(np.float32), (v_th_i * rs.randn(n_ions)).astype(np.float32))
+    xe, ye = positions(n_e)
+    eles = (xe, ye, (v_th_e * rs.randn(n_e)).astype(np.float32), (v_th_e * rs.randn(n_e)).astype(np.float32),
+            (v_th_e * rs.randn(n_e)).astype(np.float32))
+    return ions, eles
+
+
+def thermal_speeds(sim, params):
+    Te = params.get("Te_up", 3.0)
+    Ti = params.get("Ti", 0.1)
+    v_bohm = float(np.sqrt(sim.q_ion * Te / sim.m_ion))
+    v_th_i = float(np.sqrt(sim.q_ion * Ti / sim.m_ion))
+    v_th_e = float(np.sqrt(sim.q * params.get("Te", 5.0) / sim.m_e))
+    return v_bohm, v_th_i, v_th_e
