@@ -206,7 +206,8 @@ int32_t pb_sim_timing(pb_sim* s, double* out_host9);
 int32_t pb_sim_set_profiling(pb_sim* s, int32_t on);
 
 /* ---------------------------------------------------------------- host helpers */
-float pb_host_seq_add_f32(float s, float c, uint32_t n);
+/* n sequential additions s = (float)((double)s + c), as np.add.at on a float32 array */
+float pb_host_seq_add_f32d(float s, double c, uint32_t n);
 double pb_host_philox_uniform(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j);
 double pb_host_philox_normal(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j);
 float pb_host_percentile95(const float* sorted, int32_t n);

@@ -57,30 +57,37 @@ def test_struct_layout_matches_header(tmp_path):
         assert getattr(cls, name).offset == int(off), name
 
 
-def _seq_add_np(s, c, n):
-    s = np.float32(s)
-    c = np.float32(c)
-    for _ in range(n):
-        s = np.float32(s + c)
-    return s
+def _add_at(s, c, n):
+    r = np.array([s], dtype=np.float32)
+    np.add.at(r, np.zeros(n, dtype=np.int64), c)
+    return r[0]
 
 
-def test_seq_add_matches_sequential_float32_sums():
+def test_seq_add_matches_np_add_at():
+    """The run-length sum equals np.add.at on a float32 array with a Python-float value
+    (float64 partial sums rounded to float32 each time), including hot cells, both
+    signs, zero crossings and the ion-then-electron sequence of a deposit."""
     lib = _lib.load()
     rs = np.random.RandomState(0)
-    cases = [(0.0, 0.0200250, 5000), (0.0, -0.0200250, 3000), (0.5, -0.0200250, 2000), (0.0, 3.3e-3, 20000),
-             (1e-3, 1e-7, 10000), (-2.0, 0.07, 500), (0.0, 1.0, 2 ** 24 + 5)]
-    for _ in range(150):
+    cases = [(0.0, 0.00025568755727881564, 20000), (0.0, -0.00025568755727881564, 7000),
+             (0.5, -0.0200250, 2000), (0.0, 3.3e-3, 20000), (1e-3, 1e-7, 10000), (-2.0, 0.07, 500),
+             (0.0, 0.1, 100000)]
+    for _ in range(200):
         s0 = float(np.float32(rs.choice([0.0, rs.uniform(-10, 10)])))
-        c = float(np.float32(rs.uniform(-1, 1) * 10.0 ** rs.randint(-6, 3)))
-        cases.append((s0, c, int(rs.randint(1, 4000))))
+        c = float(rs.uniform(-1, 1) * 10.0 ** rs.randint(-6, 3))
+        cases.append((s0, c, int(rs.randint(1, 5000))))
     for s0, c, n in cases:
-        if n > 100000:
-            exp = np.float32(2 ** 24)  # 1.0 added 2^24+5 times stagnates at 2^24
-        else:
-            exp = _seq_add_np(s0, c, n)
-        got = np.float32(lib.pb_host_seq_add_f32(s0, c, n))
+        exp = _add_at(s0, c, n)
+        got = np.float32(lib.pb_host_seq_add_f32d(s0, c, n))
         assert got.view(np.uint32) == exp.view(np.uint32), (s0, c, n, got, exp)
+    # deposit sequence: k ions then m electrons into one cell
+    cd = 0.00025568755727881564
+    for k, m in [(5, 5), (7, 3), (100, 100), (3, 9), (20000, 7000), (1, 0), (0, 4)]:
+        r = np.zeros(1, np.float32)
+        np.add.at(r, np.zeros(k, np.int64), cd)
+        np.add.at(r, np.zeros(m, np.int64), -cd)
+        got = np.float32(lib.pb_host_seq_add_f32d(float(lib.pb_host_seq_add_f32d(0.0, cd, k)), -cd, m))
+        assert got.view(np.uint32) == r[0].view(np.uint32), (k, m, got, r[0])
 
 
 def test_host_philox_matches_oracle():

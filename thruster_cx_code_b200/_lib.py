@@ -92,7 +92,7 @@ PROTOTYPES = {
     "pb_sim_stream": (vp, [vp]),
     "pb_sim_timing": (i32, [vp, P(f64)]),
     "pb_sim_set_profiling": (i32, [vp, i32]),
-    "pb_host_seq_add_f32": (f32, [f32, f32, u32]),
+    "pb_host_seq_add_f32d": (f32, [f32, f64, u32]),
     "pb_host_philox_uniform": (f64, [u64, u64, u32, u32, u32]),
     "pb_host_philox_normal": (f64, [u64, u64, u32, u32, u32]),
     "pb_host_percentile95": (f32, [vp, i32]),

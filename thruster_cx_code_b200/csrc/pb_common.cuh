@@ -157,15 +157,20 @@ PB_HD double philox_normal(uint64_t seed, uint64_t pid, uint32_t site, uint32_t 
 }
 
 // ---------------------------------------------------------------- sequential float32 sums
-// Exact result of:  for (i < n) s = RN32(s + c);
-// Within one binade of the running sum (and away from zero) every addition moves s by
-// the same number of ulps, so whole runs are applied at once; transitions between
-// binades, sign changes and stagnation are taken one real addition at a time.
-PB_HD float f32_add_rn(float a, float b) {
+// Exact result of:  for (i < n) s = (float)((double)s + c);
+// which is what np.add.at(rho_float32, idx, python_float) does: each partial sum is formed
+// in float64 with the double addend and rounded to float32.  Within one float32 binade of
+// the running sum (away from zero) every addition moves s by the same number of float32
+// ulps, so whole runs are applied at once.  With u the float32 ulp of s, |c|/u = q + f;
+// the float64 sum rounds f onto a grid of u/2^29 (ties to even, independent of s), then
+// the float32 rounding picks q or q+1 (ties to even).  Binade changes, sign changes and
+// stagnation are taken one real addition at a time.
+PB_HD float f32_add_d_rn(float a, double b) {
 #ifdef __CUDA_ARCH__
-  return __fadd_rn(a, b);
+  return __double2float_rn(__dadd_rn((double)a, b));
 #else
-  volatile float r = a + b;
+  volatile double t = (double)a + b;
+  volatile float r = (float)t;
   return r;
 #endif
 }
@@ -178,50 +183,48 @@ PB_HD bool f32_signbit(float v) {
 #endif
 }
 
-PB_HD float seq_add_f32(float s, float c, uint32_t n) {
+PB_HD uint32_t f32_bits(float v) {
+#ifdef __CUDA_ARCH__
+  return __float_as_uint(v);
+#else
+  union { float f; uint32_t u; } a; a.f = v; return a.u;
+#endif
+}
+
+PB_HD float f32_from_bits(uint32_t b) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(b);
+#else
+  union { float f; uint32_t u; } a; a.u = b; return a.f;
+#endif
+}
+
+PB_HD float seq_add_f32d(float s, double c, uint32_t n) {
   uint32_t guard = 0;
   while (n > 0) {
-    float t = f32_add_rn(s, c);
+    float t = f32_add_d_rn(s, c);
     --n;
     if (t == s && !(t == 0.0f && f32_signbit(t) != f32_signbit(s))) return t;  // stagnation
     float prev = s;
     s = t;
     if (!(s == s) || n == 0) return s;
     if (++guard > 4096) {  // safety net: finish the remainder one addition at a time
-      while (n > 0) { s = f32_add_rn(s, c); --n; }
+      while (n > 0) { s = f32_add_d_rn(s, c); --n; }
       return s;
     }
     // try a jump: source and result in the same binade, same sign, normal range
-    uint32_t bp, bs, bc;
-#ifdef __CUDA_ARCH__
-    bp = __float_as_uint(prev); bs = __float_as_uint(s); bc = __float_as_uint(c);
-#else
-    { union { float f; uint32_t u; } a1, a2, a3; a1.f = prev; a2.f = s; a3.f = c; bp = a1.u; bs = a2.u; bc = a3.u; }
-#endif
-    uint32_t ep = (bp >> 23) & 0xFF, es = (bs >> 23) & 0xFF, ec = (bc >> 23) & 0xFF;
-    if (ep != es || (bp >> 31) != (bs >> 31) || es == 0 || es >= 254 || ec == 255) continue;
-    // units of ulp(s) = 2^(es-150);  S = significand of |s| in [2^23, 2^24)
-    int32_t S = (int32_t)((bs & 0x7FFFFF) | 0x800000);
-    bool up = ((bs >> 31) == (bc >> 31));  // |s| grows when c has the sign of s
-    // |c| / ulp as q + f, exactly: |c| = Mc 2^(ec-150) (normal) or Mc 2^-149 (subnormal)
-    uint32_t Mc = (ec == 0) ? (bc & 0x7FFFFF) : ((bc & 0x7FFFFF) | 0x800000);
-    int shift = (ec == 0 ? 1 : (int)ec) - (int)es;  // |c| = Mc * 2^shift ulps
-    int64_t q;
-    int frac_cmp;  // -1: f < 1/2, 0: f == 1/2, 1: f > 1/2
-    if (shift >= 0) {
-      if (shift > 30) continue;
-      q = (int64_t)Mc << shift;
-      frac_cmp = -1;
-    } else {
-      int sh = -shift;
-      if (sh > 40) { q = 0; frac_cmp = -1; }
-      else {
-        q = (int64_t)(Mc >> sh);
-        uint64_t rem = (uint64_t)Mc & ((1ull << sh) - 1ull);
-        uint64_t half = 1ull << (sh - 1);
-        frac_cmp = rem < half ? -1 : (rem == half ? 0 : 1);
-      }
-    }
+    uint32_t bp = f32_bits(prev), bs = f32_bits(s);
+    uint32_t ep = (bp >> 23) & 0xFF, es = (bs >> 23) & 0xFF;
+    if (ep != es || (bp >> 31) != (bs >> 31) || es == 0 || es >= 254 || !(c == c)) continue;
+    int32_t S = (int32_t)((bs & 0x7FFFFF) | 0x800000);  // |s| = S u, u = 2^(es-150)
+    bool up = ((bs >> 31) != 0) == (c < 0.0);          // |s| grows when c has the sign of s
+    double cu = ldexp(fabs(c), 150 - (int)es);          // |c| / u, exact
+    if (!(cu < 1099511627776.0)) continue;              // 2^40
+    double qd = floor(cu);
+    double fr = cu - qd;                                 // exact
+    double jf = rint(ldexp(fr, 29));                     // f on the float64 grid of the sum
+    int64_t q = (int64_t)qd;
+    int frac_cmp = jf < 268435456.0 ? -1 : (jf > 268435456.0 ? 1 : 0);  // vs 2^28
     int64_t D;  // steady increment in ulps (S stays even after a tie)
     if (frac_cmp < 0) D = q;
     else if (frac_cmp > 0) D = q + 1;
@@ -234,12 +237,7 @@ PB_HD float seq_add_f32(float s, float c, uint32_t n) {
     if (room <= 0) continue;
     int64_t m = room < (int64_t)n ? room : (int64_t)n;
     int64_t S2 = up ? S + m * D : S - m * D;
-    uint32_t nb = (bs & 0xFF800000u) | ((uint32_t)S2 & 0x7FFFFFu);
-#ifdef __CUDA_ARCH__
-    s = __uint_as_float(nb);
-#else
-    { union { float f; uint32_t u; } a4; a4.u = nb; s = a4.f; }
-#endif
+    s = f32_from_bits((bs & 0xFF800000u) | ((uint32_t)S2 & 0x7FFFFFu));
     n -= (uint32_t)m;
   }
   return s;

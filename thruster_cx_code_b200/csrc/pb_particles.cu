@@ -126,14 +126,15 @@ __global__ void k_count_cells(const float* __restrict__ x, const float* __restri
   }
 }
 
-// rho = seq(seq(rho0, +c, k_ion), -c, k_ele); counts are cleared for reuse
-__global__ void k_rho_finalize(float* rho, int* cnt_i, int* cnt_e, int G, float cd, int accumulate) {
+// rho = seq(seq(rho0, +c, k_ion), -c, k_ele) with the float64 addend of np.add.at;
+// counts are cleared for reuse
+__global__ void k_rho_finalize(float* rho, int* cnt_i, int* cnt_e, int G, double cd, int accumulate) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G; i += gridDim.x * blockDim.x) {
     float s = accumulate ? rho[i] : 0.0f;
     int ki = cnt_i ? cnt_i[i] : 0;
     int ke = cnt_e ? cnt_e[i] : 0;
-    if (ki) s = seq_add_f32(s, cd, (uint32_t)ki);
-    if (ke) s = seq_add_f32(s, -cd, (uint32_t)ke);
+    if (ki) s = seq_add_f32d(s, cd, (uint32_t)ki);
+    if (ke) s = seq_add_f32d(s, -cd, (uint32_t)ke);
     rho[i] = s;
     if (cnt_i) cnt_i[i] = 0;
     if (cnt_e) cnt_e[i] = 0;

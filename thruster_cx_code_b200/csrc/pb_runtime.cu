@@ -475,7 +475,7 @@ static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
   }
 
   // B. deposit (counts -> exact float32 sums) and the Picard field solve (:1104-1161)
-  k_rho_finalize<<<grid_for(s, N, 256), 256, 0, st>>>(s->rho, s->cnt_i, s->cnt_e, N, (float)p->charge_density, 0);
+  k_rho_finalize<<<grid_for(s, N, 256), 256, 0, st>>>(s->rho, s->cnt_i, s->cnt_e, N, p->charge_density, 0);
   ++s->launches;
   mark(s);
   if (p->do_poisson && (rc = launch_poisson(s, p->picard_iters, p))) return rc;
@@ -1015,7 +1015,7 @@ int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t nu
   int g = (int)std::min<long>((num_p + 255) / 256, 148L * 16);
   k_count_cells<<<g, 256, 0, st>>>(x, y, nullptr, num_p, 0, cnt, nx, ny, (float)dx, (float)dy);
   k_rho_finalize<<<(int)std::min<long>((G + 255) / 256, 148L * 16), 256, 0, st>>>(rho, cnt, nullptr, G,
-                                                                                  (float)charge_density, 1);
+                                                                                  charge_density, 1);
   CK(cudaFreeAsync(cnt, st));
   CK(cudaGetLastError());
   return PB_OK;
@@ -1068,7 +1068,7 @@ int32_t pb_segment_hits_grid(const uint8_t* isBound, int32_t nx, int32_t ny, dou
 }
 
 // ------------------------------------------------------------------ host helpers
-float pb_host_seq_add_f32(float s, float c, uint32_t n) { return seq_add_f32(s, c, n); }
+float pb_host_seq_add_f32d(float s, double c, uint32_t n) { return seq_add_f32d(s, c, n); }
 double pb_host_philox_uniform(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j) {
   return philox_uniform(seed, pid, site, step, j);
 }
