@@ -131,7 +131,7 @@ def make_gpu_sim(name, device, seed):
     w = W.WORKLOADS[name]
     v_b, v_ti, v_te = W.thermal_speeds(sim, params)
     ions, eles = W.preload(sim.isBound, sim.dx, sim.dy, sim.Lx, sim.Ly, w["n_ions"], w["n_e"], v_b, 4 * v_ti, v_te,
-                           seed=seed)
+                           seed=seed, x_max_ions=W.plume_boundary(sim, params))
     sim.set_particles("ions", *ions)
     sim.set_particles("electrons", *eles)
     return sim, params
@@ -265,7 +265,8 @@ def _oracle_sim(name, n_ions, n_e, seed):
     params = W.configure(o, name)
     o.build_domain(params)
     v_b, v_ti, v_te = W.thermal_speeds(o, params)
-    ions, eles = W.preload(o.isBound, o.dx, o.dy, o.Lx, o.Ly, n_ions, n_e, v_b, 4 * v_ti, v_te, seed=seed)
+    ions, eles = W.preload(o.isBound, o.dx, o.dy, o.Lx, o.Ly, n_ions, n_e, v_b, 4 * v_ti, v_te, seed=seed,
+                           x_max_ions=W.plume_boundary(o, params))
     o._add_ions(*ions, np.zeros(n_ions, bool), o.new_ion_ids(n_ions))
     o._add_electrons(*eles, o.new_e_ids(n_e))
     return o, params

@@ -59,29 +59,36 @@ def configure(sim, name, n_scale=1.0):
     return dict(w["params"])
 
 
-def preload(isBound, dx, dy, Lx, Ly, n_ions, n_e, v_bohm, v_th_i, v_th_e, seed=0):
-    """Seeded initial particles over the non-electrode cells (float32 SoA)."""
+def preload(isBound, dx, dy, Lx, Ly, n_ions, n_e, v_bohm, v_th_i, v_th_e, seed=0, x_max_ions=None):
+    """Seeded initial particles over the non-electrode cells (float32 SoA).  Ions fill
+    x in [1.5 dx, x_max_ions] (the plume boundary: ions beyond it leave at the first
+    step), electrons the whole domain."""
     rs = np.random.RandomState(seed)
     ny, nx = isBound.shape
 
-    def positions(n):
+    def positions(n, x_hi):
         xs, ys, got = [], [], 0
         while got < n:
             m = max(2 * (n - got), 1024)
-            x = rs.uniform(1.5 * dx, Lx - dx, m)
+            x = rs.uniform(1.5 * dx, x_hi, m)
             y = rs.uniform(0.0, Ly, m)
             ok = ~isBound[np.clip(np.round(y / dy).astype(np.int64), 0, ny - 1),
                           np.clip(np.round(x / dx).astype(np.int64), 0, nx - 1)]
             xs.append(x[ok]); ys.append(y[ok]); got += int(ok.sum())
         return np.concatenate(xs)[:n].astype(np.float32), np.concatenate(ys)[:n].astype(np.float32)
 
-    xi, yi = positions(n_ions)
+    xi, yi = positions(n_ions, min(Lx - dx, x_max_ions) if x_max_ions else Lx - dx)
     ions = (xi, yi, (v_bohm + v_th_i * rs.randn(n_ions)).astype(np.float32),
             (v_th_i * rs.randn(n_ions)).astype(np.float32), (v_th_i * rs.randn(n_ions)).astype(np.float32))
-    xe, ye = positions(n_e)
+    xe, ye = positions(n_e, Lx - dx)
     eles = (xe, ye, (v_th_e * rs.randn(n_e)).astype(np.float32), (v_th_e * rs.randn(n_e)).astype(np.float32),
             (v_th_e * rs.randn(n_e)).astype(np.float32))
     return ions, eles
+
+
+def plume_boundary(sim, params):
+    grids = params.get("grids", [])
+    return sim.grid_x_ends[-1] + grids[-1]["gap"] if grids else None
 
 
 def thermal_speeds(sim, params):
