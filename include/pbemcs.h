@@ -204,6 +204,11 @@ void* pb_sim_stream(pb_sim* s);
  * steps profiled, out[8] = kernels enqueued by that call. */
 int32_t pb_sim_timing(pb_sim* s, double* out_host9);
 int32_t pb_sim_set_profiling(pb_sim* s, int32_t on);
+/* Field-solve phase trace: returns the accumulated nanoseconds per phase (out32 may be
+ * NULL: [l] down leg of level l, [7] coarse part, [8+l] up leg of level l, [15] Krylov
+ * updates, [16] FP64 refinement, [17] right-hand side, [18] Picard update, [19] field,
+ * [20] set-up), clears them and switches tracing on or off. */
+int32_t pb_sim_poisson_trace(pb_sim* s, int32_t on, double* out32);
 
 /* ---------------------------------------------------------------- host helpers */
 /* n sequential additions s = (float)((double)s + c), as np.add.at on a float32 array */

@@ -22,7 +22,10 @@ struct Level {
   int ny = 0, nx = 0, per = 0, wrapP = 0, ncolors = 2;
   std::vector<uint8_t> act;   // active nodes (level 0: free nodes)
   std::vector<float> st;      // 9 * N stencil (coarse levels)
+  std::vector<float> dinv;    // omega / diagonal on active nodes (damped Jacobi smoother)
 };
+
+constexpr double JACOBI_OMEGA = 0.8;
 
 struct Hierarchy {
   std::vector<Level> lev;
@@ -170,6 +173,23 @@ inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>&
       if (C.act[c] && !(C.st[4 * Nc + c] > 0.0f)) C.act[c] = 0;
     C.ncolors = colors_for(C, (int)H.lev.size());
     H.lev.push_back(std::move(C));
+  }
+  // smoother weights omega / A_ii on every level
+  for (size_t l = 0; l < H.lev.size(); ++l) {
+    Level& L = H.lev[l];
+    size_t N = (size_t)L.ny * L.nx;
+    L.dinv.assign(N, 0.0f);
+    for (size_t i = 0; i < N; ++i) {
+      if (!L.act[i]) continue;
+      double d;
+      if (l == 0) {
+        row_of(L, 0, cls0, (long)i, row);
+        d = row.back().v;  // the diagonal entry is pushed last on level 0
+      } else {
+        d = L.st[4 * N + i];
+      }
+      L.dinv[i] = d > 0.0 ? (float)(JACOBI_OMEGA / d) : 0.0f;
+    }
   }
   // dense inverse of the coarsest operator (Cholesky, then L^-T L^-1)
   Level& Lc = H.lev.back();

@@ -20,7 +20,8 @@
 // guarantees co-residency).  Every wait is bounded: on time-out the kernel sets
 // PB_EF_SPIN_TIMEOUT, stops waiting at later barriers and runs to completion.
 // Reductions are deterministic: one partial per block, summed in block order.
-// Data written by other blocks within the launch is read with ld.global.cg (L2).
+// Data written by other blocks within the launch is read only after a grid barrier,
+// which ends with an acquire fence in every thread.
 #include "pb_common.cuh"
 #include "pb_poisson.cuh"
 
@@ -51,6 +52,20 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, uint32_t* err) {
     __threadfence();
   }
   __syncthreads();
+  // every thread acquires at gpu scope, so its later (L1-cached) loads observe the
+  // stores other blocks made before arriving
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
+// phase tracing (block 0, thread 0): time since the previous mark is added to trace[k]
+__device__ __forceinline__ void tmark(const PoissonArgs& a, int k) {
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    unsigned long long last = a.trace[31];
+    if (last) a.trace[k] += now - last;
+    a.trace[31] = now;
+  }
 }
 
 // deterministic grid-wide sum; contains one barrier
@@ -70,7 +85,7 @@ __device__ double grid_sum(double v, const PoissonArgs& a, int& slot) {
   if (threadIdx.x < 32) {
     // lanes take fixed strided subsets, then a fixed shuffle tree: same order in every block
     double s = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) s += __ldcg(part + b);
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) s += (*(part + b));
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
     if (threadIdx.x == 0) bc = s;
   }
@@ -102,11 +117,11 @@ __device__ __forceinline__ float apply0f(const PoissonArgs& a, const float* v, i
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     Nb n = nb0(a, y, x, DY[k], DX[k]);
-    if (n.c == NC_FREE) s += __ldcg(v + n.j);
+    if (n.c == NC_FREE) s += (*(v + n.j));
     else if (n.c == NC_NEU) ++nneu;
   }
   diag = (float)(4 - nneu);
-  return diag * __ldcg(v + i) - s;
+  return diag * (*(v + i)) - s;
 }
 
 __device__ __forceinline__ double apply0d(const PoissonArgs& a, const double* v, int i, int y, int x) {
@@ -116,10 +131,10 @@ __device__ __forceinline__ double apply0d(const PoissonArgs& a, const double* v,
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     Nb n = nb0(a, y, x, DY[k], DX[k]);
-    if (n.c == NC_FREE) s += __ldcg(v + n.j);
+    if (n.c == NC_FREE) s += (*(v + n.j));
     else if (n.c == NC_NEU) ++nneu;
   }
-  return (double)(4 - nneu) * __ldcg(v + i) - s;
+  return (double)(4 - nneu) * (*(v + i)) - s;
 }
 
 // ----------------------------------------------------------------- coarse (9-point) helpers
@@ -130,87 +145,75 @@ __device__ __forceinline__ int nbc(const MgLevel& L, int y, int x, int dI, int d
   return yy * L.nx + xx;
 }
 
-__device__ __forceinline__ float applyc_off(const MgLevel& L, const float* v, int i, int y, int x) {
-  const int N = L.ny * L.nx;
-  float s = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    if (k == 4) continue;
-    int j = nbc(L, y, x, k / 3 - 1, k % 3 - 1);
-    if (j >= 0) s += __ldg(L.st + (size_t)k * N + i) * __ldcg(v + j);
-  }
-  return s;
-}
-
-__device__ __forceinline__ int color_of(const MgLevel& L, int level, int y, int x) {
-  if (level == 0) return (y + x) & 1;
-  int yc = (L.per && (L.ny & 1) && y == L.ny - 1) ? 2 : (y & 1);
-  return yc * 2 + (x & 1);
-}
+// Loads and stores of level vectors.  PRIV: data only block 0 touches (the small
+// levels).  Loads go through L1 in both cases: data written by other blocks is read only
+// after a grid barrier, whose acquire fence orders the load after those stores.
+template <bool PRIV> __device__ __forceinline__ float ldv(const float* p) { return *p; }
+template <bool PRIV> __device__ __forceinline__ void stv(float* p, float v) { if (PRIV) *p = v; else __stcg(p, v); }
 
 __device__ __forceinline__ bool active(const PoissonArgs& a, int level, int i) {
   return level == 0 ? (__ldg(a.cls + i) == NC_FREE) : (__ldg(a.lev[level].act + i) != 0);
 }
 
-// one Gauss-Seidel colour on level `level`; `zero_init` writes 0 to every node not in
-// the colour (the first half-sweep from a zero guess).
-__device__ __forceinline__ void gs_color(const PoissonArgs& a, int level, int color, bool zero_init, int tid,
-                                         int nth) {
-  const MgLevel& L = a.lev[level];
-  const int N = L.ny * L.nx;
-  for (int i = tid; i < N; i += nth) {
-    int y = i / L.nx, x = i - y * L.nx;
-    bool act = active(a, level, i);
-    bool mine = act && color_of(L, level, y, x) == color;
-    if (!mine) {
-      if (zero_init) __stcg(L.z + i, 0.0f);
-      continue;
-    }
-    float r = __ldcg(L.r + i);
-    float nv;
-    if (level == 0) {
-      float diag;
-      float az = zero_init ? 0.0f : apply0f(a, L.z, i, y, x, diag);
-      if (zero_init) {
-        const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
-        int nneu = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) if (nb0(a, y, x, DY[k], DX[k]).c == NC_NEU) ++nneu;
-        diag = (float)(4 - nneu);
-        nv = r / diag;
-      } else {
-        float zi = __ldcg(L.z + i);
-        // z_i = (r_i + sum_free z_j) / diag  with  A z = diag z_i - sum_free z_j
-        nv = (r - (az - diag * zi)) / diag;
-      }
-    } else {
-      float off = zero_init ? 0.0f : applyc_off(L, L.z, i, y, x);
-      nv = (r - off) / __ldg(L.st + (size_t)4 * N + i);
-    }
-    __stcg(L.z + i, nv);
-  }
-}
-
-// residual of level `level` restricted onto level+1 (r_{l+1} = P^T (r_l - A_l z_l))
-__device__ __forceinline__ float residual_at(const PoissonArgs& a, int level, int i, int y, int x) {
-  const MgLevel& L = a.lev[level];
+// (A_l v)_i for an active node i, with v_j supplied by the callable vj(j) (inactive
+// neighbours contribute nothing: their value is zero in every vector of the cycle)
+template <class V>
+__device__ __forceinline__ float apply_A(const PoissonArgs& a, int level, int i, int y, int x, V vj) {
   if (level == 0) {
-    float diag;
-    float az = apply0f(a, L.z, i, y, x, diag);
-    return __ldcg(L.r + i) - az;
+    const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
+    float s = 0.0f;
+    int nneu = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      Nb n = nb0(a, y, x, DY[k], DX[k]);
+      if (n.c == NC_FREE) s += vj(n.j);
+      else if (n.c == NC_NEU) ++nneu;
+    }
+    return (float)(4 - nneu) * vj(i) - s;
   }
+  const MgLevel& L = a.lev[level];
   const int N = L.ny * L.nx;
-  float az = applyc_off(L, L.z, i, y, x) + __ldg(L.st + (size_t)4 * N + i) * __ldcg(L.z + i);
-  return __ldcg(L.r + i) - az;
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    int j = (k == 4) ? i : nbc(L, y, x, k / 3 - 1, k % 3 - 1);
+    if (j >= 0) s += __ldg(L.st + (size_t)k * N + i) * vj(j);
+  }
+  return s;
 }
 
-__device__ __forceinline__ void restrict_to(const PoissonArgs& a, int level, int tid, int nth) {
+// (P z_{l+1}) at fine node (y, x) of level l
+template <bool PRIV>
+__device__ __forceinline__ float prolong_at(const MgLevel& C, int y, int x) {
+  int I0 = y >> 1, J0 = x >> 1, ai = y & 1, bj = x & 1;
+  float s = 0.0f;
+  for (int da = 0; da <= ai; ++da) {
+    int I = I0 + da;
+    if (I >= C.ny) { if (C.wrapP) I -= C.ny; else continue; }
+    float wy = ai ? 0.5f : 1.0f;
+    for (int db = 0; db <= bj; ++db) {
+      int J = J0 + db;
+      if (J >= C.nx) continue;
+      float wx = bj ? 0.5f : 1.0f;
+      s += wy * wx * ldv<PRIV>(C.z + I * C.nx + J);
+    }
+  }
+  return s;
+}
+
+// Down leg of the V-cycle on level l: with the pre-smoothed z = omega D^-1 r (one damped
+// Jacobi sweep from zero), r_{l+1} = P^T (r_l - A_l z), all evaluated from r_l.
+template <bool PRIV>
+__device__ __forceinline__ void down_leg(const PoissonArgs& a, int level, int tid, int nth) {
   const MgLevel& F = a.lev[level];
   const MgLevel& C = a.lev[level + 1];
   const int Nc = C.ny * C.nx;
   const bool wrap = C.wrapP;
+  const float* r = F.r;
+  const float* dinv = F.dinv;
+  auto zpre = [&](int j) { return __ldg(dinv + j) * ldv<PRIV>(r + j); };
   for (int ic = tid; ic < Nc; ic += nth) {
-    if (!__ldg(C.act + ic)) { __stcg(C.r + ic, 0.0f); __stcg(C.z + ic, 0.0f); continue; }
+    if (!__ldg(C.act + ic)) { stv<PRIV>(C.r + ic, 0.0f); continue; }
     int I = ic / C.nx, J = ic - I * C.nx;
     float s = 0.0f;
 #pragma unroll
@@ -226,110 +229,100 @@ __device__ __forceinline__ void restrict_to(const PoissonArgs& a, int level, int
         int f = yf * F.nx + xf;
         if (!active(a, level, f)) continue;
         float wx = db == 0 ? 1.0f : 0.5f;
-        s += wy * wx * residual_at(a, level, f, yf, xf);
+        float res = ldv<PRIV>(r + f) - apply_A(a, level, f, yf, xf, zpre);
+        s += wy * wx * res;
       }
     }
-    __stcg(C.r + ic, s);
+    stv<PRIV>(C.r + ic, s);
   }
 }
 
-// z_l += P z_{l+1}
-__device__ __forceinline__ void prolong_add(const PoissonArgs& a, int level, int tid, int nth) {
+// Up leg on level l: z_mid = omega D^-1 r + P z_{l+1}; one damped Jacobi sweep,
+// z = z_mid + omega D^-1 (r - A z_mid), all evaluated from r_l and z_{l+1}.
+// PRIV_C: the coarse correction is private to block 0 as well.
+template <bool PRIV, bool PRIV_C>
+__device__ __forceinline__ void up_leg(const PoissonArgs& a, int level, int tid, int nth) {
   const MgLevel& F = a.lev[level];
   const MgLevel& C = a.lev[level + 1];
   const int N = F.ny * F.nx;
+  const float* r = F.r;
+  const float* dinv = F.dinv;
+  auto zmid = [&](int j) {
+    int yj = j / F.nx, xj = j - yj * F.nx;
+    return __ldg(dinv + j) * ldv<PRIV>(r + j) + prolong_at<PRIV_C>(C, yj, xj);
+  };
   for (int i = tid; i < N; i += nth) {
-    if (!active(a, level, i)) continue;
+    if (!active(a, level, i)) { stv<PRIV>(F.z + i, 0.0f); continue; }
     int y = i / F.nx, x = i - y * F.nx;
-    int I0 = y >> 1, J0 = x >> 1;
-    int ai = y & 1, bj = x & 1;
-    float s = 0.0f;
-    for (int da = 0; da <= ai; ++da) {
-      int I = I0 + da;
-      if (I >= C.ny) { if (C.wrapP) I -= C.ny; else continue; }
-      float wy = ai ? 0.5f : 1.0f;
-      for (int db = 0; db <= bj; ++db) {
-        int J = J0 + db;
-        if (J >= C.nx) continue;
-        float wx = bj ? 0.5f : 1.0f;
-        s += wy * wx * __ldcg(C.z + I * C.nx + J);
-      }
-    }
-    __stcg(F.z + i, __ldcg(F.z + i) + s);
+    float zm = zmid(i);
+    float az = apply_A(a, level, i, y, x, zmid);
+    stv<PRIV>(F.z + i, zm + __ldg(dinv + i) * (ldv<PRIV>(r + i) - az));
   }
 }
 
 // coarsest level: z = A_c^{-1} r (dense, one block)
+template <bool PRIV>
 __device__ void coarse_solve(const PoissonArgs& a, int level) {
   const MgLevel& L = a.lev[level];
   const int N = L.ny * L.nx;
   __shared__ float rc[1024];
-  for (int i = threadIdx.x; i < N; i += blockDim.x) __stcg(L.z + i, 0.0f);
-  for (int k = threadIdx.x; k < a.nc; k += blockDim.x) rc[k] = __ldcg(L.r + a.cidx[k]);
+  for (int i = threadIdx.x; i < N; i += blockDim.x) stv<PRIV>(L.z + i, 0.0f);
+  for (int k = threadIdx.x; k < a.nc; k += blockDim.x) rc[k] = ldv<PRIV>(L.r + a.cidx[k]);
   __syncthreads();
   for (int k = threadIdx.x; k < a.nc; k += blockDim.x) {
     float s = 0.0f;
     for (int j = 0; j < a.nc; ++j) s += __ldg(a.cinvT + (size_t)j * a.nc + k) * rc[j];
-    __stcg(L.z + a.cidx[k], s);
+    stv<PRIV>(L.z + a.cidx[k], s);
   }
   __syncthreads();
 }
 
-// the part of the V-cycle below first_small, run by block 0 with block-level syncs
+// The levels from first_small down, run by block 0 with block-level syncs.
 __device__ void small_vcycle(const PoissonArgs& a) {
   const int last = a.nlevels - 1;
   for (int l = a.first_small; l < last; ++l) {
-    const MgLevel& L = a.lev[l];
-    for (int s = 0; s < a.nu; ++s)
-      for (int c = 0; c < L.ncolors; ++c) {
-        gs_color(a, l, c, s == 0 && c == 0, threadIdx.x, blockDim.x);
-        __syncthreads();
-      }
-    restrict_to(a, l, threadIdx.x, blockDim.x);
+    down_leg<true>(a, l, threadIdx.x, blockDim.x);
     __syncthreads();
   }
-  coarse_solve(a, last);
+  coarse_solve<true>(a, last);
   for (int l = last - 1; l >= a.first_small; --l) {
-    const MgLevel& L = a.lev[l];
-    prolong_add(a, l, threadIdx.x, blockDim.x);
+    up_leg<true, true>(a, l, threadIdx.x, blockDim.x);
     __syncthreads();
-    for (int s = 0; s < a.nu; ++s)
-      for (int c = L.ncolors - 1; c >= 0; --c) {
-        gs_color(a, l, c, false, threadIdx.x, blockDim.x);
-        __syncthreads();
-      }
   }
+  // the first small level's correction is read by other blocks through L2
+  __threadfence();
 }
 
-// z0 = M^{-1} r0 (lev[0].r = r32, lev[0].z = z32)
+// z0 = M^{-1} r0 (lev[0].r = r32, lev[0].z = z32): a V(1,1) cycle with damped Jacobi
+// smoothing, two grid barriers per grid-wide level
 __device__ void vcycle(const PoissonArgs& a) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   if (a.nlevels == 1) {
-    if (blockIdx.x == 0) coarse_solve(a, 0);
+    if (blockIdx.x == 0) coarse_solve<false>(a, 0);
     grid_barrier(a.bar, a.errflags);
     return;
   }
   for (int l = 0; l < a.first_small; ++l) {
-    const MgLevel& L = a.lev[l];
-    for (int s = 0; s < a.nu; ++s)
-      for (int c = 0; c < L.ncolors; ++c) {
-        gs_color(a, l, c, s == 0 && c == 0, tid, nth);
-        grid_barrier(a.bar, a.errflags);
+    down_leg<false>(a, l, tid, nth);
+    grid_barrier(a.bar, a.errflags);
+    tmark(a, l < 7 ? l : 6);
+  }
+  if (a.first_small < a.nlevels - 1 || a.first_small == a.nlevels - 1) {
+    if (blockIdx.x == 0) {
+      if (a.first_small == a.nlevels - 1) {
+        coarse_solve<true>(a, a.first_small);
+        __threadfence();
+      } else {
+        small_vcycle(a);
       }
-    restrict_to(a, l, tid, nth);
+    }
     grid_barrier(a.bar, a.errflags);
   }
-  if (blockIdx.x == 0) small_vcycle(a);
-  grid_barrier(a.bar, a.errflags);
+  tmark(a, 7);
   for (int l = a.first_small - 1; l >= 0; --l) {
-    const MgLevel& L = a.lev[l];
-    prolong_add(a, l, tid, nth);
+    up_leg<false, false>(a, l, tid, nth);
     grid_barrier(a.bar, a.errflags);
-    for (int s = 0; s < a.nu; ++s)
-      for (int c = L.ncolors - 1; c >= 0; --c) {
-        gs_color(a, l, c, false, tid, nth);
-        grid_barrier(a.bar, a.errflags);
-      }
+    tmark(a, 8 + (l < 7 ? l : 6));
   }
 }
 
@@ -340,6 +333,7 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
   const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
   int slot = 0;
   double n_outer = 0, n_inner = 0, last_rel = 0;
+  tmark(a, 20);
 
   // Dirichlet-neighbour sums (V_fixed is constant during the launch)
   for (int i = tid; i < N; i += nth) {
@@ -359,7 +353,7 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
     double ff = 0.0, rr = 0.0;
     for (int i = tid; i < N; i += nth) {
       if (__ldg(a.cls + i) != NC_FREE) continue;
-      double Vi = __ldcg(a.V + i);
+      double Vi = (*(a.V + i));
       double vm = Vi < a.V_plasma ? Vi : a.V_plasma;
       double rho_e = DMUL(a.qn0_neg, exp(DDIV(DSUB(vm, a.V_plasma), a.Te_up)));
       double rt = DADD((double)__ldg(a.rho + i), rho_e);
@@ -370,12 +364,13 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
     for (int i = tid; i < N; i += nth) {
       if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
       int y = i / a.nx, x = i - y * a.nx;
-      double res = __ldcg(a.f + i) - apply0d(a, a.x, i, y, x);
+      double res = (*(a.f + i)) - apply0d(a, a.x, i, y, x);
       __stcg(a.r32 + i, (float)res);
       rr += res * res;
     }
     double fnorm2 = grid_sum(ff, a, slot);
     double rnorm2 = grid_sum(rr, a, slot);
+    tmark(a, 17);
     double target2 = a.tol * a.tol * fnorm2;
 
     for (int outer = 0; outer < a.max_outer && rnorm2 > target2 && fnorm2 > 0.0; ++outer) {
@@ -385,9 +380,10 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
       double rz_old = 0.0, rr0 = rnorm2;
       for (int k = 0; k < a.max_inner; ++k) {
         n_inner += 1;
+        tmark(a, 15);
         vcycle(a);  // z32 = M r32; ends with a barrier
         double rz_p = 0.0;
-        for (int i = tid; i < N; i += nth) rz_p += (double)__ldcg(a.r32 + i) * (double)__ldcg(a.z32 + i);
+        for (int i = tid; i < N; i += nth) rz_p += (double)(*(a.r32 + i)) * (double)(*(a.z32 + i));
         double rz = grid_sum(rz_p, a, slot);
         double beta = k == 0 ? 0.0 : rz / rz_old;
         double pq_p = 0.0;
@@ -396,8 +392,8 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
           int y = i / a.nx, x = i - y * a.nx;
           float diag;
           float az = apply0f(a, a.z32, i, y, x, diag);
-          float p = __ldcg(a.z32 + i) + (float)beta * (k == 0 ? 0.0f : __ldcg(a.p32 + i));
-          float q = az + (float)beta * (k == 0 ? 0.0f : __ldcg(a.q32 + i));
+          float p = (*(a.z32 + i)) + (float)beta * (k == 0 ? 0.0f : (*(a.p32 + i)));
+          float q = az + (float)beta * (k == 0 ? 0.0f : (*(a.q32 + i)));
           __stcg(a.p32 + i, p);
           __stcg(a.q32 + i, q);
           pq_p += (double)p * (double)q;
@@ -407,29 +403,31 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
         double rr_p = 0.0;
         for (int i = tid; i < N; i += nth) {
           if (__ldg(a.cls + i) != NC_FREE) continue;
-          float e = __ldcg(a.e32 + i) + (float)alpha * __ldcg(a.p32 + i);
-          float r = __ldcg(a.r32 + i) - (float)alpha * __ldcg(a.q32 + i);
+          float e = (*(a.e32 + i)) + (float)alpha * (*(a.p32 + i));
+          float r = (*(a.r32 + i)) - (float)alpha * (*(a.q32 + i));
           __stcg(a.e32 + i, e);
           __stcg(a.r32 + i, r);
           rr_p += (double)r * (double)r;
         }
         double rrk = grid_sum(rr_p, a, slot);
+        tmark(a, 15);
         rz_old = rz;
         if (rrk <= a.tol_inner * a.tol_inner * rr0 || rrk <= target2 * 1e-4) break;
       }
       // ---- FP64 correction and true residual
       for (int i = tid; i < N; i += nth)
-        if (__ldg(a.cls + i) == NC_FREE) __stcg(a.x + i, __ldcg(a.x + i) + (double)__ldcg(a.e32 + i));
+        if (__ldg(a.cls + i) == NC_FREE) __stcg(a.x + i, (*(a.x + i)) + (double)(*(a.e32 + i)));
       grid_barrier(a.bar, a.errflags);
       rr = 0.0;
       for (int i = tid; i < N; i += nth) {
         if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
         int y = i / a.nx, x = i - y * a.nx;
-        double res = __ldcg(a.f + i) - apply0d(a, a.x, i, y, x);
+        double res = (*(a.f + i)) - apply0d(a, a.x, i, y, x);
         __stcg(a.r32 + i, (float)res);
         rr += res * res;
       }
       rnorm2 = grid_sum(rr, a, slot);
+      tmark(a, 16);
     }
     if (!(rnorm2 <= target2) && fnorm2 > 0.0 && tid == 0) atomicOr(a.errflags, PB_EF_POISSON_NOCONV);
     last_rel = fnorm2 > 0.0 ? sqrt(rnorm2 / fnorm2) : 0.0;
@@ -438,7 +436,7 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
     for (int i = tid; i < N; i += nth) {
       uint8_t c = __ldg(a.cls + i);
       double vn;
-      if (c == NC_FREE) vn = __ldcg(a.x + i);
+      if (c == NC_FREE) vn = (*(a.x + i));
       else if (c == NC_DIR) vn = __ldg(a.Vfixed + i);
       else {
         int y = i / a.nx, x = i - y * a.nx;
@@ -451,13 +449,14 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
         else sy = a.ny - 2;
         int j = sy * a.nx + sx;
         uint8_t cj = __ldg(a.cls + j);
-        vn = (cj == NC_DIR) ? __ldg(a.Vfixed + j) : __ldcg(a.x + j);
+        vn = (cj == NC_DIR) ? __ldg(a.Vfixed + j) : (*(a.x + j));
       }
       if (c != NC_FREE) __stcg(a.x + i, vn);
-      double Vi = __ldcg(a.V + i);
+      double Vi = (*(a.V + i));
       __stcg(a.V + i, DADD(DMUL(a.omega_keep, Vi), DMUL(a.omega_new, vn)));
     }
     grid_barrier(a.bar, a.errflags);
+    tmark(a, 18);
   }
 
   // ---- E = -grad V (np.gradient: central inside, one-sided at the edges; periodic y fix)
@@ -466,18 +465,19 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
       int y = i / a.nx, x = i - y * a.nx;
       const double* V = a.V;
       double ex, ey;
-      if (x == 0) ex = DDIV(DSUB(-__ldcg(V + i + 1), -__ldcg(V + i)), a.hx);
-      else if (x == a.nx - 1) ex = DDIV(DSUB(-__ldcg(V + i), -__ldcg(V + i - 1)), a.hx);
-      else ex = DDIV(DSUB(-__ldcg(V + i + 1), -__ldcg(V + i - 1)), a.two_hx);
-      if (a.periodic && y == 0) ey = DDIV(DSUB(__ldcg(V + (size_t)(a.ny - 1) * a.nx + x), __ldcg(V + a.nx + x)), a.two_hy_per);
-      else if (a.periodic && y == a.ny - 1) ey = DDIV(DSUB(__ldcg(V + (size_t)(a.ny - 2) * a.nx + x), __ldcg(V + x)), a.two_hy_per);
-      else if (y == 0) ey = DDIV(DSUB(-__ldcg(V + i + a.nx), -__ldcg(V + i)), a.hy);
-      else if (y == a.ny - 1) ey = DDIV(DSUB(-__ldcg(V + i), -__ldcg(V + i - a.nx)), a.hy);
-      else ey = DDIV(DSUB(-__ldcg(V + i + a.nx), -__ldcg(V + i - a.nx)), a.two_hy);
+      if (x == 0) ex = DDIV(DSUB(-(*(V + i + 1)), -(*(V + i))), a.hx);
+      else if (x == a.nx - 1) ex = DDIV(DSUB(-(*(V + i)), -(*(V + i - 1))), a.hx);
+      else ex = DDIV(DSUB(-(*(V + i + 1)), -(*(V + i - 1))), a.two_hx);
+      if (a.periodic && y == 0) ey = DDIV(DSUB((*(V + (size_t)(a.ny - 1) * a.nx + x)), (*(V + a.nx + x))), a.two_hy_per);
+      else if (a.periodic && y == a.ny - 1) ey = DDIV(DSUB((*(V + (size_t)(a.ny - 2) * a.nx + x)), (*(V + x))), a.two_hy_per);
+      else if (y == 0) ey = DDIV(DSUB(-(*(V + i + a.nx)), -(*(V + i))), a.hy);
+      else if (y == a.ny - 1) ey = DDIV(DSUB(-(*(V + i)), -(*(V + i - a.nx))), a.hy);
+      else ey = DDIV(DSUB(-(*(V + i + a.nx)), -(*(V + i - a.nx))), a.two_hy);
       a.Ex[i] = __double2float_rn(ex);
       a.Ey[i] = __double2float_rn(ey);
     }
   }
+  tmark(a, 19);
   if (tid == 0) {
     a.stats[0] += n_outer;
     a.stats[1] += n_inner;

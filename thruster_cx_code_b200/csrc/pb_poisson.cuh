@@ -14,6 +14,7 @@ struct MgLevel {
   int ncolors;    // smoother colours (2 on level 0, 4 or 6 on coarse levels)
   const uint8_t* act;     // active (unknown) nodes; level 0: class array instead
   const float* st;        // 9-point stencil, st[k * N + i], k = (dI+1)*3 + (dJ+1); null on level 0
+  const float* dinv;      // omega / diagonal on active nodes, 0 elsewhere (Jacobi smoother)
   float *r, *z;           // right-hand side and correction on this level
 };
 
@@ -42,7 +43,6 @@ struct PoissonArgs {
   double tol;             // relative FP64 residual target ||f - A x|| / ||f||
   double tol_inner;       // relative residual reduction of each FP32 MG-PCG solve
   int max_outer, max_inner;
-  int nu;                 // smoothing sweeps per level
   // hierarchy
   int nlevels;            // including level 0 and the coarsest
   int first_small;        // first level handled by a single block
@@ -55,6 +55,7 @@ struct PoissonArgs {
   unsigned int* bar;      // [count, generation]
   uint32_t* errflags;
   double* stats;          // [outer its, inner its, final rel residual, solves] accumulated
+  unsigned long long* trace;  // optional: ns per phase category (block 0), [31] = last stamp
 };
 
 }  // namespace pb

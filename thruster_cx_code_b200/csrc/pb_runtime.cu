@@ -52,6 +52,7 @@ struct DevLevel {
   int ny = 0, nx = 0, per = 0, wrapP = 0, ncolors = 2;
   uint8_t* act = nullptr;
   float* st = nullptr;
+  float* dinv = nullptr;
   float* r = nullptr;
   float* z = nullptr;
 };
@@ -78,6 +79,8 @@ struct Sim {
   double* partials = nullptr;
   unsigned int* bar = nullptr;
   double* pstats = nullptr;
+  unsigned long long* ptrace = nullptr;  // field-solve phase trace (32 slots)
+  int trace_on = 0;
   int pgrid = 0;
   // particles
   Species sp[2];
@@ -206,6 +209,7 @@ static int32_t ensure_room(Sim* s, const pb_step_params* p, int steps) {
 
 static void free_levels(Sim* s) {
   for (size_t l = 0; l < s->lev.size(); ++l) {
+    dfree(s->lev[l].dinv);
     if (l > 0) { dfree(s->lev[l].act); dfree(s->lev[l].st); dfree(s->lev[l].r); dfree(s->lev[l].z); }
   }
   s->lev.clear();
@@ -232,6 +236,8 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
     DevLevel& D = s->lev[l];
     D.ny = L.ny; D.nx = L.nx; D.per = L.per; D.wrapP = L.wrapP; D.ncolors = L.ncolors;
     size_t N = (size_t)L.ny * L.nx;
+    CK(dalloc(&D.dinv, N));
+    CK(cudaMemcpy(D.dinv, L.dinv.data(), N * sizeof(float), cudaMemcpyHostToDevice));
     if (l == 0) {
       D.act = s->cls; D.st = nullptr; D.r = s->r32; D.z = s->z32;
     } else {
@@ -240,7 +246,7 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
       CK(cudaMemcpy(D.st, L.st.data(), 9 * N * sizeof(float), cudaMemcpyHostToDevice));
       CK(cudaMemset(D.r, 0, N * sizeof(float)));
       CK(cudaMemset(D.z, 0, N * sizeof(float)));
-      if ((int)l < s->first_small && N <= 6000) s->first_small = (int)l;
+      if ((int)l < s->first_small && N <= 2000) s->first_small = (int)l;
     }
   }
   if (s->first_small < 1) s->first_small = 1;
@@ -262,17 +268,19 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
   a.omega_keep = p->omega_keep; a.omega_new = p->omega_new;
   a.hx = p->hx; a.two_hx = p->two_hx; a.hy = p->hy; a.two_hy = p->two_hy; a.two_hy_per = p->two_hy_per;
   a.iterations = iterations; a.compute_field = 1;
-  a.tol = s->tol; a.tol_inner = s->tol_inner; a.max_outer = s->max_outer; a.max_inner = s->max_inner; a.nu = s->nu;
+  a.tol = s->tol; a.tol_inner = s->tol_inner; a.max_outer = s->max_outer; a.max_inner = s->max_inner;
   a.nlevels = (int)s->lev.size(); a.first_small = s->first_small;
   for (size_t l = 0; l < s->lev.size() && l < (size_t)MG_MAX_LEVELS; ++l) {
     const DevLevel& D = s->lev[l];
     a.lev[l].ny = D.ny; a.lev[l].nx = D.nx; a.lev[l].per = D.per; a.lev[l].wrapP = D.wrapP;
     a.lev[l].ncolors = D.ncolors; a.lev[l].act = D.act; a.lev[l].st = D.st; a.lev[l].r = D.r; a.lev[l].z = D.z;
+    a.lev[l].dinv = D.dinv;
   }
   a.nc = s->nc; a.cidx = s->cidx; a.cinvT = s->cinvT;
   a.partials = s->partials; a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
   a.stats = s->pstats;
+  a.trace = s->trace_on ? s->ptrace : nullptr;
   return a;
 }
 
@@ -622,6 +630,8 @@ int32_t pb_sim_create(pb_sim** out, int32_t device) {
   CK(dalloc(&s->partials, 4 * (size_t)s->pgrid));
   CK(dalloc(&s->bar, 2));
   CK(dalloc(&s->pstats, 4));
+  CK(dalloc(&s->ptrace, 32));
+  CK(cudaMemset(s->ptrace, 0, 32 * sizeof(unsigned long long)));
   CK(cudaMemset(s->pstats, 0, 4 * sizeof(double)));
   CK(dalloc(&s->counts, 4));
   CK(cudaMemset(s->counts, 0, 4 * sizeof(int)));
@@ -979,6 +989,19 @@ int32_t pb_sim_timing(pb_sim* h, double* out) {
       }
     out[7] = (double)steps;
   }
+  return PB_OK;
+}
+
+int32_t pb_sim_poisson_trace(pb_sim* h, int32_t on, double* out32) {
+  Sim* s = &h->s;
+  if (out32) {
+    unsigned long long t[32];
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(t, s->ptrace, sizeof(t), cudaMemcpyDeviceToHost));
+    for (int k = 0; k < 32; ++k) out32[k] = (double)t[k];
+  }
+  CK(cudaMemset(s->ptrace, 0, 32 * sizeof(unsigned long long)));
+  s->trace_on = on ? 1 : 0;
   return PB_OK;
 }
 
