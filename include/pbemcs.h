@@ -51,6 +51,18 @@ const char* pb_last_error(void);
 int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy,
                           int32_t nx, int32_t ny, double charge_density, void* stream);
 
+/* The deposit of pb_accumulate_rho without any device allocation, for callers that
+ * cannot allocate (memory already reserved by another framework's pool, real-time loops
+ * that must stay off the driver's allocation path, fixed device-memory budgets).  It has
+ * no counterpart in the reference.  The per-cell count scratch is a file-scope device
+ * array of 2^21 int32 (8 MiB) that every GPU loading the library holds until exit;
+ * grids of more than 2^21 cells are rejected with PB_ERR_ARG.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) and should come before any
+ * stream capture.  All calls share the array and it keeps the last call's counts (each
+ * call clears the cells it uses first), so calls that overlap on the GPU race. */
+int32_t pb_accumulate_rho_noalloc(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy,
+                                  int32_t nx, int32_t ny, double charge_density, void* stream);
+
 /* Bilinear E/B gather + 2D3V Boris + drift (x += vx dt 1000), in place; bit-identical
  * to push_particles_boris_cpu (physics_engine.py:188-254; Taichi form :63-144). */
 int32_t pb_push_particles_boris(float* x, float* y, float* vx, float* vy, float* vz, const float* Ex,

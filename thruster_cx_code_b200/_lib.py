@@ -66,6 +66,7 @@ PROTOTYPES = {
     "pb_version": (i32, []),
     "pb_last_error": (C.c_char_p, []),
     "pb_accumulate_rho": (i32, [vp, vp, vp, i32, f64, f64, i32, i32, f64, vp]),
+    "pb_accumulate_rho_noalloc": (i32, [vp, vp, vp, i32, f64, f64, i32, i32, f64, vp]),
     "pb_push_particles_boris": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, f64, f64, i32, i32, f64, f64, vp]),
     "pb_thermal_conduction": (i32, [vp, vp, vp, i32, i32, f64, f64, vp]),
     "pb_compute_particle_substeps": (i32, [vp, vp, vp, vp, vp, i32, vp, vp, i32, i32, f64, f64, f64, f64, f64, P(f64), vp]),

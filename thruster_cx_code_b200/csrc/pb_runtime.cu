@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1040,6 +1041,65 @@ int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t nu
   k_rho_finalize<<<(int)std::min<long>((G + 255) / 256, 148L * 16), 256, 0, st>>>(rho, cnt, nullptr, G,
                                                                                   charge_density, 1);
   CK(cudaFreeAsync(cnt, st));
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ allocation-free deposit
+// Some callers cannot allocate device memory at the point where they deposit charge: a
+// host application whose memory is already reserved by another framework's pool, a
+// real-time loop that must not take the driver's allocation path (it can block and
+// synchronise), or an embedded process whose device memory budget is fixed at start-up.
+// pb_accumulate_rho_noalloc serves them with its per-cell count scratch in this
+// file-scope device array instead of a temporary allocation.  Every GPU that loads the
+// library holds the array (PB_NOALLOC_MAX_CELLS int32 = 8 MiB) until the process exits.
+#define PB_NOALLOC_MAX_CELLS (1 << 21)
+static __device__ __align__(256) int g_noalloc_counts[PB_NOALLOC_MAX_CELLS];
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_ptr[256] = {nullptr};
+
+// Device address of the scratch array for the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once per device
+// (with that device current) and cached.
+static int32_t noalloc_scratch(int** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return fail(PB_ERR_ARG, "accumulate_rho_noalloc: device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_counts);
+    if (e != cudaSuccess || !p)
+      return fail(PB_ERR_CUDA, std::string("accumulate_rho_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = (int*)g_noalloc_ptr[dev];
+  return PB_OK;
+}
+
+extern "C" {
+
+int32_t pb_accumulate_rho_noalloc(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy,
+                                  int32_t nx, int32_t ny, double charge_density, void* stream) {
+  if (nx < 3 || ny < 3) return fail(PB_ERR_ARG, "accumulate_rho_noalloc: grid must be at least 3 x 3");
+  long long G = (long long)nx * ny;
+  if (G > PB_NOALLOC_MAX_CELLS)
+    return fail(PB_ERR_ARG, "accumulate_rho_noalloc: grid of " + std::to_string(G) + " cells exceeds the " +
+                                std::to_string(PB_NOALLOC_MAX_CELLS) + "-cell scratch; use pb_accumulate_rho");
+  int* cnt = nullptr;
+  int32_t rc = noalloc_scratch(&cnt);
+  if (rc) return rc;
+  if (num_p <= 0) return PB_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  // the array keeps the previous call's counts: clear the cells this call uses
+  CK(cudaMemsetAsync(cnt, 0, (size_t)G * sizeof(int), st));
+  int g = (int)std::min<long>((num_p + 255) / 256, 148L * 16);
+  k_count_cells<<<g, 256, 0, st>>>(x, y, nullptr, num_p, 0, cnt, nx, ny, (float)dx, (float)dy);
+  k_rho_finalize<<<(int)std::min<long>((G + 255) / 256, 148L * 16), 256, 0, st>>>(rho, cnt, nullptr, (int)G,
+                                                                                  charge_density, 1);
   CK(cudaGetLastError());
   return PB_OK;
 }
