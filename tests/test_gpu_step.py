@@ -92,7 +92,7 @@ def test_picard_potential_matches_superlu(gpu_mod, name):
         E, Eref = getattr(g, k).astype(np.float64), f[k].astype(np.float64)
         err = np.abs(E - Eref).max() / np.abs(Eref).max()
         assert err <= 1e-5, (k, err)
-    assert g.poisson_stats[2] <= 1e-10  # final relative FP64 residual of the last solve
+    assert g.poisson_stats[2] <= 1e-8  # final relative FP64 residual of the last solve (solver tol)
     # thermal-bow rebuild keeps state and re-solves
     g.grid_deflections = [0.012 * (i + 1) for i in range(len(params["grids"]))]
     g.build_domain(params, preserve_state=True)

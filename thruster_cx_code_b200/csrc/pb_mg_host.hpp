@@ -15,6 +15,8 @@
 #include <stdexcept>
 #include <vector>
 
+#include "pb_poisson.cuh"
+
 namespace pb {
 namespace mghost {
 
@@ -25,7 +27,7 @@ struct Level {
   std::vector<float> dinv;    // omega / diagonal on active nodes (damped Jacobi smoother)
 };
 
-constexpr double JACOBI_OMEGA = 0.8;
+constexpr double JACOBI_OMEGA = MG_JACOBI_OMEGA;
 
 struct Hierarchy {
   std::vector<Level> lev;
@@ -171,6 +173,14 @@ inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>&
     for (size_t k = 0; k < 9 * Nc; ++k) C.st[k] = (float)st[k];
     for (size_t c = 0; c < Nc; ++c)
       if (C.act[c] && !(C.st[4 * Nc + c] > 0.0f)) C.act[c] = 0;
+    // no coupling to or from inactive nodes (the device cycle reads every stencil entry)
+    for (size_t c = 0; c < Nc; ++c) {
+      int I = (int)(c / nxc), J = (int)(c % nxc);
+      for (int k = 0; k < 9; ++k) {
+        long j = nb(nyc, nxc, C.per, I, J, k / 3 - 1, k % 3 - 1);
+        if (!C.act[c] || j < 0 || !C.act[j]) C.st[k * Nc + c] = 0.0f;
+      }
+    }
     C.ncolors = colors_for(C, (int)H.lev.size());
     H.lev.push_back(std::move(C));
   }

@@ -11,50 +11,53 @@
 // Here the Dirichlet and Neumann rows are eliminated, which leaves the SPD operator
 //     (4 - n_neumann_nbrs) V_i - sum_{free nbrs} V_j = coeff*rho_total_i + sum_{Dirichlet nbrs} V_fixed_j
 // on the free nodes.  It is solved by FP32 MG-PCG inside an FP64 iterative-refinement
-// loop (FP64 residual f - A x, FP64 dot products).  The multigrid hierarchy is
-// Galerkin (coarse = P^T A P, 9-point stencils) with bilinear P, red-black Gauss-Seidel
-// on the 5-point fine level, 4- or 6-colour Gauss-Seidel on coarse levels (symmetric
-// ordering, so the V-cycle is an SPD preconditioner) and a dense inverse on the coarsest.
+// loop (FP64 residual f - A x, FP64 dot products).  The preconditioner is one V(1,1)
+// cycle: Galerkin coarse operators (9-point stencils, P bilinear), one damped-Jacobi
+// sweep from zero before restriction and one after prolongation, a dense inverse on
+// the coarsest level.  Both smoothing sweeps are fused into the transfers, so every
+// level costs one grid-wide phase going down and one going up:
+//     down:  r_{l+1} = P^T (r - A w D^-1 r)
+//     up:    z = m + w D^-1 (r - A m),   m = w D^-1 r + P z_{l+1}
+// With d_i = w / A_ii the diagonal terms reduce to (1 - w) r_i and (1 - w) m_i, so a
+// phase reads only the off-diagonal stencil, d and r.  Every load in these phases is
+// issued unconditionally (masked by d > 0, the active-node test) so that a thread's
+// loads overlap instead of waiting on one another.
 //
 // Grid-wide phases are separated by a software grid barrier (cooperative launch
-// guarantees co-residency).  Every wait is bounded: on time-out the kernel sets
+// guarantees co-residency).  The levels below a size threshold run on block 0 out of
+// shared memory.  Every wait is bounded: on time-out the kernel sets
 // PB_EF_SPIN_TIMEOUT, stops waiting at later barriers and runs to completion.
-// Reductions are deterministic: one partial per block, summed in block order.
-// Data written by other blocks within the launch is read only after a grid barrier,
-// which ends with an acquire fence in every thread.
+// Reductions are deterministic: one partial per block, summed in block order; the
+// partials ride on the barrier that the next phase needs anyway.
 #include "pb_common.cuh"
 #include "pb_poisson.cuh"
 
 namespace pb {
 
-constexpr int PT = 512;  // threads per block
+constexpr int PT = 1024;  // threads per block (one block per SM)
 constexpr long long BAR_SPIN_LIMIT = 1ll << 22;
+constexpr float W_KEEP = (float)(1.0 - MG_JACOBI_OMEGA);
 
+// Grid barrier on one 32-bit word: block 0 adds 2^31 - (nblocks - 1), the others add 1,
+// so the top bit flips once every block has arrived and the low bits return to their
+// start.  Arrival is a release, the poll an acquire: stores made by any thread of an
+// arriving block before the barrier are visible to every thread after it.
 __device__ __forceinline__ void grid_barrier(unsigned int* bar, uint32_t* err) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* vgen = bar + 1;
-    volatile uint32_t* verr = err;
-    unsigned int gen = *vgen;
-    __threadfence();
-    unsigned int arrived = atomicAdd(bar, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      long long spin = 0;
-      while (*vgen == gen) {
-        if ((*verr & PB_EF_SPIN_TIMEOUT) != 0u) break;
-        if (++spin > BAR_SPIN_LIMIT) { atomicOr(err, PB_EF_SPIN_TIMEOUT); break; }
+    const unsigned int inc = blockIdx.x == 0 ? (0x80000000u - (gridDim.x - 1)) : 1u;
+    unsigned int old, cur;
+    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(inc) : "memory");
+    for (long long spin = 0;; ++spin) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
+      if ((old ^ cur) & 0x80000000u) break;
+      if ((spin & 255) == 255) {
+        if ((*(volatile uint32_t*)err & PB_EF_SPIN_TIMEOUT) != 0u) break;
+        if (spin > BAR_SPIN_LIMIT) { atomicOr(err, PB_EF_SPIN_TIMEOUT); break; }
       }
     }
-    __threadfence();
   }
   __syncthreads();
-  // every thread acquires at gpu scope, so its later (L1-cached) loads observe the
-  // stores other blocks made before arriving
-  asm volatile("fence.acq_rel.gpu;" ::: "memory");
 }
 
 // phase tracing (block 0, thread 0): time since the previous mark is added to trace[k]
@@ -68,283 +71,464 @@ __device__ __forceinline__ void tmark(const PoissonArgs& a, int k) {
   }
 }
 
-// deterministic grid-wide sum; contains one barrier
-__device__ double grid_sum(double v, const PoissonArgs& a, int& slot) {
-  __shared__ double sm[PT / 32];
-  __shared__ double bc;
+// ----------------------------------------------------------------- deterministic sums
+__device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double* part = a.partials + (size_t)(slot & 3) * gridDim.x;
-  if (threadIdx.x < 32) {
-    double s = threadIdx.x < PT / 32 ? sm[threadIdx.x] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
-    if (threadIdx.x == 0) __stcg(part + blockIdx.x, s);
-  }
-  grid_barrier(a.bar, a.errflags);
-  if (threadIdx.x < 32) {
-    // lanes take fixed strided subsets, then a fixed shuffle tree: same order in every block
-    double s = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) s += (*(part + b));
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xFFFFFFFFu, s, o);
-    if (threadIdx.x == 0) bc = s;
-  }
-  __syncthreads();
-  double r = bc;
-  __syncthreads();
-  ++slot;
-  return r;
+  return v;
 }
 
-// ----------------------------------------------------------------- level-0 (5-point) helpers
-struct Nb { int j; uint8_t c; };  // neighbour index and class (NC_NEU when outside)
-
-__device__ __forceinline__ Nb nb0(const PoissonArgs& a, int y, int x, int dy, int dx) {
-  Nb r;
-  int yy = y + dy, xx = x + dx;
-  if (a.periodic) { if (yy < 0) yy += a.ny; else if (yy >= a.ny) yy -= a.ny; }
-  if (yy < 0 || yy >= a.ny || xx < 0 || xx >= a.nx) { r.j = -1; r.c = NC_NEU; return r; }
-  r.j = yy * a.nx + xx;
-  r.c = __ldg(a.cls + r.j);
-  return r;
+// Block partials of up to two values into ring slot `slot` (read after the next barrier).
+__device__ __forceinline__ void put_partials(const PoissonArgs& a, int slot, double v0, double v1) {
+  __shared__ double sm[2][PT / 32];
+  v0 = warp_sum(v0);
+  v1 = warp_sum(v1);
+  if ((threadIdx.x & 31) == 0) { sm[0][threadIdx.x >> 5] = v0; sm[1][threadIdx.x >> 5] = v1; }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double s0 = threadIdx.x < PT / 32 ? sm[0][threadIdx.x] : 0.0;
+    double s1 = threadIdx.x < PT / 32 ? sm[1][threadIdx.x] : 0.0;
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    if (threadIdx.x == 0) {
+      double* part = a.partials + (size_t)(slot & 3) * 2 * gridDim.x;
+      part[blockIdx.x] = s0;
+      part[gridDim.x + blockIdx.x] = s1;
+    }
+  }
 }
 
-// (A v)_i and diag_i on the fine level for a free node i (float vector, read via L2)
-__device__ __forceinline__ float apply0f(const PoissonArgs& a, const float* v, int i, int y, int x, float& diag) {
-  const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
+// Grid totals of a slot, after a barrier; the same order in every block.
+__device__ __forceinline__ void get_sums(const PoissonArgs& a, int slot, double& t0, double& t1) {
+  __shared__ double bc[2];
+  if (threadIdx.x < 32) {
+    const double* part = a.partials + (size_t)(slot & 3) * 2 * gridDim.x;
+    double s0 = 0.0, s1 = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
+      s0 += __ldcg(part + b);
+      s1 += __ldcg(part + gridDim.x + b);
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    if (threadIdx.x == 0) { bc[0] = s0; bc[1] = s1; }
+  }
+  __syncthreads();
+  t0 = bc[0];
+  t1 = bc[1];
+  __syncthreads();
+}
+
+// ----------------------------------------------------------------- level-0 (5-point) operator
+// neighbours W, E, S, N of node i = (y, x); -1 outside the grid
+__device__ __forceinline__ void nbrs0(const PoissonArgs& a, int i, int y, int x, int j[4]) {
+  j[0] = x > 0 ? i - 1 : -1;
+  j[1] = x < a.nx - 1 ? i + 1 : -1;
+  int ys = y - 1, yn = y + 1;
+  if (a.periodic) { if (ys < 0) ys += a.ny; if (yn >= a.ny) yn -= a.ny; }
+  j[2] = ys >= 0 ? ys * a.nx + x : -1;
+  j[3] = yn < a.ny ? yn * a.nx + x : -1;
+}
+
+// (A v)_i at a free node, v arbitrary on non-free nodes (masked); all loads issued up front
+template <class T>
+__device__ __forceinline__ T apply0(const PoissonArgs& a, const T* v, int i, int y, int x) {
+  int j[4];
+  nbrs0(a, i, y, x, j);
+  uint8_t c[4];
+  T vj[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int jj = j[k] >= 0 ? j[k] : i;
+    c[k] = j[k] >= 0 ? __ldg(a.cls + jj) : (uint8_t)NC_NEU;
+    vj[k] = *(v + jj);
+  }
+  const T vi = *(v + i);
+  T s = (T)0;
+  int nneu = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    s += c[k] == NC_FREE ? vj[k] : (T)0;
+    nneu += c[k] == NC_NEU;
+  }
+  return (T)(4 - nneu) * vi - s;
+}
+
+// ----------------------------------------------------------------- transfer phases
+// Restricted residual at coarse node (I, J) of the level below F:
+//   sum_children w_f * [f active] * ((1 - w) r_f - sum_{k != centre} A_fk d_k r_k).
+// LV0: F is the fine level (5-point operator, off-diagonals -1 to every neighbour;
+// d r is zero on non-free nodes).  wrapC: the coarse level's prolongation wraps in y.
+template <bool LV0>
+__device__ __forceinline__ float restrict_res(const MgLevel& F, const float* r, int I, int J, bool wrapC) {
+  const int ny = F.ny, nx = F.nx, Nf = ny * nx;
+  int ro[5];
+  bool rv[5];
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    int y = 2 * I + t - 2;
+    if (F.per) { if (y < 0) y += ny; else if (y >= ny) y -= ny; }
+    rv[t] = y >= 0 && y < ny;
+    ro[t] = y * nx;
+  }
+  int xo[5];
+  bool cv[5];
+#pragma unroll
+  for (int u = 0; u < 5; ++u) {
+    xo[u] = 2 * J + u - 2;
+    cv[u] = xo[u] >= 0 && xo[u] < nx;
+  }
+  float zp[5][5];
+#pragma unroll
+  for (int t = 0; t < 5; ++t)
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+      if (LV0 && (t == 0 || t == 4) && (u == 0 || u == 4)) { zp[t][u] = 0.0f; continue; }
+      const bool ok = rv[t] && cv[u];
+      const int j = ok ? ro[t] + xo[u] : 0;
+      const float d = __ldg(F.dinv + j), rj = *(r + j);
+      zp[t][u] = ok ? d * rj : 0.0f;
+    }
   float s = 0.0f;
-  int nneu = 0;
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    Nb n = nb0(a, y, x, DY[k], DX[k]);
-    if (n.c == NC_FREE) s += (*(v + n.j));
-    else if (n.c == NC_NEU) ++nneu;
+  for (int da = -1; da <= 1; ++da) {
+    const int t = da + 2;
+    const int yf = 2 * I + da;
+    const bool rowok = rv[t] && (da < 0 ? (yf >= 0 || wrapC) : (yf < ny));
+#pragma unroll
+    for (int db = -1; db <= 1; ++db) {
+      const int u = db + 2;
+      const bool ok = rowok && cv[u];
+      const int f = ok ? ro[t] + xo[u] : 0;
+      const float df = __ldg(F.dinv + f), rf = *(r + f);
+      float res;
+      if (LV0) {
+        res = W_KEEP * rf + ((zp[t][u - 1] + zp[t][u + 1]) + (zp[t - 1][u] + zp[t + 1][u]));
+      } else {
+        res = W_KEEP * rf;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+          if (k == 4) continue;
+          res -= __ldg(F.st + (size_t)k * Nf + f) * zp[t + k / 3 - 1][u + k % 3 - 1];
+        }
+      }
+      const float w = (da ? 0.5f : 1.0f) * (db ? 0.5f : 1.0f);
+      s += (ok && df > 0.0f) ? w * res : 0.0f;
+    }
   }
-  diag = (float)(4 - nneu);
-  return diag * (*(v + i)) - s;
+  return s;
 }
 
-__device__ __forceinline__ double apply0d(const PoissonArgs& a, const double* v, int i, int y, int x) {
-  const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
-  double s = 0.0;
-  int nneu = 0;
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    Nb n = nb0(a, y, x, DY[k], DX[k]);
-    if (n.c == NC_FREE) s += (*(v + n.j));
-    else if (n.c == NC_NEU) ++nneu;
-  }
-  return (double)(4 - nneu) * (*(v + i)) - s;
+// (P z_c) at fine node (y, x) of the level above C
+__device__ __forceinline__ float prolong(const MgLevel& C, const float* zc, int y, int x) {
+  const int I0 = y >> 1, J0 = x >> 1, ay = y & 1, bx = x & 1;
+  int I1 = I0 + 1;
+  bool m10 = ay != 0;
+  if (I1 >= C.ny) { if (C.wrapP) I1 -= C.ny; else m10 = false; }
+  const int J1 = J0 + 1;
+  const bool m01 = bx != 0 && J1 < C.nx;
+  const int i00 = I0 * C.nx + J0;
+  const int i01 = m01 ? I0 * C.nx + J1 : i00;
+  const int i10 = m10 ? I1 * C.nx + J0 : i00;
+  const int i11 = (m10 && m01) ? I1 * C.nx + J1 : i00;
+  const float z00 = *(zc + i00), z01 = *(zc + i01), z10 = *(zc + i10), z11 = *(zc + i11);
+  const float w = (ay ? 0.5f : 1.0f) * (bx ? 0.5f : 1.0f);
+  return w * (z00 + (m01 ? z01 : 0.0f) + (m10 ? z10 : 0.0f) + ((m10 && m01) ? z11 : 0.0f));
 }
 
-// ----------------------------------------------------------------- coarse (9-point) helpers
-__device__ __forceinline__ int nbc(const MgLevel& L, int y, int x, int dI, int dJ) {
+// Post-smoothed correction at fine node i = (y, x) of level F from z_c of the level below:
+//   z = (1 - w) m_i + d_i (r_i - sum_{k != centre} A_ik m_k),  m = [active] (d r + P z_c)
+template <bool LV0>
+__device__ __forceinline__ float smooth_up(const MgLevel& F, const MgLevel& C, const float* r, const float* zc, int y,
+                                           int x, int i, float& ri) {
+  const int ny = F.ny, nx = F.nx, Nf = ny * nx;
+  int yr[3], ro[3];
+  bool rv[3];
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    int yy = y + t - 1;
+    if (F.per) { if (yy < 0) yy += ny; else if (yy >= ny) yy -= ny; }
+    rv[t] = yy >= 0 && yy < ny;
+    yr[t] = rv[t] ? yy : y;
+    ro[t] = yr[t] * nx;
+  }
+  float m[3][3];
+  float di = 0.0f;
+  ri = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 3; ++t)
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      if (LV0 && t != 1 && u != 1) { m[t][u] = 0.0f; continue; }
+      const int xx = x + u - 1;
+      const bool ok = rv[t] && xx >= 0 && xx < nx;
+      const int j = ok ? ro[t] + xx : i;
+      const float d = __ldg(F.dinv + j), rj = *(r + j);
+      const float pz = prolong(C, zc, ok ? yr[t] : y, ok ? xx : x);
+      m[t][u] = (ok && d > 0.0f) ? d * rj + pz : 0.0f;
+      if (t == 1 && u == 1) { di = d; ri = rj; }
+    }
+  float acc = ri;
+  if (LV0) {
+    acc += (m[1][0] + m[1][2]) + (m[0][1] + m[2][1]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      if (k == 4) continue;
+      acc -= __ldg(F.st + (size_t)k * Nf + i) * m[k / 3][k % 3];
+    }
+  }
+  return di > 0.0f ? W_KEEP * m[1][1] + di * acc : 0.0f;
+}
+
+// grid-wide down leg: r_{l+1} from level l (all from global memory)
+template <bool LV0>
+__device__ void down_leg(const PoissonArgs& a, int level, int tid, int nth) {
+  const MgLevel& F = a.lev[level];
+  const MgLevel& C = a.lev[level + 1];
+  const int Nc = C.ny * C.nx;
+  for (int ic = tid; ic < Nc; ic += nth) {
+    const int I = ic / C.nx, J = ic - I * C.nx;
+    const float s = restrict_res<LV0>(F, F.r, I, J, C.wrapP != 0);
+    __stcg(C.r + ic, __ldg(C.dinv + ic) > 0.0f ? s : 0.0f);
+  }
+}
+
+// grid-wide up leg: z_l from r_l and z_{l+1}; on level 0 also the partial of (r, z)
+template <bool LV0>
+__device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth) {
+  const MgLevel& F = a.lev[level];
+  const MgLevel& C = a.lev[level + 1];
+  const int N = F.ny * F.nx;
+  double rz = 0.0;
+  for (int i = tid; i < N; i += nth) {
+    const int y = i / F.nx, x = i - y * F.nx;
+    float ri;
+    const float z = smooth_up<LV0>(F, C, F.r, C.z, y, x, i, ri);
+    __stcg(F.z + i, z);
+    if (LV0) rz += (double)ri * (double)z;
+  }
+  return rz;
+}
+
+// ----------------------------------------------------------------- block-0 levels in shared memory
+struct SLev {
+  int ny, nx, per, wrapP, N;
+  float *st, *dinv, *r, *z;
+};
+
+// offsets of the small levels in dynamic shared memory (must match small_smem_bytes on the host)
+__device__ void small_layout(const PoissonArgs& a, float* base, SLev* sl, float** tmp, float** rc) {
+  size_t off = 0;
+  int maxN = 0;
+  for (int l = a.first_small; l < a.nlevels; ++l) {
+    const MgLevel& L = a.lev[l];
+    SLev& S = sl[l];
+    S.ny = L.ny; S.nx = L.nx; S.per = L.per; S.wrapP = L.wrapP; S.N = L.ny * L.nx;
+    S.st = base + off; off += 9 * (size_t)S.N;
+    S.dinv = base + off; off += S.N;
+    S.r = base + off; off += S.N;
+    S.z = base + off; off += S.N;
+    maxN = S.N > maxN ? S.N : maxN;
+  }
+  *tmp = base + off; off += maxN;
+  *rc = base + off;
+}
+
+__device__ __forceinline__ int snb(const SLev& L, int y, int x, int dI, int dJ) {
   int yy = y + dI, xx = x + dJ;
   if (L.per) { if (yy < 0) yy += L.ny; else if (yy >= L.ny) yy -= L.ny; }
   if (yy < 0 || yy >= L.ny || xx < 0 || xx >= L.nx) return -1;
   return yy * L.nx + xx;
 }
 
-// Loads and stores of level vectors.  PRIV: data only block 0 touches (the small
-// levels).  Loads go through L1 in both cases: data written by other blocks is read only
-// after a grid barrier, whose acquire fence orders the load after those stores.
-template <bool PRIV> __device__ __forceinline__ float ldv(const float* p) { return *p; }
-template <bool PRIV> __device__ __forceinline__ void stv(float* p, float v) { if (PRIV) *p = v; else __stcg(p, v); }
-
-__device__ __forceinline__ bool active(const PoissonArgs& a, int level, int i) {
-  return level == 0 ? (__ldg(a.cls + i) == NC_FREE) : (__ldg(a.lev[level].act + i) != 0);
-}
-
-// (A_l v)_i for an active node i, with v_j supplied by the callable vj(j) (inactive
-// neighbours contribute nothing: their value is zero in every vector of the cycle)
-template <class V>
-__device__ __forceinline__ float apply_A(const PoissonArgs& a, int level, int i, int y, int x, V vj) {
-  if (level == 0) {
-    const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
-    float s = 0.0f;
-    int nneu = 0;
+// tmp_f = [f active] ((1 - w) r_f - sum_{k != c} A_fk d_k r_k); then r_c = P^T tmp
+__device__ void sdown(const SLev& F, const SLev& C, float* tmp) {
+  for (int f = threadIdx.x; f < F.N; f += blockDim.x) {
+    const int y = f / F.nx, x = f - y * F.nx;
+    float res = W_KEEP * F.r[f];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      Nb n = nb0(a, y, x, DY[k], DX[k]);
-      if (n.c == NC_FREE) s += vj(n.j);
-      else if (n.c == NC_NEU) ++nneu;
+    for (int k = 0; k < 9; ++k) {
+      if (k == 4) continue;
+      const int j = snb(F, y, x, k / 3 - 1, k % 3 - 1);
+      if (j >= 0) res -= F.st[k * F.N + f] * (F.dinv[j] * F.r[j]);
     }
-    return (float)(4 - nneu) * vj(i) - s;
+    tmp[f] = F.dinv[f] > 0.0f ? res : 0.0f;
   }
-  const MgLevel& L = a.lev[level];
-  const int N = L.ny * L.nx;
-  float s = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    int j = (k == 4) ? i : nbc(L, y, x, k / 3 - 1, k % 3 - 1);
-    if (j >= 0) s += __ldg(L.st + (size_t)k * N + i) * vj(j);
-  }
-  return s;
-}
-
-// (P z_{l+1}) at fine node (y, x) of level l
-template <bool PRIV>
-__device__ __forceinline__ float prolong_at(const MgLevel& C, int y, int x) {
-  int I0 = y >> 1, J0 = x >> 1, ai = y & 1, bj = x & 1;
-  float s = 0.0f;
-  for (int da = 0; da <= ai; ++da) {
-    int I = I0 + da;
-    if (I >= C.ny) { if (C.wrapP) I -= C.ny; else continue; }
-    float wy = ai ? 0.5f : 1.0f;
-    for (int db = 0; db <= bj; ++db) {
-      int J = J0 + db;
-      if (J >= C.nx) continue;
-      float wx = bj ? 0.5f : 1.0f;
-      s += wy * wx * ldv<PRIV>(C.z + I * C.nx + J);
-    }
-  }
-  return s;
-}
-
-// Down leg of the V-cycle on level l: with the pre-smoothed z = omega D^-1 r (one damped
-// Jacobi sweep from zero), r_{l+1} = P^T (r_l - A_l z), all evaluated from r_l.
-template <bool PRIV>
-__device__ __forceinline__ void down_leg(const PoissonArgs& a, int level, int tid, int nth) {
-  const MgLevel& F = a.lev[level];
-  const MgLevel& C = a.lev[level + 1];
-  const int Nc = C.ny * C.nx;
-  const bool wrap = C.wrapP;
-  const float* r = F.r;
-  const float* dinv = F.dinv;
-  auto zpre = [&](int j) { return __ldg(dinv + j) * ldv<PRIV>(r + j); };
-  for (int ic = tid; ic < Nc; ic += nth) {
-    if (!__ldg(C.act + ic)) { stv<PRIV>(C.r + ic, 0.0f); continue; }
-    int I = ic / C.nx, J = ic - I * C.nx;
+  __syncthreads();
+  for (int c = threadIdx.x; c < C.N; c += blockDim.x) {
+    const int I = c / C.nx, J = c - I * C.nx;
     float s = 0.0f;
 #pragma unroll
     for (int da = -1; da <= 1; ++da) {
       int yf = 2 * I + da;
-      if (yf < 0) { if (wrap) yf += F.ny; else continue; }
+      if (yf < 0) { if (C.wrapP) yf += F.ny; else continue; }
       if (yf >= F.ny) continue;
-      float wy = da == 0 ? 1.0f : 0.5f;
 #pragma unroll
       for (int db = -1; db <= 1; ++db) {
-        int xf = 2 * J + db;
+        const int xf = 2 * J + db;
         if (xf < 0 || xf >= F.nx) continue;
-        int f = yf * F.nx + xf;
-        if (!active(a, level, f)) continue;
-        float wx = db == 0 ? 1.0f : 0.5f;
-        float res = ldv<PRIV>(r + f) - apply_A(a, level, f, yf, xf, zpre);
-        s += wy * wx * res;
+        s += (da ? 0.5f : 1.0f) * (db ? 0.5f : 1.0f) * tmp[yf * F.nx + xf];
       }
     }
-    stv<PRIV>(C.r + ic, s);
+    C.r[c] = C.dinv[c] > 0.0f ? s : 0.0f;
   }
+  __syncthreads();
 }
 
-// Up leg on level l: z_mid = omega D^-1 r + P z_{l+1}; one damped Jacobi sweep,
-// z = z_mid + omega D^-1 (r - A z_mid), all evaluated from r_l and z_{l+1}.
-// PRIV_C: the coarse correction is private to block 0 as well.
-template <bool PRIV, bool PRIV_C>
-__device__ __forceinline__ void up_leg(const PoissonArgs& a, int level, int tid, int nth) {
-  const MgLevel& F = a.lev[level];
-  const MgLevel& C = a.lev[level + 1];
-  const int N = F.ny * F.nx;
-  const float* r = F.r;
-  const float* dinv = F.dinv;
-  auto zmid = [&](int j) {
-    int yj = j / F.nx, xj = j - yj * F.nx;
-    return __ldg(dinv + j) * ldv<PRIV>(r + j) + prolong_at<PRIV_C>(C, yj, xj);
-  };
-  for (int i = tid; i < N; i += nth) {
-    if (!active(a, level, i)) { stv<PRIV>(F.z + i, 0.0f); continue; }
-    int y = i / F.nx, x = i - y * F.nx;
-    float zm = zmid(i);
-    float az = apply_A(a, level, i, y, x, zmid);
-    stv<PRIV>(F.z + i, zm + __ldg(dinv + i) * (ldv<PRIV>(r + i) - az));
+// tmp = m = [active] (d r + P z_c); z = (1 - w) m + d (r - sum_{k != c} A m)
+__device__ void sup(const SLev& F, const SLev& C, float* tmp) {
+  for (int f = threadIdx.x; f < F.N; f += blockDim.x) {
+    const int y = f / F.nx, x = f - y * F.nx;
+    const int I0 = y >> 1, J0 = x >> 1, ay = y & 1, bx = x & 1;
+    float pz = 0.0f;
+    for (int da = 0; da <= ay; ++da) {
+      int I = I0 + da;
+      if (I >= C.ny) { if (C.wrapP) I -= C.ny; else continue; }
+      for (int db = 0; db <= bx; ++db) {
+        const int J = J0 + db;
+        if (J >= C.nx) continue;
+        pz += (ay ? 0.5f : 1.0f) * (bx ? 0.5f : 1.0f) * C.z[I * C.nx + J];
+      }
+    }
+    const float d = F.dinv[f];
+    tmp[f] = d > 0.0f ? d * F.r[f] + pz : 0.0f;
   }
+  __syncthreads();
+  for (int f = threadIdx.x; f < F.N; f += blockDim.x) {
+    const int y = f / F.nx, x = f - y * F.nx;
+    float acc = F.r[f];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      if (k == 4) continue;
+      const int j = snb(F, y, x, k / 3 - 1, k % 3 - 1);
+      if (j >= 0) acc -= F.st[k * F.N + f] * tmp[j];
+    }
+    const float d = F.dinv[f];
+    F.z[f] = d > 0.0f ? W_KEEP * tmp[f] + d * acc : 0.0f;
+  }
+  __syncthreads();
 }
 
-// coarsest level: z = A_c^{-1} r (dense, one block)
-template <bool PRIV>
-__device__ void coarse_solve(const PoissonArgs& a, int level) {
-  const MgLevel& L = a.lev[level];
-  const int N = L.ny * L.nx;
+// z = A_c^{-1} r on the coarsest level (dense inverse in global memory, 4 lanes per row)
+__device__ void scoarse(const PoissonArgs& a, const SLev& L, float* rc) {
+  const int nc = a.nc;
+  for (int i = threadIdx.x; i < L.N; i += blockDim.x) L.z[i] = 0.0f;
+  for (int k = threadIdx.x; k < nc; k += blockDim.x) rc[k] = L.r[__ldg(a.cidx + k)];
+  __syncthreads();
+  for (int base = 0; base < 4 * nc; base += blockDim.x) {
+    const int q = base + threadIdx.x, k = q >> 2, part = q & 3;
+    float s = 0.0f;
+    if (k < nc)
+      for (int j = part; j < nc; j += 4) s += __ldg(a.cinvT + (size_t)j * nc + k) * rc[j];
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
+    s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
+    if (k < nc && part == 0) L.z[__ldg(a.cidx + k)] = s;
+  }
+  __syncthreads();
+}
+
+// block 0: restrict from level first_small-1 (global), cycle through the small levels in
+// shared memory, publish z on level first_small for the grid-wide up leg
+__device__ void small_cycle(const PoissonArgs& a, const SLev* sl, float* tmp, float* rc) {
+  const int fs = a.first_small, last = a.nlevels - 1;
+  const MgLevel& F = a.lev[fs - 1];
+  const SLev& C0 = sl[fs];
+  for (int ic = threadIdx.x; ic < C0.N; ic += blockDim.x) {
+    const int I = ic / C0.nx, J = ic - I * C0.nx;
+    const float s = fs - 1 == 0 ? restrict_res<true>(F, F.r, I, J, C0.wrapP != 0)
+                                : restrict_res<false>(F, F.r, I, J, C0.wrapP != 0);
+    C0.r[ic] = C0.dinv[ic] > 0.0f ? s : 0.0f;
+  }
+  __syncthreads();
+  for (int l = fs; l < last; ++l) sdown(sl[l], sl[l + 1], tmp);
+  scoarse(a, sl[last], rc);
+  for (int l = last - 1; l >= fs; --l) sup(sl[l], sl[l + 1], tmp);
+  float* zg = a.lev[fs].z;
+  for (int i = threadIdx.x; i < C0.N; i += blockDim.x) __stcg(zg + i, C0.z[i]);
+}
+
+// coarsest = finest (no coarse levels): dense solve on block 0 from global memory
+__device__ void coarse_only(const PoissonArgs& a) {
   __shared__ float rc[1024];
-  for (int i = threadIdx.x; i < N; i += blockDim.x) stv<PRIV>(L.z + i, 0.0f);
-  for (int k = threadIdx.x; k < a.nc; k += blockDim.x) rc[k] = ldv<PRIV>(L.r + a.cidx[k]);
+  const int N = a.ny * a.nx;
+  for (int i = threadIdx.x; i < N; i += blockDim.x) __stcg(a.z32 + i, 0.0f);
+  for (int k = threadIdx.x; k < a.nc; k += blockDim.x) rc[k] = *(a.r32 + __ldg(a.cidx + k));
   __syncthreads();
   for (int k = threadIdx.x; k < a.nc; k += blockDim.x) {
     float s = 0.0f;
     for (int j = 0; j < a.nc; ++j) s += __ldg(a.cinvT + (size_t)j * a.nc + k) * rc[j];
-    stv<PRIV>(L.z + a.cidx[k], s);
+    __stcg(a.z32 + __ldg(a.cidx + k), s);
   }
-  __syncthreads();
 }
 
-// The levels from first_small down, run by block 0 with block-level syncs.
-__device__ void small_vcycle(const PoissonArgs& a) {
-  const int last = a.nlevels - 1;
-  for (int l = a.first_small; l < last; ++l) {
-    down_leg<true>(a, l, threadIdx.x, blockDim.x);
-    __syncthreads();
-  }
-  coarse_solve<true>(a, last);
-  for (int l = last - 1; l >= a.first_small; --l) {
-    up_leg<true, true>(a, l, threadIdx.x, blockDim.x);
-    __syncthreads();
-  }
-  // the first small level's correction is read by other blocks through L2
-  __threadfence();
-}
-
-// z0 = M^{-1} r0 (lev[0].r = r32, lev[0].z = z32): a V(1,1) cycle with damped Jacobi
-// smoothing, two grid barriers per grid-wide level
-__device__ void vcycle(const PoissonArgs& a) {
+// z32 = M^{-1} r32 by one V(1,1) cycle; leaves the partial of (r, z) in `slot` and ends
+// with a barrier
+__device__ void vcycle(const PoissonArgs& a, const SLev* sl, float* tmp, float* rc, int slot) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  double rz = 0.0;
   if (a.nlevels == 1) {
-    if (blockIdx.x == 0) coarse_solve<false>(a, 0);
+    if (blockIdx.x == 0) coarse_only(a);
+    grid_barrier(a.bar, a.errflags);
+    const int N = a.ny * a.nx;
+    for (int i = tid; i < N; i += nth) rz += (double)(*(a.r32 + i)) * (double)(*(a.z32 + i));
+    put_partials(a, slot, rz, 0.0);
     grid_barrier(a.bar, a.errflags);
     return;
   }
-  for (int l = 0; l < a.first_small; ++l) {
-    down_leg<false>(a, l, tid, nth);
+  for (int l = 0; l < a.first_small - 1; ++l) {
+    if (l == 0) down_leg<true>(a, 0, tid, nth);
+    else down_leg<false>(a, l, tid, nth);
     grid_barrier(a.bar, a.errflags);
     tmark(a, l < 7 ? l : 6);
   }
-  if (a.first_small < a.nlevels - 1 || a.first_small == a.nlevels - 1) {
-    if (blockIdx.x == 0) {
-      if (a.first_small == a.nlevels - 1) {
-        coarse_solve<true>(a, a.first_small);
-        __threadfence();
-      } else {
-        small_vcycle(a);
-      }
-    }
-    grid_barrier(a.bar, a.errflags);
-  }
+  if (blockIdx.x == 0) small_cycle(a, sl, tmp, rc);
+  grid_barrier(a.bar, a.errflags);
   tmark(a, 7);
-  for (int l = a.first_small - 1; l >= 0; --l) {
-    up_leg<false, false>(a, l, tid, nth);
+  for (int l = a.first_small - 1; l >= 1; --l) {
+    up_leg<false>(a, l, tid, nth);
     grid_barrier(a.bar, a.errflags);
     tmark(a, 8 + (l < 7 ? l : 6));
   }
+  rz = up_leg<true>(a, 0, tid, nth);
+  put_partials(a, slot, rz, 0.0);
+  grid_barrier(a.bar, a.errflags);
+  tmark(a, 8);
 }
 
 // ----------------------------------------------------------------- the persistent kernel
-__global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
+__global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
+  extern __shared__ float4 dyn_smem[];
+  __shared__ SLev sl[MG_MAX_LEVELS];
+  __shared__ float* s_tmp;
+  __shared__ float* s_rc;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const int N = a.ny * a.nx;
-  const int DY[4] = {0, 0, -1, 1}, DX[4] = {-1, 1, 0, 0};
   int slot = 0;
   double n_outer = 0, n_inner = 0, last_rel = 0;
   tmark(a, 20);
 
+  // block 0: stage the small levels' operators in shared memory
+  if (blockIdx.x == 0 && a.nlevels > 1) {
+    if (threadIdx.x == 0) small_layout(a, reinterpret_cast<float*>(dyn_smem), sl, &s_tmp, &s_rc);
+    __syncthreads();
+    for (int l = a.first_small; l < a.nlevels; ++l) {
+      const SLev& S = sl[l];
+      const MgLevel& L = a.lev[l];
+      for (int k = threadIdx.x; k < 9 * S.N; k += blockDim.x) S.st[k] = __ldg(L.st + k);
+      for (int k = threadIdx.x; k < S.N; k += blockDim.x) S.dinv[k] = __ldg(L.dinv + k);
+    }
+    __syncthreads();
+  }
+
   // Dirichlet-neighbour sums (V_fixed is constant during the launch)
   for (int i = tid; i < N; i += nth) {
     if (__ldg(a.cls + i) != NC_FREE) continue;
-    int y = i / a.nx, x = i - y * a.nx;
+    const int y = i / a.nx, x = i - y * a.nx;
+    int j[4];
+    nbrs0(a, i, y, x, j);
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      Nb n = nb0(a, y, x, DY[k], DX[k]);
-      if (n.c == NC_DIR) s += __ldg(a.Vfixed + n.j);
-    }
+    for (int k = 0; k < 4; ++k)
+      if (j[k] >= 0 && __ldg(a.cls + j[k]) == NC_DIR) s += __ldg(a.Vfixed + j[k]);
     a.dirsum[i] = s;
   }
 
@@ -363,53 +547,60 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
     }
     for (int i = tid; i < N; i += nth) {
       if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
-      int y = i / a.nx, x = i - y * a.nx;
-      double res = (*(a.f + i)) - apply0d(a, a.x, i, y, x);
+      const int y = i / a.nx, x = i - y * a.nx;
+      double res = (*(a.f + i)) - apply0<double>(a, a.x, i, y, x);
       __stcg(a.r32 + i, (float)res);
       rr += res * res;
     }
-    double fnorm2 = grid_sum(ff, a, slot);
-    double rnorm2 = grid_sum(rr, a, slot);
+    put_partials(a, slot, ff, rr);
+    grid_barrier(a.bar, a.errflags);
+    double fnorm2, rnorm2;
+    get_sums(a, slot++, fnorm2, rnorm2);
     tmark(a, 17);
-    double target2 = a.tol * a.tol * fnorm2;
+    const double target2 = a.tol * a.tol * fnorm2;
 
     for (int outer = 0; outer < a.max_outer && rnorm2 > target2 && fnorm2 > 0.0; ++outer) {
       n_outer += 1;
-      // ---- FP32 MG-PCG on A e = r32
+      // ---- FP32 MG-PCG on A e = r32 (e32 starts at zero; r32 is the current residual)
       for (int i = tid; i < N; i += nth) __stcg(a.e32 + i, 0.0f);
-      double rz_old = 0.0, rr0 = rnorm2;
+      double rz_old = 0.0, rr0 = rnorm2, dummy;
       for (int k = 0; k < a.max_inner; ++k) {
         n_inner += 1;
         tmark(a, 15);
-        vcycle(a);  // z32 = M r32; ends with a barrier
-        double rz_p = 0.0;
-        for (int i = tid; i < N; i += nth) rz_p += (double)(*(a.r32 + i)) * (double)(*(a.z32 + i));
-        double rz = grid_sum(rz_p, a, slot);
-        double beta = k == 0 ? 0.0 : rz / rz_old;
+        vcycle(a, sl, s_tmp, s_rc, slot);  // z32 = M r32, (r, z) partial in slot, barrier
+        double rz;
+        get_sums(a, slot++, rz, dummy);
+        const double beta = k == 0 ? 0.0 : rz / rz_old;
         double pq_p = 0.0;
         for (int i = tid; i < N; i += nth) {
-          if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.p32 + i, 0.0f); __stcg(a.q32 + i, 0.0f); continue; }
-          int y = i / a.nx, x = i - y * a.nx;
-          float diag;
-          float az = apply0f(a, a.z32, i, y, x, diag);
-          float p = (*(a.z32 + i)) + (float)beta * (k == 0 ? 0.0f : (*(a.p32 + i)));
-          float q = az + (float)beta * (k == 0 ? 0.0f : (*(a.q32 + i)));
+          const int y = i / a.nx, x = i - y * a.nx;
+          const bool fr = __ldg(a.cls + i) == NC_FREE;
+          const float az = apply0<float>(a, a.z32, i, y, x);
+          const float zi = *(a.z32 + i);
+          const float p = fr ? zi + (float)beta * (k == 0 ? 0.0f : (*(a.p32 + i))) : 0.0f;
+          const float q = fr ? az + (float)beta * (k == 0 ? 0.0f : (*(a.q32 + i))) : 0.0f;
           __stcg(a.p32 + i, p);
           __stcg(a.q32 + i, q);
           pq_p += (double)p * (double)q;
         }
-        double pq = grid_sum(pq_p, a, slot);
-        double alpha = pq != 0.0 ? rz / pq : 0.0;
+        put_partials(a, slot, pq_p, 0.0);
+        grid_barrier(a.bar, a.errflags);
+        double pq;
+        get_sums(a, slot++, pq, dummy);
+        const double alpha = pq != 0.0 ? rz / pq : 0.0;
         double rr_p = 0.0;
         for (int i = tid; i < N; i += nth) {
           if (__ldg(a.cls + i) != NC_FREE) continue;
-          float e = (*(a.e32 + i)) + (float)alpha * (*(a.p32 + i));
-          float r = (*(a.r32 + i)) - (float)alpha * (*(a.q32 + i));
+          const float e = (*(a.e32 + i)) + (float)alpha * (*(a.p32 + i));
+          const float r = (*(a.r32 + i)) - (float)alpha * (*(a.q32 + i));
           __stcg(a.e32 + i, e);
           __stcg(a.r32 + i, r);
           rr_p += (double)r * (double)r;
         }
-        double rrk = grid_sum(rr_p, a, slot);
+        put_partials(a, slot, rr_p, 0.0);
+        grid_barrier(a.bar, a.errflags);
+        double rrk;
+        get_sums(a, slot++, rrk, dummy);
         tmark(a, 15);
         rz_old = rz;
         if (rrk <= a.tol_inner * a.tol_inner * rr0 || rrk <= target2 * 1e-4) break;
@@ -421,12 +612,14 @@ __global__ void __launch_bounds__(PT) k_poisson(PoissonArgs a) {
       rr = 0.0;
       for (int i = tid; i < N; i += nth) {
         if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
-        int y = i / a.nx, x = i - y * a.nx;
-        double res = (*(a.f + i)) - apply0d(a, a.x, i, y, x);
+        const int y = i / a.nx, x = i - y * a.nx;
+        double res = (*(a.f + i)) - apply0<double>(a, a.x, i, y, x);
         __stcg(a.r32 + i, (float)res);
         rr += res * res;
       }
-      rnorm2 = grid_sum(rr, a, slot);
+      put_partials(a, slot, rr, 0.0);
+      grid_barrier(a.bar, a.errflags);
+      get_sums(a, slot++, rnorm2, dummy);
       tmark(a, 16);
     }
     if (!(rnorm2 <= target2) && fnorm2 > 0.0 && tid == 0) atomicOr(a.errflags, PB_EF_POISSON_NOCONV);

@@ -5,14 +5,16 @@
 namespace pb {
 
 constexpr int MG_MAX_LEVELS = 16;
+constexpr double MG_JACOBI_OMEGA = 0.8;       // damped-Jacobi weight of the V-cycle smoother
+constexpr size_t MG_SMALL_SMEM_CAP = 200 * 1024;  // shared memory for the block-0 levels
 enum NodeClass : uint8_t { NC_FREE = 0, NC_DIR = 1, NC_NEU = 2 };
 
 struct MgLevel {
   int ny, nx;
   int per;        // y is periodic on this level's operator
   int wrapP;      // prolongation from the next coarser level wraps in y
-  int ncolors;    // smoother colours (2 on level 0, 4 or 6 on coarse levels)
-  const uint8_t* act;     // active (unknown) nodes; level 0: class array instead
+  int ncolors;    // unused by the damped-Jacobi cycle (kept for the layout)
+  const uint8_t* act;     // active (unknown) nodes; level 0: class array instead (the kernel uses dinv > 0)
   const float* st;        // 9-point stencil, st[k * N + i], k = (dI+1)*3 + (dJ+1); null on level 0
   const float* dinv;      // omega / diagonal on active nodes, 0 elsewhere (Jacobi smoother)
   float *r, *z;           // right-hand side and correction on this level
@@ -45,17 +47,26 @@ struct PoissonArgs {
   int max_outer, max_inner;
   // hierarchy
   int nlevels;            // including level 0 and the coarsest
-  int first_small;        // first level handled by a single block
+  int first_small;        // first level handled by block 0 in shared memory (>= 1)
   MgLevel lev[MG_MAX_LEVELS];
   int nc;                 // coarsest active count
   const int* cidx;        // coarsest active node indices
   const float* cinvT;     // coarsest inverse, transposed (nc x nc)
   // reductions and barrier
-  double* partials;       // 4 * gridDim doubles
-  unsigned int* bar;      // [count, generation]
+  double* partials;       // 4 slots x 2 values x gridDim doubles
+  unsigned int* bar;      // barrier word (any start value)
   uint32_t* errflags;
   double* stats;          // [outer its, inner its, final rel residual, solves] accumulated
   unsigned long long* trace;  // optional: ns per phase category (block 0), [31] = last stamp
 };
+
+// dynamic shared memory of k_poisson for levels first..nlevels-1 of sizes N[l]:
+// per level 9N stencil + N dinv + N r + N z floats, then max N scratch and nc floats
+inline size_t mg_small_smem_bytes(const int* N, int first, int nlevels, int nc) {
+  size_t f = 0;
+  int maxN = 0;
+  for (int l = first; l < nlevels; ++l) { f += 12 * (size_t)N[l]; maxN = N[l] > maxN ? N[l] : maxN; }
+  return 4 * (f + (size_t)maxN + (size_t)nc);
+}
 
 }  // namespace pb

@@ -83,6 +83,7 @@ struct Sim {
   unsigned long long* ptrace = nullptr;  // field-solve phase trace (32 slots)
   int trace_on = 0;
   int pgrid = 0;
+  size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
   // particles
   Species sp[2];
   int* counts = nullptr;         // [ion buf0, ion buf1, ele buf0, ele buf1]
@@ -110,7 +111,7 @@ struct Sim {
   pb_step_report* rep_dev = nullptr;
   pb_step_report* rep_host = nullptr;
   // settings
-  double tol = 1e-10, tol_inner = 1e-5;
+  double tol = 1e-8, tol_inner = 1e-5;
   int max_outer = 8, max_inner = 40, nu = 1, max_coarse = 256;
   uint64_t seed = 0;
   bool counts_valid = false;
@@ -252,6 +253,23 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   }
   if (s->first_small < 1) s->first_small = 1;
   s->nc = (int)H.cidx.size();
+  // the block-0 levels live in shared memory: move the first one down until they fit
+  std::vector<int> Ns(H.lev.size());
+  for (size_t l = 0; l < H.lev.size(); ++l) Ns[l] = H.lev[l].ny * H.lev[l].nx;
+  const int nl = (int)H.lev.size();
+  s->psmem = 0;
+  if (nl > 1) {
+    while (s->first_small < nl - 1 && mg_small_smem_bytes(Ns.data(), s->first_small, nl, s->nc) > MG_SMALL_SMEM_CAP)
+      ++s->first_small;
+    s->psmem = mg_small_smem_bytes(Ns.data(), s->first_small, nl, s->nc);
+    if (s->psmem > MG_SMALL_SMEM_CAP)
+      return fail(PB_ERR_ARG, "multigrid build: the coarsest level needs " + std::to_string(s->psmem) +
+                                  " bytes of shared memory");
+  }
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_poisson, PT, s->psmem));
+  if (occ < 1) return fail(PB_ERR_ARG, "field solver: no resident block with " + std::to_string(s->psmem) +
+                                           " bytes of shared memory");
   CK(dalloc(&s->cidx, s->nc));
   CK(dalloc(&s->cinvT, (size_t)s->nc * s->nc));
   CK(cudaMemcpy(s->cidx, H.cidx.data(), s->nc * sizeof(int), cudaMemcpyHostToDevice));
@@ -290,7 +308,7 @@ static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
   PoissonArgs a = poisson_args(s, iterations, p);
   CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), s->stream));
   void* args[] = {&a};
-  CK(cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, 0, s->stream));
+  CK(cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream));
   ++s->launches;
   return PB_OK;
 }
@@ -625,10 +643,11 @@ int32_t pb_sim_create(pb_sim** out, int32_t device) {
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device));
-  int occ = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_poisson, PT, 0));
-  s->pgrid = s->num_sms * std::max(1, std::min(occ, 2));
-  CK(dalloc(&s->partials, 4 * (size_t)s->pgrid));
+  // field solve: one block of PT threads per SM (cooperative launch)
+  CK(cudaFuncSetAttribute((const void*)k_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)MG_SMALL_SMEM_CAP));
+  s->pgrid = s->num_sms;
+  CK(dalloc(&s->partials, 4 * 2 * (size_t)s->pgrid));
   CK(dalloc(&s->bar, 2));
   CK(dalloc(&s->pstats, 4));
   CK(dalloc(&s->ptrace, 32));
