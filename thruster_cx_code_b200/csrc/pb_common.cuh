@@ -47,6 +47,29 @@ __device__ __forceinline__ int cell_round32(float s, float d, int lo, int hi) {
   return clampi(np_f2i32(rintf(q)), lo, hi);
 }
 
+// The same roundings from q = s * (1/d) instead of the division: |q - fl(s/d)| stays below
+// 1.8e-7 |q| (three float roundings), so when q is farther than 4.8e-7 |q| from every
+// rounding boundary (half-integers for rint, integers for trunc) fl(s/d) rounds the same
+// way; otherwise (and for NaN, inf or |q| >= 2^21) the exact quotient is used.
+__device__ __forceinline__ float rint_div(float s, float d, float inv_d) {
+  float q = __fmul_rn(s, inv_d);
+  float n = rintf(q);
+  if (!(fabsf(__fsub_rn(q, n)) < __fsub_rn(0.5f, __fmul_rn(4.8e-7f, fabsf(q))))) n = rintf(__fdiv_rn(s, d));
+  return n;
+}
+__device__ __forceinline__ float trunc_div(float s, float d, float inv_d) {
+  float q = __fmul_rn(s, inv_d);
+  float n = rintf(q);
+  if (!(fabsf(__fsub_rn(q, n)) > __fmul_rn(4.8e-7f, fabsf(q))) || !(fabsf(q) < 2097152.0f)) return truncf(__fdiv_rn(s, d));
+  return truncf(q);
+}
+__device__ __forceinline__ int cell_round_f(float s, float d, float inv_d, int lo, int hi) {
+  return (int)clampll(np_f2i64(rint_div(s, d, inv_d)), lo, hi);
+}
+__device__ __forceinline__ int cell_round32_f(float s, float d, float inv_d, int lo, int hi) {
+  return clampi(np_f2i32(rint_div(s, d, inv_d)), lo, hi);
+}
+
 // np.maximum / np.minimum propagate NaN (fmaxf does not)
 __device__ __forceinline__ float np_maxf(float a, float b) { return (a != a || b != b) ? __int_as_float(0x7fc00000) : (a >= b ? a : b); }
 __device__ __forceinline__ double np_maxd(double a, double b) { return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000ll) : (a >= b ? a : b); }

@@ -29,8 +29,10 @@ struct IonStepArgs {
   const float *Ex, *Ey, *Bx, *By, *Bz;
   int has_B;
   const uint8_t *isBound;
+  const uint8_t *bdist;   // Chebyshev distance (cells) to the nearest bound node, capped
   int nx, ny;
   float dxf, dyf;
+  float inv_dx, inv_dy;   // f32(1/dxf), f32(1/dyf)
   // push
   double dt, qm, ds_lim;
   const double *ds_max;   // device: max predicted displacement (n_sub)
@@ -67,6 +69,8 @@ struct IonStepArgs {
   double n0a;          // n0 * a_corr
   double neut_vth;
   Spline cx_spline;
+  double cex_bound;    // |n0a| * sigma_max * dt * (1 + 1e-5): P <= cex_bound * g
+  float cex_g_max;     // speeds above this bypass the bound
   uint64_t seed;
   uint32_t step;
   // counts for diagnostics / next deposit
@@ -87,6 +91,7 @@ struct EleStepArgs {
   const uint8_t *isBound;
   int nx, ny;
   float dxf, dyf;
+  float inv_dx, inv_dy;
   double dt, qm, ds_lim;
   const double *ds_max;
   int *n_sub_out;

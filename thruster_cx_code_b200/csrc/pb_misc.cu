@@ -531,4 +531,37 @@ __global__ void k_sort_gather(Soa src, Soa dst, const uint32_t* perm, const int*
 // copy the device count to another slot (num_dst of a sort = num_src)
 __global__ void k_copy_int(const int* a, int* b) { *b = *a; }
 
+// ------------------------------------------------------------------ distance to electrodes
+// Chebyshev distance (in cells, capped at BDIST_CAP) from every node to the nearest bound
+// node; the ion step uses it to skip path samples that cannot reach a bound cell.  Cells
+// only ever leave isBound during a run (erosion), so the map stays a lower bound.
+constexpr int BDIST_CAP = 15;
+
+__global__ void k_bdist_rows(const uint8_t* __restrict__ isBound, uint8_t* hrow, int ny, int nx) {
+  const int N = ny * nx;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const int y = i / nx, x = i - y * nx;
+    int best = BDIST_CAP;
+    for (int d = 0; d < BDIST_CAP; ++d)
+      if ((x - d >= 0 && isBound[i - d]) || (x + d < nx && isBound[i + d])) { best = d; break; }
+    hrow[i] = (uint8_t)best;
+  }
+}
+
+__global__ void k_bdist_cols(const uint8_t* __restrict__ hrow, uint8_t* dist, int ny, int nx) {
+  const int N = ny * nx;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const int y = i / nx, x = i - y * nx;
+    int best = BDIST_CAP;
+    for (int dy = -(BDIST_CAP - 1); dy <= BDIST_CAP - 1; ++dy) {
+      const int yy = y + dy;
+      if (yy < 0 || yy >= ny) continue;
+      const int ady = dy < 0 ? -dy : dy;
+      const int v = max(ady, (int)hrow[yy * nx + x]);
+      best = min(best, v);
+    }
+    dist[i] = (uint8_t)best;
+  }
+}
+
 }  // namespace pb

@@ -34,10 +34,14 @@ __device__ __forceinline__ double gather4(const float* __restrict__ F, size_t r0
   return DADD(DADD(DADD(a, b), c), d);
 }
 
+// HAS_B = false: the B arrays are all +0 (the simulator never writes them), so
+// t = h * (+0) is a signed zero, t2 = +0 and 1 + t2 = 1 exactly; s = 2 t / 1 = 2 t.  The
+// remaining operations are kept, so signed zeros come out as in the reference.
+template <bool HAS_B>
 __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, float& vy, float& vz,
                                                const float* __restrict__ Ex, const float* __restrict__ Ey,
                                                const float* __restrict__ Bx, const float* __restrict__ By,
-                                               const float* __restrict__ Bz, bool hasB, int nx, int ny,
+                                               const float* __restrict__ Bz, int nx, int ny,
                                                float dxf, float dyf, double h, float dtf) {
   float ixf = __fdiv_rn(x, dxf);
   float iyf = __fdiv_rn(y, dyf);
@@ -52,19 +56,22 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
   size_t r0 = (size_t)iy0 * nx, r1 = (size_t)iy1 * nx;
   double ex = gather4(Ex, r0, r1, ix0, ix1, w00, w10, w01, w11);
   double ey = gather4(Ey, r0, r1, ix0, ix1, w00, w10, w01, w11);
-  double bx = 0.0, by = 0.0, bz = 0.0;
-  if (hasB) {
-    bx = gather4(Bx, r0, r1, ix0, ix1, w00, w10, w01, w11);
-    by = gather4(By, r0, r1, ix0, ix1, w00, w10, w01, w11);
-    bz = gather4(Bz, r0, r1, ix0, ix1, w00, w10, w01, w11);
-  }
   double vmx = DADD((double)vx, DMUL(h, ex));
   double vmy = DADD((double)vy, DMUL(h, ey));
   double vmz = (double)vz;
-  double tx = DMUL(h, bx), ty = DMUL(h, by), tz = DMUL(h, bz);
-  double t2 = DADD(DADD(DMUL(tx, tx), DMUL(ty, ty)), DMUL(tz, tz));
-  double den = DADD(1.0, t2);
-  double sx = DDIV(DMUL(2.0, tx), den), sy = DDIV(DMUL(2.0, ty), den), sz = DDIV(DMUL(2.0, tz), den);
+  double tx, ty, tz, sx, sy, sz;
+  if (HAS_B) {
+    double bx = gather4(Bx, r0, r1, ix0, ix1, w00, w10, w01, w11);
+    double by = gather4(By, r0, r1, ix0, ix1, w00, w10, w01, w11);
+    double bz = gather4(Bz, r0, r1, ix0, ix1, w00, w10, w01, w11);
+    tx = DMUL(h, bx); ty = DMUL(h, by); tz = DMUL(h, bz);
+    double t2 = DADD(DADD(DMUL(tx, tx), DMUL(ty, ty)), DMUL(tz, tz));
+    double den = DADD(1.0, t2);
+    sx = DDIV(DMUL(2.0, tx), den); sy = DDIV(DMUL(2.0, ty), den); sz = DDIV(DMUL(2.0, tz), den);
+  } else {
+    tx = DMUL(h, 0.0); ty = tx; tz = tx;
+    sx = DMUL(2.0, tx); sy = sx; sz = sx;
+  }
   double vpx = DADD(vmx, DSUB(DMUL(vmy, tz), DMUL(vmz, ty)));
   double vpy = DADD(vmy, DSUB(DMUL(vmz, tx), DMUL(vmx, tz)));
   double vpz = DADD(vmz, DSUB(DMUL(vmx, ty), DMUL(vmy, tx)));
@@ -94,7 +101,7 @@ __global__ void k_push_boris(float* x, float* y, float* vx, float* vy, float* vz
                              int nx, int ny, float dxf, float dyf, double h, float dtf) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float a = x[i], b = y[i], c = vx[i], d = vy[i], e = vz[i];
-    boris_push_one(a, b, c, d, e, Ex, Ey, Bx, By, Bz, true, nx, ny, dxf, dyf, h, dtf);
+    boris_push_one<true>(a, b, c, d, e, Ex, Ey, Bx, By, Bz, nx, ny, dxf, dyf, h, dtf);
     x[i] = a; y[i] = b; vx[i] = c; vy[i] = d; vz[i] = e;
   }
 }
@@ -219,6 +226,27 @@ __device__ __forceinline__ SegHit segment_hit(const uint8_t* __restrict__ isBoun
     float yi = __fadd_rn(y0, __fmul_rn(ddy, f));
     int cx = cell_round(xi, dxf, 0, nx - 1);
     int cy = cell_round(yi, dyf, 0, ny - 1);
+    if (!r.hit && __ldg(isBound + (size_t)cy * nx + cx)) { r.hit = true; r.ix = cx; r.iy = cy; }
+  }
+  return r;
+}
+
+// segment_hit with the sample cells from rint_div (same cells, fewer divisions)
+__device__ __forceinline__ SegHit segment_hit_f(const uint8_t* __restrict__ isBound, int nx, int ny, float dxf,
+                                                float dyf, float inv_dx, float inv_dy, float x0, float y0, float x1,
+                                                float y1, int ix1, int iy1) {
+  SegHit r;
+  r.hit = false;
+  r.ix = ix1;
+  r.iy = iy1;
+  float ddx = __fsub_rn(x1, x0), ddy = __fsub_rn(y1, y0);
+#pragma unroll
+  for (int i = 1; i <= 8; ++i) {
+    float f = (float)i * 0.125f;
+    float xi = __fadd_rn(x0, __fmul_rn(ddx, f));
+    float yi = __fadd_rn(y0, __fmul_rn(ddy, f));
+    int cx = cell_round_f(xi, dxf, inv_dx, 0, nx - 1);
+    int cy = cell_round_f(yi, dyf, inv_dy, 0, ny - 1);
     if (!r.hit && __ldg(isBound + (size_t)cy * nx + cx)) { r.hit = true; r.ix = cx; r.iy = cy; }
   }
   return r;
@@ -362,7 +390,8 @@ struct IonStage {
   uint8_t cex[TILE], keep[TILE];
 };
 
-__global__ void __launch_bounds__(NT) k_ion_step(IonStepArgs a) {
+template <bool HAS_B>
+__global__ void __launch_bounds__(NT, 3) k_ion_step(IonStepArgs a) {
   __shared__ IonStage st;
   __shared__ int sm_tile;
   const int n = *a.num_src;
@@ -385,20 +414,30 @@ __global__ void __launch_bounds__(NT) k_ion_step(IonStepArgs a) {
     for (int k = threadIdx.x; k < TILE; k += NT) {
       const int i = t0 + k;
       uint8_t kp = 0;
+      int dep_cell = 0, ppc_cell = 0;
       if (i < n) {
         float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
         uint8_t cx = a.src.cex[i];
         const uint32_t pid = a.src.id[i];
         const float x0 = x, y0 = y;
         for (int s = 0; s < n_sub; ++s)
-          boris_push_one(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.has_B, a.nx, a.ny, a.dxf, a.dyf, h, dtf);
+          boris_push_one<HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h, dtf);
         if (a.periodic) y = np_modf_pos(y, a.Lyf);
         // entered the optics (:1316-1324)
         if (x0 < a.x_entry && x >= a.x_entry && vx > 0.0f) cnt[0]++;
-        // final-cell and path hits (:1326-1336)
-        int icx = cell_round(x, a.dxf, 0, a.nx - 1), icy = cell_round(y, a.dyf, 0, a.ny - 1);
-        bool hit_final = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
-        SegHit sh = segment_hit(a.isBound, a.nx, a.ny, a.dxf, a.dyf, x0, y0, x, y);
+        // final-cell and path hits (:1326-1336).  The 8 path samples lie in cells at most
+        // max(|di|, |dj|) + 1 (Chebyshev) from the start cell; they are examined only when
+        // that reaches the distance from the start cell to the nearest bound node.
+        const int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1);
+        const int icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
+        const bool hit_final = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
+        const int sx0 = cell_round_f(x0, a.dxf, a.inv_dx, 0, a.nx - 1);
+        const int sy0 = cell_round_f(y0, a.dyf, a.inv_dy, 0, a.ny - 1);
+        const int reach = max(abs(icx - sx0), abs(icy - sy0)) + 1;
+        SegHit sh;
+        sh.hit = false; sh.ix = icx; sh.iy = icy;
+        if (reach >= (int)__ldg(a.bdist + (size_t)sy0 * a.nx + sx0))
+          sh = segment_hit_f(a.isBound, a.nx, a.ny, a.dxf, a.dyf, a.inv_dx, a.inv_dy, x0, y0, x, y, icx, icy);
         bool hit = hit_final || sh.hit;
         int imx = sh.hit ? sh.ix : icx, imy = sh.hit ? sh.iy : icy;
         bool oob = (x < 0.0f) || (x > a.x_plume) || (x != x);
@@ -459,60 +498,67 @@ __global__ void __launch_bounds__(NT) k_ion_step(IonStepArgs a) {
         bool alive = !(hit || oob);
         kp = alive && ((x <= a.x_plume) || (vx < 0.0f));
         if (kp) {
-          // CEX null-collision MCC on primaries (:1682-1739)
+          // CEX null-collision MCC on primaries (:1682-1739).  P = 1 - exp(-n sigma g dt)
+          // <= |n0a| sigma_max g dt, so a draw u at or above that bound (plus the rounding
+          // of the exact expression) neither collides nor ties, and the exact
+          // probability is evaluated only below it.
           if (!cx && x >= 1.0f && x <= a.Lxf) {
-            float z_m = __fmul_rn(__fsub_rn(x, 1.0f), 1e-3f);
-            z_m = z_m >= 0.0f ? z_m : 0.0f;
-            float r_m = __fmul_rn(y, 1e-3f);
-            float zr = __fadd_rn(z_m, a.rT_f);
-            float R = sqrtf(__fadd_rn(__fmul_rn(r_m, r_m), __fmul_rn(zr, zr)));
-            float th = atan2f(r_m, zr);
-            float Rm = np_maxf(R, 1e-12f);
-            float q1 = __fdiv_rn(a.rT_f, Rm);
-            float geo = __fsub_rn(1.0f, __fdiv_rn(1.0f, sqrtf(__fadd_rn(1.0f, __fmul_rn(q1, q1)))));
-            double nl = DMUL(DMUL(a.n0a, (double)geo), (double)cosf(th));
-            nl = np_maxd(nl, 0.0);
             float vm = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
             float g = np_maxf(vm, 1.0f);
-            double sigma;
-            if (a.cx_spline.enabled) {
-              float Ec = __fdiv_rn(__fmul_rn(a.k_half_m, __fmul_rn(g, g)), a.q_f);
-              sigma = user_cs(a.cx_spline, Ec);
-            } else {
-              float t = __fadd_rn(__fmul_rn(-0.8821f, logf(g)), 15.1262f);
-              sigma = (double)__fmul_rn(__fmul_rn(t, t), 1e-20f);
-            }
-            double prob = DSUB(1.0, exp(DMUL(DMUL(DMUL(-nl, sigma), (double)g), a.dt)));
             double u = philox_uniform(a.seed, pid, SITE_CEX_U, a.step, 0);
-            if (fabs(u - prob) <= fabs(prob) * 8.9e-16 + 1e-300) cnt[6]++;
-            if (u < prob) {
-              cnt[5]++;
-              u32x4 r0 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 0);
-              u32x4 r1 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 1);
-              u32x4 r2 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 2);
-              u32x4 r3 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 3);
-              u32x4 r4 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 4);
-              double fmx = DMUL(2.0, DSUB(DADD(DADD(u53(r0.x, r0.y), u53(r0.z, r0.w)), u53(r1.x, r1.y)), 1.5));
-              double fmy = DMUL(2.0, DSUB(DADD(DADD(u53(r1.z, r1.w), u53(r2.x, r2.y)), u53(r2.z, r2.w)), 1.5));
-              double fmz = DMUL(2.0, DSUB(DADD(DADD(u53(r3.x, r3.y), u53(r3.z, r3.w)), u53(r4.x, r4.y)), 1.5));
-              vx = __double2float_rn(DMUL(a.neut_vth, fmx));
-              vy = __double2float_rn(DMUL(a.neut_vth, fmy));
-              vz = __double2float_rn(DMUL(a.neut_vth, fmz));
-              cx = 1;
+            if (!(g <= a.cex_g_max && u >= DADD(DMUL(a.cex_bound, (double)g), 1e-15))) {
+              float z_m = __fmul_rn(__fsub_rn(x, 1.0f), 1e-3f);
+              z_m = z_m >= 0.0f ? z_m : 0.0f;
+              float r_m = __fmul_rn(y, 1e-3f);
+              float zr = __fadd_rn(z_m, a.rT_f);
+              float R = sqrtf(__fadd_rn(__fmul_rn(r_m, r_m), __fmul_rn(zr, zr)));
+              float th = atan2f(r_m, zr);
+              float Rm = np_maxf(R, 1e-12f);
+              float q1 = __fdiv_rn(a.rT_f, Rm);
+              float geo = __fsub_rn(1.0f, __fdiv_rn(1.0f, sqrtf(__fadd_rn(1.0f, __fmul_rn(q1, q1)))));
+              double nl = DMUL(DMUL(a.n0a, (double)geo), (double)cosf(th));
+              nl = np_maxd(nl, 0.0);
+              double sigma;
+              if (a.cx_spline.enabled) {
+                float Ec = __fdiv_rn(__fmul_rn(a.k_half_m, __fmul_rn(g, g)), a.q_f);
+                sigma = user_cs(a.cx_spline, Ec);
+              } else {
+                float t = __fadd_rn(__fmul_rn(-0.8821f, logf(g)), 15.1262f);
+                sigma = (double)__fmul_rn(__fmul_rn(t, t), 1e-20f);
+              }
+              double prob = DSUB(1.0, exp(DMUL(DMUL(DMUL(-nl, sigma), (double)g), a.dt)));
+              if (fabs(u - prob) <= fabs(prob) * 8.9e-16 + 1e-300) cnt[6]++;
+              if (u < prob) {
+                cnt[5]++;
+                u32x4 r0 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 0);
+                u32x4 r1 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 1);
+                u32x4 r2 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 2);
+                u32x4 r3 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 3);
+                u32x4 r4 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 4);
+                double fmx = DMUL(2.0, DSUB(DADD(DADD(u53(r0.x, r0.y), u53(r0.z, r0.w)), u53(r1.x, r1.y)), 1.5));
+                double fmy = DMUL(2.0, DSUB(DADD(DADD(u53(r1.z, r1.w), u53(r2.x, r2.y)), u53(r2.z, r2.w)), 1.5));
+                double fmz = DMUL(2.0, DSUB(DADD(DADD(u53(r3.x, r3.y), u53(r3.z, r3.w)), u53(r4.x, r4.y)), 1.5));
+                vx = __double2float_rn(DMUL(a.neut_vth, fmx));
+                vy = __double2float_rn(DMUL(a.neut_vth, fmy));
+                vz = __double2float_rn(DMUL(a.neut_vth, fmz));
+                cx = 1;
+              }
             }
           }
-          // PPC map with truncated cells (:1749-1757)
-          long long tx = clampll(np_f2i64(truncf(__fdiv_rn(x, a.dxf))), 0, a.nx - 1);
-          long long ty = clampll(np_f2i64(truncf(__fdiv_rn(y, a.dyf))), 0, a.ny - 1);
-          atomicAdd(a.ppc + ty * a.nx + tx, 1);
+          // PPC map with truncated cells (:1749-1757), next-step deposit cell (rounded)
+          long long tx = clampll(np_f2i64(trunc_div(x, a.dxf, a.inv_dx)), 0, a.nx - 1);
+          long long ty = clampll(np_f2i64(trunc_div(y, a.dyf, a.inv_dy)), 0, a.ny - 1);
+          ppc_cell = (int)(ty * a.nx + tx);
+          dep_cell = cell_round32_f(y, a.dyf, a.inv_dy, 1, a.ny - 2) * a.nx +
+                     cell_round32_f(x, a.dxf, a.inv_dx, 1, a.nx - 2);
         }
         st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
         st.cex[k] = cx; st.id[k] = pid;
       }
       st.keep[k] = kp;
-      // next-step deposit counts (warp-aggregated: consecutive lanes, near-sorted cells)
-      int c = kp ? deposit_cell(st.x[k], st.y[k], a.dxf, a.dyf, a.nx, a.ny) : 0;
-      warp_count_add(a.cnt, c, kp != 0);
+      // warp-aggregated counts (consecutive lanes, near-sorted cells)
+      warp_count_add(a.ppc, ppc_cell, kp != 0);
+      warp_count_add(a.cnt, dep_cell, kp != 0);
     }
     __syncthreads();
     long long base;
@@ -549,6 +595,7 @@ struct EleStage {
   uint8_t keep[TILE];
 };
 
+template <bool HAS_B>
 __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
   __shared__ EleStage st;
   __shared__ int sm_tile;
@@ -568,21 +615,24 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
     for (int k = threadIdx.x; k < TILE; k += NT) {
       const int i = t0 + k;
       uint8_t kp = 0;
+      int dep_cell = 0;
       if (i < n) {
         float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
         for (int s = 0; s < n_sub; ++s)
-          boris_push_one(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.has_B, a.nx, a.ny, a.dxf, a.dyf, h, dtf);
+          boris_push_one<HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h, dtf);
         if (a.periodic) y = np_modf_pos(y, a.Lyf);
-        int icx = cell_round(x, a.dxf, 0, a.nx - 1), icy = cell_round(y, a.dyf, 0, a.ny - 1);
+        int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1), icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
         bool dead = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
         dead = dead || (x < 0.0f) || (x > a.Lxf) || (y < 0.0f) || (y > a.Lyf) || (x != x);
         kp = !dead;
+        if (kp)
+          dep_cell = cell_round32_f(y, a.dyf, a.inv_dy, 1, a.ny - 2) * a.nx +
+                     cell_round32_f(x, a.dxf, a.inv_dx, 1, a.nx - 2);
         st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
         st.id[k] = a.src.id[i];
       }
       st.keep[k] = kp;
-      int c = kp ? deposit_cell(st.x[k], st.y[k], a.dxf, a.dyf, a.nx, a.ny) : 0;
-      warp_count_add(a.cnt, c, kp != 0);
+      warp_count_add(a.cnt, dep_cell, kp != 0);
     }
     __syncthreads();
     long long base;

@@ -69,6 +69,7 @@ struct Sim {
   float *Ex = nullptr, *Ey = nullptr, *rho = nullptr, *Tmap = nullptr;
   float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *e32 = nullptr;
   uint8_t *isBound = nullptr, *cls = nullptr;
+  uint8_t *bdist = nullptr, *bdist_tmp = nullptr;  // Chebyshev distance to the nearest bound node
   uint16_t* gridmask = nullptr;
   int *ppc = nullptr, *cnt_i = nullptr, *cnt_e = nullptr;
   // multigrid
@@ -110,6 +111,8 @@ struct Sim {
   // report
   pb_step_report* rep_dev = nullptr;
   pb_step_report* rep_host = nullptr;
+  pb_step_report* rep_run = nullptr;  // pinned per-step reports of pb_sim_run
+  int rep_run_cap = 0;
   // settings
   double tol = 1e-8, tol_inner = 1e-5;
   int max_outer = 8, max_inner = 40, nu = 1, max_coarse = 256;
@@ -220,9 +223,18 @@ static void free_levels(Sim* s) {
 }
 
 // node classes from isBound (host copy) and the multigrid hierarchy
+static int32_t update_bound_dist(Sim* s) {
+  const int N = s->ny * s->nx;
+  k_bdist_rows<<<grid_for(s, N, 256), 256, 0, s->stream>>>(s->isBound, s->bdist_tmp, s->ny, s->nx);
+  k_bdist_cols<<<grid_for(s, N, 256), 256, 0, s->stream>>>(s->bdist_tmp, s->bdist, s->ny, s->nx);
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
 static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   std::vector<uint8_t> cls = mghost::node_classes(s->ny, s->nx, s->periodic, isBound_host);
   CK(cudaMemcpyAsync(s->cls, cls.data(), cls.size(), cudaMemcpyHostToDevice, s->stream));
+  if (int32_t rc = update_bound_dist(s)) return rc;
   mghost::Hierarchy H;
   try {
     H = mghost::build(s->ny, s->nx, s->periodic, cls, s->max_coarse);
@@ -361,6 +373,7 @@ struct SplineStore {
   double* c = nullptr;
   int nt = 0;
   double lo = 0.0, hi = 0.0;
+  double cmax = 0.0;  // largest B-spline coefficient: the spline never exceeds it (convex hull)
 };
 
 struct pb_sim {
@@ -528,7 +541,8 @@ static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
   IonStepArgs a{};
   a.src = I.buf[I.cur]; a.dst = I.buf[1 - I.cur]; a.num_src = ni_src; a.num_dst = ni_dst;
   a.Ex = s->Ex; a.Ey = s->Ey; a.Bx = a.By = a.Bz = nullptr; a.has_B = 0;
-  a.isBound = s->isBound; a.nx = s->nx; a.ny = s->ny; a.dxf = dxf; a.dyf = dyf;
+  a.isBound = s->isBound; a.bdist = s->bdist; a.nx = s->nx; a.ny = s->ny; a.dxf = dxf; a.dyf = dyf;
+  a.inv_dx = 1.0f / dxf; a.inv_dy = 1.0f / dyf;
   a.dt = p->dt; a.qm = p->qm_ion; a.ds_lim = p->ds_lim; a.ds_max = (const double*)s->ds_bits; a.n_sub_out = s->n_sub;
   a.periodic = s->periodic; a.Lyf = (float)p->Ly; a.Lxf = (float)p->Lx;
   a.x_entry = (float)p->x_entry; a.x_exit = (float)p->x_exit; a.x_plume = (float)p->x_plume;
@@ -542,10 +556,17 @@ static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
   a.angles = s->angles; a.angle_count = s->angle_count; a.angle_cap = s->angle_cap;
   a.exit_sums = rep->exit_sums; a.counters = (unsigned long long*)&rep->entered;
   a.rT_f = (float)p->rT; a.n0a = p->n0a; a.neut_vth = p->neut_vth; a.cx_spline = spline_of(h->cx);
+  {
+    // collision-probability bound: sigma <= 10^cmax (spline), or <= 2.2881e-18 for the
+    // empirical law while 1 <= g <= 1e14 (|(-0.8821 ln g + 15.1262)| <= 15.1262)
+    double sig_max = h->cx.nt > 0 ? std::pow(10.0, h->cx.cmax) : 2.2881e-18;
+    a.cex_bound = std::fabs(p->n0a) * sig_max * p->dt * (1.0 + 1e-5);
+    a.cex_g_max = h->cx.nt > 0 ? INFINITY : 1e14f;
+  }
   a.seed = s->seed; a.step = (uint32_t)p->iteration;
   a.ppc = s->ppc; a.cnt = s->cnt_i;
   a.tile_status = s->tile_status; a.tile_counter = s->tile_counter; a.errflags = ef;
-  k_ion_step<<<grid_for(s, I.cap, TILE, 8), NT, 0, st>>>(a);
+  k_ion_step<false><<<grid_for(s, I.cap, TILE, 8), NT, 0, st>>>(a);
   ++s->launches;
   mark(s);
 
@@ -561,11 +582,12 @@ static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
   b.src = E.buf[E.cur]; b.dst = E.buf[1 - E.cur]; b.num_src = ne_src; b.num_dst = ne_dst;
   b.Ex = s->Ex; b.Ey = s->Ey; b.Bx = b.By = b.Bz = nullptr; b.has_B = 0;
   b.isBound = s->isBound; b.nx = s->nx; b.ny = s->ny; b.dxf = dxf; b.dyf = dyf;
+  b.inv_dx = 1.0f / dxf; b.inv_dy = 1.0f / dyf;
   b.dt = p->dt; b.qm = p->qm_e; b.ds_lim = p->ds_lim; b.ds_max = (const double*)(s->ds_bits + 1);
   b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
   b.errflags = ef;
-  k_ele_step<<<grid_for(s, E.cap, TILE, 8), NT, 0, st>>>(b);
+  k_ele_step<false><<<grid_for(s, E.cap, TILE, 8), NT, 0, st>>>(b);
   ++s->launches;
 
   // SEE electrons, appended after the surviving electrons (:1390-1417)
@@ -693,7 +715,7 @@ int32_t pb_sim_destroy(pb_sim* h) {
   for (double* q : d) if (q) cudaFree(q);
   float* fl[] = {s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->see_xy, s->angles};
   for (float* q : fl) if (q) cudaFree(q);
-  void* v[] = {s->isBound, s->cls, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->bar, s->counts, s->next_ids,
+  void* v[] = {s->isBound, s->bdist, s->bdist_tmp, s->cls, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->bar, s->counts, s->next_ids,
                s->tile_status, s->tile_counter, s->see_key, s->see_count, s->angle_scratch, s->angle_count,
                s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1], s->sval[0], s->sval[1],
                s->shist, s->rep_dev, h->cx.t, h->cx.c, h->see.t, h->see.c};
@@ -704,6 +726,7 @@ int32_t pb_sim_destroy(pb_sim* h) {
       dfree(o.x); dfree(o.y); dfree(o.vx); dfree(o.vy); dfree(o.vz); dfree(o.id); dfree(o.cex);
     }
   if (s->rep_host) cudaFreeHost(s->rep_host);
+  if (s->rep_run) cudaFreeHost(s->rep_run);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -736,6 +759,11 @@ int32_t pb_sim_set_spline(pb_sim* h, int32_t which, int32_t nt, const double* t,
   CK(cudaMemcpy(S.t, t, nt * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(S.c, c, (nt - 4) * sizeof(double), cudaMemcpyHostToDevice));
   S.nt = nt; S.lo = lo; S.hi = hi;
+  S.cmax = -INFINITY;
+  for (int k = 0; k < nt - 4; ++k) {
+    if (c[k] != c[k]) { S.cmax = NAN; break; }
+    S.cmax = std::max(S.cmax, c[k]);
+  }
   return PB_OK;
 }
 
@@ -755,6 +783,8 @@ int32_t pb_sim_set_domain(pb_sim* h, int32_t ny, int32_t nx, int32_t periodic, c
     float** ff[] = {&s->Ex, &s->Ey, &s->rho, &s->Tmap, &s->r32, &s->z32, &s->p32, &s->q32, &s->e32};
     for (float** q : ff) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(float))); }
     dfree(s->isBound); CK(dalloc(&s->isBound, N));
+    dfree(s->bdist); CK(dalloc(&s->bdist, N));
+    dfree(s->bdist_tmp); CK(dalloc(&s->bdist_tmp, N));
     dfree(s->cls); CK(dalloc(&s->cls, N));
     dfree(s->gridmask); CK(dalloc(&s->gridmask, N));
     int** ii[] = {&s->ppc, &s->cnt_i, &s->cnt_e};
@@ -914,6 +944,10 @@ int32_t pb_sim_set_field(pb_sim* h, int32_t which, const void* host, int64_t nby
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaMemcpy(p, host, nbytes, cudaMemcpyHostToDevice));
   if (which == 7) CK(cudaMemcpy(s->Vdc, host, nbytes, cudaMemcpyHostToDevice));
+  if (which == 6) {
+    if (int32_t rc = update_bound_dist(s)) return rc;
+    CK(cudaStreamSynchronize(s->stream));
+  }
   return PB_OK;
 }
 
@@ -965,13 +999,21 @@ int32_t pb_sim_run(pb_sim* h, const pb_step_params* params, int32_t nsteps, pb_s
   int32_t rc;
   if (nsteps <= 0) return PB_OK;
   if ((rc = ensure_room(s, &params[0], nsteps))) return rc;
+  // reports go to pinned memory, so the copies do not block the host between steps
+  if (reports && s->rep_run_cap < nsteps) {
+    if (s->rep_run) CK(cudaFreeHost(s->rep_run));
+    s->rep_run = nullptr;
+    s->rep_run_cap = 0;
+    CK(cudaMallocHost((void**)&s->rep_run, (size_t)nsteps * sizeof(pb_step_report)));
+    s->rep_run_cap = nsteps;
+  }
   s->mark_used = 0;
   s->launches = 0;
   CK(cudaEventRecord(s->ev0, s->stream));
   for (int k = 0; k < nsteps; ++k) {
     if ((rc = enqueue_step(h, &params[k]))) return rc;
     if (reports) {
-      CK(cudaMemcpyAsync(&reports[k], s->rep_dev, sizeof(pb_step_report), cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaMemcpyAsync(&s->rep_run[k], s->rep_dev, sizeof(pb_step_report), cudaMemcpyDeviceToHost, s->stream));
     }
   }
   CK(cudaEventRecord(s->ev1, s->stream));
@@ -980,9 +1022,11 @@ int32_t pb_sim_run(pb_sim* h, const pb_step_params* params, int32_t nsteps, pb_s
   CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
   s->last_ms = ms;
   if ((rc = read_counts(s))) return rc;
-  if (reports)
+  if (reports) {
+    std::memcpy(reports, s->rep_run, (size_t)nsteps * sizeof(pb_step_report));
     for (int k = 0; k < nsteps; ++k)
       if ((rc = check_flags(s, reports[k].errflags))) return rc;
+  }
   return PB_OK;
 }
 
