@@ -186,6 +186,13 @@ int32_t pb_sim_rebuild_operator(pb_sim* s);
 int32_t pb_sim_set_particles(pb_sim* s, int32_t species, int32_t n, const float* x, const float* y,
                              const float* vx, const float* vy, const float* vz, const uint8_t* cex,
                              const uint32_t* id, uint32_t next_id);
+/* Re-order the particles of one species (0 ions, 1 electrons, -1 both) by cell key
+ * iy * nx + ix, ix = clip(rint(x / dx), 1, nx - 2), with the device radix sort the step
+ * uses every sort interval (stable: equal keys keep their order).  Particle order is
+ * not observable in the reference's results (draws are keyed by particle id), so this
+ * only improves memory locality, e.g. right after an upload in arbitrary order.  No
+ * counterpart in the reference. */
+int32_t pb_sim_sort(pb_sim* s, int32_t species, double dx, double dy);
 int32_t pb_sim_get_particles(pb_sim* s, int32_t species, int32_t n, float* x, float* y, float* vx, float* vy,
                              float* vz, uint8_t* cex, uint32_t* id);
 int32_t pb_sim_counts(pb_sim* s, int32_t* num_p, int32_t* num_e, uint32_t* next_ion_id, uint32_t* next_e_id);
@@ -219,7 +226,8 @@ int32_t pb_sim_set_profiling(pb_sim* s, int32_t on);
 /* Field-solve phase trace: returns the accumulated nanoseconds per phase (out32 may be
  * NULL: [l] down leg of level l, [7] coarse part, [8+l] up leg of level l, [15] Krylov
  * updates, [16] FP64 refinement, [17] right-hand side, [18] Picard update, [19] field,
- * [20] set-up), clears them and switches tracing on or off. */
+ * [20] set-up; [21+p] inner iterations and [26+p] refinement passes of Picard iteration p),
+ * clears them and switches tracing on or off. */
 int32_t pb_sim_poisson_trace(pb_sim* s, int32_t on, double* out32);
 
 /* ---------------------------------------------------------------- host helpers */

@@ -48,10 +48,10 @@ def _pair(PE, name, sort_every=0):
     o.build_domain(params)
     p, cex, e = f["init_p"], f["init_p_cex"], f["init_e"]
     n, ne = p.shape[1], e.shape[1]
-    g.set_particles("ions", *p.astype(np.float32), is_cex=cex, ids=np.arange(n))
+    g.set_particles("ions", *p.astype(np.float32), is_cex=cex, ids=np.arange(n), sort=False)
     o._add_ions(*p, cex, o.new_ion_ids(n))
     if ne:
-        g.set_particles("electrons", *e.astype(np.float32), ids=np.arange(ne))
+        g.set_particles("electrons", *e.astype(np.float32), ids=np.arange(ne), sort=False)
         o._add_electrons(*e, o.new_e_ids(ne))
     return g, o, params
 
@@ -170,6 +170,21 @@ def test_cell_sort_is_stable_argsort(gpu_mod):
     b, cb, ib = _ions(gb)
     nx, ny = ga.nx, ga.ny
     dx, dy = np.float32(ga.dx), np.float32(ga.dy)
+    ix = np.clip(np.round(a[0] / dx).astype(np.int32), 1, nx - 2)
+    iy = np.clip(np.round(a[1] / dy).astype(np.int32), 1, ny - 2)
+    perm = np.argsort(iy.astype(np.int64) * nx + ix, kind="stable")
+    np.testing.assert_array_equal(b.view(np.uint32), a[:, perm].view(np.uint32))
+    np.testing.assert_array_equal(ib, ia[perm])
+    np.testing.assert_array_equal(cb, ca[perm])
+
+
+def test_upload_sort_is_stable_argsort(gpu_mod):
+    g, _, params = _pair(gpu_mod, "c1_both")
+    a, ca, ia = _ions(g)
+    g.set_particles("ions", *a, is_cex=ca, ids=ia, sort=True)
+    b, cb, ib = _ions(g)
+    nx, ny = g.nx, g.ny
+    dx, dy = np.float32(g.dx), np.float32(g.dy)
     ix = np.clip(np.round(a[0] / dx).astype(np.int32), 1, nx - 2)
     iy = np.clip(np.round(a[1] / dy).astype(np.int32), 1, ny - 2)
     perm = np.argsort(iy.astype(np.int64) * nx + ix, kind="stable")

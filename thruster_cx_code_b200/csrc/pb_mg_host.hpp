@@ -25,6 +25,8 @@ struct Level {
   std::vector<uint8_t> act;   // active nodes (level 0: free nodes)
   std::vector<float> st;      // 9 * N stencil (coarse levels)
   std::vector<float> dinv;    // omega / diagonal on active nodes (damped Jacobi smoother)
+  std::vector<float> R;       // (coarse levels >= 2) restriction of the fused cycle, 25 planes
+  std::vector<float> U;       // (levels >= 1 with a coarser level) prolongation + smoothing, 18 planes
 };
 
 constexpr double JACOBI_OMEGA = MG_JACOBI_OMEGA;
@@ -107,6 +109,79 @@ inline int p_row(int nyf, int nxf, int wrap, int nyc, int nxc, int y, int x, lon
 inline int colors_for(const Level& L, int level) {
   if (level == 0) return 2;
   return (L.per && (L.ny & 1)) ? 6 : 4;
+}
+
+// The transfers of the fused V-cycle as explicit stencils, for fine levels l >= 1 (where
+// the operator is a 9-point stencil):
+//   r_{l+1}(c) = [c active] sum_f w_cf [f active] (r_f - sum_j A_fj d_j r_j)
+//              = sum over the 5 x 5 fine patch centred on (2I, 2J) of R_k r_j,
+//   z_f = [f active] (m_f + d_f r_f - d_f sum_j A_fj m_j),  m_j = [j active] (d_j r_j + (P z)_j)
+//       = sum over the 3 x 3 fine patch of U_k r_j + sum over the 3 x 3 coarse patch centred
+//         on (y >> 1, x >> 1) of U_{9+k} z_c.
+// Coefficients are accumulated per patch offset (rows wrap as the device indexes them),
+// so periodic levels with few rows still match the device sums term by term.
+inline void transfer_ops(Hierarchy& H) {
+  for (size_t l = 1; l + 1 < H.lev.size(); ++l) {
+    Level& F = H.lev[l];
+    Level& C = H.lev[l + 1];
+    const int nyf = F.ny, nxf = F.nx, nyc = C.ny, nxc = C.nx;
+    const size_t Nf = (size_t)nyf * nxf, Nc = (size_t)nyc * nxc;
+    auto stF = [&](size_t f, int dI, int dJ) { return (double)F.st[(size_t)((dI + 1) * 3 + (dJ + 1)) * Nf + f]; };
+    C.R.assign(25 * Nc, 0.0f);
+    for (size_t c = 0; c < Nc; ++c) {
+      if (!C.act[c]) continue;
+      const int I = (int)(c / nxc), J = (int)(c % nxc);
+      double acc[25] = {0};
+      for (int da = -1; da <= 1; ++da) {
+        int yf = 2 * I + da;
+        if (yf < 0) { if (C.wrapP) yf += nyf; else continue; }
+        if (yf >= nyf) continue;
+        for (int db = -1; db <= 1; ++db) {
+          const int xf = 2 * J + db;
+          if (xf < 0 || xf >= nxf) continue;
+          const size_t f = (size_t)yf * nxf + xf;
+          if (!F.act[f]) continue;
+          const double w = (da ? 0.5 : 1.0) * (db ? 0.5 : 1.0);
+          for (int dI = -1; dI <= 1; ++dI)
+            for (int dJ = -1; dJ <= 1; ++dJ) {
+              const long j = nb(nyf, nxf, F.per, yf, xf, dI, dJ);
+              if (j < 0) continue;
+              const double v = ((dI == 0 && dJ == 0) ? 1.0 : 0.0) - stF(f, dI, dJ) * (double)F.dinv[j];
+              acc[(2 + da + dI) * 5 + (2 + db + dJ)] += w * v;
+            }
+        }
+      }
+      for (int k = 0; k < 25; ++k) C.R[(size_t)k * Nc + c] = (float)acc[k];
+    }
+    F.U.assign(18 * Nf, 0.0f);
+    long pc[4];
+    double pw[4];
+    for (size_t f = 0; f < Nf; ++f) {
+      if (!F.act[f]) continue;
+      const int y = (int)(f / nxf), x = (int)(f % nxf), I0 = y >> 1, J0 = x >> 1;
+      const double df = F.dinv[f];
+      double ur[9] = {0}, uz[9] = {0};
+      for (int dI = -1; dI <= 1; ++dI)
+        for (int dJ = -1; dJ <= 1; ++dJ) {
+          const long j = nb(nyf, nxf, F.per, y, x, dI, dJ);
+          if (j < 0 || !F.act[j]) continue;
+          const double cm = ((dI == 0 && dJ == 0) ? 1.0 : 0.0) - df * stF(f, dI, dJ);  // weight of m_j
+          ur[(dI + 1) * 3 + (dJ + 1)] += cm * (double)F.dinv[j];
+          const int n = p_row(nyf, nxf, C.wrapP, nyc, nxc, (int)(j / nxf), (int)(j % nxf), pc, pw);
+          for (int q = 0; q < n; ++q) {
+            int oI = (int)(pc[q] / nxc) - I0, oJ = (int)(pc[q] % nxc) - J0;
+            if (C.per) { if (oI > nyc / 2) oI -= nyc; else if (oI < -(nyc / 2)) oI += nyc; }
+            if (oI < -1 || oI > 1 || oJ < -1 || oJ > 1) throw std::runtime_error("prolongation outside the 3 x 3 patch");
+            uz[(oI + 1) * 3 + (oJ + 1)] += cm * pw[q];
+          }
+        }
+      ur[4] += df;
+      for (int k = 0; k < 9; ++k) {
+        F.U[(size_t)k * Nf + f] = (float)ur[k];
+        F.U[(size_t)(9 + k) * Nf + f] = (float)uz[k];
+      }
+    }
+  }
 }
 
 inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>& cls0, int max_coarse) {
@@ -201,6 +276,7 @@ inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>&
       L.dinv[i] = d > 0.0 ? (float)(JACOBI_OMEGA / d) : 0.0f;
     }
   }
+  transfer_ops(H);
   // dense inverse of the coarsest operator (Cholesky, then L^-T L^-1)
   Level& Lc = H.lev.back();
   int level = (int)H.lev.size() - 1;

@@ -54,6 +54,8 @@ struct DevLevel {
   uint8_t* act = nullptr;
   float* st = nullptr;
   float* dinv = nullptr;
+  float* R = nullptr;
+  float* U = nullptr;
   float* r = nullptr;
   float* z = nullptr;
 };
@@ -215,6 +217,8 @@ static int32_t ensure_room(Sim* s, const pb_step_params* p, int steps) {
 static void free_levels(Sim* s) {
   for (size_t l = 0; l < s->lev.size(); ++l) {
     dfree(s->lev[l].dinv);
+    dfree(s->lev[l].R);
+    dfree(s->lev[l].U);
     if (l > 0) { dfree(s->lev[l].act); dfree(s->lev[l].st); dfree(s->lev[l].r); dfree(s->lev[l].z); }
   }
   s->lev.clear();
@@ -252,6 +256,14 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
     size_t N = (size_t)L.ny * L.nx;
     CK(dalloc(&D.dinv, N));
     CK(cudaMemcpy(D.dinv, L.dinv.data(), N * sizeof(float), cudaMemcpyHostToDevice));
+    if (!L.R.empty()) {
+      CK(dalloc(&D.R, L.R.size()));
+      CK(cudaMemcpy(D.R, L.R.data(), L.R.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (!L.U.empty()) {
+      CK(dalloc(&D.U, L.U.size()));
+      CK(cudaMemcpy(D.U, L.U.data(), L.U.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
     if (l == 0) {
       D.act = s->cls; D.st = nullptr; D.r = s->r32; D.z = s->z32;
     } else {
@@ -306,6 +318,8 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
     a.lev[l].ny = D.ny; a.lev[l].nx = D.nx; a.lev[l].per = D.per; a.lev[l].wrapP = D.wrapP;
     a.lev[l].ncolors = D.ncolors; a.lev[l].act = D.act; a.lev[l].st = D.st; a.lev[l].r = D.r; a.lev[l].z = D.z;
     a.lev[l].dinv = D.dinv;
+    a.lev[l].R = D.R;
+    a.lev[l].U = D.U;
   }
   a.nc = s->nc; a.cidx = s->cidx; a.cinvT = s->cinvT;
   a.partials = s->partials; a.bar = s->bar;
@@ -864,6 +878,25 @@ int32_t pb_sim_set_particles(pb_sim* h, int32_t species, int32_t n, const float*
   CK(cudaMemcpy(s->next_ids + species, &next_id, sizeof(uint32_t), cudaMemcpyHostToDevice));
   s->host_num[species] = n;
   s->counts_valid = false;
+  return PB_OK;
+}
+
+int32_t pb_sim_sort(pb_sim* h, int32_t species, double dx, double dy) {
+  Sim* s = &h->s;
+  if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_sort: no domain");
+  if (species < -1 || species > 1 || !(dx > 0.0) || !(dy > 0.0)) return fail(PB_ERR_ARG, "pb_sim_sort");
+  s->sp_dx = dx;
+  s->sp_dy = dy;
+  const long N = (long)s->ny * s->nx;
+  int bits = 1;
+  while ((1L << bits) < N) ++bits;
+  for (int k = 0; k < 2; ++k) {
+    if (species >= 0 && k != species) continue;
+    if (s->sp[k].cap <= 0) continue;
+    int32_t rc = sort_species(s, k, bits);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(s->stream));
   return PB_OK;
 }
 

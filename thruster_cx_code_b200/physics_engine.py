@@ -363,8 +363,10 @@ class DigitalTwinSimulator:
         """``physics_engine.py:506-522``."""
         self._add_particles(1, x, y, vx, vy, vz)
 
-    def set_particles(self, species, x, y, vx, vy, vz, is_cex=None, ids=None):
-        """Replace a species wholesale (species 'ions' or 'electrons')."""
+    def set_particles(self, species, x, y, vx, vy, vz, is_cex=None, ids=None, sort=None):
+        """Replace a species wholesale (species 'ions' or 'electrons').  With ``sort``
+        (default: when cell sorting is on and a domain exists) the uploaded particles are
+        re-ordered by cell at once, so the first steps already gather from local cells."""
         sp = 0 if species in (0, 'ions', 'ion') else 1
         n = len(x)
         arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (x, y, vx, vy, vz)]
@@ -379,6 +381,10 @@ class DigitalTwinSimulator:
             self.num_p, self.next_ion_id = n, nxt
         else:
             self.num_e, self.next_e_id = n, nxt
+        if sort is None:
+            sort = self.sort_every > 0 and bool(self.laplacian_lu)
+        if sort and n > 0:
+            _lib.check(self._libh.pb_sim_sort(self._h, sp, float(self.dx), float(self.dy)), "sort")
         self._invalidate()
 
     # ------------------------------------------------------------------ domain
