@@ -371,106 +371,127 @@ __device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth) {
 }
 
 // ----------------------------------------------------------------- block-0 levels in shared memory
+// The levels from first_small down hold their r and z in block 0's shared memory and
+// apply the host-built transfer stencils (read through L1): one block-level phase per
+// level going down and one going up.
 struct SLev {
   int ny, nx, per, wrapP, N;
-  float *st, *dinv, *r, *z;
+  float *r, *z;
+  float *R, *U;  // transfer stencils staged from global memory (R: levels > first, U: levels < last)
 };
 
-// offsets of the small levels in dynamic shared memory (must match small_smem_bytes on the host)
-__device__ void small_layout(const PoissonArgs& a, float* base, SLev* sl, float** tmp, float** rc) {
+// layout of dynamic shared memory (mg_small_smem_bytes on the host): per level r and z;
+// then U of levels first..last-1, R of levels first+1..last, the coarsest inverse and
+// the coarsest right-hand side
+__device__ void small_layout(const PoissonArgs& a, float* base, SLev* sl, float** cinv, float** rc) {
   size_t off = 0;
-  int maxN = 0;
-  for (int l = a.first_small; l < a.nlevels; ++l) {
+  const int fs = a.first_small, last = a.nlevels - 1;
+  for (int l = fs; l <= last; ++l) {
     const MgLevel& L = a.lev[l];
     SLev& S = sl[l];
     S.ny = L.ny; S.nx = L.nx; S.per = L.per; S.wrapP = L.wrapP; S.N = L.ny * L.nx;
-    S.st = base + off; off += 9 * (size_t)S.N;
-    S.dinv = base + off; off += S.N;
     S.r = base + off; off += S.N;
     S.z = base + off; off += S.N;
-    maxN = S.N > maxN ? S.N : maxN;
+    S.R = S.U = nullptr;
   }
-  *tmp = base + off; off += maxN;
+  for (int l = fs; l < last; ++l) { sl[l].U = base + off; off += 18 * (size_t)sl[l].N; }
+  for (int l = fs + 1; l <= last; ++l) { sl[l].R = base + off; off += 25 * (size_t)sl[l].N; }
+  if (a.cinv_smem) { *cinv = base + off; off += (size_t)a.nc * a.nc; }
+  else *cinv = const_cast<float*>(a.cinvT);
   *rc = base + off;
 }
 
-__device__ __forceinline__ int snb(const SLev& L, int y, int x, int dI, int dJ) {
-  int yy = y + dI, xx = x + dJ;
-  if (L.per) { if (yy < 0) yy += L.ny; else if (yy >= L.ny) yy -= L.ny; }
-  if (yy < 0 || yy >= L.ny || xx < 0 || xx >= L.nx) return -1;
-  return yy * L.nx + xx;
+// r at coarse node c = (I, J) from the finer level's r (5 x 5 patch, stencil Rc)
+__device__ __forceinline__ float srestrict(const SLev& F, const float* Rc, int Nc, int I, int J,
+                                           int c) {
+  float s = 0.0f;
+#pragma unroll
+  for (int t = 0; t < 5; ++t) {
+    int y = 2 * I + t - 2;
+    if (F.per) { if (y < 0) y += F.ny; else if (y >= F.ny) y -= F.ny; }
+    const bool rv = y >= 0 && y < F.ny;
+#pragma unroll
+    for (int u = 0; u < 5; ++u) {
+      const int x = 2 * J + u - 2;
+      const bool ok = rv && x >= 0 && x < F.nx;
+      const float w = Rc[(t * 5 + u) * Nc + c];
+      const float v = F.r[ok ? y * F.nx + x : 0];
+      s += ok ? w * v : 0.0f;
+    }
+  }
+  return s;
 }
 
-// tmp_f = [f active] ((1 - w) r_f - sum_{k != c} A_fk d_k r_k); then r_c = P^T tmp
-__device__ void sdown(const SLev& F, const SLev& C, float* tmp) {
-  for (int f = threadIdx.x; f < F.N; f += blockDim.x) {
-    const int y = f / F.nx, x = f - y * F.nx;
-    float res = W_KEEP * F.r[f];
+// z at fine node f = (y, x) from its r patch and the coarser level's z (stencil Uf)
+__device__ __forceinline__ float sprolong(const SLev& F, const SLev& C, const float* Uf, int y, int x,
+                                          int f) {
+  const int I0 = y >> 1, J0 = x >> 1;
+  float s = 0.0f;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      if (k == 4) continue;
-      const int j = snb(F, y, x, k / 3 - 1, k % 3 - 1);
-      if (j >= 0) res -= F.st[k * F.N + f] * (F.dinv[j] * F.r[j]);
+  for (int t = 0; t < 3; ++t) {
+    int yy = y + t - 1;
+    if (F.per) { if (yy < 0) yy += F.ny; else if (yy >= F.ny) yy -= F.ny; }
+    const bool rv = yy >= 0 && yy < F.ny;
+    int cy = I0 + t - 1;
+    if (C.per) { if (cy < 0) cy += C.ny; else if (cy >= C.ny) cy -= C.ny; }
+    const bool cvr = cy >= 0 && cy < C.ny;
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      const int xx = x + u - 1;
+      const bool ok = rv && xx >= 0 && xx < F.nx;
+      const float vr = F.r[ok ? yy * F.nx + xx : f];
+      s += ok ? Uf[(t * 3 + u) * F.N + f] * vr : 0.0f;
+      const int cx = J0 + u - 1;
+      const bool okc = cvr && cx >= 0 && cx < C.nx;
+      const float vz = C.z[okc ? cy * C.nx + cx : 0];
+      s += okc ? Uf[(9 + t * 3 + u) * F.N + f] * vz : 0.0f;
     }
-    tmp[f] = F.dinv[f] > 0.0f ? res : 0.0f;
   }
-  __syncthreads();
-  for (int c = threadIdx.x; c < C.N; c += blockDim.x) {
-    const int I = c / C.nx, J = c - I * C.nx;
-    float s = 0.0f;
-#pragma unroll
-    for (int da = -1; da <= 1; ++da) {
-      int yf = 2 * I + da;
-      if (yf < 0) { if (C.wrapP) yf += F.ny; else continue; }
-      if (yf >= F.ny) continue;
-#pragma unroll
-      for (int db = -1; db <= 1; ++db) {
-        const int xf = 2 * J + db;
-        if (xf < 0 || xf >= F.nx) continue;
-        s += (da ? 0.5f : 1.0f) * (db ? 0.5f : 1.0f) * tmp[yf * F.nx + xf];
-      }
+  return s;
+}
+
+// two nodes per thread and pass, so that a level slightly larger than the block still
+// takes one round of loads
+template <class Fn>
+__device__ __forceinline__ void block_pairs(int N, Fn fn) {
+  for (int i0 = threadIdx.x; i0 < N; i0 += 2 * blockDim.x) {
+    const int i1 = i0 + blockDim.x;
+    fn(i0, i1 < N ? i1 : -1);
+  }
+}
+
+__device__ void sdown(const SLev& F, const SLev& C, const float* Rc) {
+  block_pairs(C.N, [&](int c0, int c1) {
+    const int I0 = c0 / C.nx, J0 = c0 - I0 * C.nx;
+    const float v0 = srestrict(F, Rc, C.N, I0, J0, c0);
+    float v1 = 0.0f;
+    if (c1 >= 0) {
+      const int I1 = c1 / C.nx, J1 = c1 - I1 * C.nx;
+      v1 = srestrict(F, Rc, C.N, I1, J1, c1);
     }
-    C.r[c] = C.dinv[c] > 0.0f ? s : 0.0f;
-  }
+    C.r[c0] = v0;
+    if (c1 >= 0) C.r[c1] = v1;
+  });
   __syncthreads();
 }
 
-// tmp = m = [active] (d r + P z_c); z = (1 - w) m + d (r - sum_{k != c} A m)
-__device__ void sup(const SLev& F, const SLev& C, float* tmp) {
-  for (int f = threadIdx.x; f < F.N; f += blockDim.x) {
-    const int y = f / F.nx, x = f - y * F.nx;
-    const int I0 = y >> 1, J0 = x >> 1, ay = y & 1, bx = x & 1;
-    float pz = 0.0f;
-    for (int da = 0; da <= ay; ++da) {
-      int I = I0 + da;
-      if (I >= C.ny) { if (C.wrapP) I -= C.ny; else continue; }
-      for (int db = 0; db <= bx; ++db) {
-        const int J = J0 + db;
-        if (J >= C.nx) continue;
-        pz += (ay ? 0.5f : 1.0f) * (bx ? 0.5f : 1.0f) * C.z[I * C.nx + J];
-      }
+__device__ void sup(const SLev& F, const SLev& C, const float* Uf) {
+  block_pairs(F.N, [&](int f0, int f1) {
+    const int y0 = f0 / F.nx, x0 = f0 - y0 * F.nx;
+    const float v0 = sprolong(F, C, Uf, y0, x0, f0);
+    float v1 = 0.0f;
+    if (f1 >= 0) {
+      const int y1 = f1 / F.nx, x1 = f1 - y1 * F.nx;
+      v1 = sprolong(F, C, Uf, y1, x1, f1);
     }
-    const float d = F.dinv[f];
-    tmp[f] = d > 0.0f ? d * F.r[f] + pz : 0.0f;
-  }
-  __syncthreads();
-  for (int f = threadIdx.x; f < F.N; f += blockDim.x) {
-    const int y = f / F.nx, x = f - y * F.nx;
-    float acc = F.r[f];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      if (k == 4) continue;
-      const int j = snb(F, y, x, k / 3 - 1, k % 3 - 1);
-      if (j >= 0) acc -= F.st[k * F.N + f] * tmp[j];
-    }
-    const float d = F.dinv[f];
-    F.z[f] = d > 0.0f ? W_KEEP * tmp[f] + d * acc : 0.0f;
-  }
+    F.z[f0] = v0;
+    if (f1 >= 0) F.z[f1] = v1;
+  });
   __syncthreads();
 }
 
 // z = A_c^{-1} r on the coarsest level (dense inverse in global memory, 4 lanes per row)
-__device__ void scoarse(const PoissonArgs& a, const SLev& L, float* rc) {
+__device__ void scoarse(const PoissonArgs& a, const SLev& L, const float* cinv, float* rc) {
   const int nc = a.nc;
   for (int i = threadIdx.x; i < L.N; i += blockDim.x) L.z[i] = 0.0f;
   for (int k = threadIdx.x; k < nc; k += blockDim.x) rc[k] = L.r[__ldg(a.cidx + k)];
@@ -479,7 +500,7 @@ __device__ void scoarse(const PoissonArgs& a, const SLev& L, float* rc) {
     const int q = base + threadIdx.x, k = q >> 2, part = q & 3;
     float s = 0.0f;
     if (k < nc)
-      for (int j = part; j < nc; j += 4) s += __ldg(a.cinvT + (size_t)j * nc + k) * rc[j];
+      for (int j = part; j < nc; j += 4) s += cinv[j * nc + k] * rc[j];
     s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
     s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
     if (k < nc && part == 0) L.z[__ldg(a.cidx + k)] = s;
@@ -489,23 +510,33 @@ __device__ void scoarse(const PoissonArgs& a, const SLev& L, float* rc) {
 
 // block 0: restrict from level first_small-1 (global), cycle through the small levels in
 // shared memory, publish z on level first_small for the grid-wide up leg
-__device__ void small_cycle(const PoissonArgs& a, const SLev* sl, float* tmp, float* rc) {
+__device__ void small_cycle(const PoissonArgs& a, const SLev* sl, const float* cinv, float* rc) {
   const int fs = a.first_small, last = a.nlevels - 1;
   const MgLevel& F = a.lev[fs - 1];
+  const MgLevel& CG = a.lev[fs];
   const SLev& C0 = sl[fs];
-  for (int ic = threadIdx.x; ic < C0.N; ic += blockDim.x) {
-    const int I = ic / C0.nx, J = ic - I * C0.nx;
-    if (fs - 1 == 0) {
-      const float s = restrict_res<true>(F, F.r, I, J, C0.wrapP != 0);
-      C0.r[ic] = C0.dinv[ic] > 0.0f ? s : 0.0f;
-    } else {
-      C0.r[ic] = restrict_pre(F, a.lev[fs], F.r, I, J, ic);
+  block_pairs(C0.N, [&](int c0, int c1) {
+    float v[2] = {0.0f, 0.0f};
+    const int cc[2] = {c0, c1};
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int c = cc[q];
+      if (c < 0) continue;
+      const int I = c / C0.nx, J = c - I * C0.nx;
+      if (fs - 1 == 0) {
+        const float s = restrict_res<true>(F, F.r, I, J, C0.wrapP != 0);
+        v[q] = __ldg(CG.dinv + c) > 0.0f ? s : 0.0f;
+      } else {
+        v[q] = restrict_pre(F, CG, F.r, I, J, c);
+      }
     }
-  }
+    C0.r[c0] = v[0];
+    if (c1 >= 0) C0.r[c1] = v[1];
+  });
   __syncthreads();
-  for (int l = fs; l < last; ++l) sdown(sl[l], sl[l + 1], tmp);
-  scoarse(a, sl[last], rc);
-  for (int l = last - 1; l >= fs; --l) sup(sl[l], sl[l + 1], tmp);
+  for (int l = fs; l < last; ++l) sdown(sl[l], sl[l + 1], sl[l + 1].R);
+  scoarse(a, sl[last], cinv, rc);
+  for (int l = last - 1; l >= fs; --l) sup(sl[l], sl[l + 1], sl[l].U);
   float* zg = a.lev[fs].z;
   for (int i = threadIdx.x; i < C0.N; i += blockDim.x) __stcg(zg + i, C0.z[i]);
 }
@@ -526,7 +557,7 @@ __device__ void coarse_only(const PoissonArgs& a) {
 
 // z32 = M^{-1} r32 by one V(1,1) cycle; leaves the partial of (r, z) in `slot` and ends
 // with a barrier
-__device__ void vcycle(const PoissonArgs& a, const SLev* sl, float* tmp, float* rc, int slot) {
+__device__ void vcycle(const PoissonArgs& a, const SLev* sl, const float* cinv, float* rc, int slot) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   double rz = 0.0;
   if (a.nlevels == 1) {
@@ -544,7 +575,7 @@ __device__ void vcycle(const PoissonArgs& a, const SLev* sl, float* tmp, float* 
     grid_barrier(a.bar, a.errflags);
     tmark(a, l < 7 ? l : 6);
   }
-  if (blockIdx.x == 0) small_cycle(a, sl, tmp, rc);
+  if (blockIdx.x == 0) small_cycle(a, sl, cinv, rc);
   grid_barrier(a.bar, a.errflags);
   tmark(a, 7);
   for (int l = a.first_small - 1; l >= 1; --l) {
@@ -562,24 +593,25 @@ __device__ void vcycle(const PoissonArgs& a, const SLev* sl, float* tmp, float* 
 __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
   extern __shared__ float4 dyn_smem[];
   __shared__ SLev sl[MG_MAX_LEVELS];
-  __shared__ float* s_tmp;
   __shared__ float* s_rc;
+  __shared__ float* s_cinv;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
   const int N = a.ny * a.nx;
   int slot = 0;
   double n_outer = 0, n_inner = 0, last_rel = 0;
   tmark(a, 20);
 
-  // block 0: stage the small levels' operators in shared memory
+  // block 0: the small levels' vectors, transfer stencils and coarsest inverse in shared memory
   if (blockIdx.x == 0 && a.nlevels > 1) {
-    if (threadIdx.x == 0) small_layout(a, reinterpret_cast<float*>(dyn_smem), sl, &s_tmp, &s_rc);
+    if (threadIdx.x == 0) small_layout(a, reinterpret_cast<float*>(dyn_smem), sl, &s_cinv, &s_rc);
     __syncthreads();
-    for (int l = a.first_small; l < a.nlevels; ++l) {
-      const SLev& S = sl[l];
-      const MgLevel& L = a.lev[l];
-      for (int k = threadIdx.x; k < 9 * S.N; k += blockDim.x) S.st[k] = __ldg(L.st + k);
-      for (int k = threadIdx.x; k < S.N; k += blockDim.x) S.dinv[k] = __ldg(L.dinv + k);
-    }
+    const int fs = a.first_small, last = a.nlevels - 1;
+    for (int l = fs; l < last; ++l)
+      for (int k = threadIdx.x; k < 18 * sl[l].N; k += blockDim.x) sl[l].U[k] = __ldg(a.lev[l].U + k);
+    for (int l = fs + 1; l <= last; ++l)
+      for (int k = threadIdx.x; k < 25 * sl[l].N; k += blockDim.x) sl[l].R[k] = __ldg(a.lev[l].R + k);
+    if (a.cinv_smem)
+      for (int k = threadIdx.x; k < a.nc * a.nc; k += blockDim.x) s_cinv[k] = __ldg(a.cinvT + k);
     __syncthreads();
   }
 
@@ -632,7 +664,7 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
       for (int k = 0; k < a.max_inner; ++k) {
         n_inner += 1;
         tmark(a, 15);
-        vcycle(a, sl, s_tmp, s_rc, slot);  // z32 = M r32, (r, z) partial in slot, barrier
+        vcycle(a, sl, s_cinv, s_rc, slot);  // z32 = M r32, (r, z) partial in slot, barrier
         double rz;
         get_sums(a, slot++, rz, dummy);
         const double beta = k == 0 ? 0.0 : rz / rz_old;

@@ -54,6 +54,7 @@ struct PoissonArgs {
   int nc;                 // coarsest active count
   const int* cidx;        // coarsest active node indices
   const float* cinvT;     // coarsest inverse, transposed (nc x nc)
+  int cinv_smem;          // block 0 stages cinvT in shared memory
   // reductions and barrier
   double* partials;       // 4 slots x 2 values x gridDim doubles
   unsigned int* bar;      // barrier word (any start value)
@@ -62,13 +63,15 @@ struct PoissonArgs {
   unsigned long long* trace;  // optional: ns per phase category (block 0), [31] = last stamp
 };
 
-// dynamic shared memory of k_poisson for levels first..nlevels-1 of sizes N[l]:
-// per level 9N stencil + N dinv + N r + N z floats, then max N scratch and nc floats
-inline size_t mg_small_smem_bytes(const int* N, int first, int nlevels, int nc) {
+// dynamic shared memory of k_poisson for levels first..nlevels-1 of sizes N[l]: r and z
+// per level, U (18 N) of levels first..last-1, R (25 N) of levels first+1..last, the
+// coarsest inverse (nc^2, when cinv_smem) and right-hand side (nc), all float
+inline size_t mg_small_smem_bytes(const int* N, int first, int nlevels, int nc, int cinv_smem) {
   size_t f = 0;
-  int maxN = 0;
-  for (int l = first; l < nlevels; ++l) { f += 12 * (size_t)N[l]; maxN = N[l] > maxN ? N[l] : maxN; }
-  return 4 * (f + (size_t)maxN + (size_t)nc);
+  for (int l = first; l < nlevels; ++l) f += 2 * (size_t)N[l];
+  for (int l = first; l < nlevels - 1; ++l) f += 18 * (size_t)N[l];
+  for (int l = first + 1; l < nlevels; ++l) f += 25 * (size_t)N[l];
+  return 4 * (f + (cinv_smem ? (size_t)nc * nc : 0) + (size_t)nc);
 }
 
 }  // namespace pb

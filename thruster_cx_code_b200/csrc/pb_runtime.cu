@@ -87,6 +87,7 @@ struct Sim {
   int trace_on = 0;
   int pgrid = 0;
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
+  int cinv_smem = 0;  // coarsest inverse staged in shared memory
   // particles
   Species sp[2];
   int* counts = nullptr;         // [ion buf0, ion buf1, ele buf0, ele buf1]
@@ -277,18 +278,24 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   }
   if (s->first_small < 1) s->first_small = 1;
   s->nc = (int)H.cidx.size();
-  // the block-0 levels live in shared memory: move the first one down until they fit
+  // the block-0 levels live in shared memory: move the first one down until they fit,
+  // with the coarsest inverse there too if possible
   std::vector<int> Ns(H.lev.size());
   for (size_t l = 0; l < H.lev.size(); ++l) Ns[l] = H.lev[l].ny * H.lev[l].nx;
   const int nl = (int)H.lev.size();
+  const int fs0 = s->first_small;
   s->psmem = 0;
+  s->cinv_smem = 0;
   if (nl > 1) {
-    while (s->first_small < nl - 1 && mg_small_smem_bytes(Ns.data(), s->first_small, nl, s->nc) > MG_SMALL_SMEM_CAP)
-      ++s->first_small;
-    s->psmem = mg_small_smem_bytes(Ns.data(), s->first_small, nl, s->nc);
-    if (s->psmem > MG_SMALL_SMEM_CAP)
-      return fail(PB_ERR_ARG, "multigrid build: the coarsest level needs " + std::to_string(s->psmem) +
-                                  " bytes of shared memory");
+    bool fit = false;
+    for (int cs = 1; cs >= 0 && !fit; --cs) {
+      int fs = fs0;
+      while (fs < nl - 1 && mg_small_smem_bytes(Ns.data(), fs, nl, s->nc, cs) > MG_SMALL_SMEM_CAP) ++fs;
+      size_t b = mg_small_smem_bytes(Ns.data(), fs, nl, s->nc, cs);
+      if (b <= MG_SMALL_SMEM_CAP) { fit = true; s->first_small = fs; s->psmem = b; s->cinv_smem = cs; }
+    }
+    if (!fit)
+      return fail(PB_ERR_ARG, "multigrid build: the coarsest level does not fit in shared memory");
   }
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_poisson, PT, s->psmem));
@@ -321,7 +328,7 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
     a.lev[l].R = D.R;
     a.lev[l].U = D.U;
   }
-  a.nc = s->nc; a.cidx = s->cidx; a.cinvT = s->cinvT;
+  a.nc = s->nc; a.cidx = s->cidx; a.cinvT = s->cinvT; a.cinv_smem = s->cinv_smem;
   a.partials = s->partials; a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
   a.stats = s->pstats;
