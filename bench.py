@@ -113,12 +113,16 @@ def measured_peak_gbs():
 
 
 def ion_step_traffic_per_ion():
-    """DRAM bytes per ion of one k_ion_step launch from the committed ncu summary, if any."""
+    """DRAM bytes per ion of one k_ion_step launch, from the 'dram_bytes_per_ion:' line of
+    the committed ncu summary, if present."""
     try:
-        with open(os.path.join(ROOT, "profiles", "k_ion_step_traffic.json")) as f:
-            return float(json.load(f)["dram_bytes_per_ion"])
+        with open(os.path.join(ROOT, "profiles", "k_ion_step_large_aperture_3grid.md")) as f:
+            for line in f:
+                if line.strip().startswith("dram_bytes_per_ion:"):
+                    return float(line.split(":", 1)[1].split()[0])
     except Exception:
-        return None
+        pass
+    return None
 
 
 # ----------------------------------------------------------------------------- GPU arm

@@ -474,6 +474,63 @@ __global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* hist, int total) {
   }
 }
 
+// Multi-block exclusive scan of a long uint32 array: per-chunk sums, a one-block scan of
+// the sums (k_sort_scan), then each chunk scanned from its base.
+constexpr int SCAN_NT = 1024, SCAN_PER = 8, SCAN_CHUNK = SCAN_NT * SCAN_PER;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t sm[SCAN_NT / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) sm[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t s = lane < SCAN_NT / 32 ? sm[lane] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xFFFFFFFFu, s, o);
+      if (lane >= o) s += t;
+    }
+    sm[lane] = s;
+  }
+  __syncthreads();
+  const uint32_t ex = (w ? sm[w - 1] : 0u) + inc - v;
+  if (total) *total = sm[SCAN_NT / 32 - 1];
+  __syncthreads();
+  return ex;
+}
+
+__global__ void __launch_bounds__(SCAN_NT) k_scan_partials(const uint32_t* a, int total, uint32_t* bsum) {
+  const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER;
+  uint32_t s = 0u;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER; ++k)
+    if (base + k < total) s += a[base + k];
+  uint32_t t;
+  block_excl_scan(s, &t);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(SCAN_NT) k_scan_apply(uint32_t* a, int total, const uint32_t* bsum) {
+  const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER;
+  uint32_t v[SCAN_PER];
+  uint32_t s = 0u;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER; ++k) {
+    v[k] = base + k < total ? a[base + k] : 0u;
+    s += v[k];
+  }
+  uint32_t ex = block_excl_scan(s, nullptr) + bsum[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_PER; ++k) {
+    if (base + k < total) a[base + k] = ex;
+    ex += v[k];
+  }
+}
+
 // stable scatter: within a tile, elements are ranked per digit in index order
 __global__ void __launch_bounds__(SORT_NT) k_sort_scatter(const uint32_t* key, const uint32_t* val, const int* n_dev,
                                                           int shift, const uint32_t* offs, int ntiles,

@@ -109,7 +109,7 @@ struct Sim {
   int* inj = nullptr;                      // 7 ints
   int* see_spawned = nullptr;
   // sort
-  uint32_t *skey[2] = {nullptr, nullptr}, *sval[2] = {nullptr, nullptr}, *shist = nullptr;
+  uint32_t *skey[2] = {nullptr, nullptr}, *sval[2] = {nullptr, nullptr}, *shist = nullptr, *sblk = nullptr;
   size_t sort_cap = 0, hist_cap = 0;
   // report
   pb_step_report* rep_dev = nullptr;
@@ -180,6 +180,8 @@ static int32_t alloc_species(Sim* s, int k, int cap, int keep_n) {
     size_t hc = (size_t)RADIX * (scap / SORT_TILE + 1);
     dfree(s->shist);
     CK(dalloc(&s->shist, hc));
+    dfree(s->sblk);
+    CK(dalloc(&s->sblk, hc / SCAN_CHUNK + 1));
     s->hist_cap = hc;
   }
   return PB_OK;
@@ -423,8 +425,13 @@ static int32_t sort_species(Sim* s, int k, int ncell_bits) {
   for (int shift = 0; shift < ncell_bits; shift += RADIX_BITS) {
     k_sort_hist<<<ntiles, SORT_NT, 0, st>>>(s->skey[a], n_src, shift, s->shist, ntiles);
     ++s->launches;
-    k_sort_scan<<<1, 1024, 0, st>>>(s->shist, RADIX * ntiles);
-    ++s->launches;
+    {
+      const int total = RADIX * ntiles, nb = (total + SCAN_CHUNK - 1) / SCAN_CHUNK;
+      k_scan_partials<<<nb, SCAN_NT, 0, st>>>(s->shist, total, s->sblk);
+      k_sort_scan<<<1, 1024, 0, st>>>(s->sblk, nb);
+      k_scan_apply<<<nb, SCAN_NT, 0, st>>>(s->shist, total, s->sblk);
+      s->launches += 3;
+    }
     k_sort_scatter<<<ntiles, SORT_NT, 0, st>>>(s->skey[a], s->sval[a], n_src, shift, s->shist, ntiles,
                                                 s->skey[1 - a], s->sval[1 - a]);
     ++s->launches;
@@ -739,7 +746,7 @@ int32_t pb_sim_destroy(pb_sim* h) {
   void* v[] = {s->isBound, s->bdist, s->bdist_tmp, s->cls, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->bar, s->counts, s->next_ids,
                s->tile_status, s->tile_counter, s->see_key, s->see_count, s->angle_scratch, s->angle_count,
                s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1], s->sval[0], s->sval[1],
-               s->shist, s->rep_dev, h->cx.t, h->cx.c, h->see.t, h->see.c};
+               s->shist, s->sblk, s->rep_dev, h->cx.t, h->cx.c, h->see.t, h->see.c};
   for (void* q : v) if (q) cudaFree(q);
   for (int k = 0; k < 2; ++k)
     for (int b = 0; b < 2; ++b) {
