@@ -237,6 +237,28 @@ double pb_host_philox_uniform(uint64_t seed, uint64_t pid, uint32_t site, uint32
 double pb_host_philox_normal(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j);
 float pb_host_percentile95(const float* sorted, int32_t n);
 
+/* ---------------------------------------------------------------- batched instances
+ * Several simulators advanced together on one GPU: sweep points of a perveance or
+ * backstreaming study (the reference runs one process per point,
+ * Python/benchmarks/benchmark_perveance.py:78-164).  No single counterpart in the
+ * reference; each instance's step is the same as pb_sim_step's. */
+typedef struct pb_batch pb_batch;
+
+int32_t pb_batch_create(pb_batch** out, int32_t device);
+int32_t pb_batch_destroy(pb_batch* b);
+/* Advance n simulators (all on the batch's device, each at most once in the list) by K
+ * steps: params[i * K + k] is step k of simulator i and reports[i * K + k] (may be NULL)
+ * receives its report.  Each instance's particle kernels run on its own stream; the field
+ * solves due in a step run as one cooperative launch with the SMs shared out in
+ * proportion to grid size.  Results per instance equal those of pb_sim_run.  Returns
+ * after the last step has completed. */
+int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_params* params, int32_t K,
+                     pb_step_report* reports);
+/* out2[0] = device time (ms) of the last pb_batch_run, out2[1] = kernel launches in it. */
+int32_t pb_batch_timing(pb_batch* b, double* out2);
+/* Device memory held by a simulator (bytes, estimated from its capacities). */
+int32_t pb_sim_memory(pb_sim* s, int64_t* bytes);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,103 @@
+"""Host logic of the batched/served mode, on the CPU: the convergence test, and the
+server's admission under a memory budget, instance cap, retirement and latency statistics
+(with a fake batch that stands in for the device)."""
+import math
+
+import numpy as np
+
+from thruster_cx_code_b200 import workloads as W
+from thruster_cx_code_b200.serving import Convergence, Request, SweepServer
+
+
+def test_convergence_window_halves():
+    c = Convergence(window=10, tol=1e-2, keys=("current", "theta95"))
+    for _ in range(9):
+        c.add(current=1.0, theta95=2.0)
+    assert not c.converged()  # fewer than min_steps
+    c.add(current=1.0, theta95=2.0)
+    assert c.converged()
+    c.add(current=2.0, theta95=2.0)  # one outlier moves the second half's mean by 20%
+    assert not c.converged()
+    assert math.isclose(c.changes()["current"], 0.2 / 1.2, rel_tol=1e-12)
+
+
+def test_convergence_nan_blocks_retirement():
+    c = Convergence(window=4, tol=1.0, keys=("theta95",))
+    for v in (1.0, float("nan"), 1.0, 1.0):
+        c.add(theta95=v)
+    assert not c.converged()
+
+
+class _FakeRep:
+    def __init__(self):
+        self.crossed = 10
+        self.injected = self.rf_injected = self.neut_injected = 0
+        self.num_p, self.num_e, self.n_sub_ion, self.n_sub_e = 100, 10, 1, 2
+
+
+class _FakeSim:
+    q_ion, macro_weight, dt = 1.602e-19, 1e3, 1e-10
+    num_p, num_e, n_sub_ion, n_sub_e = 100, 10, 1, 2
+
+    def __init__(self, mem):
+        self.mem, self.closed = mem, False
+
+    def device_bytes(self):
+        return self.mem
+
+    def close(self):
+        self.closed = True
+
+
+class _FakeBatch:
+    """Steps every instance instantly; records how many ran together."""
+
+    def __init__(self):
+        self.last_ms = 0.0
+        self.widths = []
+
+    def run(self, sims, params, k):
+        self.widths.append(len(sims))
+        return [[((False, -10.0, 5.0, [], 0.0), _FakeRep()) for _ in range(k)] for _ in sims]
+
+
+def test_server_admission_budget_and_retirement():
+    fb = _FakeBatch()
+    srv = SweepServer(hbm_budget_bytes=250, max_active=3, chunk=5, batch=fb)
+    reqs = [Request(i, (lambda m=100: (_FakeSim(m), {})), est_bytes=100, max_steps=20,
+                    convergence=Convergence(window=10, tol=1e-6)) for i in range(5)]
+    done = srv.serve([(0.0, r) for r in reqs])
+    assert len(done) == 5
+    # 250 bytes admit two 100-byte instances at a time
+    assert max(fb.widths) == 2
+    assert all(r.converged and r.steps == 10 for r in done)
+    st = srv.stats()
+    assert st["completed"] == 5 and st["converged"] == 5
+    assert st["p50_s"] <= st["p99_s"]
+    assert all(r.sim is None for r in done)
+
+
+def test_server_step_limit_without_convergence():
+    fb = _FakeBatch()
+    srv = SweepServer(hbm_budget_bytes=1e9, max_active=8, chunk=7, batch=fb)
+    reqs = [Request(i, (lambda: (_FakeSim(10), {})), est_bytes=10, max_steps=12,
+                    convergence=Convergence(window=1000, tol=1e-6)) for i in range(3)]
+    done = srv.serve([(0.0, r) for r in reqs])
+    assert [r.steps for r in done] == [12, 12, 12]
+    assert not any(r.converged for r in done)
+    assert fb.widths == [3, 3]  # 7 steps, then the 5 that remain
+
+
+def test_sweep_points_build_and_fit_estimate():
+    from oracle import pic_oracle as O
+    from thruster_cx_code_b200.domain import build_domain_geometry
+    rng = np.random.default_rng(3)
+    for i in range(6):
+        sp = W.sweep_point(rng, i)
+        o = O.OracleSimulator(build_domain_geometry)
+        o.dx = o.dy = sp["dx"]
+        o.dt = sp["dt"]
+        o.m_e = o.m_ion / sp["m_e_ratio"]
+        o.build_domain(dict(sp["params"]))  # passes the reference's numerics checks
+        nodes = o.nx * o.ny
+        assert W.sweep_point_bytes(sp) > 800 * nodes

@@ -13,8 +13,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libpbemcs.so")
-SOURCES = ["pb_runtime.cu", "pb_particles.cu", "pb_poisson.cu", "pb_misc.cu", "pb_common.cuh", "pb_kernels.cuh",
-           "pb_misc.cuh", "pb_poisson.cuh", "pb_mg_host.hpp"]
+SOURCES = ["pb_runtime.cu", "pb_particles.cu", "pb_poisson.cu", "pb_misc.cu", "pb_batch.cu", "pb_common.cuh",
+           "pb_kernels.cuh", "pb_misc.cuh", "pb_poisson.cuh", "pb_mg_host.hpp"]
 
 
 def nvcc():

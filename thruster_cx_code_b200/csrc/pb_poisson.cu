@@ -38,14 +38,20 @@ constexpr int PT = 1024;  // threads per block (one block per SM)
 constexpr long long BAR_SPIN_LIMIT = 1ll << 22;
 constexpr float W_KEEP = (float)(1.0 - MG_JACOBI_OMEGA);
 
-// Grid barrier on one 32-bit word: block 0 adds 2^31 - (nblocks - 1), the others add 1,
+// Grid barrier on one 32-bit word per instance: its block 0 adds 2^31 - (nblocks - 1), the others add 1,
 // so the top bit flips once every block has arrived and the low bits return to their
 // start.  Arrival is a release, the poll an acquire: stores made by any thread of an
 // arriving block before the barrier are visible to every thread after it.
-__device__ __forceinline__ void grid_barrier(unsigned int* bar, uint32_t* err) {
+// Block index within this instance's group of blocks (a launch may solve several
+// instances, each on its own contiguous range of blocks).
+__device__ __forceinline__ int gbid(const PoissonArgs& a) { return (int)blockIdx.x - a.blk0; }
+
+__device__ __forceinline__ void grid_barrier(const PoissonArgs& a) {
+  unsigned int* bar = a.bar;
+  uint32_t* err = a.errflags;
   __syncthreads();
   if (threadIdx.x == 0) {
-    const unsigned int inc = blockIdx.x == 0 ? (0x80000000u - (gridDim.x - 1)) : 1u;
+    const unsigned int inc = gbid(a) == 0 ? (0x80000000u - (unsigned int)(a.nblk - 1)) : 1u;
     unsigned int old, cur;
     asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(inc) : "memory");
     for (long long spin = 0;; ++spin) {
@@ -62,7 +68,7 @@ __device__ __forceinline__ void grid_barrier(unsigned int* bar, uint32_t* err) {
 
 // phase tracing (block 0, thread 0): time since the previous mark is added to trace[k]
 __device__ __forceinline__ void tmark(const PoissonArgs& a, int k) {
-  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (a.trace && gbid(a) == 0 && threadIdx.x == 0) {
     unsigned long long now;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
     unsigned long long last = a.trace[31];
@@ -90,9 +96,9 @@ __device__ __forceinline__ void put_partials(const PoissonArgs& a, int slot, dou
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
     if (threadIdx.x == 0) {
-      double* part = a.partials + (size_t)(slot & 3) * 2 * gridDim.x;
-      part[blockIdx.x] = s0;
-      part[gridDim.x + blockIdx.x] = s1;
+      double* part = a.partials + (size_t)(slot & 3) * 2 * a.nblk;
+      part[gbid(a)] = s0;
+      part[a.nblk + gbid(a)] = s1;
     }
   }
 }
@@ -101,11 +107,11 @@ __device__ __forceinline__ void put_partials(const PoissonArgs& a, int slot, dou
 __device__ __forceinline__ void get_sums(const PoissonArgs& a, int slot, double& t0, double& t1) {
   __shared__ double bc[2];
   if (threadIdx.x < 32) {
-    const double* part = a.partials + (size_t)(slot & 3) * 2 * gridDim.x;
+    const double* part = a.partials + (size_t)(slot & 3) * 2 * a.nblk;
     double s0 = 0.0, s1 = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += 32) {
+    for (int b = threadIdx.x; b < a.nblk; b += 32) {
       s0 += __ldcg(part + b);
-      s1 += __ldcg(part + gridDim.x + b);
+      s1 += __ldcg(part + a.nblk + b);
     }
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
@@ -558,51 +564,51 @@ __device__ void coarse_only(const PoissonArgs& a) {
 // z32 = M^{-1} r32 by one V(1,1) cycle; leaves the partial of (r, z) in `slot` and ends
 // with a barrier
 __device__ void vcycle(const PoissonArgs& a, const SLev* sl, const float* cinv, float* rc, int slot) {
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int tid = gbid(a) * blockDim.x + threadIdx.x, nth = a.nblk * blockDim.x;
   double rz = 0.0;
   if (a.nlevels == 1) {
-    if (blockIdx.x == 0) coarse_only(a);
-    grid_barrier(a.bar, a.errflags);
+    if (gbid(a) == 0) coarse_only(a);
+    grid_barrier(a);
     const int N = a.ny * a.nx;
     for (int i = tid; i < N; i += nth) rz += (double)(*(a.r32 + i)) * (double)(*(a.z32 + i));
     put_partials(a, slot, rz, 0.0);
-    grid_barrier(a.bar, a.errflags);
+    grid_barrier(a);
     return;
   }
   for (int l = 0; l < a.first_small - 1; ++l) {
     if (l == 0) down_leg<true>(a, 0, tid, nth);
     else down_leg<false>(a, l, tid, nth);
-    grid_barrier(a.bar, a.errflags);
+    grid_barrier(a);
     tmark(a, l < 7 ? l : 6);
   }
-  if (blockIdx.x == 0) small_cycle(a, sl, cinv, rc);
-  grid_barrier(a.bar, a.errflags);
+  if (gbid(a) == 0) small_cycle(a, sl, cinv, rc);
+  grid_barrier(a);
   tmark(a, 7);
   for (int l = a.first_small - 1; l >= 1; --l) {
     up_leg<false>(a, l, tid, nth);
-    grid_barrier(a.bar, a.errflags);
+    grid_barrier(a);
     tmark(a, 8 + (l < 7 ? l : 6));
   }
   rz = up_leg<true>(a, 0, tid, nth);
   put_partials(a, slot, rz, 0.0);
-  grid_barrier(a.bar, a.errflags);
+  grid_barrier(a);
   tmark(a, 8);
 }
 
 // ----------------------------------------------------------------- the persistent kernel
-__global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
+__device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   extern __shared__ float4 dyn_smem[];
   __shared__ SLev sl[MG_MAX_LEVELS];
   __shared__ float* s_rc;
   __shared__ float* s_cinv;
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+  const int tid = gbid(a) * blockDim.x + threadIdx.x, nth = a.nblk * blockDim.x;
   const int N = a.ny * a.nx;
   int slot = 0;
   double n_outer = 0, n_inner = 0, last_rel = 0;
   tmark(a, 20);
 
   // block 0: the small levels' vectors, transfer stencils and coarsest inverse in shared memory
-  if (blockIdx.x == 0 && a.nlevels > 1) {
+  if (gbid(a) == 0 && a.nlevels > 1) {
     if (threadIdx.x == 0) small_layout(a, reinterpret_cast<float*>(dyn_smem), sl, &s_cinv, &s_rc);
     __syncthreads();
     const int fs = a.first_small, last = a.nlevels - 1;
@@ -650,7 +656,7 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
       rr += res * res;
     }
     put_partials(a, slot, ff, rr);
-    grid_barrier(a.bar, a.errflags);
+    grid_barrier(a);
     double fnorm2, rnorm2;
     get_sums(a, slot++, fnorm2, rnorm2);
     tmark(a, 17);
@@ -681,7 +687,7 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
           pq_p += (double)p * (double)q;
         }
         put_partials(a, slot, pq_p, 0.0);
-        grid_barrier(a.bar, a.errflags);
+        grid_barrier(a);
         double pq;
         get_sums(a, slot++, pq, dummy);
         const double alpha = pq != 0.0 ? rz / pq : 0.0;
@@ -695,7 +701,7 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
           rr_p += (double)r * (double)r;
         }
         put_partials(a, slot, rr_p, 0.0);
-        grid_barrier(a.bar, a.errflags);
+        grid_barrier(a);
         double rrk;
         get_sums(a, slot++, rrk, dummy);
         tmark(a, 15);
@@ -707,7 +713,7 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
       // ---- FP64 correction and true residual
       for (int i = tid; i < N; i += nth)
         if (__ldg(a.cls + i) == NC_FREE) __stcg(a.x + i, (*(a.x + i)) + (double)(*(a.e32 + i)));
-      grid_barrier(a.bar, a.errflags);
+      grid_barrier(a);
       rr = 0.0;
       for (int i = tid; i < N; i += nth) {
         if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
@@ -717,7 +723,7 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
         rr += res * res;
       }
       put_partials(a, slot, rr, 0.0);
-      grid_barrier(a.bar, a.errflags);
+      grid_barrier(a);
       get_sums(a, slot++, rnorm2, dummy);
       tmark(a, 16);
     }
@@ -751,7 +757,7 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
       double Vi = (*(a.V + i));
       __stcg(a.V + i, DADD(DMUL(a.omega_keep, Vi), DMUL(a.omega_new, vn)));
     }
-    grid_barrier(a.bar, a.errflags);
+    grid_barrier(a);
     tmark(a, 18);
   }
 
@@ -780,6 +786,22 @@ __global__ void __launch_bounds__(PT, 1) k_poisson(PoissonArgs a) {
     a.stats[2] = last_rel;
     a.stats[3] += (double)a.iterations;
   }
+}
+
+// One instance on every block of the launch.
+__global__ void __launch_bounds__(PT, 1) k_poisson(const __grid_constant__ PoissonArgs a) { poisson_body(a); }
+
+// Several instances in one launch: block b solves instance blk_inst[b] together with the
+// other blocks of that instance's contiguous range (args[i].blk0, args[i].nblk).
+__global__ void __launch_bounds__(PT, 1) k_poisson_batch(const PoissonArgs* __restrict__ args,
+                                                         const int* __restrict__ blk_inst) {
+  __shared__ PoissonArgs sa;
+  const int inst = blk_inst[blockIdx.x];
+  const int* src = reinterpret_cast<const int*>(args + inst);
+  int* dst = reinterpret_cast<int*>(&sa);
+  for (int k = threadIdx.x; k < (int)(sizeof(PoissonArgs) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+  __syncthreads();
+  poisson_body(sa);
 }
 
 }  // namespace pb

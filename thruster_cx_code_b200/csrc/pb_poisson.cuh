@@ -55,8 +55,9 @@ struct PoissonArgs {
   const int* cidx;        // coarsest active node indices
   const float* cinvT;     // coarsest inverse, transposed (nc x nc)
   int cinv_smem;          // block 0 stages cinvT in shared memory
-  // reductions and barrier
-  double* partials;       // 4 slots x 2 values x gridDim doubles
+  // this instance's blocks in the launch and its reductions and barrier
+  int blk0, nblk;         // first block and number of blocks
+  double* partials;       // 4 slots x 2 values x nblk doubles
   unsigned int* bar;      // barrier word (any start value)
   uint32_t* errflags;
   double* stats;          // [outer its, inner its, final rel residual, solves] accumulated

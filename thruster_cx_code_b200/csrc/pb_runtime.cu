@@ -331,6 +331,7 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
     a.lev[l].U = D.U;
   }
   a.nc = s->nc; a.cidx = s->cidx; a.cinvT = s->cinvT; a.cinv_smem = s->cinv_smem;
+  a.blk0 = 0; a.nblk = s->pgrid;
   a.partials = s->partials; a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
   a.stats = s->pstats;
@@ -467,7 +468,9 @@ static void mark(Sim* s) {
   cudaEventRecord(s->marks[s->mark_used++], s->stream);
 }
 
-static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
+// A step is enqueued in two halves around the field solve, so that a batch can solve the
+// fields of several instances in one launch between them.
+static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
   Sim* s = &h->s;
   mark(s);
   cudaStream_t st = s->stream;
@@ -546,8 +549,25 @@ static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
   k_rho_finalize<<<grid_for(s, N, 256), 256, 0, st>>>(s->rho, s->cnt_i, s->cnt_e, N, p->charge_density, 0);
   ++s->launches;
   mark(s);
-  if (p->do_poisson && (rc = launch_poisson(s, p->picard_iters, p))) return rc;
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
+  Sim* s = &h->s;
   mark(s);
+  cudaStream_t st = s->stream;
+  const int N = s->ny * s->nx;
+  Species& I = s->sp[0];
+  Species& E = s->sp[1];
+  const float dxf = (float)p->dx, dyf = (float)p->dy;
+  int* ni_src = s->counts + I.cur;
+  int* ni_dst = s->counts + (1 - I.cur);
+  int* ne_src = s->counts + 2 + E.cur;
+  int* ne_dst = s->counts + 2 + (1 - E.cur);
+  pb_step_report* rep = s->rep_dev;
+  uint32_t* ef = &rep->errflags;
+  int32_t rc;
 
   // C. sub-step counts (:1177-1209)
   const float dtf = (float)p->dt;
@@ -668,6 +688,13 @@ static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
   mark(s);
   CK(cudaGetLastError());
   return PB_OK;
+}
+
+static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
+  int32_t rc;
+  if ((rc = enqueue_step_pre(h, p))) return rc;
+  if (p->do_poisson && (rc = launch_poisson(&h->s, p->picard_iters, p))) return rc;
+  return enqueue_step_post(h, p);
 }
 
 static int32_t finish_report(Sim* s, pb_step_report* out) {
@@ -1274,3 +1301,5 @@ float pb_host_percentile95(const float* sorted, int32_t n) {
 }
 
 }  // extern "C"
+
+#include "pb_batch.cu"

@@ -235,6 +235,12 @@ class DigitalTwinSimulator:
                                                    _ptr(cex), _ptr(ids)), "get_particles")
         return [x, y, vx, vy, vz, (cex.astype(bool) if cex is not None else None), ids]
 
+    def device_bytes(self):
+        """Device memory held by this simulator (bytes, from its capacities)."""
+        b = C.c_int64()
+        _lib.check(self._libh.pb_sim_memory(self._h, C.byref(b)), "pb_sim_memory")
+        return int(b.value)
+
     def close(self):
         h = self.__dict__.get("_h")
         if h is not None and h.value:

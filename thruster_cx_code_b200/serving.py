@@ -1,0 +1,250 @@
+"""Batched and served execution of many aperture simulations on one GPU.
+
+The reference runs a sweep (perveance, backstreaming limit) as one process per sweep point.
+Each process builds a DigitalTwinSimulator, steps it until the beamlet divergence or the
+saddle potential settles, and reports (Python/benchmarks/benchmark_perveance.py:17-67,
+78-164; Python/benchmarks/benchmark_ebs.py:8-49).  Here the sweep points share one GPU:
+
+* ``SweepBatch.run(sims, K)`` advances a set of simulators K steps together through
+  ``pb_batch_run``.  Each instance's particle kernels run on its own stream, and the field
+  solves due in a step run as one launch.
+* ``Convergence`` is the retirement test: the relative change of the window means of the
+  beamlet current, theta95 and the saddle potential, between the two halves of the last
+  ``window`` steps.
+* ``SweepServer`` does continuous batching.  Requests arrive over time and are admitted as
+  soon as the device-memory budget and the instance cap allow.  The active instances advance
+  together in chunks of steps, and an instance retires once it converges or reaches its step
+  limit.  Its time-to-converged (retirement minus arrival, wall clock) is recorded.
+"""
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib
+
+
+class SweepBatch:
+    """Several DigitalTwinSimulator instances stepped together on one device."""
+
+    def __init__(self, device=0):
+        self._libh = _lib.load()
+        h = C.c_void_p()
+        _lib.check(self._libh.pb_batch_create(C.byref(h), int(device)), "pb_batch_create")
+        self._h = h
+        self.device = int(device)
+        self.last_ms = 0.0
+        self.last_launches = 0
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            self._libh.pb_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, sims, params_list, K):
+        """Advance ``sims[i]`` by ``K`` steps with the step parameters of ``params_list[i]``
+        (a config dict, as for ``step``).  Returns, per instance, the list of the K pairs
+        (``step`` result ``(remeshed, min_pot, current_div, T_grids, trans_last_frame)``,
+        step report)."""
+        n = len(sims)
+        if n == 0:
+            return []
+        P = (_lib.StepParams * (n * K))()
+        for i, (s, prm) in enumerate(zip(sims, params_list)):
+            s._flush()
+            s._upload_user_cs()
+            it0 = s.iteration
+            for k in range(K):
+                s.iteration = it0 + k
+                P[i * K + k] = s.step_params(prm)
+            s.iteration = it0
+        R = (_lib.StepReport * (n * K))()
+        arr = (C.c_void_p * n)(*[s._h.value for s in sims])
+        _lib.check(self._libh.pb_batch_run(self._h, arr, n, P, int(K), R), "pb_batch_run")
+        t = (C.c_double * 2)()
+        self._libh.pb_batch_timing(self._h, t)
+        self.last_ms, self.last_launches = float(t[0]), int(t[1])
+        out = []
+        for i, (s, prm) in enumerate(zip(sims, params_list)):
+            res = []
+            s._invalidate()
+            for k in range(K):
+                s.iteration += 1
+                rep = _lib.StepReport()
+                C.memmove(C.byref(rep), C.byref(R[i * K + k]), C.sizeof(rep))
+                res.append((s._apply_report(rep, prm), rep))
+            out.append(res)
+        return out
+
+
+def pushes_of(reports, n_p0, n_e0):
+    """Particle pushes of consecutive steps of one instance, from its reports and the
+    particle counts before the first step."""
+    tot = 0
+    np_prev, ne_prev = n_p0, n_e0
+    for r in reports:
+        tot += (np_prev + r.injected) * r.n_sub_ion + (ne_prev + r.rf_injected + r.neut_injected) * r.n_sub_e
+        np_prev, ne_prev = r.num_p, r.num_e
+    return tot
+
+
+def beamlet_current(sim, rep):
+    """Ions crossing the exit plane in one step as a current (A): crossed * q * w / dt."""
+    return float(rep.crossed) * sim.q_ion * sim.macro_weight / sim.dt
+
+
+class Convergence:
+    """Relative change of window means between the halves of the last ``window`` steps,
+    for each tracked quantity; converged when every change is below ``tol`` and at least
+    ``min_steps`` steps have run.  Quantities that are NaN in a window (theta95 with five
+    or fewer crossings) count as not converged."""
+
+    def __init__(self, window=500, tol=5e-3, min_steps=None, keys=("current", "theta95", "saddle")):
+        self.window = int(window)
+        self.tol = float(tol)
+        self.min_steps = int(min_steps if min_steps is not None else window)
+        self.keys = tuple(keys)
+        self.hist = {k: [] for k in self.keys}
+        self.steps = 0
+
+    def add(self, **vals):
+        for k in self.keys:
+            self.hist[k].append(float(vals[k]))
+        self.steps += 1
+
+    def changes(self):
+        h = self.window // 2
+        out = {}
+        for k in self.keys:
+            v = self.hist[k]
+            if len(v) < 2 * h or h == 0:
+                out[k] = math.inf
+                continue
+            a = np.asarray(v[-2 * h:-h], np.float64)
+            b = np.asarray(v[-h:], np.float64)
+            if not (np.all(np.isfinite(a)) and np.all(np.isfinite(b))):
+                out[k] = math.inf
+                continue
+            ma, mb = a.mean(), b.mean()
+            scale = max(abs(ma), abs(mb))
+            out[k] = abs(mb - ma) / scale if scale > 0 else 0.0
+        return out
+
+    def converged(self):
+        if self.steps < self.min_steps:
+            return False
+        return all(c < self.tol for c in self.changes().values())
+
+
+class Request:
+    """One sweep point: ``make()`` builds and returns (sim, params) on the device."""
+
+    def __init__(self, rid, make, est_bytes, max_steps, convergence):
+        self.rid = rid
+        self.make = make
+        self.est_bytes = int(est_bytes)
+        self.max_steps = int(max_steps)
+        self.conv = convergence
+        self.sim = None
+        self.params = None
+        self.t_arrival = None
+        self.t_admit = None
+        self.t_done = None
+        self.steps = 0
+        self.converged = False
+        self.last = {}
+
+
+class SweepServer:
+    """Continuous batching of sweep points on one GPU under a device-memory budget."""
+
+    def __init__(self, device=0, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=None):
+        self.batch = batch if batch is not None else SweepBatch(device)
+        self.budget = float(hbm_budget_bytes)
+        self.max_active = int(max_active)
+        self.chunk = int(chunk)
+        self.active = []
+        self.done = []
+        self.pushes = 0
+        self.gpu_ms = 0.0
+
+    def _in_use(self):
+        return sum(r.mem for r in self.active)
+
+    def _admit(self, req, now):
+        req.sim, req.params = req.make()
+        req.t_admit = now
+        req.mem = max(int(req.sim.device_bytes()), req.est_bytes)
+        self.active.append(req)
+
+    def _retire(self, req, now):
+        req.t_done = now
+        req.sim.close()
+        req.sim = None
+        self.active.remove(req)
+        self.done.append(req)
+
+    def serve(self, arrivals, clock=time.perf_counter, idle_sleep=1e-3):
+        """``arrivals``: list of (arrival time in s from the start, Request), any order.
+        Runs until every request has retired; returns the retired requests in order."""
+        pending = sorted(arrivals, key=lambda a: a[0])
+        t0 = clock()
+        qi = 0
+        waiting = []
+        while qi < len(pending) or waiting or self.active:
+            now = clock() - t0
+            while qi < len(pending) and pending[qi][0] <= now:
+                pending[qi][1].t_arrival = pending[qi][0]
+                waiting.append(pending[qi][1])
+                qi += 1
+            # admission: first come, first served, while memory and slots allow
+            while waiting and len(self.active) < self.max_active and \
+                    self._in_use() + waiting[0].est_bytes <= self.budget:
+                self._admit(waiting.pop(0), clock() - t0)
+            if not self.active:
+                if waiting:
+                    raise RuntimeError(f"request {waiting[0].rid} needs {waiting[0].est_bytes} bytes, "
+                                       f"more than the {self.budget:.0f}-byte budget")
+                if qi < len(pending):
+                    time.sleep(max(0.0, min(pending[qi][0] - now, 0.05)) or idle_sleep)
+                continue
+            k = min(self.chunk, min(r.max_steps - r.steps for r in self.active))
+            k = max(k, 1)
+            sims = [r.sim for r in self.active]
+            n0 = [(s.num_p, s.num_e) for s in sims]
+            results = self.batch.run(sims, [r.params for r in self.active], k)
+            self.gpu_ms += self.batch.last_ms
+            for r, res, (np0, ne0) in zip(list(self.active), results, n0):
+                s = r.sim
+                self.pushes += pushes_of([rep for _, rep in res], np0, ne0)
+                for (_, min_pot, div, _, _), rep in res:
+                    r.conv.add(current=beamlet_current(s, rep), theta95=div, saddle=min_pot)
+                r.steps += k
+                (_, min_pot, div, _, _), rep = res[-1]
+                r.last = {"current": beamlet_current(s, rep), "theta95": float(div), "saddle": float(min_pot)}
+                if r.conv.converged() or r.steps >= r.max_steps:
+                    r.converged = r.conv.converged()
+                    self._retire(r, clock() - t0)
+        return self.done
+
+    def stats(self):
+        lat = np.array([r.t_done - r.t_arrival for r in self.done], np.float64)
+        if lat.size == 0:
+            return {}
+        span = max(r.t_done for r in self.done) - min(r.t_arrival for r in self.done)
+        return {"completed": int(lat.size), "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "throughput_per_hr": lat.size / span * 3600.0,
+                "converged": int(sum(r.converged for r in self.done))}
+
+    def close(self):
+        for r in list(self.active):
+            r.sim.close()
+        self.active = []
+        self.batch.close()

@@ -10,6 +10,11 @@ thick, 6.25 um spacing chosen so the derived domain is exactly 257 x 1025 nodes
 
 Particles are pre-loaded from a seeded NumPy generator: positions uniform over the
 non-electrode cells, ion velocities N(v_Bohm, v_th), electron velocities thermal.
+
+Sweep points (batched and served runs): the 2-grid stack with screen voltage uniform in
+600-1800 V, accel voltage uniform in -300..-100 V, plasma density log-uniform in
+3e16-3e17 m^-3, node spacing drawn from three resolutions (about 64 x 256, 128 x 512 and
+256 x 1024 cells; dt scales with the spacing) and a log-uniform macro-particle count.
 """
 import numpy as np
 
@@ -98,3 +103,49 @@ def thermal_speeds(sim, params):
     v_th_i = float(np.sqrt(sim.q_ion * Ti / sim.m_ion))
     v_th_e = float(np.sqrt(sim.q * params.get("Te", 5.0) / sim.m_e))
     return v_bohm, v_th_i, v_th_e
+
+
+SWEEP_SPACINGS = {"64x256": 0.025, "128x512": 0.0125, "256x1024": 0.00625}
+
+
+def sweep_point(rng, index, grids=("64x256", "128x512", "256x1024"), n_range=(2e5, 4e6)):
+    """One randomly drawn sweep point (a dict; ``make_sweep_sim`` builds it)."""
+    grid = grids[int(rng.integers(len(grids)))]
+    dx = SWEEP_SPACINGS[grid]
+    lo, hi = np.log(n_range[0]), np.log(n_range[1])
+    n = int(np.exp(rng.uniform(lo, hi)))
+    return dict(index=int(index), grid=grid, dx=dx, dt=1e-10 * dx / 0.025, m_e_ratio=100.0,
+                n_ions=int(0.75 * n), n_e=n - int(0.75 * n), seed=1000 + int(index),
+                params=dict(grids=[dict(V=float(rng.uniform(600.0, 1800.0)), t=0.38, gap=1.0, r=0.95, cham=0.0),
+                                   dict(V=float(rng.uniform(-300.0, -100.0)), t=1.0, gap=1.0, r=0.55, cham=0.0)],
+                            pitch_mm=3.75, Te_up=5.0, n0_plasma=float(np.exp(rng.uniform(np.log(3e16), np.log(3e17)))),
+                            Ti=0.1, Tn=300.0, n0=1e18, sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9))
+
+
+def sweep_point_bytes(spec):
+    """Device-memory estimate of a sweep point before it is built (for admission): two
+    buffers of 25 B per ion and 24 B per electron with 25% headroom, plus about 800 B per
+    grid node for fields, multigrid and sort scratch."""
+    Lx_mm = 0.4 + sum(g["t"] + g["gap"] for g in spec["params"]["grids"]) + 3.0
+    Ly_mm = 0.5 * spec["params"]["grids"][0]["r"] + 0.3 * spec["params"]["pitch_mm"]
+    nodes = (Lx_mm / spec["dx"] + 1) * (Ly_mm / spec["dx"] + 1)
+    return int(2 * 1.25 * (25 * spec["n_ions"] + 24 * spec["n_e"]) + 800 * nodes + (64 << 20))
+
+
+def make_sweep_sim(spec, device=0, sort_every=20):
+    """Build a sweep point on the device: returns (simulator, params)."""
+    from .physics_engine import DigitalTwinSimulator
+    sim = DigitalTwinSimulator(device=device, seed=spec["seed"], sort_every=sort_every)
+    sim.dx = sim.dy = spec["dx"]
+    sim.dt = spec["dt"]
+    sim.m_ion = M_XE
+    sim.m_e = M_XE / spec["m_e_ratio"]
+    params = dict(spec["params"])
+    sim.build_domain(params)
+    v_b, v_ti, v_te = thermal_speeds(sim, params)
+    ions, eles = preload(sim.isBound, sim.dx, sim.dy, sim.Lx, sim.Ly, spec["n_ions"], spec["n_e"], v_b, 4 * v_ti,
+                         v_te, seed=spec["seed"], x_max_ions=plume_boundary(sim, params))
+    sim.set_particles("ions", *ions)
+    sim.set_particles("electrons", *eles)
+    return sim, params
+
