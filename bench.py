@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true")
     return ap.parse_args()
 
 
@@ -255,6 +256,9 @@ def gpu_arm(args):
                        "parallelism": f"replicas x{world}", "l2": "particle state 8M x 25 B x 2 > L2 (126 MB)",
                        "sort_every": 20, "picard": "5 solves every 2nd step, FP32 MG-PCG + FP64 refinement"},
             "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": int(tm[8])}
+    if rank == 0 and world == 1 and not args.no_sweep:
+        sim.close()
+        line["sweep"] = sweep_section(local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(args.workload)
     if world > 1:
@@ -264,6 +268,94 @@ def gpu_arm(args):
     sim.close()
     if rank == 0:
         print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------- sweeps
+SWEEP_POINTS, SWEEP_WARMUP, SWEEP_STEPS, SWEEP_REF_STEPS = 16, 2, 40, 3000
+SERVE_REQUESTS, SERVE_RATE_HZ, SERVE_MAX_STEPS = 12, 20.0, 100
+
+
+def _run_plain(sim, params, K):
+    """K steps of one simulator through pb_sim_run; returns the device time (ms)."""
+    import ctypes as C
+    from thruster_cx_code_b200 import _lib
+    lib = _lib.load()
+    it0 = sim.iteration
+    plist = []
+    for k in range(K):
+        sim.iteration = it0 + k
+        plist.append(sim.step_params(params))
+    sim.iteration = it0
+    P = (_lib.StepParams * K)(*plist)
+    R = (_lib.StepReport * K)()
+    _lib.check(lib.pb_sim_run(sim._h, P, K, R), "pb_sim_run")
+    tm = (C.c_double * 9)()
+    lib.pb_sim_timing(sim._h, tm)
+    sim.iteration = it0 + K
+    sim._invalidate()
+    for r in R:
+        sim._apply_report(r, params)
+    return float(tm[0])
+
+
+def sweep_section(device):
+    """Sweep points per hour, plain (one instance at a time through pb_sim_run) against
+    batched (all points together through pb_batch_run), on two identical sets of 16
+    perveance-sweep points (C3 draws, 0.2M-1M macro-particles).  Rates use the device time
+    of 40 steps after 2 warm-up steps, scaled to 3000 steps per point; setup is not
+    included.  Then a served run: 12 backstreaming-limit requests arriving as a Poisson
+    stream at 20 per second, admitted under a 150 GB budget, stepped in chunks of 10 and
+    retired when the saddle potential and current change less than 5% between the halves
+    of a 60-step window (or at 100 steps).  Its latencies include setup."""
+    from thruster_cx_code_b200 import serving as SV
+    from thruster_cx_code_b200 import workloads as W
+    rng = np.random.default_rng(7)
+    specs = [W.sweep_point(rng, i, n_range=(2e5, 1e6)) for i in range(SWEEP_POINTS)]
+    batch = SV.SweepBatch(device)
+    plain = [W.make_sweep_sim(sp, device) for sp in specs]
+    for s, p in plain:
+        _run_plain(s, p, SWEEP_WARMUP)
+    plain_ms = sum(_run_plain(s, p, SWEEP_STEPS) for s, p in plain)
+    for s, _ in plain:
+        s.close()
+    together = [W.make_sweep_sim(sp, device) for sp in specs]
+    sims, prm = [s for s, _ in together], [p for _, p in together]
+    batch.run(sims, prm, SWEEP_WARMUP)
+    batch.run(sims, prm, SWEEP_STEPS)
+    batched_ms = batch.last_ms
+    for s in sims:
+        s.close()
+    per_point_plain_s = plain_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / SWEEP_POINTS
+    per_point_batched_s = batched_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / SWEEP_POINTS
+    out = {"points": SWEEP_POINTS, "steps_timed": SWEEP_STEPS, "steps_per_point": SWEEP_REF_STEPS,
+           "grids": sorted({sp["grid"] for sp in specs}),
+           "plain_points_per_hr": 3600.0 / per_point_plain_s,
+           "batched_points_per_hr": 3600.0 / per_point_batched_s,
+           "batched_over_plain": plain_ms / batched_ms,
+           "setup": "excluded (host geometry, multigrid build and pre-load)"}
+    # ---- served
+    rs = np.random.default_rng(11)
+    arrivals = []
+    t = 0.0
+    for i in range(SERVE_REQUESTS):
+        t += rs.exponential(1.0 / SERVE_RATE_HZ)
+        sp = W.sweep_point(rs, 100 + i, grids=("64x256", "128x512"), n_range=(2e5, 8e5))
+        sp["params"]["grids"][1]["V"] = float(rs.uniform(-300.0, -50.0))
+        sp["params"]["Te"] = 2.0
+        j = rs.uniform(0.1, 1.0)  # neutralizer electron current density, A/m^2
+        area = 0.5 * 0.95e-3 * 1e-3 + 0.3 * 3.75e-3 * 1e-3
+        sp["params"]["neut_rate"] = max(1, int(round(j * area * sp["dt"] / (1.602e-19 * 1e3))))
+        req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device)), W.sweep_point_bytes(sp), SERVE_MAX_STEPS,
+                         SV.Convergence(window=60, tol=0.05, keys=("current", "saddle")))
+        arrivals.append((t, req))
+    srv = SV.SweepServer(device, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=batch)
+    srv.serve(arrivals)
+    st = srv.stats()
+    st.update({"requests": SERVE_REQUESTS, "arrival_rate_hz": SERVE_RATE_HZ, "max_steps": SERVE_MAX_STEPS,
+               "particle_pushes": srv.pushes, "gpu_ms": srv.gpu_ms})
+    out["served"] = st
+    srv.close()
+    return out
 
 
 # ----------------------------------------------------------------------------- CPU oracle

@@ -260,7 +260,11 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       const PoissonArgs* da = b->dargs + L.args_off;
       const int* db = b->dblk + L.blk_off;
       void* kargs[] = {(void*)&da, (void*)&db};
-      CK(cudaLaunchCooperativeKernel((void*)k_poisson_batch, dim3(L.nblocks), dim3(PT), kargs, L.smem, b->stream));
+      if ((rc = coop_launch(b->device, b->stream, [&]() {
+             return cudaLaunchCooperativeKernel((void*)k_poisson_batch, dim3(L.nblocks), dim3(PT), kargs, L.smem,
+                                                b->stream);
+           })))
+        return rc;
       ++b->launches;
       CK(cudaEventRecord(b->ev_solve[li], b->stream));
     }

@@ -339,12 +339,36 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
   return a;
 }
 
+// Cooperative launches on one device are chained in enqueue order: each waits for the
+// previous one (whatever stream it was on), so two field-solve kernels, each of which
+// needs all of its blocks resident at once, never compete for the SMs.
+struct CoopChain {
+  std::mutex mu;
+  cudaEvent_t last = nullptr;
+};
+static CoopChain g_coop[64];
+
+template <class Launch>
+static int32_t coop_launch(int device, cudaStream_t st, Launch launch) {
+  if (device < 0 || device >= 64) return fail(PB_ERR_ARG, "device ordinal out of range");
+  CoopChain& c = g_coop[device];
+  std::lock_guard<std::mutex> lk(c.mu);
+  if (!c.last) CK(cudaEventCreateWithFlags(&c.last, cudaEventDisableTiming));
+  CK(cudaStreamWaitEvent(st, c.last, 0));
+  CK(launch());
+  CK(cudaEventRecord(c.last, st));
+  return PB_OK;
+}
+
 static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
   if (iterations <= 0) return PB_OK;
   PoissonArgs a = poisson_args(s, iterations, p);
   CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), s->stream));
   void* args[] = {&a};
-  CK(cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream));
+  int32_t rc = coop_launch(s->device, s->stream, [&]() {
+    return cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream);
+  });
+  if (rc) return rc;
   ++s->launches;
   return PB_OK;
 }

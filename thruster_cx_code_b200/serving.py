@@ -12,13 +12,16 @@ saddle potential settles, and reports (Python/benchmarks/benchmark_perveance.py:
   beamlet current, theta95 and the saddle potential, between the two halves of the last
   ``window`` steps.
 * ``SweepServer`` does continuous batching.  Requests arrive over time and are admitted as
-  soon as the device-memory budget and the instance cap allow.  The active instances advance
-  together in chunks of steps, and an instance retires once it converges or reaches its step
-  limit.  Its time-to-converged (retirement minus arrival, wall clock) is recorded.
+  soon as the device-memory budget and the instance cap allow.  An admitted request is built
+  (geometry, multigrid, pre-load, upload) on a worker thread while the GPU keeps stepping
+  the active ones.  The active instances advance together in chunks of steps, and an
+  instance retires once it converges or reaches its step limit.  Its time-to-converged
+  (retirement minus arrival, wall clock) is recorded.
 """
 import ctypes as C
 import math
 import time
+from concurrent.futures import ThreadPoolExecutor, wait, FIRST_COMPLETED
 
 import numpy as np
 
@@ -165,21 +168,24 @@ class Request:
 class SweepServer:
     """Continuous batching of sweep points on one GPU under a device-memory budget."""
 
-    def __init__(self, device=0, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=None):
+    def __init__(self, device=0, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=None, setup_workers=2):
         self.batch = batch if batch is not None else SweepBatch(device)
         self.budget = float(hbm_budget_bytes)
         self.max_active = int(max_active)
         self.chunk = int(chunk)
+        self.setup_workers = int(setup_workers)
         self.active = []
+        self.preparing = {}  # future -> request
         self.done = []
         self.pushes = 0
         self.gpu_ms = 0.0
 
     def _in_use(self):
-        return sum(r.mem for r in self.active)
+        return sum(r.mem for r in self.active) + sum(r.est_bytes for r in self.preparing.values())
 
-    def _admit(self, req, now):
-        req.sim, req.params = req.make()
+    def _ready(self, fut, now):
+        req = self.preparing.pop(fut)
+        req.sim, req.params = fut.result()
         req.t_admit = now
         req.mem = max(int(req.sim.device_bytes()), req.est_bytes)
         self.active.append(req)
@@ -191,47 +197,52 @@ class SweepServer:
         self.active.remove(req)
         self.done.append(req)
 
-    def serve(self, arrivals, clock=time.perf_counter, idle_sleep=1e-3):
+    def serve(self, arrivals, clock=time.perf_counter):
         """``arrivals``: list of (arrival time in s from the start, Request), any order.
         Runs until every request has retired; returns the retired requests in order."""
         pending = sorted(arrivals, key=lambda a: a[0])
         t0 = clock()
         qi = 0
         waiting = []
-        while qi < len(pending) or waiting or self.active:
-            now = clock() - t0
-            while qi < len(pending) and pending[qi][0] <= now:
-                pending[qi][1].t_arrival = pending[qi][0]
-                waiting.append(pending[qi][1])
-                qi += 1
-            # admission: first come, first served, while memory and slots allow
-            while waiting and len(self.active) < self.max_active and \
-                    self._in_use() + waiting[0].est_bytes <= self.budget:
-                self._admit(waiting.pop(0), clock() - t0)
-            if not self.active:
-                if waiting:
+        with ThreadPoolExecutor(max_workers=max(1, self.setup_workers)) as pool:
+            while qi < len(pending) or waiting or self.preparing or self.active:
+                now = clock() - t0
+                while qi < len(pending) and pending[qi][0] <= now:
+                    pending[qi][1].t_arrival = pending[qi][0]
+                    waiting.append(pending[qi][1])
+                    qi += 1
+                # admission: first come, first served, while memory and slots allow
+                while waiting and len(self.active) + len(self.preparing) < self.max_active and \
+                        self._in_use() + waiting[0].est_bytes <= self.budget:
+                    req = waiting.pop(0)
+                    self.preparing[pool.submit(req.make)] = req
+                if waiting and not self.active and not self.preparing:
                     raise RuntimeError(f"request {waiting[0].rid} needs {waiting[0].est_bytes} bytes, "
                                        f"more than the {self.budget:.0f}-byte budget")
-                if qi < len(pending):
-                    time.sleep(max(0.0, min(pending[qi][0] - now, 0.05)) or idle_sleep)
-                continue
-            k = min(self.chunk, min(r.max_steps - r.steps for r in self.active))
-            k = max(k, 1)
-            sims = [r.sim for r in self.active]
-            n0 = [(s.num_p, s.num_e) for s in sims]
-            results = self.batch.run(sims, [r.params for r in self.active], k)
-            self.gpu_ms += self.batch.last_ms
-            for r, res, (np0, ne0) in zip(list(self.active), results, n0):
-                s = r.sim
-                self.pushes += pushes_of([rep for _, rep in res], np0, ne0)
-                for (_, min_pot, div, _, _), rep in res:
-                    r.conv.add(current=beamlet_current(s, rep), theta95=div, saddle=min_pot)
-                r.steps += k
-                (_, min_pot, div, _, _), rep = res[-1]
-                r.last = {"current": beamlet_current(s, rep), "theta95": float(div), "saddle": float(min_pot)}
-                if r.conv.converged() or r.steps >= r.max_steps:
-                    r.converged = r.conv.converged()
-                    self._retire(r, clock() - t0)
+                for fut in [f for f in self.preparing if f.done()]:
+                    self._ready(fut, clock() - t0)
+                if not self.active:
+                    if self.preparing:
+                        wait(list(self.preparing), timeout=0.05, return_when=FIRST_COMPLETED)
+                    elif qi < len(pending):
+                        time.sleep(max(0.0, min(pending[qi][0] - (clock() - t0), 0.05)))
+                    continue
+                k = max(1, min(self.chunk, min(r.max_steps - r.steps for r in self.active)))
+                sims = [r.sim for r in self.active]
+                n0 = [(s.num_p, s.num_e) for s in sims]
+                results = self.batch.run(sims, [r.params for r in self.active], k)
+                self.gpu_ms += self.batch.last_ms
+                for r, res, (np0, ne0) in zip(list(self.active), results, n0):
+                    s = r.sim
+                    self.pushes += pushes_of([rep for _, rep in res], np0, ne0)
+                    for (_, min_pot, div, _, _), rep in res:
+                        r.conv.add(current=beamlet_current(s, rep), theta95=div, saddle=min_pot)
+                    r.steps += k
+                    (_, min_pot, div, _, _), rep = res[-1]
+                    r.last = {"current": beamlet_current(s, rep), "theta95": float(div), "saddle": float(min_pot)}
+                    if r.conv.converged() or r.steps >= r.max_steps:
+                        r.converged = r.conv.converged()
+                        self._retire(r, clock() - t0)
         return self.done
 
     def stats(self):
