@@ -105,6 +105,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def reduce_over_ranks(t, pushes, device):
+    """(max over ranks of the time t, sum over ranks of the pushes), every rank the same."""
+    import torch
+    import torch.distributed as dist
+    a = torch.tensor([float(t)], device=device, dtype=torch.float64)
+    dist.all_reduce(a, op=dist.ReduceOp.MAX)
+    b = torch.tensor([float(pushes)], device=device, dtype=torch.float64)
+    dist.all_reduce(b, op=dist.ReduceOp.SUM)
+    return float(a.item()), float(b.item())
+
+
 def measured_peak_gbs():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -198,12 +209,7 @@ def gpu_arm(args):
     ions_per_launch = float(np.mean([n_p0 if k == 0 else R[k - 1].num_p for k in range(K)]) +
                         np.mean([r.injected for r in R]))
     if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
-        pt = torch.tensor([float(pushes)], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(pt, op=torch.distributed.ReduceOp.SUM)
-        pushes_all = float(pt.item())
+        ms_max, pushes_all = reduce_over_ranks(ms, pushes, "cuda")
     else:
         ms_max, pushes_all = ms, float(pushes)
     value = pushes_all / (ms_max * 1e-3)
@@ -229,12 +235,7 @@ def gpu_arm(args):
         wall = time.perf_counter() - t0
         pe2e = pushes_of(reps, n_p1, n_e1)
         if world > 1:
-            t = torch.tensor([wall], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            wall = float(t.item())
-            pt = torch.tensor([float(pe2e)], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(pt, op=torch.distributed.ReduceOp.SUM)
-            pe2e = float(pt.item())
+            wall, pe2e = reduce_over_ranks(wall, pe2e, "cuda")
         e2e = {"value": pe2e / wall, "unit": "particle-pushes/s", "h2d_bytes_per_step": C.sizeof(_lib.StepParams),
                "d2h_bytes_per_step": C.sizeof(_lib.StepReport), "same_steps_as_value": pe2e == pushes_all}
     peak, peak_kind = measured_peak_gbs()
