@@ -369,7 +369,7 @@ class DigitalTwinSimulator:
         """``physics_engine.py:506-522``."""
         self._add_particles(1, x, y, vx, vy, vz)
 
-    def set_particles(self, species, x, y, vx, vy, vz, is_cex=None, ids=None, sort=None):
+    def set_particles(self, species, x, y, vx, vy, vz, is_cex=None, ids=None, sort=None, next_id=None):
         """Replace a species wholesale (species 'ions' or 'electrons').  With ``sort``
         (default: when cell sorting is on and a domain exists) the uploaded particles are
         re-ordered by cell at once, so the first steps already gather from local cells."""
@@ -381,6 +381,8 @@ class DigitalTwinSimulator:
         if sp == 0:
             cex = np.ascontiguousarray(np.zeros(n, bool) if is_cex is None else is_cex, dtype=np.uint8)
         nxt = int(ids.max()) + 1 if n else 0
+        if next_id is not None:
+            nxt = max(nxt, int(next_id))
         _lib.check(self._libh.pb_sim_set_particles(self._h, sp, n, *[_ptr(a) for a in arrs], _ptr(cex), _ptr(ids),
                                                    nxt), "set_particles")
         if sp == 0:
@@ -392,6 +394,88 @@ class DigitalTwinSimulator:
         if sort and n > 0:
             _lib.check(self._libh.pb_sim_sort(self._h, sp, float(self.dx), float(self.dy)), "sort")
         self._invalidate()
+
+    # ------------------------------------------------------------------ checkpoints
+    _CKPT_FIELDS = ("V", "Ex", "Ey", "Tmap", "damage_map", "isBound", "V_fixed", "eroded_depth", "accum_ppc_map")
+    _CKPT_SCALARS = ("iteration", "seed", "sort_every", "dx", "dy", "dt", "m_ion", "m_XE", "q_ion", "Z_ion", "m_e",
+                     "macro_weight", "thermal_accel", "injected_ions", "transmitted_ions", "entered_optics",
+                     "next_ion_id", "next_e_id", "ppc_steps_count", "max_p", "max_e")
+
+    def save_checkpoint(self, path, params):
+        """Write the simulator state to ``path`` (.npz): particles in their current order
+        with ids, every field the step reads or accumulates, the previous linear solution
+        (the field solve's warm start), counters, the material and its cell constants, the
+        cross-section tables and the config ``params``.  ``load_checkpoint`` continues the
+        run bit-for-bit."""
+        import json
+        self._flush()
+        n, ne = self.num_p, self.num_e
+        arrays = {}
+        for k in ("x", "y", "vx", "vy", "vz", "isCEX", "id"):
+            arrays["p_" + k] = np.array(getattr(self, "p_" + k)[:n])
+        for k in ("x", "y", "vx", "vy", "vz", "id"):
+            arrays["e_" + k] = np.array(getattr(self, "e_" + k)[:ne])
+        for k in self._CKPT_FIELDS:
+            arrays[k] = np.array(getattr(self, k))
+        vnew = np.empty((self.ny, self.nx), np.float64)
+        _lib.check(self._libh.pb_sim_get_field(self._h, 11, _ptr(vnew), vnew.nbytes), "get_field")
+        arrays["Vnew"] = vnew
+        for label, ds in self.user_cs.items():
+            arrays["cs_" + label] = np.stack([np.asarray(ds["energy"], np.float64), np.asarray(ds["cs"], np.float64)])
+        meta = {k: (int(v) if isinstance(v, (int, np.integer)) else float(v))
+                for k, v in ((k, getattr(self, k)) for k in self._CKPT_SCALARS)}
+        meta.update({"T_grids": [float(t) for t in self.T_grids],
+                     "grid_deflections": [float(d) for d in getattr(self, "grid_deflections", [])],
+                     "material": {"k": self.mat_k, "rho": self.mat_rho, "cp": self.mat_cp,
+                                  "emissivity": self.emissivity, "alpha": self.alpha_thermal,
+                                  "E_mod": self.E_modulus, "Y_coeff": self.sputter_Y_coeff,
+                                  "E_th": self.sputter_E_th},
+                     "C_cell": float(self.C_cell), "A_cell": float(self.A_cell),
+                     "cs_smoothing": {label: float(getattr(ds["spline"], "_pb_smoothing", 0.0))
+                                      for label, ds in self.user_cs.items()},
+                     "params": params})
+        np.savez_compressed(path, meta=np.array(json.dumps(meta)), **arrays)
+
+    @classmethod
+    def load_checkpoint(cls, path, device=0):
+        """Rebuild a simulator from ``save_checkpoint``; returns ``(sim, params)``."""
+        import json
+        from scipy.interpolate import UnivariateSpline
+        z = np.load(path)
+        meta = json.loads(str(z["meta"]))
+        sim = cls(device=device, seed=meta["seed"], sort_every=meta["sort_every"])
+        for k in cls._CKPT_SCALARS:
+            if k not in ("seed", "sort_every", "iteration"):
+                setattr(sim, k, meta[k])
+        sim.set_material(props=meta["material"])
+        sim.C_cell, sim.A_cell = meta["C_cell"], meta["A_cell"]  # as computed when the run was set up
+        cs = {}
+        for key in z.files:
+            if key.startswith("cs_"):
+                label = key[3:]
+                e, c = z[key]
+                sp = UnivariateSpline(np.log10(np.maximum(e, 1e-30)), np.log10(np.maximum(c, 1e-50)),
+                                      s=meta["cs_smoothing"].get(label, 0.0), k=3)
+                sp._pb_smoothing = meta["cs_smoothing"].get(label, 0.0)
+                cs[label] = {"energy": e, "cs": c, "spline": sp, "type": label}
+        sim.user_cs = cs
+        params = meta["params"]
+        sim.grid_deflections = list(meta["grid_deflections"])
+        sim.build_domain(params)
+        for k in cls._CKPT_FIELDS:
+            setattr(sim, k, z[k])
+        sim._flush()
+        vnew = np.ascontiguousarray(z["Vnew"], np.float64)
+        _lib.check(sim._libh.pb_sim_set_field(sim._h, 11, _ptr(vnew), vnew.nbytes), "set_field")
+        sim.set_particles("ions", z["p_x"], z["p_y"], z["p_vx"], z["p_vy"], z["p_vz"], is_cex=z["p_isCEX"],
+                          ids=z["p_id"], sort=False, next_id=meta["next_ion_id"])
+        sim.set_particles("electrons", z["e_x"], z["e_y"], z["e_vx"], z["e_vy"], z["e_vz"], ids=z["e_id"],
+                          sort=False, next_id=meta["next_e_id"])
+        for k in ("iteration", "injected_ions", "transmitted_ions", "entered_optics", "next_ion_id", "next_e_id",
+                  "ppc_steps_count", "max_p", "max_e"):
+            setattr(sim, k, meta[k])
+        sim.T_grids = [np.float32(t) for t in meta["T_grids"]]
+        return sim, params
 
     # ------------------------------------------------------------------ domain
     def _gridmask(self):
