@@ -305,7 +305,8 @@ def sweep_section(device):
     perveance-sweep points (C3 draws, 0.2M-1M macro-particles).  Rates use the device time
     of 40 steps after 2 warm-up steps, scaled to 3000 steps per point; setup is not
     included.  Then a served run: 12 backstreaming-limit requests arriving as a Poisson
-    stream at 20 per second, admitted under a 150 GB budget, stepped in chunks of 10 and
+    stream at 20 per second, admitted under a 150 GB budget, built on up to 8 setup threads,
+    stepped in chunks of 10 and
     retired when the saddle potential and current change less than 5% between the halves
     of a 60-step window (or at 100 steps).  Its latencies include setup."""
     from thruster_cx_code_b200 import serving as SV
@@ -349,7 +350,8 @@ def sweep_section(device):
         req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device)), W.sweep_point_bytes(sp), SERVE_MAX_STEPS,
                          SV.Convergence(window=60, tol=0.05, keys=("current", "saddle")))
         arrivals.append((t, req))
-    srv = SV.SweepServer(device, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=batch)
+    srv = SV.SweepServer(device, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=batch,
+                         setup_workers=max(2, min(8, (os.cpu_count() or 2) // 2)))
     srv.serve(arrivals)
     st = srv.stats()
     st.update({"requests": SERVE_REQUESTS, "arrival_rate_hz": SERVE_RATE_HZ, "max_steps": SERVE_MAX_STEPS,
