@@ -59,6 +59,17 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
   double vmx = DADD((double)vx, DMUL(h, ex));
   double vmy = DADD((double)vy, DMUL(h, ey));
   double vmz = (double)vz;
+  if (!HAS_B && vmx != 0.0 && vmy != 0.0 && vmz != 0.0 && fabs(vmx) < INFINITY && fabs(vmy) < INFINITY &&
+      fabs(vmz) < INFINITY) {
+    // every cross-product term below is a signed zero (t = s = h * (+0)), and a finite
+    // nonzero value plus a zero is that value: the rotation is the identity, bit for bit
+    vx = __double2float_rn(DADD(vmx, DMUL(h, ex)));
+    vy = __double2float_rn(DADD(vmy, DMUL(h, ey)));
+    vz = __double2float_rn(vmz);
+    x = __fadd_rn(x, __fmul_rn(__fmul_rn(vx, dtf), 1000.0f));
+    y = __fadd_rn(y, __fmul_rn(__fmul_rn(vy, dtf), 1000.0f));
+    return;
+  }
   double tx, ty, tz, sx, sy, sz;
   if (HAS_B) {
     double bx = gather4(Bx, r0, r1, ix0, ix1, w00, w10, w01, w11);
