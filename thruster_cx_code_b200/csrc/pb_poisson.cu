@@ -46,6 +46,14 @@ constexpr float W_KEEP = (float)(1.0 - MG_JACOBI_OMEGA);
 // instances, each on its own contiguous range of blocks).
 __device__ __forceinline__ int gbid(const PoissonArgs& a) { return (int)blockIdx.x - a.blk0; }
 
+// Thread index of the grid-stride loops: 32-node chunks go to the blocks in turn (warp w
+// of block b takes chunk w * nblk + b), so a level with fewer nodes than threads still
+// spreads over every SM instead of filling the first few.  A permutation of the
+// block-major index; each warp still reads 32 consecutive nodes.
+__device__ __forceinline__ int gtid(const PoissonArgs& a) {
+  return (((int)threadIdx.x >> 5) * a.nblk + gbid(a)) * 32 + ((int)threadIdx.x & 31);
+}
+
 __device__ __forceinline__ void grid_barrier(const PoissonArgs& a) {
   unsigned int* bar = a.bar;
   uint32_t* err = a.errflags;
@@ -466,7 +474,7 @@ __device__ __forceinline__ void block_pairs(int N, Fn fn) {
   }
 }
 
-__device__ void sdown(const SLev& F, const SLev& C, const float* Rc) {
+__device__ void sdown(const SLev F, const SLev C, const float* __restrict__ Rc) {
   block_pairs(C.N, [&](int c0, int c1) {
     const int I0 = c0 / C.nx, J0 = c0 - I0 * C.nx;
     const float v0 = srestrict(F, Rc, C.N, I0, J0, c0);
@@ -481,7 +489,7 @@ __device__ void sdown(const SLev& F, const SLev& C, const float* Rc) {
   __syncthreads();
 }
 
-__device__ void sup(const SLev& F, const SLev& C, const float* Uf) {
+__device__ void sup(const SLev F, const SLev C, const float* __restrict__ Uf) {
   block_pairs(F.N, [&](int f0, int f1) {
     const int y0 = f0 / F.nx, x0 = f0 - y0 * F.nx;
     const float v0 = sprolong(F, C, Uf, y0, x0, f0);
@@ -514,31 +522,15 @@ __device__ void scoarse(const PoissonArgs& a, const SLev& L, const float* cinv, 
   __syncthreads();
 }
 
-// block 0: restrict from level first_small-1 (global), cycle through the small levels in
-// shared memory, publish z on level first_small for the grid-wide up leg
+// block 0: take r of level first_small (restricted by the grid-wide legs) into shared
+// memory, cycle through the small levels there, publish z of level first_small for the
+// grid-wide up leg.  Level descriptors are copied into registers (sdown/sup take them by
+// value): stores into the shared vectors then cannot force reloads of sizes and pointers.
 __device__ void small_cycle(const PoissonArgs& a, const SLev* sl, const float* cinv, float* rc) {
   const int fs = a.first_small, last = a.nlevels - 1;
-  const MgLevel& F = a.lev[fs - 1];
-  const MgLevel& CG = a.lev[fs];
-  const SLev& C0 = sl[fs];
-  block_pairs(C0.N, [&](int c0, int c1) {
-    float v[2] = {0.0f, 0.0f};
-    const int cc[2] = {c0, c1};
-#pragma unroll
-    for (int q = 0; q < 2; ++q) {
-      const int c = cc[q];
-      if (c < 0) continue;
-      const int I = c / C0.nx, J = c - I * C0.nx;
-      if (fs - 1 == 0) {
-        const float s = restrict_res<true>(F, F.r, I, J, C0.wrapP != 0);
-        v[q] = __ldg(CG.dinv + c) > 0.0f ? s : 0.0f;
-      } else {
-        v[q] = restrict_pre(F, CG, F.r, I, J, c);
-      }
-    }
-    C0.r[c0] = v[0];
-    if (c1 >= 0) C0.r[c1] = v[1];
-  });
+  const SLev C0 = sl[fs];
+  const float* rg = a.lev[fs].r;
+  for (int i = threadIdx.x; i < C0.N; i += blockDim.x) C0.r[i] = *(rg + i);
   __syncthreads();
   for (int l = fs; l < last; ++l) sdown(sl[l], sl[l + 1], sl[l + 1].R);
   scoarse(a, sl[last], cinv, rc);
@@ -564,7 +556,7 @@ __device__ void coarse_only(const PoissonArgs& a) {
 // z32 = M^{-1} r32 by one V(1,1) cycle; leaves the partial of (r, z) in `slot` and ends
 // with a barrier
 __device__ void vcycle(const PoissonArgs& a, const SLev* sl, const float* cinv, float* rc, int slot) {
-  const int tid = gbid(a) * blockDim.x + threadIdx.x, nth = a.nblk * blockDim.x;
+  const int tid = gtid(a), nth = a.nblk * blockDim.x;
   double rz = 0.0;
   if (a.nlevels == 1) {
     if (gbid(a) == 0) coarse_only(a);
@@ -575,7 +567,7 @@ __device__ void vcycle(const PoissonArgs& a, const SLev* sl, const float* cinv, 
     grid_barrier(a);
     return;
   }
-  for (int l = 0; l < a.first_small - 1; ++l) {
+  for (int l = 0; l < a.first_small; ++l) {
     if (l == 0) down_leg<true>(a, 0, tid, nth);
     else down_leg<false>(a, l, tid, nth);
     grid_barrier(a);
@@ -601,7 +593,7 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   __shared__ SLev sl[MG_MAX_LEVELS];
   __shared__ float* s_rc;
   __shared__ float* s_cinv;
-  const int tid = gbid(a) * blockDim.x + threadIdx.x, nth = a.nblk * blockDim.x;
+  const int tid = gtid(a), nth = a.nblk * blockDim.x;
   const int N = a.ny * a.nx;
   int slot = 0;
   double n_outer = 0, n_inner = 0, last_rel = 0;
