@@ -200,7 +200,8 @@ int32_t pb_sim_reserve(pb_sim* s, int32_t species, int32_t capacity);
 
 /* Field arrays: 0 V (f64), 1 Ex, 2 Ey, 3 rho, 4 Tmap (f32), 5 damage (f64), 6 isBound (u8),
  * 7 V_fixed (f64), 8 ppc (i32), 9 accum_ppc (f64), 10 eroded (f64), 11 Vnew (f64),
- * 12 node class (u8). */
+ * 12 node class (u8), 13 fine-level smoother weights of the field solver (f32, omega / A_ii on
+ * free nodes, 0 elsewhere; read-only). */
 int32_t pb_sim_field_ptr(pb_sim* s, int32_t which, void** dptr);
 int32_t pb_sim_get_field(pb_sim* s, int32_t which, void* host, int64_t nbytes);
 int32_t pb_sim_set_field(pb_sim* s, int32_t which, const void* host, int64_t nbytes);

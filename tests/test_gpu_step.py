@@ -111,6 +111,8 @@ def test_one_step_bit_exact_given_fields(gpu_mod, name):
     np.testing.assert_array_equal(g.rho, o.rho)
     ag, cg, ig = _ions(g)
     ao, co, io = _ions(o)
+    # stable compaction: the survivors keep the oracle's array order (no cell sort here)
+    np.testing.assert_array_equal(ig, io)
     ag, ig2 = _by_id(ag, ig)
     ao, io2 = _by_id(ao, io)
     np.testing.assert_array_equal(ig2, io2)
@@ -118,6 +120,7 @@ def test_one_step_bit_exact_given_fields(gpu_mod, name):
     np.testing.assert_array_equal(cg[np.argsort(ig, kind="stable")], co[np.argsort(io, kind="stable")])
     eg, jg = _eles(g)
     eo, jo = _eles(o)
+    np.testing.assert_array_equal(jg, jo)
     eg, jg2 = _by_id(eg, jg)
     eo, jo2 = _by_id(eo, jo)
     np.testing.assert_array_equal(jg2, jo2)

@@ -3,6 +3,7 @@
 // module-level thermal_conduction (Taichi semantics).
 #include "pb_kernels.cuh"
 #include "pb_misc.cuh"
+#include "pb_poisson.cuh"
 
 namespace pb {
 
@@ -265,6 +266,33 @@ __global__ void k_erosion_break(double* damage, uint8_t* isBound, uint8_t* cls, 
     }
   }
   if (cntb) atomicAdd(broken, cntb);
+}
+
+// After a break the fine-level smoother weights follow the new node classes, so the
+// field solves left in a multi-step run precondition the freed nodes too; the coarse
+// levels keep the old operator until the host rebuilds the hierarchy.  The V-cycle stays
+// symmetric positive definite: its smoother part is, once every free node has its weight,
+// and the coarse part adds a semidefinite term.  The weights are the host build's,
+// omega / (4 - Neumann neighbours) in double rounded to float, 0 off the free nodes.
+__global__ void k_refresh_dinv0(const uint8_t* cls, float* dinv, int ny, int nx, int periodic, const int* broken) {
+  if (*broken == 0) return;
+  const int N = ny * nx;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    float d = 0.0f;
+    if (cls[i] == NC_FREE) {
+      const int y = i / nx, x = i - y * nx;
+      int nneu = 0;
+      // left, right, down, up; outside the grid counts as a Neumann neighbour
+      nneu += x == 0 || cls[i - 1] == NC_NEU;
+      nneu += x == nx - 1 || cls[i + 1] == NC_NEU;
+      int yd = y - 1, yu = y + 1;
+      if (periodic) { if (yd < 0) yd += ny; if (yu >= ny) yu -= ny; }
+      nneu += yd < 0 || cls[yd * nx + x] == NC_NEU;
+      nneu += yu >= ny || cls[yu * nx + x] == NC_NEU;
+      if (nneu < 4) d = (float)(MG_JACOBI_OMEGA / (double)(4 - nneu));
+    }
+    dinv[i] = d;
+  }
 }
 
 // ------------------------------------------------------------------ thermal

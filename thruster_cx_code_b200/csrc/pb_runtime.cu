@@ -646,7 +646,9 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   if (p->erosion_on) {
     k_erosion_break<<<grid_for(s, N, 256), 256, 0, st>>>(s->damage, s->isBound, s->cls, s->eroded, s->ny, s->nx,
                                                          s->periodic, p->thresh, p->dy, &rep->broken);
-    ++s->launches;
+    k_refresh_dinv0<<<grid_for(s, N, 256), 256, 0, st>>>(s->cls, s->lev[0].dinv, s->ny, s->nx, s->periodic,
+                                                         &rep->broken);
+    s->launches += 2;
   }
 
   // electrons: push and purge (:1248-1293, 1534-1561)
@@ -1012,6 +1014,7 @@ static void* field_of(Sim* s, int which, size_t* esize) {
     case 10: *esize = 8; return s->eroded;
     case 11: *esize = 8; return s->Vnew;
     case 12: *esize = 1; return s->cls;
+    case 13: *esize = 4; return s->lev.empty() ? nullptr : s->lev[0].dinv;
     default: *esize = 0; return nullptr;
   }
 }
@@ -1039,6 +1042,7 @@ int32_t pb_sim_set_field(pb_sim* h, int32_t which, const void* host, int64_t nby
   size_t es;
   void* p = field_of(s, which, &es);
   if (!p || (size_t)nbytes != es * (size_t)s->ny * s->nx) return fail(PB_ERR_ARG, "pb_sim_set_field: size");
+  if (which == 13) return fail(PB_ERR_ARG, "pb_sim_set_field: the smoother weights are read-only");
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaMemcpy(p, host, nbytes, cudaMemcpyHostToDevice));
   if (which == 7) CK(cudaMemcpy(s->Vdc, host, nbytes, cudaMemcpyHostToDevice));
