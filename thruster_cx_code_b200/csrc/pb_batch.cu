@@ -113,7 +113,9 @@ int32_t pb_batch_create(pb_batch** out, int32_t device) {
   CK(cudaEventCreate(&b->ev0));
   CK(cudaEventCreate(&b->ev1));
   CK(cudaFuncSetAttribute((const void*)k_poisson_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)MG_SMALL_SMEM_CAP));
+                          (int)mg_coarse_smem_bytes(MG_MAX_COARSE)));
+  CK(cudaFuncSetAttribute((const void*)k_poisson_batch, cudaFuncAttributePreferredSharedMemoryCarveout,
+                          (int)cudaSharedmemCarveoutMaxL1));
   *out = b;
   return PB_OK;
 }

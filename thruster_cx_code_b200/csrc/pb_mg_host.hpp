@@ -8,11 +8,13 @@
 // as 9-point stencils (y periodic on every level when the domain is).  Coarse nodes
 // centred on Dirichlet fine nodes, and coarse nodes no active fine node interpolates
 // from, are inactive.  Coarsening stops at <= max_coarse active nodes; that level is
-// solved with a dense inverse computed here by Cholesky factorisation.
+// solved with a dense inverse computed here from a Cholesky factorisation.
 #pragma once
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <stdexcept>
+#include <thread>
 #include <vector>
 
 #include "pb_poisson.cuh"
@@ -34,7 +36,7 @@ constexpr double JACOBI_OMEGA = MG_JACOBI_OMEGA;
 struct Hierarchy {
   std::vector<Level> lev;
   std::vector<int> cidx;      // coarsest active nodes
-  std::vector<float> cinvT;   // coarsest inverse, transposed
+  std::vector<float> cinv;    // coarsest inverse (exactly symmetric)
 };
 
 inline std::vector<uint8_t> node_classes(int ny, int nx, int periodic, const uint8_t* isBound) {
@@ -184,6 +186,67 @@ inline void transfer_ops(Hierarchy& H) {
   }
 }
 
+// a . b over n terms, four partial sums (a fixed order)
+inline double dot4(const double* a, const double* b, int n) {
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  int k = 0;
+  for (; k + 4 <= n; k += 4) {
+    s0 += a[k] * b[k];
+    s1 += a[k + 1] * b[k + 1];
+    s2 += a[k + 2] * b[k + 2];
+    s3 += a[k + 3] * b[k + 3];
+  }
+  for (; k < n; ++k) s0 += a[k] * b[k];
+  return (s0 + s1) + (s2 + s3);
+}
+
+// fn(i) for i in [0, n), split over up to 8 host threads in interleaved order
+template <class Fn>
+inline void parallel_for(int n, Fn fn) {
+  const int nt = std::max(1, std::min({8, (int)std::thread::hardware_concurrency(), n / 64}));
+  if (nt == 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&, t] {
+      for (int i = t; i < n; i += nt) fn(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+// Inverse of an SPD matrix (row-major n x n) as float, exactly symmetric: Cholesky
+// A = L L^T, the columns of M = L^-1 by forward substitution, then A^-1 = M^T M.  Every
+// inner loop is a contiguous dot product; the column stages run on host threads.
+inline std::vector<float> spd_inverse(const std::vector<double>& A, int n) {
+  std::vector<double> L((size_t)n * n, 0.0);  // row-major, lower
+  for (int j = 0; j < n; ++j) {
+    const double* Lj = &L[(size_t)j * n];
+    const double s = A[(size_t)j * n + j] - dot4(Lj, Lj, j);
+    if (!(s > 0.0)) throw std::runtime_error("coarsest operator is not positive definite");
+    const double d = std::sqrt(s);
+    L[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) L[(size_t)i * n + j] = (A[(size_t)i * n + j] - dot4(&L[(size_t)i * n], Lj, j)) / d;
+  }
+  std::vector<double> M((size_t)n * n, 0.0);  // column c of L^-1 in M[c * n + i], i >= c
+  parallel_for(n, [&](int c) {
+    double* m = &M[(size_t)c * n];
+    m[c] = 1.0 / L[(size_t)c * n + c];
+    for (int i = c + 1; i < n; ++i) m[i] = -dot4(&L[(size_t)i * n + c], m + c, i - c) / L[(size_t)i * n + i];
+  });
+  std::vector<float> inv((size_t)n * n);
+  parallel_for(n, [&](int r) {
+    const double* mr = &M[(size_t)r * n];
+    for (int c = r; c < n; ++c) {
+      const float v = (float)dot4(mr + c, &M[(size_t)c * n + c], n - c);
+      inv[(size_t)r * n + c] = v;
+      inv[(size_t)c * n + r] = v;
+    }
+  });
+  return inv;
+}
+
 inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>& cls0, int max_coarse) {
   Hierarchy H;
   Level L0;
@@ -285,49 +348,20 @@ inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>&
   for (size_t i = 0; i < N; ++i)
     if (Lc.act[i]) { pos[i] = (long)H.cidx.size(); H.cidx.push_back((int)i); }
   int n = (int)H.cidx.size();
-  if (n > 1024) throw std::runtime_error("coarsest level too large for the dense solve");
+  if (n > MG_MAX_COARSE) throw std::runtime_error("coarsest level too large for the dense solve");
   std::vector<double> A((size_t)n * n, 0.0);
   for (int r = 0; r < n; ++r) {
     row_of(Lc, level, cls0, H.cidx[r], row);
     for (const Entry& e : row)
       if (pos[e.j] >= 0) A[(size_t)r * n + pos[e.j]] += e.v;
   }
-  // symmetrise (round-off) and factor
+  // symmetrise (round-off) and invert
   for (int r = 0; r < n; ++r)
     for (int c = r + 1; c < n; ++c) {
       double v = 0.5 * (A[(size_t)r * n + c] + A[(size_t)c * n + r]);
       A[(size_t)r * n + c] = A[(size_t)c * n + r] = v;
     }
-  std::vector<double> Lm((size_t)n * n, 0.0);
-  for (int j = 0; j < n; ++j) {
-    double s = A[(size_t)j * n + j];
-    for (int k = 0; k < j; ++k) s -= Lm[(size_t)j * n + k] * Lm[(size_t)j * n + k];
-    if (!(s > 0.0)) throw std::runtime_error("coarsest operator is not positive definite");
-    double d = std::sqrt(s);
-    Lm[(size_t)j * n + j] = d;
-    for (int i = j + 1; i < n; ++i) {
-      double t = A[(size_t)i * n + j];
-      for (int k = 0; k < j; ++k) t -= Lm[(size_t)i * n + k] * Lm[(size_t)j * n + k];
-      Lm[(size_t)i * n + j] = t / d;
-    }
-  }
-  // inverse columns: solve L L^T x = e_c
-  std::vector<double> inv((size_t)n * n, 0.0), yv(n);
-  for (int c = 0; c < n; ++c) {
-    for (int i = 0; i < n; ++i) {
-      double t = (i == c) ? 1.0 : 0.0;
-      for (int k = 0; k < i; ++k) t -= Lm[(size_t)i * n + k] * yv[k];
-      yv[i] = t / Lm[(size_t)i * n + i];
-    }
-    for (int i = n - 1; i >= 0; --i) {
-      double t = yv[i];
-      for (int k = i + 1; k < n; ++k) t -= Lm[(size_t)k * n + i] * inv[(size_t)k * n + c];
-      inv[(size_t)i * n + c] = t / Lm[(size_t)i * n + i];
-    }
-  }
-  H.cinvT.resize((size_t)n * n);
-  for (int r = 0; r < n; ++r)
-    for (int c = 0; c < n; ++c) H.cinvT[(size_t)c * n + r] = (float)inv[(size_t)r * n + c];
+  H.cinv = spd_inverse(A, n);
   return H;
 }
 

@@ -14,7 +14,7 @@
 // loop (FP64 residual f - A x, FP64 dot products).  The preconditioner is one V(1,1)
 // cycle: Galerkin coarse operators (9-point stencils, P bilinear), one damped-Jacobi
 // sweep from zero before restriction and one after prolongation, a dense inverse on
-// the coarsest level.  Both smoothing sweeps are fused into the transfers, so every
+// the coarsest level (up to a few thousand nodes, applied by all blocks).  Both smoothing sweeps are fused into the transfers, so every
 // level costs one grid-wide phase going down and one going up:
 //     down:  r_{l+1} = P^T (r - A w D^-1 r)
 //     up:    z = m + w D^-1 (r - A m),   m = w D^-1 r + P z_{l+1}
@@ -24,8 +24,7 @@
 // loads overlap instead of waiting on one another.
 //
 // Grid-wide phases are separated by a software grid barrier (cooperative launch
-// guarantees co-residency).  The levels below a size threshold run on block 0 out of
-// shared memory.  Every wait is bounded: on time-out the kernel sets
+// guarantees co-residency).  Every wait is bounded: on time-out the kernel sets
 // PB_EF_SPIN_TIMEOUT, stops waiting at later barriers and runs to completion.
 // Reductions are deterministic: one partial per block, summed in block order; the
 // partials ride on the barrier that the next phase needs anyway.
@@ -117,9 +116,21 @@ __device__ __forceinline__ void get_sums(const PoissonArgs& a, int slot, double&
   if (threadIdx.x < 32) {
     const double* part = a.partials + (size_t)(slot & 3) * 2 * a.nblk;
     double s0 = 0.0, s1 = 0.0;
-    for (int b = threadIdx.x; b < a.nblk; b += 32) {
-      s0 += __ldcg(part + b);
-      s1 += __ldcg(part + a.nblk + b);
+    // all of a lane's loads issued before the first add (one L2 round trip for up to 256
+    // blocks); the adds keep the order b = lane, lane + 32, ...
+    for (int base = 0; base < a.nblk; base += 256) {
+      double v0[8], v1[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int b = base + q * 32 + (int)threadIdx.x;
+        v0[q] = b < a.nblk ? __ldcg(part + b) : 0.0;
+        v1[q] = b < a.nblk ? __ldcg(part + a.nblk + b) : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        s0 += v0[q];
+        s1 += v1[q];
+      }
     }
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
@@ -167,13 +178,14 @@ __device__ __forceinline__ T apply0(const PoissonArgs& a, const T* v, int i, int
 }
 
 // ----------------------------------------------------------------- transfer phases
-// Restricted residual at coarse node (I, J) of the level below F:
-//   sum_children w_f * [f active] * ((1 - w) r_f - sum_{k != centre} A_fk d_k r_k).
-// LV0: F is the fine level (5-point operator, off-diagonals -1 to every neighbour;
-// d r is zero on non-free nodes).  wrapC: the coarse level's prolongation wraps in y.
-template <bool LV0>
-__device__ __forceinline__ float restrict_res(const MgLevel& F, const float* r, int I, int J, bool wrapC) {
-  const int ny = F.ny, nx = F.nx, Nf = ny * nx;
+// Restricted residual at coarse node (I, J) of level 1, from the fine level F (5-point
+// operator, off-diagonals -1 to every neighbour; d r is zero on non-free nodes):
+//   sum_children w_f * [f active] * ((1 - w) r_f + sum_{k nbr of f} d_k r_k).
+// rl(j) gives the fine residual at node j; each patch node is loaded once.  wrapC: the
+// coarse level's prolongation wraps in y.
+template <class RL>
+__device__ __forceinline__ float restrict0(const MgLevel& F, const RL& rl, int I, int J, bool wrapC) {
+  const int ny = F.ny, nx = F.nx;
   int ro[5];
   bool rv[5];
 #pragma unroll
@@ -190,15 +202,17 @@ __device__ __forceinline__ float restrict_res(const MgLevel& F, const float* r, 
     xo[u] = 2 * J + u - 2;
     cv[u] = xo[u] >= 0 && xo[u] < nx;
   }
-  float zp[5][5];
+  float zp[5][5], rq[5][5], dq[5][5];
 #pragma unroll
   for (int t = 0; t < 5; ++t)
 #pragma unroll
     for (int u = 0; u < 5; ++u) {
-      if (LV0 && (t == 0 || t == 4) && (u == 0 || u == 4)) { zp[t][u] = 0.0f; continue; }
+      if ((t == 0 || t == 4) && (u == 0 || u == 4)) { zp[t][u] = rq[t][u] = dq[t][u] = 0.0f; continue; }
       const bool ok = rv[t] && cv[u];
       const int j = ok ? ro[t] + xo[u] : 0;
-      const float d = __ldg(F.dinv + j), rj = *(r + j);
+      const float d = __ldg(F.dinv + j), rj = rl(j);
+      dq[t][u] = d;
+      rq[t][u] = rj;
       zp[t][u] = ok ? d * rj : 0.0f;
     }
   float s = 0.0f;
@@ -211,25 +225,19 @@ __device__ __forceinline__ float restrict_res(const MgLevel& F, const float* r, 
     for (int db = -1; db <= 1; ++db) {
       const int u = db + 2;
       const bool ok = rowok && cv[u];
-      const int f = ok ? ro[t] + xo[u] : 0;
-      const float df = __ldg(F.dinv + f), rf = *(r + f);
-      float res;
-      if (LV0) {
-        res = W_KEEP * rf + ((zp[t][u - 1] + zp[t][u + 1]) + (zp[t - 1][u] + zp[t + 1][u]));
-      } else {
-        res = W_KEEP * rf;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-          if (k == 4) continue;
-          res -= __ldg(F.st + (size_t)k * Nf + f) * zp[t + k / 3 - 1][u + k % 3 - 1];
-        }
-      }
+      const float res = W_KEEP * rq[t][u] + ((zp[t][u - 1] + zp[t][u + 1]) + (zp[t - 1][u] + zp[t + 1][u]));
       const float w = (da ? 0.5f : 1.0f) * (db ? 0.5f : 1.0f);
-      s += (ok && df > 0.0f) ? w * res : 0.0f;
+      s += (ok && dq[t][u] > 0.0f) ? w * res : 0.0f;
     }
   }
   return s;
 }
+
+// fine residual loaders of restrict0
+struct RPlain {
+  const float* r;
+  __device__ __forceinline__ float operator()(int j) const { return *(r + j); }
+};
 
 // (P z_c) at fine node (y, x) of the level above C
 __device__ __forceinline__ float prolong(const MgLevel& C, const float* zc, int y, int x) {
@@ -355,7 +363,7 @@ __device__ void down_leg(const PoissonArgs& a, int level, int tid, int nth) {
   for (int ic = tid; ic < Nc; ic += nth) {
     const int I = ic / C.nx, J = ic - I * C.nx;
     if (LV0) {
-      const float s = restrict_res<true>(F, F.r, I, J, C.wrapP != 0);
+      const float s = restrict0(F, RPlain{F.r}, I, J, C.wrapP != 0);
       __stcg(C.r + ic, __ldg(C.dinv + ic) > 0.0f ? s : 0.0f);
     } else {
       __stcg(C.r + ic, restrict_pre(F, C, F.r, I, J, ic));
@@ -363,225 +371,91 @@ __device__ void down_leg(const PoissonArgs& a, int level, int tid, int nth) {
   }
 }
 
-// grid-wide up leg: z_l from r_l and z_{l+1}; on level 0 also the partial of (r, z)
+// grid-wide up leg: z_l from r_l and z_{l+1}; on level 0 (residual r0) also the partial
+// of (r, z)
 template <bool LV0>
-__device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth) {
+__device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth, const float* r0 = nullptr) {
   const MgLevel& F = a.lev[level];
   const MgLevel& C = a.lev[level + 1];
   const int N = F.ny * F.nx;
   double rz = 0.0;
-  for (int i = tid; i < N; i += nth) {
-    const int y = i / F.nx, x = i - y * F.nx;
-    if (LV0) {
+  if (LV0) {
+    for (int i = tid; i < N; i += nth) {
+      const int y = i / F.nx, x = i - y * F.nx;
       float ri;
-      const float z = smooth_up<true>(F, C, F.r, C.z, y, x, i, ri);
+      const float z = smooth_up<true>(F, C, r0, C.z, y, x, i, ri);
       __stcg(F.z + i, z);
       rz += (double)ri * (double)z;
-    } else {
+    }
+  } else {
+    for (int i = tid; i < N; i += nth) {
+      const int y = i / F.nx, x = i - y * F.nx;
       __stcg(F.z + i, smooth_up_pre(F, C, F.r, C.z, y, x, i));
     }
   }
   return rz;
 }
 
-// ----------------------------------------------------------------- block-0 levels in shared memory
-// The levels from first_small down hold their r and z in block 0's shared memory and
-// apply the host-built transfer stencils (read through L1): one block-level phase per
-// level going down and one going up.
-struct SLev {
-  int ny, nx, per, wrapP, N;
-  float *r, *z;
-  float *R, *U;  // transfer stencils staged from global memory (R: levels > first, U: levels < last)
-};
-
-// layout of dynamic shared memory (mg_small_smem_bytes on the host): per level r and z;
-// then U of levels first..last-1, R of levels first+1..last, the coarsest inverse and
-// the coarsest right-hand side
-__device__ void small_layout(const PoissonArgs& a, float* base, SLev* sl, float** cinv, float** rc) {
-  size_t off = 0;
-  const int fs = a.first_small, last = a.nlevels - 1;
-  for (int l = fs; l <= last; ++l) {
-    const MgLevel& L = a.lev[l];
-    SLev& S = sl[l];
-    S.ny = L.ny; S.nx = L.nx; S.per = L.per; S.wrapP = L.wrapP; S.N = L.ny * L.nx;
-    S.r = base + off; off += S.N;
-    S.z = base + off; off += S.N;
-    S.R = S.U = nullptr;
-  }
-  for (int l = fs; l < last; ++l) { sl[l].U = base + off; off += 18 * (size_t)sl[l].N; }
-  for (int l = fs + 1; l <= last; ++l) { sl[l].R = base + off; off += 25 * (size_t)sl[l].N; }
-  if (a.cinv_smem) { *cinv = base + off; off += (size_t)a.nc * a.nc; }
-  else *cinv = const_cast<float*>(a.cinvT);
-  *rc = base + off;
-}
-
-// r at coarse node c = (I, J) from the finer level's r (5 x 5 patch, stencil Rc)
-__device__ __forceinline__ float srestrict(const SLev& F, const float* Rc, int Nc, int I, int J,
-                                           int c) {
-  float s = 0.0f;
-#pragma unroll
-  for (int t = 0; t < 5; ++t) {
-    int y = 2 * I + t - 2;
-    if (F.per) { if (y < 0) y += F.ny; else if (y >= F.ny) y -= F.ny; }
-    const bool rv = y >= 0 && y < F.ny;
-#pragma unroll
-    for (int u = 0; u < 5; ++u) {
-      const int x = 2 * J + u - 2;
-      const bool ok = rv && x >= 0 && x < F.nx;
-      const float w = Rc[(t * 5 + u) * Nc + c];
-      const float v = F.r[ok ? y * F.nx + x : 0];
-      s += ok ? w * v : 0.0f;
-    }
-  }
-  return s;
-}
-
-// z at fine node f = (y, x) from its r patch and the coarser level's z (stencil Uf)
-__device__ __forceinline__ float sprolong(const SLev& F, const SLev& C, const float* Uf, int y, int x,
-                                          int f) {
-  const int I0 = y >> 1, J0 = x >> 1;
-  float s = 0.0f;
-#pragma unroll
-  for (int t = 0; t < 3; ++t) {
-    int yy = y + t - 1;
-    if (F.per) { if (yy < 0) yy += F.ny; else if (yy >= F.ny) yy -= F.ny; }
-    const bool rv = yy >= 0 && yy < F.ny;
-    int cy = I0 + t - 1;
-    if (C.per) { if (cy < 0) cy += C.ny; else if (cy >= C.ny) cy -= C.ny; }
-    const bool cvr = cy >= 0 && cy < C.ny;
-#pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      const int xx = x + u - 1;
-      const bool ok = rv && xx >= 0 && xx < F.nx;
-      const float vr = F.r[ok ? yy * F.nx + xx : f];
-      s += ok ? Uf[(t * 3 + u) * F.N + f] * vr : 0.0f;
-      const int cx = J0 + u - 1;
-      const bool okc = cvr && cx >= 0 && cx < C.nx;
-      const float vz = C.z[okc ? cy * C.nx + cx : 0];
-      s += okc ? Uf[(9 + t * 3 + u) * F.N + f] * vz : 0.0f;
-    }
-  }
-  return s;
-}
-
-// two nodes per thread and pass, so that a level slightly larger than the block still
-// takes one round of loads
-template <class Fn>
-__device__ __forceinline__ void block_pairs(int N, Fn fn) {
-  for (int i0 = threadIdx.x; i0 < N; i0 += 2 * blockDim.x) {
-    const int i1 = i0 + blockDim.x;
-    fn(i0, i1 < N ? i1 : -1);
-  }
-}
-
-__device__ void sdown(const SLev F, const SLev C, const float* __restrict__ Rc) {
-  block_pairs(C.N, [&](int c0, int c1) {
-    const int I0 = c0 / C.nx, J0 = c0 - I0 * C.nx;
-    const float v0 = srestrict(F, Rc, C.N, I0, J0, c0);
-    float v1 = 0.0f;
-    if (c1 >= 0) {
-      const int I1 = c1 / C.nx, J1 = c1 - I1 * C.nx;
-      v1 = srestrict(F, Rc, C.N, I1, J1, c1);
-    }
-    C.r[c0] = v0;
-    if (c1 >= 0) C.r[c1] = v1;
-  });
-  __syncthreads();
-}
-
-__device__ void sup(const SLev F, const SLev C, const float* __restrict__ Uf) {
-  block_pairs(F.N, [&](int f0, int f1) {
-    const int y0 = f0 / F.nx, x0 = f0 - y0 * F.nx;
-    const float v0 = sprolong(F, C, Uf, y0, x0, f0);
-    float v1 = 0.0f;
-    if (f1 >= 0) {
-      const int y1 = f1 / F.nx, x1 = f1 - y1 * F.nx;
-      v1 = sprolong(F, C, Uf, y1, x1, f1);
-    }
-    F.z[f0] = v0;
-    if (f1 >= 0) F.z[f1] = v1;
-  });
-  __syncthreads();
-}
-
-// z = A_c^{-1} r on the coarsest level (dense inverse in global memory, 4 lanes per row)
-__device__ void scoarse(const PoissonArgs& a, const SLev& L, const float* cinv, float* rc) {
+// ----------------------------------------------------------------- coarsest level
+// z_c = A_c^{-1} r_c on the coarsest level, by every block of the instance: each block
+// gathers r_c of the active nodes into shared memory, then one warp per row (rows dealt
+// to the blocks in turn) takes the dot product with that row of the dense inverse.
+// Inactive nodes of z_c are never written (zero since allocation).
+__device__ void coarse_solve(const PoissonArgs& a, const float* rlev, float* zlev, float* rcs) {
   const int nc = a.nc;
-  for (int i = threadIdx.x; i < L.N; i += blockDim.x) L.z[i] = 0.0f;
-  for (int k = threadIdx.x; k < nc; k += blockDim.x) rc[k] = L.r[__ldg(a.cidx + k)];
+  for (int k = threadIdx.x; k < nc; k += blockDim.x) rcs[k] = *(rlev + __ldg(a.cidx + k));
   __syncthreads();
-  for (int base = 0; base < 4 * nc; base += blockDim.x) {
-    const int q = base + threadIdx.x, k = q >> 2, part = q & 3;
-    float s = 0.0f;
-    if (k < nc)
-      for (int j = part; j < nc; j += 4) s += cinv[j * nc + k] * rc[j];
-    s += __shfl_xor_sync(0xFFFFFFFFu, s, 1);
-    s += __shfl_xor_sync(0xFFFFFFFFu, s, 2);
-    if (k < nc && part == 0) L.z[__ldg(a.cidx + k)] = s;
-  }
-  __syncthreads();
-}
-
-// block 0: take r of level first_small (restricted by the grid-wide legs) into shared
-// memory, cycle through the small levels there, publish z of level first_small for the
-// grid-wide up leg.  Level descriptors are copied into registers (sdown/sup take them by
-// value): stores into the shared vectors then cannot force reloads of sizes and pointers.
-__device__ void small_cycle(const PoissonArgs& a, const SLev* sl, const float* cinv, float* rc) {
-  const int fs = a.first_small, last = a.nlevels - 1;
-  const SLev C0 = sl[fs];
-  const float* rg = a.lev[fs].r;
-  for (int i = threadIdx.x; i < C0.N; i += blockDim.x) C0.r[i] = *(rg + i);
-  __syncthreads();
-  for (int l = fs; l < last; ++l) sdown(sl[l], sl[l + 1], sl[l + 1].R);
-  scoarse(a, sl[last], cinv, rc);
-  for (int l = last - 1; l >= fs; --l) sup(sl[l], sl[l + 1], sl[l].U);
-  float* zg = a.lev[fs].z;
-  for (int i = threadIdx.x; i < C0.N; i += blockDim.x) __stcg(zg + i, C0.z[i]);
-}
-
-// coarsest = finest (no coarse levels): dense solve on block 0 from global memory
-__device__ void coarse_only(const PoissonArgs& a) {
-  __shared__ float rc[1024];
-  const int N = a.ny * a.nx;
-  for (int i = threadIdx.x; i < N; i += blockDim.x) __stcg(a.z32 + i, 0.0f);
-  for (int k = threadIdx.x; k < a.nc; k += blockDim.x) rc[k] = *(a.r32 + __ldg(a.cidx + k));
-  __syncthreads();
-  for (int k = threadIdx.x; k < a.nc; k += blockDim.x) {
-    float s = 0.0f;
-    for (int j = 0; j < a.nc; ++j) s += __ldg(a.cinvT + (size_t)j * a.nc + k) * rc[j];
-    __stcg(a.z32 + __ldg(a.cidx + k), s);
+  const int lane = threadIdx.x & 31;
+  const int nw = a.nblk * (int)(blockDim.x >> 5);
+  for (int k = (int)(threadIdx.x >> 5) * a.nblk + gbid(a); k < nc; k += nw) {
+    const float* row = a.cinv + (size_t)k * nc;
+    float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f, s3 = 0.0f;
+    int j = lane;
+    for (; j + 96 < nc; j += 128) {
+      s0 += __ldg(row + j) * rcs[j];
+      s1 += __ldg(row + j + 32) * rcs[j + 32];
+      s2 += __ldg(row + j + 64) * rcs[j + 64];
+      s3 += __ldg(row + j + 96) * rcs[j + 96];
+    }
+    for (; j < nc; j += 32) s0 += __ldg(row + j) * rcs[j];
+    float s = (s0 + s1) + (s2 + s3);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    if (lane == 0) __stcg(zlev + __ldg(a.cidx + k), s);
   }
 }
 
-// z32 = M^{-1} r32 by one V(1,1) cycle; leaves the partial of (r, z) in `slot` and ends
-// with a barrier
-__device__ void vcycle(const PoissonArgs& a, const SLev* sl, const float* cinv, float* rc, int slot) {
+// z32 = M^{-1} r0 by one V(1,1) cycle, after the phase that restricted r0 to level 1
+// (down_leg<true>):
+// the down legs from level 1, the coarse solve, the up legs and the fine-level up leg.
+// Leaves the partial of (r0, z) in `slot` and ends with a barrier.
+__device__ void vcycle_below(const PoissonArgs& a, float* rcs, int slot, const float* r0) {
   const int tid = gtid(a), nth = a.nblk * blockDim.x;
   double rz = 0.0;
-  if (a.nlevels == 1) {
-    if (gbid(a) == 0) coarse_only(a);
+  const int last = a.nlevels - 1;
+  if (last == 0) {
+    coarse_solve(a, r0, a.z32, rcs);
     grid_barrier(a);
     const int N = a.ny * a.nx;
-    for (int i = tid; i < N; i += nth) rz += (double)(*(a.r32 + i)) * (double)(*(a.z32 + i));
+    for (int i = tid; i < N; i += nth) rz += (double)(*(r0 + i)) * (double)(*(a.z32 + i));
     put_partials(a, slot, rz, 0.0);
     grid_barrier(a);
     return;
   }
-  for (int l = 0; l < a.first_small; ++l) {
-    if (l == 0) down_leg<true>(a, 0, tid, nth);
-    else down_leg<false>(a, l, tid, nth);
+  for (int l = 1; l < last; ++l) {
+    down_leg<false>(a, l, tid, nth);
     grid_barrier(a);
     tmark(a, l < 7 ? l : 6);
   }
-  if (gbid(a) == 0) small_cycle(a, sl, cinv, rc);
+  coarse_solve(a, a.lev[last].r, a.lev[last].z, rcs);
   grid_barrier(a);
   tmark(a, 7);
-  for (int l = a.first_small - 1; l >= 1; --l) {
+  for (int l = last - 1; l >= 1; --l) {
     up_leg<false>(a, l, tid, nth);
     grid_barrier(a);
     tmark(a, 8 + (l < 7 ? l : 6));
   }
-  rz = up_leg<true>(a, 0, tid, nth);
+  rz = up_leg<true>(a, 0, tid, nth, r0);
   put_partials(a, slot, rz, 0.0);
   grid_barrier(a);
   tmark(a, 8);
@@ -590,28 +464,12 @@ __device__ void vcycle(const PoissonArgs& a, const SLev* sl, const float* cinv, 
 // ----------------------------------------------------------------- the persistent kernel
 __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   extern __shared__ float4 dyn_smem[];
-  __shared__ SLev sl[MG_MAX_LEVELS];
-  __shared__ float* s_rc;
-  __shared__ float* s_cinv;
+  float* rcs = reinterpret_cast<float*>(dyn_smem);  // nc floats: the coarsest r, gathered
   const int tid = gtid(a), nth = a.nblk * blockDim.x;
   const int N = a.ny * a.nx;
   int slot = 0;
   double n_outer = 0, n_inner = 0, last_rel = 0;
   tmark(a, 20);
-
-  // block 0: the small levels' vectors, transfer stencils and coarsest inverse in shared memory
-  if (gbid(a) == 0 && a.nlevels > 1) {
-    if (threadIdx.x == 0) small_layout(a, reinterpret_cast<float*>(dyn_smem), sl, &s_cinv, &s_rc);
-    __syncthreads();
-    const int fs = a.first_small, last = a.nlevels - 1;
-    for (int l = fs; l < last; ++l)
-      for (int k = threadIdx.x; k < 18 * sl[l].N; k += blockDim.x) sl[l].U[k] = __ldg(a.lev[l].U + k);
-    for (int l = fs + 1; l <= last; ++l)
-      for (int k = threadIdx.x; k < 25 * sl[l].N; k += blockDim.x) sl[l].R[k] = __ldg(a.lev[l].R + k);
-    if (a.cinv_smem)
-      for (int k = threadIdx.x; k < a.nc * a.nc; k += blockDim.x) s_cinv[k] = __ldg(a.cinvT + k);
-    __syncthreads();
-  }
 
   // Dirichlet-neighbour sums (V_fixed is constant during the launch)
   for (int i = tid; i < N; i += nth) {
@@ -661,8 +519,11 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
       double rz_old = 0.0, rr0 = rnorm2, dummy;
       for (int k = 0; k < a.max_inner; ++k) {
         n_inner += 1;
-        tmark(a, 15);
-        vcycle(a, sl, s_cinv, s_rc, slot);  // z32 = M r32, (r, z) partial in slot, barrier
+        // z32 = M r32: fine-level restriction, then the rest of the V-cycle
+        if (a.nlevels > 1) down_leg<true>(a, 0, tid, nth);
+        grid_barrier(a);
+        tmark(a, 0);
+        vcycle_below(a, rcs, slot, a.r32);  // (r, z) partial in slot, barrier
         double rz;
         get_sums(a, slot++, rz, dummy);
         const double beta = k == 0 ? 0.0 : rz / rz_old;

@@ -6,7 +6,7 @@ namespace pb {
 
 constexpr int MG_MAX_LEVELS = 16;
 constexpr double MG_JACOBI_OMEGA = 0.8;       // damped-Jacobi weight of the V-cycle smoother
-constexpr size_t MG_SMALL_SMEM_CAP = 200 * 1024;  // shared memory for the block-0 levels
+constexpr int MG_MAX_COARSE = 4096;          // largest coarsest level (dense inverse, nc^2 floats)
 enum NodeClass : uint8_t { NC_FREE = 0, NC_DIR = 1, NC_NEU = 2 };
 
 struct MgLevel {
@@ -49,12 +49,10 @@ struct PoissonArgs {
   int max_outer, max_inner;
   // hierarchy
   int nlevels;            // including level 0 and the coarsest
-  int first_small;        // first level handled by block 0 in shared memory (>= 1)
   MgLevel lev[MG_MAX_LEVELS];
-  int nc;                 // coarsest active count
+  int nc;                 // coarsest active count (<= MG_MAX_COARSE)
   const int* cidx;        // coarsest active node indices
-  const float* cinvT;     // coarsest inverse, transposed (nc x nc)
-  int cinv_smem;          // block 0 stages cinvT in shared memory
+  const float* cinv;      // coarsest inverse (nc x nc, exactly symmetric)
   // this instance's blocks in the launch and its reductions and barrier
   int blk0, nblk;         // first block and number of blocks
   double* partials;       // 4 slots x 2 values x nblk doubles
@@ -64,15 +62,7 @@ struct PoissonArgs {
   unsigned long long* trace;  // optional: ns per phase category (block 0), [31] = last stamp
 };
 
-// dynamic shared memory of k_poisson for levels first..nlevels-1 of sizes N[l]: r and z
-// per level, U (18 N) of levels first..last-1, R (25 N) of levels first+1..last, the
-// coarsest inverse (nc^2, when cinv_smem) and right-hand side (nc), all float
-inline size_t mg_small_smem_bytes(const int* N, int first, int nlevels, int nc, int cinv_smem) {
-  size_t f = 0;
-  for (int l = first; l < nlevels; ++l) f += 2 * (size_t)N[l];
-  for (int l = first; l < nlevels - 1; ++l) f += 18 * (size_t)N[l];
-  for (int l = first + 1; l < nlevels; ++l) f += 25 * (size_t)N[l];
-  return 4 * (f + (cinv_smem ? (size_t)nc * nc : 0) + (size_t)nc);
-}
+// dynamic shared memory of k_poisson: the coarsest right-hand side gathered by each block
+inline size_t mg_coarse_smem_bytes(int nc) { return 4 * (size_t)(nc > 0 ? nc : 1); }
 
 }  // namespace pb

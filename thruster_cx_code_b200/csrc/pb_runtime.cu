@@ -76,10 +76,9 @@ struct Sim {
   int *ppc = nullptr, *cnt_i = nullptr, *cnt_e = nullptr;
   // multigrid
   std::vector<DevLevel> lev;
-  int first_small = 1;
   int nc = 0;
   int* cidx = nullptr;
-  float* cinvT = nullptr;
+  float* cinv = nullptr;
   double* partials = nullptr;
   unsigned int* bar = nullptr;
   double* pstats = nullptr;
@@ -87,7 +86,6 @@ struct Sim {
   int trace_on = 0;
   int pgrid = 0;
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
-  int cinv_smem = 0;  // coarsest inverse staged in shared memory
   // particles
   Species sp[2];
   int* counts = nullptr;         // [ion buf0, ion buf1, ele buf0, ele buf1]
@@ -118,7 +116,7 @@ struct Sim {
   int rep_run_cap = 0;
   // settings
   double tol = 1e-8, tol_inner = 1e-5;
-  int max_outer = 8, max_inner = 40, nu = 1, max_coarse = 256;
+  int max_outer = 8, max_inner = 40, nu = 1, max_coarse = 1536;
   uint64_t seed = 0;
   bool counts_valid = false;
   bool domain_set = false;
@@ -226,7 +224,7 @@ static void free_levels(Sim* s) {
   }
   s->lev.clear();
   dfree(s->cidx);
-  dfree(s->cinvT);
+  dfree(s->cinv);
 }
 
 // node classes from isBound (host copy) and the multigrid hierarchy
@@ -251,7 +249,6 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   CK(cudaStreamSynchronize(s->stream));
   free_levels(s);
   s->lev.resize(H.lev.size());
-  s->first_small = (int)H.lev.size() - 1;
   for (size_t l = 0; l < H.lev.size(); ++l) {
     const auto& L = H.lev[l];
     DevLevel& D = s->lev[l];
@@ -275,38 +272,18 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
       CK(cudaMemcpy(D.st, L.st.data(), 9 * N * sizeof(float), cudaMemcpyHostToDevice));
       CK(cudaMemset(D.r, 0, N * sizeof(float)));
       CK(cudaMemset(D.z, 0, N * sizeof(float)));
-      if ((int)l < s->first_small && N <= 2000) s->first_small = (int)l;
     }
   }
-  if (s->first_small < 1) s->first_small = 1;
   s->nc = (int)H.cidx.size();
-  // the block-0 levels live in shared memory: move the first one down until they fit,
-  // with the coarsest inverse there too if possible
-  std::vector<int> Ns(H.lev.size());
-  for (size_t l = 0; l < H.lev.size(); ++l) Ns[l] = H.lev[l].ny * H.lev[l].nx;
-  const int nl = (int)H.lev.size();
-  const int fs0 = s->first_small;
-  s->psmem = 0;
-  s->cinv_smem = 0;
-  if (nl > 1) {
-    bool fit = false;
-    for (int cs = 1; cs >= 0 && !fit; --cs) {
-      int fs = fs0;
-      while (fs < nl - 1 && mg_small_smem_bytes(Ns.data(), fs, nl, s->nc, cs) > MG_SMALL_SMEM_CAP) ++fs;
-      size_t b = mg_small_smem_bytes(Ns.data(), fs, nl, s->nc, cs);
-      if (b <= MG_SMALL_SMEM_CAP) { fit = true; s->first_small = fs; s->psmem = b; s->cinv_smem = cs; }
-    }
-    if (!fit)
-      return fail(PB_ERR_ARG, "multigrid build: the coarsest level does not fit in shared memory");
-  }
+  s->psmem = mg_coarse_smem_bytes(s->nc);
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_poisson, PT, s->psmem));
   if (occ < 1) return fail(PB_ERR_ARG, "field solver: no resident block with " + std::to_string(s->psmem) +
                                            " bytes of shared memory");
   CK(dalloc(&s->cidx, s->nc));
-  CK(dalloc(&s->cinvT, (size_t)s->nc * s->nc));
+  CK(dalloc(&s->cinv, (size_t)s->nc * s->nc));
   CK(cudaMemcpy(s->cidx, H.cidx.data(), s->nc * sizeof(int), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(s->cinvT, H.cinvT.data(), (size_t)s->nc * s->nc * sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->cinv, H.cinv.data(), (size_t)s->nc * s->nc * sizeof(float), cudaMemcpyHostToDevice));
   return PB_OK;
 }
 
@@ -321,7 +298,7 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
   a.hx = p->hx; a.two_hx = p->two_hx; a.hy = p->hy; a.two_hy = p->two_hy; a.two_hy_per = p->two_hy_per;
   a.iterations = iterations; a.compute_field = 1;
   a.tol = s->tol; a.tol_inner = s->tol_inner; a.max_outer = s->max_outer; a.max_inner = s->max_inner;
-  a.nlevels = (int)s->lev.size(); a.first_small = s->first_small;
+  a.nlevels = (int)s->lev.size();
   for (size_t l = 0; l < s->lev.size() && l < (size_t)MG_MAX_LEVELS; ++l) {
     const DevLevel& D = s->lev[l];
     a.lev[l].ny = D.ny; a.lev[l].nx = D.nx; a.lev[l].per = D.per; a.lev[l].wrapP = D.wrapP;
@@ -330,7 +307,7 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
     a.lev[l].R = D.R;
     a.lev[l].U = D.U;
   }
-  a.nc = s->nc; a.cidx = s->cidx; a.cinvT = s->cinvT; a.cinv_smem = s->cinv_smem;
+  a.nc = s->nc; a.cidx = s->cidx; a.cinv = s->cinv;
   a.blk0 = 0; a.nblk = s->pgrid;
   a.partials = s->partials; a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
@@ -746,9 +723,12 @@ int32_t pb_sim_create(pb_sim** out, int32_t device) {
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   CK(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device));
-  // field solve: one block of PT threads per SM (cooperative launch)
+  // field solve: one block of PT threads per SM (cooperative launch); the little shared
+  // memory it uses leaves the rest of the SM's L1 to cache the grid
   CK(cudaFuncSetAttribute((const void*)k_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)MG_SMALL_SMEM_CAP));
+                          (int)mg_coarse_smem_bytes(MG_MAX_COARSE)));
+  CK(cudaFuncSetAttribute((const void*)k_poisson, cudaFuncAttributePreferredSharedMemoryCarveout,
+                          (int)cudaSharedmemCarveoutMaxL1));
   s->pgrid = s->num_sms;
   CK(dalloc(&s->partials, 4 * 2 * (size_t)s->pgrid));
   CK(dalloc(&s->bar, 2));
@@ -820,7 +800,7 @@ int32_t pb_sim_set_seed(pb_sim* h, uint64_t seed) { h->s.seed = seed; return PB_
 int32_t pb_sim_set_solver(pb_sim* h, double tol, double tol_inner, int32_t max_outer, int32_t max_inner, int32_t nu,
                           int32_t max_coarse) {
   Sim* s = &h->s;
-  if (!(tol > 0) || !(tol_inner > 0) || max_outer < 1 || max_inner < 1 || nu < 1 || max_coarse < 4 || max_coarse > 1024)
+  if (!(tol > 0) || !(tol_inner > 0) || max_outer < 1 || max_inner < 1 || nu < 1 || max_coarse < 4 || max_coarse > MG_MAX_COARSE)
     return fail(PB_ERR_ARG, "pb_sim_set_solver: invalid value");
   s->tol = tol; s->tol_inner = tol_inner; s->max_outer = max_outer; s->max_inner = max_inner; s->nu = nu;
   s->max_coarse = max_coarse;
