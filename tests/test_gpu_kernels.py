@@ -105,6 +105,16 @@ def test_substeps_exact(torch_cuda):
         res = f[f"{tag}_res"]
         assert int(out[0]) == int(res[0])
         assert out[1] == res[1] and out[2] == res[2]
+        # the same particles in arrays that start 4 bytes past a 16-byte boundary
+        # (the kernel's 16-byte loads do not apply there)
+        tm = [torch.zeros(a.numel() + 1, dtype=a.dtype, device=dev) for a in t]
+        for a, b in zip(tm, t):
+            a[1:] = b
+        _lib.check(lib.pb_compute_particle_substeps(*[a[1:].data_ptr() for a in tm], t[0].numel(), Ex.data_ptr(),
+                                                    Ey.data_ptr(), nx, ny, dx, dy, float(f[f"{tag}_qm"]), 1e-10,
+                                                    0.25, out, None), "substeps, unaligned")
+        assert int(out[0]) == int(res[0])
+        assert out[1] == res[1] and out[2] == res[2]
 
 
 def test_segment_hits_exact(torch_cuda):

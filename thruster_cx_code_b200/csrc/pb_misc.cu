@@ -374,6 +374,23 @@ __global__ void __launch_bounds__(256) k_thermal(float* T, const uint8_t* isBoun
 }
 
 // grid means over each electrode mask (bit g of gridmask) -> sums[2g], counts[2g+1]
+// Block-wide reduction with op; the result is valid in thread 0.  Ends with a barrier, so
+// it can be called again at once.  blockDim.x is a multiple of 32.
+template <class T, class Op>
+__device__ __forceinline__ T block_reduce(T v, Op op, T ident) {
+  __shared__ T sm[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_down_sync(0xFFFFFFFFu, v, o));
+  if (lane == 0) sm[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? sm[lane] : ident;
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_down_sync(0xFFFFFFFFu, v, o));
+  }
+  __syncthreads();
+  return v;
+}
+
 __global__ void k_grid_sums(const float* T, const uint16_t* gridmask, int N, int ngrids, double* out) {
   double s[16];
   double c[16];
@@ -385,10 +402,12 @@ __global__ void k_grid_sums(const float* T, const uint16_t* gridmask, int N, int
     for (int g = 0; g < ngrids; ++g)
       if (m & (1u << g)) { s[g] += t; c[g] += 1.0; }
   }
+  // one pair of atomics per block and grid (per-warp atomics on the same 2 * ngrids
+  // words serialised at L2)
+  const auto add = [](double a, double b) { return a + b; };
   for (int g = 0; g < ngrids; ++g) {
-    double a = s[g], b = c[g];
-    for (int o = 16; o > 0; o >>= 1) { a += __shfl_down_sync(0xFFFFFFFFu, a, o); b += __shfl_down_sync(0xFFFFFFFFu, b, o); }
-    if ((threadIdx.x & 31) == 0 && b != 0.0) { atomicAdd(out + 2 * g, a); atomicAdd(out + 2 * g + 1, b); }
+    const double a = block_reduce(s[g], add, 0.0), b = block_reduce(c[g], add, 0.0);
+    if (threadIdx.x == 0 && b != 0.0) { atomicAdd(out + 2 * g, a); atomicAdd(out + 2 * g + 1, b); }
   }
 }
 
@@ -402,12 +421,11 @@ __global__ void k_ppc_stats(const int* ppc, double* accum, int N, unsigned long 
     accum[i] += (double)v;
     if (v > 0) { ++act; if (v < 3) ++low; mn = v < mn ? v : mn; }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    act += __shfl_down_sync(0xFFFFFFFFu, act, o);
-    low += __shfl_down_sync(0xFFFFFFFFu, low, o);
-    mn = min(mn, __shfl_down_sync(0xFFFFFFFFu, mn, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
+  const auto add = [](unsigned long long a, unsigned long long b) { return a + b; };
+  act = block_reduce(act, add, 0ull);
+  low = block_reduce(low, add, 0ull);
+  mn = block_reduce(mn, [](int a, int b) { return a < b ? a : b; }, 0x7fffffff);
+  if (threadIdx.x == 0) {
     if (act) atomicAdd(stats, act);
     if (low) atomicAdd(stats + 1, low);
     atomicMin(stats + 2, (unsigned long long)mn);

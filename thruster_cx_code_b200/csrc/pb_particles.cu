@@ -193,7 +193,33 @@ __global__ void k_substep_reduce(const float* __restrict__ x, const float* __res
                                  double dt2, unsigned long long* ds_max_bits) {
   int n = n_dev ? *n_dev : n_host;
   unsigned long long m = 0ull;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  // four particles per thread and pass (16-byte loads of each array), so that a thread
+  // has four sets of loads and gathers in flight; the maximum does not depend on the
+  // order.  Arrays that do not all start 16-byte aligned take the one-by-one loop.
+  const bool vec = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) |
+                     reinterpret_cast<uintptr_t>(vx) | reinterpret_cast<uintptr_t>(vy) |
+                     reinterpret_cast<uintptr_t>(vz)) & 15u) == 0;
+  const int n4 = vec ? n >> 2 : 0;
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int q = t0; q < n4; q += stride) {
+    const float4 X = __ldg(reinterpret_cast<const float4*>(x) + q);
+    const float4 Y = __ldg(reinterpret_cast<const float4*>(y) + q);
+    const float4 U = __ldg(reinterpret_cast<const float4*>(vx) + q);
+    const float4 V = __ldg(reinterpret_cast<const float4*>(vy) + q);
+    const float4 W = __ldg(reinterpret_cast<const float4*>(vz) + q);
+    const double d0 = predicted_ds(X.x, Y.x, U.x, V.x, W.x, Ex, Ey, nx, ny, dxf, dyf, qm, dtf, dt2);
+    const double d1 = predicted_ds(X.y, Y.y, U.y, V.y, W.y, Ex, Ey, nx, ny, dxf, dyf, qm, dtf, dt2);
+    const double d2 = predicted_ds(X.z, Y.z, U.z, V.z, W.z, Ex, Ey, nx, ny, dxf, dyf, qm, dtf, dt2);
+    const double d3 = predicted_ds(X.w, Y.w, U.w, V.w, W.w, Ex, Ey, nx, ny, dxf, dyf, qm, dtf, dt2);
+    const unsigned long long b0 = (unsigned long long)__double_as_longlong(d0);
+    const unsigned long long b1 = (unsigned long long)__double_as_longlong(d1);
+    const unsigned long long b2 = (unsigned long long)__double_as_longlong(d2);
+    const unsigned long long b3 = (unsigned long long)__double_as_longlong(d3);
+    const unsigned long long b01 = b0 > b1 ? b0 : b1, b23 = b2 > b3 ? b2 : b3;
+    const unsigned long long b = b01 > b23 ? b01 : b23;
+    m = b > m ? b : m;
+  }
+  for (int i = 4 * n4 + t0; i < n; i += stride) {
     double ds = predicted_ds(x[i], y[i], vx[i], vy[i], vz[i], Ex, Ey, nx, ny, dxf, dyf, qm, dtf, dt2);
     unsigned long long b = (unsigned long long)__double_as_longlong(ds);
     m = b > m ? b : m;

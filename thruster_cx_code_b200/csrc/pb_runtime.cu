@@ -572,11 +572,11 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
 
   // C. sub-step counts (:1177-1209)
   const float dtf = (float)p->dt;
-  k_substep_reduce<<<grid_for(s, I.cap, 256), 256, 0, st>>>(I.buf[I.cur].x, I.buf[I.cur].y, I.buf[I.cur].vx,
+  k_substep_reduce<<<grid_for(s, I.cap / 4, 256, 4), 256, 0, st>>>(I.buf[I.cur].x, I.buf[I.cur].y, I.buf[I.cur].vx,
       I.buf[I.cur].vy, I.buf[I.cur].vz, ni_src, 0, s->Ex, s->Ey, s->nx, s->ny, dxf, dyf, p->qm_ion, dtf, p->dt2,
       s->ds_bits);
   ++s->launches;
-  k_substep_reduce<<<grid_for(s, E.cap, 256), 256, 0, st>>>(E.buf[E.cur].x, E.buf[E.cur].y, E.buf[E.cur].vx,
+  k_substep_reduce<<<grid_for(s, E.cap / 4, 256, 4), 256, 0, st>>>(E.buf[E.cur].x, E.buf[E.cur].y, E.buf[E.cur].vx,
       E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->nx, s->ny, dxf, dyf, p->qm_e, dtf, p->dt2,
       s->ds_bits + 1);
   ++s->launches;
