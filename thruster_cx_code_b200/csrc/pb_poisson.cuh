@@ -56,7 +56,7 @@ struct PoissonArgs {
   // this instance's blocks in the launch and its reductions and barrier
   int blk0, nblk;         // first block and number of blocks
   double* partials;       // 4 slots x 2 values x nblk doubles
-  unsigned int* bar;      // barrier word (any start value)
+  unsigned int* bar;      // barrier word, zero at launch (its low bits must start at zero)
   uint32_t* errflags;
   double* stats;          // [outer its, inner its, final rel residual, solves] accumulated
   unsigned long long* trace;  // optional: ns per phase category (block 0), [31] = last stamp
