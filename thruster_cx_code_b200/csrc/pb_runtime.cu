@@ -115,7 +115,7 @@ struct Sim {
   pb_step_report* rep_run = nullptr;  // pinned per-step reports of pb_sim_run
   int rep_run_cap = 0;
   // settings
-  double tol = 1e-8, tol_inner = 1e-5;
+  double tol = 1e-8, tol_inner = 1e-3;
   int max_outer = 8, max_inner = 40, nu = 1, max_coarse = 1536;
   uint64_t seed = 0;
   bool counts_valid = false;
