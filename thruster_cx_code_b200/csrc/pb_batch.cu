@@ -76,7 +76,7 @@ int64_t sim_device_bytes(const Sim* s) {
   const int64_t N = (int64_t)s->ny * s->nx;
   int64_t b = 0;
   for (int k = 0; k < 2; ++k) b += 2LL * s->sp[k].cap * (5 * 4 + 4 + (s->sp[k].ion ? 1 : 0));
-  b += N * (9 * 8 + 9 * 4 + 4 + 2 + 3 * 4);  // double and float fields, masks, count maps
+  b += N * (9 * 8 + 9 * 4 + 32 + 4 + 2 + 3 * 4);  // double and float fields, E corners, masks, count maps
   for (size_t l = 0; l < s->lev.size(); ++l) {
     const int64_t Nl = (int64_t)s->lev[l].ny * s->lev[l].nx;
     b += Nl * 4 * (1 + (l ? 11 : 0)) + (l ? Nl : 0);

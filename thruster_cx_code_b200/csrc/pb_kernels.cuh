@@ -27,6 +27,7 @@ struct IonStepArgs {
   int *num_dst;
   // fields
   const float *Ex, *Ey, *Bx, *By, *Bz;
+  const float4* Ec;       // per-cell corners of Ex, Ey (the gather when B = 0)
   int has_B;
   const uint8_t *isBound;
   const uint8_t *bdist;   // Chebyshev distance (cells) to the nearest bound node, capped
@@ -87,6 +88,7 @@ struct EleStepArgs {
   const int *num_src;
   int *num_dst;
   const float *Ex, *Ey, *Bx, *By, *Bz;
+  const float4* Ec;       // per-cell corners of Ex, Ey (the gather when B = 0)
   int has_B;
   const uint8_t *isBound;
   int nx, ny;

@@ -70,6 +70,7 @@ struct Sim {
   double *accum_ppc = nullptr, *f = nullptr, *dirsum = nullptr;
   float *Ex = nullptr, *Ey = nullptr, *rho = nullptr, *Tmap = nullptr;
   float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *e32 = nullptr;
+  float4* ecorn = nullptr;  // per-cell corners of Ex and Ey, 2 x float4 per node
   uint8_t *isBound = nullptr, *cls = nullptr;
   uint8_t *bdist = nullptr, *bdist_tmp = nullptr;  // Chebyshev distance to the nearest bound node
   uint16_t* gridmask = nullptr;
@@ -570,14 +571,19 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   uint32_t* ef = &rep->errflags;
   int32_t rc;
 
+  // corners of Ex, Ey for the gathers below (rebuilt every step: fields change in the
+  // solve, through pb_sim_set_field or through pb_sim_field_ptr)
+  k_e_corners<<<grid_for(s, N, 256), 256, 0, st>>>(s->Ex, s->Ey, s->ecorn, s->ny, s->nx);
+  ++s->launches;
+
   // C. sub-step counts (:1177-1209)
   const float dtf = (float)p->dt;
   k_substep_reduce<<<grid_for(s, I.cap / 4, 256, 4), 256, 0, st>>>(I.buf[I.cur].x, I.buf[I.cur].y, I.buf[I.cur].vx,
-      I.buf[I.cur].vy, I.buf[I.cur].vz, ni_src, 0, s->Ex, s->Ey, s->nx, s->ny, dxf, dyf, p->qm_ion, dtf, p->dt2,
+      I.buf[I.cur].vy, I.buf[I.cur].vz, ni_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf, dyf, p->qm_ion, dtf, p->dt2,
       s->ds_bits);
   ++s->launches;
   k_substep_reduce<<<grid_for(s, E.cap / 4, 256, 4), 256, 0, st>>>(E.buf[E.cur].x, E.buf[E.cur].y, E.buf[E.cur].vx,
-      E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->nx, s->ny, dxf, dyf, p->qm_e, dtf, p->dt2,
+      E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf, dyf, p->qm_e, dtf, p->dt2,
       s->ds_bits + 1);
   ++s->launches;
   k_substep_finish<<<1, 1, 0, st>>>((const double*)s->ds_bits, p->ds_lim, s->n_sub, ef);
@@ -589,7 +595,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   // ions: push, hits, tallies, exit diagnostics, compaction, CEX, PPC (:1211-1739)
   IonStepArgs a{};
   a.src = I.buf[I.cur]; a.dst = I.buf[1 - I.cur]; a.num_src = ni_src; a.num_dst = ni_dst;
-  a.Ex = s->Ex; a.Ey = s->Ey; a.Bx = a.By = a.Bz = nullptr; a.has_B = 0;
+  a.Ex = s->Ex; a.Ey = s->Ey; a.Ec = s->ecorn; a.Bx = a.By = a.Bz = nullptr; a.has_B = 0;
   a.isBound = s->isBound; a.bdist = s->bdist; a.nx = s->nx; a.ny = s->ny; a.dxf = dxf; a.dyf = dyf;
   a.inv_dx = 1.0f / dxf; a.inv_dy = 1.0f / dyf;
   a.dt = p->dt; a.qm = p->qm_ion; a.ds_lim = p->ds_lim; a.ds_max = (const double*)s->ds_bits; a.n_sub_out = s->n_sub;
@@ -631,7 +637,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   // electrons: push and purge (:1248-1293, 1534-1561)
   EleStepArgs b{};
   b.src = E.buf[E.cur]; b.dst = E.buf[1 - E.cur]; b.num_src = ne_src; b.num_dst = ne_dst;
-  b.Ex = s->Ex; b.Ey = s->Ey; b.Bx = b.By = b.Bz = nullptr; b.has_B = 0;
+  b.Ex = s->Ex; b.Ey = s->Ey; b.Ec = s->ecorn; b.Bx = b.By = b.Bz = nullptr; b.has_B = 0;
   b.isBound = s->isBound; b.nx = s->nx; b.ny = s->ny; b.dxf = dxf; b.dyf = dyf;
   b.inv_dx = 1.0f / dxf; b.inv_dy = 1.0f / dyf;
   b.dt = p->dt; b.qm = p->qm_e; b.ds_lim = p->ds_lim; b.ds_max = (const double*)(s->ds_bits + 1);
@@ -776,6 +782,7 @@ int32_t pb_sim_destroy(pb_sim* h) {
   for (double* q : d) if (q) cudaFree(q);
   float* fl[] = {s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->see_xy, s->angles};
   for (float* q : fl) if (q) cudaFree(q);
+  if (s->ecorn) cudaFree(s->ecorn);
   void* v[] = {s->isBound, s->bdist, s->bdist_tmp, s->cls, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->bar, s->counts, s->next_ids,
                s->tile_status, s->tile_counter, s->see_key, s->see_count, s->angle_scratch, s->angle_count,
                s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1], s->sval[0], s->sval[1],
@@ -843,6 +850,7 @@ int32_t pb_sim_set_domain(pb_sim* h, int32_t ny, int32_t nx, int32_t periodic, c
     for (double** q : dd) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(double))); }
     float** ff[] = {&s->Ex, &s->Ey, &s->rho, &s->Tmap, &s->r32, &s->z32, &s->p32, &s->q32, &s->e32};
     for (float** q : ff) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(float))); }
+    dfree(s->ecorn); CK(dalloc(&s->ecorn, 2 * N)); CK(cudaMemset(s->ecorn, 0, 2 * N * sizeof(float4)));
     dfree(s->isBound); CK(dalloc(&s->isBound, N));
     dfree(s->bdist); CK(dalloc(&s->bdist, N));
     dfree(s->bdist_tmp); CK(dalloc(&s->bdist_tmp, N));
@@ -1269,7 +1277,7 @@ int32_t pb_compute_particle_substeps(const float* x, const float* y, const float
   CK(cudaMallocAsync((void**)&bits, sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), st));
   int g = (int)std::min<long>((n + 255) / 256, 148L * 16);
-  k_substep_reduce<<<g, 256, 0, st>>>(x, y, vx, vy, vz, nullptr, n, Ex, Ey, nx, ny, (float)dx, (float)dy, qm, (float)dt,
+  k_substep_reduce<<<g, 256, 0, st>>>(x, y, vx, vy, vz, nullptr, n, Ex, Ey, nullptr, nx, ny, (float)dx, (float)dy, qm, (float)dt,
                                       dt * dt, bits);
   unsigned long long hb = 0;
   CK(cudaMemcpyAsync(&hb, bits, sizeof(hb), cudaMemcpyDeviceToHost, st));
