@@ -63,8 +63,23 @@ __global__ void k_e_corners(const float* __restrict__ Ex, const float* __restric
 // HAS_B = false: the B arrays are all +0 (the simulator never writes them), so
 // t = h * (+0) is a signed zero, t2 = +0 and 1 + t2 = 1 exactly; s = 2 t / 1 = 2 t.  The
 // remaining operations are kept, so signed zeros come out as in the reference.
+// floor(q) as an int and the fraction q - floor(q), exactly and without conversion
+// instructions, for 0 <= q < 2^22: adding 2^23 with rounding down leaves floor(q) in the
+// low mantissa bits of the sum, and q minus the floor is exact in float.  Returns false
+// for any other q (NaN included); the caller then takes the general path.
+__device__ __forceinline__ bool floor_frac(float q, int& fl, float& frac) {
+  if (!(q >= 0.0f && q < 4194304.0f)) return false;
+  const float t = __fadd_rd(q, 8388608.0f);
+  fl = __float_as_int(t) - 0x4B000000;
+  frac = __fsub_rn(q, __fsub_rn(t, 8388608.0f));
+  return true;
+}
+
 // CORN: E is gathered from the corner array Ec (B = 0 only); otherwise from Ex, Ey.
-template <bool HAS_B, bool CORN = false>
+// FLOOR: the cell index and fraction come from floor_frac inside the grid.  That takes
+// four conversions per substep off the XU pipe, which limits the electron kernel (many
+// substeps); kernels with fewer substeps and more live registers run faster without it.
+template <bool HAS_B, bool CORN = false, bool FLOOR = false>
 __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, float& vy, float& vz,
                                                const float* __restrict__ Ex, const float* __restrict__ Ey,
                                                const float* __restrict__ Bx, const float* __restrict__ By,
@@ -74,10 +89,24 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
   static_assert(!(HAS_B && CORN), "the corner gather has no B field");
   float ixf = __fdiv_rn(x, dxf);
   float iyf = __fdiv_rn(y, dyf);
-  int ix0 = clampi(np_f2i32(floorf(ixf)), 0, nx - 2);
-  int iy0 = clampi(np_f2i32(floorf(iyf)), 0, ny - 2);
-  double fx = DSUB((double)ixf, (double)ix0);
-  double fy = DSUB((double)iyf, (double)iy0);
+  int ix0, iy0;
+  double fx, fy;
+  {
+    // inside the grid the clamp is a no-op and ixf - ix0 is the exact float fraction
+    int fxi, fyi;
+    float frx, fry;
+    if (FLOOR && floor_frac(ixf, fxi, frx) && fxi <= nx - 2 && floor_frac(iyf, fyi, fry) && fyi <= ny - 2) {
+      ix0 = fxi;
+      iy0 = fyi;
+      fx = (double)frx;
+      fy = (double)fry;
+    } else {
+      ix0 = clampi(np_f2i32(floorf(ixf)), 0, nx - 2);
+      iy0 = clampi(np_f2i32(floorf(iyf)), 0, ny - 2);
+      fx = DSUB((double)ixf, (double)ix0);
+      fy = DSUB((double)iyf, (double)iy0);
+    }
+  }
   int ix1 = min(ix0 + 1, nx - 1);
   int iy1 = min(iy0 + 1, ny - 1);
   double gx = DSUB(1.0, fx), gy = DSUB(1.0, fy);
@@ -702,8 +731,8 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
       if (i < n) {
         float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
         for (int s = 0; s < n_sub; ++s)
-          boris_push_one<HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h,
-                                        dtf, a.Ec);
+          boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
+                                                a.dyf, h, dtf, a.Ec);
         if (a.periodic) y = np_modf_pos(y, a.Lyf);
         int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1), icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
         bool dead = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
