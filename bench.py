@@ -187,6 +187,7 @@ def gpu_arm(args):
     P = (_lib.StepParams * K)(*plist)
     R = (_lib.StepReport * K)()
     n_p0, n_e0 = sim.num_p, sim.num_e
+    stats_before = list(sim.last_report.poisson_stats) if sim.last_report is not None else None
     lib.pb_sim_set_profiling(sim._h, 1)
     clocks = ClockSampler(local)
     if world > 1:
@@ -257,6 +258,8 @@ def gpu_arm(args):
                        "parallelism": f"replicas x{world}", "l2": "particle state 8M x 25 B x 2 > L2 (126 MB)",
                        "sort_every": 20, "picard": "5 solves every 2nd step, FP32 MG-PCG + FP64 refinement"},
             "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": int(tm[8])}
+    if rank == 0 and world == 1 and stats_before is not None:
+        line["poisson"] = poisson_section(sim, stats_before, R, float(tm[2]), peak)
     if rank == 0 and world == 1 and not args.no_sweep:
         sim.close()
         line["sweep"] = sweep_section(local)
@@ -269,6 +272,46 @@ def gpu_arm(args):
     sim.close()
     if rank == 0:
         print(json.dumps(line))
+
+
+# ----------------------------------------------------------------------------- field solve
+POISSON_BYTES_LB = 9     # per unknown and linear solve: right-hand side read, phi written, class
+POISSON_BYTES_ITER = 72  # per unknown and PCG iteration: ~40 B of Krylov vectors + ~32 B of V-cycle
+
+
+def poisson_section(sim, stats_before, reports, field_ms, peak):
+    """Linear solves/s of the field solve inside the timed steps (recalc_poisson(5) every
+    second step, solving for the charge the particles just deposited): solves and PCG
+    iterations from the step reports' cumulative solver statistics, time from the
+    field-solve phase (CUDA events).  The solve is L2-resident and latency-bound (about 11
+    grid-wide phases per PCG iteration), so its bytes are reported against HBM for scale
+    only: the lower bound of 9 B per unknown and solve, and a model of 72 B per unknown
+    and PCG iteration."""
+    import ctypes as C
+    from thruster_cx_code_b200 import _lib
+    lib = _lib.load()
+    cls = np.empty((sim.ny, sim.nx), np.uint8)
+    _lib.check(lib.pb_sim_get_field(sim._h, 12, cls.ctypes.data_as(C.c_void_p), cls.nbytes), "get_field")
+    unknowns = int(np.count_nonzero(cls == 0))
+    last = reports[-1].poisson_stats
+    solves = last[3] - stats_before[3]
+    if solves <= 0 or field_ms <= 0:
+        return {"metric": "linear solves/s", "value": None}
+    its = (last[1] - stats_before[1]) / solves
+    passes = (last[0] - stats_before[0]) / solves
+    s_per_solve = field_ms * 1e-3 / solves
+    lb = POISSON_BYTES_LB * unknowns / s_per_solve / 1e9
+    model = POISSON_BYTES_ITER * unknowns * its / s_per_solve / 1e9
+    return {"metric": "linear solves/s", "value": 1.0 / s_per_solve, "unknowns": unknowns,
+            "solves_timed": solves, "ms_per_solve": s_per_solve * 1e3, "pcg_iterations_per_solve": its,
+            "refinement_passes_per_solve": passes, "tolerance": sim.solver["tol"],
+            "bound": "latency (L2-resident grid)", "peak_hbm_gbs": peak,
+            "lower_bound_bytes_per_solve": POISSON_BYTES_LB * unknowns, "lower_bound_gbs": lb,
+            "lower_bound_frac": lb / peak if peak else None,
+            "model_bytes_per_solve": POISSON_BYTES_ITER * unknowns * its, "model_gbs": model,
+            "model_frac": model / peak if peak else None,
+            "note": "time is the field-solve phase of the timed steps (Picard right-hand sides, FP64 "
+                    "refinement and E included)"}
 
 
 # ----------------------------------------------------------------------------- sweeps
