@@ -157,11 +157,20 @@ int32_t pb_sim_create(pb_sim** out, int32_t device);
 int32_t pb_sim_destroy(pb_sim* s);
 int32_t pb_sim_set_seed(pb_sim* s, uint64_t seed);
 
-/* Field solver controls: FP64 relative residual target, FP32 inner reduction, loop caps,
- * smoothing sweeps per level and the largest coarsest-level size (4 to 4096 active nodes;
- * default 1536; that level is solved with a dense inverse). */
+/* Field solver controls: FP64 relative residual target, FP32 reduction per refinement pass
+ * (default 1e-3), loop caps, smoothing sweeps per level (1: the fused cycle smooths once on
+ * each side of a coarse correction; other values are rejected) and the largest coarsest-level
+ * size (4 to 4096 active nodes; default 1536; that level is solved with a dense inverse).
+ * A new max_coarse takes effect at the next pb_sim_set_domain / pb_sim_rebuild_operator.
+ * Stands in for the reference's fixed SuperLU factorisation (physics_engine.py:603-608). */
 int32_t pb_sim_set_solver(pb_sim* s, double tol, double tol_inner, int32_t max_outer, int32_t max_inner,
                           int32_t nu, int32_t max_coarse);
+/* Launch shapes (the autotuner's knobs; the reference has no counterpart): blocks per SM
+ * of the ion and electron step kernels (1-32, default 8; tiles are handed out by a counter,
+ * so any grid covers every particle) and blocks of the field-solve launch (1 to the number
+ * of SMs, default all). Results do not depend on either, except the field solve's
+ * block-order sums, whose rounding follows the block count. */
+int32_t pb_sim_set_launch(pb_sim* s, int32_t particle_blocks_per_sm, int32_t solve_blocks);
 
 /* Upload the domain of build_domain (physics_engine.py:629-847): node masks, Dirichlet
  * values, electrode masks (bit g of gridmask = grid g), plus the state arrays to keep.

@@ -75,6 +75,7 @@ PROTOTYPES = {
     "pb_sim_destroy": (i32, [vp]),
     "pb_sim_set_seed": (i32, [vp, u64]),
     "pb_sim_set_solver": (i32, [vp, f64, f64, i32, i32, i32, i32]),
+    "pb_sim_set_launch": (i32, [vp, i32, i32]),
     "pb_sim_set_spline": (i32, [vp, i32, i32, P(f64), P(f64), f64, f64]),
     "pb_sim_set_domain": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, vp, vp, vp, i32]),
     "pb_sim_set_particles": (i32, [vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, u32]),

@@ -85,7 +85,8 @@ struct Sim {
   double* pstats = nullptr;
   unsigned long long* ptrace = nullptr;  // field-solve phase trace (32 slots)
   int trace_on = 0;
-  int pgrid = 0;
+  int pgrid = 0;      // blocks of the field-solve launch (<= num_sms)
+  int pbps = 8;       // step-kernel blocks per SM (the grid; tiles are handed out by a counter)
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
   // particles
   Species sp[2];
@@ -621,7 +622,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   a.seed = s->seed; a.step = (uint32_t)p->iteration;
   a.ppc = s->ppc; a.cnt = s->cnt_i;
   a.tile_status = s->tile_status; a.tile_counter = s->tile_counter; a.errflags = ef;
-  k_ion_step<false><<<grid_for(s, I.cap, TILE, 8), NT, 0, st>>>(a);
+  k_ion_step<false><<<grid_for(s, I.cap, TILE, s->pbps), NT, 0, st>>>(a);
   ++s->launches;
   mark(s);
 
@@ -644,7 +645,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
   b.errflags = ef;
-  k_ele_step<false><<<grid_for(s, E.cap, TILE, 8), NT, 0, st>>>(b);
+  k_ele_step<false><<<grid_for(s, E.cap, TILE, s->pbps), NT, 0, st>>>(b);
   ++s->launches;
 
   // SEE electrons, appended after the surviving electrons (:1390-1417)
@@ -807,10 +808,24 @@ int32_t pb_sim_set_seed(pb_sim* h, uint64_t seed) { h->s.seed = seed; return PB_
 int32_t pb_sim_set_solver(pb_sim* h, double tol, double tol_inner, int32_t max_outer, int32_t max_inner, int32_t nu,
                           int32_t max_coarse) {
   Sim* s = &h->s;
-  if (!(tol > 0) || !(tol_inner > 0) || max_outer < 1 || max_inner < 1 || nu < 1 || max_coarse < 4 || max_coarse > MG_MAX_COARSE)
+  if (!(tol > 0) || !(tol_inner > 0) || max_outer < 1 || max_inner < 1 || max_coarse < 4 || max_coarse > MG_MAX_COARSE)
     return fail(PB_ERR_ARG, "pb_sim_set_solver: invalid value");
+  if (nu != 1)
+    return fail(PB_ERR_ARG, "pb_sim_set_solver: nu must be 1 (the fused cycle smooths once on each side of a "
+                            "coarse correction)");
   s->tol = tol; s->tol_inner = tol_inner; s->max_outer = max_outer; s->max_inner = max_inner; s->nu = nu;
   s->max_coarse = max_coarse;
+  return PB_OK;
+}
+
+int32_t pb_sim_set_launch(pb_sim* h, int32_t particle_blocks_per_sm, int32_t solve_blocks) {
+  Sim* s = &h->s;
+  if (particle_blocks_per_sm < 1 || particle_blocks_per_sm > 32)
+    return fail(PB_ERR_ARG, "pb_sim_set_launch: particle_blocks_per_sm must be 1 to 32");
+  if (solve_blocks < 1 || solve_blocks > s->num_sms)
+    return fail(PB_ERR_ARG, "pb_sim_set_launch: solve_blocks must be 1 to " + std::to_string(s->num_sms));
+  s->pbps = particle_blocks_per_sm;
+  s->pgrid = solve_blocks;
   return PB_OK;
 }
 
