@@ -74,8 +74,11 @@ __device__ __forceinline__ int cell_round32_f(float s, float d, float inv_d, int
 __device__ __forceinline__ float np_maxf(float a, float b) { return (a != a || b != b) ? __int_as_float(0x7fc00000) : (a >= b ? a : b); }
 __device__ __forceinline__ double np_maxd(double a, double b) { return (a != a || b != b) ? __longlong_as_double(0x7ff8000000000000ll) : (a >= b ? a : b); }
 
-// np.mod for float32 with a positive divisor: fmod, then shift into [0, b)
+// np.mod for float32 with a positive divisor: fmod, then shift into [0, b).  For
+// 0 < a < b, fmod(a, b) is a itself, which skips the remainder routine for the particles
+// that did not cross the periodic boundary.
 __device__ __forceinline__ float np_modf_pos(float a, float b) {
+  if (a > 0.0f && a < b) return a;
   float m = fmodf(a, b);
   if (m != 0.0f) {
     if ((b < 0.0f) != (m < 0.0f)) m = __fadd_rn(m, b);

@@ -107,10 +107,11 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
                                                const float* __restrict__ Bz, int nx, int ny,
                                                float dxf, float dyf, double h, float dtf,
                                                const float4* __restrict__ Ec = nullptr, float inv_dx = 0.0f,
-                                               float inv_dy = 0.0f) {
+                                               float inv_dy = 0.0f, float* q_start = nullptr) {
   static_assert(!(HAS_B && CORN), "the corner gather has no B field");
   const float ixf = LIGHT ? div_rn_checked(x, dxf, inv_dx) : __fdiv_rn(x, dxf);
   const float iyf = LIGHT ? div_rn_checked(y, dyf, inv_dy) : __fdiv_rn(y, dyf);
+  if (q_start) { q_start[0] = ixf; q_start[1] = iyf; }  // x / dx, y / dy at the start position
   int ix0, iy0;
   double fx, fy;
   {
@@ -555,20 +556,26 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
         uint8_t cx = a.src.cex[i];
         const uint32_t pid = a.src.id[i];
         const float x0 = x, y0 = y;
-        for (int s = 0; s < n_sub; ++s)
+        float q0[2];  // x0 / dx, y0 / dy (correctly rounded), from the first substep
+        boris_push_one<HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h,
+                                      dtf, a.Ec, 0.0f, 0.0f, q0);
+        for (int s = 1; s < n_sub; ++s)
           boris_push_one<HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h,
                                         dtf, a.Ec);
         if (a.periodic) y = np_modf_pos(y, a.Lyf);
+        // the final cell, the PPC cell and the deposit cell all round or truncate the same
+        // correctly rounded quotients (what rint_div and trunc_div return)
+        const float qx = div_rn_checked(x, a.dxf, a.inv_dx), qy = div_rn_checked(y, a.dyf, a.inv_dy);
         // entered the optics (:1316-1324)
         if (x0 < a.x_entry && x >= a.x_entry && vx > 0.0f) cnt[0]++;
         // final-cell and path hits (:1326-1336).  The 8 path samples lie in cells at most
         // max(|di|, |dj|) + 1 (Chebyshev) from the start cell; they are examined only when
         // that reaches the distance from the start cell to the nearest bound node.
-        const int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1);
-        const int icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
+        const int icx = (int)clampll(np_f2i64(rintf(qx)), 0, a.nx - 1);
+        const int icy = (int)clampll(np_f2i64(rintf(qy)), 0, a.ny - 1);
         const bool hit_final = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
-        const int sx0 = cell_round_f(x0, a.dxf, a.inv_dx, 0, a.nx - 1);
-        const int sy0 = cell_round_f(y0, a.dyf, a.inv_dy, 0, a.ny - 1);
+        const int sx0 = (int)clampll(np_f2i64(rintf(q0[0])), 0, a.nx - 1);
+        const int sy0 = (int)clampll(np_f2i64(rintf(q0[1])), 0, a.ny - 1);
         const int reach = max(abs(icx - sx0), abs(icy - sy0)) + 1;
         SegHit sh;
         sh.hit = false; sh.ix = icx; sh.iy = icy;
@@ -682,11 +689,10 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
             }
           }
           // PPC map with truncated cells (:1749-1757), next-step deposit cell (rounded)
-          long long tx = clampll(np_f2i64(trunc_div(x, a.dxf, a.inv_dx)), 0, a.nx - 1);
-          long long ty = clampll(np_f2i64(trunc_div(y, a.dyf, a.inv_dy)), 0, a.ny - 1);
+          long long tx = clampll(np_f2i64(truncf(qx)), 0, a.nx - 1);
+          long long ty = clampll(np_f2i64(truncf(qy)), 0, a.ny - 1);
           ppc_cell = (int)(ty * a.nx + tx);
-          dep_cell = cell_round32_f(y, a.dyf, a.inv_dy, 1, a.ny - 2) * a.nx +
-                     cell_round32_f(x, a.dxf, a.inv_dx, 1, a.nx - 2);
+          dep_cell = clampi(np_f2i32(rintf(qy)), 1, a.ny - 2) * a.nx + clampi(np_f2i32(rintf(qx)), 1, a.nx - 2);
         }
         st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
         st.cex[k] = cx; st.id[k] = pid;
