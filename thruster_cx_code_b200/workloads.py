@@ -8,6 +8,10 @@ thick, 6.25 um spacing chosen so the derived domain is exactly 257 x 1025 nodes
 (256 x 1024 cells), 8M FP32 macro-particles (6M Xe+ and 2M electrons at mass ratio
 1/400), CEX cross-section 7e-19 E^-0.1 m^2 as a log-log table over 1-1000 eV, sputtering on.
 
+``long_erosion_3grid``: the same 3-grid stack at 3.125 um spacing (513 x 2049 nodes,
+512 x 2048 cells), 64M FP32 macro-particles (48M Xe+ and 16M electrons), CEX neutral
+density 5e18 m^-3, sputtering and grid heating with conduction on ("Both").
+
 Particles are pre-loaded from a seeded NumPy generator: positions uniform over the
 non-electrode cells, ion velocities N(v_Bohm, v_th), electron velocities thermal.
 
@@ -49,6 +53,14 @@ WORKLOADS = {
                            dict(V=0.0, t=0.5, gap=0.5, r=0.7, cham=0.0)],
                     pitch_mm=4.0, upstream_gap_mm=0.4, Te_up=5.0, n0_plasma=1e17, Ti=0.1, Tn=300.0,
                     n0=1e18, sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9)),
+    "long_erosion_3grid": dict(
+        dx=0.003125, dy=0.003125, dt=1.25e-11, m_e_ratio=400.0, n_ions=48_000_000, n_e=16_000_000,
+        cx=cx_table_power_law(),
+        params=dict(grids=[dict(V=1000.0, t=0.5, gap=0.5, r=0.8, cham=0.0),
+                           dict(V=-250.0, t=0.5, gap=0.5, r=0.5, cham=0.0),
+                           dict(V=0.0, t=0.5, gap=0.5, r=0.7, cham=0.0)],
+                    pitch_mm=4.0, upstream_gap_mm=0.4, Te_up=5.0, n0_plasma=1e17, Ti=0.1, Tn=300.0,
+                    n0=5e18, sim_mode="Both", neut_rate=30, Te=5.0, Thresh=1e9)),
 }
 
 
