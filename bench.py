@@ -317,6 +317,10 @@ def poisson_section(sim, stats_before, reports, field_ms, peak):
 # ----------------------------------------------------------------------------- sweeps
 SWEEP_POINTS, SWEEP_WARMUP, SWEEP_STEPS, SWEEP_REF_STEPS = 16, 2, 40, 3000
 SERVE_REQUESTS, SERVE_RATE_HZ, SERVE_MAX_STEPS = 12, 20.0, 100
+# Served requests live for at most a few hundred steps, so their host set-up weighs more
+# than their stepping: a coarsest multigrid level of <= 256 nodes builds its dense inverse
+# in milliseconds instead of about 0.1-0.2 s (17 x 65 nodes), for one more level per V-cycle.
+SERVE_SOLVER = {"max_coarse": 256}
 
 
 def _run_plain(sim, params, K):
@@ -348,10 +352,10 @@ def sweep_section(device):
     perveance-sweep points (C3 draws, 0.2M-1M macro-particles).  Rates use the device time
     of 40 steps after 2 warm-up steps, scaled to 3000 steps per point; setup is not
     included.  Then a served run: 12 backstreaming-limit requests arriving as a Poisson
-    stream at 20 per second, admitted under a 150 GB budget, built on up to 8 setup threads,
-    stepped in chunks of 10 and
-    retired when the saddle potential and current change less than 5% between the halves
-    of a 60-step window (or at 100 steps).  Its latencies include setup."""
+    stream at 20 per second, admitted under a 150 GB budget, built on up to 8 setup threads
+    (with a coarsest multigrid level of <= 256 nodes, SERVE_SOLVER), stepped in chunks of 10
+    and retired when the saddle potential and current change less than 5% between the
+    halves of a 60-step window (or at 100 steps).  Its latencies include setup."""
     from thruster_cx_code_b200 import serving as SV
     from thruster_cx_code_b200 import workloads as W
     rng = np.random.default_rng(7)
@@ -390,7 +394,8 @@ def sweep_section(device):
         j = rs.uniform(0.1, 1.0)  # neutralizer electron current density, A/m^2
         area = 0.5 * 0.95e-3 * 1e-3 + 0.3 * 3.75e-3 * 1e-3
         sp["params"]["neut_rate"] = max(1, int(round(j * area * sp["dt"] / (1.602e-19 * 1e3))))
-        req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device)), W.sweep_point_bytes(sp), SERVE_MAX_STEPS,
+        req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device, solver=SERVE_SOLVER)),
+                         W.sweep_point_bytes(sp), SERVE_MAX_STEPS,
                          SV.Convergence(window=60, tol=0.05, keys=("current", "saddle")))
         arrivals.append((t, req))
     srv = SV.SweepServer(device, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=batch,

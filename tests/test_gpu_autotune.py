@@ -7,6 +7,7 @@
 * Out-of-range launch shapes and nu != 1 are rejected.
 * A tuning run over two knobs applies and caches the best setting, and the tuned simulator
   keeps stepping.
+* With a short horizon the multigrid build time counts, and a small coarsest level wins.
 """
 import ctypes as C
 
@@ -90,3 +91,15 @@ def test_tune_two_knobs(mods):
     assert A.current(twin)["max_coarse"] == best["max_coarse"]
     sim.close()
     twin.close()
+
+
+def test_horizon_prefers_a_quick_build(mods):
+    """Over a 50-step horizon the dense inverse of a 17 x 65 coarsest level (about 0.1 s on
+    the host) costs more per step than the extra V-cycle level of a <= 256-node one."""
+    _lib, A = mods
+    sim, params = W.make_sweep_sim(_spec())
+    sim.step(params)
+    tuner = A.Autotuner(steps=2, warmup=1, horizon_steps=50, space={"max_coarse": (1536, 256)})
+    best, table = tuner.tune(sim, params)
+    assert best["max_coarse"] == 256, table
+    sim.close()

@@ -18,6 +18,10 @@ which changes only the array order.  The field solve reaches the same FP64 toler
 whatever ``max_coarse``, ``tol_inner`` and ``solve_blocks`` are, but its rounding follows
 them.
 
+With ``horizon_steps`` set, the cost of a setting is its step time plus its multigrid
+build time (host, measured) spread over that many steps: short-lived simulators, such as
+served requests, favour a small coarsest level that builds in milliseconds.
+
 ``Autotuner.tune(sim, params)`` saves a checkpoint of ``sim``, then, by coordinate descent
 (one knob at a time, the others at their best so far), restores a fresh copy from it for
 every candidate, runs warm-up steps and times ``steps`` steps on the device
@@ -144,7 +148,8 @@ def workload_key(sim):
 
 
 class Autotuner:
-    def __init__(self, steps=6, warmup=2, passes=1, min_gain=0.01, space=None, device=0):
+    def __init__(self, steps=6, warmup=2, passes=1, min_gain=0.01, space=None, device=0, horizon_steps=None):
+        self.horizon = int(horizon_steps) if horizon_steps else None
         self.steps = int(steps)
         self.warmup = int(warmup)
         self.passes = int(passes)
@@ -156,7 +161,8 @@ class Autotuner:
 
     def measure(self, ckpt, knobs, base_solver=None):
         """ms per step of a fresh copy restored from ``ckpt`` with ``knobs`` applied (the
-        remaining solver settings taken from ``base_solver``)."""
+        remaining solver settings taken from ``base_solver``), plus the multigrid build
+        time spread over ``horizon_steps`` when that is set."""
         from .physics_engine import DigitalTwinSimulator
         trial, params = DigitalTwinSimulator.load_checkpoint(ckpt, device=self.device)
         try:
@@ -165,9 +171,16 @@ class Autotuner:
                 s.update({k: base_solver[k] for k in ("tol", "max_outer", "max_inner")})
                 trial.solver = s
             apply(trial, knobs)
+            build_ms = 0.0
+            if self.horizon:
+                import time
+                t0 = time.perf_counter()
+                _lib.check(_lib.load().pb_sim_rebuild_operator(trial._h), "rebuild_operator")
+                build_ms = (time.perf_counter() - t0) * 1e3
             if self.warmup:
                 run_timed(trial, params, self.warmup)
-            return run_timed(trial, params, self.steps) / self.steps
+            ms = run_timed(trial, params, self.steps) / self.steps
+            return ms + (build_ms / self.horizon if self.horizon else 0.0)
         finally:
             trial.close()
 

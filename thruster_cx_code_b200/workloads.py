@@ -144,10 +144,11 @@ def sweep_point_bytes(spec):
     return int(2 * 1.25 * (25 * spec["n_ions"] + 24 * spec["n_e"]) + 800 * nodes + (64 << 20))
 
 
-def make_sweep_sim(spec, device=0, sort_every=20):
-    """Build a sweep point on the device: returns (simulator, params)."""
+def make_sweep_sim(spec, device=0, sort_every=20, solver=None):
+    """Build a sweep point on the device: returns (simulator, params).  ``solver``: field
+    solver settings other than the defaults (see DigitalTwinSimulator)."""
     from .physics_engine import DigitalTwinSimulator
-    sim = DigitalTwinSimulator(device=device, seed=spec["seed"], sort_every=sort_every)
+    sim = DigitalTwinSimulator(device=device, seed=spec["seed"], sort_every=sort_every, solver=solver)
     sim.dx = sim.dy = spec["dx"]
     sim.dt = spec["dt"]
     sim.m_ion = M_XE
