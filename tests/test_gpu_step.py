@@ -4,7 +4,9 @@
   SuperLU result (fixtures), |V - V_ref| <= 1e-7 max|V| and |E - E_ref| <= 1e-5 max|E|.
 * One timestep given identical fields (an odd step, so no field solve inside): particles
   compared per id bit-for-bit, deposit bit-exact, counters exact, Tmap within 1e-6
-  (float atomics order and the last ulp of T**4), damage within 1e-12.
+  (float atomics order and the last ulp of T**4), damage within 1e-12.  Again with
+  particles on and around cell boundaries and the domain edges, where the step kernels'
+  exact shortcuts take their fallback branches.
 * Eight timesteps with each side solving its own fields: per-id positions within 1e-4.
 * The cell sort reproduces np.argsort(key, kind="stable").
 """
@@ -137,6 +139,72 @@ def test_one_step_bit_exact_given_fields(gpu_mod, name):
     np.testing.assert_allclose(g.damage_map, o.damage_map, rtol=1e-12, atol=0)
     np.testing.assert_array_equal(g.isBound, o.isBound)
     assert g.transmitted_ions == o.transmitted_ions and g.entered_optics == o.entered_optics
+
+
+def _edge_particles(g, n, rng):
+    """Positions on exact cell boundaries k * dx (float32), one ulp either side, at zero,
+    just outside the domain and on the far edges, paired over x and y; velocities small,
+    zero or mixed in sign.  They reach the fallback branches of the step kernels' exact
+    shortcuts (checked division, round-down floor, quotient reuse, periodic wrap)."""
+    dx, dy = np.float32(g.dx), np.float32(g.dy)
+    Lx, Ly = np.float32(g.Lx), np.float32(g.Ly)
+
+    def edges(d, m, L):
+        b = np.array([k * d for k in (0, 1, 2, m // 2, m - 2, m - 1)], np.float32)
+        b = np.concatenate([b, np.nextafter(b, np.float32(np.inf)), np.nextafter(b, np.float32(-np.inf)),
+                            np.array([-1e-6, L, np.nextafter(L, np.float32(np.inf)), L + d], np.float32)])
+        return b
+
+    xs, ys = edges(dx, g.nx, Lx), edges(dy, g.ny, Ly)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")
+    X, Y = X.ravel(), Y.ravel()
+    k = rng.choice(X.size, size=min(n, X.size), replace=False)
+    X, Y = X[k], Y[k]
+    v = rng.choice(np.array([0.0, 1.0, -1.0], np.float32), size=(3, X.size)).astype(np.float32)
+    return X, Y, v
+
+
+@pytest.mark.parametrize("name", ["c1_both", "two_holes_thermal"])
+def test_one_step_bit_exact_at_cell_boundaries(gpu_mod, name):
+    """One step, identical fields, with particles placed on and around cell boundaries and
+    the domain edges appended to the case's own: per-id state bit-exact."""
+    f, case, params = _case(name)
+    PE = gpu_mod
+    g = PE.DigitalTwinSimulator(seed=SEED, sort_every=0)
+    o = O.OracleSimulator(build_domain_geometry)
+    for s in (g, o):
+        s.dx, s.dy, s.dt = case["dx"], case["dy"], case["dt"]
+        if "cx_table" in case:
+            s.user_cs = cx_store(case["cx_table"])
+    g.build_domain(params)
+    o.build_domain(params)
+    rng = np.random.default_rng(3)
+    p = f["init_p"].astype(np.float32)
+    e = f["init_e"].astype(np.float32)
+    xi, yi, vi = _edge_particles(g, 150, rng)
+    xe, ye, ve = _edge_particles(g, 150, rng)
+    pi = np.concatenate([p, np.stack([xi, yi, 2e3 * vi[0] + 1e3, 2e3 * vi[1], 2e3 * vi[2]]).astype(np.float32)], axis=1)
+    pe = np.concatenate([e, np.stack([xe, ye, 3e5 * ve[0], 3e5 * ve[1], 3e5 * ve[2]]).astype(np.float32)], axis=1)
+    cex = np.concatenate([f["init_p_cex"], np.zeros(xi.size, bool)])
+    n, ne = pi.shape[1], pe.shape[1]
+    g.set_particles("ions", *pi, is_cex=cex, ids=np.arange(n), sort=False)
+    g.set_particles("electrons", *pe, ids=np.arange(ne), sort=False)
+    o._add_ions(*pi, cex, o.new_ion_ids(n))
+    o._add_electrons(*pe, o.new_e_ids(ne))
+    g.V, g.Ex, g.Ey = o.V, o.Ex, o.Ey
+    g.step(params)
+    o.step(params, O.PhiloxDraws(SEED))
+    assert g.num_p == o.num_p and g.num_e == o.num_e
+    np.testing.assert_array_equal(g.rho, o.rho)
+    ag, _, ig = _ions(g)
+    ao, _, io = _ions(o)
+    np.testing.assert_array_equal(ig, io)
+    np.testing.assert_array_equal(ag.view(np.uint32), ao.view(np.uint32))
+    eg, jg = _eles(g)
+    eo, jo = _eles(o)
+    np.testing.assert_array_equal(jg, jo)
+    np.testing.assert_array_equal(eg.view(np.uint32), eo.view(np.uint32))
+    np.testing.assert_array_equal(g.current_ppc_map, o.current_ppc_map)
 
 
 @pytest.mark.parametrize("name", ["c1_both", "one_hole_rf", "two_holes_thermal"])
