@@ -22,6 +22,7 @@ from tests.helpers import cx_store, load
 pytestmark = pytest.mark.gpu
 
 SEED = 20240611
+PB_ERR_ARG = 2  # include/pbemcs.h
 
 
 @pytest.fixture(scope="module")
@@ -262,3 +263,26 @@ def test_upload_sort_is_stable_argsort(gpu_mod):
     np.testing.assert_array_equal(b.view(np.uint32), a[:, perm].view(np.uint32))
     np.testing.assert_array_equal(ib, ia[perm])
     np.testing.assert_array_equal(cb, ca[perm])
+
+
+def test_bad_step_params_rejected(gpu_mod):
+    """Indices the kernels dereference are checked before anything of the step is enqueued:
+    the call fails and the simulator keeps stepping."""
+    import ctypes as C
+    from thruster_cx_code_b200 import _lib
+    g, _, params = _pair(gpu_mod, "c1_both")
+    lib = _lib.load()
+    n0 = g.num_p
+    for field, value in (("saddle_idx", 10 ** 9), ("rf_grid", 40)):
+        P = g.step_params(params)
+        if field == "saddle_idx":
+            P.n_saddle = 1
+            P.saddle_idx[0] = value
+        else:
+            P.rf_grid = value
+        rep = _lib.StepReport()
+        assert lib.pb_sim_step(g._h, C.byref(P), C.byref(rep)) == PB_ERR_ARG
+    assert g.num_p == n0
+    g.step(params)
+    assert g.num_p > 0
+    g.close()

@@ -230,6 +230,9 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     b->ev_solve.push_back(e);
   }
   if (reports && (rc = grow_pinned(&b->hrep, &b->rep_cap, (size_t)n * K))) return rc;
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < K; ++k)
+      if ((rc = check_step_params(&sims[i]->s, &params[(size_t)i * K + k]))) return rc;
   // ---- enqueue
   CK(cudaEventRecord(b->ev0, b->stream));
   if (nargs > 0) {

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -352,15 +353,49 @@ static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
   return PB_OK;
 }
 
+// The per-step resets in one launch instead of a dozen memsets (each of which is an
+// operation of its own on the GPU timeline): the step report (zero, ppc_min all ones),
+// the PPC map, both step kernels' tile descriptors and the small counters.
+struct StepResetArgs {
+  pb_step_report* rep;
+  int* ppc;
+  int N;
+  unsigned long long* tile_status;
+  long long ntile;
+  int *angle_count, *see_count, *see_spawned, *tile_counter, *ni_dst, *ne_dst, *inj;
+  unsigned long long* ds_bits;
+};
+
+__global__ void k_step_reset(StepResetArgs a) {
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
+  static_assert(sizeof(pb_step_report) % 4 == 0 && offsetof(pb_step_report, ppc_min) % 4 == 0, "report words");
+  constexpr long long nw = sizeof(pb_step_report) / 4, w0 = offsetof(pb_step_report, ppc_min) / 4;
+  uint32_t* r = reinterpret_cast<uint32_t*>(a.rep);
+  for (long long i = tid; i < nw; i += nth) r[i] = (i == w0 || i == w0 + 1) ? 0xFFFFFFFFu : 0u;
+  for (long long i = tid; i < a.N; i += nth) a.ppc[i] = 0;
+  for (long long i = tid; i < a.ntile; i += nth) a.tile_status[i] = 0ull;
+  if (tid == 0) {
+    *a.angle_count = 0; *a.see_count = 0; *a.see_spawned = 0;
+    a.ds_bits[0] = 0ull; a.ds_bits[1] = 0ull;
+    a.tile_counter[0] = 0; a.tile_counter[1] = 0;
+    *a.ni_dst = 0; *a.ne_dst = 0;
+    for (int k = 0; k < 7; ++k) a.inj[k] = 0;
+  }
+}
+
 // RF: V_fixed on grid g = Vdc + v_rf
 __global__ void k_rf_update(double* Vfixed, const double* Vdc, const uint16_t* gridmask, int N, int g, double v_rf) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     if (gridmask[i] & (1u << g)) Vfixed[i] = Vdc[i] + v_rf;
 }
 
+struct SaddleIdx { int v[8]; };
+
+// The step report's device-side fields, the saddle potential (the minimum of V over up to
+// eight saddle nodes; 0 without any) and the solver statistics, in one thread.
 __global__ void k_report(pb_step_report* r, const int* counts, int ci, int ce, const int* n_sub,
                          const unsigned long long* ds_bits, const int* inj, const int* see_spawned, const double* V,
-                         int n_saddle, const int* saddle_idx8, const double* pstats, int rf_on) {
+                         int n_saddle, SaddleIdx sidx, const double* pstats) {
   r->num_p = counts[ci];
   r->num_e = counts[2 + ce];
   r->n_sub_ion = n_sub[0];
@@ -373,22 +408,17 @@ __global__ void k_report(pb_step_report* r, const int* counts, int ci, int ce, c
   r->see_spawned = *see_spawned;
   double mp = 0.0;
   for (int k = 0; k < n_saddle; ++k) {
-    double v = V[saddle_idx8[k]];
+    double v = V[sidx.v[k]];
     mp = (k == 0 || v < mp) ? v : mp;
   }
   r->min_pot = mp;
   for (int k = 0; k < 4; ++k) r->poisson_stats[k] = pstats[k];
-  (void)rf_on;
 }
 
-struct SaddleIdx { int v[8]; };
-__global__ void k_report_saddle(pb_step_report* r, const double* V, int n, SaddleIdx idx) {
-  double mp = 0.0;
-  for (int k = 0; k < n; ++k) {
-    double v = V[idx.v[k]];
-    mp = (k == 0 || v < mp) ? v : mp;
-  }
-  r->min_pot = mp;
+// n_sub of both species from their reduced displacements, one thread
+__global__ void k_substep_finish2(const double* ds_max, double ds_lim, int* n_sub_out, uint32_t* errflags) {
+  n_sub_out[0] = substep_count(ds_max[0], ds_lim, errflags);
+  n_sub_out[1] = substep_count(ds_max[1], ds_lim, errflags);
 }
 
 }  // namespace pb
@@ -473,8 +503,20 @@ static void mark(Sim* s) {
 
 // A step is enqueued in two halves around the field solve, so that a batch can solve the
 // fields of several instances in one launch between them.
+// Indices in the step parameters that kernels dereference, checked before anything of the
+// step is enqueued.
+static int32_t check_step_params(const Sim* s, const pb_step_params* p) {
+  const long N = (long)s->ny * s->nx;
+  const int ns = std::max(0, std::min(p->n_saddle, 8));
+  for (int k = 0; k < ns; ++k)
+    if (p->saddle_idx[k] < 0 || p->saddle_idx[k] >= N) return fail(PB_ERR_ARG, "step: saddle index outside the grid");
+  if (p->rf_grid < -1 || p->rf_grid > 15) return fail(PB_ERR_ARG, "step: rf_grid must be -1 (off) or 0 to 15");
+  return PB_OK;
+}
+
 static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
   Sim* s = &h->s;
+  if (int32_t rc = check_step_params(s, p)) return rc;
   mark(s);
   cudaStream_t st = s->stream;
   const int N = s->ny * s->nx;
@@ -490,19 +532,16 @@ static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
   pb_step_report* rep = s->rep_dev;
   uint32_t* ef = &rep->errflags;
 
-  // per-step resets
-  CK(cudaMemsetAsync(rep, 0, sizeof(pb_step_report), st));
-  CK(cudaMemsetAsync(&rep->ppc_min, 0xFF, sizeof(uint64_t), st));
-  CK(cudaMemsetAsync(s->ppc, 0, (size_t)N * sizeof(int), st));
-  CK(cudaMemsetAsync(s->angle_count, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(s->see_count, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(s->see_spawned, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(s->ds_bits, 0, 2 * sizeof(unsigned long long), st));
-  CK(cudaMemsetAsync(s->tile_counter, 0, 2 * sizeof(int), st));
-  CK(cudaMemsetAsync(s->tile_status, 0, 2 * s->tile_cap * sizeof(unsigned long long), st));
-  CK(cudaMemsetAsync(ni_dst, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(ne_dst, 0, sizeof(int), st));
-  CK(cudaMemsetAsync(s->inj, 0, 7 * sizeof(int), st));
+  // per-step resets, one launch
+  {
+    StepResetArgs r{};
+    r.rep = rep; r.ppc = s->ppc; r.N = N;
+    r.tile_status = s->tile_status; r.ntile = 2 * (long long)s->tile_cap;
+    r.angle_count = s->angle_count; r.see_count = s->see_count; r.see_spawned = s->see_spawned;
+    r.ds_bits = s->ds_bits; r.tile_counter = s->tile_counter; r.ni_dst = ni_dst; r.ne_dst = ne_dst; r.inj = s->inj;
+    k_step_reset<<<grid_for(s, std::max<long>(N, 2 * (long)s->tile_cap), 256), 256, 0, st>>>(r);
+    ++s->launches;
+  }
 
   if (!s->counts_valid) {
     CK(cudaMemsetAsync(s->cnt_i, 0, (size_t)N * sizeof(int), st));
@@ -587,9 +626,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
       E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf, dyf, p->qm_e, dtf, p->dt2,
       s->ds_bits + 1);
   ++s->launches;
-  k_substep_finish<<<1, 1, 0, st>>>((const double*)s->ds_bits, p->ds_lim, s->n_sub, ef);
-  ++s->launches;
-  k_substep_finish<<<1, 1, 0, st>>>((const double*)(s->ds_bits + 1), p->ds_lim, s->n_sub + 1, ef);
+  k_substep_finish2<<<1, 1, 0, st>>>((const double*)s->ds_bits, p->ds_lim, s->n_sub, ef);
   ++s->launches;
   mark(s);
 
@@ -676,15 +713,11 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   // exit divergence, saddle potential, PPC map (:1482-1488, 1655-1676, 1741-1767)
   k_theta95<<<1, 1024, 0, st>>>(s->angles, s->angle_count, s->angle_cap, s->angle_scratch, &rep->theta95);
   ++s->launches;
-  k_report<<<1, 1, 0, st>>>(rep, s->counts, I.cur, E.cur, s->n_sub, s->ds_bits, s->inj, s->see_spawned, s->V,
-                            0, nullptr, s->pstats, 0);
-  ++s->launches;
   SaddleIdx sidx{};
   for (int k = 0; k < 8; ++k) sidx.v[k] = p->saddle_idx[k];
-  if (p->n_saddle > 0) {
-    k_report_saddle<<<1, 1, 0, st>>>(rep, s->V, p->n_saddle, sidx);
-    ++s->launches;
-  }
+  k_report<<<1, 1, 0, st>>>(rep, s->counts, I.cur, E.cur, s->n_sub, s->ds_bits, s->inj, s->see_spawned, s->V,
+                            std::max(0, std::min(p->n_saddle, 8)), sidx, s->pstats);
+  ++s->launches;
   k_ppc_stats<<<grid_for(s, N, 256), 256, 0, st>>>(s->ppc, s->accum_ppc, N, (unsigned long long*)&rep->ppc_active);
   ++s->launches;
 
@@ -1103,6 +1136,8 @@ int32_t pb_sim_run(pb_sim* h, const pb_step_params* params, int32_t nsteps, pb_s
   if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_run: no domain");
   int32_t rc;
   if (nsteps <= 0) return PB_OK;
+  for (int k = 0; k < nsteps; ++k)
+    if ((rc = check_step_params(s, &params[k]))) return rc;
   if ((rc = ensure_room(s, &params[0], nsteps))) return rc;
   // reports go to pinned memory, so the copies do not block the host between steps
   if (reports && s->rep_run_cap < nsteps) {
