@@ -323,11 +323,13 @@ SERVE_REQUESTS, SERVE_RATE_HZ, SERVE_MAX_STEPS = 12, 20.0, 100
 SERVE_SOLVER = {"max_coarse": 256}
 
 
-def _run_plain(sim, params, K):
-    """K steps of one simulator through pb_sim_run; returns the device time (ms)."""
+def _run_plain(sim, params, K, pushes_out=None):
+    """K steps of one simulator through pb_sim_run; returns the device time (ms) and, if
+    ``pushes_out`` is a list, appends the particle-pushes of those steps."""
     import ctypes as C
     from thruster_cx_code_b200 import _lib
     lib = _lib.load()
+    n_p0, n_e0 = sim.num_p, sim.num_e
     it0 = sim.iteration
     plist = []
     for k in range(K):
@@ -343,6 +345,8 @@ def _run_plain(sim, params, K):
     sim._invalidate()
     for r in R:
         sim._apply_report(r, params)
+    if pushes_out is not None:
+        pushes_out.append(pushes_of(R, n_p0, n_e0))
     return float(tm[0])
 
 
@@ -351,7 +355,8 @@ def sweep_section(device):
     batched (all points together through pb_batch_run), on two identical sets of 16
     perveance-sweep points (C3 draws, 0.2M-1M macro-particles).  Rates use the device time
     of 40 steps after 2 warm-up steps, scaled to 3000 steps per point; setup is not
-    included.  Then a served run: 12 backstreaming-limit requests arriving as a Poisson
+    included.  The same steps are also given as particle-pushes/s and as the fraction of
+    HBM peak their algorithmic bytes (41 B per push) would take.  Then a served run: 12 backstreaming-limit requests arriving as a Poisson
     stream at 20 per second, admitted under a 150 GB budget, built on up to 8 setup threads
     (with a coarsest multigrid level of <= 256 nodes, SERVE_SOLVER), stepped in chunks of 10
     and retired when the saddle potential and current change less than 5% between the
@@ -364,14 +369,17 @@ def sweep_section(device):
     plain = [W.make_sweep_sim(sp, device) for sp in specs]
     for s, p in plain:
         _run_plain(s, p, SWEEP_WARMUP)
-    plain_ms = sum(_run_plain(s, p, SWEEP_STEPS) for s, p in plain)
+    plain_pushes = []
+    plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes) for s, p in plain)
     for s, _ in plain:
         s.close()
     together = [W.make_sweep_sim(sp, device) for sp in specs]
     sims, prm = [s for s, _ in together], [p for _, p in together]
     batch.run(sims, prm, SWEEP_WARMUP)
-    batch.run(sims, prm, SWEEP_STEPS)
+    n0 = [(s.num_p, s.num_e) for s in sims]
+    res = batch.run(sims, prm, SWEEP_STEPS)
     batched_ms = batch.last_ms
+    batched_pushes = sum(SV.pushes_of([rep for _, rep in r], a, b) for r, (a, b) in zip(res, n0))
     for s in sims:
         s.close()
     per_point_plain_s = plain_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / SWEEP_POINTS
@@ -382,6 +390,13 @@ def sweep_section(device):
            "batched_points_per_hr": 3600.0 / per_point_batched_s,
            "batched_over_plain": plain_ms / batched_ms,
            "setup": "excluded (host geometry, multigrid build and pre-load)"}
+    # the same steps as particle-pushes/s, and their algorithmic bytes (41 B per push) against HBM
+    peak, _ = measured_peak_gbs()
+    for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms), ("batched", float(batched_pushes),
+                                                                             batched_ms)):
+        rate = pushes / (ms * 1e-3)
+        out[f"{name}_pushes_per_s"] = rate
+        out[f"{name}_hbm_frac"] = rate * ALG_BYTES_PER_ION / 1e9 / peak if peak else None
     # ---- served
     rs = np.random.default_rng(11)
     arrivals = []
