@@ -79,7 +79,7 @@ int64_t sim_device_bytes(const Sim* s) {
   b += N * (9 * 8 + 9 * 4 + 32 + 4 + 2 + 3 * 4);  // double and float fields, E corners, masks, count maps
   for (size_t l = 0; l < s->lev.size(); ++l) {
     const int64_t Nl = (int64_t)s->lev[l].ny * s->lev[l].nx;
-    b += Nl * 4 * (1 + (l ? 11 : 0)) + (l ? Nl : 0);
+    b += Nl * 4 * (1 + (l ? 2 : 0));  // dinv; r and z below the fine level
     b += Nl * 4 * ((s->lev[l].R ? 25 : 0) + (s->lev[l].U ? 18 : 0));
   }
   b += (int64_t)s->nc * s->nc * 4;

@@ -23,7 +23,7 @@ namespace pb {
 namespace mghost {
 
 struct Level {
-  int ny = 0, nx = 0, per = 0, wrapP = 0, ncolors = 2;
+  int ny = 0, nx = 0, per = 0, wrapP = 0;
   std::vector<uint8_t> act;   // active nodes (level 0: free nodes)
   std::vector<float> st;      // 9 * N stencil (coarse levels)
   std::vector<float> dinv;    // omega / diagonal on active nodes (damped Jacobi smoother)
@@ -106,11 +106,6 @@ inline int p_row(int nyf, int nxf, int wrap, int nyc, int nxc, int y, int x, lon
   }
   (void)nyf; (void)nxf;
   return n;
-}
-
-inline int colors_for(const Level& L, int level) {
-  if (level == 0) return 2;
-  return (L.per && (L.ny & 1)) ? 6 : 4;
 }
 
 // The transfers of the fused V-cycle as explicit stencils, for fine levels l >= 1 (where
@@ -250,7 +245,7 @@ inline std::vector<float> spd_inverse(const std::vector<double>& A, int n) {
 inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>& cls0, int max_coarse) {
   Hierarchy H;
   Level L0;
-  L0.ny = ny; L0.nx = nx; L0.per = periodic; L0.wrapP = 0; L0.ncolors = 2;
+  L0.ny = ny; L0.nx = nx; L0.per = periodic; L0.wrapP = 0;
   L0.act.resize((size_t)ny * nx);
   for (size_t i = 0; i < L0.act.size(); ++i) L0.act[i] = cls0[i] == 0;
   H.lev.push_back(L0);
@@ -319,7 +314,6 @@ inline Hierarchy build(int ny, int nx, int periodic, const std::vector<uint8_t>&
         if (!C.act[c] || j < 0 || !C.act[j]) C.st[k * Nc + c] = 0.0f;
       }
     }
-    C.ncolors = colors_for(C, (int)H.lev.size());
     H.lev.push_back(std::move(C));
   }
   // smoother weights omega / A_ii on every level

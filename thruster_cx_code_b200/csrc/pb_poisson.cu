@@ -256,12 +256,12 @@ __device__ __forceinline__ float prolong(const MgLevel& C, const float* zc, int 
   return w * (z00 + (m01 ? z01 : 0.0f) + (m10 ? z10 : 0.0f) + ((m10 && m01) ? z11 : 0.0f));
 }
 
-// Post-smoothed correction at fine node i = (y, x) of level F from z_c of the level below:
-//   z = (1 - w) m_i + d_i (r_i - sum_{k != centre} A_ik m_k),  m = [active] (d r + P z_c)
-template <bool LV0>
-__device__ __forceinline__ float smooth_up(const MgLevel& F, const MgLevel& C, const float* r, const float* zc, int y,
-                                           int x, int i, float& ri) {
-  const int ny = F.ny, nx = F.nx, Nf = ny * nx;
+// Post-smoothed correction at fine node i = (y, x) of the fine level F (5-point operator,
+// off-diagonals -1) from z_c of level 1:
+//   z = (1 - w) m_i + d_i (r_i + sum_{k nbr of i} m_k),  m = [active] (d r + P z_c)
+__device__ __forceinline__ float smooth_up0(const MgLevel& F, const MgLevel& C, const float* r, const float* zc,
+                                            int y, int x, int i, float& ri) {
+  const int ny = F.ny, nx = F.nx;
   int yr[3], ro[3];
   bool rv[3];
 #pragma unroll
@@ -279,7 +279,7 @@ __device__ __forceinline__ float smooth_up(const MgLevel& F, const MgLevel& C, c
   for (int t = 0; t < 3; ++t)
 #pragma unroll
     for (int u = 0; u < 3; ++u) {
-      if (LV0 && t != 1 && u != 1) { m[t][u] = 0.0f; continue; }
+      if (t != 1 && u != 1) { m[t][u] = 0.0f; continue; }  // the 5-point star only
       const int xx = x + u - 1;
       const bool ok = rv[t] && xx >= 0 && xx < nx;
       const int j = ok ? ro[t] + xx : i;
@@ -288,16 +288,7 @@ __device__ __forceinline__ float smooth_up(const MgLevel& F, const MgLevel& C, c
       m[t][u] = (ok && d > 0.0f) ? d * rj + pz : 0.0f;
       if (t == 1 && u == 1) { di = d; ri = rj; }
     }
-  float acc = ri;
-  if (LV0) {
-    acc += (m[1][0] + m[1][2]) + (m[0][1] + m[2][1]);
-  } else {
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      if (k == 4) continue;
-      acc -= __ldg(F.st + (size_t)k * Nf + i) * m[k / 3][k % 3];
-    }
-  }
+  const float acc = ri + ((m[1][0] + m[1][2]) + (m[0][1] + m[2][1]));
   return di > 0.0f ? W_KEEP * m[1][1] + di * acc : 0.0f;
 }
 
@@ -383,7 +374,7 @@ __device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth, cons
     for (int i = tid; i < N; i += nth) {
       const int y = i / F.nx, x = i - y * F.nx;
       float ri;
-      const float z = smooth_up<true>(F, C, r0, C.z, y, x, i, ri);
+      const float z = smooth_up0(F, C, r0, C.z, y, x, i, ri);
       __stcg(F.z + i, z);
       rz += (double)ri * (double)z;
     }

@@ -13,10 +13,8 @@ struct MgLevel {
   int ny, nx;
   int per;        // y is periodic on this level's operator
   int wrapP;      // prolongation from the next coarser level wraps in y
-  int ncolors;    // unused by the damped-Jacobi cycle (kept for the layout)
-  const uint8_t* act;     // active (unknown) nodes; level 0: class array instead (the kernel uses dinv > 0)
-  const float* st;        // 9-point stencil, st[k * N + i], k = (dI+1)*3 + (dJ+1); null on level 0
-  const float* dinv;      // omega / diagonal on active nodes, 0 elsewhere (Jacobi smoother)
+  const float* dinv;      // omega / diagonal on active nodes, 0 elsewhere (Jacobi smoother; d > 0 marks
+                          // the active nodes)
   const float* R;         // levels >= 2: restriction from the finer level, R[k * N + i], 5 x 5 patch
   const float* U;         // levels >= 1: prolongation + smoothing, U[k * N + i], 3 x 3 r then 3 x 3 z
   float *r, *z;           // right-hand side and correction on this level

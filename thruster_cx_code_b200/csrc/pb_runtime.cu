@@ -51,9 +51,7 @@ struct Species {
 };
 
 struct DevLevel {
-  int ny = 0, nx = 0, per = 0, wrapP = 0, ncolors = 2;
-  uint8_t* act = nullptr;
-  float* st = nullptr;
+  int ny = 0, nx = 0, per = 0, wrapP = 0;
   float* dinv = nullptr;
   float* R = nullptr;
   float* U = nullptr;
@@ -223,7 +221,7 @@ static void free_levels(Sim* s) {
     dfree(s->lev[l].dinv);
     dfree(s->lev[l].R);
     dfree(s->lev[l].U);
-    if (l > 0) { dfree(s->lev[l].act); dfree(s->lev[l].st); dfree(s->lev[l].r); dfree(s->lev[l].z); }
+    if (l > 0) { dfree(s->lev[l].r); dfree(s->lev[l].z); }
   }
   s->lev.clear();
   dfree(s->cidx);
@@ -255,7 +253,7 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   for (size_t l = 0; l < H.lev.size(); ++l) {
     const auto& L = H.lev[l];
     DevLevel& D = s->lev[l];
-    D.ny = L.ny; D.nx = L.nx; D.per = L.per; D.wrapP = L.wrapP; D.ncolors = L.ncolors;
+    D.ny = L.ny; D.nx = L.nx; D.per = L.per; D.wrapP = L.wrapP;
     size_t N = (size_t)L.ny * L.nx;
     CK(dalloc(&D.dinv, N));
     CK(cudaMemcpy(D.dinv, L.dinv.data(), N * sizeof(float), cudaMemcpyHostToDevice));
@@ -268,11 +266,9 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
       CK(cudaMemcpy(D.U, L.U.data(), L.U.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     if (l == 0) {
-      D.act = s->cls; D.st = nullptr; D.r = s->r32; D.z = s->z32;
+      D.r = s->r32; D.z = s->z32;
     } else {
-      CK(dalloc(&D.act, N)); CK(dalloc(&D.st, 9 * N)); CK(dalloc(&D.r, N)); CK(dalloc(&D.z, N));
-      CK(cudaMemcpy(D.act, L.act.data(), N, cudaMemcpyHostToDevice));
-      CK(cudaMemcpy(D.st, L.st.data(), 9 * N * sizeof(float), cudaMemcpyHostToDevice));
+      CK(dalloc(&D.r, N)); CK(dalloc(&D.z, N));
       CK(cudaMemset(D.r, 0, N * sizeof(float)));
       CK(cudaMemset(D.z, 0, N * sizeof(float)));
     }
@@ -305,7 +301,7 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
   for (size_t l = 0; l < s->lev.size() && l < (size_t)MG_MAX_LEVELS; ++l) {
     const DevLevel& D = s->lev[l];
     a.lev[l].ny = D.ny; a.lev[l].nx = D.nx; a.lev[l].per = D.per; a.lev[l].wrapP = D.wrapP;
-    a.lev[l].ncolors = D.ncolors; a.lev[l].act = D.act; a.lev[l].st = D.st; a.lev[l].r = D.r; a.lev[l].z = D.z;
+    a.lev[l].r = D.r; a.lev[l].z = D.z;
     a.lev[l].dinv = D.dinv;
     a.lev[l].R = D.R;
     a.lev[l].U = D.U;
