@@ -36,6 +36,17 @@ PB_HD long long np_f2i64(float v) {
 PB_HD int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 PB_HD long long clampll(long long v, long long lo, long long hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization
+// may be scheduled while the previous kernel in its stream drains.  Every kernel that such a
+// launch can reach starts here.  griddepcontrol.wait returns once the previous kernel has
+// completed and its memory operations are visible (at once after a plain launch), so the
+// kernels' effects keep plain stream order; only the launch overlaps.  The kernel then lets
+// its own successor be scheduled.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // cell index of np.clip(np.round(s / d).astype(int), lo, hi)   (float32 division)
 __device__ __forceinline__ int cell_round(float s, float d, int lo, int hi) {
   float q = __fdiv_rn(s, d);

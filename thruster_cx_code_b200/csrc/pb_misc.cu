@@ -32,6 +32,7 @@ __device__ int poisson_inversion(double u, double lam) {
 // ------------------------------------------------------------------ injection
 // inject step A (physics_engine.py:996-1099): counts, slots and ids for this step
 __global__ void k_inject_prep(InjectArgs a) {
+  pdl_enter();
   int n_ion = 0, n_rf = 0;
   if (a.ion_on) n_ion = poisson_inversion(philox_uniform(a.seed, 0, SITE_ION_COUNT, a.step, 0), a.lam);
   if (a.rf_on) {
@@ -61,6 +62,7 @@ __global__ void k_inject_prep(InjectArgs a) {
 
 // inject step B: one thread per new particle; blockIdx.y selects ions / rf / neutralizer
 __global__ void k_inject_gen(InjectArgs a) {
+  pdl_enter();
   const int seg = blockIdx.y;
   const int n = a.inj[seg];
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
@@ -152,6 +154,7 @@ __device__ void block_sort_u64(uint64_t* keys, int n) {
 // the parent ion, purge test against the current isBound, appended after the step's
 // surviving electrons (physics_engine.py:1400-1417, 1541-1561).
 __global__ void k_see_finish(SeeArgs a) {
+  pdl_enter();
   __shared__ int sm[32];
   __shared__ int s_base, s_total;
   int n = *a.see_count;
@@ -230,6 +233,7 @@ PB_HD float percentile95_sorted(const float* s, int n) {
 }
 
 __global__ void k_theta95(float* angles, const int* count, int cap, uint64_t* scratch, double* out) {
+  pdl_enter();
   int n = *count;
   if (n > cap) n = cap;
   if (n <= 5) {
@@ -250,6 +254,7 @@ __global__ void k_theta95(float* angles, const int* count, int cap, uint64_t* sc
 // (physics_engine.py:1443-1449, 525-552).
 __global__ void k_erosion_break(double* damage, uint8_t* isBound, uint8_t* cls, double* eroded, int ny, int nx,
                                 int periodic, double thresh, double dy, int* broken) {
+  pdl_enter();
   int N = ny * nx;
   int cntb = 0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
@@ -275,6 +280,7 @@ __global__ void k_erosion_break(double* damage, uint8_t* isBound, uint8_t* cls, 
 // and the coarse part adds a semidefinite term.  The weights are the host build's,
 // omega / (4 - Neumann neighbours) in double rounded to float, 0 off the free nodes.
 __global__ void k_refresh_dinv0(const uint8_t* cls, float* dinv, int ny, int nx, int periodic, const int* broken) {
+  pdl_enter();
   if (*broken == 0) return;
   const int N = ny * nx;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
@@ -306,6 +312,7 @@ constexpr int TW = TT + 2 * HALO;
 
 __global__ void __launch_bounds__(256) k_thermal(float* T, const uint8_t* isBound, int ny, int nx, float cf,
                                                  float T4_300, float Fo_x, float Fo_y, int sweeps) {
+  pdl_enter();
   __shared__ float A[TW * TW], B[TW * TW];
   __shared__ uint8_t M[TW * TW];
   __shared__ int any;
@@ -392,6 +399,7 @@ __device__ __forceinline__ T block_reduce(T v, Op op, T ident) {
 }
 
 __global__ void k_grid_sums(const float* T, const uint16_t* gridmask, int N, int ngrids, double* out) {
+  pdl_enter();
   double s[16];
   double c[16];
   for (int g = 0; g < ngrids; ++g) { s[g] = 0; c[g] = 0; }
@@ -414,6 +422,7 @@ __global__ void k_grid_sums(const float* T, const uint16_t* gridmask, int N, int
 // ------------------------------------------------------------------ PPC statistics
 // accum += ppc; total active cells, cells with 0 < ppc < 3, min nonzero
 __global__ void k_ppc_stats(const int* ppc, double* accum, int N, unsigned long long* stats) {
+  pdl_enter();
   unsigned long long act = 0, low = 0;
   int mn = 0x7fffffff;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
@@ -437,6 +446,7 @@ __global__ void k_ppc_stats(const int* ppc, double* accum, int N, unsigned long 
 // inside the domain and masked, T_new = max(T + dT, 300); unmasked cells copied.
 __global__ void k_thermal_taichi(const float* T, float* Tn, const int32_t* mask, int nx, int ny, float Fo_x,
                                  float Fo_y) {
+  pdl_enter();
   int N = nx * ny;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     int iy = i / nx, ix = i - iy * nx;
@@ -463,6 +473,7 @@ __global__ void k_thermal_taichi(const float* T, float* Tn, const int32_t* mask,
 // a digit-major exclusive scan, and a stable scatter (warp-ordered ranks).
 __global__ void k_sort_keys(const float* x, const float* y, const int* n_dev, int nx, int ny, float dxf, float dyf,
                             uint32_t* key, uint32_t* val) {
+  pdl_enter();
   int n = *n_dev;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     key[i] = (uint32_t)dep_cell(x[i], y[i], dxf, dyf, nx, ny);
@@ -472,6 +483,7 @@ __global__ void k_sort_keys(const float* x, const float* y, const int* n_dev, in
 
 __global__ void __launch_bounds__(SORT_NT) k_sort_hist(const uint32_t* key, const int* n_dev, int shift,
                                                        uint32_t* hist, int ntiles) {
+  pdl_enter();
   __shared__ uint32_t h[RADIX];
   int n = *n_dev;
   for (int d = threadIdx.x; d < RADIX; d += blockDim.x) h[d] = 0;
@@ -488,6 +500,7 @@ __global__ void __launch_bounds__(SORT_NT) k_sort_hist(const uint32_t* key, cons
 
 // exclusive scan of hist (RADIX * ntiles, digit-major) in one block
 __global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* hist, int total) {
+  pdl_enter();
   __shared__ uint32_t carry;
   __shared__ uint32_t sm[32];
   if (threadIdx.x == 0) carry = 0;
@@ -550,6 +563,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* total)
 }
 
 __global__ void __launch_bounds__(SCAN_NT) k_scan_partials(const uint32_t* a, int total, uint32_t* bsum) {
+  pdl_enter();
   const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER;
   uint32_t s = 0u;
 #pragma unroll
@@ -561,6 +575,7 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_partials(const uint32_t* a, in
 }
 
 __global__ void __launch_bounds__(SCAN_NT) k_scan_apply(uint32_t* a, int total, const uint32_t* bsum) {
+  pdl_enter();
   const int base = blockIdx.x * SCAN_CHUNK + threadIdx.x * SCAN_PER;
   uint32_t v[SCAN_PER];
   uint32_t s = 0u;
@@ -581,6 +596,7 @@ __global__ void __launch_bounds__(SCAN_NT) k_scan_apply(uint32_t* a, int total, 
 __global__ void __launch_bounds__(SORT_NT) k_sort_scatter(const uint32_t* key, const uint32_t* val, const int* n_dev,
                                                           int shift, const uint32_t* offs, int ntiles,
                                                           uint32_t* key_out, uint32_t* val_out) {
+  pdl_enter();
   __shared__ uint32_t base[RADIX];
   __shared__ uint32_t wcount[SORT_NT / 32][RADIX];
   int n = *n_dev;
@@ -621,6 +637,7 @@ __global__ void __launch_bounds__(SORT_NT) k_sort_scatter(const uint32_t* key, c
 
 // gather one species' SoA through the permutation
 __global__ void k_sort_gather(Soa src, Soa dst, const uint32_t* perm, const int* n_dev) {
+  pdl_enter();
   int n = *n_dev;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t j = perm[i];
@@ -632,7 +649,7 @@ __global__ void k_sort_gather(Soa src, Soa dst, const uint32_t* perm, const int*
 }
 
 // copy the device count to another slot (num_dst of a sort = num_src)
-__global__ void k_copy_int(const int* a, int* b) { *b = *a; }
+__global__ void k_copy_int(const int* a, int* b) { pdl_enter(); *b = *a; }
 
 // ------------------------------------------------------------------ distance to electrodes
 // Chebyshev distance (in cells, capped at BDIST_CAP) from every node to the nearest bound
@@ -641,6 +658,7 @@ __global__ void k_copy_int(const int* a, int* b) { *b = *a; }
 constexpr int BDIST_CAP = 15;
 
 __global__ void k_bdist_rows(const uint8_t* __restrict__ isBound, uint8_t* hrow, int ny, int nx) {
+  pdl_enter();
   const int N = ny * nx;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     const int y = i / nx, x = i - y * nx;
@@ -652,6 +670,7 @@ __global__ void k_bdist_rows(const uint8_t* __restrict__ isBound, uint8_t* hrow,
 }
 
 __global__ void k_bdist_cols(const uint8_t* __restrict__ hrow, uint8_t* dist, int ny, int nx) {
+  pdl_enter();
   const int N = ny * nx;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     const int y = i / nx, x = i - y * nx;

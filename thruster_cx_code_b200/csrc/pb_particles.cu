@@ -50,6 +50,7 @@ __device__ __forceinline__ void gather4c(const float4* __restrict__ Ec, size_t c
 // the gather clamps the lower corner to ny - 2, nx - 2).
 __global__ void k_e_corners(const float* __restrict__ Ex, const float* __restrict__ Ey, float4* __restrict__ Ec,
                             int ny, int nx) {
+  pdl_enter();
   const int N = ny * nx;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < N; c += gridDim.x * blockDim.x) {
     const int iy = c / nx, ix = c - iy * nx;
@@ -196,6 +197,7 @@ __device__ __forceinline__ int substep_count(double ds_max, double ds_lim, uint3
 __global__ void k_push_boris(float* x, float* y, float* vx, float* vy, float* vz, const float* Ex,
                              const float* Ey, const float* Bx, const float* By, const float* Bz, int n,
                              int nx, int ny, float dxf, float dyf, double h, float dtf) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float a = x[i], b = y[i], c = vx[i], d = vy[i], e = vz[i];
     boris_push_one<true>(a, b, c, d, e, Ex, Ey, Bx, By, Bz, nx, ny, dxf, dyf, h, dtf);
@@ -220,6 +222,7 @@ __device__ __forceinline__ int deposit_cell(float x, float y, float dxf, float d
 
 __global__ void k_count_cells(const float* __restrict__ x, const float* __restrict__ y, const int* n_dev, int n_host,
                               int start, int* cnt, int nx, int ny, float dxf, float dyf) {
+  pdl_enter();
   int n = n_dev ? *n_dev : n_host;
   int base = blockIdx.x * blockDim.x;
   for (int i0 = base; i0 < n - start; i0 += gridDim.x * blockDim.x) {
@@ -233,6 +236,7 @@ __global__ void k_count_cells(const float* __restrict__ x, const float* __restri
 // rho = seq(seq(rho0, +c, k_ion), -c, k_ele) with the float64 addend of np.add.at;
 // counts are cleared for reuse
 __global__ void k_rho_finalize(float* rho, int* cnt_i, int* cnt_e, int G, double cd, int accumulate) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < G; i += gridDim.x * blockDim.x) {
     float s = accumulate ? rho[i] : 0.0f;
     int ki = cnt_i ? cnt_i[i] : 0;
@@ -288,6 +292,7 @@ __global__ void k_substep_reduce(const float* __restrict__ x, const float* __res
                                  const float* __restrict__ vz, const int* n_dev, int n_host, const float* Ex,
                                  const float* Ey, const float4* Ec, int nx, int ny, float dxf, float dyf, double qm,
                                  float dtf, double dt2, unsigned long long* ds_max_bits) {
+  pdl_enter();
   int n = n_dev ? *n_dev : n_host;
   unsigned long long m = 0ull;
   // four particles per thread and pass (16-byte loads of each array), so that a thread
@@ -340,6 +345,7 @@ __global__ void k_substep_reduce(const float* __restrict__ x, const float* __res
 
 // n_sub for the host-facing report: read ds_max, write n_sub
 __global__ void k_substep_finish(const double* ds_max, double ds_lim, int* n_sub_out, uint32_t* errflags) {
+  pdl_enter();
   *n_sub_out = substep_count(*ds_max, ds_lim, errflags);
 }
 
@@ -389,6 +395,7 @@ __device__ __forceinline__ SegHit segment_hit_f(const uint8_t* __restrict__ isBo
 __global__ void k_segment_hits(const uint8_t* isBound, int nx, int ny, float dxf, float dyf, const float* x0,
                                const float* y0, const float* x1, const float* y1, int n, uint8_t* hit,
                                int64_t* hix, int64_t* hiy) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     SegHit s = segment_hit(isBound, nx, ny, dxf, dyf, x0[i], y0[i], x1[i], y1[i]);
     hit[i] = s.hit;
@@ -528,6 +535,7 @@ struct IonStage {
 // more than the spills cost (12% faster than three blocks at 80 registers).
 template <bool HAS_B>
 __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
+  pdl_enter();
   __shared__ IonStage st;
   __shared__ int sm_tile;
   const int n = *a.num_src;
@@ -739,6 +747,7 @@ struct EleStage {
 
 template <bool HAS_B>
 __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
+  pdl_enter();
   __shared__ EleStage st;
   __shared__ int sm_tile;
   const int n = *a.num_src;

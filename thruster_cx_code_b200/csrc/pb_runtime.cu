@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "pbemcs.h"
@@ -131,6 +132,26 @@ struct Sim {
   long long launches = 0;   // kernels enqueued by the last pb_sim_run / pb_sim_step
   double sp_dx = 1.0, sp_dy = 1.0;   // grid spacing of the last step (cell keys of the sort)
 };
+
+// A launch with programmatic stream serialization (the step's kernels): the kernel may be
+// scheduled while its predecessor in the stream drains, and waits in pdl_enter() until that
+// predecessor has completed.  A predecessor that is not a kernel (a copy, a memset, an
+// event) orders it as a plain launch would.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // ------------------------------------------------------------------ helpers
 static int grid_for(const Sim* s, long n, int bs, int per_sm = 8) {
@@ -363,6 +384,7 @@ struct StepResetArgs {
 };
 
 __global__ void k_step_reset(StepResetArgs a) {
+  pdl_enter();
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, nth = (long long)gridDim.x * blockDim.x;
   static_assert(sizeof(pb_step_report) % 4 == 0 && offsetof(pb_step_report, ppc_min) % 4 == 0, "report words");
   constexpr long long nw = sizeof(pb_step_report) / 4, w0 = offsetof(pb_step_report, ppc_min) / 4;
@@ -381,6 +403,7 @@ __global__ void k_step_reset(StepResetArgs a) {
 
 // RF: V_fixed on grid g = Vdc + v_rf
 __global__ void k_rf_update(double* Vfixed, const double* Vdc, const uint16_t* gridmask, int N, int g, double v_rf) {
+  pdl_enter();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
     if (gridmask[i] & (1u << g)) Vfixed[i] = Vdc[i] + v_rf;
 }
@@ -392,6 +415,7 @@ struct SaddleIdx { int v[8]; };
 __global__ void k_report(pb_step_report* r, const int* counts, int ci, int ce, const int* n_sub,
                          const unsigned long long* ds_bits, const int* inj, const int* see_spawned, const double* V,
                          int n_saddle, SaddleIdx sidx, const double* pstats) {
+  pdl_enter();
   r->num_p = counts[ci];
   r->num_e = counts[2 + ce];
   r->n_sub_ion = n_sub[0];
@@ -413,6 +437,7 @@ __global__ void k_report(pb_step_report* r, const int* counts, int ci, int ce, c
 
 // n_sub of both species from their reduced displacements, one thread
 __global__ void k_substep_finish2(const double* ds_max, double ds_lim, int* n_sub_out, uint32_t* errflags) {
+  pdl_enter();
   n_sub_out[0] = substep_count(ds_max[0], ds_lim, errflags);
   n_sub_out[1] = substep_count(ds_max[1], ds_lim, errflags);
 }
@@ -448,28 +473,28 @@ static int32_t sort_species(Sim* s, int k, int ncell_bits) {
   int cap = S.cap;
   int ntiles = (cap + SORT_TILE - 1) / SORT_TILE;
   const Soa& src = S.buf[S.cur];
-  k_sort_keys<<<grid_for(s, cap, 256), 256, 0, st>>>(src.x, src.y, n_src, s->nx, s->ny, (float)s->sp_dx,
-                                                     (float)s->sp_dy, s->skey[0], s->sval[0]);
+  CK(launch_pdl(k_sort_keys, grid_for(s, cap, 256), 256, 0, st, src.x, src.y, n_src, s->nx, s->ny, (float)s->sp_dx,
+                                                     (float)s->sp_dy, s->skey[0], s->sval[0]));
   ++s->launches;
   int a = 0;
   for (int shift = 0; shift < ncell_bits; shift += RADIX_BITS) {
-    k_sort_hist<<<ntiles, SORT_NT, 0, st>>>(s->skey[a], n_src, shift, s->shist, ntiles);
+    CK(launch_pdl(k_sort_hist, ntiles, SORT_NT, 0, st, s->skey[a], n_src, shift, s->shist, ntiles));
     ++s->launches;
     {
       const int total = RADIX * ntiles, nb = (total + SCAN_CHUNK - 1) / SCAN_CHUNK;
-      k_scan_partials<<<nb, SCAN_NT, 0, st>>>(s->shist, total, s->sblk);
-      k_sort_scan<<<1, 1024, 0, st>>>(s->sblk, nb);
-      k_scan_apply<<<nb, SCAN_NT, 0, st>>>(s->shist, total, s->sblk);
+      CK(launch_pdl(k_scan_partials, nb, SCAN_NT, 0, st, s->shist, total, s->sblk));
+      CK(launch_pdl(k_sort_scan, 1, 1024, 0, st, s->sblk, nb));
+      CK(launch_pdl(k_scan_apply, nb, SCAN_NT, 0, st, s->shist, total, s->sblk));
       s->launches += 3;
     }
-    k_sort_scatter<<<ntiles, SORT_NT, 0, st>>>(s->skey[a], s->sval[a], n_src, shift, s->shist, ntiles,
-                                                s->skey[1 - a], s->sval[1 - a]);
+    CK(launch_pdl(k_sort_scatter, ntiles, SORT_NT, 0, st, s->skey[a], s->sval[a], n_src, shift, s->shist, ntiles,
+                                                s->skey[1 - a], s->sval[1 - a]));
     ++s->launches;
     a = 1 - a;
   }
-  k_sort_gather<<<grid_for(s, cap, 256), 256, 0, st>>>(src, S.buf[1 - S.cur], s->sval[a], n_src);
+  CK(launch_pdl(k_sort_gather, grid_for(s, cap, 256), 256, 0, st, src, S.buf[1 - S.cur], s->sval[a], n_src));
   ++s->launches;
-  k_copy_int<<<1, 1, 0, st>>>(n_src, n_dst);
+  CK(launch_pdl(k_copy_int, 1, 1, 0, st, n_src, n_dst));
   ++s->launches;
   S.cur ^= 1;
   CK(cudaGetLastError());
@@ -535,18 +560,18 @@ static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
     r.tile_status = s->tile_status; r.ntile = 2 * (long long)s->tile_cap;
     r.angle_count = s->angle_count; r.see_count = s->see_count; r.see_spawned = s->see_spawned;
     r.ds_bits = s->ds_bits; r.tile_counter = s->tile_counter; r.ni_dst = ni_dst; r.ne_dst = ne_dst; r.inj = s->inj;
-    k_step_reset<<<grid_for(s, std::max<long>(N, 2 * (long)s->tile_cap), 256), 256, 0, st>>>(r);
+    CK(launch_pdl(k_step_reset, grid_for(s, std::max<long>(N, 2 * (long)s->tile_cap), 256), 256, 0, st, r));
     ++s->launches;
   }
 
   if (!s->counts_valid) {
     CK(cudaMemsetAsync(s->cnt_i, 0, (size_t)N * sizeof(int), st));
     CK(cudaMemsetAsync(s->cnt_e, 0, (size_t)N * sizeof(int), st));
-    k_count_cells<<<grid_for(s, I.cap, 256), 256, 0, st>>>(I.buf[I.cur].x, I.buf[I.cur].y, ni_src, 0, 0, s->cnt_i,
-                                                           s->nx, s->ny, dxf, dyf);
+    CK(launch_pdl(k_count_cells, grid_for(s, I.cap, 256), 256, 0, st, I.buf[I.cur].x, I.buf[I.cur].y, ni_src, 0, 0,
+                  s->cnt_i, s->nx, s->ny, dxf, dyf));
     ++s->launches;
-    k_count_cells<<<grid_for(s, E.cap, 256), 256, 0, st>>>(E.buf[E.cur].x, E.buf[E.cur].y, ne_src, 0, 0, s->cnt_e,
-                                                           s->nx, s->ny, dxf, dyf);
+    CK(launch_pdl(k_count_cells, grid_for(s, E.cap, 256), 256, 0, st, E.buf[E.cur].x, E.buf[E.cur].y, ne_src, 0, 0,
+                  s->cnt_e, s->nx, s->ny, dxf, dyf));
     ++s->launches;
     s->counts_valid = true;
   }
@@ -554,7 +579,8 @@ static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
   // RF co-extraction: V_fixed on one grid, then recalc_poisson(2) (:984-991)
   int32_t rc;
   if (p->rf_grid >= 0) {
-    k_rf_update<<<grid_for(s, N, 256), 256, 0, st>>>(s->Vfixed, s->Vdc, s->gridmask, N, p->rf_grid, p->v_rf);
+    CK(launch_pdl(k_rf_update, grid_for(s, N, 256), 256, 0, st, s->Vfixed, s->Vdc, s->gridmask, N, p->rf_grid,
+                  p->v_rf));
     ++s->launches;
     if ((rc = launch_poisson(s, 2, p))) return rc;
   }
@@ -574,17 +600,17 @@ static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
   ia.ions = I.buf[I.cur]; ia.eles = E.buf[E.cur];
   ia.cnt_i = s->cnt_i; ia.cnt_e = s->cnt_e;
   ia.nx = s->nx; ia.ny = s->ny; ia.dxf = dxf; ia.dyf = dyf; ia.errflags = ef;
-  k_inject_prep<<<1, 1, 0, st>>>(ia);
+  CK(launch_pdl(k_inject_prep, 1, 1, 0, st, ia));
   ++s->launches;
   {
     long mx = std::max<long>({(long)(p->lam + 40.0 * std::sqrt(std::max(p->lam, 0.0)) + 100.0),
                               (long)p->neut_n, (long)p->rf_num_float + 1, 1L});
-    k_inject_gen<<<dim3(grid_for(s, mx, 128, 2), 3), 128, 0, st>>>(ia);
+    CK(launch_pdl(k_inject_gen, dim3(grid_for(s, mx, 128, 2), 3), 128, 0, st, ia));
     ++s->launches;
   }
 
   // B. deposit (counts -> exact float32 sums) and the Picard field solve (:1104-1161)
-  k_rho_finalize<<<grid_for(s, N, 256), 256, 0, st>>>(s->rho, s->cnt_i, s->cnt_e, N, p->charge_density, 0);
+  CK(launch_pdl(k_rho_finalize, grid_for(s, N, 256), 256, 0, st, s->rho, s->cnt_i, s->cnt_e, N, p->charge_density, 0));
   ++s->launches;
   mark(s);
   CK(cudaGetLastError());
@@ -609,20 +635,20 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
 
   // corners of Ex, Ey for the gathers below (rebuilt every step: fields change in the
   // solve, through pb_sim_set_field or through pb_sim_field_ptr)
-  k_e_corners<<<grid_for(s, N, 256), 256, 0, st>>>(s->Ex, s->Ey, s->ecorn, s->ny, s->nx);
+  CK(launch_pdl(k_e_corners, grid_for(s, N, 256), 256, 0, st, s->Ex, s->Ey, s->ecorn, s->ny, s->nx));
   ++s->launches;
 
   // C. sub-step counts (:1177-1209)
   const float dtf = (float)p->dt;
-  k_substep_reduce<<<grid_for(s, I.cap / 4, 256, 4), 256, 0, st>>>(I.buf[I.cur].x, I.buf[I.cur].y, I.buf[I.cur].vx,
-      I.buf[I.cur].vy, I.buf[I.cur].vz, ni_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf, dyf, p->qm_ion, dtf, p->dt2,
-      s->ds_bits);
+  CK(launch_pdl(k_substep_reduce, grid_for(s, I.cap / 4, 256, 4), 256, 0, st, I.buf[I.cur].x, I.buf[I.cur].y,
+                I.buf[I.cur].vx, I.buf[I.cur].vy, I.buf[I.cur].vz, ni_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf,
+                dyf, p->qm_ion, dtf, p->dt2, s->ds_bits));
   ++s->launches;
-  k_substep_reduce<<<grid_for(s, E.cap / 4, 256, 4), 256, 0, st>>>(E.buf[E.cur].x, E.buf[E.cur].y, E.buf[E.cur].vx,
-      E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf, dyf, p->qm_e, dtf, p->dt2,
-      s->ds_bits + 1);
+  CK(launch_pdl(k_substep_reduce, grid_for(s, E.cap / 4, 256, 4), 256, 0, st, E.buf[E.cur].x, E.buf[E.cur].y,
+                E.buf[E.cur].vx, E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf,
+                dyf, p->qm_e, dtf, p->dt2, s->ds_bits + 1));
   ++s->launches;
-  k_substep_finish2<<<1, 1, 0, st>>>((const double*)s->ds_bits, p->ds_lim, s->n_sub, ef);
+  CK(launch_pdl(k_substep_finish2, 1, 1, 0, st, (const double*)s->ds_bits, p->ds_lim, s->n_sub, ef));
   ++s->launches;
   mark(s);
 
@@ -655,16 +681,16 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   a.seed = s->seed; a.step = (uint32_t)p->iteration;
   a.ppc = s->ppc; a.cnt = s->cnt_i;
   a.tile_status = s->tile_status; a.tile_counter = s->tile_counter; a.errflags = ef;
-  k_ion_step<false><<<grid_for(s, I.cap, TILE, s->pbps), NT, 0, st>>>(a);
+  CK(launch_pdl(k_ion_step<false>, grid_for(s, I.cap, TILE, s->pbps), NT, 0, st, a));
   ++s->launches;
   mark(s);
 
   // sputter cell break (:1443-1449) before the electron purge, which sees the new mask
   if (p->erosion_on) {
-    k_erosion_break<<<grid_for(s, N, 256), 256, 0, st>>>(s->damage, s->isBound, s->cls, s->eroded, s->ny, s->nx,
-                                                         s->periodic, p->thresh, p->dy, &rep->broken);
-    k_refresh_dinv0<<<grid_for(s, N, 256), 256, 0, st>>>(s->cls, s->lev[0].dinv, s->ny, s->nx, s->periodic,
-                                                         &rep->broken);
+    CK(launch_pdl(k_erosion_break, grid_for(s, N, 256), 256, 0, st, s->damage, s->isBound, s->cls, s->eroded, s->ny,
+                  s->nx, s->periodic, p->thresh, p->dy, &rep->broken));
+    CK(launch_pdl(k_refresh_dinv0, grid_for(s, N, 256), 256, 0, st, s->cls, s->lev[0].dinv, s->ny, s->nx, s->periodic,
+                                                         &rep->broken));
     s->launches += 2;
   }
 
@@ -678,7 +704,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
   b.errflags = ef;
-  k_ele_step<false><<<grid_for(s, E.cap, TILE, s->pbps), NT, 0, st>>>(b);
+  CK(launch_pdl(k_ele_step<false>, grid_for(s, E.cap, TILE, s->pbps), NT, 0, st, b));
   ++s->launches;
 
   // SEE electrons, appended after the surviving electrons (:1390-1417)
@@ -688,7 +714,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   sa.eles = E.buf[1 - E.cur]; sa.num_e = ne_dst; sa.cap_e = E.cap; sa.next_e_id = s->next_ids + 1;
   sa.isBound = s->isBound; sa.nx = s->nx; sa.ny = s->ny; sa.dxf = dxf; sa.dyf = dyf;
   sa.Lxf = (float)p->Lx; sa.Lyf = (float)p->Ly; sa.cnt_e = s->cnt_e; sa.errflags = ef;
-  k_see_finish<<<1, 1024, 0, st>>>(sa);
+  CK(launch_pdl(k_see_finish, 1, 1024, 0, st, sa));
   ++s->launches;
   mark(s);
   I.cur ^= 1;
@@ -696,25 +722,27 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
 
   // F. thermal (:1566-1620)
   if (p->thermal_on) {
-    k_thermal<<<dim3((s->nx + TT - 1) / TT, (s->ny + TT - 1) / TT), 256, 0, st>>>(
+    CK(launch_pdl(k_thermal, dim3((s->nx + TT - 1) / TT, (s->ny + TT - 1) / TT), 256, 0, st,
         s->Tmap, s->isBound, s->ny, s->nx, (float)p->cooling_factor, (float)p->T4_300, (float)p->Fo_x,
-        (float)p->Fo_y, p->sweeps);
+        (float)p->Fo_y, p->sweeps));
     ++s->launches;
   }
   if (s->ngrids > 0) {
-    k_grid_sums<<<grid_for(s, N, 256), 256, 0, st>>>(s->Tmap, s->gridmask, N, std::min(s->ngrids, 16), rep->grid_sums);
+    CK(launch_pdl(k_grid_sums, grid_for(s, N, 256), 256, 0, st, s->Tmap, s->gridmask, N, std::min(s->ngrids, 16),
+                  rep->grid_sums));
     ++s->launches;
   }
 
   // exit divergence, saddle potential, PPC map (:1482-1488, 1655-1676, 1741-1767)
-  k_theta95<<<1, 1024, 0, st>>>(s->angles, s->angle_count, s->angle_cap, s->angle_scratch, &rep->theta95);
+  CK(launch_pdl(k_theta95, 1, 1024, 0, st, s->angles, s->angle_count, s->angle_cap, s->angle_scratch, &rep->theta95));
   ++s->launches;
   SaddleIdx sidx{};
   for (int k = 0; k < 8; ++k) sidx.v[k] = p->saddle_idx[k];
-  k_report<<<1, 1, 0, st>>>(rep, s->counts, I.cur, E.cur, s->n_sub, s->ds_bits, s->inj, s->see_spawned, s->V,
-                            std::max(0, std::min(p->n_saddle, 8)), sidx, s->pstats);
+  CK(launch_pdl(k_report, 1, 1, 0, st, rep, s->counts, I.cur, E.cur, s->n_sub, s->ds_bits, s->inj, s->see_spawned, s->V,
+                            std::max(0, std::min(p->n_saddle, 8)), sidx, s->pstats));
   ++s->launches;
-  k_ppc_stats<<<grid_for(s, N, 256), 256, 0, st>>>(s->ppc, s->accum_ppc, N, (unsigned long long*)&rep->ppc_active);
+  CK(launch_pdl(k_ppc_stats, grid_for(s, N, 256), 256, 0, st, s->ppc, s->accum_ppc, N,
+                (unsigned long long*)&rep->ppc_active));
   ++s->launches;
 
   // periodic re-sort by cell (north-star (a)); the permutation equals a stable argsort
