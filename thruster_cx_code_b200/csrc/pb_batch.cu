@@ -206,6 +206,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       if (nb[j] > s->pgrid) return fail(PB_ERR_STATE, "pb_batch_run: block share above the instance's grid");
       a.blk0 = blk0;
       a.nblk = nb[j];
+      set_up_tiles(s, &a);
       a.trace = nullptr;
       b->hargs[L.args_off + j] = a;
       for (int q = 0; q < nb[j]; ++q) b->hblk[L.blk_off + blk0 + q] = (int)j;

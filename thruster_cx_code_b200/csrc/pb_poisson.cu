@@ -256,40 +256,49 @@ __device__ __forceinline__ float prolong(const MgLevel& C, const float* zc, int 
   return w * (z00 + (m01 ? z01 : 0.0f) + (m10 ? z10 : 0.0f) + ((m10 && m01) ? z11 : 0.0f));
 }
 
-// Post-smoothed correction at fine node i = (y, x) of the fine level F (5-point operator,
-// off-diagonals -1) from z_c of level 1:
-//   z = (1 - w) m_i + d_i (r_i + sum_{k nbr of i} m_k),  m = [active] (d r + P z_c)
-__device__ __forceinline__ float smooth_up0(const MgLevel& F, const MgLevel& C, const float* r, const float* zc,
-                                            int y, int x, int i, float& ri) {
-  const int ny = F.ny, nx = F.nx;
-  int yr[3], ro[3];
-  bool rv[3];
-#pragma unroll
-  for (int t = 0; t < 3; ++t) {
-    int yy = y + t - 1;
-    if (F.per) { if (yy < 0) yy += ny; else if (yy >= ny) yy -= ny; }
-    rv[t] = yy >= 0 && yy < ny;
-    yr[t] = rv[t] ? yy : y;
-    ro[t] = yr[t] * nx;
-  }
-  float m[3][3];
-  float di = 0.0f;
-  ri = 0.0f;
-#pragma unroll
-  for (int t = 0; t < 3; ++t)
-#pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      if (t != 1 && u != 1) { m[t][u] = 0.0f; continue; }  // the 5-point star only
-      const int xx = x + u - 1;
-      const bool ok = rv[t] && xx >= 0 && xx < nx;
-      const int j = ok ? ro[t] + xx : i;
-      const float d = __ldg(F.dinv + j), rj = *(r + j);
-      const float pz = prolong(C, zc, ok ? yr[t] : y, ok ? xx : x);
-      m[t][u] = (ok && d > 0.0f) ? d * rj + pz : 0.0f;
-      if (t == 1 && u == 1) { di = d; ri = rj; }
+// Post-smoothed correction on the fine level F (5-point operator, off-diagonals -1) from
+// z_c of level 1, tile by tile:
+//   z_i = (1 - w) m_i + d_i (r_i + sum_{k nbr of i} m_k),  m = [active] (d r + P z_c).
+// The block forms m once per node of its tile and a one-node halo in shared memory (a node's
+// m is used by the five stars that contain it), then z from the tile.  The tiles are
+// a.ut_y x a.ut_x nearly equal rectangles, dealt to the blocks in turn; each holds at most
+// UP_TILE_MAX nodes with its halo.
+__device__ double up_leg0_tiled(const PoissonArgs& a, const float* r0) {
+  __shared__ float mt[UP_TILE_MAX];
+  const MgLevel& F = a.lev[0];
+  const MgLevel& C = a.lev[1];
+  const int ny = F.ny, nx = F.nx, nty = a.ut_y, ntx = a.ut_x;
+  double rz = 0.0;
+  for (int t = gbid(a); t < nty * ntx; t += a.nblk) {
+    const int ty = t / ntx, tx = t - ty * ntx;
+    const int y0 = (int)((long long)ty * ny / nty), y1 = (int)((long long)(ty + 1) * ny / nty);
+    const int x0 = (int)((long long)tx * nx / ntx), x1 = (int)((long long)(tx + 1) * nx / ntx);
+    const int h = y1 - y0, w = x1 - x0, w2 = w + 2, nm = (h + 2) * w2;
+    for (int k = threadIdx.x; k < nm; k += blockDim.x) {
+      const int ly = k / w2, lx = k - ly * w2;
+      int yy = y0 + ly - 1;
+      const int xx = x0 + lx - 1;
+      if (F.per) { if (yy < 0) yy += ny; else if (yy >= ny) yy -= ny; }
+      const bool ok = yy >= 0 && yy < ny && xx >= 0 && xx < nx;
+      const int j = ok ? yy * nx + xx : 0;
+      const float d = __ldg(F.dinv + j), rj = *(r0 + j);
+      const float pz = prolong(C, C.z, ok ? yy : 0, ok ? xx : 0);
+      mt[k] = (ok && d > 0.0f) ? d * rj + pz : 0.0f;
     }
-  const float acc = ri + ((m[1][0] + m[1][2]) + (m[0][1] + m[2][1]));
-  return di > 0.0f ? W_KEEP * m[1][1] + di * acc : 0.0f;
+    __syncthreads();
+    for (int k = threadIdx.x; k < h * w; k += blockDim.x) {
+      const int ly = k / w, lx = k - ly * w;
+      const int i = (y0 + ly) * nx + (x0 + lx);
+      const float di = __ldg(F.dinv + i), ri = *(r0 + i);
+      const float* mc = mt + (ly + 1) * w2 + (lx + 1);
+      const float acc = ri + ((mc[-1] + mc[1]) + (mc[-w2] + mc[w2]));
+      const float z = di > 0.0f ? W_KEEP * mc[0] + di * acc : 0.0f;
+      __stcg(F.z + i, z);
+      rz += (double)ri * (double)z;
+    }
+    __syncthreads();
+  }
+  return rz;
 }
 
 // Levels >= 1: the same transfers from the host-built stencils (R on the coarse level,
@@ -371,13 +380,7 @@ __device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth, cons
   const int N = F.ny * F.nx;
   double rz = 0.0;
   if (LV0) {
-    for (int i = tid; i < N; i += nth) {
-      const int y = i / F.nx, x = i - y * F.nx;
-      float ri;
-      const float z = smooth_up0(F, C, r0, C.z, y, x, i, ri);
-      __stcg(F.z + i, z);
-      rz += (double)ri * (double)z;
-    }
+    rz = up_leg0_tiled(a, r0);
   } else {
     for (int i = tid; i < N; i += nth) {
       const int y = i / F.nx, x = i - y * F.nx;

@@ -1,5 +1,6 @@
 // Poisson solver data layout (device pointers) shared by the kernel and the host builder.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 
 namespace pb {
@@ -53,6 +54,7 @@ struct PoissonArgs {
   const float* cinv;      // coarsest inverse (nc x nc, exactly symmetric)
   // this instance's blocks in the launch and its reductions and barrier
   int blk0, nblk;         // first block and number of blocks
+  int ut_y, ut_x;         // tiles of the fine-level up leg (fine_up_tiles)
   double* partials;       // 4 slots x 2 values x nblk doubles
   unsigned int* bar;      // barrier word, zero at launch (its low bits must start at zero)
   uint32_t* errflags;
@@ -62,5 +64,45 @@ struct PoissonArgs {
 
 // dynamic shared memory of k_poisson: the coarsest right-hand side gathered by each block
 inline size_t mg_coarse_smem_bytes(int nc) { return 4 * (size_t)(nc > 0 ? nc : 1); }
+
+// Tiling of the fine-level up leg: at most UP_TILE_MAX nodes per tile with its one-node halo.
+constexpr int UP_TILE_MAX = 4096;
+
+// Tile counts (ty rows x tx columns of nearly equal rectangles) for an ny x nx fine level
+// solved by nblk blocks of 1024 threads: the fewest rounds of tiles per block times the
+// passes a block makes over one tile (three units per pass that forms m, one per pass that
+// forms z), then the fewest m a block forms (rounds x nodes of a tile with its halo), then the
+// most tiles.  Tile counts up to about four rounds are searched; the smallest tiles (one row)
+// always fit.
+inline void fine_up_tiles(int ny, int nx, int nblk, int* ty_out, int* tx_out) {
+  const long cap = 4L * nblk + 4L * ((long)ny * nx / 1024 + 1);
+  long best_cost = -1, best_work = 0, best_tiles = 0;
+  int bty = ny, btx = nx;
+  for (int ty = 1; ty <= ny; ++ty) {
+    const long h = (ny + ty - 1) / ty;
+    const long wmax = UP_TILE_MAX / (h + 2) - 2;
+    if (wmax < 1) continue;
+    const long tx_min = (nx + wmax - 1) / wmax;
+    const long tx_max = std::max(tx_min, std::min<long>(nx, cap / ty));
+    for (long tx = tx_min; tx <= tx_max; ++tx) {
+      const long w = (nx + tx - 1) / tx;
+      const long tiles = (long)ty * tx;
+      const long rounds = (tiles + nblk - 1) / nblk;
+      const long cost = rounds * (3 * (((h + 2) * (w + 2) + 1023) / 1024) + (h * w + 1023) / 1024);
+      const long work = rounds * (h + 2) * (w + 2);
+      if (best_cost < 0 || cost < best_cost ||
+          (cost == best_cost && (work < best_work || (work == best_work && tiles > best_tiles)))) {
+        best_cost = cost;
+        best_work = work;
+        best_tiles = tiles;
+        bty = ty;
+        btx = (int)tx;
+      }
+    }
+    if ((long)ty * tx_min > cap && best_cost >= 0) break;
+  }
+  *ty_out = bty;
+  *tx_out = btx;
+}
 
 }  // namespace pb

@@ -86,6 +86,7 @@ struct Sim {
   unsigned long long* ptrace = nullptr;  // field-solve phase trace (32 slots)
   int trace_on = 0;
   int pgrid = 0;      // blocks of the field-solve launch (<= num_sms)
+  int ut_key[3] = {0, 0, 0}, ut[2] = {1, 1};  // fine up-leg tiling for (ny, nx, blocks)
   int pbps = 8;       // step-kernel blocks per SM (the grid; tiles are handed out by a counter)
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
   // particles
@@ -307,6 +308,16 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   return PB_OK;
 }
 
+// the fine up-leg tiling of a.nblk blocks, computed once per grid shape and block count
+static void set_up_tiles(Sim* s, PoissonArgs* a) {
+  if (s->ut_key[0] != s->ny || s->ut_key[1] != s->nx || s->ut_key[2] != a->nblk) {
+    fine_up_tiles(s->ny, s->nx, a->nblk, &s->ut[0], &s->ut[1]);
+    s->ut_key[0] = s->ny; s->ut_key[1] = s->nx; s->ut_key[2] = a->nblk;
+  }
+  a->ut_y = s->ut[0];
+  a->ut_x = s->ut[1];
+}
+
 static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p) {
   PoissonArgs a{};
   a.ny = s->ny; a.nx = s->nx; a.periodic = s->periodic;
@@ -329,6 +340,7 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
   }
   a.nc = s->nc; a.cidx = s->cidx; a.cinv = s->cinv;
   a.blk0 = 0; a.nblk = s->pgrid;
+  set_up_tiles(s, &a);
   a.partials = s->partials; a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
   a.stats = s->pstats;
