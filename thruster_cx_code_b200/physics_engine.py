@@ -27,6 +27,24 @@ from .domain import build_domain_geometry, compute_debye_upstream_gap  # noqa: F
 
 _NP_FP = np.float32
 
+
+def _sqrt(x):
+    """np.sqrt of a scalar.  A non-negative Python float takes math.sqrt, which is also
+    correctly rounded, without NumPy's dispatch; any other value (a NumPy scalar keeps its
+    dtype, NaN and negatives their NumPy results) goes through np.sqrt."""
+    return math.sqrt(x) if type(x) is float and x >= 0.0 else np.sqrt(x)
+
+
+def _clip(x, lo, hi):
+    """np.clip of a scalar without NumPy's dispatch where that is exact: Python ints with
+    lo <= hi (no NaN, no signed zero), or a nonzero Python number within [lo, hi], which
+    clips to itself.  Everything else goes through np.clip."""
+    if type(x) is int and type(lo) is int and type(hi) is int and lo <= hi:
+        return min(max(x, lo), hi)
+    if type(x) in (int, float) and type(lo) in (int, float) and type(hi) in (int, float) and lo <= x <= hi and x != 0:
+        return x
+    return np.clip(x, lo, hi)
+
 MATERIAL_PRESETS = {
     'Molybdenum': {'k': 138.0, 'rho': 10280.0, 'cp': 250.0, 'emissivity': 0.80, 'alpha': 4.8e-6,
                    'E_mod': 329e9, 'Y_coeff': 1.05e-4, 'E_th': 30.0},
@@ -582,7 +600,7 @@ class DigitalTwinSimulator:
         n0 = params.get('n0_plasma', 1e17)
         Te_up = params.get('Te_up', 3.0)
         Ti = params.get('Ti', 0.1)
-        v_bohm = np.sqrt(self.q_ion * Te_up / self.m_ion)
+        v_bohm = _sqrt(self.q_ion * Te_up / self.m_ion)
         injection_area = self.Ly * 1e-3 * 0.005
         charge_per_macro = self.q_ion * self.macro_weight
         if self.injection_enabled and (self.injection_stop_time is None or t_current <= self.injection_stop_time):
@@ -612,10 +630,10 @@ class DigitalTwinSimulator:
                 P.ylo, P.yhi = self.dy, self.Ly - self.dy
             P.x_inj = self.dx * 1.5
             P.v_bohm = v_bohm
-            P.v_spread = np.sqrt(self.q_ion * Ti / self.m_ion)
+            P.v_spread = _sqrt(self.q_ion * Ti / self.m_ion)
             if params.get('rf_enable'):
                 P.rf_on = 1
-                v_e_th_source = np.sqrt(2.0 * self.q * Te_up / self.m_e)
+                v_e_th_source = _sqrt(2.0 * self.q * Te_up / self.m_e)
                 I_e = self.q * 0.25 * n0 * v_e_th_source * injection_area
                 P.rf_num_float = (I_e * self.dt) / charge_per_macro
                 y_margin = max(self.dy, 1e-9)
@@ -624,9 +642,9 @@ class DigitalTwinSimulator:
                 P.v_e_src = v_e_th_source
         num_e_neut = int(params.get('neut_rate', 30))
         P.neut_n = max(num_e_neut, 0)
-        P.neut_x = float(np.clip(params.get('neut_x', self.Lx - 0.5), self.dx, self.Lx - self.dx))
-        P.neut_r = float(np.clip(params.get('neut_r', self.Ly), self.dy, self.Ly))
-        P.v_e_th = np.sqrt(2.0 * self.q * params.get('Te', 5.0) / self.m_e)
+        P.neut_x = float(_clip(params.get('neut_x', self.Lx - 0.5), self.dx, self.Lx - self.dx))
+        P.neut_r = float(_clip(params.get('neut_r', self.Ly), self.dy, self.Ly))
+        P.v_e_th = _sqrt(2.0 * self.q * params.get('Te', 5.0) / self.m_e)
         cell_vol = (self.dx * 1e-3) * (self.dy * 1e-3) * 1e-3
         P.charge_density = self.q * self.macro_weight / cell_vol
         self._poisson_params(P, params)
@@ -652,10 +670,10 @@ class DigitalTwinSimulator:
         P.E_th = self.sputter_E_th
         P.thresh = params.get('Thresh', 1e5)
         P.rT = self.Ly * 1e-3
-        a_corr = 1.0 / (1.0 - 1.0 / np.sqrt(2.0))
+        a_corr = 1.0 / (1.0 - 1.0 / _sqrt(2.0))
         P.n0a = params.get('n0', 1e20) * a_corr
-        P.neut_vth = np.sqrt(2.0 * self.kB * params.get('Tn', 300.0) / self.m_ion)
-        P.v_see_th = np.sqrt(2.0 * self.q * 2.0 / self.m_e)
+        P.neut_vth = _sqrt(2.0 * self.kB * params.get('Tn', 300.0) / self.m_ion)
+        P.v_see_th = _sqrt(2.0 * self.q * 2.0 / self.m_e)
         P.cooling_factor = (self.emissivity * self.sb_sigma * self.A_cell * self.dt * self.thermal_accel) / self.C_cell
         P.T4_300 = 300.0 ** 4
         alpha_diff = self.mat_k / (self.mat_rho * self.mat_cp)
@@ -683,9 +701,9 @@ class DigitalTwinSimulator:
             x_grid_mm = 0.5 * (self.grid_x_starts[0] + self.grid_x_ends[0])
         else:
             x_grid_mm = self.Lx * 0.5
-        x_idx = int(np.clip(round(x_grid_mm / self.dx), 0, self.nx - 1))
+        x_idx = int(_clip(round(x_grid_mm / self.dx), 0, self.nx - 1))
         if hole_centers:
-            return [int(np.clip(round(yc / self.dy), 0, self.ny - 1)) * self.nx + x_idx for yc in hole_centers]
+            return [int(_clip(round(yc / self.dy), 0, self.ny - 1)) * self.nx + x_idx for yc in hole_centers]
         return [(self.ny // 2) * self.nx + x_idx]
 
     # ------------------------------------------------------------------ the timestep
