@@ -240,6 +240,12 @@ int32_t pb_sim_set_profiling(pb_sim* s, int32_t on);
  * [20] set-up; [21+p] inner iterations and [26+p] refinement passes of Picard iteration p),
  * clears them and switches tracing on or off. */
 int32_t pb_sim_poisson_trace(pb_sim* s, int32_t on, double* out32);
+/* The three float32 sums of get_total_energy (physics_engine.py:1800-1866) on the device,
+ * each equal bit for bit to NumPy's np.sum (pairwise summation) of the same float32 array:
+ * out3[0] = sum(p_vx**2 + p_vy**2 + p_vz**2) over the ions, out3[1] the same over the
+ * electrons, out3[2] = sum(Ex**2 + Ey**2) over the grid (0 before a domain is set).
+ * Synchronises the simulator's stream. */
+int32_t pb_sim_energy_sums(pb_sim* s, double* out3);
 
 /* ---------------------------------------------------------------- host helpers */
 /* n sequential additions s = (float)((double)s + c), as np.add.at on a float32 array */

@@ -95,6 +95,7 @@ PROTOTYPES = {
     "pb_sim_timing": (i32, [vp, P(f64)]),
     "pb_sim_set_profiling": (i32, [vp, i32]),
     "pb_sim_poisson_trace": (i32, [vp, i32, P(f64)]),
+    "pb_sim_energy_sums": (i32, [vp, P(f64)]),
     "pb_sim_sort": (i32, [vp, i32, f64, f64]),
     "pb_batch_create": (i32, [P(vp), i32]),
     "pb_batch_destroy": (i32, [vp]),

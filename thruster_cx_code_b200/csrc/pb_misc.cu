@@ -686,4 +686,69 @@ __global__ void k_bdist_cols(const uint8_t* __restrict__ hrow, uint8_t* dist, in
   }
 }
 
+// ------------------------------------------------------------------ NumPy float32 sums
+// np.sum of a C-contiguous float32 array is 0 + pw(a, n), where pw is NumPy's pairwise
+// summation: for n < 8 a running sum from 0; for 8 <= n <= 128 eight running sums over
+// a[q], a[q + 8], ... (q = 0..7, started at a[q]) while a full group of eight remains,
+// combined as ((r0 + r1) + (r2 + r3)) + ((r4 + r5) + (r6 + r7)), then the remaining
+// elements in order; above 128, pw(a, m) + pw(a + m, n - m) with m = n / 2 rounded down to
+// a multiple of 8.  All in float32.  The host lays out that tree for n (leaf ranges, and
+// the internal nodes by height); k_pw_leaves sums the leaves and k_pw_combine the internal
+// nodes, so the result is NumPy's, bit for bit.  Element i is a_i^2 + b_i^2 (+ c_i^2),
+// rounded as NumPy evaluates a**2 + b**2 + c**2 on float32 arrays.
+struct PwSrc {
+  const float* a;
+  const float* b;
+  const float* c;  // may be null
+};
+
+__device__ __forceinline__ float pw_elem(const PwSrc& s, long long i) {
+  const float a = __ldg(s.a + i), b = __ldg(s.b + i);
+  float v = __fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b));
+  if (s.c) {
+    const float c = __ldg(s.c + i);
+    v = __fadd_rn(v, __fmul_rn(c, c));
+  }
+  return v;
+}
+
+__global__ void k_pw_leaves(PwSrc src, const long long* __restrict__ leaf_lo, int nleaves, float* vals) {
+  pdl_enter();
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nleaves; k += gridDim.x * blockDim.x) {
+    const long long lo = leaf_lo[k];
+    const int n = (int)(leaf_lo[k + 1] - lo);
+    float res;
+    if (n < 8) {
+      res = 0.0f;
+      for (int i = 0; i < n; ++i) res = __fadd_rn(res, pw_elem(src, lo + i));
+    } else {
+      float r[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) r[q] = pw_elem(src, lo + q);
+      int i = 8;
+      for (; i < n - (n % 8); i += 8) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) r[q] = __fadd_rn(r[q], pw_elem(src, lo + i + q));
+      }
+      res = __fadd_rn(__fadd_rn(__fadd_rn(r[0], r[1]), __fadd_rn(r[2], r[3])),
+                      __fadd_rn(__fadd_rn(r[4], r[5]), __fadd_rn(r[6], r[7])));
+      for (; i < n; ++i) res = __fadd_rn(res, pw_elem(src, lo + i));
+    }
+    vals[k] = res;
+  }
+}
+
+// one block: internal node j (height order) = vals[left[j]] + vals[right[j]], stored at
+// vals[nleaves + j]; then *out = 0 + the root (root < 0: no elements)
+__global__ void k_pw_combine(float* vals, const int* __restrict__ left, const int* __restrict__ right,
+                             const int* __restrict__ height_off, int nheights, int nleaves, int root, float* out) {
+  pdl_enter();
+  for (int h = 0; h < nheights; ++h) {
+    for (int j = height_off[h] + (int)threadIdx.x; j < height_off[h + 1]; j += blockDim.x)
+      vals[nleaves + j] = __fadd_rn(vals[left[j]], vals[right[j]]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = __fadd_rn(0.0f, root >= 0 ? vals[root] : 0.0f);
+}
+
 }  // namespace pb

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <functional>
 #include <utility>
 #include <vector>
 
@@ -124,6 +125,19 @@ struct Sim {
   bool counts_valid = false;
   bool domain_set = false;
   int host_num[2] = {0, 0};
+  // NumPy float32 sums (pb_sim_energy_sums): the summation tree per source (ions,
+  // electrons, field) and grow-only device copies of one tree at a time
+  struct PwTree {
+    long long n = -1;
+    std::vector<long long> leaf_lo;  // leaf k covers [leaf_lo[k], leaf_lo[k + 1])
+    std::vector<int> left, right;    // internal nodes in height order; node ids: leaves first
+    std::vector<int> height_off;     // internal nodes of height h + 1: [height_off[h], height_off[h + 1])
+    int root = -1;
+  } pw[3];
+  long long* pw_lo = nullptr;
+  int *pw_left = nullptr, *pw_right = nullptr, *pw_hoff = nullptr;
+  float *pw_vals = nullptr, *pw_out = nullptr;
+  size_t pw_cap_leaves = 0, pw_cap_nodes = 0, pw_cap_h = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
   // optional per-phase timing: events at 7 marks per step, reused across runs
@@ -863,6 +877,7 @@ int32_t pb_sim_destroy(pb_sim* h) {
       Soa& o = s->sp[k].buf[b];
       dfree(o.x); dfree(o.y); dfree(o.vx); dfree(o.vy); dfree(o.vz); dfree(o.id); dfree(o.cex);
     }
+  dfree(s->pw_lo); dfree(s->pw_left); dfree(s->pw_right); dfree(s->pw_hoff); dfree(s->pw_vals); dfree(s->pw_out);
   if (s->rep_host) cudaFreeHost(s->rep_host);
   if (s->rep_run) cudaFreeHost(s->rep_run);
   if (s->ev0) cudaEventDestroy(s->ev0);
@@ -1212,6 +1227,103 @@ int32_t pb_sim_synchronize(pb_sim* h) {
 }
 
 void* pb_sim_stream(pb_sim* h) { return (void*)h->s.stream; }
+
+// NumPy's pairwise summation tree for n elements (see k_pw_leaves): leaves of at most 128
+// elements in array order, internal nodes numbered after the leaves by height.
+static void pw_build(Sim::PwTree& t, long long n) {
+  t.n = n;
+  t.leaf_lo.clear();
+  t.left.clear();
+  t.right.clear();
+  t.height_off.assign(1, 0);
+  t.root = -1;
+  if (n <= 0) { t.leaf_lo.push_back(0); return; }
+  struct Node { int l, r, h; };  // children: >= 0 a leaf, < 0 internal node -(k + 1)
+  std::vector<Node> in;
+  std::function<std::pair<int, int>(long long, long long)> rec = [&](long long lo, long long len) {
+    if (len <= 128) {
+      t.leaf_lo.push_back(lo);
+      return std::make_pair((int)t.leaf_lo.size() - 1, 0);
+    }
+    long long m = len / 2;
+    m -= m % 8;
+    const std::pair<int, int> a = rec(lo, m), b = rec(lo + m, len - m);
+    const int h = std::max(a.second, b.second) + 1;
+    in.push_back({a.first, b.first, h});
+    return std::make_pair(-(int)in.size(), h);
+  };
+  const std::pair<int, int> top = rec(0, n);
+  const int L = (int)t.leaf_lo.size();
+  t.leaf_lo.push_back(n);
+  const int H = top.second;
+  t.height_off.assign(H + 1, 0);
+  for (const Node& x : in) ++t.height_off[x.h];  // count per height, shifted by one
+  for (int h = 1; h <= H; ++h) t.height_off[h] += t.height_off[h - 1];
+  std::vector<int> pos(in.size()), fill(t.height_off.begin(), t.height_off.end() - 1);
+  for (size_t k = 0; k < in.size(); ++k) pos[k] = fill[in[k].h - 1]++;
+  auto id = [&](int c) { return c >= 0 ? c : L + pos[-c - 1]; };
+  t.left.assign(in.size(), 0);
+  t.right.assign(in.size(), 0);
+  for (size_t k = 0; k < in.size(); ++k) {
+    t.left[pos[k]] = id(in[k].l);
+    t.right[pos[k]] = id(in[k].r);
+  }
+  t.root = id(top.first);
+}
+
+// np.sum of one float32 source on the device, NumPy's rounding; result in *out_dev
+static int32_t pw_sum(Sim* s, int which, long long n, PwSrc src, float* out_dev) {
+  Sim::PwTree& t = s->pw[which];
+  if (t.n != n) pw_build(t, n);
+  const size_t L = t.leaf_lo.size() - 1, I = t.left.size(), H = t.height_off.size();
+  if (L + 1 > s->pw_cap_leaves) {
+    dfree(s->pw_lo);
+    CK(dalloc(&s->pw_lo, L + 1));
+    s->pw_cap_leaves = L + 1;
+  }
+  if (L + I + 1 > s->pw_cap_nodes) {
+    dfree(s->pw_vals); dfree(s->pw_left); dfree(s->pw_right);
+    CK(dalloc(&s->pw_vals, L + I + 1)); CK(dalloc(&s->pw_left, L + I + 1)); CK(dalloc(&s->pw_right, L + I + 1));
+    s->pw_cap_nodes = L + I + 1;
+  }
+  if (H > s->pw_cap_h) {
+    dfree(s->pw_hoff);
+    CK(dalloc(&s->pw_hoff, H));
+    s->pw_cap_h = H;
+  }
+  cudaStream_t st = s->stream;
+  CK(cudaMemcpyAsync(s->pw_lo, t.leaf_lo.data(), (L + 1) * sizeof(long long), cudaMemcpyHostToDevice, st));
+  if (I) {
+    CK(cudaMemcpyAsync(s->pw_left, t.left.data(), I * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(s->pw_right, t.right.data(), I * sizeof(int), cudaMemcpyHostToDevice, st));
+  }
+  CK(cudaMemcpyAsync(s->pw_hoff, t.height_off.data(), H * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (L) k_pw_leaves<<<grid_for(s, (long)L, 128), 128, 0, st>>>(src, s->pw_lo, (int)L, s->pw_vals);
+  k_pw_combine<<<1, 1024, 0, st>>>(s->pw_vals, s->pw_left, s->pw_right, s->pw_hoff, (int)H - 1, (int)L, t.root,
+                                   out_dev);
+  CK(cudaGetLastError());
+  return PB_OK;
+}
+
+int32_t pb_sim_energy_sums(pb_sim* h, double* out3) {
+  Sim* s = &h->s;
+  if (!out3) return fail(PB_ERR_ARG, "pb_sim_energy_sums: null output");
+  CK(cudaSetDevice(s->device));
+  int32_t rc;
+  if ((rc = read_counts(s))) return rc;
+  if (!s->pw_out) CK(dalloc(&s->pw_out, 3));
+  const Soa& I = s->sp[0].buf[s->sp[0].cur];
+  const Soa& E = s->sp[1].buf[s->sp[1].cur];
+  const PwSrc src[3] = {{I.vx, I.vy, I.vz}, {E.vx, E.vy, E.vz}, {s->Ex, s->Ey, nullptr}};
+  const long long n[3] = {s->host_num[0], s->host_num[1], s->domain_set ? (long long)s->ny * s->nx : 0};
+  for (int k = 0; k < 3; ++k)
+    if ((rc = pw_sum(s, k, n[k], src[k], s->pw_out + k))) return rc;
+  float f[3];
+  CK(cudaMemcpyAsync(f, s->pw_out, sizeof(f), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < 3; ++k) out3[k] = (double)f[k];
+  return PB_OK;
+}
 
 int32_t pb_sim_timing(pb_sim* h, double* out) {
   Sim* s = &h->s;

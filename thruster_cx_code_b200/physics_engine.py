@@ -867,13 +867,17 @@ class DigitalTwinSimulator:
         return self.current_ppc_map.astype(np.float64)
 
     def get_total_energy(self):
+        """``physics_engine.py:1800-1866``.  The three float32 sums run on the device
+        (pb_sim_energy_sums), equal bit for bit to NumPy's np.sum of the same arrays, so
+        no particle or field array is copied to the host."""
         t_now = self.iteration * self.dt
-        ke_i = float(np.sum(self.p_vx ** 2 + self.p_vy ** 2 + self.p_vz ** 2)) * 0.5 * self.m_ion * self.macro_weight \
-            if self.num_p > 0 else 0.0
-        ke_e = float(np.sum(self.e_vx ** 2 + self.e_vy ** 2 + self.e_vz ** 2)) * 0.5 * self.m_e * self.macro_weight \
-            if self.num_e > 0 else 0.0
+        self._flush()
+        sums = (C.c_double * 3)()
+        _lib.check(self._libh.pb_sim_energy_sums(self._h, sums), "get_total_energy")
+        ke_i = float(sums[0]) * 0.5 * self.m_ion * self.macro_weight if self.num_p > 0 else 0.0
+        ke_e = float(sums[1]) * 0.5 * self.m_e * self.macro_weight if self.num_e > 0 else 0.0
         cell_area = (self.dx * 1e-3) * (self.dy * 1e-3)
-        e_field = float(np.sum(self.Ex ** 2 + self.Ey ** 2)) * 0.5 * self.eps0 * cell_area
+        e_field = float(sums[2]) * 0.5 * self.eps0 * cell_area
         total = ke_i + ke_e + e_field
         if self._prev_total_energy is not None and self._prev_total_energy > 0.0:
             rel = abs(total - self._prev_total_energy) / self._prev_total_energy
