@@ -181,10 +181,9 @@ __device__ __forceinline__ T apply0(const PoissonArgs& a, const T* v, int i, int
 // Restricted residual at coarse node (I, J) of level 1, from the fine level F (5-point
 // operator, off-diagonals -1 to every neighbour; d r is zero on non-free nodes):
 //   sum_children w_f * [f active] * ((1 - w) r_f + sum_{k nbr of f} d_k r_k).
-// rl(j) gives the fine residual at node j; each patch node is loaded once.  wrapC: the
-// coarse level's prolongation wraps in y.
-template <class RL>
-__device__ __forceinline__ float restrict0(const MgLevel& F, const RL& rl, int I, int J, bool wrapC) {
+// r is the fine residual; each patch node is loaded once.  wrapC: the coarse level's
+// prolongation wraps in y.
+__device__ __forceinline__ float restrict0(const MgLevel& F, const float* r, int I, int J, bool wrapC) {
   const int ny = F.ny, nx = F.nx;
   int ro[5];
   bool rv[5];
@@ -210,7 +209,7 @@ __device__ __forceinline__ float restrict0(const MgLevel& F, const RL& rl, int I
       if ((t == 0 || t == 4) && (u == 0 || u == 4)) { zp[t][u] = rq[t][u] = dq[t][u] = 0.0f; continue; }
       const bool ok = rv[t] && cv[u];
       const int j = ok ? ro[t] + xo[u] : 0;
-      const float d = __ldg(F.dinv + j), rj = rl(j);
+      const float d = __ldg(F.dinv + j), rj = *(r + j);
       dq[t][u] = d;
       rq[t][u] = rj;
       zp[t][u] = ok ? d * rj : 0.0f;
@@ -232,12 +231,6 @@ __device__ __forceinline__ float restrict0(const MgLevel& F, const RL& rl, int I
   }
   return s;
 }
-
-// fine residual loaders of restrict0
-struct RPlain {
-  const float* r;
-  __device__ __forceinline__ float operator()(int j) const { return *(r + j); }
-};
 
 // (P z_c) at fine node (y, x) of the level above C
 __device__ __forceinline__ float prolong(const MgLevel& C, const float* zc, int y, int x) {
@@ -363,7 +356,7 @@ __device__ void down_leg(const PoissonArgs& a, int level, int tid, int nth) {
   for (int ic = tid; ic < Nc; ic += nth) {
     const int I = ic / C.nx, J = ic - I * C.nx;
     if (LV0) {
-      const float s = restrict0(F, RPlain{F.r}, I, J, C.wrapP != 0);
+      const float s = restrict0(F, F.r, I, J, C.wrapP != 0);
       __stcg(C.r + ic, __ldg(C.dinv + ic) > 0.0f ? s : 0.0f);
     } else {
       __stcg(C.r + ic, restrict_pre(F, C, F.r, I, J, ic));
