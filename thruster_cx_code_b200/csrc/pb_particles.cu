@@ -545,8 +545,13 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
   const float dtf = __double2float_rn(dt_sub);
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.n_sub_out = n_sub;
   const float pi_f = 3.14159265358979323846f;
-  unsigned long long cnt[7] = {0, 0, 0, 0, 0, 0, 0};
-  double sums[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  // per-thread event counts (32-bit: a thread sees far fewer than 2^32 ions); the exit
+  // sums, whose ions are rare, go straight to shared memory, so neither holds registers
+  // across the loop
+  unsigned int cnt[7] = {0, 0, 0, 0, 0, 0, 0};
+  __shared__ double sums[9];
+  if (threadIdx.x < 9) sums[threadIdx.x] = 0.0;
+  __syncthreads();
 
   while (true) {
     if (threadIdx.x == 0) sm_tile = atomicAdd(a.tile_counter, 1);
@@ -639,9 +644,10 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
           cnt[1]++;
           float ve = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
           float Ee = __fdiv_rn(__fmul_rn(a.k_half_m, __fmul_rn(ve, ve)), a.q_f);
-          sums[0] += vx; sums[1] += ve; sums[2] += Ee;
-          sums[7] += (double)vx * vx; sums[8] += (double)ve * ve;
-          if (cx) { sums[5] += ve; sums[6] += 1.0; } else { sums[3] += ve; sums[4] += 1.0; }
+          atomicAdd(&sums[0], (double)vx); atomicAdd(&sums[1], (double)ve); atomicAdd(&sums[2], (double)Ee);
+          atomicAdd(&sums[7], (double)vx * vx); atomicAdd(&sums[8], (double)ve * ve);
+          if (cx) { atomicAdd(&sums[5], (double)ve); atomicAdd(&sums[6], 1.0); }
+          else { atomicAdd(&sums[3], (double)ve); atomicAdd(&sums[4], 1.0); }
           int r = atomicAdd(a.angle_count, 1);
           float ang = __fdiv_rn(__fmul_rn(fabsf(atan2f(vy, vx)), 180.0f), pi_f);
           if (r < a.angle_cap) a.angles[r] = ang; else atomicOr(a.errflags, PB_EF_ANGLE_OVERFLOW);
@@ -729,12 +735,8 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(a.counters + j, v);
   }
-#pragma unroll
-  for (int j = 0; j < 9; ++j) {
-    double v = sums[j];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
-    if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(a.exit_sums + j, v);
-  }
+  __syncthreads();
+  if (threadIdx.x < 9 && sums[threadIdx.x] != 0.0) atomicAdd(a.exit_sums + threadIdx.x, sums[threadIdx.x]);
 }
 
 // ------------------------------------------------------------------ fused electron step
