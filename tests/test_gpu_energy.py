@@ -67,3 +67,25 @@ def test_sums_at_pairwise_edges(lib, n):
     for d, r in zip(dev, ref):
         assert d.tobytes() == r.tobytes(), (n, d, r)
     sim.close()
+
+
+def test_energy_warning_on_a_jump(lib, capsys):
+    """The reference's conservation check (physics_engine.py:1847-1856): a call whose total
+    energy differs from the previous call's by more than energy_warning_threshold prints the
+    warning, a smaller change does not, and every call is kept in the history."""
+    sim, params = W.make_sweep_sim(_spec())
+    sim.step(params)
+    capsys.readouterr()
+    first = sim.get_total_energy()
+    again = sim.get_total_energy()  # no change
+    assert again["total_J"] == first["total_J"]
+    assert "[Energy Warning]" not in capsys.readouterr().out
+    # the electrode field holds nearly all of the energy here: doubling it quadruples the total
+    sim.Ex = np.asarray(sim.Ex) * np.float32(2.0)
+    sim.Ey = np.asarray(sim.Ey) * np.float32(2.0)
+    second = sim.get_total_energy()
+    rel = abs(second["total_J"] - first["total_J"]) / first["total_J"]
+    assert rel > sim.energy_warning_threshold, rel
+    assert "[Energy Warning]" in capsys.readouterr().out
+    assert len(sim.energy_history_tot) == 3
+    sim.close()
