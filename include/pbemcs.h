@@ -56,10 +56,12 @@ int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t nu
  * that must stay off the driver's allocation path, fixed device-memory budgets).  It has
  * no counterpart in the reference.  The per-cell count scratch is a file-scope device
  * array of 2^21 int32 (8 MiB) that every GPU loading the library holds until exit;
- * grids of more than 2^21 cells are rejected with PB_ERR_ARG.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress) and should come before any
- * stream capture.  All calls share the array and it keeps the last call's counts (each
- * call clears the cells it uses first), so calls that overlap on the GPU race. */
+ * grids of more than 2^21 cells are rejected with PB_ERR_ARG.  Each call looks up the
+ * array's device address in the current context (cudaGetSymbolAddress); the first call in
+ * a context loads the module and should come before any stream capture.  All calls share
+ * the array, so calls that overlap on the GPU race.  A completed call leaves the cells it
+ * used at zero (the rho pass clears every count it reads); each call still clears them
+ * first, in case an earlier call was cut off between its count and rho passes. */
 int32_t pb_accumulate_rho_noalloc(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy,
                                   int32_t nx, int32_t ny, double charge_density, void* stream);
 

@@ -1,8 +1,9 @@
 """Golden outputs of the reference's config parser (parse_config in
 Python/run_simulation_from_config.py:30-194) for three configs written here, saved as
-config_cases.json next to this file.  Run where the reference checkout is mounted:
+config_cases.json next to this file.  Run where the reference checkout is mounted, naming
+its root in PYBEMCS_REFERENCE:
 
-    python tests/golden/make_config_golden.py
+    PYBEMCS_REFERENCE=<checkout root> python tests/golden/make_config_golden.py
 
 The cross-section tables in config/ are data of this test (a power law and a linear
 yield), not reference files.

@@ -1,9 +1,8 @@
 """Generate the golden fixtures by running the reference PY-BEMCS engine itself.
 
-Run where the reference checkout is mounted (``PYBEMCS_REFERENCE`` or the default path
-in ``reference_loader``):
+Run where the reference checkout is mounted, naming its root in ``PYBEMCS_REFERENCE``:
 
-    python tests/golden/make_golden.py
+    PYBEMCS_REFERENCE=<checkout root> python tests/golden/make_golden.py
 
 Every fixture is produced by calling the reference module (``Python/physics_engine.py``,
 loaded unmodified with a taichi stand-in) on seeded synthetic inputs.  The outputs

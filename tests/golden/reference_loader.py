@@ -20,12 +20,14 @@ import types
 
 import numpy as np
 
-REFERENCE_ROOT = os.environ.get("PYBEMCS_REFERENCE", "/root/reference")
-ENGINE_PATH = os.path.join(REFERENCE_ROOT, "Python", "physics_engine.py")
+# The reference checkout is named by the environment only (no default path):
+#   PYBEMCS_REFERENCE=<checkout root> python tests/golden/make_golden.py
+REFERENCE_ROOT = os.environ.get("PYBEMCS_REFERENCE", "")
+ENGINE_PATH = os.path.join(REFERENCE_ROOT, "Python", "physics_engine.py") if REFERENCE_ROOT else ""
 
 
 def reference_available():
-    return os.path.isfile(ENGINE_PATH)
+    return bool(ENGINE_PATH) and os.path.isfile(ENGINE_PATH)
 
 
 def _taichi_stub():
@@ -45,7 +47,8 @@ def load_engine(fp64=False, name=None):
     mode).  Each call returns an independent module object.
     """
     if not reference_available():
-        raise FileNotFoundError(ENGINE_PATH)
+        raise FileNotFoundError("set PYBEMCS_REFERENCE to the reference checkout root (found: "
+                                f"{REFERENCE_ROOT!r})")
     sys.modules.setdefault("taichi", _taichi_stub())
     had_frozen = hasattr(sys, "frozen")
     old_frozen = getattr(sys, "frozen", None)

@@ -6,11 +6,11 @@ another framework's pool, a real-time loop that has to stay off the driver's all
 path, or a process with a device-memory budget fixed at start-up.  It keeps its count
 scratch in a static device array of 2^21 cells instead of allocating.
 
-The test compares it with the regular pb_accumulate_rho (bit for bit, the tolerance all
-deposit tests use) on two calls in a row on the same rho, so that a second call that
-saw the first call's stale counts would be caught, and checks that a grid above the
-array's size is refused.  This file is collected last so that a failure here leaves
-every other test already run.
+The test compares it with the regular pb_accumulate_rho bit for bit (the tolerance all
+deposit tests use) on two calls in a row on the same rho, ions then electrons, and
+against the reference's deposit fixture; it also checks that a grid above the array's
+size is refused before any work.  This file is collected last so that a failure here
+leaves every other test already run.
 """
 import numpy as np
 import pytest

@@ -1380,10 +1380,13 @@ int32_t pb_push_particles_boris(float* x, float* y, float* vx, float* vy, float*
 
 int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy, int32_t nx,
                           int32_t ny, double charge_density, void* stream) {
-  if (num_p <= 0) return PB_OK;
   if (nx < 3 || ny < 3) return fail(PB_ERR_ARG, "accumulate_rho: grid must be at least 3 x 3");
+  const long long G64 = (long long)nx * ny;
+  if (G64 > INT32_MAX) return fail(PB_ERR_ARG, "accumulate_rho: grid of " + std::to_string(G64) +
+                                                   " cells exceeds 2^31 - 1");
+  if (num_p <= 0) return PB_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  int G = nx * ny;
+  const int G = (int)G64;
   int* cnt = nullptr;
   CK(cudaMallocAsync((void**)&cnt, (size_t)G * sizeof(int), st));
   CK(cudaMemsetAsync(cnt, 0, (size_t)G * sizeof(int), st));
@@ -1409,25 +1412,18 @@ int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t nu
 #define PB_NOALLOC_MAX_CELLS (1 << 21)
 static __device__ __align__(256) int g_noalloc_counts[PB_NOALLOC_MAX_CELLS];
 
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[256] = {nullptr};
-
-// Device address of the scratch array for the current device.  In host code the
-// array's name is only a host-side stand-in, so the address is looked up once per device
-// (with that device current) and cached.
+// Device address of the scratch array in the context current on the calling thread.  In
+// host code the array's name is only a host-side stand-in, so the address is looked up on
+// every call: that is cheap once the module is loaded, and it stays right after
+// cudaDeviceReset or under a context other than the device's primary one (a cached
+// address would belong to the context it was taken in).  The first call in a context
+// loads the module.
 static int32_t noalloc_scratch(int** out) {
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 256) return fail(PB_ERR_ARG, "accumulate_rho_noalloc: device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_counts);
-    if (e != cudaSuccess || !p)
-      return fail(PB_ERR_CUDA, std::string("accumulate_rho_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_noalloc_ptr[dev] = p;
-  }
-  *out = (int*)g_noalloc_ptr[dev];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_counts);
+  if (e != cudaSuccess || !p)
+    return fail(PB_ERR_CUDA, std::string("accumulate_rho_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  *out = (int*)p;
   return PB_OK;
 }
 
@@ -1445,7 +1441,9 @@ int32_t pb_accumulate_rho_noalloc(const float* x, const float* y, float* rho, in
   if (rc) return rc;
   if (num_p <= 0) return PB_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  // the array keeps the previous call's counts: clear the cells this call uses
+  // k_rho_finalize zeroes every count it reads, so after a call has completed the cells it
+  // used are zero again.  This clear guards against a call that was cut off between its
+  // two kernels (an error or a cancelled stream), which would leave counts behind.
   CK(cudaMemsetAsync(cnt, 0, (size_t)G * sizeof(int), st));
   int g = (int)std::min<long>((num_p + 255) / 256, 148L * 16);
   k_count_cells<<<g, 256, 0, st>>>(x, y, nullptr, num_p, 0, cnt, nx, ny, (float)dx, (float)dy);

@@ -5,7 +5,7 @@ Restates the geometry part of ``DigitalTwinSimulator.build_domain``
 stack, node counts, electrode masks with chamfer and thermal bow, Dirichlet values,
 the plasma boundary column and the macro-particle weight.  The arithmetic follows the
 reference operation by operation (Python floats, NumPy float64 meshes) so that node
-counts, spacings and masks come out identical; ``tests/test_domain.py`` pins them
+counts, spacings and masks come out identical; ``tests/test_oracle_golden.py`` pins them
 against the reference's own outputs.
 
 The function mutates the simulator object it is given, exactly as the reference

@@ -907,31 +907,40 @@ class DigitalTwinSimulator:
         return (self.num_p > 0) or (self.num_e > 0)
 
     def get_groove_profile(self, grid_idx, thresh=None, accumulate_subcell=True, face='upstream'):
-        if grid_idx < 0 or grid_idx >= len(self.mask_grids):
-            return np.array([]), np.array([])
-        mask = self.mask_grids[grid_idx]
-        if not np.any(mask):
-            return np.array([]), np.array([])
-        depth = self.eroded_depth
-        if accumulate_subcell and thresh and thresh > 0:
-            depth = depth + (self.damage_map / thresh) * self.dy
-        y_mm = np.arange(self.ny) * self.dy
-        per_y = np.zeros(self.ny, dtype=np.float64)
-        has_any = mask.any(axis=1)
-        if face == 'any':
-            cols = np.any(mask, axis=0)
-            if not np.any(cols):
-                return np.array([]), np.array([])
-            per_y[has_any] = depth[has_any][:, cols].max(axis=1)
-        elif face == 'upstream':
-            first_idx = np.argmax(mask, axis=1)
-            per_y[has_any] = depth[np.where(has_any)[0], first_idx[has_any]]
-        elif face == 'downstream':
-            last_idx = self.nx - 1 - np.argmax(mask[:, ::-1], axis=1)
-            per_y[has_any] = depth[np.where(has_any)[0], last_idx[has_any]]
-        else:
+        """Eroded depth along y on one face of grid ``grid_idx`` (the reference's diagnostic
+        of ``Python/physics_engine.py:1903-1932``, same arguments and results).
+
+        A row's depth is read where the grid's mask meets it: at the row's first mask column
+        for ``face='upstream'``, at its last one for ``'downstream'``, or as the largest depth
+        over every column the grid occupies (in any row) for ``'any'``.  The depth map is the
+        eroded depth of broken cells, plus the worn fraction of a cell (damage / thresh * dy)
+        when ``accumulate_subcell`` and a positive ``thresh`` are given.  Rows the mask does
+        not meet read 0.  Returns (y in mm per row, depth in um per row); two empty arrays
+        for an unknown grid or an empty mask, and ValueError for any other face."""
+        nothing = (np.array([]), np.array([]))
+        if not 0 <= grid_idx < len(self.mask_grids):
+            return nothing
+        rows, cols = np.nonzero(np.asarray(self.mask_grids[grid_idx], dtype=bool))
+        if rows.size == 0:
+            return nothing
+        if face not in ('upstream', 'downstream', 'any'):
             raise ValueError(f"face must be 'upstream','downstream', or 'any' (got {face!r})")
-        return y_mm, per_y * 1000.0
+        dmap = self.eroded_depth
+        if accumulate_subcell and thresh and thresh > 0:
+            dmap = dmap + (self.damage_map / thresh) * self.dy
+        # np.nonzero lists mask cells row by row with columns ascending, so each row's run
+        # starts at its first mask column and ends at its last
+        met, run_start = np.unique(rows, return_index=True)
+        run_end = np.append(run_start[1:], rows.size) - 1
+        if face == 'upstream':
+            at_face = dmap[met, cols[run_start]]
+        elif face == 'downstream':
+            at_face = dmap[met, cols[run_end]]
+        else:
+            at_face = dmap[np.ix_(met, np.unique(cols))].max(axis=1)
+        profile = np.zeros(self.ny, dtype=np.float64)
+        profile[met] = at_face
+        return np.arange(self.ny) * self.dy, profile * 1000.0
 
     def get_particle_kinematics(self):
         t_current = self.iteration * self.dt
