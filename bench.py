@@ -7,19 +7,32 @@ solve on even steps, sub-stepped push with absorption and tallies, compaction, C
 and diagnostics) over the workload's particles.  particle-pushes = sum over species of
 particles pushed x sub-steps, as the reference counts push calls.
 
+The headline workload is long_erosion_3grid: 513 x 2049 nodes, 48M Xe+ and 16M electrons,
+the largest configuration that one GPU holds.  large_aperture_3grid (257 x 1025 nodes, 8M
+particles) is reported beside it under "workloads".
+
 value: K steps enqueued back to back with the state resident in HBM, timed with CUDA
        events on the simulator's stream, max over ranks (replicas, weak scaling).
 e2e:   K calls of the public DigitalTwinSimulator.step(params) (per-step parameters copied
-       in, the step report copied out), wall clock after a device synchronize.
-roofline: the fused ion-step kernel, algorithmic bytes 41 B per ion per launch
-       (20 B state read + 20 B written + 1 B flag) over its event-timed duration, against
-       the measured HBM copy bandwidth.
-cpu_baseline: the CPU oracle (a NumPy restatement of the reference step, numerically the
-       reference's own path) on one core, on a bounded sample of the same workload.
---impl reference: the same oracle on all host cores (one process per core, each stepping
-       the workload's grid with an equal share of the particles), rank 0 only.
+       in, the step report copied out), wall clock after a device synchronize, on a fresh
+       simulator that repeats the timed steps exactly.
+roofline: the fused particle kernels, algorithmic bytes 41 B per particle and launch
+       (20 B state read + 20 B written + 1 B flag) over each kernel's event-timed duration,
+       against the measured HBM copy bandwidth; push + deposit together at 49 B per
+       particle-step.  DRAM traffic per particle comes from the committed ncu summary and is
+       reported only while the kernel sources still hash to the value recorded there.
+sweep: C3-scale perveance sweep (64 points, 0.2M-4M particles, three grid sizes) plain
+       against batched, and a C4-scale served run (Poisson arrivals, 1M-6M particles,
+       retirement at < 0.5% change over 500 steps).
+cpu_baseline: the CPU oracle (a NumPy restatement of the reference step, pinned bit for bit
+       to the reference's own outputs) on one core.  A bounded particle sample runs on the
+       full grid; its particle time is scaled linearly to the workload's particle count and
+       the measured full-grid field-solve time is added once per step.
+--impl reference: the same measurement on all host cores, one full-workload replica per
+       core (forked after one shared domain build), rank 0 only.
 """
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -33,8 +46,15 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-DEFAULT_WORKLOAD = "large_aperture_3grid"
-ALG_BYTES_PER_ION = 41
+DEFAULT_WORKLOAD = "long_erosion_3grid"
+SECOND_WORKLOAD = "large_aperture_3grid"
+ALG_BYTES_PUSH = 41     # per particle and fused step-kernel launch
+ALG_BYTES_DEPOSIT = 8   # per particle deposited (x, y)
+TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "dram_traffic_large_aperture_3grid.md")
+KERNEL_SOURCES = ("pb_particles.cu", "pb_common.cuh", "pb_kernels.cuh")
+# fine phases of pb_sim_phase_times
+PHASES = ("inject_deposit", "field_solve", "corners_substeps", "ion_step", "sputter_break", "electron_step",
+          "see_spawn", "thermal_grid_sums", "diagnostics_sort")
 
 
 def parse():
@@ -47,6 +67,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-second", action="store_true", help="skip the large_aperture_3grid line")
+    ap.add_argument("--sweep-points", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-max-steps", type=int, default=4000)
     return ap.parse_args()
 
 
@@ -124,17 +148,36 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
-def ion_step_traffic_per_ion():
-    """DRAM bytes per ion of one k_ion_step launch, from the 'dram_bytes_per_ion:' line of
-    the committed ncu summary, if present."""
+def kernel_source_sha():
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        with open(os.path.join(ROOT, "thruster_cx_code_b200", "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
+def traffic_table():
+    """DRAM bytes per particle of each step kernel from the committed ncu summary:
+    ({kernel: bytes per particle}, note).  Empty when the summary was taken on kernel
+    sources other than the current ones (its 'kernel_source_sha:' line)."""
     try:
-        with open(os.path.join(ROOT, "profiles", "k_ion_step_large_aperture_3grid.md")) as f:
-            for line in f:
-                if line.strip().startswith("dram_bytes_per_ion:"):
-                    return float(line.split(":", 1)[1].split()[0])
-    except Exception:
-        pass
-    return None
+        with open(TRAFFIC_PROFILE) as f:
+            lines = f.read().splitlines()
+    except OSError:
+        return {}, "no ncu traffic summary"
+    sha, table = None, {}
+    for ln in lines:
+        s = ln.strip()
+        if s.startswith("kernel_source_sha:"):
+            sha = s.split(":", 1)[1].strip()
+        elif s.startswith("dram_bytes_per_particle:"):
+            parts = s.split(":", 1)[1].split()
+            if len(parts) >= 2:
+                table[parts[0]] = float(parts[1])
+    cur = kernel_source_sha()
+    if sha != cur:
+        return {}, f"stale: ncu summary taken on kernel sources {sha}, current {cur}"
+    return table, f"ncu summary on kernel sources {cur}"
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -162,6 +205,64 @@ def pushes_of(reports, n_p0, n_e0):
     return tot
 
 
+def timed_run(sim, params, K, profile=True):
+    """K steps through pb_sim_run.  Returns a dict: device ms, reports, fine phase sums
+    (ms over the K steps), launches, pushes and the mean particles per step-kernel launch."""
+    import ctypes as C
+    from thruster_cx_code_b200 import _lib
+    lib = _lib.load()
+    it0 = sim.iteration
+    plist = []
+    for k in range(K):
+        sim.iteration = it0 + k
+        plist.append(sim.step_params(params))
+    sim.iteration = it0
+    P = (_lib.StepParams * K)(*plist)
+    R = (_lib.StepReport * K)()
+    n_p0, n_e0 = sim.num_p, sim.num_e
+    stats_before = list(sim.last_report.poisson_stats) if sim.last_report is not None else None
+    lib.pb_sim_set_profiling(sim._h, 1 if profile else 0)
+    _lib.check(lib.pb_sim_run(sim._h, P, K, R), "pb_sim_run")
+    tm = (C.c_double * 9)()
+    lib.pb_sim_timing(sim._h, tm)
+    ph = (C.c_double * 10)()
+    lib.pb_sim_phase_times(sim._h, ph)
+    lib.pb_sim_set_profiling(sim._h, 0)
+    sim.iteration = it0 + K
+    sim._invalidate()
+    for r in R:
+        sim._apply_report(r, params)
+    ions = [(n_p0 if k == 0 else R[k - 1].num_p) + R[k].injected for k in range(K)]
+    eles = [(n_e0 if k == 0 else R[k - 1].num_e) + R[k].rf_injected + R[k].neut_injected for k in range(K)]
+    return {"ms": float(tm[0]), "reports": R, "phases": {k: float(ph[i]) for i, k in enumerate(PHASES)},
+            "launches": int(tm[8]), "pushes": pushes_of(R, n_p0, n_e0), "n_p0": n_p0, "n_e0": n_e0,
+            "ions_per_launch": float(np.mean(ions)), "eles_per_launch": float(np.mean(eles)),
+            "stats_before": stats_before}
+
+
+def kernel_rooflines(run, K, peak, traffic):
+    """Roofline entries of the fused particle kernels and of push + deposit together."""
+    ph = run["phases"]
+    out = {}
+    for kern, phase, n in (("k_ion_step", "ion_step", run["ions_per_launch"]),
+                           ("k_ele_step", "electron_step", run["eles_per_launch"])):
+        t = ph[phase] / K * 1e-3
+        ach = ALG_BYTES_PUSH * n / t / 1e9 if t > 0 else None
+        tb = traffic.get(kern)
+        out[kern] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak if ach else None, "launch_ms": t * 1e3, "particles_per_launch": n,
+                     "algorithmic_bytes_per_launch": ALG_BYTES_PUSH * n,
+                     "traffic": tb * n if tb else None}
+    n_all = run["ions_per_launch"] + run["eles_per_launch"]
+    t_pd = (ph["ion_step"] + ph["electron_step"] + ph["inject_deposit"]) / K * 1e-3
+    ach = (ALG_BYTES_PUSH + ALG_BYTES_DEPOSIT) * n_all / t_pd / 1e9 if t_pd > 0 else None
+    out["push_deposit"] = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                           "frac": ach / peak if ach else None, "bytes_per_particle_step": 49,
+                           "time": "ion step + electron step + injection/deposit phase per step",
+                           "ms_per_step": t_pd * 1e3}
+    return out
+
+
 def gpu_arm(args):
     import ctypes as C
     import torch
@@ -172,48 +273,26 @@ def gpu_arm(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    lib = _lib.load()
+    _lib.load()
     sim, params = make_gpu_sim(args.workload, local, seed=1000 + rank)
     for _ in range(args.warmup):
         sim.step(params)
-    # ---- device-timed region: K steps enqueued back to back
     K = args.steps
-    plist = []
-    it0 = sim.iteration
-    for k in range(K):
-        sim.iteration = it0 + k
-        plist.append(sim.step_params(params))
-    sim.iteration = it0
-    P = (_lib.StepParams * K)(*plist)
-    R = (_lib.StepReport * K)()
-    n_p0, n_e0 = sim.num_p, sim.num_e
-    stats_before = list(sim.last_report.poisson_stats) if sim.last_report is not None else None
-    lib.pb_sim_set_profiling(sim._h, 1)
     clocks = ClockSampler(local)
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    _lib.check(lib.pb_sim_run(sim._h, P, K, R), "pb_sim_run")
+    run = timed_run(sim, params, K)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    tm = (C.c_double * 9)()
-    lib.pb_sim_timing(sim._h, tm)
-    lib.pb_sim_set_profiling(sim._h, 0)
-    ms = float(tm[0])
-    sim.iteration = it0 + K
-    sim._invalidate()
-    for r in R:
-        sim._apply_report(r, params)
-    pushes = pushes_of(R, n_p0, n_e0)
-    ion_ms_total = float(tm[4])
-    ions_per_launch = float(np.mean([n_p0 if k == 0 else R[k - 1].num_p for k in range(K)]) +
-                        np.mean([r.injected for r in R]))
+    ms, pushes = run["ms"], run["pushes"]
     if world > 1:
         ms_max, pushes_all = reduce_over_ranks(ms, pushes, "cuda")
     else:
         ms_max, pushes_all = ms, float(pushes)
     value = pushes_all / (ms_max * 1e-3)
+    ny, nx = sim.ny, sim.nx
     # ---- end to end through the public API, on the same steps: a fresh simulator with
     # the same seed and warm-up reproduces the timed region's workload exactly
     e2e = None
@@ -240,38 +319,57 @@ def gpu_arm(args):
         e2e = {"value": pe2e / wall, "unit": "particle-pushes/s", "h2d_bytes_per_step": C.sizeof(_lib.StepParams),
                "d2h_bytes_per_step": C.sizeof(_lib.StepReport), "same_steps_as_value": pe2e == pushes_all}
     peak, peak_kind = measured_peak_gbs()
-    ion_launch_s = ion_ms_total / K * 1e-3
-    achieved = ALG_BYTES_PER_ION * ions_per_launch / ion_launch_s / 1e9 if ion_launch_s > 0 else None
-    tpi = ion_step_traffic_per_ion()
-    roof = {"kernel": "k_ion_step", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
-            "traffic": tpi * ions_per_launch if tpi else None,
-            "algorithmic_bytes_per_launch": ALG_BYTES_PER_ION * ions_per_launch,
-            "launch_ms": ion_launch_s * 1e3,
-            "phase_ms_per_step": {k: float(tm[i + 1]) / K for i, k in enumerate(
-                ["inject_deposit", "field_solve", "substep_reduce", "ion_step", "electron_step", "thermal_diag_sort"])}}
+    traffic, traffic_note = traffic_table()
+    kr = kernel_rooflines(run, K, peak, traffic)
+    # the dominant kernel of the step: the electron step (many sub-steps per launch)
+    dom = "k_ele_step" if kr["k_ele_step"]["launch_ms"] >= kr["k_ion_step"]["launch_ms"] else "k_ion_step"
+    roof = dict(kr[dom])
+    roof.update({"kernel": dom, "peak_source": peak_kind, "traffic_source": traffic_note,
+                 "limiter": "instruction issue (float64 weights and conversions per sub-step), not DRAM",
+                 "kernels": kr,
+                 "phase_ms_per_step": {k: v / K for k, v in run["phases"].items()}})
     line = {"metric": "particle-pushes/s", "value": value, "unit": "particle-pushes/s", "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": ms_max / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 weights, field solve and damage)",
             "data": "synthetic (seeded pre-load, Philox injection)",
-            "config": {"workload": args.workload, "grid_nodes": [sim.ny, sim.nx], "ions": n_p0, "electrons": n_e0,
-                       "parallelism": f"replicas x{world}", "l2": "particle state 8M x 25 B x 2 > L2 (126 MB)",
-                       "sort_every": 20, "picard": "5 solves every 2nd step, FP32 MG-PCG + FP64 refinement"},
-            "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": int(tm[8])}
-    if rank == 0 and world == 1 and stats_before is not None:
-        line["poisson"] = poisson_section(sim, stats_before, R, float(tm[2]), peak)
+            "config": {"workload": args.workload, "grid_nodes": [ny, nx], "ions": run["n_p0"],
+                       "electrons": run["n_e0"], "parallelism": f"replicas x{world}",
+                       "l2": "particle state > L2 (126 MB); no flush needed", "sort_every": 20,
+                       "picard": "5 solves every 2nd step, FP32 MG-PCG + FP64 refinement"},
+            "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": run["launches"]}
+    if rank == 0 and world == 1 and run["stats_before"] is not None:
+        line["poisson"] = poisson_section(sim, run["stats_before"], run["reports"], run["phases"]["field_solve"],
+                                          peak)
+    sim.close()
+    del sim
+    if rank == 0 and world == 1 and not args.no_second and args.workload != SECOND_WORKLOAD:
+        line["workloads"] = {SECOND_WORKLOAD: second_workload(args, local, peak, traffic)}
     if rank == 0 and world == 1 and not args.no_sweep:
-        sim.close()
-        line["sweep"] = sweep_section(local)
+        line["sweep"] = sweep_section(local, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_port(args.workload)
+        line["cpu_baseline"] = cpu_baseline_port(args.workload, args.warmup)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
-    sim.close()
     if rank == 0:
         print(json.dumps(line))
+
+
+def second_workload(args, device, peak, traffic):
+    sim, params = make_gpu_sim(SECOND_WORKLOAD, device, seed=1000)
+    for _ in range(args.warmup):
+        sim.step(params)
+    K = args.steps
+    run = timed_run(sim, params, K)
+    out = {"value": run["pushes"] / (run["ms"] * 1e-3), "unit": "particle-pushes/s", "ms_per_step": run["ms"] / K,
+           "grid_nodes": [sim.ny, sim.nx], "ions": run["n_p0"], "electrons": run["n_e0"],
+           "roofline": kernel_rooflines(run, K, peak, traffic),
+           "phase_ms_per_step": {k: v / K for k, v in run["phases"].items()}}
+    if run["stats_before"] is not None:
+        out["poisson"] = poisson_section(sim, run["stats_before"], run["reports"], run["phases"]["field_solve"], peak)
+    sim.close()
+    return out
 
 
 # ----------------------------------------------------------------------------- field solve
@@ -315,66 +413,53 @@ def poisson_section(sim, stats_before, reports, field_ms, peak):
 
 
 # ----------------------------------------------------------------------------- sweeps
-SWEEP_POINTS, SWEEP_WARMUP, SWEEP_STEPS, SWEEP_REF_STEPS = 16, 2, 40, 3000
-SERVE_REQUESTS, SERVE_RATE_HZ, SERVE_MAX_STEPS = 12, 20.0, 100
-# Served requests live for at most a few hundred steps, so their host set-up weighs more
-# than their stepping: a coarsest multigrid level of <= 256 nodes builds its dense inverse
-# in milliseconds instead of about 0.1-0.2 s (17 x 65 nodes), for one more level per V-cycle.
+SWEEP_WARMUP, SWEEP_STEPS, SWEEP_REF_STEPS = 3, 40, 3000
+SERVE_RATE_HZ, SERVE_WINDOW, SERVE_TOL, SERVE_CHUNK = 20.0, 500, 5e-3, 50
+# Served requests live for a few thousand steps at most, so their host set-up weighs on
+# the latency: a coarsest multigrid level of <= 256 nodes builds its dense inverse in
+# milliseconds instead of about 0.1-0.2 s (17 x 65 nodes), for one more level per V-cycle.
 SERVE_SOLVER = {"max_coarse": 256}
 
 
 def _run_plain(sim, params, K, pushes_out=None):
     """K steps of one simulator through pb_sim_run; returns the device time (ms) and, if
     ``pushes_out`` is a list, appends the particle-pushes of those steps."""
-    import ctypes as C
-    from thruster_cx_code_b200 import _lib
-    lib = _lib.load()
-    n_p0, n_e0 = sim.num_p, sim.num_e
-    it0 = sim.iteration
-    plist = []
-    for k in range(K):
-        sim.iteration = it0 + k
-        plist.append(sim.step_params(params))
-    sim.iteration = it0
-    P = (_lib.StepParams * K)(*plist)
-    R = (_lib.StepReport * K)()
-    _lib.check(lib.pb_sim_run(sim._h, P, K, R), "pb_sim_run")
-    tm = (C.c_double * 9)()
-    lib.pb_sim_timing(sim._h, tm)
-    sim.iteration = it0 + K
-    sim._invalidate()
-    for r in R:
-        sim._apply_report(r, params)
+    run = timed_run(sim, params, K, profile=False)
     if pushes_out is not None:
-        pushes_out.append(pushes_of(R, n_p0, n_e0))
-    return float(tm[0])
+        pushes_out.append(run["pushes"])
+    return run["ms"]
 
 
-def sweep_section(device):
-    """Sweep points per hour, plain (one instance at a time through pb_sim_run) against
-    batched (all points together through pb_batch_run), on two identical sets of 16
-    perveance-sweep points (C3 draws, 0.2M-1M macro-particles).  Rates use the device time
-    of 40 steps after 2 warm-up steps, scaled to 3000 steps per point; setup is not
-    included.  The same steps are also given as particle-pushes/s and as the fraction of
-    HBM peak their algorithmic bytes (41 B per push) would take.  Then a served run: 12 backstreaming-limit requests arriving as a Poisson
-    stream at 20 per second, admitted under a 150 GB budget, built on up to 8 setup threads
-    (with a coarsest multigrid level of <= 256 nodes, SERVE_SOLVER), stepped in chunks of 10
-    and retired when the saddle potential and current change less than 5% between the
-    halves of a 60-step window (or at 100 steps).  Its latencies include setup."""
+def _build_all(specs, device, solver=None, workers=8):
+    from concurrent.futures import ThreadPoolExecutor
+    from thruster_cx_code_b200 import workloads as W
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        return list(pool.map(lambda sp: W.make_sweep_sim(sp, device, solver=solver), specs))
+
+
+def sweep_section(device, args):
+    """Sweep points per hour, plain against batched, on one set of C3 perveance-sweep
+    points: screen 600-1800 V, accel -300..-100 V, plasma density log-uniform
+    3e16-3e17 m^-3, grids drawn from {64x256, 128x512, 256x1024} cells and 0.2M-4M
+    macro-particles log-uniform.  Plain: each point alone through pb_sim_run (3 warm-up
+    steps, then 40 timed).  Batched: all points together through pb_batch_run, from the
+    state the plain steps left (3 warm-up steps, then 40 timed).  Rates use device time,
+    scaled to 3000 steps per point; setup is excluded.  The particle-pushes of both halves
+    are reported, so their workloads can be compared.  Then the C4 served run."""
     from thruster_cx_code_b200 import serving as SV
     from thruster_cx_code_b200 import workloads as W
     rng = np.random.default_rng(7)
-    specs = [W.sweep_point(rng, i, n_range=(2e5, 1e6)) for i in range(SWEEP_POINTS)]
-    batch = SV.SweepBatch(device)
-    plain = [W.make_sweep_sim(sp, device) for sp in specs]
-    for s, p in plain:
+    npts = args.sweep_points
+    specs = [W.sweep_point(rng, i, n_range=(2e5, 4e6)) for i in range(npts)]
+    t_setup = time.perf_counter()
+    built = _build_all(specs, device)
+    t_setup = time.perf_counter() - t_setup
+    sims, prm = [s for s, _ in built], [p for _, p in built]
+    for s, p in built:
         _run_plain(s, p, SWEEP_WARMUP)
     plain_pushes = []
-    plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes) for s, p in plain)
-    for s, _ in plain:
-        s.close()
-    together = [W.make_sweep_sim(sp, device) for sp in specs]
-    sims, prm = [s for s, _ in together], [p for _, p in together]
+    plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes) for s, p in built)
+    batch = SV.SweepBatch(device)
     batch.run(sims, prm, SWEEP_WARMUP)
     n0 = [(s.num_p, s.num_e) for s in sims]
     res = batch.run(sims, prm, SWEEP_STEPS)
@@ -382,67 +467,93 @@ def sweep_section(device):
     batched_pushes = sum(SV.pushes_of([rep for _, rep in r], a, b) for r, (a, b) in zip(res, n0))
     for s in sims:
         s.close()
-    per_point_plain_s = plain_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / SWEEP_POINTS
-    per_point_batched_s = batched_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / SWEEP_POINTS
-    out = {"points": SWEEP_POINTS, "steps_timed": SWEEP_STEPS, "steps_per_point": SWEEP_REF_STEPS,
+    per_point_plain_s = plain_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts
+    per_point_batched_s = batched_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts
+    peak, _ = measured_peak_gbs()
+    out = {"points": npts, "steps_timed": SWEEP_STEPS, "steps_per_point": SWEEP_REF_STEPS,
            "grids": sorted({sp["grid"] for sp in specs}),
+           "particles": [int(min(sp["n_ions"] + sp["n_e"] for sp in specs)),
+                         int(max(sp["n_ions"] + sp["n_e"] for sp in specs))],
            "plain_points_per_hr": 3600.0 / per_point_plain_s,
            "batched_points_per_hr": 3600.0 / per_point_batched_s,
            "batched_over_plain": plain_ms / batched_ms,
-           "setup": "excluded (host geometry, multigrid build and pre-load)"}
-    # the same steps as particle-pushes/s, and their algorithmic bytes (41 B per push) against HBM
-    peak, _ = measured_peak_gbs()
-    for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms), ("batched", float(batched_pushes),
-                                                                             batched_ms)):
+           "setup": f"excluded ({t_setup:.1f} s of host geometry, multigrid build and pre-load on 8 threads)"}
+    for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms),
+                             ("batched", float(batched_pushes), batched_ms)):
         rate = pushes / (ms * 1e-3)
+        out[f"{name}_pushes"] = pushes
         out[f"{name}_pushes_per_s"] = rate
-        out[f"{name}_hbm_frac"] = rate * ALG_BYTES_PER_ION / 1e9 / peak if peak else None
-    # ---- served
-    rs = np.random.default_rng(11)
-    arrivals = []
-    t = 0.0
-    for i in range(SERVE_REQUESTS):
-        t += rs.exponential(1.0 / SERVE_RATE_HZ)
-        sp = W.sweep_point(rs, 100 + i, grids=("64x256", "128x512"), n_range=(2e5, 8e5))
-        sp["params"]["grids"][1]["V"] = float(rs.uniform(-300.0, -50.0))
-        sp["params"]["Te"] = 2.0
-        j = rs.uniform(0.1, 1.0)  # neutralizer electron current density, A/m^2
-        area = 0.5 * 0.95e-3 * 1e-3 + 0.3 * 3.75e-3 * 1e-3
-        sp["params"]["neut_rate"] = max(1, int(round(j * area * sp["dt"] / (1.602e-19 * 1e3))))
-        req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device, solver=SERVE_SOLVER)),
-                         W.sweep_point_bytes(sp), SERVE_MAX_STEPS,
-                         SV.Convergence(window=60, tol=0.05, keys=("current", "saddle")))
-        arrivals.append((t, req))
-    srv = SV.SweepServer(device, hbm_budget_bytes=150e9, max_active=64, chunk=10, batch=batch,
-                         setup_workers=max(2, min(8, (os.cpu_count() or 2) // 2)))
-    srv.serve(arrivals)
-    st = srv.stats()
-    st.update({"requests": SERVE_REQUESTS, "arrival_rate_hz": SERVE_RATE_HZ, "max_steps": SERVE_MAX_STEPS,
-               "particle_pushes": srv.pushes, "gpu_ms": srv.gpu_ms})
-    out["served"] = st
-    srv.close()
+        out[f"{name}_hbm_frac"] = rate * ALG_BYTES_PUSH / 1e9 / peak if peak else None
+    out["served"] = served_section(device, batch, args)
+    batch.close()
     return out
 
 
+def served_section(device, batch, args):
+    """C4 served backstreaming-limit sweep: requests arrive as a Poisson stream (20/s);
+    each draws accel voltage -300..-50 V, neutralizer electron injection 0.1-1 A/m^2 at
+    2 eV, a grid of 128x512 or 256x1024 cells and 1M-6M macro-particles.  Admission is
+    gated at 150 GB of device memory, set-up runs on host threads while the GPU steps the
+    admitted requests in chunks of 50, and a request retires once its centreline saddle
+    potential and beamlet current change by less than 0.5% between the two halves of its
+    last 500 steps (or at the step cap).  Latencies include set-up."""
+    from thruster_cx_code_b200 import serving as SV
+    from thruster_cx_code_b200 import workloads as W
+    rs = np.random.default_rng(11)
+    arrivals = []
+    t = 0.0
+    for i in range(args.serve_requests):
+        t += rs.exponential(1.0 / SERVE_RATE_HZ)
+        sp = W.served_point(rs, 100 + i)
+        req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device, solver=SERVE_SOLVER)),
+                         W.sweep_point_bytes(sp), args.serve_max_steps,
+                         SV.Convergence(window=SERVE_WINDOW, tol=SERVE_TOL, keys=("current", "saddle")))
+        arrivals.append((t, req))
+    srv = SV.SweepServer(device, hbm_budget_bytes=150e9, max_active=64, chunk=SERVE_CHUNK, batch=batch,
+                         setup_workers=max(2, min(8, (os.cpu_count() or 2) // 2)))
+    srv.serve(arrivals)
+    st = srv.stats()
+    st.update({"requests": args.serve_requests, "arrival_rate_hz": SERVE_RATE_HZ, "max_steps": args.serve_max_steps,
+               "retire_rule": f"saddle and current change < {SERVE_TOL:g} over {SERVE_WINDOW} steps",
+               "steps": [r.steps for r in srv.done], "particle_pushes": srv.pushes, "gpu_ms": srv.gpu_ms})
+    srv.active = []
+    return st
+
+
 # ----------------------------------------------------------------------------- CPU oracle
-def _oracle_sim(name, n_ions, n_e, seed):
+def _oracle_domain(name):
     from oracle.pic_oracle import OracleSimulator
     from thruster_cx_code_b200.domain import build_domain_geometry
     from thruster_cx_code_b200 import workloads as W
     o = OracleSimulator(build_domain_geometry)
     params = W.configure(o, name)
     o.build_domain(params)
+    return o, params
+
+
+def _oracle_load(o, params, name, n_ions, n_e, seed):
+    from thruster_cx_code_b200 import workloads as W
     v_b, v_ti, v_te = W.thermal_speeds(o, params)
     ions, eles = W.preload(o.isBound, o.dx, o.dy, o.Lx, o.Ly, n_ions, n_e, v_b, 4 * v_ti, v_te, seed=seed,
                            x_max_ions=W.plume_boundary(o, params))
     o._add_ions(*ions, np.zeros(n_ions, bool), o.new_ion_ids(n_ions))
     o._add_electrons(*eles, o.new_e_ids(n_e))
-    return o, params
 
 
 def _oracle_steps(o, params, k, seed):
+    """k oracle steps: (pushes, particle-phase seconds, field-solve seconds)."""
     from oracle.pic_oracle import PhiloxDraws
     draws = PhiloxDraws(seed)
+    solve = o.recalc_poisson
+    t_field = [0.0]
+
+    def timed_solve(*a, **kw):
+        t0 = time.perf_counter()
+        r = solve(*a, **kw)
+        t_field[0] += time.perf_counter() - t0
+        return r
+
+    o.recalc_poisson = timed_solve
     pushes = 0
     t0 = time.perf_counter()
     for _ in range(k):
@@ -450,59 +561,90 @@ def _oracle_steps(o, params, k, seed):
         o.step(params, draws)
         inj = o.injected_ions_step
         pushes += (n_p + inj) * o.n_sub_ion + (n_e + int(params.get("neut_rate", 30))) * o.n_sub_e
-    return pushes, time.perf_counter() - t0
+    total = time.perf_counter() - t0
+    o.recalc_poisson = solve
+    return pushes, total - t_field[0], t_field[0]
 
 
-def cpu_baseline_port(name, frac=1 / 16, steps=2):
+def _extrapolate(name, frac, pushes, t_part, t_field, k):
+    """Full-workload step of one instance from a sample of ``frac`` of its particles on
+    the full grid: particle work scales with the particle count, the field solve does not.
+    Returns (pushes per full step, seconds per full step)."""
+    return pushes / k / frac, t_part / k / frac + t_field / k
+
+
+def cpu_baseline_port(name, warmup, frac=1 / 1000, steps=4):
     from thruster_cx_code_b200 import workloads as W
     w = W.WORKLOADS[name]
-    ni, ne = int(w["n_ions"] * frac), int(w["n_e"] * frac)
-    o, params = _oracle_sim(name, ni, ne, seed=5)
-    pushes, dt = _oracle_steps(o, params, steps, seed=5)
-    return {"value": pushes / dt, "unit": "particle-pushes/s", "cores": 1, "kind": "port",
-            "sample": f"{name} grid, {ni} ions + {ne} electrons ({frac:.4g} of the workload), {steps} steps "
-                      f"(one with the 5-solve SuperLU Picard loop), NumPy/SciPy oracle of the reference step"}
+    ni, ne = max(1, int(w["n_ions"] * frac)), max(1, int(w["n_e"] * frac))
+    o, params = _oracle_domain(name)
+    _oracle_load(o, params, name, ni, ne, seed=5)
+    if warmup:
+        _oracle_steps(o, params, warmup, seed=5)
+    pushes, t_part, t_field = _oracle_steps(o, params, steps, seed=5)
+    ps, ts = _extrapolate(name, frac, pushes, t_part, t_field, steps)
+    return {"value": ps / ts, "unit": "particle-pushes/s", "cores": 1, "kind": "port",
+            "sample": f"{name}: {ni} ions + {ne} electrons ({frac:.4g} of the workload) on the full "
+                      f"{o.ny} x {o.nx} grid, {warmup} warm-up + {steps} timed steps of the NumPy/SciPy oracle of "
+                      f"the reference step; particle time x {1 / frac:.0f} plus the measured SuperLU Picard "
+                      f"time per step ({t_field / steps:.3f} s)",
+            "sample_pushes_per_s": pushes / (t_part + t_field)}
 
 
-def _worker(args):
-    name, ni, ne, seed, warm, k, q = args
-    os.environ["OMP_NUM_THREADS"] = "1"
-    o, params = _oracle_sim(name, ni, ne, seed)
+def _ref_worker(args):
+    name, ni, ne, seed, warm, k, frac = args
+    o, params = _REF_DOMAIN
+    _oracle_load(o, params, name, ni, ne, seed)
     if warm:
         _oracle_steps(o, params, warm, seed)
-    q.put(_oracle_steps(o, params, k, seed))
+    return _oracle_steps(o, params, k, seed)
+
+
+_REF_DOMAIN = None
 
 
 def reference_arm(args):
+    """The reference's CPU path (the oracle port: /root/reference is not on the bench
+    host) on all host cores.  One domain build, then one forked worker per core, each a
+    replica of the workload run on a particle sample; each replica's step time is its
+    particle time scaled to the workload's particle count plus its full-grid field-solve
+    time.  value = replicas x pushes per full step / the slowest replica's step time."""
+    global _REF_DOMAIN
     rank, _, world = dist_env()
     if rank != 0:
         return
+    os.environ["OMP_NUM_THREADS"] = "1"
     import multiprocessing as mp
     from thruster_cx_code_b200 import workloads as W
     w = W.WORKLOADS[args.workload]
-    P = max(1, min(os.cpu_count() or 1, 32))
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    ni, ne = w["n_ions"] // P, w["n_e"] // P
-    warm = min(args.warmup, 1)
-    procs = [ctx.Process(target=_worker, args=((args.workload, ni, ne, 11 + i, warm, args.steps, q),))
-             for i in range(P)]
-    for p in procs:
-        p.start()
-    res = [q.get() for _ in procs]
-    for p in procs:
-        p.join()
-    pushes = sum(r[0] for r in res)
-    wall = max(r[1] for r in res)
-    value = pushes / wall
+    P = max(1, min(os.cpu_count() or 1, 64))
+    frac = 1 / 1000 if w["n_ions"] + w["n_e"] > 20_000_000 else 1 / 200
+    ni, ne = max(1, int(w["n_ions"] * frac)), max(1, int(w["n_e"] * frac))
+    t0 = time.perf_counter()
+    _REF_DOMAIN = _oracle_domain(args.workload)
+    t_build = time.perf_counter() - t0
+    ctx = mp.get_context("fork")  # no GPU is touched in this process
+    with ctx.Pool(P) as pool:
+        res = pool.map(_ref_worker, [(args.workload, ni, ne, 11 + i, args.warmup, args.steps, frac)
+                                     for i in range(P)])
+    full = [_extrapolate(args.workload, frac, *r, args.steps) for r in res]
+    step_s = max(t for _, t in full)
+    pushes_step = sum(p for p, _ in full)
+    value = pushes_step / step_s
+    o = _REF_DOMAIN[0]
+    sample = (f"{P} forked processes, each a replica of {args.workload} ({o.ny} x {o.nx} grid) run on "
+              f"{ni} ions + {ne} electrons ({frac:.4g} of the workload's particles) for {args.warmup} warm-up + "
+              f"{args.steps} timed steps; each replica's particle time x {1 / frac:.0f} plus its full-grid "
+              f"SuperLU Picard time ({statistics.mean(r[2] for r in res) / args.steps:.3f} s per step) is its "
+              f"full-workload step; domain build {t_build:.1f} s, once, not timed")
     line = {"impl": "reference", "metric": "particle-pushes/s", "value": value, "unit": "particle-pushes/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (NumPy, f64 potential)",
             "data": "synthetic (seeded pre-load)",
-            "config": {"workload": args.workload, "processes": P},
+            "config": {"workload": args.workload, "grid_nodes": [o.ny, o.nx], "ions": w["n_ions"],
+                       "electrons": w["n_e"], "replicas": P},
             "cpu_baseline": {"value": value, "unit": "particle-pushes/s", "cores": P, "kind": "port",
-                             "sample": f"{P} processes, each the {args.workload} grid with {ni} ions + {ne} electrons "
-                                       f"(1/{P} of the workload), {args.steps} timed steps"},
+                             "sample": sample},
             "e2e": {"value": value, "unit": "particle-pushes/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 

@@ -135,6 +135,13 @@ typedef struct pb_step_params {
   /* saddle sample indices (flat), -1 unused */
   int32_t n_saddle;
   int32_t saddle_idx[8];
+  /* options without a reference counterpart (params 'neutral_profile', 'sputter_exponent'):
+   * neutral_uniform = 1 takes the CEX neutral density as n0_uniform everywhere instead of
+   * the point-source profile of physics_engine.py:1696-1706; sputter_exp != 1 uses the
+   * yield Y_coeff (E - E_th)^sputter_exp in float64 instead of the linear law of :1432 */
+  int32_t neutral_uniform;
+  double n0_uniform;
+  double sputter_exp;
 } pb_step_params;
 
 typedef struct pb_step_report {
@@ -235,6 +242,13 @@ void* pb_sim_stream(pb_sim* s);
  * step kernel, sputter break + electron step + SEE, thermal/diagnostics/sort), out[7] =
  * steps profiled, out[8] = kernels enqueued by that call. */
 int32_t pb_sim_timing(pb_sim* s, double* out_host9);
+/* The same profiled steps by kernel group (summed ms): out[0] injection + deposit,
+ * [1] field solve, [2] E corners + sub-step counts, [3] ion step kernel, [4] sputter
+ * break, [5] electron step kernel, [6] SEE spawn, [7] thermal + grid sums,
+ * [8] diagnostics + cell sort; out[9] = steps profiled.  No counterpart in the
+ * reference (its runner prints wall time per iteration,
+ * run_simulation_from_config.py:246-273). */
+int32_t pb_sim_phase_times(pb_sim* s, double* out_host10);
 int32_t pb_sim_set_profiling(pb_sim* s, int32_t on);
 /* Field-solve phase trace: returns the accumulated nanoseconds per phase (out32 may be
  * NULL: [l] down leg of level l, [7] coarse part, [8+l] up leg of level l, [15] Krylov

@@ -840,7 +840,14 @@ class OracleSimulator:
             E_eV = (0.5 * self.m_ion * (p_vx[hot] ** 2 + p_vy[hot] ** 2 + p_vz[hot] ** 2)) / self.q
             ok = E_eV > self.sputter_E_th
             if np.any(ok):
-                dmg = (self.sputter_Y_coeff * (E_eV[ok] - self.sputter_E_th)) * self.macro_weight
+                p_exp = float(params.get('sputter_exponent', 1.0))
+                if p_exp == 1.0:
+                    dmg = (self.sputter_Y_coeff * (E_eV[ok] - self.sputter_E_th)) * self.macro_weight
+                else:
+                    # option without a reference counterpart: Y = Y_coeff (E - E_th)^p,
+                    # evaluated in float64 from the float32 excess energy
+                    excess = (E_eV[ok] - self.sputter_E_th).astype(np.float64)
+                    dmg = (self.sputter_Y_coeff * excess ** p_exp) * self.macro_weight
                 np.add.at(self.damage_map, (impact_iy[hot][ok], impact_ix[hot][ok]), dmg)
             broken = (self.damage_map > params.get('Thresh', 1e5)) & self.isBound
             if np.any(broken):
@@ -976,8 +983,12 @@ class OracleSimulator:
                 a_corr = 1.0 / (1.0 - 1.0 / np.sqrt(2.0))
                 R_dist = np.sqrt(r_m ** 2 + (z_m + r_T) ** 2)
                 theta = np.arctan2(r_m, z_m + r_T)
-                n_local = params.get('n0', 1e20) * a_corr * (
-                    1.0 - 1.0 / np.sqrt(1.0 + (r_T / np.maximum(R_dist, 1e-12)) ** 2)) * np.cos(theta)
+                if params.get('neutral_profile', 'point_source') == 'uniform':
+                    # option without a reference counterpart: a uniform background n0
+                    n_local = np.full(px_m.shape, float(params.get('n0', 1e20)))
+                else:
+                    n_local = params.get('n0', 1e20) * a_corr * (
+                        1.0 - 1.0 / np.sqrt(1.0 + (r_T / np.maximum(R_dist, 1e-12)) ** 2)) * np.cos(theta)
                 n_local = np.maximum(n_local, 0.0)
                 v_mag = np.sqrt(p_vx[primary] ** 2 + p_vy[primary] ** 2 + p_vz[primary] ** 2)
                 g = np.maximum(v_mag, 1.0)

@@ -19,6 +19,11 @@ Fixture list
   segment.npz        _segment_hits_grid on a real electrode mask
   thermal.npz        one step with only the thermal block active (cooling + 10 sweeps)
   run_<case>.npz     short full-step runs with the reference's np.random stream recorded
+
+With the argument ``large`` it writes the fixtures of the benchmarked configurations
+instead (every 8th / 16th row of the potential, field and deposit, plus sums):
+  domain_large_aperture_3grid.npz, domain_long_erosion_3grid.npz
+  run_large_aperture_3grid.npz, run_large_aperture_3grid_fp64.npz
 """
 import json
 import os
@@ -28,6 +33,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from reference_loader import install_recorder, load_engine  # noqa: E402
 
 # ---------------------------------------------------------------------------
@@ -323,7 +329,85 @@ def make_runs(pe_factory, tag_suffix=""):
             outs=np.array(outs), log_names=log_names, v_bohm=v_b, fp64=(fp is np.float64), **log_vals, **flat)
 
 
+def _rows(a, step):
+    """Every ``step``-th row and the last one: the fixtures of the large grids keep these
+    (full potentials of 263k and 1.05M nodes would be megabytes each)."""
+    idx = np.unique(np.concatenate([np.arange(0, a.shape[0], step), [a.shape[0] - 1]]))
+    return idx, np.array(a[idx])
+
+
+def _large_sim(pe, case):
+    from tests.helpers import M_XE
+    sim = new_sim(pe, case["dx"], case["dy"], case["dt"])
+    sim.m_ion = M_XE
+    sim.m_e = M_XE / case["m_e_ratio"]
+    return sim
+
+
+def make_large(pe_factory):
+    """The benchmarked configurations: their domains and Picard potentials, and a short
+    run of the 257 x 1025 case in FP32 (snapshots after each step) and FP64 (the last)."""
+    from tests.helpers import CX_POWER_LAW, LARGE_CASES, large_case_particles
+    for name, case in LARGE_CASES.items():
+        pe = pe_factory(False)
+        sim = _large_sim(pe, case)
+        sim.build_domain(case["params"])
+        rows, V = _rows(sim.V, case["row_step"])
+        _, Ex = _rows(sim.Ex, case["row_step"])
+        _, Ey = _rows(sim.Ey, case["row_step"])
+        np.savez_compressed(
+            os.path.join(HERE, f"domain_{name}.npz"), params=json.dumps(case["params"]),
+            case=json.dumps({k: v for k, v in case.items() if k != "params"}), nx=sim.nx, ny=sim.ny, dx=sim.dx,
+            dy=sim.dy, Lx=sim.Lx, Ly=sim.Ly, macro_weight=sim.macro_weight, isBound_bits=np.packbits(sim.isBound),
+            V_fixed_sum=float(np.sum(sim.V_fixed)), rows=rows, V_rows=V, Ex_rows=Ex, Ey_rows=Ey,
+            V_sum=float(np.sum(sim.V)), V_absmax=float(np.abs(sim.V).max()))
+        if "steps" not in case:
+            continue
+        import contextlib, io
+        for fp64 in (False, True):
+            pe = pe_factory(fp64)
+            fp = pe._NP_FP
+            sim = _large_sim(pe, case)
+            sim.user_cs = cx_spline(CX_POWER_LAW)
+            params = case["params"]
+            sim.build_domain(params)
+            ions, cex, eles = large_case_particles(sim.isBound, sim.dx, sim.dy, sim.Lx, sim.Ly, case["n_ions"],
+                                                   case["n_e"], case["seed"])
+            sim._add_ions(*ions.astype(fp), cex)
+            sim._add_electrons(*eles.astype(fp))
+            rec = install_recorder(pe, 2000 + case["seed"])
+            out = {}
+            outs = []
+            for s in range(case["steps"]):
+                with contextlib.redirect_stdout(io.StringIO()):
+                    r = sim.step(params)
+                outs.append([float(r[0]), float(r[1]), float(r[2]), float(r[4])] + [float(t) for t in r[3]])
+                if fp64 and s < case["steps"] - 1:
+                    continue
+                n, ne = sim.num_p, sim.num_e
+                out[f"s{s}_p"] = np.array(np.stack([sim.p_x[:n], sim.p_y[:n], sim.p_vx[:n], sim.p_vy[:n],
+                                                    sim.p_vz[:n]]), dtype=fp)
+                out[f"s{s}_p_cex"] = np.array(sim.p_isCEX[:n])
+                out[f"s{s}_e"] = np.array(np.stack([sim.e_x[:ne], sim.e_y[:ne], sim.e_vx[:ne], sim.e_vy[:ne],
+                                                    sim.e_vz[:ne]]), dtype=fp)
+                for k, attr in (("V", "V"), ("rho", "rho"), ("damage", "damage_map")):
+                    a = np.asarray(getattr(sim, attr))
+                    out[f"s{s}_{k}_rows"] = _rows(a, case["row_step"])[1]
+                    out[f"s{s}_{k}_sum"] = float(np.sum(a.astype(np.float64)))
+                out[f"s{s}_isBound_bits"] = np.packbits(sim.isBound)
+            log_names = json.dumps([m for m, _ in rec.log])
+            log_vals = {f"draw_{i}": v for i, (_, v) in enumerate(rec.log)}
+            np.savez_compressed(
+                os.path.join(HERE, f"run_{name}{'_fp64' if fp64 else ''}.npz"),
+                case=json.dumps({k: v for k, v in case.items() if k != "params"}), params=json.dumps(params),
+                outs=np.array(outs), log_names=log_names, fp64=fp64, **log_vals, **out)
+
+
 def main():
+    if sys.argv[1:] == ["large"]:
+        make_large(lambda fp64: load_engine(fp64=fp64, name="_ref_large64" if fp64 else "_ref_large32"))
+        print("large fixtures written to", HERE)
+        return
     pe = load_engine()
     make_domains(pe)
     make_push(pe)

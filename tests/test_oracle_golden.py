@@ -159,3 +159,80 @@ def test_full_steps_replay_bit_exact(name, fp64):
             np.testing.assert_array_equal(np.asarray(getattr(sim, attr), f[f"s{s}_{k}"].dtype), f[f"s{s}_{k}"],
                                           err_msg=f"step {s} {k}")
     assert draws.pos == len(draws.log)
+
+
+# ---------------------------------------------------------------------------
+# the benchmarked configurations (make_golden.py "large"): rows of the fixtures
+# ---------------------------------------------------------------------------
+def _large_oracle(name, fp=np.float32, cx=True):
+    from tests.helpers import CX_POWER_LAW, LARGE_CASES, M_XE, cx_store
+    case = LARGE_CASES[name]
+    s = O.OracleSimulator(build_domain_geometry, fp=fp)
+    s.dx, s.dy, s.dt = case["dx"], case["dy"], case["dt"]
+    s.m_ion = M_XE
+    s.m_e = M_XE / case["m_e_ratio"]
+    if cx:
+        s.user_cs = cx_store(CX_POWER_LAW)
+    s.build_domain(case["params"])
+    return s, case
+
+
+def _unpack(bits, shape):
+    return np.unpackbits(bits)[: shape[0] * shape[1]].reshape(shape).astype(bool)
+
+
+@pytest.mark.parametrize("name", ["large_aperture_3grid", "long_erosion_3grid"])
+def test_large_domain_and_potential(name):
+    """The 257 x 1025 and 513 x 2049 domains: geometry and the 30-iteration SuperLU
+    Picard potential equal the reference's bit for bit (sampled rows and sums)."""
+    f = load(f"domain_{name}.npz")
+    s, case = _large_oracle(name, cx=False)
+    assert (s.nx, s.ny) == (int(f["nx"]), int(f["ny"]))
+    assert s.dx == float(f["dx"]) and s.Lx == float(f["Lx"]) and s.Ly == float(f["Ly"])
+    assert s.macro_weight == float(f["macro_weight"])
+    np.testing.assert_array_equal(s.isBound, _unpack(f["isBound_bits"], (s.ny, s.nx)))
+    assert float(np.sum(s.V_fixed)) == float(f["V_fixed_sum"])
+    rows = f["rows"]
+    np.testing.assert_array_equal(s.V[rows], f["V_rows"])
+    np.testing.assert_array_equal(s.Ex[rows], f["Ex_rows"])
+    np.testing.assert_array_equal(s.Ey[rows], f["Ey_rows"])
+    assert float(np.sum(s.V)) == float(f["V_sum"])
+
+
+@pytest.mark.parametrize("fp64", [False, True])
+def test_large_aperture_steps_replay_bit_exact(fp64):
+    """Two steps of the 257 x 1025 case (3 grids, the 7e-19 E^-0.1 CX table, m_e = M/400,
+    dt = 2.5e-11, sputtering with cells breaking) with the reference's draws replayed."""
+    from tests.helpers import large_case_particles
+    from oracle.pic_oracle import ReplayDraws
+    import json as _json
+    name = "large_aperture_3grid"
+    f = load(f"run_{name}{'_fp64' if fp64 else ''}.npz")
+    fp = np.float64 if fp64 else np.float32
+    s, case = _large_oracle(name, fp=fp)
+    ions, cex, eles = large_case_particles(s.isBound, s.dx, s.dy, s.Lx, s.Ly, case["n_ions"], case["n_e"],
+                                           case["seed"])
+    s._add_ions(*ions.astype(fp), cex, s.new_ion_ids(ions.shape[1]))
+    s._add_electrons(*eles.astype(fp), s.new_e_ids(eles.shape[1]))
+    names = _json.loads(str(f["log_names"]))
+    draws = ReplayDraws([(nm, f[f"draw_{i}"]) for i, nm in enumerate(names)])
+    params = case["params"]
+    rows = np.unique(np.concatenate([np.arange(0, s.ny, case["row_step"]), [s.ny - 1]]))
+    for k in range(case["steps"]):
+        r = s.step(params, draws)
+        got = [float(r[0]), float(r[1]), float(r[2]), float(r[4])] + [float(t) for t in r[3]]
+        np.testing.assert_array_equal(np.array(got), f["outs"][k], err_msg=f"step {k} outputs")
+        if f"s{k}_p" not in f.files:
+            continue
+        n, ne = s.num_p, s.num_e
+        p = np.stack([s.p_x[:n], s.p_y[:n], s.p_vx[:n], s.p_vy[:n], s.p_vz[:n]])
+        np.testing.assert_array_equal(p, f[f"s{k}_p"], err_msg=f"step {k} ions")
+        np.testing.assert_array_equal(s.p_isCEX[:n], f[f"s{k}_p_cex"])
+        e = np.stack([s.e_x[:ne], s.e_y[:ne], s.e_vx[:ne], s.e_vy[:ne], s.e_vz[:ne]])
+        np.testing.assert_array_equal(e, f[f"s{k}_e"], err_msg=f"step {k} electrons")
+        for key, attr in (("V", "V"), ("rho", "rho"), ("damage", "damage_map")):
+            a = np.asarray(getattr(s, attr))
+            np.testing.assert_array_equal(a[rows], f[f"s{k}_{key}_rows"], err_msg=f"step {k} {key}")
+            assert float(np.sum(a.astype(np.float64))) == float(f[f"s{k}_{key}_sum"]), (k, key)
+        np.testing.assert_array_equal(s.isBound, _unpack(f[f"s{k}_isBound_bits"], s.isBound.shape))
+    assert draws.pos == len(draws.log)

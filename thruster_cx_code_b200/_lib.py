@@ -41,6 +41,9 @@ class StepParams(C.Structure):
         ("v_rf", f64),
         ("n_saddle", i32),
         ("saddle_idx", i32 * 8),
+        ("neutral_uniform", i32),
+        ("n0_uniform", f64),
+        ("sputter_exp", f64),
     ]
 
 
@@ -93,6 +96,7 @@ PROTOTYPES = {
     "pb_sim_synchronize": (i32, [vp]),
     "pb_sim_stream": (vp, [vp]),
     "pb_sim_timing": (i32, [vp, P(f64)]),
+    "pb_sim_phase_times": (i32, [vp, P(f64)]),
     "pb_sim_set_profiling": (i32, [vp, i32]),
     "pb_sim_poisson_trace": (i32, [vp, i32, P(f64)]),
     "pb_sim_energy_sums": (i32, [vp, P(f64)]),

@@ -4,7 +4,9 @@
 and defaults as ``parse_config`` in Python/run_simulation_from_config.py:30-194:
 ``beam_species``, ``grid_material`` (preset or custom), ``advanced_settings``,
 ``cross_sections`` (log-log cubic splines of two-column tables), ``simulation``,
-``rf_co_extraction``, ``neutralizer``, ``grids`` and ``terminal_output``.  It returns
+``rf_co_extraction``, ``neutralizer``, ``grids`` and ``terminal_output``, plus a ``gpu``
+section the reference does not read (``neutral_profile``: ``point_source`` or ``uniform``;
+``sputter_exponent``: the power of the sputter yield, 1 for the reference's linear law).  It returns
 ``(params, output_selection)``.  ``apply_config`` then sets up a simulator the way the
 reference runner does before ``build_domain`` (:209-231): species mass and charge,
 electron mass ratio, material, cross-section store.  A config can also be given as a dict,
@@ -100,6 +102,12 @@ def parse_config(config):
                         'cham': g.get('cham', 0.0)} for g in cfg.get('grids', [])]
     if not params['grids']:
         raise ValueError("No grids found in config.json. Add at least one entry in the 'grids' list.")
+
+    # options of this implementation that the reference ignores (a section it never reads)
+    gpu = cfg.get('gpu', {})
+    for key in ('neutral_profile', 'sputter_exponent'):
+        if key in gpu:
+            params[key] = gpu[key]
 
     out = cfg.get('terminal_output', {})
     output_selection = {k: out.get(k, True) for k in ('grid_temperatures', 'beam_divergence',

@@ -52,6 +52,8 @@ struct IonStepArgs {
   float accel_f;    // f32(thermal_accel)
   float q_f;        // f32(q)
   float Y_f, Eth_f; // f32(Y_coeff), f32(E_th)
+  double Y_d, mw_d; // Y_coeff, macro_weight (float64 power-law yield)
+  double Y_exp;     // yield exponent: 1 = the reference's linear law in float32
   float dt_f;       // f32(dt) (SEE spawn offset)
   Spline see_spline;
   // SEE spawn records
@@ -68,6 +70,8 @@ struct IonStepArgs {
   // CEX
   float rT_f;          // f32(Ly*1e-3)
   double n0a;          // n0 * a_corr
+  int n_uniform;       // 1: uniform neutral density n0u (no point-source profile)
+  double n0u;
   double neut_vth;
   Spline cx_spline;
   double cex_bound;    // |n0a| * sigma_max * dt * (1 + 1e-5): P <= cex_bound * g

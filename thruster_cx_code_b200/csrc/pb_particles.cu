@@ -633,8 +633,13 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
             }
           }
           if (a.erosion_on && E_eV > a.Eth_f) {
-            float dmg = __fmul_rn(__fmul_rn(a.Y_f, __fsub_rn(E_eV, a.Eth_f)), a.mw_f);
-            atomicAdd(a.damage + cell, (double)dmg);
+            double dmg;
+            if (a.Y_exp == 1.0) {  // the reference's linear law, float32 (:1432-1433)
+              dmg = (double)__fmul_rn(__fmul_rn(a.Y_f, __fsub_rn(E_eV, a.Eth_f)), a.mw_f);
+            } else {               // Y_coeff (E - E_th)^p, float64 from the float32 excess
+              dmg = DMUL(DMUL(a.Y_d, pow((double)__fsub_rn(E_eV, a.Eth_f), a.Y_exp)), a.mw_d);
+            }
+            atomicAdd(a.damage + cell, dmg);
           }
         }
         // exit plane diagnostics (:1451-1494), pre-collision velocities and flag
@@ -664,16 +669,21 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
             float g = np_maxf(vm, 1.0f);
             double u = philox_uniform(a.seed, pid, SITE_CEX_U, a.step, 0);
             if (!(g <= a.cex_g_max && u >= DADD(DMUL(a.cex_bound, (double)g), 1e-15))) {
-              float z_m = __fmul_rn(__fsub_rn(x, 1.0f), 1e-3f);
-              z_m = z_m >= 0.0f ? z_m : 0.0f;
-              float r_m = __fmul_rn(y, 1e-3f);
-              float zr = __fadd_rn(z_m, a.rT_f);
-              float R = sqrtf(__fadd_rn(__fmul_rn(r_m, r_m), __fmul_rn(zr, zr)));
-              float th = atan2f(r_m, zr);
-              float Rm = np_maxf(R, 1e-12f);
-              float q1 = __fdiv_rn(a.rT_f, Rm);
-              float geo = __fsub_rn(1.0f, __fdiv_rn(1.0f, sqrtf(__fadd_rn(1.0f, __fmul_rn(q1, q1)))));
-              double nl = DMUL(DMUL(a.n0a, (double)geo), (double)cosf(th));
+              double nl;
+              if (a.n_uniform) {
+                nl = a.n0u;
+              } else {
+                float z_m = __fmul_rn(__fsub_rn(x, 1.0f), 1e-3f);
+                z_m = z_m >= 0.0f ? z_m : 0.0f;
+                float r_m = __fmul_rn(y, 1e-3f);
+                float zr = __fadd_rn(z_m, a.rT_f);
+                float R = sqrtf(__fadd_rn(__fmul_rn(r_m, r_m), __fmul_rn(zr, zr)));
+                float th = atan2f(r_m, zr);
+                float Rm = np_maxf(R, 1e-12f);
+                float q1 = __fdiv_rn(a.rT_f, Rm);
+                float geo = __fsub_rn(1.0f, __fdiv_rn(1.0f, sqrtf(__fadd_rn(1.0f, __fmul_rn(q1, q1)))));
+                nl = DMUL(DMUL(a.n0a, (double)geo), (double)cosf(th));
+              }
               nl = np_maxd(nl, 0.0);
               double sigma;
               if (a.cx_spline.enabled) {

@@ -537,7 +537,10 @@ static int32_t check_flags(Sim* s, uint32_t f) {
 }
 
 // one timestep, enqueued on the instance stream (physics_engine.py:969-1784)
-// record a phase mark (profiling only); marks k..k+6 of one step bracket its six phases
+// record a phase mark (profiling only); marks k..k+PB_MARKS-1 of one step bracket its
+// PB_MARKS - 1 phases: inject + deposit, field solve, E corners + sub-step counts, ion
+// step, sputter break, electron step, SEE spawn, thermal + grid sums, diagnostics + sort
+constexpr int PB_MARKS = 10;
 static void mark(Sim* s) {
   if (!s->profiling) return;
   if (s->mark_used >= s->marks.size()) {
@@ -691,17 +694,21 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   a.Tmap = s->Tmap; a.damage = s->damage;
   a.k_half_m = (float)p->half_m_ion; a.mw_f = (float)p->macro_w; a.ccell_f = (float)p->C_cell;
   a.accel_f = (float)p->thermal_accel; a.q_f = (float)p->q; a.Y_f = (float)p->Y_coeff; a.Eth_f = (float)p->E_th;
+  a.Y_d = p->Y_coeff; a.mw_d = p->macro_w; a.Y_exp = p->sputter_exp;
   a.dt_f = dtf;
   a.see_spline = spline_of(h->see);
   a.see_key = s->see_key; a.see_xy = s->see_xy; a.see_count = s->see_count; a.see_cap = s->see_cap;
   a.angles = s->angles; a.angle_count = s->angle_count; a.angle_cap = s->angle_cap;
   a.exit_sums = rep->exit_sums; a.counters = (unsigned long long*)&rep->entered;
   a.rT_f = (float)p->rT; a.n0a = p->n0a; a.neut_vth = p->neut_vth; a.cx_spline = spline_of(h->cx);
+  a.n_uniform = p->neutral_uniform ? 1 : 0; a.n0u = p->n0_uniform;
   {
     // collision-probability bound: sigma <= 10^cmax (spline), or <= 2.2881e-18 for the
-    // empirical law while 1 <= g <= 1e14 (|(-0.8821 ln g + 15.1262)| <= 15.1262)
+    // empirical law while 1 <= g <= 1e14 (|(-0.8821 ln g + 15.1262)| <= 15.1262); the
+    // point-source density never exceeds |n0 a_corr| (its geometric factor is below 1)
     double sig_max = h->cx.nt > 0 ? std::pow(10.0, h->cx.cmax) : 2.2881e-18;
-    a.cex_bound = std::fabs(p->n0a) * sig_max * p->dt * (1.0 + 1e-5);
+    const double n_max = a.n_uniform ? std::fabs(p->n0_uniform) : std::fabs(p->n0a);
+    a.cex_bound = n_max * sig_max * p->dt * (1.0 + 1e-5);
     a.cex_g_max = h->cx.nt > 0 ? INFINITY : 1e14f;
   }
   a.seed = s->seed; a.step = (uint32_t)p->iteration;
@@ -719,6 +726,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
                                                          &rep->broken));
     s->launches += 2;
   }
+  mark(s);
 
   // electrons: push and purge (:1248-1293, 1534-1561)
   EleStepArgs b{};
@@ -732,6 +740,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.errflags = ef;
   CK(launch_pdl(k_ele_step<false>, grid_for(s, E.cap, TILE, s->pbps), NT, 0, st, b));
   ++s->launches;
+  mark(s);
 
   // SEE electrons, appended after the surviving electrons (:1390-1417)
   SeeArgs sa{};
@@ -758,6 +767,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
                   rep->grid_sums));
     ++s->launches;
   }
+  mark(s);
 
   // exit divergence, saddle potential, PPC map (:1482-1488, 1655-1676, 1741-1767)
   CK(launch_pdl(k_theta95, 1, 1024, 0, st, s->angles, s->angle_count, s->angle_cap, s->angle_scratch, &rep->theta95));
@@ -1325,22 +1335,44 @@ int32_t pb_sim_energy_sums(pb_sim* h, double* out3) {
   return PB_OK;
 }
 
+// summed fine phase times of the profiled steps (PB_MARKS - 1 of them) and the step count
+static int32_t phase_sums(Sim* s, double* ph, double* steps_out) {
+  for (int k = 0; k < PB_MARKS - 1; ++k) ph[k] = 0.0;
+  *steps_out = 0.0;
+  if (!s->profiling || s->mark_used < (size_t)PB_MARKS) return PB_OK;
+  CK(cudaStreamSynchronize(s->stream));
+  size_t steps = s->mark_used / PB_MARKS;
+  for (size_t t = 0; t < steps; ++t)
+    for (int k = 0; k < PB_MARKS - 1; ++k) {
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, s->marks[t * PB_MARKS + k], s->marks[t * PB_MARKS + k + 1]));
+      ph[k] += ms;
+    }
+  *steps_out = (double)steps;
+  return PB_OK;
+}
+
 int32_t pb_sim_timing(pb_sim* h, double* out) {
   Sim* s = &h->s;
   for (int k = 0; k < 9; ++k) out[k] = 0.0;
   out[0] = s->last_ms;
   out[8] = (double)s->launches;
-  if (s->profiling && s->mark_used >= 7) {
-    CK(cudaStreamSynchronize(s->stream));
-    size_t steps = s->mark_used / 7;
-    for (size_t t = 0; t < steps; ++t)
-      for (int k = 0; k < 6; ++k) {
-        float ms = 0.0f;
-        CK(cudaEventElapsedTime(&ms, s->marks[t * 7 + k], s->marks[t * 7 + k + 1]));
-        out[1 + k] += ms;
-      }
-    out[7] = (double)steps;
+  double ph[PB_MARKS - 1], steps = 0.0;
+  if (int32_t rc = phase_sums(s, ph, &steps)) return rc;
+  if (steps > 0.0) {
+    out[1] = ph[0]; out[2] = ph[1]; out[3] = ph[2]; out[4] = ph[3];
+    out[5] = ph[4] + ph[5] + ph[6];
+    out[6] = ph[7] + ph[8];
+    out[7] = steps;
   }
+  return PB_OK;
+}
+
+int32_t pb_sim_phase_times(pb_sim* h, double* out10) {
+  Sim* s = &h->s;
+  double steps = 0.0;
+  if (int32_t rc = phase_sums(s, out10, &steps)) return rc;
+  out10[PB_MARKS - 1] = steps;
   return PB_OK;
 }
 

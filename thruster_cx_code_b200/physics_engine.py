@@ -672,6 +672,14 @@ class DigitalTwinSimulator:
         P.rT = self.Ly * 1e-3
         a_corr = 1.0 / (1.0 - 1.0 / _sqrt(2.0))
         P.n0a = params.get('n0', 1e20) * a_corr
+        # options of the benchmarked configurations, ignored by the reference: a uniform
+        # neutral background instead of the point-source profile, and a power-law yield
+        profile = params.get('neutral_profile', 'point_source')
+        if profile not in ('point_source', 'uniform'):
+            raise ValueError(f"neutral_profile must be 'point_source' or 'uniform' (got {profile!r})")
+        P.neutral_uniform = int(profile == 'uniform')
+        P.n0_uniform = float(params.get('n0', 1e20))
+        P.sputter_exp = float(params.get('sputter_exponent', 1.0))
         P.neut_vth = _sqrt(2.0 * self.kB * params.get('Tn', 300.0) / self.m_ion)
         P.v_see_th = _sqrt(2.0 * self.q * 2.0 / self.m_e)
         P.cooling_factor = (self.emissivity * self.sb_sigma * self.A_cell * self.dt * self.thermal_accel) / self.C_cell

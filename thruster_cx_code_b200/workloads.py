@@ -1,16 +1,20 @@
 """Named aperture workloads (params dicts in the reference's config.json vocabulary).
 
 ``single_aperture_2grid``: 2-grid screen/accel optics at 25 um spacing (65 x 284 nodes,
-the geometry of the reference's own CPU-runnable case), 100k macro-particles.
+the geometry of the reference's own CPU-runnable case), 100k macro-particles, a uniform
+neutral background of 1e18 m^-3 and a constant CEX cross-section of 5e-19 m^2 (a flat
+log-log table, evaluated by the reference's own spline path).
 
 ``large_aperture_3grid``: 3-grid screen +1000 V / accel -250 V / decel 0 V, each 0.5 mm
 thick, 6.25 um spacing chosen so the derived domain is exactly 257 x 1025 nodes
 (256 x 1024 cells), 8M FP32 macro-particles (6M Xe+ and 2M electrons at mass ratio
-1/400), CEX cross-section 7e-19 E^-0.1 m^2 as a log-log table over 1-1000 eV, sputtering on.
+1/400), CEX cross-section 7e-19 E^-0.1 m^2 as a log-log table over 1-1000 eV, sputtering
+on with the Mo yield 1e-3 (E - 30)^1.2.
 
 ``long_erosion_3grid``: the same 3-grid stack at 3.125 um spacing (513 x 2049 nodes,
-512 x 2048 cells), 64M FP32 macro-particles (48M Xe+ and 16M electrons), CEX neutral
-density 5e18 m^-3, sputtering and grid heating with conduction on ("Both").
+512 x 2048 cells), 64M FP32 macro-particles (48M Xe+ and 16M electrons), a uniform CEX
+neutral density of 5e18 m^-3, sputtering with the power-law yield and grid heating with
+conduction on ("Both").
 
 Particles are pre-loaded from a seeded NumPy generator: positions uniform over the
 non-electrode cells, ion velocities N(v_Bohm, v_th), electron velocities thermal.
@@ -38,39 +42,50 @@ def cx_store(table):
                    "spline": UnivariateSpline(np.log10(t[:, 0]), np.log10(t[:, 1]), s=0.0, k=3)}}
 
 
+# a constant cross-section as a table for the reference's log-log cubic spline (at least
+# four points for k = 3; a flat table makes the spline constant)
+CX_CONSTANT_5E19 = np.array([[1.0, 5e-19], [10.0, 5e-19], [100.0, 5e-19], [1000.0, 5e-19]])
+# the molybdenum preset with the yield coefficient of the power law 1e-3 (E - 30)^1.2
+MO_POWER_LAW = {'k': 138.0, 'rho': 10280.0, 'cp': 250.0, 'emissivity': 0.80, 'alpha': 4.8e-6,
+                'E_mod': 329e9, 'Y_coeff': 1e-3, 'E_th': 30.0}
+
 WORKLOADS = {
     "single_aperture_2grid": dict(
-        dx=0.025, dy=0.025, dt=1e-10, m_e_ratio=100.0, n_ions=80000, n_e=20000, cx=None,
+        dx=0.025, dy=0.025, dt=1e-10, m_e_ratio=100.0, n_ions=80000, n_e=20000, cx=CX_CONSTANT_5E19,
+        material=None,
         params=dict(grids=[dict(V=1000.0, t=0.38, gap=1.0, r=0.95, cham=0.0),
                            dict(V=-200.0, t=1.0, gap=1.0, r=0.55, cham=0.0)],
                     pitch_mm=3.75, Te_up=5.0, n0_plasma=1e17, Ti=0.1, Tn=300.0, n0=1e18,
-                    sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9)),
+                    neutral_profile="uniform", sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9)),
     "large_aperture_3grid": dict(
         dx=0.00625, dy=0.00625, dt=2.5e-11, m_e_ratio=400.0, n_ions=6_000_000, n_e=2_000_000,
-        cx=cx_table_power_law(),
+        cx=cx_table_power_law(), material=MO_POWER_LAW,
         params=dict(grids=[dict(V=1000.0, t=0.5, gap=0.5, r=0.8, cham=0.0),
                            dict(V=-250.0, t=0.5, gap=0.5, r=0.5, cham=0.0),
                            dict(V=0.0, t=0.5, gap=0.5, r=0.7, cham=0.0)],
                     pitch_mm=4.0, upstream_gap_mm=0.4, Te_up=5.0, n0_plasma=1e17, Ti=0.1, Tn=300.0,
-                    n0=1e18, sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9)),
+                    n0=1e18, sim_mode="Erosion", sputter_exponent=1.2, neut_rate=30, Te=5.0, Thresh=1e9)),
     "long_erosion_3grid": dict(
         dx=0.003125, dy=0.003125, dt=1.25e-11, m_e_ratio=400.0, n_ions=48_000_000, n_e=16_000_000,
-        cx=cx_table_power_law(),
+        cx=cx_table_power_law(), material=MO_POWER_LAW,
         params=dict(grids=[dict(V=1000.0, t=0.5, gap=0.5, r=0.8, cham=0.0),
                            dict(V=-250.0, t=0.5, gap=0.5, r=0.5, cham=0.0),
                            dict(V=0.0, t=0.5, gap=0.5, r=0.7, cham=0.0)],
                     pitch_mm=4.0, upstream_gap_mm=0.4, Te_up=5.0, n0_plasma=1e17, Ti=0.1, Tn=300.0,
-                    n0=5e18, sim_mode="Both", neut_rate=30, Te=5.0, Thresh=1e9)),
+                    n0=5e18, neutral_profile="uniform", sim_mode="Both", sputter_exponent=1.2, neut_rate=30,
+                    Te=5.0, Thresh=1e9)),
 }
 
 
 def configure(sim, name, n_scale=1.0):
-    """Apply a workload's spacing, species and cross-section to a simulator (either the
-    GPU one or the oracle) before build_domain; returns the params dict."""
+    """Apply a workload's spacing, species, material and cross-section to a simulator
+    (either the GPU one or the oracle) before build_domain; returns the params dict."""
     w = WORKLOADS[name]
     sim.dx, sim.dy, sim.dt = w["dx"], w["dy"], w["dt"]
     sim.m_ion = M_XE
     sim.m_e = M_XE / w["m_e_ratio"]
+    if w.get("material") is not None:
+        sim.set_material(props=dict(w["material"]))
     if w["cx"] is not None:
         sim.user_cs = cx_store(w["cx"])
     return dict(w["params"])
@@ -132,6 +147,27 @@ def sweep_point(rng, index, grids=("64x256", "128x512", "256x1024"), n_range=(2e
                                    dict(V=float(rng.uniform(-300.0, -100.0)), t=1.0, gap=1.0, r=0.55, cham=0.0)],
                             pitch_mm=3.75, Te_up=5.0, n0_plasma=float(np.exp(rng.uniform(np.log(3e16), np.log(3e17)))),
                             Ti=0.1, Tn=300.0, n0=1e18, sim_mode="Erosion", neut_rate=30, Te=5.0, Thresh=1e9))
+
+
+def served_point(rng, index, grids=("128x512", "256x1024"), n_range=(1e6, 6e6)):
+    """One request of the served backstreaming-limit sweep: the 2-grid stack with accel
+    voltage uniform in -300..-50 V, neutralizer electrons injected at 2 eV with a current
+    density uniform in 0.1-1 A/m^2 (macro-electrons per step from the density, the
+    neutralizer band Ly x 1 mm, dt and the macro-particle weight), a grid drawn from
+    ``grids`` and a macro-particle count uniform in ``n_range``."""
+    sp = sweep_point(rng, index, grids=grids, n_range=(1.0, 1.0))
+    n = int(rng.uniform(n_range[0], n_range[1]))
+    sp["n_ions"], sp["n_e"] = int(0.75 * n), n - int(0.75 * n)
+    prm = sp["params"]
+    prm["grids"][1]["V"] = float(rng.uniform(-300.0, -50.0))
+    prm["Te"] = 2.0
+    j = float(rng.uniform(0.1, 1.0))
+    Ly_mm = 0.5 * prm["grids"][0]["r"] + 0.3 * prm["pitch_mm"]
+    cell_vol = (sp["dx"] * 1e-3) ** 2 * 1e-3
+    w = max(prm["n0_plasma"] * cell_vol / 80.0, 1e3)
+    prm["neut_rate"] = max(1, int(round(j * (Ly_mm * 1e-3 * 1e-3) * sp["dt"] / (Q * w))))
+    sp["neut_j"] = j
+    return sp
 
 
 def sweep_point_bytes(spec):
