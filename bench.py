@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--sweep-points", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-max-steps", type=int, default=4000)
+    ap.add_argument("--kernel-options", type=int, default=None,
+                    help="PB_OPT_* bits for the step kernels (default: the library's)")
     return ap.parse_args()
 
 
@@ -181,10 +183,16 @@ def traffic_table():
 
 
 # ----------------------------------------------------------------------------- GPU arm
+KERNEL_OPTIONS = None
+
+
 def make_gpu_sim(name, device, seed):
     from thruster_cx_code_b200 import physics_engine as PE
     from thruster_cx_code_b200 import workloads as W
+    from thruster_cx_code_b200 import _lib
     sim = PE.DigitalTwinSimulator(device=device, seed=seed, sort_every=20)
+    if KERNEL_OPTIONS is not None:
+        _lib.check(sim._libh.pb_sim_set_kernel_options(sim._h, KERNEL_OPTIONS), "set_kernel_options")
     params = W.configure(sim, name)
     sim.build_domain(params)
     w = W.WORKLOADS[name]
@@ -336,7 +344,8 @@ def gpu_arm(args):
                        "electrons": run["n_e0"], "parallelism": f"replicas x{world}",
                        "l2": "particle state > L2 (126 MB); no flush needed", "sort_every": 20,
                        "picard": "5 solves every 2nd step, FP32 MG-PCG + FP64 refinement"},
-            "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": run["launches"]}
+            "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": run["launches"],
+            "kernel_options": kernel_options_of(local)}
     if rank == 0 and world == 1 and run["stats_before"] is not None:
         line["poisson"] = poisson_section(sim, run["stats_before"], run["reports"], run["phases"]["field_solve"],
                                           peak)
@@ -354,6 +363,19 @@ def gpu_arm(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def kernel_options_of(device):
+    """The PB_OPT_* bits the step kernels ran with (a fresh simulator's, or the override)."""
+    import ctypes as C
+    from thruster_cx_code_b200 import physics_engine as PE
+    if KERNEL_OPTIONS is not None:
+        return KERNEL_OPTIONS
+    s = PE.DigitalTwinSimulator(device=device)
+    v = C.c_uint32()
+    s._libh.pb_sim_get_kernel_options(s._h, C.byref(v))
+    s.close()
+    return int(v.value)
 
 
 def second_workload(args, device, peak, traffic):
@@ -651,6 +673,7 @@ def reference_arm(args):
 
 if __name__ == "__main__":
     a = parse()
+    KERNEL_OPTIONS = a.kernel_options
     if a.impl == "reference":
         reference_arm(a)
     else:

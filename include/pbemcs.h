@@ -180,6 +180,15 @@ int32_t pb_sim_set_solver(pb_sim* s, double tol, double tol_inner, int32_t max_o
  * of SMs, default all). Results do not depend on either, except the field solve's
  * block-order sums, whose rounding follows the block count. */
 int32_t pb_sim_set_launch(pb_sim* s, int32_t particle_blocks_per_sm, int32_t solve_blocks);
+/* Kernel variants of the step (the autotuner's knobs; no counterpart in the reference).
+ * Every combination gives bit-identical results; they differ in speed only.
+ *   PB_OPT_SMEM_HIST  deposit and PPC counts go through shared-memory cell histograms per
+ *                     tile of cell-sorted particles, flushed to HBM once per tile
+ *   PB_OPT_TMA_TILE   the ion step stages each tile's window of the E-corner array in
+ *                     shared memory with a TMA tensor copy before pushing */
+enum { PB_OPT_SMEM_HIST = 1 << 0, PB_OPT_TMA_TILE = 1 << 1 };
+int32_t pb_sim_set_kernel_options(pb_sim* s, uint32_t flags);
+int32_t pb_sim_get_kernel_options(pb_sim* s, uint32_t* flags);
 
 /* Upload the domain of build_domain (physics_engine.py:629-847): node masks, Dirichlet
  * values, electrode masks (bit g of gridmask = grid g), plus the state arrays to keep.

@@ -2,9 +2,12 @@
 
     python -m thruster_cx_code_b200._build
 
-Compiles csrc/pb_runtime.cu (a unity build that includes the kernel sources) with nvcc
-for sm_100a.  Fused multiply-add contraction is disabled for the whole library: the
-particle arithmetic reproduces NumPy's separately rounded operations.
+Compiles two translation units with nvcc for sm_100a and links them:
+  csrc/pb_runtime.cu  the runtime, the C-ABI and (included) the particle and diagnostic
+                      kernels, with fused multiply-add contraction disabled: the particle
+                      arithmetic reproduces NumPy's separately rounded operations;
+  csrc/pb_poisson.cu  the FP32 MG-PCG field solve, with contraction allowed (its result is
+                      compared with SuperLU to a tolerance, not bit for bit).
 """
 import os
 import subprocess
@@ -32,13 +35,10 @@ def needs_build():
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force=False, verbose=False):
-    if not force and not needs_build():
-        return LIB
-    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-           "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-I", os.path.join(HERE, "csrc"),
-           os.path.join(HERE, "csrc", "pb_runtime.cu"), "-o", LIB + ".tmp"]
+UNITS = (("pb_runtime.cu", "false"), ("pb_poisson.cu", "true"))
+
+
+def _run(cmd, verbose):
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -47,6 +47,30 @@ def build(force=False, verbose=False):
         raise RuntimeError("nvcc failed building libpbemcs.so")
     if verbose:
         sys.stderr.write(r.stderr)
+
+
+def build(force=False, verbose=False):
+    if not force and not needs_build():
+        return LIB
+    common = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+              "-I", os.path.join(ROOT, "include"), "-I", os.path.join(HERE, "csrc")]
+    objs = []
+    tmp = LIB + ".objs"
+    os.makedirs(tmp, exist_ok=True)
+    try:
+        for src, fmad in UNITS:
+            obj = os.path.join(tmp, src.replace(".cu", ".o"))
+            contract = "fast" if fmad == "true" else "off"
+            _run([nvcc()] + common + [f"-fmad={fmad}", "-Xcompiler", f"-fPIC,-ffp-contract={contract}", "-c",
+                                      os.path.join(HERE, "csrc", src), "-o", obj], verbose)
+            objs.append(obj)
+        _run([nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a"] + objs + ["-o", LIB + ".tmp"], False)
+    finally:
+        for o in objs:
+            if os.path.exists(o):
+                os.remove(o)
+        if os.path.isdir(tmp):
+            os.rmdir(tmp)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

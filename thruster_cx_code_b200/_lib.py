@@ -97,6 +97,8 @@ PROTOTYPES = {
     "pb_sim_stream": (vp, [vp]),
     "pb_sim_timing": (i32, [vp, P(f64)]),
     "pb_sim_phase_times": (i32, [vp, P(f64)]),
+    "pb_sim_set_kernel_options": (i32, [vp, u32]),
+    "pb_sim_get_kernel_options": (i32, [vp, P(u32)]),
     "pb_sim_set_profiling": (i32, [vp, i32]),
     "pb_sim_poisson_trace": (i32, [vp, i32, P(f64)]),
     "pb_sim_energy_sums": (i32, [vp, P(f64)]),
@@ -132,6 +134,10 @@ def load():
     _lib = lib
     return lib
 
+
+# kernel variants of the step (pb_sim_set_kernel_options)
+PB_OPT_SMEM_HIST = 1 << 0
+PB_OPT_TMA_TILE = 1 << 1
 
 ERRORS = {1: "CUDA error", 2: "invalid argument", 3: "capacity", 4: "device wait timed out",
           5: "field solve did not converge", 6: "call out of order"}

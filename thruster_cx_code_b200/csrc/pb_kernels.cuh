@@ -21,7 +21,15 @@ struct Spline {
 };
 
 // Everything the ion step kernel reads besides the particles.
+// E-corner window that the ion step stages per tile with a TMA copy (PB_OPT_TMA_TILE):
+// TB_W x TB_H cells of 8 floats (8 KB)
+constexpr int TB_W = 64, TB_H = 4;
+constexpr unsigned TB_BYTES = TB_W * TB_H * 32u;
+
 struct IonStepArgs {
+  // tensor map of the corner array viewed as float [ny][nx][8], box 8 x TB_W x TB_H
+  // (read by the TMA unit from the kernel's parameter space)
+  CUtensorMap ec_map;
   Soa src, dst;
   const int *num_src;
   int *num_dst;

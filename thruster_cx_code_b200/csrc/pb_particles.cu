@@ -37,14 +37,24 @@ __device__ __forceinline__ double gather4(const float* __restrict__ F, size_t r0
 // The same from the per-cell corner array: Ec[2c] holds Ex at (iy0, ix0), (iy0, ix0 + 1),
 // (iy0 + 1, ix0), (iy0 + 1, ix0 + 1) of cell c = iy0 * nx + ix0, Ec[2c + 1] the same of
 // Ey: one 16-byte load per component instead of four scalar loads, same arithmetic.
-__device__ __forceinline__ void gather4c(const float4* __restrict__ Ec, size_t c, double w00, double w10,
-                                         double w01, double w11, double& ex, double& ey) {
-  const float4 a = __ldg(Ec + 2 * c), b = __ldg(Ec + 2 * c + 1);
+__device__ __forceinline__ void gather4v(const float4 a, const float4 b, double w00, double w10, double w01,
+                                         double w11, double& ex, double& ey) {
   ex = DADD(DADD(DADD(DMUL((double)a.x, w00), DMUL((double)a.y, w10)), DMUL((double)a.z, w01)),
             DMUL((double)a.w, w11));
   ey = DADD(DADD(DADD(DMUL((double)b.x, w00), DMUL((double)b.y, w10)), DMUL((double)b.z, w01)),
             DMUL((double)b.w, w11));
 }
+__device__ __forceinline__ void gather4c(const float4* __restrict__ Ec, size_t c, double w00, double w10,
+                                         double w01, double w11, double& ex, double& ey) {
+  gather4v(__ldg(Ec + 2 * c), __ldg(Ec + 2 * c + 1), w00, w10, w01, w11, ex, ey);
+}
+
+// The window of the corner array staged in shared memory for a tile (PB_OPT_TMA_TILE):
+// cells [bx, bx + TB_W) x [by, by + TB_H); cells outside it are read from global memory.
+struct EBox {
+  const float4* box;  // nullptr: no window staged
+  int bx, by;
+};
 
 // Builds the corner array from Ex and Ey (cells of the last row and column are not used:
 // the gather clamps the lower corner to ny - 2, nx - 2).
@@ -108,7 +118,8 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
                                                const float* __restrict__ Bz, int nx, int ny,
                                                float dxf, float dyf, double h, float dtf,
                                                const float4* __restrict__ Ec = nullptr, float inv_dx = 0.0f,
-                                               float inv_dy = 0.0f, float* q_start = nullptr) {
+                                               float inv_dy = 0.0f, float* q_start = nullptr,
+                                               EBox eb = EBox{nullptr, 0, 0}) {
   static_assert(!(HAS_B && CORN), "the corner gather has no B field");
   const float ixf = LIGHT ? div_rn_checked(x, dxf, inv_dx) : __fdiv_rn(x, dxf);
   const float iyf = LIGHT ? div_rn_checked(y, dyf, inv_dy) : __fdiv_rn(y, dyf);
@@ -138,7 +149,13 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
   size_t r0 = (size_t)iy0 * nx, r1 = (size_t)iy1 * nx;
   double ex, ey;
   if (CORN) {
-    gather4c(Ec, r0 + ix0, w00, w10, w01, w11, ex, ey);
+    const unsigned ox = (unsigned)(ix0 - eb.bx), oy = (unsigned)(iy0 - eb.by);
+    if (eb.box && ox < (unsigned)TB_W && oy < (unsigned)TB_H) {
+      const float4* q = eb.box + 2 * (oy * TB_W + ox);
+      gather4v(q[0], q[1], w00, w10, w01, w11, ex, ey);
+    } else {
+      gather4c(Ec, r0 + ix0, w00, w10, w01, w11, ex, ey);
+    }
   } else {
     ex = gather4(Ex, r0, r1, ix0, ix1, w00, w10, w01, w11);
     ey = gather4(Ey, r0, r1, ix0, ix1, w00, w10, w01, w11);
@@ -212,6 +229,60 @@ __device__ __forceinline__ void warp_count_add(int* cnt, int cell, bool valid) {
   unsigned peers = __match_any_sync(act, key);
   int leader = __ffs(peers) - 1;
   if (valid && (int)(threadIdx.x & 31) == leader) atomicAdd(cnt + cell, __popc(peers));
+}
+
+// Shared-memory cell histograms of one tile (kernel option PB_OPT_SMEM_HIST).  The cells of
+// the tile's kept particles are staged in shared memory; when they span fewer than HBINS
+// consecutive cell keys (the usual case for particles re-sorted by cell), each warp adds
+// its runs of equal cells to shared bins (one atomic per run: consecutive lanes of sorted
+// particles share cells) and the block then adds every nonzero bin to the global counts
+// once.  Wider tiles (particles that moved far since the last sort) count with warp-
+// aggregated global atomics as before.  Counts are integers, so the result does not depend
+// on the order of the additions.
+constexpr int HBINS = 1024;
+
+// bins[c] += length of the run of equal valid c that starts at this lane (run heads only)
+__device__ __forceinline__ void warp_run_add(int* bins, int c, bool valid) {
+  const int lane = threadIdx.x & 31;
+  const int v = valid ? c : -1;
+  const int prev = __shfl_up_sync(0xFFFFFFFFu, v, 1);
+  const bool head = lane == 0 || v != prev;
+  const unsigned heads = __ballot_sync(0xFFFFFFFFu, head);
+  const unsigned later = lane == 31 ? 0u : heads & (0xFFFFFFFFu << (lane + 1));
+  const int next = later ? __ffs(later) - 1 : 32;
+  if (head && valid) atomicAdd(bins + c, next - lane);
+}
+
+template <int NTHR, int TILE_SZ>
+__device__ __forceinline__ void tile_hist(const int* cell, const uint8_t* keep, int* gcnt, int* bins) {
+  __shared__ int red[2 * (NTHR / 32)];
+  int lo = INT_MAX, hi = INT_MIN;
+  for (int k = threadIdx.x; k < TILE_SZ; k += NTHR)
+    if (keep[k]) { lo = min(lo, cell[k]); hi = max(hi, cell[k]); }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = lo; red[NTHR / 32 + (threadIdx.x >> 5)] = hi; }
+  __syncthreads();
+  lo = INT_MAX; hi = INT_MIN;
+#pragma unroll
+  for (int j = 0; j < NTHR / 32; ++j) { lo = min(lo, red[j]); hi = max(hi, red[NTHR / 32 + j]); }
+  if (hi >= lo && hi - lo < HBINS) {
+    for (int k = threadIdx.x; k < TILE_SZ; k += NTHR) {
+      const bool v = keep[k] != 0;
+      warp_run_add(bins, v ? cell[k] - lo : 0, v);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b <= hi - lo; b += NTHR) {
+      const int v = bins[b];
+      if (v) { atomicAdd(gcnt + lo + b, v); bins[b] = 0; }
+    }
+  } else if (hi >= lo) {
+    for (int k = threadIdx.x; k < TILE_SZ; k += NTHR) warp_count_add(gcnt, cell[k], keep[k] != 0);
+  }
+  __syncthreads();
 }
 
 __device__ __forceinline__ int deposit_cell(float x, float y, float dxf, float dyf, int nx, int ny) {
@@ -527,17 +598,57 @@ __device__ __forceinline__ int tile_compact_ranks(const uint8_t* keep, int* rank
 struct IonStage {
   float x[TILE], y[TILE], vx[TILE], vy[TILE], vz[TILE];
   uint32_t id[TILE];
-  int rank[TILE];
+  int rank[TILE];          // deposit cells (PB_OPT_SMEM_HIST) until the compaction ranks them
   uint8_t cex[TILE], keep[TILE];
 };
 
 // Four resident blocks of 256 per SM (64 registers, some spilled): latency hiding gains
 // more than the spills cost (12% faster than three blocks at 80 registers).
-template <bool HAS_B>
-__global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
+// Lower-left start cell of a tile's particles (a rough floor of x / dx and y / dy, which
+// only places the staged window; every gather checks membership exactly), block-wide.
+__device__ __forceinline__ void tile_low_cell(const IonStepArgs& a, int t0, int n, int& xlo, int& ylo) {
+  __shared__ int red[2 * (NT / 32)];
+  int lx = INT_MAX, ly = INT_MAX;
+  for (int k = threadIdx.x; k < TILE; k += NT) {
+    const int i = t0 + k;
+    if (i >= n) break;
+    const float qx = __fmul_rn(a.src.x[i], a.inv_dx), qy = __fmul_rn(a.src.y[i], a.inv_dy);
+    const int cx = qx >= 0.0f ? (qx < (float)(a.nx - 2) ? (int)qx : a.nx - 2) : 0;
+    const int cy = qy >= 0.0f ? (qy < (float)(a.ny - 2) ? (int)qy : a.ny - 2) : 0;
+    lx = min(lx, cx);
+    ly = min(ly, cy);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lx = min(lx, __shfl_xor_sync(0xFFFFFFFFu, lx, o));
+    ly = min(ly, __shfl_xor_sync(0xFFFFFFFFu, ly, o));
+  }
+  if ((threadIdx.x & 31) == 0) { red[threadIdx.x >> 5] = lx; red[NT / 32 + (threadIdx.x >> 5)] = ly; }
+  __syncthreads();
+  xlo = ylo = INT_MAX;
+#pragma unroll
+  for (int j = 0; j < NT / 32; ++j) { xlo = min(xlo, red[j]); ylo = min(ylo, red[NT / 32 + j]); }
+  __syncthreads();
+}
+
+constexpr long long TMA_SPIN_LIMIT = 1ll << 22;  // polls of the window's mbarrier before giving up
+
+template <bool HAS_B, int OPT>
+__global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonStepArgs a) {
+  constexpr bool HIST = (OPT & PB_OPT_SMEM_HIST) != 0;
+  constexpr bool TMA = (OPT & PB_OPT_TMA_TILE) != 0 && !HAS_B;
   pdl_enter();
   __shared__ IonStage st;
   __shared__ int sm_tile;
+  __shared__ int hbins[HIST ? HBINS : 1];
+  __shared__ int pcell[HIST ? TILE : 1];
+  __shared__ __align__(128) float4 ebox[TMA ? 2 * TB_W * TB_H : 1];
+  __shared__ __align__(8) uint64_t ebar;
+  if (HIST)
+    for (int b = threadIdx.x; b < HBINS; b += NT) hbins[b] = 0;
+  if (TMA && threadIdx.x == 0) mbar_init(&ebar, 1);
+  uint32_t tma_phase = 0;
+  bool tma_live = TMA;   // block-uniform; false after a window copy failed to complete
   const int n = *a.num_src;
   const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
   const double dt_sub = DDIV(a.dt, (double)n_sub);
@@ -559,6 +670,31 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
     const int tile = sm_tile;
     const int t0 = tile * TILE;
     if (t0 >= n) break;
+    EBox eb{nullptr, 0, 0};
+    if (TMA && tma_live) {
+      // stage the window of E corners around the tile's particles (one TMA copy), one
+      // cell of margin below and left of the lowest start cell
+      int xlo, ylo;
+      tile_low_cell(a, t0, n, xlo, ylo);
+      eb.bx = xlo - 1;
+      eb.by = ylo - 1;
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&ebar, TB_BYTES);
+        tma_load_3d(ebox, &a.ec_map, &ebar, 0, eb.bx, eb.by);
+      }
+      long long spin = 0;
+      bool done;
+      while (!(done = mbar_try_wait(&ebar, tma_phase)) && ++spin < TMA_SPIN_LIMIT) {
+      }
+      tma_phase ^= 1u;
+      if (__syncthreads_and(done)) {
+        eb.box = ebox;
+      } else {
+        tma_live = false;
+        if (threadIdx.x == 0) atomicOr(a.errflags, PB_EF_SPIN_TIMEOUT);
+      }
+    }
 #pragma unroll 1
     for (int k = threadIdx.x; k < TILE; k += NT) {
       const int i = t0 + k;
@@ -571,10 +707,10 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
         const float x0 = x, y0 = y;
         float q0[2];  // x0 / dx, y0 / dy (correctly rounded), from the first substep
         boris_push_one<HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h,
-                                      dtf, a.Ec, 0.0f, 0.0f, q0);
+                                      dtf, a.Ec, 0.0f, 0.0f, q0, eb);
         for (int s = 1; s < n_sub; ++s)
           boris_push_one<HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h,
-                                        dtf, a.Ec);
+                                        dtf, a.Ec, 0.0f, 0.0f, nullptr, eb);
         if (a.periodic) y = np_modf_pos(y, a.Lyf);
         // the final cell, the PPC cell and the deposit cell all round or truncate the same
         // correctly rounded quotients (what rint_div and trunc_div return)
@@ -722,11 +858,20 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
         st.cex[k] = cx; st.id[k] = pid;
       }
       st.keep[k] = kp;
-      // warp-aggregated counts (consecutive lanes, near-sorted cells)
-      warp_count_add(a.ppc, ppc_cell, kp != 0);
-      warp_count_add(a.cnt, dep_cell, kp != 0);
+      if (HIST) {
+        st.rank[k] = dep_cell;
+        pcell[k] = ppc_cell;
+      } else {
+        // warp-aggregated counts (consecutive lanes, near-sorted cells)
+        warp_count_add(a.ppc, ppc_cell, kp != 0);
+        warp_count_add(a.cnt, dep_cell, kp != 0);
+      }
     }
     __syncthreads();
+    if (HIST) {
+      tile_hist<NT, TILE>(pcell, st.keep, a.ppc, hbins);
+      tile_hist<NT, TILE>(st.rank, st.keep, a.cnt, hbins);
+    }
     long long base;
     tile_compact_ranks<NT, TILE>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
     for (int k = threadIdx.x; k < TILE; k += NT) {
@@ -737,6 +882,13 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(IonStepArgs a) {
       a.dst.cex[pos] = st.cex[k]; a.dst.id[pos] = st.id[k];
     }
     __syncthreads();
+  }
+  if (TMA && !tma_live && threadIdx.x == 0) {
+    // a window copy did not complete in time: wait (bounded) for it before the block's
+    // shared memory is released
+    long long spin = 0;
+    while (!mbar_try_wait(&ebar, tma_phase ^ 1u) && ++spin < TMA_SPIN_LIMIT) {
+    }
   }
   // flush per-thread tallies
 #pragma unroll
@@ -757,11 +909,15 @@ struct EleStage {
   uint8_t keep[TILE];
 };
 
-template <bool HAS_B>
+template <bool HAS_B, int OPT>
 __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
+  constexpr bool HIST = (OPT & PB_OPT_SMEM_HIST) != 0;
   pdl_enter();
   __shared__ EleStage st;
   __shared__ int sm_tile;
+  __shared__ int hbins[HIST ? HBINS : 1];
+  if (HIST)
+    for (int b = threadIdx.x; b < HBINS; b += NT) hbins[b] = 0;
   const int n = *a.num_src;
   const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
   const double dt_sub = DDIV(a.dt, (double)n_sub);
@@ -796,9 +952,11 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
         st.id[k] = a.src.id[i];
       }
       st.keep[k] = kp;
-      warp_count_add(a.cnt, dep_cell, kp != 0);
+      if (HIST) st.rank[k] = dep_cell;
+      else warp_count_add(a.cnt, dep_cell, kp != 0);
     }
     __syncthreads();
+    if (HIST) tile_hist<NT, TILE>(st.rank, st.keep, a.cnt, hbins);
     long long base;
     tile_compact_ranks<NT, TILE>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
     for (int k = threadIdx.x; k < TILE; k += NT) {

@@ -33,7 +33,6 @@
 
 namespace pb {
 
-constexpr int PT = 1024;  // threads per block (one block per SM)
 constexpr long long BAR_SPIN_LIMIT = 1ll << 22;
 constexpr float W_KEEP = (float)(1.0 - MG_JACOBI_OMEGA);
 
@@ -631,11 +630,8 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   }
 }
 
-// One instance on every block of the launch.
 __global__ void __launch_bounds__(PT, 1) k_poisson(const __grid_constant__ PoissonArgs a) { poisson_body(a); }
 
-// Several instances in one launch: block b solves instance blk_inst[b] together with the
-// other blocks of that instance's contiguous range (args[i].blk0, args[i].nblk).
 __global__ void __launch_bounds__(PT, 1) k_poisson_batch(const PoissonArgs* __restrict__ args,
                                                          const int* __restrict__ blk_inst) {
   __shared__ PoissonArgs sa;

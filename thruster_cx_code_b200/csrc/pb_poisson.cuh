@@ -5,6 +5,7 @@
 
 namespace pb {
 
+constexpr int PT = 1024;  // threads per block of the field-solve kernels (one block per SM)
 constexpr int MG_MAX_LEVELS = 16;
 constexpr double MG_JACOBI_OMEGA = 0.8;       // damped-Jacobi weight of the V-cycle smoother
 constexpr int MG_MAX_COARSE = 4096;          // largest coarsest level (dense inverse, nc^2 floats)
@@ -104,5 +105,16 @@ inline void fine_up_tiles(int ny, int nx, int nblk, int* ty_out, int* tx_out) {
   *ty_out = bty;
   *tx_out = btx;
 }
+
+#ifdef __CUDACC__
+// The field-solve kernels live in their own translation unit (pb_poisson.cu), compiled
+// with fused multiply-add contraction: the FP32 MG-PCG is compared with SuperLU to a
+// tolerance, not bit for bit, unlike the particle arithmetic.
+// One instance on every block of the launch.
+__global__ void k_poisson(const __grid_constant__ PoissonArgs a);
+// Several instances in one launch: block b solves instance blk_inst[b] together with the
+// other blocks of that instance's contiguous range (args[i].blk0, args[i].nblk).
+__global__ void k_poisson_batch(const PoissonArgs* __restrict__ args, const int* __restrict__ blk_inst);
+#endif
 
 }  // namespace pb

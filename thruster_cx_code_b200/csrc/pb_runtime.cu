@@ -1,5 +1,7 @@
 // libpbemcs runtime: device state of one simulation instance, the timestep sequence and
-// the C-ABI (include/pbemcs.h).  Unity build: the kernel sources are included here.
+// the C-ABI (include/pbemcs.h).  The particle and diagnostic kernel sources are included
+// here (one translation unit, no multiply-add contraction); the field solve is compiled
+// separately (pb_poisson.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,7 +16,7 @@
 
 #include "pbemcs.h"
 #include "pb_particles.cu"
-#include "pb_poisson.cu"
+#include "pb_poisson.cuh"
 #include "pb_misc.cu"
 #include "pb_mg_host.hpp"
 
@@ -72,6 +74,9 @@ struct Sim {
   float *Ex = nullptr, *Ey = nullptr, *rho = nullptr, *Tmap = nullptr;
   float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *e32 = nullptr;
   float4* ecorn = nullptr;  // per-cell corners of Ex and Ey, 2 x float4 per node
+  CUtensorMap ec_map;       // TMA view of ecorn (PB_OPT_TMA_TILE), valid for the array and shape below
+  const float4* ec_map_for = nullptr;
+  int ec_map_ny = 0, ec_map_nx = 0;
   uint8_t *isBound = nullptr, *cls = nullptr;
   uint8_t *bdist = nullptr, *bdist_tmp = nullptr;  // Chebyshev distance to the nearest bound node
   uint16_t* gridmask = nullptr;
@@ -89,6 +94,7 @@ struct Sim {
   int pgrid = 0;      // blocks of the field-solve launch (<= num_sms)
   int ut_key[3] = {0, 0, 0}, ut[2] = {1, 1};  // fine up-leg tiling for (ny, nx, blocks)
   int pbps = 8;       // step-kernel blocks per SM (the grid; tiles are handed out by a counter)
+  uint32_t kopts = PB_OPT_SMEM_HIST;  // kernel variants of the step (PB_OPT_*)
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
   // particles
   Species sp[2];
@@ -169,11 +175,53 @@ static cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, s
 }
 
 // ------------------------------------------------------------------ helpers
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (no link
+// against libcuda)
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  });
+  return fn;
+}
+
+// The corner array as a 3-D tensor of floats [ny][nx][8] with a box of 8 x TB_W x TB_H
+// (one cell's eight corner values innermost, 32 B; rows 32 nx B apart).  Boxes that reach
+// past the grid read zeros, which no gather uses: the gathered cell is clamped into it.
+static int32_t ensure_ec_map(struct Sim* s);
+
 static int grid_for(const Sim* s, long n, int bs, int per_sm = 8) {
   long g = (n + bs - 1) / bs;
   long cap = (long)s->num_sms * per_sm;
   if (g > cap) g = cap;
   return (int)std::max(1L, g);
+}
+
+static int32_t ensure_ec_map(Sim* s) {
+  if (s->ecorn && s->ec_map_for == s->ecorn && s->ec_map_ny == s->ny && s->ec_map_nx == s->nx) return PB_OK;
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return fail(PB_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const cuuint64_t dims[3] = {8, (cuuint64_t)s->nx, (cuuint64_t)s->ny};
+  const cuuint64_t strides[2] = {32, (cuuint64_t)s->nx * 32};
+  const cuuint32_t box[3] = {8, (cuuint32_t)TB_W, (cuuint32_t)TB_H};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(&s->ec_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)s->ecorn, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(PB_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  s->ec_map_for = s->ecorn;
+  s->ec_map_ny = s->ny;
+  s->ec_map_nx = s->nx;
+  return PB_OK;
 }
 
 static int32_t alloc_species(Sim* s, int k, int cap, int keep_n) {
@@ -714,7 +762,19 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   a.seed = s->seed; a.step = (uint32_t)p->iteration;
   a.ppc = s->ppc; a.cnt = s->cnt_i;
   a.tile_status = s->tile_status; a.tile_counter = s->tile_counter; a.errflags = ef;
-  CK(launch_pdl(k_ion_step<false>, grid_for(s, I.cap, TILE, s->pbps), NT, 0, st, a));
+  {
+    const dim3 g(grid_for(s, I.cap, TILE, s->pbps));
+    if (s->kopts & PB_OPT_TMA_TILE) {
+      if ((rc = ensure_ec_map(s))) return rc;
+      a.ec_map = s->ec_map;
+    }
+    switch (s->kopts & (PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE)) {
+      case 0: CK(launch_pdl(k_ion_step<false, 0>, g, NT, 0, st, a)); break;
+      case PB_OPT_SMEM_HIST: CK(launch_pdl(k_ion_step<false, PB_OPT_SMEM_HIST>, g, NT, 0, st, a)); break;
+      case PB_OPT_TMA_TILE: CK(launch_pdl(k_ion_step<false, PB_OPT_TMA_TILE>, g, NT, 0, st, a)); break;
+      default: CK(launch_pdl(k_ion_step<false, PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE>, g, NT, 0, st, a)); break;
+    }
+  }
   ++s->launches;
   mark(s);
 
@@ -738,7 +798,11 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
   b.errflags = ef;
-  CK(launch_pdl(k_ele_step<false>, grid_for(s, E.cap, TILE, s->pbps), NT, 0, st, b));
+  {
+    const dim3 g(grid_for(s, E.cap, TILE, s->pbps));
+    if (s->kopts & PB_OPT_SMEM_HIST) CK(launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST>, g, NT, 0, st, b));
+    else CK(launch_pdl(k_ele_step<false, 0>, g, NT, 0, st, b));
+  }
   ++s->launches;
   mark(s);
 
@@ -909,6 +973,18 @@ int32_t pb_sim_set_solver(pb_sim* h, double tol, double tol_inner, int32_t max_o
                             "coarse correction)");
   s->tol = tol; s->tol_inner = tol_inner; s->max_outer = max_outer; s->max_inner = max_inner; s->nu = nu;
   s->max_coarse = max_coarse;
+  return PB_OK;
+}
+
+int32_t pb_sim_set_kernel_options(pb_sim* h, uint32_t flags) {
+  if (flags & ~(uint32_t)(PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE))
+    return fail(PB_ERR_ARG, "pb_sim_set_kernel_options: unknown flag bits " + std::to_string(flags));
+  h->s.kopts = flags;
+  return PB_OK;
+}
+
+int32_t pb_sim_get_kernel_options(pb_sim* h, uint32_t* flags) {
+  *flags = h->s.kopts;
   return PB_OK;
 }
 
