@@ -185,8 +185,10 @@ int32_t pb_sim_set_launch(pb_sim* s, int32_t particle_blocks_per_sm, int32_t sol
  *   PB_OPT_SMEM_HIST  deposit and PPC counts go through shared-memory cell histograms per
  *                     tile of cell-sorted particles, flushed to HBM once per tile
  *   PB_OPT_TMA_TILE   the ion step stages each tile's window of the E-corner array in
- *                     shared memory with a TMA tensor copy before pushing */
-enum { PB_OPT_SMEM_HIST = 1 << 0, PB_OPT_TMA_TILE = 1 << 1 };
+ *                     shared memory with a TMA tensor copy before pushing
+ *   PB_OPT_ELE_PAIRS  the electron step pushes two particles per thread side by side, so
+ *                     that one particle's field loads overlap the other's arithmetic */
+enum { PB_OPT_SMEM_HIST = 1 << 0, PB_OPT_TMA_TILE = 1 << 1, PB_OPT_ELE_PAIRS = 1 << 2 };
 int32_t pb_sim_set_kernel_options(pb_sim* s, uint32_t flags);
 int32_t pb_sim_get_kernel_options(pb_sim* s, uint32_t* flags);
 

@@ -69,6 +69,30 @@ def test_launch_knobs(mods):
         sim.close()
 
 
+def test_kernel_options_knob(mods):
+    """The kernel-variant knob applies and reads back, and a tuning run over it picks one
+    of its values; particle state does not depend on it."""
+    _lib, A = mods
+    sp = _spec()
+    a, pa = W.make_sweep_sim(sp)
+    b, pb = W.make_sweep_sim(sp)
+    A.apply(a, {"kernel_options": 0})
+    A.apply(b, {"kernel_options": _lib.PB_OPT_SMEM_HIST | _lib.PB_OPT_TMA_TILE})
+    assert A.current(a)["kernel_options"] == 0 and A.current(b)["kernel_options"] == 3
+    for _ in range(3):
+        a.step(pa)
+        b.step(pb)
+    ia, sa = _ions_by_id(a)
+    ib, sb = _ions_by_id(b)
+    np.testing.assert_array_equal(ia, ib)
+    np.testing.assert_array_equal(sa, sb)
+    tuner = A.Autotuner(steps=2, warmup=1, space={"kernel_options": (0, 1, 2, 3)})
+    best, table = tuner.tune(a, pa)
+    assert best["kernel_options"] in (0, 1, 2, 3) and len(table) == 4
+    a.close()
+    b.close()
+
+
 def test_tune_two_knobs(mods):
     _lib, A = mods
     sp = _spec()

@@ -1,13 +1,14 @@
 """The step kernels' variants give the same bits.
 
-PB_OPT_SMEM_HIST (deposit and PPC counts through shared-memory cell histograms per tile)
-and PB_OPT_TMA_TILE (the ion step stages each tile's window of the E-corner array in
-shared memory with a TMA copy) change how the kernels move data, not what they compute.
+PB_OPT_SMEM_HIST (deposit and PPC counts through shared-memory cell histograms per tile),
+PB_OPT_TMA_TILE (the ion step stages each tile's window of the E-corner array in shared
+memory with a TMA copy) and PB_OPT_ELE_PAIRS (two electrons per thread pushed side by
+side) change how the kernels move data and schedule work, not what they compute.
 Three steps of the 257 x 1025 case from the same state, with the particles re-sorted by
 cell every step (so that tiles are compact and the windows and histograms are used) and
 once without sorting (wide tiles take the fallback paths), must agree bit for bit in every
-particle, the charge density, the PPC map and the damage map, under all four
-combinations.  The oracle pins the default combination (tests/test_gpu_large.py)."""
+particle, the charge density, the PPC map and the damage map, under every
+combination.  The oracle pins the default combination (tests/test_gpu_large.py)."""
 import numpy as np
 import pytest
 
@@ -56,7 +57,8 @@ def _run(PE, flags, sort_every, steps=3):
 def test_kernel_variants_bit_identical(PE, sort_every):
     from thruster_cx_code_b200 import _lib
     ref = _run(PE, 0, sort_every)
-    for flags in (_lib.PB_OPT_SMEM_HIST, _lib.PB_OPT_TMA_TILE, _lib.PB_OPT_SMEM_HIST | _lib.PB_OPT_TMA_TILE):
+    H, T, P = _lib.PB_OPT_SMEM_HIST, _lib.PB_OPT_TMA_TILE, _lib.PB_OPT_ELE_PAIRS
+    for flags in (H, T, H | T, P, H | P, H | T | P):
         got = _run(PE, flags, sort_every)
         for k in ("p", "e", "rho"):
             np.testing.assert_array_equal(got[k].view(np.uint32), ref[k].view(np.uint32), err_msg=f"{flags} {k}")

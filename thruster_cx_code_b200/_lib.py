@@ -138,6 +138,7 @@ def load():
 # kernel variants of the step (pb_sim_set_kernel_options)
 PB_OPT_SMEM_HIST = 1 << 0
 PB_OPT_TMA_TILE = 1 << 1
+PB_OPT_ELE_PAIRS = 1 << 2
 
 ERRORS = {1: "CUDA error", 2: "invalid argument", 3: "capacity", 4: "device wait timed out",
           5: "field solve did not converge", 6: "call out of order"}

@@ -12,6 +12,10 @@ best values depend on the grid size and the particle count:
   gathers against the cost of the sort).
 * ``particle_blocks_per_sm``: the grid of the ion and electron step kernels.
 * ``solve_blocks``: blocks of the field-solve launch ("all" SMs or "half").
+* ``kernel_options``: the step kernels' variants (``PB_OPT_*`` bits): shared-memory cell
+  histograms for the deposit and PPC counts, the TMA-staged E-corner window of the ion
+  step, and two electrons per thread pushed side by side.  Every combination computes the
+  same bits.
 
 Particle results are identical for every value of these knobs except ``sort_every``,
 which changes only the array order.  The field solve reaches the same FP64 tolerance
@@ -43,15 +47,18 @@ KNOBS = {
     "sort_every": (10, 20, 40),
     "particle_blocks_per_sm": (4, 8, 16),
     "solve_blocks": ("all", "half"),
+    "kernel_options": (0, 1, 2, 3, 4, 5, 6, 7),
 }
 
 
 def current(sim):
     """The simulator's knob values."""
     s = sim.solver
+    opts = C.c_uint32()
+    _lib.check(_lib.load().pb_sim_get_kernel_options(sim._h, C.byref(opts)), "pb_sim_get_kernel_options")
     return {"max_coarse": int(s["max_coarse"]), "tol_inner": float(s["tol_inner"]),
             "sort_every": int(sim.sort_every), "particle_blocks_per_sm": int(getattr(sim, "_pbps", 8)),
-            "solve_blocks": getattr(sim, "_solve_blocks", "all")}
+            "solve_blocks": getattr(sim, "_solve_blocks", "all"), "kernel_options": int(opts.value)}
 
 
 def _num_sms(sim):
@@ -77,6 +84,8 @@ def apply(sim, knobs):
         _lib.check(lib.pb_sim_rebuild_operator(sim._h), "rebuild_operator")
     if "sort_every" in knobs:
         sim.sort_every = int(knobs["sort_every"])
+    if "kernel_options" in knobs:
+        _lib.check(lib.pb_sim_set_kernel_options(sim._h, int(knobs["kernel_options"])), "pb_sim_set_kernel_options")
     if "particle_blocks_per_sm" in knobs or "solve_blocks" in knobs:
         pbps = int(knobs.get("particle_blocks_per_sm", getattr(sim, "_pbps", 8)))
         sb = knobs.get("solve_blocks", getattr(sim, "_solve_blocks", "all"))

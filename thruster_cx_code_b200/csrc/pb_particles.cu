@@ -111,6 +111,66 @@ __device__ __forceinline__ float div_rn_checked(float x, float d, float inv) {
 // fraction from floor_frac: six fewer XU-pipe instructions (reciprocal and conversions)
 // per substep.  The XU pipe limits the electron kernel (many substeps); kernels with
 // fewer substeps and more live registers run faster without it.
+// Cell and bilinear weights of a push at (x, y): float32 quotients x / dx, y / dy, the
+// clamped floor cell (ix0, iy0) and the float64 weights of the reference's gather.
+template <bool LIGHT>
+__device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, float dxf, float dyf, float inv_dx,
+                                          float inv_dy, float* q_start, int& ix0, int& iy0, double& w00,
+                                          double& w10, double& w01, double& w11) {
+  const float ixf = LIGHT ? div_rn_checked(x, dxf, inv_dx) : __fdiv_rn(x, dxf);
+  const float iyf = LIGHT ? div_rn_checked(y, dyf, inv_dy) : __fdiv_rn(y, dyf);
+  if (q_start) { q_start[0] = ixf; q_start[1] = iyf; }  // x / dx, y / dy at the start position
+  double fx, fy;
+  // inside the grid the clamp is a no-op and ixf - ix0 is the exact float fraction
+  int fxi, fyi;
+  float frx, fry;
+  if (LIGHT && floor_frac(ixf, fxi, frx) && fxi <= nx - 2 && floor_frac(iyf, fyi, fry) && fyi <= ny - 2) {
+    ix0 = fxi;
+    iy0 = fyi;
+    fx = (double)frx;
+    fy = (double)fry;
+  } else {
+    ix0 = clampi(np_f2i32(floorf(ixf)), 0, nx - 2);
+    iy0 = clampi(np_f2i32(floorf(iyf)), 0, ny - 2);
+    fx = DSUB((double)ixf, (double)ix0);
+    fy = DSUB((double)iyf, (double)iy0);
+  }
+  const double gx = DSUB(1.0, fx), gy = DSUB(1.0, fy);
+  w00 = DMUL(gx, gy); w10 = DMUL(fx, gy); w01 = DMUL(gx, fy); w11 = DMUL(fx, fy);
+}
+
+// Half kick, rotation (B = 0: t = s = h * (+0)), half kick and drift from the gathered E.
+__device__ __forceinline__ void push_update_b0(float& x, float& y, float& vx, float& vy, float& vz, double ex,
+                                               double ey, double h, float dtf) {
+  const double vmx = DADD((double)vx, DMUL(h, ex));
+  const double vmy = DADD((double)vy, DMUL(h, ey));
+  if (vmx != 0.0 && vmy != 0.0 && vz != 0.0f && fabs(vmx) < INFINITY && fabs(vmy) < INFINITY &&
+      fabsf(vz) < INFINITY) {
+    // every cross-product term below is a signed zero (t = s = h * (+0)), and a finite
+    // nonzero value plus a zero is that value: the rotation is the identity, bit for bit
+    // (vz goes to double and back unchanged, so it is left as it is)
+    vx = __double2float_rn(DADD(vmx, DMUL(h, ex)));
+    vy = __double2float_rn(DADD(vmy, DMUL(h, ey)));
+    x = __fadd_rn(x, __fmul_rn(__fmul_rn(vx, dtf), 1000.0f));
+    y = __fadd_rn(y, __fmul_rn(__fmul_rn(vy, dtf), 1000.0f));
+    return;
+  }
+  const double vmz = (double)vz;
+  const double tx = DMUL(h, 0.0), ty = tx, tz = tx;
+  const double sx = DMUL(2.0, tx), sy = sx, sz = sx;
+  const double vpx = DADD(vmx, DSUB(DMUL(vmy, tz), DMUL(vmz, ty)));
+  const double vpy = DADD(vmy, DSUB(DMUL(vmz, tx), DMUL(vmx, tz)));
+  const double vpz = DADD(vmz, DSUB(DMUL(vmx, ty), DMUL(vmy, tx)));
+  const double wx = DADD(vmx, DSUB(DMUL(vpy, sz), DMUL(vpz, sy)));
+  const double wy = DADD(vmy, DSUB(DMUL(vpz, sx), DMUL(vpx, sz)));
+  const double wz = DADD(vmz, DSUB(DMUL(vpx, sy), DMUL(vpy, sx)));
+  vx = __double2float_rn(DADD(wx, DMUL(h, ex)));
+  vy = __double2float_rn(DADD(wy, DMUL(h, ey)));
+  vz = __double2float_rn(wz);
+  x = __fadd_rn(x, __fmul_rn(__fmul_rn(vx, dtf), 1000.0f));
+  y = __fadd_rn(y, __fmul_rn(__fmul_rn(vy, dtf), 1000.0f));
+}
+
 template <bool HAS_B, bool CORN = false, bool LIGHT = false>
 __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, float& vy, float& vz,
                                                const float* __restrict__ Ex, const float* __restrict__ Ey,
@@ -121,31 +181,11 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
                                                float inv_dy = 0.0f, float* q_start = nullptr,
                                                EBox eb = EBox{nullptr, 0, 0}) {
   static_assert(!(HAS_B && CORN), "the corner gather has no B field");
-  const float ixf = LIGHT ? div_rn_checked(x, dxf, inv_dx) : __fdiv_rn(x, dxf);
-  const float iyf = LIGHT ? div_rn_checked(y, dyf, inv_dy) : __fdiv_rn(y, dyf);
-  if (q_start) { q_start[0] = ixf; q_start[1] = iyf; }  // x / dx, y / dy at the start position
   int ix0, iy0;
-  double fx, fy;
-  {
-    // inside the grid the clamp is a no-op and ixf - ix0 is the exact float fraction
-    int fxi, fyi;
-    float frx, fry;
-    if (LIGHT && floor_frac(ixf, fxi, frx) && fxi <= nx - 2 && floor_frac(iyf, fyi, fry) && fyi <= ny - 2) {
-      ix0 = fxi;
-      iy0 = fyi;
-      fx = (double)frx;
-      fy = (double)fry;
-    } else {
-      ix0 = clampi(np_f2i32(floorf(ixf)), 0, nx - 2);
-      iy0 = clampi(np_f2i32(floorf(iyf)), 0, ny - 2);
-      fx = DSUB((double)ixf, (double)ix0);
-      fy = DSUB((double)iyf, (double)iy0);
-    }
-  }
+  double w00, w10, w01, w11;
+  push_cell<LIGHT>(x, y, nx, ny, dxf, dyf, inv_dx, inv_dy, q_start, ix0, iy0, w00, w10, w01, w11);
   int ix1 = min(ix0 + 1, nx - 1);
   int iy1 = min(iy0 + 1, ny - 1);
-  double gx = DSUB(1.0, fx), gy = DSUB(1.0, fy);
-  double w00 = DMUL(gx, gy), w10 = DMUL(fx, gy), w01 = DMUL(gx, fy), w11 = DMUL(fx, fy);
   size_t r0 = (size_t)iy0 * nx, r1 = (size_t)iy1 * nx;
   double ex, ey;
   if (CORN) {
@@ -160,44 +200,59 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
     ex = gather4(Ex, r0, r1, ix0, ix1, w00, w10, w01, w11);
     ey = gather4(Ey, r0, r1, ix0, ix1, w00, w10, w01, w11);
   }
-  double vmx = DADD((double)vx, DMUL(h, ex));
-  double vmy = DADD((double)vy, DMUL(h, ey));
-  if (!HAS_B && vmx != 0.0 && vmy != 0.0 && vz != 0.0f && fabs(vmx) < INFINITY && fabs(vmy) < INFINITY &&
-      fabsf(vz) < INFINITY) {
-    // every cross-product term below is a signed zero (t = s = h * (+0)), and a finite
-    // nonzero value plus a zero is that value: the rotation is the identity, bit for bit
-    // (vz goes to double and back unchanged, so it is left as it is)
-    vx = __double2float_rn(DADD(vmx, DMUL(h, ex)));
-    vy = __double2float_rn(DADD(vmy, DMUL(h, ey)));
-    x = __fadd_rn(x, __fmul_rn(__fmul_rn(vx, dtf), 1000.0f));
-    y = __fadd_rn(y, __fmul_rn(__fmul_rn(vy, dtf), 1000.0f));
+  if (!HAS_B) {
+    push_update_b0(x, y, vx, vy, vz, ex, ey, h, dtf);
     return;
   }
+  const double vmx = DADD((double)vx, DMUL(h, ex));
+  const double vmy = DADD((double)vy, DMUL(h, ey));
   const double vmz = (double)vz;
-  double tx, ty, tz, sx, sy, sz;
-  if (HAS_B) {
-    double bx = gather4(Bx, r0, r1, ix0, ix1, w00, w10, w01, w11);
-    double by = gather4(By, r0, r1, ix0, ix1, w00, w10, w01, w11);
-    double bz = gather4(Bz, r0, r1, ix0, ix1, w00, w10, w01, w11);
-    tx = DMUL(h, bx); ty = DMUL(h, by); tz = DMUL(h, bz);
-    double t2 = DADD(DADD(DMUL(tx, tx), DMUL(ty, ty)), DMUL(tz, tz));
-    double den = DADD(1.0, t2);
-    sx = DDIV(DMUL(2.0, tx), den); sy = DDIV(DMUL(2.0, ty), den); sz = DDIV(DMUL(2.0, tz), den);
-  } else {
-    tx = DMUL(h, 0.0); ty = tx; tz = tx;
-    sx = DMUL(2.0, tx); sy = sx; sz = sx;
-  }
-  double vpx = DADD(vmx, DSUB(DMUL(vmy, tz), DMUL(vmz, ty)));
-  double vpy = DADD(vmy, DSUB(DMUL(vmz, tx), DMUL(vmx, tz)));
-  double vpz = DADD(vmz, DSUB(DMUL(vmx, ty), DMUL(vmy, tx)));
-  double wx = DADD(vmx, DSUB(DMUL(vpy, sz), DMUL(vpz, sy)));
-  double wy = DADD(vmy, DSUB(DMUL(vpz, sx), DMUL(vpx, sz)));
-  double wz = DADD(vmz, DSUB(DMUL(vpx, sy), DMUL(vpy, sx)));
+  double bx = gather4(Bx, r0, r1, ix0, ix1, w00, w10, w01, w11);
+  double by = gather4(By, r0, r1, ix0, ix1, w00, w10, w01, w11);
+  double bz = gather4(Bz, r0, r1, ix0, ix1, w00, w10, w01, w11);
+  const double tx = DMUL(h, bx), ty = DMUL(h, by), tz = DMUL(h, bz);
+  const double t2 = DADD(DADD(DMUL(tx, tx), DMUL(ty, ty)), DMUL(tz, tz));
+  const double den = DADD(1.0, t2);
+  const double sx = DDIV(DMUL(2.0, tx), den), sy = DDIV(DMUL(2.0, ty), den), sz = DDIV(DMUL(2.0, tz), den);
+  const double vpx = DADD(vmx, DSUB(DMUL(vmy, tz), DMUL(vmz, ty)));
+  const double vpy = DADD(vmy, DSUB(DMUL(vmz, tx), DMUL(vmx, tz)));
+  const double vpz = DADD(vmz, DSUB(DMUL(vmx, ty), DMUL(vmy, tx)));
+  const double wx = DADD(vmx, DSUB(DMUL(vpy, sz), DMUL(vpz, sy)));
+  const double wy = DADD(vmy, DSUB(DMUL(vpz, sx), DMUL(vpx, sz)));
+  const double wz = DADD(vmz, DSUB(DMUL(vpx, sy), DMUL(vpy, sx)));
   vx = __double2float_rn(DADD(wx, DMUL(h, ex)));
   vy = __double2float_rn(DADD(wy, DMUL(h, ey)));
   vz = __double2float_rn(wz);
   x = __fadd_rn(x, __fmul_rn(__fmul_rn(vx, dtf), 1000.0f));
   y = __fadd_rn(y, __fmul_rn(__fmul_rn(vy, dtf), 1000.0f));
+}
+
+// Two electrons pushed n_sub times side by side (PB_OPT_ELE_PAIRS): both cells and both
+// corner loads are issued before either particle's arithmetic, so one particle's load
+// latency overlaps the other's.  Each particle's operations are those of boris_push_one.
+__device__ __forceinline__ void push_pair_b0(float (&x)[2], float (&y)[2], float (&vx)[2], float (&vy)[2],
+                                             float (&vz)[2], int n_sub, const float4* __restrict__ Ec, int nx,
+                                             int ny, float dxf, float dyf, float inv_dx, float inv_dy, double h,
+                                             float dtf) {
+  for (int s = 0; s < n_sub; ++s) {
+    int ix0[2], iy0[2];
+    double w[2][4];
+    float4 A[2], B[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      push_cell<true>(x[q], y[q], nx, ny, dxf, dyf, inv_dx, inv_dy, nullptr, ix0[q], iy0[q], w[q][0], w[q][1],
+                      w[q][2], w[q][3]);
+      const size_t c = (size_t)iy0[q] * nx + ix0[q];
+      A[q] = __ldg(Ec + 2 * c);
+      B[q] = __ldg(Ec + 2 * c + 1);
+    }
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      double ex, ey;
+      gather4v(A[q], B[q], w[q][0], w[q][1], w[q][2], w[q][3], ex, ey);
+      push_update_b0(x[q], y[q], vx[q], vy[q], vz[q], ex, ey, h, dtf);
+    }
+  }
 }
 
 // n_sub from the reduced displacement: max(1, ceil(ds_max / max(ds_lim, 1e-30)))
@@ -909,9 +964,25 @@ struct EleStage {
   uint8_t keep[TILE];
 };
 
+// The end of one electron's step after its pushes: periodic wrap, purge test and the
+// next step's deposit cell; the survivor is staged in shared memory at tile slot k.
+__device__ __forceinline__ void ele_finish(const EleStepArgs& a, EleStage& st, int k, int i, float x, float y,
+                                           float vx, float vy, float vz, uint8_t& kp, int& dep_cell) {
+  if (a.periodic) y = np_modf_pos(y, a.Lyf);
+  int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1), icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
+  bool dead = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
+  dead = dead || (x < 0.0f) || (x > a.Lxf) || (y < 0.0f) || (y > a.Lyf) || (x != x);
+  kp = !dead;
+  if (kp)
+    dep_cell = cell_round32_f(y, a.dyf, a.inv_dy, 1, a.ny - 2) * a.nx + cell_round32_f(x, a.dxf, a.inv_dx, 1, a.nx - 2);
+  st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
+  st.id[k] = a.src.id[i];
+}
+
 template <bool HAS_B, int OPT>
 __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
   constexpr bool HIST = (OPT & PB_OPT_SMEM_HIST) != 0;
+  constexpr bool PAIRS = (OPT & PB_OPT_ELE_PAIRS) != 0 && !HAS_B;
   pdl_enter();
   __shared__ EleStage st;
   __shared__ int sm_tile;
@@ -930,30 +1001,47 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
     const int tile = sm_tile;
     const int t0 = tile * TILE;
     if (t0 >= n) break;
+    if (PAIRS) {
+      // items k and k + NT of a thread pushed side by side (TILE = 4 NT: two pairs)
 #pragma unroll 1
-    for (int k = threadIdx.x; k < TILE; k += NT) {
-      const int i = t0 + k;
-      uint8_t kp = 0;
-      int dep_cell = 0;
-      if (i < n) {
-        float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
-        for (int s = 0; s < n_sub; ++s)
-          boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
-                                                a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy);
-        if (a.periodic) y = np_modf_pos(y, a.Lyf);
-        int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1), icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
-        bool dead = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
-        dead = dead || (x < 0.0f) || (x > a.Lxf) || (y < 0.0f) || (y > a.Lyf) || (x != x);
-        kp = !dead;
-        if (kp)
-          dep_cell = cell_round32_f(y, a.dyf, a.inv_dy, 1, a.ny - 2) * a.nx +
-                     cell_round32_f(x, a.dxf, a.inv_dx, 1, a.nx - 2);
-        st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
-        st.id[k] = a.src.id[i];
+      for (int k = threadIdx.x; k < TILE; k += 2 * NT) {
+        float x[2], y[2], vx[2], vy[2], vz[2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int i = t0 + k + q * NT;
+          // a slot past the end pushes a copy of an in-range particle (never stored)
+          const int j = i < n ? i : t0;
+          x[q] = a.src.x[j]; y[q] = a.src.y[j]; vx[q] = a.src.vx[j]; vy[q] = a.src.vy[j]; vz[q] = a.src.vz[j];
+        }
+        push_pair_b0(x, y, vx, vy, vz, n_sub, a.Ec, a.nx, a.ny, a.dxf, a.dyf, a.inv_dx, a.inv_dy, h, dtf);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int kk = k + q * NT, i = t0 + kk;
+          uint8_t kp = 0;
+          int dep_cell = 0;
+          if (i < n) ele_finish(a, st, kk, i, x[q], y[q], vx[q], vy[q], vz[q], kp, dep_cell);
+          st.keep[kk] = kp;
+          if (HIST) st.rank[kk] = dep_cell;
+          else warp_count_add(a.cnt, dep_cell, kp != 0);
+        }
       }
-      st.keep[k] = kp;
-      if (HIST) st.rank[k] = dep_cell;
-      else warp_count_add(a.cnt, dep_cell, kp != 0);
+    } else {
+#pragma unroll 1
+      for (int k = threadIdx.x; k < TILE; k += NT) {
+        const int i = t0 + k;
+        uint8_t kp = 0;
+        int dep_cell = 0;
+        if (i < n) {
+          float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
+          for (int s = 0; s < n_sub; ++s)
+            boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
+                                                  a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy);
+          ele_finish(a, st, k, i, x, y, vx, vy, vz, kp, dep_cell);
+        }
+        st.keep[k] = kp;
+        if (HIST) st.rank[k] = dep_cell;
+        else warp_count_add(a.cnt, dep_cell, kp != 0);
+      }
     }
     __syncthreads();
     if (HIST) tile_hist<NT, TILE>(st.rank, st.keep, a.cnt, hbins);

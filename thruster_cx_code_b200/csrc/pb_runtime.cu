@@ -800,8 +800,12 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.errflags = ef;
   {
     const dim3 g(grid_for(s, E.cap, TILE, s->pbps));
-    if (s->kopts & PB_OPT_SMEM_HIST) CK(launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST>, g, NT, 0, st, b));
-    else CK(launch_pdl(k_ele_step<false, 0>, g, NT, 0, st, b));
+    switch (s->kopts & (PB_OPT_SMEM_HIST | PB_OPT_ELE_PAIRS)) {
+      case 0: CK(launch_pdl(k_ele_step<false, 0>, g, NT, 0, st, b)); break;
+      case PB_OPT_SMEM_HIST: CK(launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST>, g, NT, 0, st, b)); break;
+      case PB_OPT_ELE_PAIRS: CK(launch_pdl(k_ele_step<false, PB_OPT_ELE_PAIRS>, g, NT, 0, st, b)); break;
+      default: CK(launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST | PB_OPT_ELE_PAIRS>, g, NT, 0, st, b)); break;
+    }
   }
   ++s->launches;
   mark(s);
@@ -977,7 +981,7 @@ int32_t pb_sim_set_solver(pb_sim* h, double tol, double tol_inner, int32_t max_o
 }
 
 int32_t pb_sim_set_kernel_options(pb_sim* h, uint32_t flags) {
-  if (flags & ~(uint32_t)(PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE))
+  if (flags & ~(uint32_t)(PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE | PB_OPT_ELE_PAIRS))
     return fail(PB_ERR_ARG, "pb_sim_set_kernel_options: unknown flag bits " + std::to_string(flags));
   h->s.kopts = flags;
   return PB_OK;

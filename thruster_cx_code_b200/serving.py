@@ -147,14 +147,18 @@ class Convergence:
 
 
 class Request:
-    """One sweep point: ``make()`` builds and returns (sim, params) on the device."""
+    """One sweep point: ``make()`` builds and returns (sim, params) on the device.
+    ``finish(sim)``, if given, runs at retirement before the simulator is released; its
+    return value is kept as ``result`` (e.g. the final state or diagnostics to report)."""
 
-    def __init__(self, rid, make, est_bytes, max_steps, convergence):
+    def __init__(self, rid, make, est_bytes, max_steps, convergence, finish=None):
         self.rid = rid
         self.make = make
         self.est_bytes = int(est_bytes)
         self.max_steps = int(max_steps)
         self.conv = convergence
+        self.finish = finish
+        self.result = None
         self.sim = None
         self.params = None
         self.t_arrival = None
@@ -192,6 +196,8 @@ class SweepServer:
 
     def _retire(self, req, now):
         req.t_done = now
+        if req.finish is not None:
+            req.result = req.finish(req.sim)
         req.sim.close()
         req.sim = None
         self.active.remove(req)
