@@ -190,6 +190,18 @@ int32_t pb_sim_set_launch(pb_sim* s, int32_t particle_blocks_per_sm, int32_t sol
  *                     that one particle's field loads overlap the other's arithmetic */
 enum { PB_OPT_SMEM_HIST = 1 << 0, PB_OPT_TMA_TILE = 1 << 1, PB_OPT_ELE_PAIRS = 1 << 2 };
 int32_t pb_sim_set_kernel_options(pb_sim* s, uint32_t flags);
+/* CUDA graphs of whole steps in pb_sim_run and pb_sim_step (no counterpart in the
+ * reference): with on != 0 each step shape (its parameters apart from the step number,
+ * and the buffers and settings its launches take) is captured once and replayed; the step
+ * number that keys the Philox draws is read from device memory.  Results are the same bits
+ * as without graphs.  Steps with RF co-extraction and profiled steps are enqueued as usual,
+ * and so are all steps after a capture fails (see pb_sim_graph_stats).  A simulator in
+ * graph mode should not run concurrently with another simulator's cooperative field solve
+ * on the same device (batches use pb_batch_run). */
+int32_t pb_sim_set_graphs(pb_sim* s, int32_t on);
+/* out4: captures, replays, steps enqueued without a graph while graph mode was on, and 1
+ * if a capture failed (then pb_last_error() gives the reason). */
+int32_t pb_sim_graph_stats(pb_sim* s, int64_t* out4);
 int32_t pb_sim_get_kernel_options(pb_sim* s, uint32_t* flags);
 
 /* Upload the domain of build_domain (physics_engine.py:629-847): node masks, Dirichlet

@@ -86,6 +86,7 @@ struct IonStepArgs {
   float cex_g_max;     // speeds above this bypass the bound
   uint64_t seed;
   uint32_t step;
+  const uint32_t* step_dev;  // non-null in a captured step: the step key is read from here
   // counts for diagnostics / next deposit
   int *ppc;            // int32 (ny, nx) current PPC map (trunc cells)
   int *cnt;            // int32 (ny, nx) deposit counts for the next step (round cells)

@@ -33,6 +33,7 @@ __device__ int poisson_inversion(double u, double lam) {
 // inject step A (physics_engine.py:996-1099): counts, slots and ids for this step
 __global__ void k_inject_prep(InjectArgs a) {
   pdl_enter();
+  if (a.step_dev) a.step = *a.step_dev;
   int n_ion = 0, n_rf = 0;
   if (a.ion_on) n_ion = poisson_inversion(philox_uniform(a.seed, 0, SITE_ION_COUNT, a.step, 0), a.lam);
   if (a.rf_on) {
@@ -63,6 +64,7 @@ __global__ void k_inject_prep(InjectArgs a) {
 // inject step B: one thread per new particle; blockIdx.y selects ions / rf / neutralizer
 __global__ void k_inject_gen(InjectArgs a) {
   pdl_enter();
+  if (a.step_dev) a.step = *a.step_dev;
   const int seg = blockIdx.y;
   const int n = a.inj[seg];
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
@@ -155,6 +157,7 @@ __device__ void block_sort_u64(uint64_t* keys, int n) {
 // surviving electrons (physics_engine.py:1400-1417, 1541-1561).
 __global__ void k_see_finish(SeeArgs a) {
   pdl_enter();
+  if (a.step_dev) a.step = *a.step_dev;
   __shared__ int sm[32];
   __shared__ int s_base, s_total;
   int n = *a.see_count;

@@ -28,6 +28,7 @@ struct InjectArgs {
   // keys and state
   uint64_t seed;
   uint32_t step;
+  const uint32_t* step_dev;  // non-null in a captured step: the step key is read from here
   int *num_p, *num_e;
   int cap_p, cap_e;
   uint32_t *next_ion_id, *next_e_id;
@@ -47,6 +48,7 @@ struct SeeArgs {
   int *see_spawned;
   uint64_t seed;
   uint32_t step;
+  const uint32_t* step_dev;  // non-null in a captured step: the step key is read from here
   double v_see_th;
   Soa eles;
   int *num_e;

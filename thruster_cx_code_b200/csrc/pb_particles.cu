@@ -693,6 +693,7 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
   constexpr bool HIST = (OPT & PB_OPT_SMEM_HIST) != 0;
   constexpr bool TMA = (OPT & PB_OPT_TMA_TILE) != 0 && !HAS_B;
   pdl_enter();
+  const uint32_t stepk = a.step_dev ? *a.step_dev : a.step;  // Philox step key
   __shared__ IonStage st;
   __shared__ int sm_tile;
   __shared__ int hbins[HIST ? HBINS : 1];
@@ -810,7 +811,7 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
             g = (g != g) ? g : (g < 0.0f ? 0.0f : (g > 1.0f ? 1.0f : g));
             gamma = (double)g;
           }
-          double u = philox_uniform(a.seed, pid, SITE_SEE_SPAWN, a.step, 0);
+          double u = philox_uniform(a.seed, pid, SITE_SEE_SPAWN, stepk, 0);
           if (u < gamma) {
             int r = atomicAdd(a.see_count, 1);
             if (r < a.see_cap) {
@@ -858,7 +859,7 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
           if (!cx && x >= 1.0f && x <= a.Lxf) {
             float vm = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)), __fmul_rn(vz, vz)));
             float g = np_maxf(vm, 1.0f);
-            double u = philox_uniform(a.seed, pid, SITE_CEX_U, a.step, 0);
+            double u = philox_uniform(a.seed, pid, SITE_CEX_U, stepk, 0);
             if (!(g <= a.cex_g_max && u >= DADD(DMUL(a.cex_bound, (double)g), 1e-15))) {
               double nl;
               if (a.n_uniform) {
@@ -888,11 +889,11 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
               if (fabs(u - prob) <= fabs(prob) * 8.9e-16 + 1e-300) cnt[6]++;
               if (u < prob) {
                 cnt[5]++;
-                u32x4 r0 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 0);
-                u32x4 r1 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 1);
-                u32x4 r2 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 2);
-                u32x4 r3 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 3);
-                u32x4 r4 = philox_block(a.seed, pid, SITE_CEX_FM, a.step, 4);
+                u32x4 r0 = philox_block(a.seed, pid, SITE_CEX_FM, stepk, 0);
+                u32x4 r1 = philox_block(a.seed, pid, SITE_CEX_FM, stepk, 1);
+                u32x4 r2 = philox_block(a.seed, pid, SITE_CEX_FM, stepk, 2);
+                u32x4 r3 = philox_block(a.seed, pid, SITE_CEX_FM, stepk, 3);
+                u32x4 r4 = philox_block(a.seed, pid, SITE_CEX_FM, stepk, 4);
                 double fmx = DMUL(2.0, DSUB(DADD(DADD(u53(r0.x, r0.y), u53(r0.z, r0.w)), u53(r1.x, r1.y)), 1.5));
                 double fmy = DMUL(2.0, DSUB(DADD(DADD(u53(r1.z, r1.w), u53(r2.x, r2.y)), u53(r2.z, r2.w)), 1.5));
                 double fmz = DMUL(2.0, DSUB(DADD(DADD(u53(r3.x, r3.y), u53(r3.z, r3.w)), u53(r4.x, r4.y)), 1.5));

@@ -152,6 +152,20 @@ struct Sim {
   size_t mark_used = 0;
   long long launches = 0;   // kernels enqueued by the last pb_sim_run / pb_sim_step
   double sp_dx = 1.0, sp_dy = 1.0;   // grid spacing of the last step (cell keys of the sort)
+  // CUDA graphs of whole steps (pb_sim_set_graphs): a step is captured once per shape (its
+  // parameters without the step number, and the simulator state its launches bake in) and
+  // replayed; the step number the Philox draws are keyed by comes from step_dev
+  int graphs_on = 0, graphs_broken = 0, capturing = 0;
+  uint32_t* step_dev = nullptr;
+  long long step_dev_val = -1;     // the value step_dev holds once the stream reaches this point
+  struct StepGraph {
+    uint64_t pkey = 0, skey = 0;   // parameter digest, state signature before the step
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
+  };
+  std::vector<StepGraph> graphs;
+  long long graph_captures = 0, graph_replays = 0, graph_plain_steps = 0;
+  std::string graph_error;
 };
 
 // A launch with programmatic stream serialization (the step's kernels): the kernel may be
@@ -436,9 +450,17 @@ static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
   PoissonArgs a = poisson_args(s, iterations, p);
   CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), s->stream));
   void* args[] = {&a};
-  int32_t rc = coop_launch(s->device, s->stream, [&]() {
-    return cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream);
-  });
+  int32_t rc;
+  if (s->capturing) {
+    // inside a step graph: ordered by the simulator's own stream (a graph runs its
+    // simulator alone, so no other cooperative launch is chained against it)
+    CK(cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream));
+    rc = PB_OK;
+  } else {
+    rc = coop_launch(s->device, s->stream, [&]() {
+      return cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream);
+    });
+  }
   if (rc) return rc;
   ++s->launches;
   return PB_OK;
@@ -670,7 +692,7 @@ static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
   ia.rf_on = p->rf_on; ia.rf_num_float = p->rf_num_float; ia.rf_ylo = p->rf_ylo; ia.rf_yhi = p->rf_yhi;
   ia.v_e_src = p->v_e_src;
   ia.neut_n = p->neut_n; ia.neut_r = p->neut_r; ia.v_e_th = p->v_e_th; ia.neut_x = (float)p->neut_x;
-  ia.seed = s->seed; ia.step = (uint32_t)p->iteration;
+  ia.seed = s->seed; ia.step = (uint32_t)p->iteration; ia.step_dev = s->capturing ? s->step_dev : nullptr;
   ia.num_p = ni_src; ia.num_e = ne_src; ia.cap_p = I.cap; ia.cap_e = E.cap;
   ia.next_ion_id = s->next_ids; ia.next_e_id = s->next_ids + 1;
   ia.inj = s->inj;
@@ -759,7 +781,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
     a.cex_bound = n_max * sig_max * p->dt * (1.0 + 1e-5);
     a.cex_g_max = h->cx.nt > 0 ? INFINITY : 1e14f;
   }
-  a.seed = s->seed; a.step = (uint32_t)p->iteration;
+  a.seed = s->seed; a.step = (uint32_t)p->iteration; a.step_dev = s->capturing ? s->step_dev : nullptr;
   a.ppc = s->ppc; a.cnt = s->cnt_i;
   a.tile_status = s->tile_status; a.tile_counter = s->tile_counter; a.errflags = ef;
   {
@@ -813,7 +835,8 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   // SEE electrons, appended after the surviving electrons (:1390-1417)
   SeeArgs sa{};
   sa.see_key = s->see_key; sa.see_xy = s->see_xy; sa.see_count = s->see_count; sa.see_cap = s->see_cap;
-  sa.see_spawned = s->see_spawned; sa.seed = s->seed; sa.step = (uint32_t)p->iteration; sa.v_see_th = p->v_see_th;
+  sa.see_spawned = s->see_spawned; sa.seed = s->seed; sa.step = (uint32_t)p->iteration;
+  sa.step_dev = s->capturing ? s->step_dev : nullptr; sa.v_see_th = p->v_see_th;
   sa.eles = E.buf[1 - E.cur]; sa.num_e = ne_dst; sa.cap_e = E.cap; sa.next_e_id = s->next_ids + 1;
   sa.isBound = s->isBound; sa.nx = s->nx; sa.ny = s->ny; sa.dxf = dxf; sa.dyf = dyf;
   sa.Lxf = (float)p->Lx; sa.Lyf = (float)p->Ly; sa.cnt_e = s->cnt_e; sa.errflags = ef;
@@ -866,6 +889,157 @@ static int32_t enqueue_step(pb_sim* h, const pb_step_params* p) {
   if ((rc = enqueue_step_pre(h, p))) return rc;
   if (p->do_poisson && (rc = launch_poisson(&h->s, p->picard_iters, p))) return rc;
   return enqueue_step_post(h, p);
+}
+
+// ------------------------------------------------------------------ step graphs
+__global__ void k_step_advance(uint32_t* step) { *step += 1u; }
+__global__ void k_step_set(uint32_t* step, uint32_t v) { *step = v; }
+
+static uint64_t fnv(uint64_t h, const void* data, size_t n) {
+  const unsigned char* c = static_cast<const unsigned char*>(data);
+  for (size_t i = 0; i < n; ++i) { h ^= c[i]; h *= 1099511628211ull; }
+  return h;
+}
+template <class T>
+static uint64_t fnv_v(uint64_t h, const T& v) { return fnv(h, &v, sizeof(T)); }
+
+// The step's parameters without the step number (which the captured kernels read from
+// step_dev).
+static uint64_t params_digest(const pb_step_params* p) {
+  pb_step_params q = *p;
+  q.iteration = 0;
+  return fnv(1469598103934665603ull, &q, sizeof(q));
+}
+
+// Everything of the simulator that a step's launches take as arguments: buffers, sizes,
+// settings and the host-side state (buffer parity, counts validity).  A cached graph is
+// replayed only while this is unchanged.
+static uint64_t state_signature(const pb_sim* h) {
+  const Sim* s = &h->s;
+  uint64_t k = 1469598103934665603ull;
+  for (int sp = 0; sp < 2; ++sp) {
+    const Species& S = s->sp[sp];
+    k = fnv_v(k, S.cur); k = fnv_v(k, S.cap);
+    for (int b = 0; b < 2; ++b) k = fnv_v(k, S.buf[b]);
+  }
+  const void* ptrs[] = {s->V, s->Vnew, s->Vfixed, s->Vdc, s->damage, s->eroded, s->accum_ppc, s->f, s->dirsum,
+                        s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->ecorn,
+                        s->isBound, s->cls, s->bdist, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->cidx, s->cinv,
+                        s->partials, s->bar, s->pstats, s->ptrace, s->counts, s->next_ids, s->tile_status,
+                        s->tile_counter, s->see_key, s->see_xy, s->see_count, s->angles, s->angle_scratch,
+                        s->angle_count, s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1],
+                        s->sval[0], s->sval[1], s->shist, s->sblk, s->rep_dev, h->cx.t, h->cx.c, h->see.t,
+                        h->see.c, s->step_dev};
+  k = fnv(k, ptrs, sizeof(ptrs));
+  for (const DevLevel& L : s->lev) k = fnv_v(k, L);
+  const long long vals[] = {s->ny, s->nx, s->periodic, s->ngrids, s->nc, s->trace_on, s->pgrid, s->ut[0], s->ut[1],
+                            s->pbps, (long long)s->kopts, (long long)s->psmem, (long long)s->tile_cap, s->see_cap,
+                            s->angle_cap, (long long)s->sort_cap, (long long)s->hist_cap, s->counts_valid ? 1 : 0,
+                            s->max_outer, s->max_inner, h->cx.nt, h->see.nt, s->profiling};
+  k = fnv(k, vals, sizeof(vals));
+  const double dv[] = {s->tol, s->tol_inner, h->cx.lo, h->cx.hi, h->cx.cmax, h->see.lo, h->see.hi};
+  k = fnv(k, dv, sizeof(dv));
+  k = fnv_v(k, s->seed);
+  return k;
+}
+
+static void free_graphs(Sim* s) {
+  for (auto& g : s->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  s->graphs.clear();
+}
+
+// A step that a graph can hold: no RF co-extraction (its grid voltage changes every step)
+// and no phase marks.
+static bool graph_eligible(const Sim* s, const pb_step_params* p) {
+  return s->graphs_on && !s->graphs_broken && !s->profiling && p->rf_grid < 0;
+}
+
+// One step through a graph: replay the graph of this shape, or capture it first.  Sets
+// *done = false (and leaves the host state as it was) when the step cannot be captured;
+// the caller then enqueues it as usual.
+static int32_t graph_step(pb_sim* h, const pb_step_params* p, bool* done) {
+  Sim* s = &h->s;
+  *done = false;
+  const uint64_t pkey = params_digest(p), skey = state_signature(h);
+  if ((long long)(uint32_t)p->iteration != s->step_dev_val) {
+    k_step_set<<<1, 1, 0, s->stream>>>(s->step_dev, (uint32_t)p->iteration);
+    CK(cudaGetLastError());
+  }
+  for (auto& g : s->graphs) {
+    if (g.pkey != pkey || g.skey != skey) continue;
+    CK(cudaGraphLaunch(g.exec, s->stream));
+    // the host-side effects of the step: buffer parity, counts, spacing of the sort keys
+    const int flips = 1 + (p->sort_now ? 1 : 0);
+    for (int sp = 0; sp < 2; ++sp) s->sp[sp].cur ^= (flips & 1);
+    s->counts_valid = true;
+    s->sp_dx = p->dx;
+    s->sp_dy = p->dy;
+    s->launches += g.launches;
+    s->step_dev_val = (long long)(uint32_t)p->iteration + 1;
+    ++s->graph_replays;
+    *done = true;
+    return PB_OK;
+  }
+  // capture: the step is enqueued into the graph, not run; the host state it advances is
+  // kept only when the capture succeeds
+  const int cur0 = s->sp[0].cur, cur1 = s->sp[1].cur;
+  const bool cv0 = s->counts_valid;
+  const double dx0 = s->sp_dx, dy0 = s->sp_dy;
+  const long long l0 = s->launches;
+  if (s->graphs.size() >= 8) free_graphs(s);
+  cudaError_t ce = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+  if (ce != cudaSuccess) {
+    s->graphs_broken = 1;
+    s->graph_error = std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(ce);
+    cudaGetLastError();
+    return PB_OK;
+  }
+  s->capturing = 1;
+  int32_t rc = enqueue_step(h, p);
+  if (rc == PB_OK) {
+    k_step_advance<<<1, 1, 0, s->stream>>>(s->step_dev);
+    if (cudaGetLastError() != cudaSuccess) rc = PB_ERR_CUDA;
+  }
+  s->capturing = 0;
+  cudaGraph_t graph = nullptr;
+  ce = cudaStreamEndCapture(s->stream, &graph);
+  cudaGraphExec_t exec = nullptr;
+  if (rc == PB_OK && ce == cudaSuccess && graph) ce = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (rc != PB_OK || ce != cudaSuccess || !exec) {
+    // not capturable here: restore the host state and let the caller enqueue the step
+    s->graphs_broken = 1;
+    s->graph_error = rc != PB_OK ? g_err : std::string("step capture: ") + cudaGetErrorString(ce);
+    cudaGetLastError();
+    s->sp[0].cur = cur0; s->sp[1].cur = cur1;
+    s->counts_valid = cv0; s->sp_dx = dx0; s->sp_dy = dy0; s->launches = l0;
+    return PB_OK;
+  }
+  Sim::StepGraph g;
+  g.pkey = pkey;
+  g.skey = skey;
+  g.exec = exec;
+  g.launches = s->launches - l0 + 1;
+  s->launches = l0 + g.launches;
+  s->graphs.push_back(g);
+  CK(cudaGraphLaunch(exec, s->stream));
+  s->step_dev_val = (long long)(uint32_t)p->iteration + 1;
+  ++s->graph_captures;
+  *done = true;
+  return PB_OK;
+}
+
+// one step of pb_sim_run / pb_sim_step: through a graph when enabled and possible
+static int32_t run_one_step(pb_sim* h, const pb_step_params* p) {
+  Sim* s = &h->s;
+  if (graph_eligible(s, p)) {
+    bool done = false;
+    if (int32_t rc = graph_step(h, p, &done)) return rc;
+    if (done) return PB_OK;
+  }
+  if (s->graphs_on) ++s->graph_plain_steps;
+  return enqueue_step(h, p);
 }
 
 static int32_t finish_report(Sim* s, pb_step_report* out) {
@@ -923,6 +1097,8 @@ int32_t pb_sim_create(pb_sim** out, int32_t device) {
   CK(dalloc(&s->angle_scratch, 2 * (size_t)s->angle_cap));
   CK(dalloc(&s->rep_dev, 1));
   CK(cudaMemset(s->rep_dev, 0, sizeof(pb_step_report)));
+  CK(dalloc(&s->step_dev, 1));
+  CK(cudaMemset(s->step_dev, 0, sizeof(uint32_t)));
   CK(cudaMallocHost((void**)&s->rep_host, sizeof(pb_step_report)));
   s->sp[0].ion = true;
   s->sp[1].ion = false;
@@ -939,6 +1115,8 @@ int32_t pb_sim_destroy(pb_sim* h) {
   Sim* s = &h->s;
   cudaSetDevice(s->device);
   cudaStreamSynchronize(s->stream);
+  free_graphs(s);
+  if (s->step_dev) cudaFree(s->step_dev);
   free_levels(s);
   double* d[] = {s->V, s->Vnew, s->Vfixed, s->Vdc, s->damage, s->eroded, s->accum_ppc, s->f, s->dirsum, s->partials, s->pstats};
   for (double* q : d) if (q) cudaFree(q);
@@ -977,6 +1155,27 @@ int32_t pb_sim_set_solver(pb_sim* h, double tol, double tol_inner, int32_t max_o
                             "coarse correction)");
   s->tol = tol; s->tol_inner = tol_inner; s->max_outer = max_outer; s->max_inner = max_inner; s->nu = nu;
   s->max_coarse = max_coarse;
+  return PB_OK;
+}
+
+int32_t pb_sim_set_graphs(pb_sim* h, int32_t on) {
+  Sim* s = &h->s;
+  CK(cudaStreamSynchronize(s->stream));
+  s->graphs_on = on ? 1 : 0;
+  s->graphs_broken = 0;
+  s->graph_error.clear();
+  free_graphs(s);
+  s->step_dev_val = -1;
+  return PB_OK;
+}
+
+int32_t pb_sim_graph_stats(pb_sim* h, int64_t* out4) {
+  const Sim* s = &h->s;
+  out4[0] = s->graph_captures;
+  out4[1] = s->graph_replays;
+  out4[2] = s->graph_plain_steps;
+  out4[3] = s->graphs_broken;
+  if (s->graphs_broken) g_err = s->graph_error;
   return PB_OK;
 }
 
@@ -1261,7 +1460,7 @@ int32_t pb_sim_step(pb_sim* h, const pb_step_params* p, pb_step_report* report) 
   s->mark_used = 0;
   s->launches = 0;
   CK(cudaEventRecord(s->ev0, s->stream));
-  if ((rc = enqueue_step(h, p))) return rc;
+  if ((rc = run_one_step(h, p))) return rc;
   CK(cudaEventRecord(s->ev1, s->stream));
   if (report) {
     if ((rc = finish_report(s, report))) return rc;
@@ -1292,7 +1491,7 @@ int32_t pb_sim_run(pb_sim* h, const pb_step_params* params, int32_t nsteps, pb_s
   s->launches = 0;
   CK(cudaEventRecord(s->ev0, s->stream));
   for (int k = 0; k < nsteps; ++k) {
-    if ((rc = enqueue_step(h, &params[k]))) return rc;
+    if ((rc = run_one_step(h, &params[k]))) return rc;
     if (reports) {
       CK(cudaMemcpyAsync(&s->rep_run[k], s->rep_dev, sizeof(pb_step_report), cudaMemcpyDeviceToHost, s->stream));
     }
