@@ -203,6 +203,10 @@ int32_t pb_sim_set_graphs(pb_sim* s, int32_t on);
  * if a capture failed (then pb_last_error() gives the reason). */
 int32_t pb_sim_graph_stats(pb_sim* s, int64_t* out4);
 int32_t pb_sim_get_kernel_options(pb_sim* s, uint32_t* flags);
+/* Particles per block of the ion and electron step kernels (their tile of staging,
+ * compaction and histograms): 1024 (default) or 512; an autotuner knob without a
+ * counterpart in the reference.  Results do not depend on it. */
+int32_t pb_sim_set_tile(pb_sim* s, int32_t particles_per_block);
 
 /* Upload the domain of build_domain (physics_engine.py:629-847): node masks, Dirichlet
  * values, electrode masks (bit g of gridmask = grid g), plus the state arrays to keep.

@@ -3,7 +3,8 @@
 PB_OPT_SMEM_HIST (deposit and PPC counts through shared-memory cell histograms per tile),
 PB_OPT_TMA_TILE (the ion step stages each tile's window of the E-corner array in shared
 memory with a TMA copy) and PB_OPT_ELE_PAIRS (two electrons per thread pushed side by
-side) change how the kernels move data and schedule work, not what they compute.
+side), and the tile of 512 instead of 1024 particles per block, change how the kernels move
+data and schedule work, not what they compute.
 Three steps of the 257 x 1025 case from the same state, with the particles re-sorted by
 cell every step (so that tiles are compact and the windows and histograms are used) and
 once without sorting (wide tiles take the fallback paths), must agree bit for bit in every
@@ -27,7 +28,7 @@ def PE():
     return physics_engine
 
 
-def _run(PE, flags, sort_every, steps=3):
+def _run(PE, flags, sort_every, steps=3, ppb=1024):
     from thruster_cx_code_b200 import _lib
     case = LARGE_CASES["large_aperture_3grid"]
     params = dict(case["params"], Thresh=1e9)
@@ -37,6 +38,7 @@ def _run(PE, flags, sort_every, steps=3):
     g.m_e = M_XE / case["m_e_ratio"]
     g.user_cs = cx_store(CX_POWER_LAW)
     _lib.check(g._libh.pb_sim_set_kernel_options(g._h, flags), "set_kernel_options")
+    _lib.check(g._libh.pb_sim_set_tile(g._h, ppb), "set_tile")
     g.build_domain(params)
     ions, cex, eles = large_case_particles(g.isBound, g.dx, g.dy, g.Lx, g.Ly, 60000, 20000, 5)
     g.set_particles("ions", *ions, is_cex=cex, ids=np.arange(ions.shape[1]), sort=sort_every > 0)
@@ -58,12 +60,13 @@ def test_kernel_variants_bit_identical(PE, sort_every):
     from thruster_cx_code_b200 import _lib
     ref = _run(PE, 0, sort_every)
     H, T, P = _lib.PB_OPT_SMEM_HIST, _lib.PB_OPT_TMA_TILE, _lib.PB_OPT_ELE_PAIRS
-    for flags in (H, T, H | T, P, H | P, H | T | P):
-        got = _run(PE, flags, sort_every)
+    cases = [(f, 1024) for f in (H, T, H | T, P, H | P, H | T | P)] + [(0, 512), (H | T | P, 512)]
+    for flags, ppb in cases:
+        got = _run(PE, flags, sort_every, ppb=ppb)
         for k in ("p", "e", "rho"):
-            np.testing.assert_array_equal(got[k].view(np.uint32), ref[k].view(np.uint32), err_msg=f"{flags} {k}")
+            np.testing.assert_array_equal(got[k].view(np.uint32), ref[k].view(np.uint32), err_msg=f"{flags} {ppb} {k}")
         for k in ("pid", "cex", "eid", "ppc", "V"):
-            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{flags} {k}")
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"{flags} {ppb} {k}")
         # damage adds float64 atomics in whatever order the blocks reach them
         np.testing.assert_allclose(got["damage"], ref["damage"], rtol=1e-12, atol=0)
 
@@ -72,4 +75,5 @@ def test_unknown_option_bits_rejected(PE):
     from thruster_cx_code_b200 import _lib
     g = PE.DigitalTwinSimulator()
     assert g._libh.pb_sim_set_kernel_options(g._h, 1 << 7) == 2
+    assert g._libh.pb_sim_set_tile(g._h, 768) == 2
     g.close()

@@ -12,6 +12,8 @@ best values depend on the grid size and the particle count:
   gathers against the cost of the sort).
 * ``particle_blocks_per_sm``: the grid of the ion and electron step kernels.
 * ``solve_blocks``: blocks of the field-solve launch ("all" SMs or "half").
+* ``particles_per_block``: the tile of the ion and electron step kernels (1024 or 512
+  particles staged, compacted and histogrammed per block).
 * ``kernel_options``: the step kernels' variants (``PB_OPT_*`` bits): shared-memory cell
   histograms for the deposit and PPC counts, the TMA-staged E-corner window of the ion
   step, and two electrons per thread pushed side by side.  Every combination computes the
@@ -48,6 +50,7 @@ KNOBS = {
     "particle_blocks_per_sm": (4, 8, 16),
     "solve_blocks": ("all", "half"),
     "kernel_options": (0, 1, 2, 3, 4, 5, 6, 7),
+    "particles_per_block": (1024, 512),
 }
 
 
@@ -58,7 +61,8 @@ def current(sim):
     _lib.check(_lib.load().pb_sim_get_kernel_options(sim._h, C.byref(opts)), "pb_sim_get_kernel_options")
     return {"max_coarse": int(s["max_coarse"]), "tol_inner": float(s["tol_inner"]),
             "sort_every": int(sim.sort_every), "particle_blocks_per_sm": int(getattr(sim, "_pbps", 8)),
-            "solve_blocks": getattr(sim, "_solve_blocks", "all"), "kernel_options": int(opts.value)}
+            "solve_blocks": getattr(sim, "_solve_blocks", "all"), "kernel_options": int(opts.value),
+            "particles_per_block": int(getattr(sim, "_ppb", 1024))}
 
 
 def _num_sms(sim):
@@ -84,6 +88,9 @@ def apply(sim, knobs):
         _lib.check(lib.pb_sim_rebuild_operator(sim._h), "rebuild_operator")
     if "sort_every" in knobs:
         sim.sort_every = int(knobs["sort_every"])
+    if "particles_per_block" in knobs:
+        _lib.check(lib.pb_sim_set_tile(sim._h, int(knobs["particles_per_block"])), "pb_sim_set_tile")
+        sim._ppb = int(knobs["particles_per_block"])
     if "kernel_options" in knobs:
         _lib.check(lib.pb_sim_set_kernel_options(sim._h, int(knobs["kernel_options"])), "pb_sim_set_kernel_options")
     if "particle_blocks_per_sm" in knobs or "solve_blocks" in knobs:

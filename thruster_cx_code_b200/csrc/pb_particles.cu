@@ -20,8 +20,9 @@
 namespace pb {
 
 constexpr int NT = 256;    // threads per block of the step kernels
-constexpr int IPT = 4;     // particles per thread (one float4 of each array)
-constexpr int TILE = NT * IPT;
+constexpr int IPT = 4;     // particles per thread of the default tile
+constexpr int TILE = NT * IPT;       // particles per block and tile (default)
+constexpr int TILE_MIN = NT * 2;     // the smaller tile of the particles-per-block knob
 constexpr long long SPIN_LIMIT = 1ll << 22;  // polls of a predecessor tile (~1-2 s) before giving up
 
 // ------------------------------------------------------------------ field gather + push
@@ -650,21 +651,23 @@ __device__ __forceinline__ int tile_compact_ranks(const uint8_t* keep, int* rank
 // Tile of TILE particles: item k of the tile is particle t0 + k; thread t handles
 // k = t, t + NT, ... (coalesced loads), results are staged in shared memory, ranked by a
 // block scan in index order and written compacted (stable) at the global offset.
+template <int TL>
 struct IonStage {
-  float x[TILE], y[TILE], vx[TILE], vy[TILE], vz[TILE];
-  uint32_t id[TILE];
-  int rank[TILE];          // deposit cells (PB_OPT_SMEM_HIST) until the compaction ranks them
-  uint8_t cex[TILE], keep[TILE];
+  float x[TL], y[TL], vx[TL], vy[TL], vz[TL];
+  uint32_t id[TL];
+  int rank[TL];            // deposit cells (PB_OPT_SMEM_HIST) until the compaction ranks them
+  uint8_t cex[TL], keep[TL];
 };
 
 // Four resident blocks of 256 per SM (64 registers, some spilled): latency hiding gains
 // more than the spills cost (12% faster than three blocks at 80 registers).
 // Lower-left start cell of a tile's particles (a rough floor of x / dx and y / dy, which
 // only places the staged window; every gather checks membership exactly), block-wide.
+template <int TL>
 __device__ __forceinline__ void tile_low_cell(const IonStepArgs& a, int t0, int n, int& xlo, int& ylo) {
   __shared__ int red[2 * (NT / 32)];
   int lx = INT_MAX, ly = INT_MAX;
-  for (int k = threadIdx.x; k < TILE; k += NT) {
+  for (int k = threadIdx.x; k < TL; k += NT) {
     const int i = t0 + k;
     if (i >= n) break;
     const float qx = __fmul_rn(a.src.x[i], a.inv_dx), qy = __fmul_rn(a.src.y[i], a.inv_dy);
@@ -688,16 +691,16 @@ __device__ __forceinline__ void tile_low_cell(const IonStepArgs& a, int t0, int 
 
 constexpr long long TMA_SPIN_LIMIT = 1ll << 22;  // polls of the window's mbarrier before giving up
 
-template <bool HAS_B, int OPT>
+template <bool HAS_B, int OPT, int TL>
 __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonStepArgs a) {
   constexpr bool HIST = (OPT & PB_OPT_SMEM_HIST) != 0;
   constexpr bool TMA = (OPT & PB_OPT_TMA_TILE) != 0 && !HAS_B;
   pdl_enter();
   const uint32_t stepk = a.step_dev ? *a.step_dev : a.step;  // Philox step key
-  __shared__ IonStage st;
+  __shared__ IonStage<TL> st;
   __shared__ int sm_tile;
   __shared__ int hbins[HIST ? HBINS : 1];
-  __shared__ int pcell[HIST ? TILE : 1];
+  __shared__ int pcell[HIST ? TL : 1];
   __shared__ __align__(128) float4 ebox[TMA ? 2 * TB_W * TB_H : 1];
   __shared__ __align__(8) uint64_t ebar;
   if (HIST)
@@ -724,14 +727,14 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
     if (threadIdx.x == 0) sm_tile = atomicAdd(a.tile_counter, 1);
     __syncthreads();
     const int tile = sm_tile;
-    const int t0 = tile * TILE;
+    const int t0 = tile * TL;
     if (t0 >= n) break;
     EBox eb{nullptr, 0, 0};
     if (TMA && tma_live) {
       // stage the window of E corners around the tile's particles (one TMA copy), one
       // cell of margin below and left of the lowest start cell
       int xlo, ylo;
-      tile_low_cell(a, t0, n, xlo, ylo);
+      tile_low_cell<TL>(a, t0, n, xlo, ylo);
       eb.bx = xlo - 1;
       eb.by = ylo - 1;
       if (threadIdx.x == 0) {
@@ -752,7 +755,7 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
       }
     }
 #pragma unroll 1
-    for (int k = threadIdx.x; k < TILE; k += NT) {
+    for (int k = threadIdx.x; k < TL; k += NT) {
       const int i = t0 + k;
       uint8_t kp = 0;
       int dep_cell = 0, ppc_cell = 0;
@@ -925,12 +928,12 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
     }
     __syncthreads();
     if (HIST) {
-      tile_hist<NT, TILE>(pcell, st.keep, a.ppc, hbins);
-      tile_hist<NT, TILE>(st.rank, st.keep, a.cnt, hbins);
+      tile_hist<NT, TL>(pcell, st.keep, a.ppc, hbins);
+      tile_hist<NT, TL>(st.rank, st.keep, a.cnt, hbins);
     }
     long long base;
-    tile_compact_ranks<NT, TILE>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
-    for (int k = threadIdx.x; k < TILE; k += NT) {
+    tile_compact_ranks<NT, TL>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
+    for (int k = threadIdx.x; k < TL; k += NT) {
       if (!st.keep[k]) continue;
       long long pos = base + st.rank[k];
       a.dst.x[pos] = st.x[k]; a.dst.y[pos] = st.y[k];
@@ -958,16 +961,18 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
 }
 
 // ------------------------------------------------------------------ fused electron step
+template <int TL>
 struct EleStage {
-  float x[TILE], y[TILE], vx[TILE], vy[TILE], vz[TILE];
-  uint32_t id[TILE];
-  int rank[TILE];
-  uint8_t keep[TILE];
+  float x[TL], y[TL], vx[TL], vy[TL], vz[TL];
+  uint32_t id[TL];
+  int rank[TL];
+  uint8_t keep[TL];
 };
 
 // The end of one electron's step after its pushes: periodic wrap, purge test and the
 // next step's deposit cell; the survivor is staged in shared memory at tile slot k.
-__device__ __forceinline__ void ele_finish(const EleStepArgs& a, EleStage& st, int k, int i, float x, float y,
+template <int TL>
+__device__ __forceinline__ void ele_finish(const EleStepArgs& a, EleStage<TL>& st, int k, int i, float x, float y,
                                            float vx, float vy, float vz, uint8_t& kp, int& dep_cell) {
   if (a.periodic) y = np_modf_pos(y, a.Lyf);
   int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1), icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
@@ -980,12 +985,12 @@ __device__ __forceinline__ void ele_finish(const EleStepArgs& a, EleStage& st, i
   st.id[k] = a.src.id[i];
 }
 
-template <bool HAS_B, int OPT>
+template <bool HAS_B, int OPT, int TL>
 __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
   constexpr bool HIST = (OPT & PB_OPT_SMEM_HIST) != 0;
   constexpr bool PAIRS = (OPT & PB_OPT_ELE_PAIRS) != 0 && !HAS_B;
   pdl_enter();
-  __shared__ EleStage st;
+  __shared__ EleStage<TL> st;
   __shared__ int sm_tile;
   __shared__ int hbins[HIST ? HBINS : 1];
   if (HIST)
@@ -1000,12 +1005,12 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
     if (threadIdx.x == 0) sm_tile = atomicAdd(a.tile_counter, 1);
     __syncthreads();
     const int tile = sm_tile;
-    const int t0 = tile * TILE;
+    const int t0 = tile * TL;
     if (t0 >= n) break;
     if (PAIRS) {
-      // items k and k + NT of a thread pushed side by side (TILE = 4 NT: two pairs)
+      // items k and k + NT of a thread pushed side by side (TL = 2 NT or 4 NT: one or two pairs)
 #pragma unroll 1
-      for (int k = threadIdx.x; k < TILE; k += 2 * NT) {
+      for (int k = threadIdx.x; k < TL; k += 2 * NT) {
         float x[2], y[2], vx[2], vy[2], vz[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -1028,7 +1033,7 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
       }
     } else {
 #pragma unroll 1
-      for (int k = threadIdx.x; k < TILE; k += NT) {
+      for (int k = threadIdx.x; k < TL; k += NT) {
         const int i = t0 + k;
         uint8_t kp = 0;
         int dep_cell = 0;
@@ -1045,10 +1050,10 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
       }
     }
     __syncthreads();
-    if (HIST) tile_hist<NT, TILE>(st.rank, st.keep, a.cnt, hbins);
+    if (HIST) tile_hist<NT, TL>(st.rank, st.keep, a.cnt, hbins);
     long long base;
-    tile_compact_ranks<NT, TILE>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
-    for (int k = threadIdx.x; k < TILE; k += NT) {
+    tile_compact_ranks<NT, TL>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
+    for (int k = threadIdx.x; k < TL; k += NT) {
       if (!st.keep[k]) continue;
       long long pos = base + st.rank[k];
       a.dst.x[pos] = st.x[k]; a.dst.y[pos] = st.y[k];

@@ -95,6 +95,7 @@ struct Sim {
   int ut_key[3] = {0, 0, 0}, ut[2] = {1, 1};  // fine up-leg tiling for (ny, nx, blocks)
   int pbps = 8;       // step-kernel blocks per SM (the grid; tiles are handed out by a counter)
   uint32_t kopts = PB_OPT_SMEM_HIST;  // kernel variants of the step (PB_OPT_*)
+  int ppb = TILE;                     // particles per block (tile) of the step kernels
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
   // particles
   Species sp[2];
@@ -264,7 +265,7 @@ static int32_t alloc_species(Sim* s, int k, int cap, int keep_n) {
   }
   S.cap = cap;
   // per-step scratch sized by the largest species
-  size_t tiles = (size_t)std::max(s->sp[0].cap, s->sp[1].cap) / TILE + 2;
+  size_t tiles = (size_t)std::max(s->sp[0].cap, s->sp[1].cap) / TILE_MIN + 2;
   if (tiles > s->tile_cap) {
     dfree(s->tile_status);
     CK(dalloc(&s->tile_status, 2 * tiles));
@@ -634,6 +635,26 @@ static int32_t check_step_params(const Sim* s, const pb_step_params* p) {
   return PB_OK;
 }
 
+// the step kernels' variant for the option bits and tile size
+template <int TL>
+static cudaError_t launch_ion(uint32_t kopts, dim3 g, cudaStream_t st, const IonStepArgs& a) {
+  switch (kopts & (PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE)) {
+    case 0: return launch_pdl(k_ion_step<false, 0, TL>, g, NT, 0, st, a);
+    case PB_OPT_SMEM_HIST: return launch_pdl(k_ion_step<false, PB_OPT_SMEM_HIST, TL>, g, NT, 0, st, a);
+    case PB_OPT_TMA_TILE: return launch_pdl(k_ion_step<false, PB_OPT_TMA_TILE, TL>, g, NT, 0, st, a);
+    default: return launch_pdl(k_ion_step<false, PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE, TL>, g, NT, 0, st, a);
+  }
+}
+template <int TL>
+static cudaError_t launch_ele(uint32_t kopts, dim3 g, cudaStream_t st, const EleStepArgs& b) {
+  switch (kopts & (PB_OPT_SMEM_HIST | PB_OPT_ELE_PAIRS)) {
+    case 0: return launch_pdl(k_ele_step<false, 0, TL>, g, NT, 0, st, b);
+    case PB_OPT_SMEM_HIST: return launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST, TL>, g, NT, 0, st, b);
+    case PB_OPT_ELE_PAIRS: return launch_pdl(k_ele_step<false, PB_OPT_ELE_PAIRS, TL>, g, NT, 0, st, b);
+    default: return launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST | PB_OPT_ELE_PAIRS, TL>, g, NT, 0, st, b);
+  }
+}
+
 static int32_t enqueue_step_pre(pb_sim* h, const pb_step_params* p) {
   Sim* s = &h->s;
   if (int32_t rc = check_step_params(s, p)) return rc;
@@ -785,17 +806,12 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   a.ppc = s->ppc; a.cnt = s->cnt_i;
   a.tile_status = s->tile_status; a.tile_counter = s->tile_counter; a.errflags = ef;
   {
-    const dim3 g(grid_for(s, I.cap, TILE, s->pbps));
+    const dim3 g(grid_for(s, I.cap, s->ppb, s->pbps));
     if (s->kopts & PB_OPT_TMA_TILE) {
       if ((rc = ensure_ec_map(s))) return rc;
       a.ec_map = s->ec_map;
     }
-    switch (s->kopts & (PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE)) {
-      case 0: CK(launch_pdl(k_ion_step<false, 0>, g, NT, 0, st, a)); break;
-      case PB_OPT_SMEM_HIST: CK(launch_pdl(k_ion_step<false, PB_OPT_SMEM_HIST>, g, NT, 0, st, a)); break;
-      case PB_OPT_TMA_TILE: CK(launch_pdl(k_ion_step<false, PB_OPT_TMA_TILE>, g, NT, 0, st, a)); break;
-      default: CK(launch_pdl(k_ion_step<false, PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE>, g, NT, 0, st, a)); break;
-    }
+    CK(s->ppb == TILE_MIN ? launch_ion<TILE_MIN>(s->kopts, g, st, a) : launch_ion<TILE>(s->kopts, g, st, a));
   }
   ++s->launches;
   mark(s);
@@ -821,13 +837,8 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
   b.errflags = ef;
   {
-    const dim3 g(grid_for(s, E.cap, TILE, s->pbps));
-    switch (s->kopts & (PB_OPT_SMEM_HIST | PB_OPT_ELE_PAIRS)) {
-      case 0: CK(launch_pdl(k_ele_step<false, 0>, g, NT, 0, st, b)); break;
-      case PB_OPT_SMEM_HIST: CK(launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST>, g, NT, 0, st, b)); break;
-      case PB_OPT_ELE_PAIRS: CK(launch_pdl(k_ele_step<false, PB_OPT_ELE_PAIRS>, g, NT, 0, st, b)); break;
-      default: CK(launch_pdl(k_ele_step<false, PB_OPT_SMEM_HIST | PB_OPT_ELE_PAIRS>, g, NT, 0, st, b)); break;
-    }
+    const dim3 g(grid_for(s, E.cap, s->ppb, s->pbps));
+    CK(s->ppb == TILE_MIN ? launch_ele<TILE_MIN>(s->kopts, g, st, b) : launch_ele<TILE>(s->kopts, g, st, b));
   }
   ++s->launches;
   mark(s);
@@ -933,7 +944,7 @@ static uint64_t state_signature(const pb_sim* h) {
   k = fnv(k, ptrs, sizeof(ptrs));
   for (const DevLevel& L : s->lev) k = fnv_v(k, L);
   const long long vals[] = {s->ny, s->nx, s->periodic, s->ngrids, s->nc, s->trace_on, s->pgrid, s->ut[0], s->ut[1],
-                            s->pbps, (long long)s->kopts, (long long)s->psmem, (long long)s->tile_cap, s->see_cap,
+                            s->pbps, s->ppb, (long long)s->kopts, (long long)s->psmem, (long long)s->tile_cap, s->see_cap,
                             s->angle_cap, (long long)s->sort_cap, (long long)s->hist_cap, s->counts_valid ? 1 : 0,
                             s->max_outer, s->max_inner, h->cx.nt, h->see.nt, s->profiling};
   k = fnv(k, vals, sizeof(vals));
@@ -1176,6 +1187,14 @@ int32_t pb_sim_graph_stats(pb_sim* h, int64_t* out4) {
   out4[2] = s->graph_plain_steps;
   out4[3] = s->graphs_broken;
   if (s->graphs_broken) g_err = s->graph_error;
+  return PB_OK;
+}
+
+int32_t pb_sim_set_tile(pb_sim* h, int32_t particles_per_block) {
+  if (particles_per_block != TILE && particles_per_block != TILE_MIN)
+    return fail(PB_ERR_ARG, "pb_sim_set_tile: particles per block must be " + std::to_string(TILE_MIN) + " or " +
+                                std::to_string(TILE));
+  h->s.ppb = particles_per_block;
   return PB_OK;
 }
 
