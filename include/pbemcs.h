@@ -167,8 +167,9 @@ int32_t pb_sim_destroy(pb_sim* s);
 int32_t pb_sim_set_seed(pb_sim* s, uint64_t seed);
 
 /* Field solver controls: FP64 relative residual target, FP32 reduction per refinement pass
- * (default 1e-3), loop caps, smoothing sweeps per level (1: the fused cycle smooths once on
- * each side of a coarse correction; other values are rejected) and the largest coarsest-level
+ * (default 1e-3), loop caps, damped-Jacobi sweeps on the fine level on each side of the
+ * coarse correction (nu = 1, fused into the transfers, or 2: one more grid-wide phase on each
+ * side; the cycle stays symmetric; other values are rejected) and the largest coarsest-level
  * size (4 to 4096 active nodes; default 1536; that level is solved with a dense inverse).
  * A new max_coarse takes effect at the next pb_sim_set_domain / pb_sim_rebuild_operator.
  * Stands in for the reference's fixed SuperLU factorisation (physics_engine.py:603-608). */

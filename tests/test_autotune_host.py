@@ -51,5 +51,5 @@ def test_second_pass_uses_new_incumbent():
 
 def test_knob_space_matches_the_library():
     assert set(A.KNOBS) == {"max_coarse", "tol_inner", "sort_every", "particle_blocks_per_sm", "solve_blocks",
-                            "kernel_options", "particles_per_block"}
+                            "kernel_options", "particles_per_block", "smoother_sweeps"}
     assert max(A.KNOBS["max_coarse"]) <= 4096 and min(A.KNOBS["max_coarse"]) >= 4

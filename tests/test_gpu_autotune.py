@@ -4,7 +4,7 @@
   three steps is bit-identical per id.
 * Half the SMs for the field solve changes only the rounding of its block-order sums:
   phi within 1e-6 of max|phi| (the bar for independent field solves).
-* Out-of-range launch shapes and nu != 1 are rejected.
+* Out-of-range launch shapes and smoother counts other than 1 or 2 are rejected.
 * A tuning run over two knobs applies and caches the best setting, and the tuned simulator
   keeps stepping.
 * With a short horizon the multigrid build time counts, and a small coarsest level wins.
@@ -63,7 +63,7 @@ def test_launch_knobs(mods):
     assert lib.pb_sim_set_launch(a._h, 0, 8) != 0
     assert lib.pb_sim_set_launch(a._h, 8, 100000) != 0
     s = a.solver
-    assert lib.pb_sim_set_solver(a._h, s["tol"], s["tol_inner"], s["max_outer"], s["max_inner"], 2,
+    assert lib.pb_sim_set_solver(a._h, s["tol"], s["tol_inner"], s["max_outer"], s["max_inner"], 3,
                                  s["max_coarse"]) != 0
     for sim in (a, b, c):
         sim.close()

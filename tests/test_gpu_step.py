@@ -78,12 +78,15 @@ def _eles(sim):
     return a, np.asarray(sim.e_id[:n]).astype(np.int64)
 
 
+@pytest.mark.parametrize("nu", [1, 2])
 @pytest.mark.parametrize("name", ["c1_half", "one_hole", "two_holes", "bulk"])
-def test_picard_potential_matches_superlu(gpu_mod, name):
+def test_picard_potential_matches_superlu(gpu_mod, name, nu):
+    """nu: damped-Jacobi sweeps on the fine level on each side of the coarse correction
+    (the autotuner's smoother knob); the solve meets the same tolerance either way."""
     f = load(f"domain_{name}.npz")
     case = json.loads(str(f["case"]))
     params = json.loads(str(f["params"]))
-    g = gpu_mod.DigitalTwinSimulator()
+    g = gpu_mod.DigitalTwinSimulator(solver={"nu": nu})
     g.dx, g.dy, g.dt = case["dx"], case["dy"], case["dt"]
     g.build_domain(params)
     assert (g.ny, g.nx) == f["V"].shape

@@ -8,6 +8,9 @@ best values depend on the grid size and the particle count:
   Fewer levels mean fewer grid-wide phases per PCG iteration; a larger coarsest level
   costs host set-up time and a larger dense product.
 * ``tol_inner``: the FP32 reduction per refinement pass of the field solve.
+* ``smoother_sweeps``: damped-Jacobi sweeps on the fine multigrid level on each side of the
+  coarse correction (1 or 2): a second sweep costs two grid-wide phases per PCG iteration
+  and may save iterations.
 * ``sort_every``: steps between cell sorts of the particles (L1 locality of the field
   gathers against the cost of the sort).
 * ``particle_blocks_per_sm``: the grid of the ion and electron step kernels.
@@ -51,6 +54,7 @@ KNOBS = {
     "solve_blocks": ("all", "half"),
     "kernel_options": (0, 1, 2, 3, 4, 5, 6, 7),
     "particles_per_block": (1024, 512),
+    "smoother_sweeps": (1, 2),
 }
 
 
@@ -59,7 +63,7 @@ def current(sim):
     s = sim.solver
     opts = C.c_uint32()
     _lib.check(_lib.load().pb_sim_get_kernel_options(sim._h, C.byref(opts)), "pb_sim_get_kernel_options")
-    return {"max_coarse": int(s["max_coarse"]), "tol_inner": float(s["tol_inner"]),
+    return {"max_coarse": int(s["max_coarse"]), "tol_inner": float(s["tol_inner"]), "smoother_sweeps": int(s["nu"]),
             "sort_every": int(sim.sort_every), "particle_blocks_per_sm": int(getattr(sim, "_pbps", 8)),
             "solve_blocks": getattr(sim, "_solve_blocks", "all"), "kernel_options": int(opts.value),
             "particles_per_block": int(getattr(sim, "_ppb", 1024))}
@@ -81,6 +85,7 @@ def apply(sim, knobs):
     rebuild = "max_coarse" in knobs and int(knobs["max_coarse"]) != int(s["max_coarse"])
     s["max_coarse"] = int(knobs.get("max_coarse", s["max_coarse"]))
     s["tol_inner"] = float(knobs.get("tol_inner", s["tol_inner"]))
+    s["nu"] = int(knobs.get("smoother_sweeps", s["nu"]))
     _lib.check(lib.pb_sim_set_solver(sim._h, s["tol"], s["tol_inner"], s["max_outer"], s["max_inner"], s["nu"],
                                      s["max_coarse"]), "pb_sim_set_solver")
     sim.solver = s

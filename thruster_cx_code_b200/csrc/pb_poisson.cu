@@ -255,8 +255,12 @@ __device__ __forceinline__ float prolong(const MgLevel& C, const float* zc, int 
 // m is used by the five stars that contain it), then z from the tile.  The tiles are
 // a.ut_y x a.ut_x nearly equal rectangles, dealt to the blocks in turn; each holds at most
 // UP_TILE_MAX nodes with its halo.
+// With nu0 = 2 the pre-smoothed correction is d (r + s), s = r - A d r (a.s32), and this leg
+// writes the once post-smoothed m2 to a.m32; smooth0 applies the second post-sweep.
 __device__ double up_leg0_tiled(const PoissonArgs& a, const float* r0) {
   __shared__ float mt[UP_TILE_MAX];
+  const bool two = a.nu0 == 2;
+  float* out = two ? a.m32 : a.lev[0].z;
   const MgLevel& F = a.lev[0];
   const MgLevel& C = a.lev[1];
   const int ny = F.ny, nx = F.nx, nty = a.ut_y, ntx = a.ut_x;
@@ -274,8 +278,9 @@ __device__ double up_leg0_tiled(const PoissonArgs& a, const float* r0) {
       const bool ok = yy >= 0 && yy < ny && xx >= 0 && xx < nx;
       const int j = ok ? yy * nx + xx : 0;
       const float d = __ldg(F.dinv + j), rj = *(r0 + j);
+      const float sj = two ? *(a.s32 + j) : 0.0f;
       const float pz = prolong(C, C.z, ok ? yy : 0, ok ? xx : 0);
-      mt[k] = (ok && d > 0.0f) ? d * rj + pz : 0.0f;
+      mt[k] = (ok && d > 0.0f) ? d * (rj + sj) + pz : 0.0f;
     }
     __syncthreads();
     for (int k = threadIdx.x; k < h * w; k += blockDim.x) {
@@ -285,10 +290,52 @@ __device__ double up_leg0_tiled(const PoissonArgs& a, const float* r0) {
       const float* mc = mt + (ly + 1) * w2 + (lx + 1);
       const float acc = ri + ((mc[-1] + mc[1]) + (mc[-w2] + mc[w2]));
       const float z = di > 0.0f ? W_KEEP * mc[0] + di * acc : 0.0f;
-      __stcg(F.z + i, z);
-      rz += (double)ri * (double)z;
+      __stcg(out + i, z);
+      if (!two) rz += (double)ri * (double)z;
     }
     __syncthreads();
+  }
+  return rz;
+}
+
+// Second fine-level pre-sweep (nu0 = 2): s = r - A (d r) on the free nodes, i.e.
+// s_i = (1 - w) r_i + sum_{k nbr of i} d_k r_k (d is zero off the free nodes).
+__device__ void presmooth0(const PoissonArgs& a, const float* r, float* s_out, int tid, int nth) {
+  const MgLevel& F = a.lev[0];
+  const int N = F.ny * F.nx;
+  for (int i = tid; i < N; i += nth) {
+    const int y = i / F.nx, x = i - y * F.nx;
+    int j[4];
+    nbrs0(a, i, y, x, j);
+    const float di = __ldg(F.dinv + i), ri = *(r + i);
+    float acc = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int jj = j[k] >= 0 ? j[k] : i;
+      const float dk = j[k] >= 0 ? __ldg(F.dinv + jj) : 0.0f;
+      acc += dk * *(r + jj);
+    }
+    __stcg(s_out + i, di > 0.0f ? W_KEEP * ri + acc : 0.0f);
+  }
+}
+
+// Second fine-level post-sweep (nu0 = 2): z = m + d (r - A m) = (1 - w) m + d (r + sum_nbr m)
+// from m = a.m32 (zero off the active nodes); returns the partial of (r, z).
+__device__ double smooth0(const PoissonArgs& a, const float* r, int tid, int nth) {
+  const MgLevel& F = a.lev[0];
+  const int N = F.ny * F.nx;
+  double rz = 0.0;
+  for (int i = tid; i < N; i += nth) {
+    const int y = i / F.nx, x = i - y * F.nx;
+    int j[4];
+    nbrs0(a, i, y, x, j);
+    const float di = __ldg(F.dinv + i), ri = *(r + i), mi = *(a.m32 + i);
+    float sm = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sm += j[k] >= 0 ? *(a.m32 + j[k]) : 0.0f;
+    const float z = di > 0.0f ? W_KEEP * mi + di * (ri + sm) : 0.0f;
+    __stcg(F.z + i, z);
+    rz += (double)ri * (double)z;
   }
   return rz;
 }
@@ -348,14 +395,15 @@ __device__ __forceinline__ float smooth_up_pre(const MgLevel& F, const MgLevel& 
 
 // grid-wide down leg: r_{l+1} from level l (all from global memory)
 template <bool LV0>
-__device__ void down_leg(const PoissonArgs& a, int level, int tid, int nth) {
+__device__ void down_leg(const PoissonArgs& a, int level, int tid, int nth, const float* src0 = nullptr) {
   const MgLevel& F = a.lev[level];
   const MgLevel& C = a.lev[level + 1];
   const int Nc = C.ny * C.nx;
   for (int ic = tid; ic < Nc; ic += nth) {
     const int I = ic / C.nx, J = ic - I * C.nx;
     if (LV0) {
-      const float s = restrict0(F, F.r, I, J, C.wrapP != 0);
+      // level 0 restricts (1 - w) v + sum_nbr d v of v = r (one pre-sweep) or v = s (two)
+      const float s = restrict0(F, src0 ? src0 : F.r, I, J, C.wrapP != 0);
       __stcg(C.r + ic, __ldg(C.dinv + ic) > 0.0f ? s : 0.0f);
     } else {
       __stcg(C.r + ic, restrict_pre(F, C, F.r, I, J, ic));
@@ -442,6 +490,10 @@ __device__ void vcycle_below(const PoissonArgs& a, float* rcs, int slot, const f
     tmark(a, 8 + (l < 7 ? l : 6));
   }
   rz = up_leg<true>(a, 0, tid, nth, r0);
+  if (a.nu0 == 2) {
+    grid_barrier(a);
+    rz = smooth0(a, r0, tid, nth);
+  }
   put_partials(a, slot, rz, 0.0);
   grid_barrier(a);
   tmark(a, 8);
@@ -505,8 +557,13 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
       double rz_old = 0.0, rr0 = rnorm2, dummy;
       for (int k = 0; k < a.max_inner; ++k) {
         n_inner += 1;
-        // z32 = M r32: fine-level restriction, then the rest of the V-cycle
-        if (a.nlevels > 1) down_leg<true>(a, 0, tid, nth);
+        // z32 = M r32: fine-level restriction (after a second pre-sweep when nu0 = 2),
+        // then the rest of the V-cycle
+        if (a.nlevels > 1 && a.nu0 == 2) {
+          presmooth0(a, a.r32, a.s32, tid, nth);
+          grid_barrier(a);
+        }
+        if (a.nlevels > 1) down_leg<true>(a, 0, tid, nth, a.nu0 == 2 ? a.s32 : nullptr);
         grid_barrier(a);
         tmark(a, 0);
         vcycle_below(a, rcs, slot, a.r32);  // (r, z) partial in slot, barrier

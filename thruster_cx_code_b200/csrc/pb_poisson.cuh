@@ -33,6 +33,8 @@ struct PoissonArgs {
   double* f;              // reduced right-hand side
   double* dirsum;         // sum of Dirichlet neighbour values
   float *r32, *z32, *p32, *q32, *e32;
+  float *s32, *m32;       // fine-level smoothing temporaries (nu0 = 2)
+  int nu0;                // damped-Jacobi sweeps on the fine level on each side of the coarse correction
   float *Ex, *Ey;
   // physics scalars (host double precision, as the reference computes them)
   double coeff;           // (dx*1e-3)^2 / eps0

@@ -73,6 +73,7 @@ struct Sim {
   double *accum_ppc = nullptr, *f = nullptr, *dirsum = nullptr;
   float *Ex = nullptr, *Ey = nullptr, *rho = nullptr, *Tmap = nullptr;
   float *r32 = nullptr, *z32 = nullptr, *p32 = nullptr, *q32 = nullptr, *e32 = nullptr;
+  float *s32 = nullptr, *m32 = nullptr;  // fine-level smoothing temporaries (nu = 2)
   float4* ecorn = nullptr;  // per-cell corners of Ex and Ey, 2 x float4 per node
   CUtensorMap ec_map;       // TMA view of ecorn (PB_OPT_TMA_TILE), valid for the array and shape below
   const float4* ec_map_for = nullptr;
@@ -400,6 +401,7 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
   a.ny = s->ny; a.nx = s->nx; a.periodic = s->periodic;
   a.cls = s->cls; a.Vfixed = s->Vfixed; a.rho = s->rho; a.V = s->V; a.x = s->Vnew; a.f = s->f; a.dirsum = s->dirsum;
   a.r32 = s->r32; a.z32 = s->z32; a.p32 = s->p32; a.q32 = s->q32; a.e32 = s->e32;
+  a.s32 = s->s32; a.m32 = s->m32; a.nu0 = s->nu;
   a.Ex = s->Ex; a.Ey = s->Ey;
   a.coeff = p->coeff; a.qn0_neg = p->qn0_neg; a.V_plasma = p->V_plasma; a.Te_up = p->Te_up;
   a.omega_keep = p->omega_keep; a.omega_new = p->omega_new;
@@ -934,7 +936,8 @@ static uint64_t state_signature(const pb_sim* h) {
     for (int b = 0; b < 2; ++b) k = fnv_v(k, S.buf[b]);
   }
   const void* ptrs[] = {s->V, s->Vnew, s->Vfixed, s->Vdc, s->damage, s->eroded, s->accum_ppc, s->f, s->dirsum,
-                        s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->ecorn,
+                        s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->s32, s->m32,
+                        s->ecorn,
                         s->isBound, s->cls, s->bdist, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->cidx, s->cinv,
                         s->partials, s->bar, s->pstats, s->ptrace, s->counts, s->next_ids, s->tile_status,
                         s->tile_counter, s->see_key, s->see_xy, s->see_count, s->angles, s->angle_scratch,
@@ -946,7 +949,7 @@ static uint64_t state_signature(const pb_sim* h) {
   const long long vals[] = {s->ny, s->nx, s->periodic, s->ngrids, s->nc, s->trace_on, s->pgrid, s->ut[0], s->ut[1],
                             s->pbps, s->ppb, (long long)s->kopts, (long long)s->psmem, (long long)s->tile_cap, s->see_cap,
                             s->angle_cap, (long long)s->sort_cap, (long long)s->hist_cap, s->counts_valid ? 1 : 0,
-                            s->max_outer, s->max_inner, h->cx.nt, h->see.nt, s->profiling};
+                            s->max_outer, s->max_inner, s->nu, h->cx.nt, h->see.nt, s->profiling};
   k = fnv(k, vals, sizeof(vals));
   const double dv[] = {s->tol, s->tol_inner, h->cx.lo, h->cx.hi, h->cx.cmax, h->see.lo, h->see.hi};
   k = fnv(k, dv, sizeof(dv));
@@ -1131,7 +1134,8 @@ int32_t pb_sim_destroy(pb_sim* h) {
   free_levels(s);
   double* d[] = {s->V, s->Vnew, s->Vfixed, s->Vdc, s->damage, s->eroded, s->accum_ppc, s->f, s->dirsum, s->partials, s->pstats};
   for (double* q : d) if (q) cudaFree(q);
-  float* fl[] = {s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->see_xy, s->angles};
+  float* fl[] = {s->Ex, s->Ey, s->rho, s->Tmap, s->r32, s->z32, s->p32, s->q32, s->e32, s->s32, s->m32,
+                 s->see_xy, s->angles};
   for (float* q : fl) if (q) cudaFree(q);
   if (s->ecorn) cudaFree(s->ecorn);
   void* v[] = {s->isBound, s->bdist, s->bdist_tmp, s->cls, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->bar, s->counts, s->next_ids,
@@ -1161,9 +1165,9 @@ int32_t pb_sim_set_solver(pb_sim* h, double tol, double tol_inner, int32_t max_o
   Sim* s = &h->s;
   if (!(tol > 0) || !(tol_inner > 0) || max_outer < 1 || max_inner < 1 || max_coarse < 4 || max_coarse > MG_MAX_COARSE)
     return fail(PB_ERR_ARG, "pb_sim_set_solver: invalid value");
-  if (nu != 1)
-    return fail(PB_ERR_ARG, "pb_sim_set_solver: nu must be 1 (the fused cycle smooths once on each side of a "
-                            "coarse correction)");
+  if (nu != 1 && nu != 2)
+    return fail(PB_ERR_ARG, "pb_sim_set_solver: nu must be 1 or 2 (damped-Jacobi sweeps on the fine level on "
+                            "each side of the coarse correction)");
   s->tol = tol; s->tol_inner = tol_inner; s->max_outer = max_outer; s->max_inner = max_inner; s->nu = nu;
   s->max_coarse = max_coarse;
   return PB_OK;
@@ -1255,7 +1259,8 @@ int32_t pb_sim_set_domain(pb_sim* h, int32_t ny, int32_t nx, int32_t periodic, c
     if (keep_state && s->domain_set) return fail(PB_ERR_ARG, "pb_sim_set_domain: keep_state with a new grid size");
     double** dd[] = {&s->V, &s->Vnew, &s->Vfixed, &s->Vdc, &s->damage, &s->eroded, &s->accum_ppc, &s->f, &s->dirsum};
     for (double** q : dd) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(double))); }
-    float** ff[] = {&s->Ex, &s->Ey, &s->rho, &s->Tmap, &s->r32, &s->z32, &s->p32, &s->q32, &s->e32};
+    float** ff[] = {&s->Ex, &s->Ey, &s->rho, &s->Tmap, &s->r32, &s->z32, &s->p32, &s->q32, &s->e32, &s->s32,
+                    &s->m32};
     for (float** q : ff) { dfree(*q); CK(dalloc(q, N)); CK(cudaMemset(*q, 0, N * sizeof(float))); }
     dfree(s->ecorn); CK(dalloc(&s->ecorn, 2 * N)); CK(cudaMemset(s->ecorn, 0, 2 * N * sizeof(float4)));
     dfree(s->isBound); CK(dalloc(&s->isBound, N));
