@@ -188,8 +188,10 @@ int32_t pb_sim_set_launch(pb_sim* s, int32_t particle_blocks_per_sm, int32_t sol
  *   PB_OPT_TMA_TILE   the ion step stages each tile's window of the E-corner array in
  *                     shared memory with a TMA tensor copy before pushing
  *   PB_OPT_ELE_PAIRS  the electron step pushes two particles per thread side by side, so
- *                     that one particle's field loads overlap the other's arithmetic */
-enum { PB_OPT_SMEM_HIST = 1 << 0, PB_OPT_TMA_TILE = 1 << 1, PB_OPT_ELE_PAIRS = 1 << 2 };
+ *                     that one particle's field loads overlap the other's arithmetic
+ *   PB_OPT_ELE_SPLIT  the electron step runs as a barrier-free push kernel followed by a
+ *                     separate stable compaction (overrides the other electron variants) */
+enum { PB_OPT_SMEM_HIST = 1 << 0, PB_OPT_TMA_TILE = 1 << 1, PB_OPT_ELE_PAIRS = 1 << 2, PB_OPT_ELE_SPLIT = 1 << 3 };
 int32_t pb_sim_set_kernel_options(pb_sim* s, uint32_t flags);
 /* CUDA graphs of whole steps in pb_sim_run and pb_sim_step (no counterpart in the
  * reference): with on != 0 each step shape (its parameters apart from the step number,
@@ -315,8 +317,10 @@ int32_t pb_batch_destroy(pb_batch* b);
  * after the last step has completed. */
 int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_params* params, int32_t K,
                      pb_step_report* reports);
-/* out2[0] = device time (ms) of the last pb_batch_run, out2[1] = kernel launches in it. */
-int32_t pb_batch_timing(pb_batch* b, double* out2);
+/* out3[0] = device time (ms) of the last pb_batch_run, out3[1] = kernel launches in it,
+ * out3[2] = host time (ms) from its first enqueue to its last (when this approaches the
+ * device time, the run is bound by launch overhead). */
+int32_t pb_batch_timing(pb_batch* b, double* out3);
 /* Device memory held by a simulator (bytes, estimated from its capacities). */
 int32_t pb_sim_memory(pb_sim* s, int64_t* bytes);
 

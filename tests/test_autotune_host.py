@@ -51,5 +51,15 @@ def test_second_pass_uses_new_incumbent():
 
 def test_knob_space_matches_the_library():
     assert set(A.KNOBS) == {"max_coarse", "tol_inner", "sort_every", "particle_blocks_per_sm", "solve_blocks",
-                            "kernel_options", "particles_per_block", "smoother_sweeps"}
+                            "deposit_hist", "ion_tma_window", "electron_kernel", "particles_per_block",
+                            "smoother_sweeps"}
     assert max(A.KNOBS["max_coarse"]) <= 4096 and min(A.KNOBS["max_coarse"]) >= 4
+
+
+def test_kernel_variant_knobs_round_trip():
+    from thruster_cx_code_b200 import _lib
+    for bits in (0, _lib.PB_OPT_SMEM_HIST, _lib.PB_OPT_TMA_TILE | _lib.PB_OPT_ELE_PAIRS,
+                 _lib.PB_OPT_SMEM_HIST | _lib.PB_OPT_ELE_SPLIT):
+        assert A.options_bits(A.options_knobs(bits)) == bits
+    assert A.options_bits({"electron_kernel": "split"}, _lib.PB_OPT_SMEM_HIST) == \
+        _lib.PB_OPT_SMEM_HIST | _lib.PB_OPT_ELE_SPLIT

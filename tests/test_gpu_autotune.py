@@ -69,16 +69,19 @@ def test_launch_knobs(mods):
         sim.close()
 
 
-def test_kernel_options_knob(mods):
-    """The kernel-variant knob applies and reads back, and a tuning run over it picks one
-    of its values; particle state does not depend on it."""
+def test_kernel_variant_knobs(mods):
+    """The kernel-variant knobs apply and read back, and a tuning run over them picks a
+    setting; particle state does not depend on them."""
     _lib, A = mods
     sp = _spec()
     a, pa = W.make_sweep_sim(sp)
     b, pb = W.make_sweep_sim(sp)
-    A.apply(a, {"kernel_options": 0})
-    A.apply(b, {"kernel_options": _lib.PB_OPT_SMEM_HIST | _lib.PB_OPT_TMA_TILE})
-    assert A.current(a)["kernel_options"] == 0 and A.current(b)["kernel_options"] == 3
+    A.apply(a, {"deposit_hist": False, "ion_tma_window": False, "electron_kernel": "fused"})
+    A.apply(b, {"deposit_hist": True, "ion_tma_window": True, "electron_kernel": "split",
+                "particles_per_block": 512, "smoother_sweeps": 2})
+    cb = A.current(b)
+    assert cb["deposit_hist"] and cb["ion_tma_window"] and cb["electron_kernel"] == "split"
+    assert cb["particles_per_block"] == 512 and cb["smoother_sweeps"] == 2
     for _ in range(3):
         a.step(pa)
         b.step(pb)
@@ -86,9 +89,10 @@ def test_kernel_options_knob(mods):
     ib, sb = _ions_by_id(b)
     np.testing.assert_array_equal(ia, ib)
     np.testing.assert_array_equal(sa, sb)
-    tuner = A.Autotuner(steps=2, warmup=1, space={"kernel_options": (0, 1, 2, 3)})
+    tuner = A.Autotuner(steps=2, warmup=1, space={"electron_kernel": ("fused", "pairs", "split"),
+                                                  "deposit_hist": (False, True)})
     best, table = tuner.tune(a, pa)
-    assert best["kernel_options"] in (0, 1, 2, 3) and len(table) == 4
+    assert best["electron_kernel"] in ("fused", "pairs", "split") and 3 <= len(table) <= 4
     a.close()
     b.close()
 

@@ -2,8 +2,9 @@
 
 PB_OPT_SMEM_HIST (deposit and PPC counts through shared-memory cell histograms per tile),
 PB_OPT_TMA_TILE (the ion step stages each tile's window of the E-corner array in shared
-memory with a TMA copy) and PB_OPT_ELE_PAIRS (two electrons per thread pushed side by
-side), and the tile of 512 instead of 1024 particles per block, change how the kernels move
+memory with a TMA copy), PB_OPT_ELE_PAIRS (two electrons per thread pushed side by
+side), PB_OPT_ELE_SPLIT (the electron step as a barrier-free push and a separate
+compaction), and the tile of 512 instead of 1024 particles per block, change how the kernels move
 data and schedule work, not what they compute.
 Three steps of the 257 x 1025 case from the same state, with the particles re-sorted by
 cell every step (so that tiles are compact and the windows and histograms are used) and
@@ -59,8 +60,8 @@ def _run(PE, flags, sort_every, steps=3, ppb=1024):
 def test_kernel_variants_bit_identical(PE, sort_every):
     from thruster_cx_code_b200 import _lib
     ref = _run(PE, 0, sort_every)
-    H, T, P = _lib.PB_OPT_SMEM_HIST, _lib.PB_OPT_TMA_TILE, _lib.PB_OPT_ELE_PAIRS
-    cases = [(f, 1024) for f in (H, T, H | T, P, H | P, H | T | P)] + [(0, 512), (H | T | P, 512)]
+    H, T, P, S = _lib.PB_OPT_SMEM_HIST, _lib.PB_OPT_TMA_TILE, _lib.PB_OPT_ELE_PAIRS, _lib.PB_OPT_ELE_SPLIT
+    cases = [(f, 1024) for f in (H, T, H | T, P, H | P, H | T | P, S, H | T | S)] + [(0, 512), (H | T | P, 512)]
     for flags, ppb in cases:
         got = _run(PE, flags, sort_every, ppb=ppb)
         for k in ("p", "e", "rho"):
@@ -74,6 +75,6 @@ def test_kernel_variants_bit_identical(PE, sort_every):
 def test_unknown_option_bits_rejected(PE):
     from thruster_cx_code_b200 import _lib
     g = PE.DigitalTwinSimulator()
-    assert g._libh.pb_sim_set_kernel_options(g._h, 1 << 7) == 2
+    assert g._libh.pb_sim_set_kernel_options(g._h, 1 << 9) == 2
     assert g._libh.pb_sim_set_tile(g._h, 768) == 2
     g.close()

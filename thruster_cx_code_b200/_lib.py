@@ -142,6 +142,7 @@ def load():
 PB_OPT_SMEM_HIST = 1 << 0
 PB_OPT_TMA_TILE = 1 << 1
 PB_OPT_ELE_PAIRS = 1 << 2
+PB_OPT_ELE_SPLIT = 1 << 3
 
 ERRORS = {1: "CUDA error", 2: "invalid argument", 3: "capacity", 4: "device wait timed out",
           5: "field solve did not converge", 6: "call out of order"}

@@ -17,10 +17,11 @@ best values depend on the grid size and the particle count:
 * ``solve_blocks``: blocks of the field-solve launch ("all" SMs or "half").
 * ``particles_per_block``: the tile of the ion and electron step kernels (1024 or 512
   particles staged, compacted and histogrammed per block).
-* ``kernel_options``: the step kernels' variants (``PB_OPT_*`` bits): shared-memory cell
-  histograms for the deposit and PPC counts, the TMA-staged E-corner window of the ion
-  step, and two electrons per thread pushed side by side.  Every combination computes the
-  same bits.
+* ``deposit_hist``, ``ion_tma_window``, ``electron_kernel``: the step kernels' variants
+  (``PB_OPT_*`` bits): shared-memory cell histograms for the deposit and PPC counts, the
+  TMA-staged E-corner window of the ion step, and the electron step fused, with two
+  electrons per thread side by side, or split into a barrier-free push and a separate
+  compaction.  Every combination computes the same bits.
 
 Particle results are identical for every value of these knobs except ``sort_every``,
 which changes only the array order.  The field solve reaches the same FP64 tolerance
@@ -52,7 +53,9 @@ KNOBS = {
     "sort_every": (10, 20, 40),
     "particle_blocks_per_sm": (4, 8, 16),
     "solve_blocks": ("all", "half"),
-    "kernel_options": (0, 1, 2, 3, 4, 5, 6, 7),
+    "deposit_hist": (False, True),
+    "ion_tma_window": (False, True),
+    "electron_kernel": ("fused", "pairs", "split"),
     "particles_per_block": (1024, 512),
     "smoother_sweeps": (1, 2),
 }
@@ -65,8 +68,24 @@ def current(sim):
     _lib.check(_lib.load().pb_sim_get_kernel_options(sim._h, C.byref(opts)), "pb_sim_get_kernel_options")
     return {"max_coarse": int(s["max_coarse"]), "tol_inner": float(s["tol_inner"]), "smoother_sweeps": int(s["nu"]),
             "sort_every": int(sim.sort_every), "particle_blocks_per_sm": int(getattr(sim, "_pbps", 8)),
-            "solve_blocks": getattr(sim, "_solve_blocks", "all"), "kernel_options": int(opts.value),
-            "particles_per_block": int(getattr(sim, "_ppb", 1024))}
+            "solve_blocks": getattr(sim, "_solve_blocks", "all"),
+            "particles_per_block": int(getattr(sim, "_ppb", 1024)), **options_knobs(int(opts.value))}
+
+
+def options_knobs(bits):
+    """The kernel-variant knobs of PB_OPT_* bits."""
+    ele = "split" if bits & _lib.PB_OPT_ELE_SPLIT else ("pairs" if bits & _lib.PB_OPT_ELE_PAIRS else "fused")
+    return {"deposit_hist": bool(bits & _lib.PB_OPT_SMEM_HIST), "ion_tma_window": bool(bits & _lib.PB_OPT_TMA_TILE),
+            "electron_kernel": ele}
+
+
+def options_bits(knobs, base=0):
+    """PB_OPT_* bits from the kernel-variant knobs present in ``knobs`` (others from ``base``)."""
+    cur = options_knobs(base)
+    cur.update({k: knobs[k] for k in cur if k in knobs})
+    bits = (_lib.PB_OPT_SMEM_HIST if cur["deposit_hist"] else 0) | (_lib.PB_OPT_TMA_TILE if cur["ion_tma_window"] else 0)
+    bits |= {"fused": 0, "pairs": _lib.PB_OPT_ELE_PAIRS, "split": _lib.PB_OPT_ELE_SPLIT}[cur["electron_kernel"]]
+    return bits
 
 
 def _num_sms(sim):
@@ -96,8 +115,11 @@ def apply(sim, knobs):
     if "particles_per_block" in knobs:
         _lib.check(lib.pb_sim_set_tile(sim._h, int(knobs["particles_per_block"])), "pb_sim_set_tile")
         sim._ppb = int(knobs["particles_per_block"])
-    if "kernel_options" in knobs:
-        _lib.check(lib.pb_sim_set_kernel_options(sim._h, int(knobs["kernel_options"])), "pb_sim_set_kernel_options")
+    if any(k in knobs for k in ("deposit_hist", "ion_tma_window", "electron_kernel")):
+        opts = C.c_uint32()
+        _lib.check(lib.pb_sim_get_kernel_options(sim._h, C.byref(opts)), "pb_sim_get_kernel_options")
+        _lib.check(lib.pb_sim_set_kernel_options(sim._h, options_bits(knobs, int(opts.value))),
+                   "pb_sim_set_kernel_options")
     if "particle_blocks_per_sm" in knobs or "solve_blocks" in knobs:
         pbps = int(knobs.get("particle_blocks_per_sm", getattr(sim, "_pbps", 8)))
         sb = knobs.get("solve_blocks", getattr(sim, "_solve_blocks", "all"))

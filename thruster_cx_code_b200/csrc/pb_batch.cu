@@ -24,6 +24,7 @@ struct pb_batch {
   std::vector<cudaEvent_t> ev_inst;  // per instance: "pre-solve half enqueued" / "stream done"
   std::vector<cudaEvent_t> ev_solve; // per launch of a step
   double last_ms = 0.0;
+  double last_host_ms = 0.0;   // host time spent enqueuing the last run (ev0 to the last enqueue)
   long long launches = 0;
 };
 
@@ -235,6 +236,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     for (int k = 0; k < K; ++k)
       if ((rc = check_step_params(&sims[i]->s, &params[(size_t)i * K + k]))) return rc;
   // ---- enqueue
+  const auto t_enq0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(b->ev0, b->stream));
   if (nargs > 0) {
     CK(cudaMemcpyAsync(b->dargs, b->hargs, nargs * sizeof(PoissonArgs), cudaMemcpyHostToDevice, b->stream));
@@ -288,6 +290,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     CK(cudaStreamWaitEvent(b->stream, b->ev_inst[i], 0));
   }
   CK(cudaEventRecord(b->ev1, b->stream));
+  b->last_host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_enq0).count();
   CK(cudaEventSynchronize(b->ev1));
   float ms = 0.0f;
   CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
@@ -310,6 +313,7 @@ int32_t pb_batch_timing(pb_batch* b, double* out2) {
   if (!b || !out2) return fail(PB_ERR_ARG, "pb_batch_timing");
   out2[0] = b->last_ms;
   out2[1] = (double)b->launches;
+  out2[2] = b->last_host_ms;
   return PB_OK;
 }
 

@@ -1064,4 +1064,87 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
   }
 }
 
+// ------------------------------------------------------------------ split electron step
+// PB_OPT_ELE_SPLIT: the electron step as two kernels.  k_ele_push advances every electron
+// independently (no shared-memory staging, no block barriers), writes it back in place and
+// records whether it survives; k_ele_compact then moves the survivors to the other buffer
+// in order (the same single-pass look-back as the fused kernel).  The push is compute-bound
+// at many sub-steps per electron, so the extra pass over the state costs less than the
+// barriers it removes.  Same operations, same bits as k_ele_step.
+__global__ void __launch_bounds__(NT, 6) k_ele_push(EleStepArgs a, uint8_t* __restrict__ keep) {
+  pdl_enter();
+  const int n = *a.num_src;
+  const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
+  const double dt_sub = DDIV(a.dt, (double)n_sub);
+  const double h = DMUL(DMUL(0.5, a.qm), dt_sub);
+  const float dtf = __double2float_rn(dt_sub);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.n_sub_out = n_sub;
+  const int stride = gridDim.x * blockDim.x;
+  // trip count uniform across a warp (the deposit count is a warp-wide vote)
+  const int n_pad = (n + 31) & ~31;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
+    int dep_cell = 0;
+    bool kp = false;
+    if (i < n) {
+      float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
+      for (int s = 0; s < n_sub; ++s)
+        boris_push_one<false, true, true>(x, y, vx, vy, vz, a.Ex, a.Ey, nullptr, nullptr, nullptr, a.nx, a.ny, a.dxf,
+                                          a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy);
+      if (a.periodic) y = np_modf_pos(y, a.Lyf);
+      const int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1);
+      const int icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
+      bool dead = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
+      dead = dead || (x < 0.0f) || (x > a.Lxf) || (y < 0.0f) || (y > a.Lyf) || (x != x);
+      kp = !dead;
+      if (kp)
+        dep_cell = cell_round32_f(y, a.dyf, a.inv_dy, 1, a.ny - 2) * a.nx +
+                   cell_round32_f(x, a.dxf, a.inv_dx, 1, a.nx - 2);
+      a.src.x[i] = x; a.src.y[i] = y; a.src.vx[i] = vx; a.src.vy[i] = vy; a.src.vz[i] = vz;
+      keep[i] = kp ? 1 : 0;
+    }
+    warp_count_add(a.cnt, dep_cell, kp);
+  }
+}
+
+struct EleCompactStage {
+  float x[TILE], y[TILE], vx[TILE], vy[TILE], vz[TILE];
+  uint32_t id[TILE];
+  int rank[TILE];
+  uint8_t keep[TILE];
+};
+
+__global__ void __launch_bounds__(NT) k_ele_compact(EleStepArgs a, const uint8_t* __restrict__ keep) {
+  pdl_enter();
+  __shared__ EleCompactStage st;
+  __shared__ int sm_tile;
+  const int n = *a.num_src;
+  while (true) {
+    if (threadIdx.x == 0) sm_tile = atomicAdd(a.tile_counter, 1);
+    __syncthreads();
+    const int tile = sm_tile;
+    const int t0 = tile * TILE;
+    if (t0 >= n) break;
+    for (int k = threadIdx.x; k < TILE; k += NT) {
+      const int i = t0 + k;
+      const uint8_t kp = i < n ? keep[i] : 0;
+      st.keep[k] = kp;
+      if (kp) {
+        st.x[k] = a.src.x[i]; st.y[k] = a.src.y[i]; st.vx[k] = a.src.vx[i]; st.vy[k] = a.src.vy[i];
+        st.vz[k] = a.src.vz[i]; st.id[k] = a.src.id[i];
+      }
+    }
+    __syncthreads();
+    long long base;
+    tile_compact_ranks<NT, TILE>(st.keep, st.rank, tile, t0, n, a.tile_status, a.num_dst, base, a.errflags);
+    for (int k = threadIdx.x; k < TILE; k += NT) {
+      if (!st.keep[k]) continue;
+      const long long pos = base + st.rank[k];
+      a.dst.x[pos] = st.x[k]; a.dst.y[pos] = st.y[k];
+      a.dst.vx[pos] = st.vx[k]; a.dst.vy[pos] = st.vy[k]; a.dst.vz[pos] = st.vz[k];
+      a.dst.id[pos] = st.id[k];
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace pb

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -95,7 +96,7 @@ struct Sim {
   int pgrid = 0;      // blocks of the field-solve launch (<= num_sms)
   int ut_key[3] = {0, 0, 0}, ut[2] = {1, 1};  // fine up-leg tiling for (ny, nx, blocks)
   int pbps = 8;       // step-kernel blocks per SM (the grid; tiles are handed out by a counter)
-  uint32_t kopts = PB_OPT_SMEM_HIST;  // kernel variants of the step (PB_OPT_*)
+  uint32_t kopts = 0;                 // kernel variants of the step (PB_OPT_*; the plain ones measured fastest)
   int ppb = TILE;                     // particles per block (tile) of the step kernels
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
   // particles
@@ -116,6 +117,8 @@ struct Sim {
   int* angle_count = nullptr;
   unsigned long long* ds_bits = nullptr;  // [ion, ele]
   int* n_sub = nullptr;                    // [ion, ele]
+  uint8_t* ekeep = nullptr;                // survivor flags of the split electron step
+  size_t ekeep_cap = 0;
   int* inj = nullptr;                      // 7 ints
   int* see_spawned = nullptr;
   // sort
@@ -271,6 +274,11 @@ static int32_t alloc_species(Sim* s, int k, int cap, int keep_n) {
     dfree(s->tile_status);
     CK(dalloc(&s->tile_status, 2 * tiles));
     s->tile_cap = tiles;
+  }
+  if ((size_t)s->sp[1].cap > s->ekeep_cap) {
+    dfree(s->ekeep);
+    CK(dalloc(&s->ekeep, (size_t)s->sp[1].cap));
+    s->ekeep_cap = (size_t)s->sp[1].cap;
   }
   size_t scap = (size_t)std::max(s->sp[0].cap, s->sp[1].cap);
   if (scap > s->sort_cap) {
@@ -838,7 +846,11 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
   b.errflags = ef;
-  {
+  if (s->kopts & PB_OPT_ELE_SPLIT) {
+    CK(launch_pdl(k_ele_push, grid_for(s, E.cap, NT, s->pbps), NT, 0, st, b, s->ekeep));
+    CK(launch_pdl(k_ele_compact, grid_for(s, E.cap, TILE, s->pbps), NT, 0, st, b, (const uint8_t*)s->ekeep));
+    ++s->launches;
+  } else {
     const dim3 g(grid_for(s, E.cap, s->ppb, s->pbps));
     CK(s->ppb == TILE_MIN ? launch_ele<TILE_MIN>(s->kopts, g, st, b) : launch_ele<TILE>(s->kopts, g, st, b));
   }
@@ -943,7 +955,7 @@ static uint64_t state_signature(const pb_sim* h) {
                         s->tile_counter, s->see_key, s->see_xy, s->see_count, s->angles, s->angle_scratch,
                         s->angle_count, s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1],
                         s->sval[0], s->sval[1], s->shist, s->sblk, s->rep_dev, h->cx.t, h->cx.c, h->see.t,
-                        h->see.c, s->step_dev};
+                        h->see.c, s->step_dev, s->ekeep};
   k = fnv(k, ptrs, sizeof(ptrs));
   for (const DevLevel& L : s->lev) k = fnv_v(k, L);
   const long long vals[] = {s->ny, s->nx, s->periodic, s->ngrids, s->nc, s->trace_on, s->pgrid, s->ut[0], s->ut[1],
@@ -1131,6 +1143,7 @@ int32_t pb_sim_destroy(pb_sim* h) {
   cudaStreamSynchronize(s->stream);
   free_graphs(s);
   if (s->step_dev) cudaFree(s->step_dev);
+  if (s->ekeep) cudaFree(s->ekeep);
   free_levels(s);
   double* d[] = {s->V, s->Vnew, s->Vfixed, s->Vdc, s->damage, s->eroded, s->accum_ppc, s->f, s->dirsum, s->partials, s->pstats};
   for (double* q : d) if (q) cudaFree(q);
@@ -1203,7 +1216,7 @@ int32_t pb_sim_set_tile(pb_sim* h, int32_t particles_per_block) {
 }
 
 int32_t pb_sim_set_kernel_options(pb_sim* h, uint32_t flags) {
-  if (flags & ~(uint32_t)(PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE | PB_OPT_ELE_PAIRS))
+  if (flags & ~(uint32_t)(PB_OPT_SMEM_HIST | PB_OPT_TMA_TILE | PB_OPT_ELE_PAIRS | PB_OPT_ELE_SPLIT))
     return fail(PB_ERR_ARG, "pb_sim_set_kernel_options: unknown flag bits " + std::to_string(flags));
   h->s.kopts = flags;
   return PB_OK;

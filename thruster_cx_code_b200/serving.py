@@ -39,6 +39,7 @@ class SweepBatch:
         self.device = int(device)
         self.last_ms = 0.0
         self.last_launches = 0
+        self.last_host_ms = 0.0
 
     def close(self):
         if self._h is not None and self._h.value:
@@ -71,9 +72,9 @@ class SweepBatch:
         R = (_lib.StepReport * (n * K))()
         arr = (C.c_void_p * n)(*[s._h.value for s in sims])
         _lib.check(self._libh.pb_batch_run(self._h, arr, n, P, int(K), R), "pb_batch_run")
-        t = (C.c_double * 2)()
+        t = (C.c_double * 3)()
         self._libh.pb_batch_timing(self._h, t)
-        self.last_ms, self.last_launches = float(t[0]), int(t[1])
+        self.last_ms, self.last_launches, self.last_host_ms = float(t[0]), int(t[1]), float(t[2])
         out = []
         for i, (s, prm) in enumerate(zip(sims, params_list)):
             res = []
