@@ -137,8 +137,9 @@ typedef struct pb_step_params {
   int32_t saddle_idx[8];
   /* options without a reference counterpart (params 'neutral_profile', 'sputter_exponent'):
    * neutral_uniform = 1 takes the CEX neutral density as n0_uniform everywhere instead of
-   * the point-source profile of physics_engine.py:1696-1706; sputter_exp != 1 uses the
-   * yield Y_coeff (E - E_th)^sputter_exp in float64 instead of the linear law of :1432 */
+   * the point-source profile of physics_engine.py:1696-1706; sputter_exp other than 0 or 1
+   * uses the yield Y_coeff (E - E_th)^sputter_exp in float64 instead of the linear law of
+   * :1432 (a zero-filled struct keeps the reference's physics) */
   int32_t neutral_uniform;
   double n0_uniform;
   double sputter_exp;

@@ -96,7 +96,7 @@ struct Sim {
   int pgrid = 0;      // blocks of the field-solve launch (<= num_sms)
   int ut_key[3] = {0, 0, 0}, ut[2] = {1, 1};  // fine up-leg tiling for (ny, nx, blocks)
   int pbps = 8;       // step-kernel blocks per SM (the grid; tiles are handed out by a counter)
-  uint32_t kopts = 0;                 // kernel variants of the step (PB_OPT_*; the plain ones measured fastest)
+  uint32_t kopts = PB_OPT_ELE_SPLIT;  // kernel variants of the step (PB_OPT_*; the fastest measured)
   int ppb = TILE;                     // particles per block (tile) of the step kernels
   size_t psmem = 0;  // dynamic shared memory of the field-solve kernel
   // particles
@@ -795,7 +795,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   a.Tmap = s->Tmap; a.damage = s->damage;
   a.k_half_m = (float)p->half_m_ion; a.mw_f = (float)p->macro_w; a.ccell_f = (float)p->C_cell;
   a.accel_f = (float)p->thermal_accel; a.q_f = (float)p->q; a.Y_f = (float)p->Y_coeff; a.Eth_f = (float)p->E_th;
-  a.Y_d = p->Y_coeff; a.mw_d = p->macro_w; a.Y_exp = p->sputter_exp;
+  a.Y_d = p->Y_coeff; a.mw_d = p->macro_w; a.Y_exp = p->sputter_exp == 0.0 ? 1.0 : p->sputter_exp;
   a.dt_f = dtf;
   a.see_spline = spline_of(h->see);
   a.see_key = s->see_key; a.see_xy = s->see_xy; a.see_count = s->see_count; a.see_cap = s->see_cap;
