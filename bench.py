@@ -467,9 +467,11 @@ def sweep_section(device, args):
     3e16-3e17 m^-3, grids drawn from {64x256, 128x512, 256x1024} cells and 0.2M-4M
     macro-particles log-uniform.  Plain: each point alone through pb_sim_run (3 warm-up
     steps, then 40 timed).  Batched: all points together through pb_batch_run, from the
-    state the plain steps left (3 warm-up steps, then 40 timed).  Rates use device time,
-    scaled to 3000 steps per point; setup is excluded.  The particle-pushes of both halves
-    are reported, so their workloads can be compared.  Then the C4 served run."""
+    state the plain steps left (3 warm-up steps, then 40 timed), first with every member's
+    kernels enqueued on its own stream, then with each batch step shape captured as one CUDA
+    graph and replayed (the warm-up steps capture).  Rates use device time, scaled to 3000
+    steps per point; setup is excluded.  The particle-pushes of each part are reported, so
+    their workloads can be compared.  Then the C4 served run."""
     from thruster_cx_code_b200 import serving as SV
     from thruster_cx_code_b200 import workloads as W
     rng = np.random.default_rng(7)
@@ -483,13 +485,24 @@ def sweep_section(device, args):
         _run_plain(s, p, SWEEP_WARMUP)
     plain_pushes = []
     plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes) for s, p in built)
+    def batched(graphs):
+        batch.set_graphs(graphs)
+        batch.run(sims, prm, SWEEP_WARMUP)
+        n0 = [(s.num_p, s.num_e) for s in sims]
+        res = batch.run(sims, prm, SWEEP_STEPS)
+        pushes = sum(SV.pushes_of([rep for _, rep in r], a, b) for r, (a, b) in zip(res, n0))
+        return batch.last_ms, batch.last_host_ms, pushes
+
     batch = SV.SweepBatch(device)
-    batch.run(sims, prm, SWEEP_WARMUP)
-    n0 = [(s.num_p, s.num_e) for s in sims]
-    res = batch.run(sims, prm, SWEEP_STEPS)
-    batched_ms = batch.last_ms
-    batched_host_ms = batch.last_host_ms
-    batched_pushes = sum(SV.pushes_of([rep for _, rep in r], a, b) for r, (a, b) in zip(res, n0))
+    streams_ms, streams_host_ms, streams_pushes = batched(False)
+    graph_ms, graph_host_ms, graph_pushes = batched(True)
+    g_stats = batch.graph_stats()
+    # the batched form: CUDA graphs of whole batch steps when they captured, else the streams
+    if not g_stats[2]:
+        batched_ms, batched_host_ms, batched_pushes = graph_ms, graph_host_ms, graph_pushes
+    else:
+        batched_ms, batched_host_ms, batched_pushes = streams_ms, streams_host_ms, streams_pushes
+    batch.set_graphs(False)
     for s in sims:
         s.close()
     per_point_plain_s = plain_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts
@@ -503,6 +516,11 @@ def sweep_section(device, args):
            "batched_points_per_hr": 3600.0 / per_point_batched_s,
            "batched_over_plain": plain_ms / batched_ms,
            "batched_device_ms": batched_ms, "batched_host_enqueue_ms": batched_host_ms,
+           "batched_form": "graphs" if not g_stats[2] else "streams",
+           "graph_captures_replays_failed": list(g_stats),
+           "streams": {"points_per_hr": 3600.0 / (streams_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts),
+                       "device_ms": streams_ms, "host_enqueue_ms": streams_host_ms,
+                       "over_plain": plain_ms / streams_ms},
            "setup": f"excluded ({t_setup:.1f} s of host geometry, multigrid build and pre-load on 8 threads)"}
     for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms),
                              ("batched", float(batched_pushes), batched_ms)):

@@ -318,6 +318,16 @@ int32_t pb_batch_destroy(pb_batch* b);
  * after the last step has completed. */
 int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_params* params, int32_t K,
                      pb_step_report* reports);
+/* CUDA graphs of whole batch steps (no counterpart in the reference): with on != 0 each
+ * step shape of the set (every member's step parameters apart from the step number, and
+ * the state its launches take) is captured once, with every member's work on the graph's
+ * branches and the shared field solve between them, and replayed; the host then issues one
+ * launch per step instead of one per kernel and member.  Results are the same bits as
+ * without graphs.  Steps that cannot be captured are enqueued as usual (and graphs stay
+ * off for the batch until re-enabled; see pb_batch_graph_stats). */
+int32_t pb_batch_set_graphs(pb_batch* b, int32_t on);
+/* out3: captures, replays, 1 if a capture failed (pb_last_error() gives the reason). */
+int32_t pb_batch_graph_stats(pb_batch* b, int64_t* out3);
 /* out3[0] = device time (ms) of the last pb_batch_run, out3[1] = kernel launches in it,
  * out3[2] = host time (ms) from its first enqueue to its last (when this approaches the
  * device time, the run is bound by launch overhead). */

@@ -88,3 +88,31 @@ def test_point_in_a_mix_matches_alone(mods):
     for m in mix:
         m[0].close()
     alone.close()
+
+
+def test_batch_graphs_bit_identical(mods):
+    """pb_batch_set_graphs: every batch step shape of a three-member mix captured once and
+    replayed gives the same bits as enqueueing each kernel, over 25 steps (a sort step and
+    alternating field-solve steps included)."""
+    specs = [_spec("64x256", 120000, 5), _spec("128x512", 200000, 6), _spec("64x256", 80000, 7)]
+    plain = [W.make_sweep_sim(sp) for sp in specs]
+    graph = [W.make_sweep_sim(sp) for sp in specs]
+    b0, b1 = mods.SweepBatch(), mods.SweepBatch(graphs=True)
+    r0 = b0.run([m[0] for m in plain], [m[1] for m in plain], 25)
+    r1 = b1.run([m[0] for m in graph], [m[1] for m in graph], 25)
+    captures, replays, broken = b1.graph_stats()
+    assert not broken and captures >= 2 and replays >= 15, (captures, replays, broken)
+    for ra, rb in zip(r0, r1):
+        assert [bytes(rep) for _, rep in ra] == [bytes(rep) for _, rep in rb]
+    for (a, _), (g, _) in zip(plain, graph):
+        for x, y in zip(_state(a), _state(g)):
+            np.testing.assert_array_equal(np.asarray(x).view(np.uint32) if x.dtype == np.float32 else x,
+                                          np.asarray(y).view(np.uint32) if y.dtype == np.float32 else y)
+        np.testing.assert_array_equal(a.V, g.V)
+    # a second run of the same set replays the graphs it has
+    b1.run([m[0] for m in graph], [m[1] for m in graph], 4)
+    assert b1.graph_stats()[1] > replays
+    for m in plain + graph:
+        m[0].close()
+    b0.close()
+    b1.close()

@@ -26,6 +26,26 @@ struct pb_batch {
   double last_ms = 0.0;
   double last_host_ms = 0.0;   // host time spent enqueuing the last run (ev0 to the last enqueue)
   long long launches = 0;
+  // CUDA graphs of whole batch steps (pb_batch_set_graphs): one graph per step shape of the
+  // set (each member's step parameters without the step number and its state signature)
+  int graphs_on = 0, graphs_broken = 0;
+  std::string graph_error;
+  struct StepGraph {
+    uint64_t key = 0;
+    cudaGraphExec_t exec = nullptr;
+    PoissonArgs* dargs = nullptr;     // the step's field-solve argument blocks, owned by the graph
+    int* dblk = nullptr;
+    pb_step_report** dreps = nullptr; // the members' report buffers, gathered at the end of the step
+    std::vector<long long> launches;  // kernels of each member in the step
+    long long own_launches = 0;       // the step's field solves and report gather
+  };
+  std::vector<StepGraph> graphs;
+  pb_step_report* ring = nullptr;     // reports of a run, [step][member]
+  pb_step_report* hring = nullptr;
+  size_t ring_cap = 0;
+  int* slot = nullptr;                // next ring row
+  cudaEvent_t ev_fork = nullptr;
+  long long graph_captures = 0, graph_replays = 0;
 };
 
 namespace {
@@ -89,6 +109,27 @@ int64_t sim_device_bytes(const Sim* s) {
   return b;
 }
 
+__global__ void k_batch_reports(pb_step_report* const* src, int n, pb_step_report* ring, int* slot) {
+  const int row = *slot;
+  constexpr int W = (int)(sizeof(pb_step_report) / 4);
+  for (int t = threadIdx.x; t < n * W; t += blockDim.x) {
+    const int i = t / W, w = t - i * W;
+    reinterpret_cast<uint32_t*>(ring + (size_t)row * n + i)[w] = reinterpret_cast<const uint32_t*>(src[i])[w];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *slot = row + 1;
+}
+
+void free_batch_graphs(pb_batch* b) {
+  for (auto& g : b->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.dargs) cudaFree(g.dargs);
+    if (g.dblk) cudaFree(g.dblk);
+    if (g.dreps) cudaFree(g.dreps);
+  }
+  b->graphs.clear();
+}
+
 template <class T>
 int32_t grow_pinned(T** p, size_t* cap, size_t need) {
   if (need <= *cap) return PB_OK;
@@ -102,6 +143,187 @@ int32_t grow_pinned(T** p, size_t* cap, size_t need) {
 
 }  // namespace
 
+// ------------------------------------------------------------------ batch steps as graphs
+// One step of every member: fork from the batch stream, the pre-solve halves on the members'
+// streams, the step's cooperative field-solve launches on the batch stream, the post-solve
+// halves, then the members' report buffers gathered into row `slot` of the ring.  Enqueued
+// into a graph while the members are in capture mode (the Philox step keys then come from
+// each member's step_dev, which the captured step advances), or directly otherwise.
+static int32_t enqueue_batch_step(pb_batch* b, pb_sim* const* sims, int n, const pb_step_params* const* P,
+                                  const std::vector<const SolveLaunch*>& Ls, const PoissonArgs* dargs,
+                                  const int* dblk, size_t args0, size_t blk0, pb_step_report** dreps,
+                                  bool capturing, std::vector<long long>* launches) {
+  int32_t rc;
+  CK(cudaEventRecord(b->ev_fork, b->stream));
+  for (int i = 0; i < n; ++i) CK(cudaStreamWaitEvent(sims[i]->s.stream, b->ev_fork, 0));
+  std::vector<long long> l0(n);
+  for (int i = 0; i < n; ++i) {
+    l0[i] = sims[i]->s.launches;
+    if ((rc = enqueue_step_pre(sims[i], P[i]))) return rc;
+    CK(cudaEventRecord(b->ev_inst[i], sims[i]->s.stream));
+  }
+  std::vector<int> solved_by(n, -1);
+  for (size_t li = 0; li < Ls.size(); ++li) {
+    const SolveLaunch& L = *Ls[li];
+    for (int i : L.inst) {
+      CK(cudaStreamWaitEvent(b->stream, b->ev_inst[i], 0));
+      solved_by[i] = (int)li;
+    }
+    const PoissonArgs* da = dargs + (L.args_off - args0);
+    const int* db = dblk + (L.blk_off - blk0);
+    void* kargs[] = {(void*)&da, (void*)&db};
+    if (capturing) {
+      CK(cudaLaunchCooperativeKernel((void*)k_poisson_batch, dim3(L.nblocks), dim3(PT), kargs, L.smem, b->stream));
+    } else if ((rc = coop_launch(b->device, b->stream, [&]() {
+                  return cudaLaunchCooperativeKernel((void*)k_poisson_batch, dim3(L.nblocks), dim3(PT), kargs, L.smem,
+                                                     b->stream);
+                }))) {
+      return rc;
+    }
+    ++b->launches;
+    CK(cudaEventRecord(b->ev_solve[li], b->stream));
+  }
+  for (int i = 0; i < n; ++i) {
+    Sim* s = &sims[i]->s;
+    if (solved_by[i] >= 0) CK(cudaStreamWaitEvent(s->stream, b->ev_solve[solved_by[i]], 0));
+    if ((rc = enqueue_step_post(sims[i], P[i]))) return rc;
+    if (capturing) {
+      k_step_advance<<<1, 1, 0, s->stream>>>(s->step_dev);
+      CK(cudaGetLastError());
+      ++s->launches;
+    }
+    CK(cudaEventRecord(b->ev_inst[i], s->stream));
+    CK(cudaStreamWaitEvent(b->stream, b->ev_inst[i], 0));
+    if (launches) (*launches)[i] = s->launches - l0[i];
+  }
+  k_batch_reports<<<1, 256, 0, b->stream>>>(dreps, n, b->ring, b->slot);
+  CK(cudaGetLastError());
+  ++b->launches;
+  return PB_OK;
+}
+
+template <class T>
+static cudaError_t dcopy(T** dst, const T* src, size_t n) {
+  *dst = nullptr;
+  cudaError_t e = cudaMalloc((void**)dst, std::max<size_t>(n, 1) * sizeof(T));
+  if (e == cudaSuccess && n) e = cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice);
+  return e;
+}
+
+// pb_batch_run with graphs: each step's shape is captured once and replayed; a step that
+// cannot be captured is enqueued directly (and graphs stay off for the batch).
+static int32_t batch_run_graphs(pb_batch* b, pb_sim* const* sims, int n, const pb_step_params* params, int K,
+                                const std::vector<SolveLaunch>& plan) {
+  int32_t rc = PB_OK;
+  std::vector<pb_step_report*> reps(n);
+  for (int i = 0; i < n; ++i) reps[i] = sims[i]->s.rep_dev;
+  pb_step_report** dreps_run = nullptr;
+  CK(dcopy(&dreps_run, reps.data(), (size_t)n));
+  size_t pi = 0;
+  for (int k = 0; k < K && rc == PB_OK; ++k) {
+    std::vector<const pb_step_params*> P(n);
+    for (int i = 0; i < n; ++i) P[i] = &params[(size_t)i * K + k];
+    std::vector<const SolveLaunch*> Ls;
+    for (; pi < plan.size() && plan[pi].step == k; ++pi) Ls.push_back(&plan[pi]);
+    const size_t args0 = Ls.empty() ? 0 : Ls.front()->args_off, blk0 = Ls.empty() ? 0 : Ls.front()->blk_off;
+    size_t nargs = 0, nblk = 0;
+    for (const SolveLaunch* L : Ls) { nargs += L->inst.size(); nblk += (size_t)L->nblocks; }
+    uint64_t key = fnv_v(1469598103934665603ull, n);
+    for (int i = 0; i < n; ++i) {
+      key = fnv_v(key, sims[i]);
+      key = fnv_v(key, params_digest(P[i]));
+      key = fnv_v(key, state_signature(sims[i]));
+    }
+    pb_batch::StepGraph* g = nullptr;
+    for (auto& e : b->graphs)
+      if (e.key == key) g = &e;
+    // the members' step keys as the step expects them (they advance inside a replayed graph)
+    for (int i = 0; i < n; ++i) {
+      Sim* s = &sims[i]->s;
+      if ((long long)(uint32_t)P[i]->iteration != s->step_dev_val) {
+        k_step_set<<<1, 1, 0, b->stream>>>(s->step_dev, (uint32_t)P[i]->iteration);
+        CK(cudaGetLastError());
+      }
+    }
+    if (g) {
+      for (int i = 0; i < n; ++i) {
+        Sim* s = &sims[i]->s;
+        const int flips = 1 + (P[i]->sort_now ? 1 : 0);
+        for (int sp = 0; sp < 2; ++sp) s->sp[sp].cur ^= (flips & 1);
+        s->counts_valid = true;
+        s->sp_dx = P[i]->dx;
+        s->sp_dy = P[i]->dy;
+        s->launches += g->launches[i];
+      }
+      CK(cudaGraphLaunch(g->exec, b->stream));
+      b->launches += g->own_launches;
+      ++b->graph_replays;
+    } else if (!b->graphs_broken) {
+      pb_batch::StepGraph ng;
+      ng.key = key;
+      ng.launches.assign(n, 0);
+      CK(dcopy(&ng.dargs, b->hargs + args0, nargs));
+      CK(dcopy(&ng.dblk, b->hblk + blk0, nblk));
+      CK(dcopy(&ng.dreps, reps.data(), (size_t)n));
+      // host state of the members, restored if the step cannot be captured
+      std::vector<std::array<double, 6>> saved(n);
+      for (int i = 0; i < n; ++i) {
+        const Sim* s = &sims[i]->s;
+        saved[i] = {(double)s->sp[0].cur, (double)s->sp[1].cur, (double)s->counts_valid, s->sp_dx, s->sp_dy,
+                    (double)s->launches};
+      }
+      const long long bl0 = b->launches;
+      cudaError_t ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+      int32_t crc = ce == cudaSuccess ? PB_OK : PB_ERR_CUDA;
+      if (crc == PB_OK) {
+        for (int i = 0; i < n; ++i) sims[i]->s.capturing = 1;
+        crc = enqueue_batch_step(b, sims, n, P.data(), Ls, ng.dargs, ng.dblk, args0, blk0, ng.dreps, true,
+                                 &ng.launches);
+        for (int i = 0; i < n; ++i) sims[i]->s.capturing = 0;
+        cudaGraph_t graph = nullptr;
+        ce = cudaStreamEndCapture(b->stream, &graph);
+        if (crc == PB_OK && ce == cudaSuccess && graph) ce = cudaGraphInstantiate(&ng.exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (ce != cudaSuccess || !ng.exec) crc = crc ? crc : PB_ERR_CUDA;
+      }
+      if (crc != PB_OK) {
+        b->graphs_broken = 1;
+        b->graph_error = crc == PB_ERR_CUDA && ce != cudaSuccess ? std::string("batch step capture: ") +
+                                                                       cudaGetErrorString(ce)
+                                                                 : g_err;
+        cudaGetLastError();
+        for (int i = 0; i < n; ++i) {
+          Sim* s = &sims[i]->s;
+          s->sp[0].cur = (int)saved[i][0]; s->sp[1].cur = (int)saved[i][1];
+          s->counts_valid = saved[i][2] != 0.0; s->sp_dx = saved[i][3]; s->sp_dy = saved[i][4];
+          s->launches = (long long)saved[i][5];
+        }
+        b->launches = bl0;
+        if (ng.exec) cudaGraphExecDestroy(ng.exec);
+        cudaFree(ng.dargs); cudaFree(ng.dblk); cudaFree(ng.dreps);
+      } else {
+        if (b->graphs.size() >= 16) free_batch_graphs(b);
+        ng.own_launches = b->launches - bl0;
+        b->graphs.push_back(ng);
+        CK(cudaGraphLaunch(ng.exec, b->stream));
+        ++b->graph_captures;
+      }
+    }
+    if (b->graphs_broken && !g) {
+      // enqueue this step directly (arguments from the run's device copy)
+      for (int i = 0; i < n; ++i) sims[i]->s.step_dev_val = -1;
+      if ((rc = enqueue_batch_step(b, sims, n, P.data(), Ls, b->dargs, b->dblk, 0, 0, dreps_run, false, nullptr))) {
+        cudaFree(dreps_run);
+        return rc;
+      }
+      continue;
+    }
+    for (int i = 0; i < n; ++i) sims[i]->s.step_dev_val = (long long)(uint32_t)P[i]->iteration + 1;
+  }
+  cudaFree(dreps_run);
+  return PB_OK;
+}
+
 extern "C" {
 
 int32_t pb_batch_create(pb_batch** out, int32_t device) {
@@ -113,6 +335,8 @@ int32_t pb_batch_create(pb_batch** out, int32_t device) {
   CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&b->ev0));
   CK(cudaEventCreate(&b->ev1));
+  CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  CK(cudaMalloc((void**)&b->slot, sizeof(int)));
   CK(cudaFuncSetAttribute((const void*)k_poisson_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           (int)mg_coarse_smem_bytes(MG_MAX_COARSE)));
   CK(cudaFuncSetAttribute((const void*)k_poisson_batch, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -130,6 +354,11 @@ int32_t pb_batch_destroy(pb_batch* b) {
   if (b->hargs) cudaFreeHost(b->hargs);
   if (b->hblk) cudaFreeHost(b->hblk);
   if (b->hrep) cudaFreeHost(b->hrep);
+  free_batch_graphs(b);
+  if (b->ring) cudaFree(b->ring);
+  if (b->hring) cudaFreeHost(b->hring);
+  if (b->slot) cudaFree(b->slot);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   for (cudaEvent_t e : b->ev_inst) cudaEventDestroy(e);
   for (cudaEvent_t e : b->ev_solve) cudaEventDestroy(e);
   if (b->ev0) cudaEventDestroy(b->ev0);
@@ -235,6 +464,58 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
   for (int i = 0; i < n; ++i)
     for (int k = 0; k < K; ++k)
       if ((rc = check_step_params(&sims[i]->s, &params[(size_t)i * K + k]))) return rc;
+  bool use_graphs = b->graphs_on != 0;
+  for (int i = 0; i < n; ++i)
+    if (sims[i]->s.profiling) use_graphs = false;
+  if (use_graphs) {
+    // the report ring (its address is part of every graph)
+    if ((size_t)K * n > b->ring_cap) {
+      free_batch_graphs(b);
+      if (b->ring) cudaFree(b->ring);
+      if (b->hring) cudaFreeHost(b->hring);
+      b->ring = nullptr; b->hring = nullptr; b->ring_cap = 0;
+      const size_t cap = std::max<size_t>((size_t)K * n, 256);
+      CK(cudaMalloc((void**)&b->ring, cap * sizeof(pb_step_report)));
+      CK(cudaMallocHost((void**)&b->hring, cap * sizeof(pb_step_report)));
+      b->ring_cap = cap;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    CK(cudaEventRecord(b->ev0, b->stream));
+    if (nargs > 0) {
+      CK(cudaMemcpyAsync(b->dargs, b->hargs, nargs * sizeof(PoissonArgs), cudaMemcpyHostToDevice, b->stream));
+      CK(cudaMemcpyAsync(b->dblk, b->hblk, nblk * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    }
+    CK(cudaMemsetAsync(b->slot, 0, sizeof(int), b->stream));
+    for (int i = 0; i < n; ++i) {
+      Sim* s = &sims[i]->s;
+      s->mark_used = 0;
+      s->launches = 0;
+      CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), b->stream));
+    }
+    b->launches = 0;
+    if ((rc = batch_run_graphs(b, sims, n, params, K, plan))) return rc;
+    CK(cudaMemcpyAsync(b->hring, b->ring, (size_t)K * n * sizeof(pb_step_report), cudaMemcpyDeviceToHost,
+                       b->stream));
+    CK(cudaEventRecord(b->ev1, b->stream));
+    b->last_host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    CK(cudaEventSynchronize(b->ev1));
+    float gms = 0.0f;
+    CK(cudaEventElapsedTime(&gms, b->ev0, b->ev1));
+    b->last_ms = gms;
+    for (int i = 0; i < n; ++i) {
+      Sim* s = &sims[i]->s;
+      b->launches += s->launches;
+      if ((rc = read_counts(s))) return rc;
+    }
+    if (reports) {
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < K; ++k) reports[(size_t)i * K + k] = b->hring[(size_t)k * n + i];
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < K; ++k)
+          if ((rc = check_flags(&sims[i]->s, reports[(size_t)i * K + k].errflags))) return rc;
+    }
+    return PB_OK;
+  }
   // ---- enqueue
   const auto t_enq0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(b->ev0, b->stream));
@@ -306,6 +587,26 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       for (int k = 0; k < K; ++k)
         if ((rc = check_flags(&sims[i]->s, reports[(size_t)i * K + k].errflags))) return rc;
   }
+  return PB_OK;
+}
+
+int32_t pb_batch_set_graphs(pb_batch* b, int32_t on) {
+  if (!b) return fail(PB_ERR_ARG, "pb_batch_set_graphs");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  free_batch_graphs(b);
+  b->graphs_on = on ? 1 : 0;
+  b->graphs_broken = 0;
+  b->graph_error.clear();
+  return PB_OK;
+}
+
+int32_t pb_batch_graph_stats(pb_batch* b, int64_t* out3) {
+  if (!b || !out3) return fail(PB_ERR_ARG, "pb_batch_graph_stats");
+  out3[0] = b->graph_captures;
+  out3[1] = b->graph_replays;
+  out3[2] = b->graphs_broken;
+  if (b->graphs_broken) g_err = b->graph_error;
   return PB_OK;
 }
 

@@ -31,15 +31,27 @@ from . import _lib
 class SweepBatch:
     """Several DigitalTwinSimulator instances stepped together on one device."""
 
-    def __init__(self, device=0):
+    def __init__(self, device=0, graphs=False):
         self._libh = _lib.load()
         h = C.c_void_p()
         _lib.check(self._libh.pb_batch_create(C.byref(h), int(device)), "pb_batch_create")
         self._h = h
+        self.set_graphs(graphs)
         self.device = int(device)
         self.last_ms = 0.0
         self.last_launches = 0
         self.last_host_ms = 0.0
+
+    def set_graphs(self, on):
+        """Capture each batch step shape as a CUDA graph and replay it (pb_batch_set_graphs)."""
+        _lib.check(self._libh.pb_batch_set_graphs(self._h, 1 if on else 0), "pb_batch_set_graphs")
+        self.graphs = bool(on)
+
+    def graph_stats(self):
+        """(captures, replays, capture failed)."""
+        out = (C.c_int64 * 3)()
+        _lib.check(self._libh.pb_batch_graph_stats(self._h, out), "pb_batch_graph_stats")
+        return int(out[0]), int(out[1]), bool(out[2])
 
     def close(self):
         if self._h is not None and self._h.value:
