@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--serve-max-steps", type=int, default=4000)
     ap.add_argument("--kernel-options", type=int, default=None,
                     help="PB_OPT_* bits for the step kernels (default: the library's)")
+    ap.add_argument("--smoother-sweeps", type=int, default=1,
+                    help="damped-Jacobi sweeps on the fine multigrid level (1 or 2)")
     return ap.parse_args()
 
 
@@ -184,13 +186,14 @@ def traffic_table():
 
 # ----------------------------------------------------------------------------- GPU arm
 KERNEL_OPTIONS = None
+SMOOTHER_SWEEPS = 1
 
 
 def make_gpu_sim(name, device, seed):
     from thruster_cx_code_b200 import physics_engine as PE
     from thruster_cx_code_b200 import workloads as W
     from thruster_cx_code_b200 import _lib
-    sim = PE.DigitalTwinSimulator(device=device, seed=seed, sort_every=20)
+    sim = PE.DigitalTwinSimulator(device=device, seed=seed, sort_every=20, solver={"nu": SMOOTHER_SWEEPS})
     if KERNEL_OPTIONS is not None:
         _lib.check(sim._libh.pb_sim_set_kernel_options(sim._h, KERNEL_OPTIONS), "set_kernel_options")
     params = W.configure(sim, name)
@@ -445,12 +448,15 @@ SERVE_RATE_HZ, SERVE_WINDOW, SERVE_TOL, SERVE_CHUNK = 20.0, 1000, 5e-3, 50
 SERVE_SOLVER = {"max_coarse": 256}
 
 
-def _run_plain(sim, params, K, pushes_out=None):
+def _run_plain(sim, params, K, pushes_out=None, solve_out=None):
     """K steps of one simulator through pb_sim_run; returns the device time (ms) and, if
-    ``pushes_out`` is a list, appends the particle-pushes of those steps."""
-    run = timed_run(sim, params, K, profile=False)
+    ``pushes_out`` / ``solve_out`` are lists, appends the particle-pushes and the field-solve
+    time (ms) of those steps."""
+    run = timed_run(sim, params, K, profile=solve_out is not None)
     if pushes_out is not None:
         pushes_out.append(run["pushes"])
+    if solve_out is not None:
+        solve_out.append(run["phases"]["field_solve"])
     return run["ms"]
 
 
@@ -483,18 +489,20 @@ def sweep_section(device, args):
     sims, prm = [s for s, _ in built], [p for _, p in built]
     for s, p in built:
         _run_plain(s, p, SWEEP_WARMUP)
-    plain_pushes = []
-    plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes) for s, p in built)
+    plain_pushes, plain_solve = [], []
+    plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes, plain_solve) for s, p in built)
     def batched(graphs):
         batch.set_graphs(graphs)
         batch.run(sims, prm, SWEEP_WARMUP)
         n0 = [(s.num_p, s.num_e) for s in sims]
         res = batch.run(sims, prm, SWEEP_STEPS)
         pushes = sum(SV.pushes_of([rep for _, rep in r], a, b) for r, (a, b) in zip(res, n0))
+        batched.solve_ms = batch.last_solve_ms
         return batch.last_ms, batch.last_host_ms, pushes
 
     batch = SV.SweepBatch(device)
     streams_ms, streams_host_ms, streams_pushes = batched(False)
+    streams_solve_ms = batched.solve_ms
     graph_ms, graph_host_ms, graph_pushes = batched(True)
     g_stats = batch.graph_stats()
     # the batched form: CUDA graphs of whole batch steps when they captured, else the streams
@@ -515,11 +523,13 @@ def sweep_section(device, args):
            "plain_points_per_hr": 3600.0 / per_point_plain_s,
            "batched_points_per_hr": 3600.0 / per_point_batched_s,
            "batched_over_plain": plain_ms / batched_ms,
+           "plain_device_ms": plain_ms, "plain_field_solve_ms": float(sum(plain_solve)),
            "batched_device_ms": batched_ms, "batched_host_enqueue_ms": batched_host_ms,
            "batched_form": "graphs" if not g_stats[2] else "streams",
            "graph_captures_replays_failed": list(g_stats),
            "streams": {"points_per_hr": 3600.0 / (streams_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts),
                        "device_ms": streams_ms, "host_enqueue_ms": streams_host_ms,
+                       "field_solve_ms": streams_solve_ms,
                        "over_plain": plain_ms / streams_ms},
            "setup": f"excluded ({t_setup:.1f} s of host geometry, multigrid build and pre-load on 8 threads)"}
     for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms),
@@ -704,6 +714,7 @@ def reference_arm(args):
 if __name__ == "__main__":
     a = parse()
     KERNEL_OPTIONS = a.kernel_options
+    SMOOTHER_SWEEPS = a.smoother_sweeps
     if a.impl == "reference":
         reference_arm(a)
     else:

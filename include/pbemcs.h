@@ -328,10 +328,11 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
 int32_t pb_batch_set_graphs(pb_batch* b, int32_t on);
 /* out3: captures, replays, 1 if a capture failed (pb_last_error() gives the reason). */
 int32_t pb_batch_graph_stats(pb_batch* b, int64_t* out3);
-/* out3[0] = device time (ms) of the last pb_batch_run, out3[1] = kernel launches in it,
- * out3[2] = host time (ms) from its first enqueue to its last (when this approaches the
- * device time, the run is bound by launch overhead). */
-int32_t pb_batch_timing(pb_batch* b, double* out3);
+/* out4[0] = device time (ms) of the last pb_batch_run, out4[1] = kernel launches in it,
+ * out4[2] = host time (ms) from its first enqueue to its last (when this approaches the
+ * device time, the run is bound by launch overhead), out4[3] = device time of its
+ * field-solve launches (without graphs; 0 with them). */
+int32_t pb_batch_timing(pb_batch* b, double* out4);
 /* Device memory held by a simulator (bytes, estimated from its capacities). */
 int32_t pb_sim_memory(pb_sim* s, int64_t* bytes);
 

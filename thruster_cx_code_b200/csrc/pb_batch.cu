@@ -25,6 +25,8 @@ struct pb_batch {
   std::vector<cudaEvent_t> ev_solve; // per launch of a step
   double last_ms = 0.0;
   double last_host_ms = 0.0;   // host time spent enqueuing the last run (ev0 to the last enqueue)
+  double last_solve_ms = 0.0;  // device time of the field-solve launches of the last run (streams form)
+  std::vector<cudaEvent_t> tev; // timing events around the solve launches
   long long launches = 0;
   // CUDA graphs of whole batch steps (pb_batch_set_graphs): one graph per step shape of the
   // set (each member's step parameters without the step number and its state signature)
@@ -359,6 +361,7 @@ int32_t pb_batch_destroy(pb_batch* b) {
   if (b->hring) cudaFreeHost(b->hring);
   if (b->slot) cudaFree(b->slot);
   if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  for (cudaEvent_t e : b->tev) cudaEventDestroy(e);
   for (cudaEvent_t e : b->ev_inst) cudaEventDestroy(e);
   for (cudaEvent_t e : b->ev_solve) cudaEventDestroy(e);
   if (b->ev0) cudaEventDestroy(b->ev0);
@@ -517,6 +520,11 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     return PB_OK;
   }
   // ---- enqueue
+  while (b->tev.size() < 2 * plan.size()) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    b->tev.push_back(e);
+  }
   const auto t_enq0 = std::chrono::steady_clock::now();
   CK(cudaEventRecord(b->ev0, b->stream));
   if (nargs > 0) {
@@ -549,11 +557,13 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       const PoissonArgs* da = b->dargs + L.args_off;
       const int* db = b->dblk + L.blk_off;
       void* kargs[] = {(void*)&da, (void*)&db};
+      CK(cudaEventRecord(b->tev[2 * pi], b->stream));
       if ((rc = coop_launch(b->device, b->stream, [&]() {
              return cudaLaunchCooperativeKernel((void*)k_poisson_batch, dim3(L.nblocks), dim3(PT), kargs, L.smem,
                                                 b->stream);
            })))
         return rc;
+      CK(cudaEventRecord(b->tev[2 * pi + 1], b->stream));
       ++b->launches;
       CK(cudaEventRecord(b->ev_solve[li], b->stream));
     }
@@ -576,6 +586,12 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
   float ms = 0.0f;
   CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
   b->last_ms = ms;
+  b->last_solve_ms = 0.0;
+  for (size_t j = 0; j < plan.size(); ++j) {
+    float sm = 0.0f;
+    CK(cudaEventElapsedTime(&sm, b->tev[2 * j], b->tev[2 * j + 1]));
+    b->last_solve_ms += sm;
+  }
   for (int i = 0; i < n; ++i) {
     Sim* s = &sims[i]->s;
     b->launches += s->launches;
@@ -615,6 +631,7 @@ int32_t pb_batch_timing(pb_batch* b, double* out2) {
   out2[0] = b->last_ms;
   out2[1] = (double)b->launches;
   out2[2] = b->last_host_ms;
+  out2[3] = b->last_solve_ms;
   return PB_OK;
 }
 

@@ -84,9 +84,10 @@ class SweepBatch:
         R = (_lib.StepReport * (n * K))()
         arr = (C.c_void_p * n)(*[s._h.value for s in sims])
         _lib.check(self._libh.pb_batch_run(self._h, arr, n, P, int(K), R), "pb_batch_run")
-        t = (C.c_double * 3)()
+        t = (C.c_double * 4)()
         self._libh.pb_batch_timing(self._h, t)
         self.last_ms, self.last_launches, self.last_host_ms = float(t[0]), int(t[1]), float(t[2])
+        self.last_solve_ms = float(t[3])
         out = []
         for i, (s, prm) in enumerate(zip(sims, params_list)):
             res = []
