@@ -70,11 +70,14 @@ def parse():
     ap.add_argument("--no-second", action="store_true", help="skip the large_aperture_3grid line")
     ap.add_argument("--sweep-points", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=16)
-    ap.add_argument("--serve-max-steps", type=int, default=4000)
+    ap.add_argument("--serve-max-steps", type=int, default=20000)
     ap.add_argument("--kernel-options", type=int, default=None,
                     help="PB_OPT_* bits for the step kernels (default: the library's)")
-    ap.add_argument("--smoother-sweeps", type=int, default=1,
+    ap.add_argument("--smoother-sweeps", type=int, default=2,
                     help="damped-Jacobi sweeps on the fine multigrid level (1 or 2)")
+    ap.add_argument("--batch-max-coarse", type=int, default=256,
+                    help="coarsest multigrid level of the batched sweep points (the dense coarse inverse is "
+                         "applied by each point's few blocks in a batch)")
     return ap.parse_args()
 
 
@@ -186,7 +189,7 @@ def traffic_table():
 
 # ----------------------------------------------------------------------------- GPU arm
 KERNEL_OPTIONS = None
-SMOOTHER_SWEEPS = 1
+SMOOTHER_SWEEPS = 2
 
 
 def make_gpu_sim(name, device, seed):
@@ -500,6 +503,11 @@ def sweep_section(device, args):
         batched.solve_ms = batch.last_solve_ms
         return batch.last_ms, batch.last_host_ms, pushes
 
+    # the batched points' own solver setting: a small coarsest level (each point solves it with
+    # the few blocks of its share of the launch), applied by rebuilding each point's hierarchy
+    from thruster_cx_code_b200 import autotune as AT
+    for s in sims:
+        AT.apply(s, {"max_coarse": args.batch_max_coarse})
     batch = SV.SweepBatch(device)
     streams_ms, streams_host_ms, streams_pushes = batched(False)
     streams_solve_ms = batched.solve_ms
@@ -526,6 +534,8 @@ def sweep_section(device, args):
            "plain_device_ms": plain_ms, "plain_field_solve_ms": float(sum(plain_solve)),
            "batched_device_ms": batched_ms, "batched_host_enqueue_ms": batched_host_ms,
            "batched_form": "graphs" if not g_stats[2] else "streams",
+           "solver": {"plain_max_coarse": 1536, "batched_max_coarse": args.batch_max_coarse,
+                      "smoother_sweeps": SMOOTHER_SWEEPS},
            "graph_captures_replays_failed": list(g_stats),
            "streams": {"points_per_hr": 3600.0 / (streams_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts),
                        "device_ms": streams_ms, "host_enqueue_ms": streams_host_ms,
@@ -559,13 +569,15 @@ def served_section(device, batch, args):
     for i in range(args.serve_requests):
         t += rs.exponential(1.0 / SERVE_RATE_HZ)
         sp = W.served_point(rs, 100 + i)
-        req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device, solver=SERVE_SOLVER)),
-                         W.sweep_point_bytes(sp), args.serve_max_steps,
-                         SV.Convergence(window=SERVE_WINDOW, tol=SERVE_TOL, keys=("current", "saddle")))
-        # beamlet current (A) -> ions crossing per step: dt / (q w)
+        # beamlet current (A) = ions crossing per step x q w / dt
         cell_vol = (sp["dx"] * 1e-3) ** 2 * 1e-3
         w = max(sp["params"]["n0_plasma"] * cell_vol / 80.0, 1e3)
-        req.dt_over_qw = sp["dt"] / (1.602e-19 * w)
+        per_crossing = 1.602e-19 * w / sp["dt"]
+        req = SV.Request(i, (lambda sp=sp: W.make_sweep_sim(sp, device, solver=SERVE_SOLVER)),
+                         W.sweep_point_bytes(sp), args.serve_max_steps,
+                         SV.Convergence(window=SERVE_WINDOW, tol=SERVE_TOL, keys=("current", "saddle"),
+                                        counts={"current": per_crossing}))
+        req.dt_over_qw = 1.0 / per_crossing
         arrivals.append((t, req))
     srv = SV.SweepServer(device, hbm_budget_bytes=150e9, max_active=64, chunk=SERVE_CHUNK, batch=batch,
                          setup_workers=max(2, min(8, (os.cpu_count() or 2) // 2)))
@@ -573,7 +585,9 @@ def served_section(device, batch, args):
     st = srv.stats()
     st.update({"requests": args.serve_requests, "arrival_rate_hz": SERVE_RATE_HZ, "max_steps": args.serve_max_steps,
                "retire_rule": f"{SERVE_WINDOW // 2}-step means of saddle and current change < {SERVE_TOL:g} "
-                              f"over {SERVE_WINDOW // 2} steps",
+                              f"over {SERVE_WINDOW // 2} steps (the current: or within twice the Poisson noise "
+                              f"of its crossing counts)",
+               "current_noise": [round(r.conv.noise("current"), 5) for r in srv.done],
                "steps": [r.steps for r in srv.done], "particle_pushes": srv.pushes, "gpu_ms": srv.gpu_ms,
                "final_changes": [{k: round(v, 5) for k, v in r.conv.changes().items()} for r in srv.done],
                "mean_crossings_per_step": [float(np.mean(r.conv.hist["current"][-SERVE_WINDOW:])) * r.dt_over_qw

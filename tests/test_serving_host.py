@@ -101,3 +101,22 @@ def test_sweep_points_build_and_fit_estimate():
         o.build_domain(dict(sp["params"]))  # passes the reference's numerics checks
         nodes = o.nx * o.ny
         assert W.sweep_point_bytes(sp) > 800 * nodes
+
+
+def test_count_key_settles_within_its_poisson_noise():
+    """A current made of ~25 macro-particle crossings per step (factor 2 A per crossing)
+    fluctuates by several percent between window halves: the strict 0.5% test fails, the
+    count-aware test passes; a real drift far above the noise still fails both."""
+    rng = np.random.default_rng(0)
+    f = 2.0
+    flat = Convergence(window=400, tol=5e-3, keys=("current",), counts={"current": f})
+    strict = Convergence(window=400, tol=5e-3, keys=("current",))
+    drift = Convergence(window=400, tol=5e-3, keys=("current",), counts={"current": f})
+    for k in range(400):
+        c = f * rng.poisson(25)
+        flat.add(current=c)
+        strict.add(current=c)
+        drift.add(current=f * rng.poisson(25 if k < 200 else 35))
+    assert flat.converged() and not strict.converged()
+    assert not drift.converged()
+    assert flat.noise("current") > 5e-3 and strict.noise("current") == 0.0

@@ -132,7 +132,7 @@ struct Sim {
   int rep_run_cap = 0;
   // settings
   double tol = 1e-8, tol_inner = 1e-3;
-  int max_outer = 8, max_inner = 40, nu = 1, max_coarse = 1536;
+  int max_outer = 8, max_inner = 40, nu = 2, max_coarse = 1536;
   uint64_t seed = 0;
   bool counts_valid = false;
   bool domain_set = false;

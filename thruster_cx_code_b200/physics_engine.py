@@ -101,7 +101,7 @@ class DigitalTwinSimulator:
         lib.pb_sim_set_seed(h, C.c_uint64(self.seed))
         self.sort_every = int(sort_every)
         self.verbose = bool(verbose)
-        s = dict(tol=1e-8, tol_inner=1e-3, max_outer=8, max_inner=40, nu=1, max_coarse=1536)
+        s = dict(tol=1e-8, tol_inner=1e-3, max_outer=8, max_inner=40, nu=2, max_coarse=1536)
         s.update(solver or {})
         self.solver = s
         _lib.check(lib.pb_sim_set_solver(h, s["tol"], s["tol_inner"], s["max_outer"], s["max_inner"], s["nu"],

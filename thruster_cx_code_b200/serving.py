@@ -121,13 +121,20 @@ class Convergence:
     """Relative change of window means between the halves of the last ``window`` steps,
     for each tracked quantity; converged when every change is below ``tol`` and at least
     ``min_steps`` steps have run.  Quantities that are NaN in a window (theta95 with five
-    or fewer crossings) count as not converged."""
+    or fewer crossings) count as not converged.
 
-    def __init__(self, window=500, tol=5e-3, min_steps=None, keys=("current", "theta95", "saddle")):
+    ``counts`` maps a key whose values are a count of macro-particles times a known factor
+    (the beamlet current: crossings x q w / dt) to that factor.  Such a key also counts as
+    settled when its change is within twice the Poisson noise of the difference of the two
+    window means (sqrt(Na + Nb) / max(Na, Nb) for Na and Nb crossings in the halves): a
+    current carried by a few macro-particles per step cannot settle below its own noise."""
+
+    def __init__(self, window=500, tol=5e-3, min_steps=None, keys=("current", "theta95", "saddle"), counts=None):
         self.window = int(window)
         self.tol = float(tol)
         self.min_steps = int(min_steps if min_steps is not None else window)
         self.keys = tuple(keys)
+        self.counts = dict(counts or {})
         self.hist = {k: [] for k in self.keys}
         self.steps = 0
 
@@ -154,10 +161,25 @@ class Convergence:
             out[k] = abs(mb - ma) / scale if scale > 0 else 0.0
         return out
 
+    def noise(self, key):
+        """Twice the relative Poisson noise of the difference of the window-half means of a
+        count key (inf without counts in the window); 0 for other keys."""
+        f = self.counts.get(key)
+        if not f:
+            return 0.0
+        h = self.window // 2
+        v = self.hist[key]
+        if len(v) < 2 * h or h == 0:
+            return math.inf
+        na = float(np.sum(v[-2 * h:-h])) / f
+        nb = float(np.sum(v[-h:])) / f
+        top = max(na, nb)
+        return 2.0 * math.sqrt(na + nb) / top if top > 0 else math.inf
+
     def converged(self):
         if self.steps < self.min_steps:
             return False
-        return all(c < self.tol for c in self.changes().values())
+        return all(c < max(self.tol, self.noise(k)) for k, c in self.changes().items())
 
 
 class Request:
