@@ -75,9 +75,8 @@ def parse():
                     help="PB_OPT_* bits for the step kernels (default: the library's)")
     ap.add_argument("--smoother-sweeps", type=int, default=2,
                     help="damped-Jacobi sweeps on the fine multigrid level (1 or 2)")
-    ap.add_argument("--batch-max-coarse", type=int, default=256,
-                    help="coarsest multigrid level of the batched sweep points (the dense coarse inverse is "
-                         "applied by each point's few blocks in a batch)")
+    ap.add_argument("--batch-max-coarse", type=int, default=1536,
+                    help="coarsest multigrid level of the batched sweep points")
     return ap.parse_args()
 
 
@@ -503,11 +502,11 @@ def sweep_section(device, args):
         batched.solve_ms = batch.last_solve_ms
         return batch.last_ms, batch.last_host_ms, pushes
 
-    # the batched points' own solver setting: a small coarsest level (each point solves it with
-    # the few blocks of its share of the launch), applied by rebuilding each point's hierarchy
-    from thruster_cx_code_b200 import autotune as AT
-    for s in sims:
-        AT.apply(s, {"max_coarse": args.batch_max_coarse})
+    # the batched points' coarsest level (default: the plain points' own; 256 measured slower)
+    if args.batch_max_coarse != 1536:
+        from thruster_cx_code_b200 import autotune as AT
+        for s in sims:
+            AT.apply(s, {"max_coarse": args.batch_max_coarse})
     batch = SV.SweepBatch(device)
     streams_ms, streams_host_ms, streams_pushes = batched(False)
     streams_solve_ms = batched.solve_ms

@@ -34,6 +34,7 @@
 namespace pb {
 
 constexpr long long BAR_SPIN_LIMIT = 1ll << 22;
+constexpr int FU = 4;  // fine-level nodes per thread and pass of the vector loops (their loads overlap)
 constexpr float W_KEEP = (float)(1.0 - MG_JACOBI_OMEGA);
 
 // Grid barrier on one 32-bit word per instance: its block 0 adds 2^31 - (nblocks - 1), the others add 1,
@@ -303,19 +304,27 @@ __device__ double up_leg0_tiled(const PoissonArgs& a, const float* r0) {
 __device__ void presmooth0(const PoissonArgs& a, const float* r, float* s_out, int tid, int nth) {
   const MgLevel& F = a.lev[0];
   const int N = F.ny * F.nx;
-  for (int i = tid; i < N; i += nth) {
-    const int y = i / F.nx, x = i - y * F.nx;
-    int j[4];
-    nbrs0(a, i, y, x, j);
-    const float di = __ldg(F.dinv + i), ri = *(r + i);
-    float acc = 0.0f;
+  for (int i0 = tid; i0 < N; i0 += FU * nth) {
+    float sv[FU];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int jj = j[k] >= 0 ? j[k] : i;
-      const float dk = j[k] >= 0 ? __ldg(F.dinv + jj) : 0.0f;
-      acc += dk * *(r + jj);
+    for (int u = 0; u < FU; ++u) {
+      const int i = i0 + u * nth < N ? i0 + u * nth : i0;
+      const int y = i / F.nx, x = i - y * F.nx;
+      int j[4];
+      nbrs0(a, i, y, x, j);
+      const float di = __ldg(F.dinv + i), ri = *(r + i);
+      float acc = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int jj = j[k] >= 0 ? j[k] : i;
+        const float dk = j[k] >= 0 ? __ldg(F.dinv + jj) : 0.0f;
+        acc += dk * *(r + jj);
+      }
+      sv[u] = di > 0.0f ? W_KEEP * ri + acc : 0.0f;
     }
-    __stcg(s_out + i, di > 0.0f ? W_KEEP * ri + acc : 0.0f);
+#pragma unroll
+    for (int u = 0; u < FU; ++u)
+      if (i0 + u * nth < N) __stcg(s_out + i0 + u * nth, sv[u]);
   }
 }
 
@@ -325,17 +334,27 @@ __device__ double smooth0(const PoissonArgs& a, const float* r, int tid, int nth
   const MgLevel& F = a.lev[0];
   const int N = F.ny * F.nx;
   double rz = 0.0;
-  for (int i = tid; i < N; i += nth) {
-    const int y = i / F.nx, x = i - y * F.nx;
-    int j[4];
-    nbrs0(a, i, y, x, j);
-    const float di = __ldg(F.dinv + i), ri = *(r + i), mi = *(a.m32 + i);
-    float sm = 0.0f;
+  for (int i0 = tid; i0 < N; i0 += FU * nth) {
+    float zv[FU], rv[FU];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) sm += j[k] >= 0 ? *(a.m32 + j[k]) : 0.0f;
-    const float z = di > 0.0f ? W_KEEP * mi + di * (ri + sm) : 0.0f;
-    __stcg(F.z + i, z);
-    rz += (double)ri * (double)z;
+    for (int u = 0; u < FU; ++u) {
+      const int i = i0 + u * nth < N ? i0 + u * nth : i0;
+      const int y = i / F.nx, x = i - y * F.nx;
+      int j[4];
+      nbrs0(a, i, y, x, j);
+      const float di = __ldg(F.dinv + i), ri = *(r + i), mi = *(a.m32 + i);
+      float sm = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sm += j[k] >= 0 ? *(a.m32 + j[k]) : 0.0f;
+      zv[u] = di > 0.0f ? W_KEEP * mi + di * (ri + sm) : 0.0f;
+      rv[u] = ri;
+    }
+#pragma unroll
+    for (int u = 0; u < FU; ++u) {
+      if (i0 + u * nth >= N) continue;
+      __stcg(F.z + i0 + u * nth, zv[u]);
+      rz += (double)rv[u] * (double)zv[u];
+    }
   }
   return rz;
 }
@@ -571,16 +590,27 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
         get_sums(a, slot++, rz, dummy);
         const double beta = k == 0 ? 0.0 : rz / rz_old;
         double pq_p = 0.0;
-        for (int i = tid; i < N; i += nth) {
-          const int y = i / a.nx, x = i - y * a.nx;
-          const bool fr = __ldg(a.cls + i) == NC_FREE;
-          const float az = apply0<float>(a, a.z32, i, y, x);
-          const float zi = *(a.z32 + i);
-          const float p = fr ? zi + (float)beta * (k == 0 ? 0.0f : (*(a.p32 + i))) : 0.0f;
-          const float q = fr ? az + (float)beta * (k == 0 ? 0.0f : (*(a.q32 + i))) : 0.0f;
-          __stcg(a.p32 + i, p);
-          __stcg(a.q32 + i, q);
-          pq_p += (double)p * (double)q;
+        // FU nodes per thread and pass: every load of the pass is issued before the first
+        // store, so the loads of different nodes overlap (the sums keep the node order)
+        for (int i0 = tid; i0 < N; i0 += FU * nth) {
+          float pv[FU], qv[FU];
+#pragma unroll
+          for (int u = 0; u < FU; ++u) {
+            const int i = i0 + u * nth < N ? i0 + u * nth : i0;
+            const int y = i / a.nx, x = i - y * a.nx;
+            const bool fr = __ldg(a.cls + i) == NC_FREE;
+            const float az = apply0<float>(a, a.z32, i, y, x);
+            const float zi = *(a.z32 + i);
+            pv[u] = fr ? zi + (float)beta * (k == 0 ? 0.0f : (*(a.p32 + i))) : 0.0f;
+            qv[u] = fr ? az + (float)beta * (k == 0 ? 0.0f : (*(a.q32 + i))) : 0.0f;
+          }
+#pragma unroll
+          for (int u = 0; u < FU; ++u) {
+            if (i0 + u * nth >= N) continue;
+            __stcg(a.p32 + i0 + u * nth, pv[u]);
+            __stcg(a.q32 + i0 + u * nth, qv[u]);
+            pq_p += (double)pv[u] * (double)qv[u];
+          }
         }
         put_partials(a, slot, pq_p, 0.0);
         grid_barrier(a);
@@ -588,13 +618,23 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
         get_sums(a, slot++, pq, dummy);
         const double alpha = pq != 0.0 ? rz / pq : 0.0;
         double rr_p = 0.0;
-        for (int i = tid; i < N; i += nth) {
-          if (__ldg(a.cls + i) != NC_FREE) continue;
-          const float e = (*(a.e32 + i)) + (float)alpha * (*(a.p32 + i));
-          const float r = (*(a.r32 + i)) - (float)alpha * (*(a.q32 + i));
-          __stcg(a.e32 + i, e);
-          __stcg(a.r32 + i, r);
-          rr_p += (double)r * (double)r;
+        for (int i0 = tid; i0 < N; i0 += FU * nth) {
+          float ev[FU], rv[FU];
+          bool fr[FU];
+#pragma unroll
+          for (int u = 0; u < FU; ++u) {
+            const int i = i0 + u * nth < N ? i0 + u * nth : i0;
+            fr[u] = i0 + u * nth < N && __ldg(a.cls + i) == NC_FREE;
+            ev[u] = (*(a.e32 + i)) + (float)alpha * (*(a.p32 + i));
+            rv[u] = (*(a.r32 + i)) - (float)alpha * (*(a.q32 + i));
+          }
+#pragma unroll
+          for (int u = 0; u < FU; ++u) {
+            if (!fr[u]) continue;
+            __stcg(a.e32 + i0 + u * nth, ev[u]);
+            __stcg(a.r32 + i0 + u * nth, rv[u]);
+            rr_p += (double)rv[u] * (double)rv[u];
+          }
         }
         put_partials(a, slot, rr_p, 0.0);
         grid_barrier(a);
