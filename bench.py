@@ -69,6 +69,7 @@ def parse():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-second", action="store_true", help="skip the large_aperture_3grid line")
     ap.add_argument("--sweep-points", type=int, default=64)
+    ap.add_argument("--no-served", action="store_true", help="skip the served section of the sweep")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-max-steps", type=int, default=20000)
     ap.add_argument("--kernel-options", type=int, default=None,
@@ -235,7 +236,11 @@ def timed_run(sim, params, K, profile=True):
     n_p0, n_e0 = sim.num_p, sim.num_e
     stats_before = list(sim.last_report.poisson_stats) if sim.last_report is not None else None
     lib.pb_sim_set_profiling(sim._h, 1 if profile else 0)
+    mg0 = (C.c_int64 * 4)()
+    _lib.check(lib.pb_sim_mg_stats(sim._h, mg0), "pb_sim_mg_stats")
     _lib.check(lib.pb_sim_run(sim._h, P, K, R), "pb_sim_run")
+    mg1 = (C.c_int64 * 4)()
+    _lib.check(lib.pb_sim_mg_stats(sim._h, mg1), "pb_sim_mg_stats")
     tm = (C.c_double * 9)()
     lib.pb_sim_timing(sim._h, tm)
     ph = (C.c_double * 10)()
@@ -250,7 +255,9 @@ def timed_run(sim, params, K, profile=True):
     return {"ms": float(tm[0]), "reports": R, "phases": {k: float(ph[i]) for i, k in enumerate(PHASES)},
             "launches": int(tm[8]), "pushes": pushes_of(R, n_p0, n_e0), "n_p0": n_p0, "n_e0": n_e0,
             "ions_per_launch": float(np.mean(ions)), "eles_per_launch": float(np.mean(eles)),
-            "stats_before": stats_before}
+            "stats_before": stats_before, "cells_broken": int(sum(r.broken for r in R)),
+            "mg_rebuilds": {"device": int(mg1[0] - mg0[0]), "left_to_host": int(mg1[1] - mg0[1]),
+                            "host": int(mg1[2] - mg0[2])}}
 
 
 def kernel_rooflines(run, K, peak, traffic):
@@ -349,6 +356,7 @@ def gpu_arm(args):
                        "electrons": run["n_e0"], "parallelism": f"replicas x{world}",
                        "l2": "particle state > L2 (126 MB); no flush needed", "sort_every": 20,
                        "picard": "5 solves every 2nd step, FP32 MG-PCG + FP64 refinement"},
+            "cells_broken": run["cells_broken"], "mg_rebuilds": run["mg_rebuilds"],
             "e2e": e2e, "roofline": roof, "clocks": clk, "gpu_launches": run["launches"],
             "kernel_options": kernel_options_of(local)}
     if rank == 0 and world == 1 and run["stats_before"] is not None:
@@ -392,7 +400,8 @@ def second_workload(args, device, peak, traffic):
     out = {"value": run["pushes"] / (run["ms"] * 1e-3), "unit": "particle-pushes/s", "ms_per_step": run["ms"] / K,
            "grid_nodes": [sim.ny, sim.nx], "ions": run["n_p0"], "electrons": run["n_e0"],
            "roofline": kernel_rooflines(run, K, peak, traffic),
-           "phase_ms_per_step": {k: v / K for k, v in run["phases"].items()}}
+           "phase_ms_per_step": {k: v / K for k, v in run["phases"].items()},
+           "cells_broken": run["cells_broken"], "mg_rebuilds": run["mg_rebuilds"]}
     if run["stats_before"] is not None:
         out["poisson"] = poisson_section(sim, run["stats_before"], run["reports"], run["phases"]["field_solve"], peak)
     sim.close()
@@ -477,7 +486,8 @@ def sweep_section(device, args):
     steps, then 40 timed).  Batched: all points together through pb_batch_run, from the
     state the plain steps left (3 warm-up steps, then 40 timed), first with every member's
     kernels enqueued on its own stream, then with each batch step shape captured as one CUDA
-    graph and replayed (the warm-up steps capture).  Rates use device time, scaled to 3000
+    graph and replayed (the warm-up steps capture); the faster form is the one reported as
+    batched, both are listed.  Rates use device time, scaled to 3000
     steps per point; setup is excluded.  The particle-pushes of each part are reported, so
     their workloads can be compared.  Then the C4 served run."""
     from thruster_cx_code_b200 import serving as SV
@@ -511,9 +521,11 @@ def sweep_section(device, args):
     streams_ms, streams_host_ms, streams_pushes = batched(False)
     streams_solve_ms = batched.solve_ms
     graph_ms, graph_host_ms, graph_pushes = batched(True)
+    graph_solve_ms = batched.solve_ms
     g_stats = batch.graph_stats()
-    # the batched form: CUDA graphs of whole batch steps when they captured, else the streams
-    if not g_stats[2]:
+    # the batched form reported: the faster of the two (graphs only when no capture failed)
+    use_graphs = not g_stats[2] and graph_ms < streams_ms
+    if use_graphs:
         batched_ms, batched_host_ms, batched_pushes = graph_ms, graph_host_ms, graph_pushes
     else:
         batched_ms, batched_host_ms, batched_pushes = streams_ms, streams_host_ms, streams_pushes
@@ -532,7 +544,7 @@ def sweep_section(device, args):
            "batched_over_plain": plain_ms / batched_ms,
            "plain_device_ms": plain_ms, "plain_field_solve_ms": float(sum(plain_solve)),
            "batched_device_ms": batched_ms, "batched_host_enqueue_ms": batched_host_ms,
-           "batched_form": "graphs" if not g_stats[2] else "streams",
+           "batched_form": "graphs" if use_graphs else "streams",
            "solver": {"plain_max_coarse": 1536, "batched_max_coarse": args.batch_max_coarse,
                       "smoother_sweeps": SMOOTHER_SWEEPS},
            "graph_captures_replays_failed": list(g_stats),
@@ -540,6 +552,10 @@ def sweep_section(device, args):
                        "device_ms": streams_ms, "host_enqueue_ms": streams_host_ms,
                        "field_solve_ms": streams_solve_ms,
                        "over_plain": plain_ms / streams_ms},
+           "graphs": {"points_per_hr": 3600.0 / (graph_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts),
+                      "device_ms": graph_ms, "host_enqueue_ms": graph_host_ms,
+                      "field_solve_ms": graph_solve_ms,
+                      "over_plain": plain_ms / graph_ms},
            "setup": f"excluded ({t_setup:.1f} s of host geometry, multigrid build and pre-load on 8 threads)"}
     for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms),
                              ("batched", float(batched_pushes), batched_ms)):
@@ -547,7 +563,7 @@ def sweep_section(device, args):
         out[f"{name}_pushes"] = pushes
         out[f"{name}_pushes_per_s"] = rate
         out[f"{name}_hbm_frac"] = rate * ALG_BYTES_PUSH / 1e9 / peak if peak else None
-    out["served"] = served_section(device, batch, args)
+    out["served"] = None if args.no_served else served_section(device, batch, args)
     batch.close()
     return out
 

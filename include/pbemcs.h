@@ -228,8 +228,21 @@ int32_t pb_sim_set_spline(pb_sim* s, int32_t which, int32_t nt, const double* t,
                           double hi);
 
 /* Rebuild node classes and the multigrid hierarchy from the device isBound (after cells
- * broke by sputtering; build_sparse_matrix, physics_engine.py:1448). */
+ * broke by sputtering; build_sparse_matrix, physics_engine.py:1448).  Inside pb_sim_run,
+ * pb_sim_step and pb_batch_run the same rebuild runs on the device before the first field
+ * solve after a break, bit-equal to this host build.  When the freed nodes would make this
+ * build choose other levels, or the coarsest level outgrows 1.25 x max(its size at the last
+ * host build, max_coarse), those calls run this host build before returning (the solves
+ * before it use the device's rebuild with the old level count, or the old hierarchy). */
 int32_t pb_sim_rebuild_operator(pb_sim* s);
+/* out4: hierarchy rebuilds done on the device, rebuilds left to the host, host rebuilds
+ * run after pb_sim_run / pb_sim_step / pb_batch_run for them, and the current coarsest
+ * active count. */
+int32_t pb_sim_mg_stats(pb_sim* s, int64_t* out4);
+/* FNV-1a digest of the hierarchy the field solve reads (per level the smoother weights and
+ * the transfer stencils, then the coarsest index set and its dense inverse): equal digests
+ * mean bit-equal operators (a diagnostic without a reference counterpart). */
+int32_t pb_sim_operator_digest(pb_sim* s, uint64_t* out);
 
 /* Replace one species' particles (species 0 ions, 1 electrons); host arrays; cex may be
  * NULL for electrons. */
@@ -333,6 +346,10 @@ int32_t pb_batch_graph_stats(pb_batch* b, int64_t* out3);
  * device time, the run is bound by launch overhead), out4[3] = device time of its
  * field-solve launches (without graphs; 0 with them). */
 int32_t pb_batch_timing(pb_batch* b, double* out4);
+/* A member's field-solve cost as the batch measured it (out2[0]: block-milliseconds per
+ * launch in its last batch run, 0 before one) and its block share in the last launch planned
+ * (out2[1]); pb_batch_run shares each launch's blocks in proportion to the first. */
+int32_t pb_sim_batch_share(pb_sim* s, double* out2);
 /* Device memory held by a simulator (bytes, estimated from its capacities). */
 int32_t pb_sim_memory(pb_sim* s, int64_t* bytes);
 

@@ -2,11 +2,11 @@
 
 * A batch of one is the single-instance step: particles, fields and reports bit-identical
   to K calls of DigitalTwinSimulator.step.
-* A sweep point stepped in a mix with two others of different grid sizes matches the same
-  point stepped alone.  The field solves of the mix share the SMs, so the deterministic
-  block-order reductions run over fewer blocks and round differently.  The tolerance is
-  therefore the one used for independent field solves: phi within 1e-6 of max|phi|,
-  positions and velocities per particle id within 1e-4 of scale, counts within 0.2%.
+* A sweep point stepped in a mix with two others of different grid sizes is the same point
+  stepped alone, bit for bit.  The field solves of the mix share the SMs, so each instance
+  runs on fewer blocks, but every reduction of the solve sums a fixed set of virtual-block
+  partials in a fixed order, whatever the block count.
+* The same holds for the block shares the batch picks from measured solve times.
 """
 import numpy as np
 import pytest
@@ -65,26 +65,25 @@ def test_batch_of_one_is_step(mods):
     b.close()
 
 
+def _same(a, b):
+    assert a.num_p == b.num_p and a.num_e == b.num_e
+    for x, y in zip(_state(a), _state(b)):
+        np.testing.assert_array_equal(np.asarray(x).view(np.uint32) if x.dtype == np.float32 else x,
+                                      np.asarray(y).view(np.uint32) if y.dtype == np.float32 else y)
+    np.testing.assert_array_equal(a.V, b.V)
+
+
 def test_point_in_a_mix_matches_alone(mods):
     specs = [_spec("64x256", 200000, 2), _spec("128x512", 400000, 3), _spec("256x1024", 300000, 4)]
     alone, pal = W.make_sweep_sim(specs[0])
     batch = mods.SweepBatch()
     batch.run([alone], [pal], K)
     mix = [W.make_sweep_sim(sp) for sp in specs]
-    batch.run([m[0] for m in mix], [m[1] for m in mix], K)
+    # two runs: the second takes its block shares from the first run's measured solve times
+    batch.run([m[0] for m in mix], [m[1] for m in mix], K // 2)
+    batch.run([m[0] for m in mix], [m[1] for m in mix], K - K // 2)
     batch.close()
-    g = mix[0][0]
-    assert abs(g.num_p - alone.num_p) <= max(2, 0.002 * alone.num_p)
-    assert abs(g.num_e - alone.num_e) <= max(2, 0.002 * alone.num_e)
-    errV = np.abs(g.V - alone.V).max() / np.abs(alone.V).max()
-    assert errV <= 1e-6, errV
-    ia, ida, _, _ = _state(alone)
-    ig, idg, _, _ = _state(g)
-    common, ai, gi = np.intersect1d(ida, idg, return_indices=True)
-    assert common.size >= 0.99 * min(ida.size, idg.size)
-    d = np.abs(ia[:, ai].astype(np.float64) - ig[:, gi].astype(np.float64))
-    scale = np.abs(ia[:, ai]).astype(np.float64).max(axis=1, keepdims=True)
-    assert (d / scale).max() <= 1e-4
+    _same(mix[0][0], alone)
     for m in mix:
         m[0].close()
     alone.close()

@@ -7,10 +7,9 @@
   admitted while the others are on the GPU; each retires at its step limit, and its final
   state (taken at retirement) is compared with the same request run alone.
 
-A point in a mix shares the field-solve launch with the others, so its block-order dot
-products run over fewer blocks and round differently from a solo run.  The tolerance is
-the one for independent field solves: potential within 1e-6 of max|phi|, positions and
-velocities per particle id within 1e-4 of scale, particle counts within 0.2%.
+A point in a mix shares the field-solve launch with the others and runs on fewer blocks,
+but every reduction of its solve sums a fixed set of virtual-block partials in a fixed
+order: its particles and potential are the solo run's, bit for bit.
 """
 import numpy as np
 import pytest
@@ -43,16 +42,11 @@ def _snap(sim):
             "V": np.array(sim.V, copy=True)}
 
 
-def _close_to(a, b):
-    assert abs(a["num_p"] - b["num_p"]) <= max(2, 0.002 * b["num_p"])
-    assert abs(a["num_e"] - b["num_e"]) <= max(2, 0.002 * b["num_e"])
-    errV = np.abs(a["V"] - b["V"]).max() / np.abs(b["V"]).max()
-    assert errV <= 1e-6, errV
-    common, ai, bi = np.intersect1d(a["ids"], b["ids"], return_indices=True)
-    assert common.size >= 0.99 * min(a["ids"].size, b["ids"].size)
-    d = np.abs(a["ions"][:, ai] - b["ions"][:, bi])
-    scale = np.abs(b["ions"][:, bi]).max(axis=1, keepdims=True)
-    assert (d / scale).max() <= 1e-4
+def _same_as(a, b):
+    assert (a["num_p"], a["num_e"]) == (b["num_p"], b["num_e"])
+    np.testing.assert_array_equal(a["V"], b["V"])
+    np.testing.assert_array_equal(a["ids"], b["ids"])
+    np.testing.assert_array_equal(a["ions"], b["ions"])
 
 
 def test_join_and_retire_mid_run(SV):
@@ -69,7 +63,7 @@ def test_join_and_retire_mid_run(SV):
     B.close()                                 # B retires
     batch.run([A, C], [pA, pC], 8)            # A finishes its 24 steps beside C
     assert A.iteration == 24
-    _close_to(_snap(A), ref)
+    _same_as(_snap(A), ref)
     A.close()
     C.close()
     batch.close()
@@ -96,5 +90,5 @@ def test_served_requests_match_alone(SV):
     assert sorted(r.rid for r in done) == [0, 1, 2]
     for r in done:
         assert r.steps == steps[r.rid] and not r.converged
-        _close_to(r.result, refs[r.rid])
+        _same_as(r.result, refs[r.rid])
     srv.close()

@@ -2,12 +2,14 @@
 
     python -m thruster_cx_code_b200._build
 
-Compiles two translation units with nvcc for sm_100a and links them:
+Compiles three translation units with nvcc for sm_100a and links them:
   csrc/pb_runtime.cu  the runtime, the C-ABI and (included) the particle and diagnostic
                       kernels, with fused multiply-add contraction disabled: the particle
                       arithmetic reproduces NumPy's separately rounded operations;
   csrc/pb_poisson.cu  the FP32 MG-PCG field solve, with contraction allowed (its result is
-                      compared with SuperLU to a tolerance, not bit for bit).
+                      compared with SuperLU to a tolerance, not bit for bit);
+  csrc/pb_mgdev.cu    the multigrid hierarchy rebuilt on the device after cells break
+                      (explicitly rounded arithmetic, bit-equal to the host build).
 """
 import os
 import subprocess
@@ -16,7 +18,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libpbemcs.so")
-SOURCES = ["pb_runtime.cu", "pb_particles.cu", "pb_poisson.cu", "pb_misc.cu", "pb_batch.cu", "pb_common.cuh",
+SOURCES = ["pb_runtime.cu", "pb_particles.cu", "pb_poisson.cu", "pb_mgdev.cu", "pb_misc.cu", "pb_batch.cu",
+           "pb_common.cuh",
            "pb_kernels.cuh", "pb_misc.cuh", "pb_poisson.cuh", "pb_mg_host.hpp"]
 
 
@@ -35,7 +38,7 @@ def needs_build():
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-UNITS = (("pb_runtime.cu", "false"), ("pb_poisson.cu", "true"))
+UNITS = (("pb_runtime.cu", "false"), ("pb_poisson.cu", "true"), ("pb_mgdev.cu", "false"))
 
 
 def _run(cmd, verbose):

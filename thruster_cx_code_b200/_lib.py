@@ -86,6 +86,9 @@ PROTOTYPES = {
     "pb_sim_counts": (i32, [vp, P(i32), P(i32), P(u32), P(u32)]),
     "pb_sim_reserve": (i32, [vp, i32, i32]),
     "pb_sim_rebuild_operator": (i32, [vp]),
+    "pb_sim_mg_stats": (i32, [vp, P(C.c_int64)]),
+    "pb_sim_batch_share": (i32, [vp, P(f64)]),
+    "pb_sim_operator_digest": (i32, [vp, P(u64)]),
     "pb_sim_field_ptr": (i32, [vp, i32, P(vp)]),
     "pb_sim_get_field": (i32, [vp, i32, vp, C.c_int64]),
     "pb_sim_set_field": (i32, [vp, i32, vp, C.c_int64]),

@@ -16,6 +16,9 @@ struct pb_batch {
   PoissonArgs* dargs = nullptr;  // device copy of every field-solve argument block of a run
   PoissonArgs* hargs = nullptr;  // pinned staging
   size_t args_cap = 0, dargs_cap = 0;
+  MgRebuildArgs* dmg = nullptr;  // the hierarchy-rebuild argument blocks, one beside each of the above
+  MgRebuildArgs* hmg = nullptr;
+  size_t mg_cap = 0, dmg_cap = 0;
   int* dblk = nullptr;           // block -> argument-block maps of every launch of a run
   int* hblk = nullptr;
   size_t blk_cap = 0, dblk_cap = 0;
@@ -36,6 +39,7 @@ struct pb_batch {
     uint64_t key = 0;
     cudaGraphExec_t exec = nullptr;
     PoissonArgs* dargs = nullptr;     // the step's field-solve argument blocks, owned by the graph
+    MgRebuildArgs* dmg = nullptr;     // and the hierarchy-rebuild blocks beside them
     int* dblk = nullptr;
     pb_step_report** dreps = nullptr; // the members' report buffers, gathered at the end of the step
     std::vector<long long> launches;  // kernels of each member in the step
@@ -63,6 +67,42 @@ struct SolveLaunch {
 
 // Blocks of one launch shared out in proportion to each instance's node count (at least
 // one block each, at most the instance's own full-device grid).
+// After a batch run: block-ns per field-solve launch of the run's solves (their counters
+// were cleared at its start).
+static int32_t measure_solve(Sim* s) {
+  unsigned long long ns[2] = {0, 0};
+  CK(cudaMemcpy(ns, s->solve_ns, sizeof(ns), cudaMemcpyDeviceToHost));
+  if (ns[1] > 0) s->solve_work = (double)ns[0] / (double)ns[1];
+  return PB_OK;
+}
+
+// Work of one field-solve launch of each instance, for its block share: the block-ns its
+// solves took in the last batch run it was part of (quantised to steps of 2^(1/4), so that
+// the shares, and with them the captured step graphs, change only when the cost does), or,
+// for an instance not yet measured, its node count times the median block-ns per node of
+// the measured ones (its node count alone when none is measured).
+std::vector<long> solve_work(pb_sim* const* sims, const std::vector<int>& inst) {
+  std::vector<double> ratio;
+  for (int i : inst) {
+    const Sim* s = &sims[i]->s;
+    if (s->solve_work > 0.0) ratio.push_back(s->solve_work / ((double)s->ny * s->nx));
+  }
+  double med = 0.0;
+  if (!ratio.empty()) {
+    std::sort(ratio.begin(), ratio.end());
+    med = ratio[ratio.size() / 2];
+  }
+  std::vector<long> work;
+  for (int i : inst) {
+    const Sim* s = &sims[i]->s;
+    const double nodes = (double)s->ny * s->nx;
+    double w = s->solve_work > 0.0 ? s->solve_work : (med > 0.0 ? med * nodes : nodes);
+    if (med > 0.0 || s->solve_work > 0.0) w = std::exp2(std::round(4.0 * std::log2(std::max(w, 1.0))) / 4.0);
+    work.push_back((long)std::min(w, 1e15));
+  }
+  return work;
+}
+
 std::vector<int> share_blocks(const std::vector<long>& work, int total) {
   const int m = (int)work.size();
   std::vector<int> nb(m, 1);
@@ -105,7 +145,8 @@ int64_t sim_device_bytes(const Sim* s) {
     b += Nl * 4 * (1 + (l ? 2 : 0));  // dinv; r and z below the fine level
     b += Nl * 4 * ((s->lev[l].R ? 25 : 0) + (s->lev[l].U ? 18 : 0));
   }
-  b += (int64_t)s->nc * s->nc * 4;
+  b += (int64_t)s->ncap * s->ncap * (4 + 8);  // coarsest inverse and the rebuild's dense scratch
+  for (size_t l = 1; l < s->lev.size(); ++l) b += (int64_t)s->lev[l].ny * s->lev[l].nx * (1 + 9 * 4);
   b += 4LL * (int64_t)s->sort_cap * 4 + (int64_t)s->hist_cap * 4 + 2LL * (int64_t)s->tile_cap * 8;
   b += (int64_t)s->see_cap * 16 + (int64_t)s->angle_cap * 8;
   return b;
@@ -126,6 +167,7 @@ void free_batch_graphs(pb_batch* b) {
   for (auto& g : b->graphs) {
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.dargs) cudaFree(g.dargs);
+    if (g.dmg) cudaFree(g.dmg);
     if (g.dblk) cudaFree(g.dblk);
     if (g.dreps) cudaFree(g.dreps);
   }
@@ -145,6 +187,26 @@ int32_t grow_pinned(T** p, size_t* cap, size_t need) {
 
 }  // namespace
 
+// The hierarchy rebuild of the instances of one solve launch, on the launch's blocks, before
+// their field solve (when any of them has had sputter breaks; a clean instance returns at once).
+static int32_t launch_mg_rebuild_batch(pb_batch* b, pb_sim* const* sims, const SolveLaunch& L,
+                                       const MgRebuildArgs* dm, const int* db, bool capturing) {
+  bool any = false;
+  for (int i : L.inst) any = any || sims[i]->s.erosion_seen;
+  if (!any) return PB_OK;
+  void* kargs[] = {(void*)&dm, (void*)&db};
+  if (capturing) {
+    CK(cudaLaunchCooperativeKernel((void*)k_mg_rebuild_batch, dim3(L.nblocks), dim3(PT), kargs, 0, b->stream));
+  } else if (int32_t rc = coop_launch(b->device, b->stream, [&]() {
+               return cudaLaunchCooperativeKernel((void*)k_mg_rebuild_batch, dim3(L.nblocks), dim3(PT), kargs, 0,
+                                                  b->stream);
+             })) {
+    return rc;
+  }
+  ++b->launches;
+  return PB_OK;
+}
+
 // ------------------------------------------------------------------ batch steps as graphs
 // One step of every member: fork from the batch stream, the pre-solve halves on the members'
 // streams, the step's cooperative field-solve launches on the batch stream, the post-solve
@@ -153,8 +215,8 @@ int32_t grow_pinned(T** p, size_t* cap, size_t need) {
 // each member's step_dev, which the captured step advances), or directly otherwise.
 static int32_t enqueue_batch_step(pb_batch* b, pb_sim* const* sims, int n, const pb_step_params* const* P,
                                   const std::vector<const SolveLaunch*>& Ls, const PoissonArgs* dargs,
-                                  const int* dblk, size_t args0, size_t blk0, pb_step_report** dreps,
-                                  bool capturing, std::vector<long long>* launches) {
+                                  const MgRebuildArgs* dmg, const int* dblk, size_t args0, size_t blk0,
+                                  pb_step_report** dreps, bool capturing, std::vector<long long>* launches) {
   int32_t rc;
   CK(cudaEventRecord(b->ev_fork, b->stream));
   for (int i = 0; i < n; ++i) CK(cudaStreamWaitEvent(sims[i]->s.stream, b->ev_fork, 0));
@@ -173,6 +235,7 @@ static int32_t enqueue_batch_step(pb_batch* b, pb_sim* const* sims, int n, const
     }
     const PoissonArgs* da = dargs + (L.args_off - args0);
     const int* db = dblk + (L.blk_off - blk0);
+    if ((rc = launch_mg_rebuild_batch(b, sims, L, dmg + (L.args_off - args0), db, capturing))) return rc;
     void* kargs[] = {(void*)&da, (void*)&db};
     if (capturing) {
       CK(cudaLaunchCooperativeKernel((void*)k_poisson_batch, dim3(L.nblocks), dim3(PT), kargs, L.smem, b->stream));
@@ -236,6 +299,7 @@ static int32_t batch_run_graphs(pb_batch* b, pb_sim* const* sims, int n, const p
       key = fnv_v(key, params_digest(P[i]));
       key = fnv_v(key, state_signature(sims[i]));
     }
+    key = fnv(key, b->hblk + blk0, nblk * sizeof(int));  // the step's block shares
     pb_batch::StepGraph* g = nullptr;
     for (auto& e : b->graphs)
       if (e.key == key) g = &e;
@@ -255,6 +319,7 @@ static int32_t batch_run_graphs(pb_batch* b, pb_sim* const* sims, int n, const p
         s->counts_valid = true;
         s->sp_dx = P[i]->dx;
         s->sp_dy = P[i]->dy;
+        if (P[i]->erosion_on) s->erosion_seen = true;
         s->launches += g->launches[i];
       }
       CK(cudaGraphLaunch(g->exec, b->stream));
@@ -265,21 +330,22 @@ static int32_t batch_run_graphs(pb_batch* b, pb_sim* const* sims, int n, const p
       ng.key = key;
       ng.launches.assign(n, 0);
       CK(dcopy(&ng.dargs, b->hargs + args0, nargs));
+      CK(dcopy(&ng.dmg, b->hmg + args0, nargs));
       CK(dcopy(&ng.dblk, b->hblk + blk0, nblk));
       CK(dcopy(&ng.dreps, reps.data(), (size_t)n));
       // host state of the members, restored if the step cannot be captured
-      std::vector<std::array<double, 6>> saved(n);
+      std::vector<std::array<double, 7>> saved(n);
       for (int i = 0; i < n; ++i) {
         const Sim* s = &sims[i]->s;
         saved[i] = {(double)s->sp[0].cur, (double)s->sp[1].cur, (double)s->counts_valid, s->sp_dx, s->sp_dy,
-                    (double)s->launches};
+                    (double)s->launches, (double)s->erosion_seen};
       }
       const long long bl0 = b->launches;
       cudaError_t ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
       int32_t crc = ce == cudaSuccess ? PB_OK : PB_ERR_CUDA;
       if (crc == PB_OK) {
         for (int i = 0; i < n; ++i) sims[i]->s.capturing = 1;
-        crc = enqueue_batch_step(b, sims, n, P.data(), Ls, ng.dargs, ng.dblk, args0, blk0, ng.dreps, true,
+        crc = enqueue_batch_step(b, sims, n, P.data(), Ls, ng.dargs, ng.dmg, ng.dblk, args0, blk0, ng.dreps, true,
                                  &ng.launches);
         for (int i = 0; i < n; ++i) sims[i]->s.capturing = 0;
         cudaGraph_t graph = nullptr;
@@ -299,10 +365,11 @@ static int32_t batch_run_graphs(pb_batch* b, pb_sim* const* sims, int n, const p
           s->sp[0].cur = (int)saved[i][0]; s->sp[1].cur = (int)saved[i][1];
           s->counts_valid = saved[i][2] != 0.0; s->sp_dx = saved[i][3]; s->sp_dy = saved[i][4];
           s->launches = (long long)saved[i][5];
+          s->erosion_seen = saved[i][6] != 0.0;
         }
         b->launches = bl0;
         if (ng.exec) cudaGraphExecDestroy(ng.exec);
-        cudaFree(ng.dargs); cudaFree(ng.dblk); cudaFree(ng.dreps);
+        cudaFree(ng.dargs); cudaFree(ng.dmg); cudaFree(ng.dblk); cudaFree(ng.dreps);
       } else {
         if (b->graphs.size() >= 16) free_batch_graphs(b);
         ng.own_launches = b->launches - bl0;
@@ -314,7 +381,8 @@ static int32_t batch_run_graphs(pb_batch* b, pb_sim* const* sims, int n, const p
     if (b->graphs_broken && !g) {
       // enqueue this step directly (arguments from the run's device copy)
       for (int i = 0; i < n; ++i) sims[i]->s.step_dev_val = -1;
-      if ((rc = enqueue_batch_step(b, sims, n, P.data(), Ls, b->dargs, b->dblk, 0, 0, dreps_run, false, nullptr))) {
+      if ((rc = enqueue_batch_step(b, sims, n, P.data(), Ls, b->dargs, b->dmg, b->dblk, 0, 0, dreps_run, false,
+                                   nullptr))) {
         cudaFree(dreps_run);
         return rc;
       }
@@ -352,8 +420,10 @@ int32_t pb_batch_destroy(pb_batch* b) {
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->dargs) cudaFree(b->dargs);
+  if (b->dmg) cudaFree(b->dmg);
   if (b->dblk) cudaFree(b->dblk);
   if (b->hargs) cudaFreeHost(b->hargs);
+  if (b->hmg) cudaFreeHost(b->hmg);
   if (b->hblk) cudaFreeHost(b->hblk);
   if (b->hrep) cudaFreeHost(b->hrep);
   free_batch_graphs(b);
@@ -412,6 +482,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     }
   }
   if ((rc = grow_pinned(&b->hargs, &b->args_cap, std::max<size_t>(nargs, 1)))) return rc;
+  if ((rc = grow_pinned(&b->hmg, &b->mg_cap, std::max<size_t>(nargs, 1)))) return rc;
   if ((rc = grow_pinned(&b->hblk, &b->blk_cap, std::max<size_t>(nblk, 1)))) return rc;
   if (b->dargs_cap < b->args_cap) {
     if (b->dargs) CK(cudaFree(b->dargs));
@@ -419,6 +490,13 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     b->dargs_cap = 0;
     CK(cudaMalloc((void**)&b->dargs, b->args_cap * sizeof(PoissonArgs)));
     b->dargs_cap = b->args_cap;
+  }
+  if (b->dmg_cap < b->mg_cap) {
+    if (b->dmg) CK(cudaFree(b->dmg));
+    b->dmg = nullptr;
+    b->dmg_cap = 0;
+    CK(cudaMalloc((void**)&b->dmg, b->mg_cap * sizeof(MgRebuildArgs)));
+    b->dmg_cap = b->mg_cap;
   }
   if (b->dblk_cap < b->blk_cap) {
     if (b->dblk) CK(cudaFree(b->dblk));
@@ -428,20 +506,23 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     b->dblk_cap = b->blk_cap;
   }
   for (const SolveLaunch& L : plan) {
-    std::vector<long> work;
-    for (int i : L.inst) work.push_back((long)sims[i]->s.ny * sims[i]->s.nx);
-    std::vector<int> nb = share_blocks(work, L.nblocks);
+    std::vector<int> nb = share_blocks(solve_work(sims, L.inst), L.nblocks);
     int blk0 = 0;
     for (size_t j = 0; j < L.inst.size(); ++j) {
       Sim* s = &sims[L.inst[j]]->s;
       const pb_step_params& p = params[(size_t)L.inst[j] * K + L.step];
       PoissonArgs a = poisson_args(s, p.picard_iters, &p);
-      if (nb[j] > s->pgrid) return fail(PB_ERR_STATE, "pb_batch_run: block share above the instance's grid");
+      if (nb[j] > s->num_sms) return fail(PB_ERR_STATE, "pb_batch_run: block share above the device's SM count");
       a.blk0 = blk0;
       a.nblk = nb[j];
       set_up_tiles(s, &a);
-      a.trace = nullptr;
+      a.trace = s->trace_on ? s->ptrace : nullptr;  // traced members run without graphs
       b->hargs[L.args_off + j] = a;
+      MgRebuildArgs m = mg_rebuild_args(s);
+      m.blk0 = blk0;
+      m.nblk = nb[j];
+      b->hmg[L.args_off + j] = m;
+      s->batch_blocks = nb[j];
       for (int q = 0; q < nb[j]; ++q) b->hblk[L.blk_off + blk0 + q] = (int)j;
       blk0 += nb[j];
     }
@@ -469,7 +550,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       if ((rc = check_step_params(&sims[i]->s, &params[(size_t)i * K + k]))) return rc;
   bool use_graphs = b->graphs_on != 0;
   for (int i = 0; i < n; ++i)
-    if (sims[i]->s.profiling) use_graphs = false;
+    if (sims[i]->s.profiling || sims[i]->s.trace_on) use_graphs = false;
   if (use_graphs) {
     // the report ring (its address is part of every graph)
     if ((size_t)K * n > b->ring_cap) {
@@ -486,6 +567,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     CK(cudaEventRecord(b->ev0, b->stream));
     if (nargs > 0) {
       CK(cudaMemcpyAsync(b->dargs, b->hargs, nargs * sizeof(PoissonArgs), cudaMemcpyHostToDevice, b->stream));
+      CK(cudaMemcpyAsync(b->dmg, b->hmg, nargs * sizeof(MgRebuildArgs), cudaMemcpyHostToDevice, b->stream));
       CK(cudaMemcpyAsync(b->dblk, b->hblk, nblk * sizeof(int), cudaMemcpyHostToDevice, b->stream));
     }
     CK(cudaMemsetAsync(b->slot, 0, sizeof(int), b->stream));
@@ -494,6 +576,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       s->mark_used = 0;
       s->launches = 0;
       CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), b->stream));
+      CK(cudaMemsetAsync(s->solve_ns, 0, 2 * sizeof(unsigned long long), b->stream));
     }
     b->launches = 0;
     if ((rc = batch_run_graphs(b, sims, n, params, K, plan))) return rc;
@@ -509,6 +592,8 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       Sim* s = &sims[i]->s;
       b->launches += s->launches;
       if ((rc = read_counts(s))) return rc;
+      if ((rc = settle_mg(s))) return rc;
+      if ((rc = measure_solve(s))) return rc;
     }
     if (reports) {
       for (int i = 0; i < n; ++i)
@@ -529,6 +614,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
   CK(cudaEventRecord(b->ev0, b->stream));
   if (nargs > 0) {
     CK(cudaMemcpyAsync(b->dargs, b->hargs, nargs * sizeof(PoissonArgs), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->dmg, b->hmg, nargs * sizeof(MgRebuildArgs), cudaMemcpyHostToDevice, b->stream));
     CK(cudaMemcpyAsync(b->dblk, b->hblk, nblk * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   }
   for (int i = 0; i < n; ++i) {
@@ -536,6 +622,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     s->mark_used = 0;
     s->launches = 0;
     CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), b->stream));
+    CK(cudaMemsetAsync(s->solve_ns, 0, 2 * sizeof(unsigned long long), b->stream));
   }
   CK(cudaEventRecord(b->ev_solve[0], b->stream));
   for (int i = 0; i < n; ++i) CK(cudaStreamWaitEvent(sims[i]->s.stream, b->ev_solve[0], 0));
@@ -556,6 +643,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       }
       const PoissonArgs* da = b->dargs + L.args_off;
       const int* db = b->dblk + L.blk_off;
+      if ((rc = launch_mg_rebuild_batch(b, sims, L, b->dmg + L.args_off, db, false))) return rc;
       void* kargs[] = {(void*)&da, (void*)&db};
       CK(cudaEventRecord(b->tev[2 * pi], b->stream));
       if ((rc = coop_launch(b->device, b->stream, [&]() {
@@ -596,6 +684,8 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     Sim* s = &sims[i]->s;
     b->launches += s->launches;
     if ((rc = read_counts(s))) return rc;
+    if ((rc = settle_mg(s))) return rc;
+    if ((rc = measure_solve(s))) return rc;
   }
   if (reports) {
     std::memcpy(reports, b->hrep, (size_t)n * K * sizeof(pb_step_report));

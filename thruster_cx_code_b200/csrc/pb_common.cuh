@@ -48,6 +48,34 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// ---------------------------------------------------------------- grid barrier
+// Barrier of the nblk blocks of a cooperative launch (or of one instance's contiguous range
+// of blocks in a launch that serves several) on one 32-bit word: block gb == 0 adds
+// 2^31 - (nblk - 1), the others add 1, so the top bit flips once every block has arrived and
+// the low bits return to their start.  Arrival is a release, the poll an acquire: stores made
+// by any thread of an arriving block before the barrier are visible to every thread after
+// it.  The wait is bounded: on time-out PB_EF_SPIN_TIMEOUT is set in *err, and this and every
+// later barrier stop waiting, so the kernel runs to completion and the host sees the flag.
+constexpr long long GRID_SPIN_LIMIT = 1ll << 22;
+
+__device__ __forceinline__ void grid_sync(unsigned int* bar, uint32_t* err, int nblk, int gb) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned int inc = gb == 0 ? (0x80000000u - (unsigned int)(nblk - 1)) : 1u;
+    unsigned int old, cur;
+    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(inc) : "memory");
+    for (long long spin = 0;; ++spin) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
+      if ((old ^ cur) & 0x80000000u) break;
+      if ((spin & 255) == 255) {
+        if ((*(volatile uint32_t*)err & PB_EF_SPIN_TIMEOUT) != 0u) break;
+        if (spin > GRID_SPIN_LIMIT) { atomicOr(err, PB_EF_SPIN_TIMEOUT); break; }
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------- TMA tensor copies
 // A tile of a tensor in global memory copied into shared memory by the TMA unit, its
 // completion tracked by an mbarrier (one arrival with the byte count, then the copy's

@@ -282,9 +282,11 @@ __global__ void k_erosion_break(double* damage, uint8_t* isBound, uint8_t* cls, 
 // symmetric positive definite: its smoother part is, once every free node has its weight,
 // and the coarse part adds a semidefinite term.  The weights are the host build's,
 // omega / (4 - Neumann neighbours) in double rounded to float, 0 off the free nodes.
-__global__ void k_refresh_dinv0(const uint8_t* cls, float* dinv, int ny, int nx, int periodic, const int* broken) {
+__global__ void k_refresh_dinv0(const uint8_t* cls, float* dinv, int ny, int nx, int periodic, const int* broken,
+                                int* mg_dirty) {
   pdl_enter();
   if (*broken == 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *mg_dirty = 1;  // the coarse levels follow before the next solve
   const int N = ny * nx;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
     float d = 0.0f;

@@ -33,14 +33,9 @@
 
 namespace pb {
 
-constexpr long long BAR_SPIN_LIMIT = 1ll << 22;
-constexpr int FU = 4;  // fine-level nodes per thread and pass of the vector loops (their loads overlap)
+constexpr int FU = 1;  // fine-level nodes per thread and pass of the vector loops (4 measured slower on 257 x 1025)
 constexpr float W_KEEP = (float)(1.0 - MG_JACOBI_OMEGA);
 
-// Grid barrier on one 32-bit word per instance: its block 0 adds 2^31 - (nblocks - 1), the others add 1,
-// so the top bit flips once every block has arrived and the low bits return to their
-// start.  Arrival is a release, the poll an acquire: stores made by any thread of an
-// arriving block before the barrier are visible to every thread after it.
 // Block index within this instance's group of blocks (a launch may solve several
 // instances, each on its own contiguous range of blocks).
 __device__ __forceinline__ int gbid(const PoissonArgs& a) { return (int)blockIdx.x - a.blk0; }
@@ -53,25 +48,19 @@ __device__ __forceinline__ int gtid(const PoissonArgs& a) {
   return (((int)threadIdx.x >> 5) * a.nblk + gbid(a)) * 32 + ((int)threadIdx.x & 31);
 }
 
-__device__ __forceinline__ void grid_barrier(const PoissonArgs& a) {
-  unsigned int* bar = a.bar;
-  uint32_t* err = a.errflags;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned int inc = gbid(a) == 0 ? (0x80000000u - (unsigned int)(a.nblk - 1)) : 1u;
-    unsigned int old, cur;
-    asm volatile("atom.release.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(bar), "r"(inc) : "memory");
-    for (long long spin = 0;; ++spin) {
-      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(cur) : "l"(bar) : "memory");
-      if ((old ^ cur) & 0x80000000u) break;
-      if ((spin & 255) == 255) {
-        if ((*(volatile uint32_t*)err & PB_EF_SPIN_TIMEOUT) != 0u) break;
-        if (spin > BAR_SPIN_LIMIT) { atomicOr(err, PB_EF_SPIN_TIMEOUT); break; }
-      }
-    }
-  }
-  __syncthreads();
+// Reductions run over a fixed set of a.nvb virtual blocks (the device's SM count), whatever
+// the number of blocks the instance runs on: virtual block v owns the nodes that the
+// grid-stride mapping gives block v of an nvb-block launch, its partial is summed in the same
+// order by whichever block runs it, and the totals add the nvb partials in a fixed order.  So
+// every dot product, and with them the solve, has the same bits on any block count: a batch
+// member equals its solo run, and the field-solve block count is a pure speed knob.  Block b
+// runs the virtual blocks b, b + nblk, ...; with nblk = nvb the mapping is gtid's.
+__device__ __forceinline__ int vtid(const PoissonArgs& a, int v) {
+  return (((int)threadIdx.x >> 5) * a.nvb + v) * 32 + ((int)threadIdx.x & 31);
 }
+
+// grid barrier of this instance's blocks (grid_sync: bounded, release/acquire)
+__device__ __forceinline__ void grid_barrier(const PoissonArgs& a) { grid_sync(a.bar, a.errflags, a.nblk, gbid(a)); }
 
 // phase tracing (block 0, thread 0): time since the previous mark is added to trace[k]
 __device__ __forceinline__ void tmark(const PoissonArgs& a, int k) {
@@ -90,8 +79,9 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Block partials of up to two values into ring slot `slot` (read after the next barrier).
-__device__ __forceinline__ void put_partials(const PoissonArgs& a, int slot, double v0, double v1) {
+// Partials of virtual block v, up to two values, into ring slot `slot` (read after the next
+// barrier); called by every thread of the block.
+__device__ __forceinline__ void put_partials(const PoissonArgs& a, int slot, int v, double v0, double v1) {
   __shared__ double sm[2][PT / 32];
   v0 = warp_sum(v0);
   v1 = warp_sum(v1);
@@ -103,28 +93,29 @@ __device__ __forceinline__ void put_partials(const PoissonArgs& a, int slot, dou
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
     if (threadIdx.x == 0) {
-      double* part = a.partials + (size_t)(slot & 3) * 2 * a.nblk;
-      part[gbid(a)] = s0;
-      part[a.nblk + gbid(a)] = s1;
+      double* part = a.partials + (size_t)(slot & 3) * 2 * a.nvb;
+      part[v] = s0;
+      part[a.nvb + v] = s1;
     }
   }
+  __syncthreads();  // sm is reused by the next virtual block's call
 }
 
 // Grid totals of a slot, after a barrier; the same order in every block.
 __device__ __forceinline__ void get_sums(const PoissonArgs& a, int slot, double& t0, double& t1) {
   __shared__ double bc[2];
   if (threadIdx.x < 32) {
-    const double* part = a.partials + (size_t)(slot & 3) * 2 * a.nblk;
+    const double* part = a.partials + (size_t)(slot & 3) * 2 * a.nvb;
     double s0 = 0.0, s1 = 0.0;
     // all of a lane's loads issued before the first add (one L2 round trip for up to 256
-    // blocks); the adds keep the order b = lane, lane + 32, ...
-    for (int base = 0; base < a.nblk; base += 256) {
+    // virtual blocks); the adds keep the order v = lane, lane + 32, ...
+    for (int base = 0; base < a.nvb; base += 256) {
       double v0[8], v1[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int b = base + q * 32 + (int)threadIdx.x;
-        v0[q] = b < a.nblk ? __ldcg(part + b) : 0.0;
-        v1[q] = b < a.nblk ? __ldcg(part + a.nblk + b) : 0.0;
+        v0[q] = b < a.nvb ? __ldcg(part + b) : 0.0;
+        v1[q] = b < a.nvb ? __ldcg(part + a.nvb + b) : 0.0;
       }
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -255,18 +246,16 @@ __device__ __forceinline__ float prolong(const MgLevel& C, const float* zc, int 
 // The block forms m once per node of its tile and a one-node halo in shared memory (a node's
 // m is used by the five stars that contain it), then z from the tile.  The tiles are
 // a.ut_y x a.ut_x nearly equal rectangles, dealt to the blocks in turn; each holds at most
-// UP_TILE_MAX nodes with its halo.
-// With nu0 = 2 the pre-smoothed correction is d (r + s), s = r - A d r (a.s32), and this leg
-// writes the once post-smoothed m2 to a.m32; smooth0 applies the second post-sweep.
-__device__ double up_leg0_tiled(const PoissonArgs& a, const float* r0) {
+// UP_TILE_MAX nodes with its halo.  up_tile0 does tile t and returns this thread's part of
+// (r, z) over the tile's nodes when nu0 = 1.
+__device__ double up_tile0(const PoissonArgs& a, const float* r0, int t, bool two) {
   __shared__ float mt[UP_TILE_MAX];
-  const bool two = a.nu0 == 2;
   float* out = two ? a.m32 : a.lev[0].z;
   const MgLevel& F = a.lev[0];
   const MgLevel& C = a.lev[1];
   const int ny = F.ny, nx = F.nx, nty = a.ut_y, ntx = a.ut_x;
   double rz = 0.0;
-  for (int t = gbid(a); t < nty * ntx; t += a.nblk) {
+  {
     const int ty = t / ntx, tx = t - ty * ntx;
     const int y0 = (int)((long long)ty * ny / nty), y1 = (int)((long long)(ty + 1) * ny / nty);
     const int x0 = (int)((long long)tx * nx / ntx), x1 = (int)((long long)(tx + 1) * nx / ntx);
@@ -299,6 +288,23 @@ __device__ double up_leg0_tiled(const PoissonArgs& a, const float* r0) {
   return rz;
 }
 
+// With nu0 = 2 the pre-smoothed correction is d (r + s), s = r - A d r (a.s32), and this leg
+// writes the once post-smoothed m2 to a.m32; smooth0 applies the second post-sweep and the
+// partial of (r, z).  With nu0 = 1 this leg leaves that partial in `slot`: the tiles are then
+// laid out for nvb blocks and tile t belongs to virtual block t mod nvb.
+__device__ void up_leg0_tiled(const PoissonArgs& a, const float* r0, int slot) {
+  const bool two = a.nu0 == 2;
+  if (two) {
+    for (int t = gbid(a); t < a.ut_y * a.ut_x; t += a.nblk) up_tile0(a, r0, t, true);
+    return;
+  }
+  for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+    double rz = 0.0;
+    for (int t = v; t < a.ut_y * a.ut_x; t += a.nvb) rz += up_tile0(a, r0, t, false);
+    put_partials(a, slot, v, rz, 0.0);
+  }
+}
+
 // Second fine-level pre-sweep (nu0 = 2): s = r - A (d r) on the free nodes, i.e.
 // s_i = (1 - w) r_i + sum_{k nbr of i} d_k r_k (d is zero off the free nodes).
 __device__ void presmooth0(const PoissonArgs& a, const float* r, float* s_out, int tid, int nth) {
@@ -329,12 +335,13 @@ __device__ void presmooth0(const PoissonArgs& a, const float* r, float* s_out, i
 }
 
 // Second fine-level post-sweep (nu0 = 2): z = m + d (r - A m) = (1 - w) m + d (r + sum_nbr m)
-// from m = a.m32 (zero off the active nodes); returns the partial of (r, z).
-__device__ double smooth0(const PoissonArgs& a, const float* r, int tid, int nth) {
+// from m = a.m32 (zero off the active nodes); leaves the partials of (r, z) in `slot`.
+__device__ void smooth0(const PoissonArgs& a, const float* r, int slot) {
   const MgLevel& F = a.lev[0];
-  const int N = F.ny * F.nx;
+  const int N = F.ny * F.nx, nth = a.nvb * (int)blockDim.x;
+  for (int v = gbid(a); v < a.nvb; v += a.nblk) {
   double rz = 0.0;
-  for (int i0 = tid; i0 < N; i0 += FU * nth) {
+  for (int i0 = vtid(a, v); i0 < N; i0 += FU * nth) {
     float zv[FU], rv[FU];
 #pragma unroll
     for (int u = 0; u < FU; ++u) {
@@ -356,7 +363,8 @@ __device__ double smooth0(const PoissonArgs& a, const float* r, int tid, int nth
       rz += (double)rv[u] * (double)zv[u];
     }
   }
-  return rz;
+  put_partials(a, slot, v, rz, 0.0);
+  }
 }
 
 // Levels >= 1: the same transfers from the host-built stencils (R on the coarse level,
@@ -430,23 +438,15 @@ __device__ void down_leg(const PoissonArgs& a, int level, int tid, int nth, cons
   }
 }
 
-// grid-wide up leg: z_l from r_l and z_{l+1}; on level 0 (residual r0) also the partial
-// of (r, z)
-template <bool LV0>
-__device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth, const float* r0 = nullptr) {
+// grid-wide up leg of level l >= 1: z_l from r_l and z_{l+1}
+__device__ void up_leg(const PoissonArgs& a, int level, int tid, int nth) {
   const MgLevel& F = a.lev[level];
   const MgLevel& C = a.lev[level + 1];
   const int N = F.ny * F.nx;
-  double rz = 0.0;
-  if (LV0) {
-    rz = up_leg0_tiled(a, r0);
-  } else {
-    for (int i = tid; i < N; i += nth) {
-      const int y = i / F.nx, x = i - y * F.nx;
-      __stcg(F.z + i, smooth_up_pre(F, C, F.r, C.z, y, x, i));
-    }
+  for (int i = tid; i < N; i += nth) {
+    const int y = i / F.nx, x = i - y * F.nx;
+    __stcg(F.z + i, smooth_up_pre(F, C, F.r, C.z, y, x, i));
   }
-  return rz;
 }
 
 // ----------------------------------------------------------------- coarsest level
@@ -455,7 +455,7 @@ __device__ double up_leg(const PoissonArgs& a, int level, int tid, int nth, cons
 // to the blocks in turn) takes the dot product with that row of the dense inverse.
 // Inactive nodes of z_c are never written (zero since allocation).
 __device__ void coarse_solve(const PoissonArgs& a, const float* rlev, float* zlev, float* rcs) {
-  const int nc = a.nc;
+  const int nc = __ldg(a.nc_dev);
   for (int k = threadIdx.x; k < nc; k += blockDim.x) rcs[k] = *(rlev + __ldg(a.cidx + k));
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -484,14 +484,16 @@ __device__ void coarse_solve(const PoissonArgs& a, const float* rlev, float* zle
 // Leaves the partial of (r0, z) in `slot` and ends with a barrier.
 __device__ void vcycle_below(const PoissonArgs& a, float* rcs, int slot, const float* r0) {
   const int tid = gtid(a), nth = a.nblk * blockDim.x;
-  double rz = 0.0;
   const int last = a.nlevels - 1;
   if (last == 0) {
     coarse_solve(a, r0, a.z32, rcs);
     grid_barrier(a);
-    const int N = a.ny * a.nx;
-    for (int i = tid; i < N; i += nth) rz += (double)(*(r0 + i)) * (double)(*(a.z32 + i));
-    put_partials(a, slot, rz, 0.0);
+    const int N = a.ny * a.nx, nv = a.nvb * (int)blockDim.x;
+    for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+      double rz = 0.0;
+      for (int i = vtid(a, v); i < N; i += nv) rz += (double)(*(r0 + i)) * (double)(*(a.z32 + i));
+      put_partials(a, slot, v, rz, 0.0);
+    }
     grid_barrier(a);
     return;
   }
@@ -504,16 +506,15 @@ __device__ void vcycle_below(const PoissonArgs& a, float* rcs, int slot, const f
   grid_barrier(a);
   tmark(a, 7);
   for (int l = last - 1; l >= 1; --l) {
-    up_leg<false>(a, l, tid, nth);
+    up_leg(a, l, tid, nth);
     grid_barrier(a);
     tmark(a, 8 + (l < 7 ? l : 6));
   }
-  rz = up_leg<true>(a, 0, tid, nth, r0);
+  up_leg0_tiled(a, r0, slot);  // nu0 = 1: the partials of (r, z)
   if (a.nu0 == 2) {
     grid_barrier(a);
-    rz = smooth0(a, r0, tid, nth);
+    smooth0(a, r0, slot);
   }
-  put_partials(a, slot, rz, 0.0);
   grid_barrier(a);
   tmark(a, 8);
 }
@@ -523,9 +524,12 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   extern __shared__ float4 dyn_smem[];
   float* rcs = reinterpret_cast<float*>(dyn_smem);  // nc floats: the coarsest r, gathered
   const int tid = gtid(a), nth = a.nblk * blockDim.x;
+  const int nv = a.nvb * (int)blockDim.x;  // stride of a virtual block's nodes (reduction loops)
   const int N = a.ny * a.nx;
   int slot = 0;
   double n_outer = 0, n_inner = 0, last_rel = 0;
+  unsigned long long t_start = 0;
+  if (gbid(a) == 0 && threadIdx.x == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
   tmark(a, 20);
 
   // Dirichlet-neighbour sums (V_fixed is constant during the launch)
@@ -544,25 +548,28 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   for (int pic = 0; pic < a.iterations; ++pic) {
     const double inner_at_pic = n_inner, outer_at_pic = n_outer;
     // right-hand side from the Boltzmann electron density of the current V, residual
-    double ff = 0.0, rr = 0.0;
-    for (int i = tid; i < N; i += nth) {
-      if (__ldg(a.cls + i) != NC_FREE) continue;
-      double Vi = (*(a.V + i));
-      double vm = Vi < a.V_plasma ? Vi : a.V_plasma;
-      double rho_e = DMUL(a.qn0_neg, exp(DDIV(DSUB(vm, a.V_plasma), a.Te_up)));
-      double rt = DADD((double)__ldg(a.rho + i), rho_e);
-      double fi = DMUL(a.coeff, rt) + a.dirsum[i];
-      __stcg(a.f + i, fi);
-      ff += fi * fi;
+    for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+      const int t0 = vtid(a, v);
+      double ff = 0.0, rr = 0.0;
+      for (int i = t0; i < N; i += nv) {
+        if (__ldg(a.cls + i) != NC_FREE) continue;
+        double Vi = (*(a.V + i));
+        double vm = Vi < a.V_plasma ? Vi : a.V_plasma;
+        double rho_e = DMUL(a.qn0_neg, exp(DDIV(DSUB(vm, a.V_plasma), a.Te_up)));
+        double rt = DADD((double)__ldg(a.rho + i), rho_e);
+        double fi = DMUL(a.coeff, rt) + a.dirsum[i];
+        __stcg(a.f + i, fi);
+        ff += fi * fi;
+      }
+      for (int i = t0; i < N; i += nv) {
+        if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
+        const int y = i / a.nx, x = i - y * a.nx;
+        double res = (*(a.f + i)) - apply0<double>(a, a.x, i, y, x);
+        __stcg(a.r32 + i, (float)res);
+        rr += res * res;
+      }
+      put_partials(a, slot, v, ff, rr);
     }
-    for (int i = tid; i < N; i += nth) {
-      if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
-      const int y = i / a.nx, x = i - y * a.nx;
-      double res = (*(a.f + i)) - apply0<double>(a, a.x, i, y, x);
-      __stcg(a.r32 + i, (float)res);
-      rr += res * res;
-    }
-    put_partials(a, slot, ff, rr);
     grid_barrier(a);
     double fnorm2, rnorm2;
     get_sums(a, slot++, fnorm2, rnorm2);
@@ -589,54 +596,58 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
         double rz;
         get_sums(a, slot++, rz, dummy);
         const double beta = k == 0 ? 0.0 : rz / rz_old;
-        double pq_p = 0.0;
         // FU nodes per thread and pass: every load of the pass is issued before the first
         // store, so the loads of different nodes overlap (the sums keep the node order)
-        for (int i0 = tid; i0 < N; i0 += FU * nth) {
-          float pv[FU], qv[FU];
+        for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+          double pq_p = 0.0;
+          for (int i0 = vtid(a, v); i0 < N; i0 += FU * nv) {
+            float pv[FU], qv[FU];
 #pragma unroll
-          for (int u = 0; u < FU; ++u) {
-            const int i = i0 + u * nth < N ? i0 + u * nth : i0;
-            const int y = i / a.nx, x = i - y * a.nx;
-            const bool fr = __ldg(a.cls + i) == NC_FREE;
-            const float az = apply0<float>(a, a.z32, i, y, x);
-            const float zi = *(a.z32 + i);
-            pv[u] = fr ? zi + (float)beta * (k == 0 ? 0.0f : (*(a.p32 + i))) : 0.0f;
-            qv[u] = fr ? az + (float)beta * (k == 0 ? 0.0f : (*(a.q32 + i))) : 0.0f;
-          }
+            for (int u = 0; u < FU; ++u) {
+              const int i = i0 + u * nv < N ? i0 + u * nv : i0;
+              const int y = i / a.nx, x = i - y * a.nx;
+              const bool fr = __ldg(a.cls + i) == NC_FREE;
+              const float az = apply0<float>(a, a.z32, i, y, x);
+              const float zi = *(a.z32 + i);
+              pv[u] = fr ? zi + (float)beta * (k == 0 ? 0.0f : (*(a.p32 + i))) : 0.0f;
+              qv[u] = fr ? az + (float)beta * (k == 0 ? 0.0f : (*(a.q32 + i))) : 0.0f;
+            }
 #pragma unroll
-          for (int u = 0; u < FU; ++u) {
-            if (i0 + u * nth >= N) continue;
-            __stcg(a.p32 + i0 + u * nth, pv[u]);
-            __stcg(a.q32 + i0 + u * nth, qv[u]);
-            pq_p += (double)pv[u] * (double)qv[u];
+            for (int u = 0; u < FU; ++u) {
+              if (i0 + u * nv >= N) continue;
+              __stcg(a.p32 + i0 + u * nv, pv[u]);
+              __stcg(a.q32 + i0 + u * nv, qv[u]);
+              pq_p += (double)pv[u] * (double)qv[u];
+            }
           }
+          put_partials(a, slot, v, pq_p, 0.0);
         }
-        put_partials(a, slot, pq_p, 0.0);
         grid_barrier(a);
         double pq;
         get_sums(a, slot++, pq, dummy);
         const double alpha = pq != 0.0 ? rz / pq : 0.0;
-        double rr_p = 0.0;
-        for (int i0 = tid; i0 < N; i0 += FU * nth) {
-          float ev[FU], rv[FU];
-          bool fr[FU];
+        for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+          double rr_p = 0.0;
+          for (int i0 = vtid(a, v); i0 < N; i0 += FU * nv) {
+            float ev[FU], rv[FU];
+            bool fr[FU];
 #pragma unroll
-          for (int u = 0; u < FU; ++u) {
-            const int i = i0 + u * nth < N ? i0 + u * nth : i0;
-            fr[u] = i0 + u * nth < N && __ldg(a.cls + i) == NC_FREE;
-            ev[u] = (*(a.e32 + i)) + (float)alpha * (*(a.p32 + i));
-            rv[u] = (*(a.r32 + i)) - (float)alpha * (*(a.q32 + i));
-          }
+            for (int u = 0; u < FU; ++u) {
+              const int i = i0 + u * nv < N ? i0 + u * nv : i0;
+              fr[u] = i0 + u * nv < N && __ldg(a.cls + i) == NC_FREE;
+              ev[u] = (*(a.e32 + i)) + (float)alpha * (*(a.p32 + i));
+              rv[u] = (*(a.r32 + i)) - (float)alpha * (*(a.q32 + i));
+            }
 #pragma unroll
-          for (int u = 0; u < FU; ++u) {
-            if (!fr[u]) continue;
-            __stcg(a.e32 + i0 + u * nth, ev[u]);
-            __stcg(a.r32 + i0 + u * nth, rv[u]);
-            rr_p += (double)rv[u] * (double)rv[u];
+            for (int u = 0; u < FU; ++u) {
+              if (!fr[u]) continue;
+              __stcg(a.e32 + i0 + u * nv, ev[u]);
+              __stcg(a.r32 + i0 + u * nv, rv[u]);
+              rr_p += (double)rv[u] * (double)rv[u];
+            }
           }
+          put_partials(a, slot, v, rr_p, 0.0);
         }
-        put_partials(a, slot, rr_p, 0.0);
         grid_barrier(a);
         double rrk;
         get_sums(a, slot++, rrk, dummy);
@@ -653,15 +664,17 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
       for (int i = tid; i < N; i += nth)
         if (__ldg(a.cls + i) == NC_FREE) __stcg(a.x + i, (*(a.x + i)) + (double)(*(a.e32 + i)));
       grid_barrier(a);
-      rr = 0.0;
-      for (int i = tid; i < N; i += nth) {
-        if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
-        const int y = i / a.nx, x = i - y * a.nx;
-        double res = (*(a.f + i)) - apply0<double>(a, a.x, i, y, x);
-        __stcg(a.r32 + i, (float)res);
-        rr += res * res;
+      for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+        double rr = 0.0;
+        for (int i = vtid(a, v); i < N; i += nv) {
+          if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
+          const int y = i / a.nx, x = i - y * a.nx;
+          double res = (*(a.f + i)) - apply0<double>(a, a.x, i, y, x);
+          __stcg(a.r32 + i, (float)res);
+          rr += res * res;
+        }
+        put_partials(a, slot, v, rr, 0.0);
       }
-      put_partials(a, slot, rr, 0.0);
       grid_barrier(a);
       get_sums(a, slot++, rnorm2, dummy);
       tmark(a, 16);
@@ -724,6 +737,12 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
     a.stats[1] += n_inner;
     a.stats[2] = last_rel;
     a.stats[3] += (double)a.iterations;
+  }
+  if (gbid(a) == 0 && threadIdx.x == 0) {
+    unsigned long long t_end;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_end));
+    a.solve_ns[0] += (t_end - t_start) * (unsigned long long)a.nblk;  // block-ns
+    a.solve_ns[1] += 1;
   }
 }
 

@@ -52,21 +52,71 @@ struct PoissonArgs {
   // hierarchy
   int nlevels;            // including level 0 and the coarsest
   MgLevel lev[MG_MAX_LEVELS];
-  int nc;                 // coarsest active count (<= MG_MAX_COARSE)
+  const int* nc_dev;      // coarsest active count nc (<= MG_MAX_COARSE), in device memory: the
+                          // hierarchy rebuild on the device may change it between launches
   const int* cidx;        // coarsest active node indices
   const float* cinv;      // coarsest inverse (nc x nc, exactly symmetric)
   // this instance's blocks in the launch and its reductions and barrier
   int blk0, nblk;         // first block and number of blocks
-  int ut_y, ut_x;         // tiles of the fine-level up leg (fine_up_tiles)
-  double* partials;       // 4 slots x 2 values x nblk doubles
+  int nvb;                // virtual blocks of the reductions (the device's SM count, >= nblk):
+                          // the order of every sum, whatever nblk is
+  int ut_y, ut_x;         // tiles of the fine-level up leg (fine_up_tiles for nblk blocks, or
+                          // for nvb when nu0 = 1: its tiles then carry the (r, z) partials)
+  double* partials;       // 4 slots x 2 values x nvb doubles
   unsigned int* bar;      // barrier word, zero at launch (its low bits must start at zero)
   uint32_t* errflags;
   double* stats;          // [outer its, inner its, final rel residual, solves] accumulated
+  unsigned long long* solve_ns;  // [block-ns, launches] of this instance's solves (block 0's clock
+                                 // times the instance's block count)
   unsigned long long* trace;  // optional: ns per phase category (block 0), [31] = last stamp
 };
 
 // dynamic shared memory of k_poisson: the coarsest right-hand side gathered by each block
+// (sized for the capacity of the coarsest level, which a rebuild on the device may fill)
 inline size_t mg_coarse_smem_bytes(int nc) { return 4 * (size_t)(nc > 0 ? nc : 1); }
+
+// ---------------------------------------------------------------- rebuild on the device
+// Arrays of one level for k_mg_rebuild: the hierarchy the solve reads (dinv, R, U, z) and
+// the rebuild's own scratch (act, st).
+struct MgBuildLevel {
+  int ny, nx, per, wrapP;
+  float* dinv;            // omega / diagonal on active nodes (levels >= 1 written here)
+  float* R;               // levels >= 2: fused-cycle restriction, 25 planes (or null)
+  float* U;               // levels >= 1 with a coarser level: prolongation + smoothing, 18 planes
+  float* z;               // correction (the coarsest level's is cleared by a rebuild)
+  uint8_t* act;           // levels >= 1, scratch: bit 0 = a parent of an active finer node, bit 1 = active
+  float* st;              // levels >= 1, scratch: Galerkin 9-point stencil, st[k * N + i]
+};
+
+// slots of MgRebuildArgs::counts
+enum : int {
+  MG_CNT_FLAGS = MG_MAX_LEVELS,   // bit 0: coupling outside the 9-point pattern, bit 1: not SPD
+  MG_CNT_REBUILDS,                // rebuilds completed on the device (cumulative)
+  MG_CNT_DEFERRED,                // rebuilds left to the host (cumulative)
+  MG_CNT_SLOTS = 32
+};
+// MgRebuildArgs::status bit: the freed nodes change the level structure; the host rebuilds
+constexpr uint32_t MG_STATUS_HOST = 1u;
+
+struct MgRebuildArgs {
+  int nlevels, max_coarse, ncap;  // ncap: capacity of the coarsest level (cidx, cinv, dense)
+  const uint8_t* cls;             // level-0 node classes (updated by the cell break)
+  MgBuildLevel lev[MG_MAX_LEVELS];
+  int* cidx;                      // coarsest active node indices (ncap)
+  float* cinv;                    // coarsest inverse (ncap^2 floats, row stride nc)
+  int* nc_dev;                    // coarsest active count
+  double* dense;                  // scratch ncap^2: the coarsest operator, its Cholesky factor
+                                  // (lower triangle) and the columns of its inverse (upper)
+  double* mdiag;                  // scratch ncap: diagonal of the inverse factor
+  int* cidx_new;                  // scratch ncap
+  int* pos;                       // scratch, one per node of the coarsest level
+  int* counts;                    // MG_CNT_SLOTS ints: active counts per level, flags, totals
+  int* dirty;                     // set when cells break; cleared by the rebuild
+  uint32_t* status;               // MG_STATUS_HOST
+  unsigned int* bar;              // barrier word, zero at launch
+  uint32_t* errflags;
+  int blk0, nblk;
+};
 
 // Tiling of the fine-level up leg: at most UP_TILE_MAX nodes per tile with its one-node halo.
 constexpr int UP_TILE_MAX = 4096;
@@ -117,6 +167,10 @@ __global__ void k_poisson(const __grid_constant__ PoissonArgs a);
 // Several instances in one launch: block b solves instance blk_inst[b] together with the
 // other blocks of that instance's contiguous range (args[i].blk0, args[i].nblk).
 __global__ void k_poisson_batch(const PoissonArgs* __restrict__ args, const int* __restrict__ blk_inst);
+// The hierarchy rebuilt from the node classes after cells broke (no-op unless *dirty), on
+// every block of the launch, or per instance as k_poisson_batch.
+__global__ void k_mg_rebuild(const __grid_constant__ MgRebuildArgs a);
+__global__ void k_mg_rebuild_batch(const MgRebuildArgs* __restrict__ args, const int* __restrict__ blk_inst);
 #endif
 
 }  // namespace pb

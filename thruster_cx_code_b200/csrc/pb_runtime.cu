@@ -63,6 +63,8 @@ struct DevLevel {
   float* U = nullptr;
   float* r = nullptr;
   float* z = nullptr;
+  uint8_t* act = nullptr;  // scratch of the device rebuild (levels >= 1)
+  float* st = nullptr;
 };
 
 struct Sim {
@@ -86,12 +88,26 @@ struct Sim {
   int *ppc = nullptr, *cnt_i = nullptr, *cnt_e = nullptr;
   // multigrid
   std::vector<DevLevel> lev;
-  int nc = 0;
+  int nc = 0;             // coarsest active count of the last host build (nc_dev holds the current one)
+  int ncap = 0;           // capacity of the coarsest level (cidx, cinv and the rebuild's dense scratch)
   int* cidx = nullptr;
   float* cinv = nullptr;
+  int* nc_dev = nullptr;
+  // rebuild of the hierarchy on the device after cells break (k_mg_rebuild)
+  double* mg_dense = nullptr;
+  double* mg_mdiag = nullptr;
+  int *mg_cidx_new = nullptr, *mg_pos = nullptr;
+  int* mg_counts = nullptr;      // MG_CNT_SLOTS (persist across host builds)
+  int* mg_dirty = nullptr;
+  uint32_t* mg_status = nullptr;
+  bool erosion_seen = false;     // a step with sputter breaks was enqueued: field solves rebuild first
+  long long mg_host_rebuilds = 0;
   double* partials = nullptr;
   unsigned int* bar = nullptr;
   double* pstats = nullptr;
+  unsigned long long* solve_ns = nullptr;  // [block-ns, launches] of the field solves (k_poisson*)
+  double solve_work = 0.0;    // block-ns of one field-solve launch, measured in the last batch run
+  int batch_blocks = 0;       // this instance's block share in the last batch launch planned
   unsigned long long* ptrace = nullptr;  // field-solve phase trace (32 slots)
   int trace_on = 0;
   int pgrid = 0;      // blocks of the field-solve launch (<= num_sms)
@@ -330,11 +346,17 @@ static void free_levels(Sim* s) {
     dfree(s->lev[l].dinv);
     dfree(s->lev[l].R);
     dfree(s->lev[l].U);
+    dfree(s->lev[l].act);
+    dfree(s->lev[l].st);
     if (l > 0) { dfree(s->lev[l].r); dfree(s->lev[l].z); }
   }
   s->lev.clear();
   dfree(s->cidx);
   dfree(s->cinv);
+  dfree(s->mg_dense);
+  dfree(s->mg_mdiag);
+  dfree(s->mg_cidx_new);
+  dfree(s->mg_pos);
 }
 
 // node classes from isBound (host copy) and the multigrid hierarchy
@@ -380,26 +402,72 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
       CK(dalloc(&D.r, N)); CK(dalloc(&D.z, N));
       CK(cudaMemset(D.r, 0, N * sizeof(float)));
       CK(cudaMemset(D.z, 0, N * sizeof(float)));
+      CK(dalloc(&D.act, N));
+      CK(dalloc(&D.st, 9 * N));
     }
   }
   s->nc = (int)H.cidx.size();
-  s->psmem = mg_coarse_smem_bytes(s->nc);
+  // the coarsest level grows as cells break (more free nodes): room for a quarter more than
+  // max(nc, max_coarse) nodes for the device rebuild, within the dense solve's limit
+  s->ncap = std::min(MG_MAX_COARSE, std::max(s->nc, s->max_coarse) * 5 / 4);
+  s->psmem = mg_coarse_smem_bytes(s->ncap);
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_poisson, PT, s->psmem));
   if (occ < 1) return fail(PB_ERR_ARG, "field solver: no resident block with " + std::to_string(s->psmem) +
                                            " bytes of shared memory");
-  CK(dalloc(&s->cidx, s->nc));
-  CK(dalloc(&s->cinv, (size_t)s->nc * s->nc));
+  const size_t ncap = (size_t)s->ncap;
+  CK(dalloc(&s->cidx, ncap));
+  CK(dalloc(&s->cinv, ncap * ncap));
   CK(cudaMemcpy(s->cidx, H.cidx.data(), s->nc * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(s->cinv, H.cinv.data(), (size_t)s->nc * s->nc * sizeof(float), cudaMemcpyHostToDevice));
+  CK(dalloc(&s->mg_dense, ncap * ncap));
+  CK(dalloc(&s->mg_mdiag, ncap));
+  CK(dalloc(&s->mg_cidx_new, ncap));
+  CK(dalloc(&s->mg_pos, (size_t)H.lev.back().ny * H.lev.back().nx));
+  if (!s->nc_dev) CK(dalloc(&s->nc_dev, 1));
+  if (!s->mg_counts) {
+    CK(dalloc(&s->mg_counts, MG_CNT_SLOTS));
+    CK(cudaMemset(s->mg_counts, 0, MG_CNT_SLOTS * sizeof(int)));
+  }
+  if (!s->mg_dirty) CK(dalloc(&s->mg_dirty, 1));
+  if (!s->mg_status) CK(dalloc(&s->mg_status, 1));
+  CK(cudaMemcpy(s->nc_dev, &s->nc, sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemset(s->mg_dirty, 0, sizeof(int)));
+  CK(cudaMemset(s->mg_status, 0, sizeof(uint32_t)));
   return PB_OK;
 }
 
-// the fine up-leg tiling of a.nblk blocks, computed once per grid shape and block count
+// Arguments of k_mg_rebuild for this simulator's hierarchy (the field solve's blocks).
+static MgRebuildArgs mg_rebuild_args(Sim* s) {
+  MgRebuildArgs a{};
+  a.nlevels = (int)s->lev.size();
+  a.max_coarse = s->max_coarse;
+  a.ncap = s->ncap;
+  a.cls = s->cls;
+  for (size_t l = 0; l < s->lev.size() && l < (size_t)MG_MAX_LEVELS; ++l) {
+    const DevLevel& D = s->lev[l];
+    MgBuildLevel& B = a.lev[l];
+    B.ny = D.ny; B.nx = D.nx; B.per = D.per; B.wrapP = D.wrapP;
+    B.dinv = D.dinv; B.R = D.R; B.U = D.U; B.z = D.z; B.act = D.act; B.st = D.st;
+  }
+  a.cidx = s->cidx; a.cinv = s->cinv; a.nc_dev = s->nc_dev;
+  a.dense = s->mg_dense; a.mdiag = s->mg_mdiag; a.cidx_new = s->mg_cidx_new; a.pos = s->mg_pos;
+  a.counts = s->mg_counts; a.dirty = s->mg_dirty; a.status = s->mg_status;
+  a.bar = s->bar;
+  a.errflags = &s->rep_dev->errflags;
+  a.blk0 = 0;
+  a.nblk = s->pgrid;
+  return a;
+}
+
+// the fine up-leg tiling, computed once per grid shape and block count: for the launch's
+// a.nblk blocks, or for the a.nvb virtual blocks when one smoothing sweep (nu = 1) makes
+// that leg carry the (r, z) partials
 static void set_up_tiles(Sim* s, PoissonArgs* a) {
-  if (s->ut_key[0] != s->ny || s->ut_key[1] != s->nx || s->ut_key[2] != a->nblk) {
-    fine_up_tiles(s->ny, s->nx, a->nblk, &s->ut[0], &s->ut[1]);
-    s->ut_key[0] = s->ny; s->ut_key[1] = s->nx; s->ut_key[2] = a->nblk;
+  const int nb = a->nu0 == 2 ? a->nblk : a->nvb;
+  if (s->ut_key[0] != s->ny || s->ut_key[1] != s->nx || s->ut_key[2] != nb) {
+    fine_up_tiles(s->ny, s->nx, nb, &s->ut[0], &s->ut[1]);
+    s->ut_key[0] = s->ny; s->ut_key[1] = s->nx; s->ut_key[2] = nb;
   }
   a->ut_y = s->ut[0];
   a->ut_x = s->ut[1];
@@ -426,12 +494,14 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
     a.lev[l].R = D.R;
     a.lev[l].U = D.U;
   }
-  a.nc = s->nc; a.cidx = s->cidx; a.cinv = s->cinv;
+  a.nc_dev = s->nc_dev; a.cidx = s->cidx; a.cinv = s->cinv;
   a.blk0 = 0; a.nblk = s->pgrid;
+  a.nvb = s->num_sms;
   set_up_tiles(s, &a);
   a.partials = s->partials; a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
   a.stats = s->pstats;
+  a.solve_ns = s->solve_ns;
   a.trace = s->trace_on ? s->ptrace : nullptr;
   return a;
 }
@@ -457,25 +527,36 @@ static int32_t coop_launch(int device, cudaStream_t st, Launch launch) {
   return PB_OK;
 }
 
-static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
-  if (iterations <= 0) return PB_OK;
-  PoissonArgs a = poisson_args(s, iterations, p);
+// A cooperative launch of the field-solve grid: inside a step graph ordered by the
+// simulator's own stream (a graph runs its simulator alone, so no other cooperative launch
+// is chained against it), otherwise through the device's chain.
+static int32_t coop_field_launch(Sim* s, const void* kernel, void** args, size_t smem) {
   CK(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned int), s->stream));
-  void* args[] = {&a};
-  int32_t rc;
   if (s->capturing) {
-    // inside a step graph: ordered by the simulator's own stream (a graph runs its
-    // simulator alone, so no other cooperative launch is chained against it)
-    CK(cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream));
-    rc = PB_OK;
+    CK(cudaLaunchCooperativeKernel(kernel, dim3(s->pgrid), dim3(PT), args, smem, s->stream));
   } else {
-    rc = coop_launch(s->device, s->stream, [&]() {
-      return cudaLaunchCooperativeKernel((void*)k_poisson, dim3(s->pgrid), dim3(PT), args, s->psmem, s->stream);
+    int32_t rc = coop_launch(s->device, s->stream, [&]() {
+      return cudaLaunchCooperativeKernel(kernel, dim3(s->pgrid), dim3(PT), args, smem, s->stream);
     });
+    if (rc) return rc;
   }
-  if (rc) return rc;
   ++s->launches;
   return PB_OK;
+}
+
+static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
+  if (iterations <= 0) return PB_OK;
+  int32_t rc;
+  if (s->erosion_seen) {
+    // cells may have broken since the last solve: the hierarchy follows the node classes
+    // first (k_mg_rebuild returns at once unless a break set mg_dirty)
+    MgRebuildArgs m = mg_rebuild_args(s);
+    void* margs[] = {&m};
+    if ((rc = coop_field_launch(s, (const void*)k_mg_rebuild, margs, 0))) return rc;
+  }
+  PoissonArgs a = poisson_args(s, iterations, p);
+  void* args[] = {&a};
+  return coop_field_launch(s, (const void*)k_poisson, args, s->psmem);
 }
 
 // The per-step resets in one launch instead of a dozen memsets (each of which is an
@@ -832,8 +913,9 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
     CK(launch_pdl(k_erosion_break, grid_for(s, N, 256), 256, 0, st, s->damage, s->isBound, s->cls, s->eroded, s->ny,
                   s->nx, s->periodic, p->thresh, p->dy, &rep->broken));
     CK(launch_pdl(k_refresh_dinv0, grid_for(s, N, 256), 256, 0, st, s->cls, s->lev[0].dinv, s->ny, s->nx, s->periodic,
-                                                         &rep->broken));
+                                                         &rep->broken, s->mg_dirty));
     s->launches += 2;
+    s->erosion_seen = true;
   }
   mark(s);
 
@@ -956,13 +1038,15 @@ static uint64_t state_signature(const pb_sim* h) {
                         s->tile_counter, s->see_key, s->see_xy, s->see_count, s->angles, s->angle_scratch,
                         s->angle_count, s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1],
                         s->sval[0], s->sval[1], s->shist, s->sblk, s->rep_dev, h->cx.t, h->cx.c, h->see.t,
-                        h->see.c, s->step_dev, s->ekeep};
+                        h->see.c, s->step_dev, s->ekeep, s->nc_dev, s->mg_dense, s->mg_mdiag, s->mg_cidx_new,
+                        s->mg_pos, s->mg_counts, s->mg_dirty, s->mg_status};
   k = fnv(k, ptrs, sizeof(ptrs));
   for (const DevLevel& L : s->lev) k = fnv_v(k, L);
   const long long vals[] = {s->ny, s->nx, s->periodic, s->ngrids, s->nc, s->trace_on, s->pgrid, s->ut[0], s->ut[1],
                             s->pbps, s->ppb, (long long)s->kopts, (long long)s->psmem, (long long)s->tile_cap, s->see_cap,
                             s->angle_cap, (long long)s->sort_cap, (long long)s->hist_cap, s->counts_valid ? 1 : 0,
-                            s->max_outer, s->max_inner, s->nu, h->cx.nt, h->see.nt, s->profiling};
+                            s->max_outer, s->max_inner, s->nu, h->cx.nt, h->see.nt, s->profiling, s->ncap,
+                            s->max_coarse, s->erosion_seen ? 1 : 0};
   k = fnv(k, vals, sizeof(vals));
   const double dv[] = {s->tol, s->tol_inner, h->cx.lo, h->cx.hi, h->cx.cmax, h->see.lo, h->see.hi};
   k = fnv(k, dv, sizeof(dv));
@@ -1002,6 +1086,7 @@ static int32_t graph_step(pb_sim* h, const pb_step_params* p, bool* done) {
     s->counts_valid = true;
     s->sp_dx = p->dx;
     s->sp_dy = p->dy;
+    if (p->erosion_on) s->erosion_seen = true;
     s->launches += g.launches;
     s->step_dev_val = (long long)(uint32_t)p->iteration + 1;
     ++s->graph_replays;
@@ -1013,6 +1098,7 @@ static int32_t graph_step(pb_sim* h, const pb_step_params* p, bool* done) {
   const int cur0 = s->sp[0].cur, cur1 = s->sp[1].cur;
   const bool cv0 = s->counts_valid;
   const double dx0 = s->sp_dx, dy0 = s->sp_dy;
+  const bool es0 = s->erosion_seen;
   const long long l0 = s->launches;
   if (s->graphs.size() >= 8) free_graphs(s);
   cudaError_t ce = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
@@ -1040,7 +1126,7 @@ static int32_t graph_step(pb_sim* h, const pb_step_params* p, bool* done) {
     s->graph_error = rc != PB_OK ? g_err : std::string("step capture: ") + cudaGetErrorString(ce);
     cudaGetLastError();
     s->sp[0].cur = cur0; s->sp[1].cur = cur1;
-    s->counts_valid = cv0; s->sp_dx = dx0; s->sp_dy = dy0; s->launches = l0;
+    s->counts_valid = cv0; s->sp_dx = dx0; s->sp_dy = dy0; s->erosion_seen = es0; s->launches = l0;
     return PB_OK;
   }
   Sim::StepGraph g;
@@ -1099,9 +1185,11 @@ int32_t pb_sim_create(pb_sim** out, int32_t device) {
   CK(cudaFuncSetAttribute((const void*)k_poisson, cudaFuncAttributePreferredSharedMemoryCarveout,
                           (int)cudaSharedmemCarveoutMaxL1));
   s->pgrid = s->num_sms;
-  CK(dalloc(&s->partials, 4 * 2 * (size_t)s->pgrid));
+  CK(dalloc(&s->partials, 4 * 2 * (size_t)s->num_sms));
   CK(dalloc(&s->bar, 2));
   CK(dalloc(&s->pstats, 4));
+  CK(dalloc(&s->solve_ns, 2));
+  CK(cudaMemset(s->solve_ns, 0, 2 * sizeof(unsigned long long)));
   CK(dalloc(&s->ptrace, 32));
   CK(cudaMemset(s->ptrace, 0, 32 * sizeof(unsigned long long)));
   CK(cudaMemset(s->pstats, 0, 4 * sizeof(double)));
@@ -1155,7 +1243,8 @@ int32_t pb_sim_destroy(pb_sim* h) {
   void* v[] = {s->isBound, s->bdist, s->bdist_tmp, s->cls, s->gridmask, s->ppc, s->cnt_i, s->cnt_e, s->bar, s->counts, s->next_ids,
                s->tile_status, s->tile_counter, s->see_key, s->see_count, s->angle_scratch, s->angle_count,
                s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1], s->sval[0], s->sval[1],
-               s->shist, s->sblk, s->rep_dev, h->cx.t, h->cx.c, h->see.t, h->see.c};
+               s->shist, s->sblk, s->rep_dev, h->cx.t, h->cx.c, h->see.t, h->see.c, s->solve_ns, s->nc_dev,
+               s->mg_counts, s->mg_dirty, s->mg_status, s->ptrace};
   for (void* q : v) if (q) cudaFree(q);
   for (int k = 0; k < 2; ++k)
     for (int b = 0; b < 2; ++b) {
@@ -1313,6 +1402,22 @@ int32_t pb_sim_set_domain(pb_sim* h, int32_t ny, int32_t nx, int32_t periodic, c
   CK(cudaStreamSynchronize(s->stream));
   s->domain_set = true;
   s->counts_valid = false;
+  return PB_OK;
+}
+
+// After a run: a break whose freed nodes change the level structure was left to the host
+// by k_mg_rebuild (MG_STATUS_HOST); rebuild the hierarchy here before the next solve.
+static int32_t settle_mg(Sim* s) {
+  if (!s->erosion_seen || !s->mg_status) return PB_OK;
+  uint32_t st = 0;
+  CK(cudaMemcpyAsync(&st, s->mg_status, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (!(st & MG_STATUS_HOST)) return PB_OK;
+  std::vector<uint8_t> ib((size_t)s->ny * s->nx);
+  CK(cudaMemcpy(ib.data(), s->isBound, ib.size(), cudaMemcpyDeviceToHost));
+  if (int32_t rc = build_operator(s, ib.data())) return rc;
+  CK(cudaStreamSynchronize(s->stream));
+  ++s->mg_host_rebuilds;
   return PB_OK;
 }
 
@@ -1505,6 +1610,7 @@ int32_t pb_sim_step(pb_sim* h, const pb_step_params* p, pb_step_report* report) 
     float ms = 0.0f;
     CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     s->last_ms = ms;
+    if ((rc = settle_mg(s))) return rc;
   }
   return PB_OK;
 }
@@ -1540,6 +1646,7 @@ int32_t pb_sim_run(pb_sim* h, const pb_step_params* params, int32_t nsteps, pb_s
   CK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
   s->last_ms = ms;
   if ((rc = read_counts(s))) return rc;
+  if ((rc = settle_mg(s))) return rc;
   if (reports) {
     std::memcpy(reports, s->rep_run, (size_t)nsteps * sizeof(pb_step_report));
     for (int k = 0; k < nsteps; ++k)
@@ -1690,6 +1797,64 @@ int32_t pb_sim_phase_times(pb_sim* h, double* out10) {
   double steps = 0.0;
   if (int32_t rc = phase_sums(s, out10, &steps)) return rc;
   out10[PB_MARKS - 1] = steps;
+  return PB_OK;
+}
+
+int32_t pb_sim_batch_share(pb_sim* h, double* out2) {
+  if (!out2) return fail(PB_ERR_ARG, "pb_sim_batch_share: null output");
+  out2[0] = h->s.solve_work * 1e-6;
+  out2[1] = h->s.batch_blocks;
+  return PB_OK;
+}
+
+int32_t pb_sim_mg_stats(pb_sim* h, int64_t* out4) {
+  Sim* s = &h->s;
+  if (!out4) return fail(PB_ERR_ARG, "pb_sim_mg_stats: null output");
+  if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_mg_stats: no domain");
+  int c[MG_CNT_SLOTS];
+  int nc = 0;
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaMemcpy(c, s->mg_counts, sizeof(c), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&nc, s->nc_dev, sizeof(int), cudaMemcpyDeviceToHost));
+  out4[0] = c[MG_CNT_REBUILDS];
+  out4[1] = c[MG_CNT_DEFERRED];
+  out4[2] = s->mg_host_rebuilds;
+  out4[3] = nc;
+  return PB_OK;
+}
+
+// FNV-1a over the bytes the field solve reads of the hierarchy: per level the smoother
+// weights and the transfer stencils, then the coarsest count, index set and inverse.
+int32_t pb_sim_operator_digest(pb_sim* h, uint64_t* out) {
+  Sim* s = &h->s;
+  if (!out) return fail(PB_ERR_ARG, "pb_sim_operator_digest: null output");
+  if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_operator_digest: no domain");
+  CK(cudaStreamSynchronize(s->stream));
+  uint64_t k = 1469598103934665603ull;
+  std::vector<float> buf;
+  auto add_dev = [&](const float* p, size_t n) -> cudaError_t {
+    buf.resize(n);
+    cudaError_t e = cudaMemcpy(buf.data(), p, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) k = fnv(k, buf.data(), n * sizeof(float));
+    return e;
+  };
+  const int L = (int)s->lev.size();
+  k = fnv_v(k, L);
+  for (int l = 0; l < L; ++l) {
+    const DevLevel& D = s->lev[l];
+    const size_t N = (size_t)D.ny * D.nx;
+    CK(add_dev(D.dinv, N));
+    if (D.R) CK(add_dev(D.R, 25 * N));
+    if (D.U) CK(add_dev(D.U, 18 * N));
+  }
+  int nc = 0;
+  CK(cudaMemcpy(&nc, s->nc_dev, sizeof(int), cudaMemcpyDeviceToHost));
+  k = fnv_v(k, nc);
+  std::vector<int> ci((size_t)std::max(nc, 1));
+  CK(cudaMemcpy(ci.data(), s->cidx, (size_t)nc * sizeof(int), cudaMemcpyDeviceToHost));
+  k = fnv(k, ci.data(), (size_t)nc * sizeof(int));
+  CK(add_dev(s->cinv, (size_t)nc * nc));
+  *out = k;
   return PB_OK;
 }
 
