@@ -236,10 +236,10 @@ def timed_run(sim, params, K, profile=True):
     n_p0, n_e0 = sim.num_p, sim.num_e
     stats_before = list(sim.last_report.poisson_stats) if sim.last_report is not None else None
     lib.pb_sim_set_profiling(sim._h, 1 if profile else 0)
-    mg0 = (C.c_int64 * 4)()
+    mg0 = (C.c_int64 * 8)()
     _lib.check(lib.pb_sim_mg_stats(sim._h, mg0), "pb_sim_mg_stats")
     _lib.check(lib.pb_sim_run(sim._h, P, K, R), "pb_sim_run")
-    mg1 = (C.c_int64 * 4)()
+    mg1 = (C.c_int64 * 8)()
     _lib.check(lib.pb_sim_mg_stats(sim._h, mg1), "pb_sim_mg_stats")
     tm = (C.c_double * 9)()
     lib.pb_sim_timing(sim._h, tm)
@@ -257,7 +257,9 @@ def timed_run(sim, params, K, profile=True):
             "ions_per_launch": float(np.mean(ions)), "eles_per_launch": float(np.mean(eles)),
             "stats_before": stats_before, "cells_broken": int(sum(r.broken for r in R)),
             "mg_rebuilds": {"device": int(mg1[0] - mg0[0]), "left_to_host": int(mg1[1] - mg0[1]),
-                            "host": int(mg1[2] - mg0[2])}}
+                            "host": int(mg1[2] - mg0[2]),
+                            "device_ms": {k: (mg1[4 + j] - mg0[4 + j]) / 1e3 for j, k in
+                                          enumerate(("levels", "cholesky", "inverse", "transfer"))}}}
 
 
 def kernel_rooflines(run, K, peak, traffic):
@@ -450,6 +452,10 @@ def poisson_section(sim, stats_before, reports, field_ms, peak):
 
 # ----------------------------------------------------------------------------- sweeps
 SWEEP_WARMUP, SWEEP_STEPS, SWEEP_REF_STEPS = 3, 40, 3000
+# warm-up of each batched form: 20 steps hold every step shape (field solve or not, buffer
+# parity, the sort step), so the graph form captures before the timed steps, and the block
+# shares come from a measured run
+SWEEP_WARMUP_BATCH = 20
 # a request retires when the 500-step means of its saddle potential and beamlet current
 # change by less than 0.5% from one 500 steps to the next
 SERVE_RATE_HZ, SERVE_WINDOW, SERVE_TOL, SERVE_CHUNK = 20.0, 1000, 5e-3, 50
@@ -484,7 +490,7 @@ def sweep_section(device, args):
     3e16-3e17 m^-3, grids drawn from {64x256, 128x512, 256x1024} cells and 0.2M-4M
     macro-particles log-uniform.  Plain: each point alone through pb_sim_run (3 warm-up
     steps, then 40 timed).  Batched: all points together through pb_batch_run, from the
-    state the plain steps left (3 warm-up steps, then 40 timed), first with every member's
+    state the plain steps left (20 warm-up steps, then 40 timed), first with every member's
     kernels enqueued on its own stream, then with each batch step shape captured as one CUDA
     graph and replayed (the warm-up steps capture); the faster form is the one reported as
     batched, both are listed.  Rates use device time, scaled to 3000
@@ -505,9 +511,11 @@ def sweep_section(device, args):
     plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes, plain_solve) for s, p in built)
     def batched(graphs):
         batch.set_graphs(graphs)
-        batch.run(sims, prm, SWEEP_WARMUP)
+        batch.run(sims, prm, SWEEP_WARMUP_BATCH)
         n0 = [(s.num_p, s.num_e) for s in sims]
+        g0 = batch.graph_stats()
         res = batch.run(sims, prm, SWEEP_STEPS)
+        batched.timed_captures = batch.graph_stats()[0] - g0[0]
         pushes = sum(SV.pushes_of([rep for _, rep in r], a, b) for r, (a, b) in zip(res, n0))
         batched.solve_ms = batch.last_solve_ms
         return batch.last_ms, batch.last_host_ms, pushes
@@ -522,6 +530,7 @@ def sweep_section(device, args):
     streams_solve_ms = batched.solve_ms
     graph_ms, graph_host_ms, graph_pushes = batched(True)
     graph_solve_ms = batched.solve_ms
+    graph_timed_captures = batched.timed_captures
     g_stats = batch.graph_stats()
     # the batched form reported: the faster of the two (graphs only when no capture failed)
     use_graphs = not g_stats[2] and graph_ms < streams_ms
@@ -548,13 +557,14 @@ def sweep_section(device, args):
            "solver": {"plain_max_coarse": 1536, "batched_max_coarse": args.batch_max_coarse,
                       "smoother_sweeps": SMOOTHER_SWEEPS},
            "graph_captures_replays_failed": list(g_stats),
+           "graph_captures_in_timed_steps": graph_timed_captures,
            "streams": {"points_per_hr": 3600.0 / (streams_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts),
                        "device_ms": streams_ms, "host_enqueue_ms": streams_host_ms,
                        "field_solve_ms": streams_solve_ms,
                        "over_plain": plain_ms / streams_ms},
            "graphs": {"points_per_hr": 3600.0 / (graph_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts),
                       "device_ms": graph_ms, "host_enqueue_ms": graph_host_ms,
-                      "field_solve_ms": graph_solve_ms,
+                      "field_solve_ms": graph_solve_ms if graph_solve_ms >= 0 else None,
                       "over_plain": plain_ms / graph_ms},
            "setup": f"excluded ({t_setup:.1f} s of host geometry, multigrid build and pre-load on 8 threads)"}
     for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms),

@@ -235,10 +235,12 @@ int32_t pb_sim_set_spline(pb_sim* s, int32_t which, int32_t nt, const double* t,
  * host build, max_coarse), those calls run this host build before returning (the solves
  * before it use the device's rebuild with the old level count, or the old hierarchy). */
 int32_t pb_sim_rebuild_operator(pb_sim* s);
-/* out4: hierarchy rebuilds done on the device, rebuilds left to the host, host rebuilds
- * run after pb_sim_run / pb_sim_step / pb_batch_run for them, and the current coarsest
- * active count. */
-int32_t pb_sim_mg_stats(pb_sim* s, int64_t* out4);
+/* out8: hierarchy rebuilds done on the device, rebuilds left to the host, host rebuilds
+ * run after pb_sim_run / pb_sim_step / pb_batch_run for them, the current coarsest active
+ * count, then the microseconds the device rebuilds spent in the coarse levels, in the dense
+ * assembly and Cholesky factor, in the inverse factor and smoother weights, and in the
+ * transfer stencils and dense inverse (cumulative). */
+int32_t pb_sim_mg_stats(pb_sim* s, int64_t* out8);
 /* FNV-1a digest of the hierarchy the field solve reads (per level the smoother weights and
  * the transfer stencils, then the coarsest index set and its dense inverse): equal digests
  * mean bit-equal operators (a diagnostic without a reference counterpart). */
@@ -344,7 +346,7 @@ int32_t pb_batch_graph_stats(pb_batch* b, int64_t* out3);
 /* out4[0] = device time (ms) of the last pb_batch_run, out4[1] = kernel launches in it,
  * out4[2] = host time (ms) from its first enqueue to its last (when this approaches the
  * device time, the run is bound by launch overhead), out4[3] = device time of its
- * field-solve launches (without graphs; 0 with them). */
+ * field-solve launches (without graphs; -1 with them: not timed inside a graph). */
 int32_t pb_batch_timing(pb_batch* b, double* out4);
 /* A member's field-solve cost as the batch measured it (out2[0]: block-milliseconds per
  * launch in its last batch run, 0 before one) and its block share in the last launch planned

@@ -105,9 +105,9 @@ def _digest(lib, sim):
 
 
 def _mg_stats(lib, sim):
-    out = (C.c_int64 * 4)()
+    out = (C.c_int64 * 8)()
     lib.check(lib.load().pb_sim_mg_stats(sim._h, out), "pb_sim_mg_stats")
-    return list(out)
+    return list(out)[:4]
 
 
 def _run(lib, sim, p, steps=K, graphs=False):

@@ -68,11 +68,15 @@ struct SolveLaunch {
 // Blocks of one launch shared out in proportion to each instance's node count (at least
 // one block each, at most the instance's own full-device grid).
 // After a batch run: block-ns per field-solve launch of the run's solves (their counters
-// were cleared at its start).
+// were cleared at its start).  The estimate moves only when the run's figure is off by more
+// than 30%, so that the block shares, and the step graphs captured with them, stay put while
+// the cost does.
 static int32_t measure_solve(Sim* s) {
   unsigned long long ns[2] = {0, 0};
   CK(cudaMemcpy(ns, s->solve_ns, sizeof(ns), cudaMemcpyDeviceToHost));
-  if (ns[1] > 0) s->solve_work = (double)ns[0] / (double)ns[1];
+  if (ns[1] == 0) return PB_OK;
+  const double w = (double)ns[0] / (double)ns[1];
+  if (!(s->solve_work > 0.0) || w > 1.3 * s->solve_work || w * 1.3 < s->solve_work) s->solve_work = w;
   return PB_OK;
 }
 
@@ -408,7 +412,7 @@ int32_t pb_batch_create(pb_batch** out, int32_t device) {
   CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
   CK(cudaMalloc((void**)&b->slot, sizeof(int)));
   CK(cudaFuncSetAttribute((const void*)k_poisson_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)mg_coarse_smem_bytes(MG_MAX_COARSE)));
+                          (int)mg_solve_smem_bytes(MG_MAX_COARSE, b->num_sms, 1)));
   CK(cudaFuncSetAttribute((const void*)k_poisson_batch, cudaFuncAttributePreferredSharedMemoryCarveout,
                           (int)cudaSharedmemCarveoutMaxL1));
   *out = b;
@@ -474,8 +478,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       L.args_off = nargs;
       L.blk_off = nblk;
       L.nblocks = b->num_sms;
-      L.smem = 0;
-      for (int i : L.inst) L.smem = std::max(L.smem, sims[i]->s.psmem);
+      L.smem = 0;  // set with the block shares
       nargs += L.inst.size();
       nblk += (size_t)L.nblocks;
       plan.push_back(L);
@@ -505,8 +508,9 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     CK(cudaMalloc((void**)&b->dblk, b->blk_cap * sizeof(int)));
     b->dblk_cap = b->blk_cap;
   }
-  for (const SolveLaunch& L : plan) {
+  for (SolveLaunch& L : plan) {
     std::vector<int> nb = share_blocks(solve_work(sims, L.inst), L.nblocks);
+    L.smem = 0;
     int blk0 = 0;
     for (size_t j = 0; j < L.inst.size(); ++j) {
       Sim* s = &sims[L.inst[j]]->s;
@@ -516,6 +520,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       a.blk0 = blk0;
       a.nblk = nb[j];
       set_up_tiles(s, &a);
+      L.smem = std::max(L.smem, mg_solve_smem_bytes(s->ncap, a.nvb, a.nblk));
       a.trace = s->trace_on ? s->ptrace : nullptr;  // traced members run without graphs
       b->hargs[L.args_off + j] = a;
       MgRebuildArgs m = mg_rebuild_args(s);
@@ -579,6 +584,7 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       CK(cudaMemsetAsync(s->solve_ns, 0, 2 * sizeof(unsigned long long), b->stream));
     }
     b->launches = 0;
+    b->last_solve_ms = -1.0;  // not timed inside graphs
     if ((rc = batch_run_graphs(b, sims, n, params, K, plan))) return rc;
     CK(cudaMemcpyAsync(b->hring, b->ring, (size_t)K * n * sizeof(pb_step_report), cudaMemcpyDeviceToHost,
                        b->stream));

@@ -131,7 +131,20 @@ template <class GA, class GB>
 __device__ __forceinline__ double quad_dot4(GA ga, GB gb, int len, int t, unsigned qmask) {
   double s = 0.0;
   const int m4 = len & ~3;
-  for (int k = t; k < m4; k += 4) s = dadd(s, dmul(ga(k), gb(k)));
+  int k = t;
+  // eight terms of the lane's chain loaded before they are added (in order): the loads of a
+  // dot product overlap instead of each waiting on the L2
+  for (; k + 28 < m4; k += 32) {
+    double pa[8], pb[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      pa[u] = ga(k + 4 * u);
+      pb[u] = gb(k + 4 * u);
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) s = dadd(s, dmul(pa[u], pb[u]));
+  }
+  for (; k < m4; k += 4) s = dadd(s, dmul(ga(k), gb(k)));
   if (t == 0)
     for (int k = m4; k < len; ++k) s = dadd(s, dmul(ga(k), gb(k)));
   const double nxt = __shfl_down_sync(qmask, s, 1, 4);
@@ -477,9 +490,20 @@ __device__ void inverse_product(const MgRebuildArgs& a, int n) {
   }
 }
 
+// block 0's clock: microseconds since *t0 are added to counts[slot] and *t0 moves on
+__device__ __forceinline__ void mg_clock(const MgRebuildArgs& a, unsigned long long* t0, int slot) {
+  if (mgb(a) != 0 || threadIdx.x != 0) return;
+  unsigned long long now;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+  if (slot >= 0) atomicAdd(a.counts + slot, (int)((now - *t0) / 1000ull));
+  *t0 = now;
+}
+
 __device__ void mg_rebuild_body(const MgRebuildArgs& a) {
   if (*(volatile int*)a.dirty == 0) return;  // every block reads it before any barrier
   const int L = a.nlevels, tid = mg_tid(a), nth = mg_nth(a);
+  unsigned long long t0 = 0;
+  mg_clock(a, &t0, -1);
   if (mgb(a) == 0 && threadIdx.x < MG_CNT_REBUILDS) a.counts[threadIdx.x] = 0;
   mg_sync(a);
   {
@@ -495,6 +519,7 @@ __device__ void mg_rebuild_body(const MgRebuildArgs& a) {
     count_add(a.counts + l + 1, phase_galerkin(a, l));
     mg_sync(a);
   }
+  mg_clock(a, &t0, MG_CNT_US_LEVELS);
   const int kind = structure_of(a);
   const int n = __ldcg(a.counts + L - 1);
   if (kind == 2) {
@@ -511,6 +536,7 @@ __device__ void mg_rebuild_body(const MgRebuildArgs& a) {
   assemble_dense(a, n);
   mg_sync(a);
   cholesky(a, n);
+  mg_clock(a, &t0, MG_CNT_US_CHOLESKY);
   if (__ldcg(a.counts + MG_CNT_FLAGS) & 2) {
     // not positive definite: the host build reports it
     if (mgb(a) == 0 && threadIdx.x == 0) {
@@ -539,6 +565,7 @@ __device__ void mg_rebuild_body(const MgRebuildArgs& a) {
   }
   inverse_factor(a, n);
   mg_sync(a);
+  mg_clock(a, &t0, MG_CNT_US_INVERSE);
   for (int l = 1; l + 1 < L; ++l) {
     const int Nc = a.lev[l + 1].ny * a.lev[l + 1].nx, Nf = a.lev[l].ny * a.lev[l].nx;
     for (int c = tid; c < Nc; c += nth) transfer_R(a, l, c);
@@ -546,6 +573,7 @@ __device__ void mg_rebuild_body(const MgRebuildArgs& a) {
   }
   inverse_product(a, n);
   mg_sync(a);
+  mg_clock(a, &t0, MG_CNT_US_TRANSFER);
   if (mgb(a) == 0 && threadIdx.x == 0) {
     *a.dirty = 0;
     atomicAdd(a.counts + MG_CNT_REBUILDS, 1);

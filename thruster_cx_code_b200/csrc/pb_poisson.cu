@@ -59,6 +59,17 @@ __device__ __forceinline__ int vtid(const PoissonArgs& a, int v) {
   return (((int)threadIdx.x >> 5) * a.nvb + v) * 32 + ((int)threadIdx.x & 31);
 }
 
+// virtual blocks run by this block
+__device__ __forceinline__ int vb_count(const PoissonArgs& a) {
+  return gbid(a) < a.nvb ? (a.nvb - gbid(a) + a.nblk - 1) / a.nblk : 0;
+}
+
+// the virtual-block sums' shared memory, after the coarsest right-hand side
+__device__ __forceinline__ double* vb_scratch(const PoissonArgs& a) {
+  extern __shared__ float4 dyn_smem[];
+  return reinterpret_cast<double*>(dyn_smem + a.vb_off);
+}
+
 // grid barrier of this instance's blocks (grid_sync: bounded, release/acquire)
 __device__ __forceinline__ void grid_barrier(const PoissonArgs& a) { grid_sync(a.bar, a.errflags, a.nblk, gbid(a)); }
 
@@ -79,26 +90,36 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Partials of virtual block v, up to two values, into ring slot `slot` (read after the next
-// barrier); called by every thread of the block.
-__device__ __forceinline__ void put_partials(const PoissonArgs& a, int slot, int v, double v0, double v1) {
-  __shared__ double sm[2][PT / 32];
+// Partials of the virtual blocks a block runs: after the loop of its k-th virtual block each
+// warp adds its two sums to shared memory (vb_add, no block barrier); vb_flush then sums each
+// virtual block's 32 warp sums in warp order (the tree of one warp_sum) and writes them to
+// ring slot `slot` (read after the next barrier).  vbs holds 2 x 32 doubles per virtual
+// block of the block (PoissonArgs::vb_off).
+__device__ __forceinline__ void vb_add(double* vbs, int k, double v0, double v1) {
   v0 = warp_sum(v0);
   v1 = warp_sum(v1);
-  if ((threadIdx.x & 31) == 0) { sm[0][threadIdx.x >> 5] = v0; sm[1][threadIdx.x >> 5] = v1; }
+  if ((threadIdx.x & 31) == 0) {
+    double* w = vbs + (size_t)(k * 32 + (threadIdx.x >> 5)) * 2;
+    w[0] = v0;
+    w[1] = v1;
+  }
+}
+
+__device__ __forceinline__ void vb_flush(const PoissonArgs& a, double* vbs, int slot, int nk) {
   __syncthreads();
-  if (threadIdx.x < 32) {
-    double s0 = threadIdx.x < PT / 32 ? sm[0][threadIdx.x] : 0.0;
-    double s1 = threadIdx.x < PT / 32 ? sm[1][threadIdx.x] : 0.0;
+  const int lane = threadIdx.x & 31;
+  double* part = a.partials + (size_t)(slot & 3) * 2 * a.nvb;
+  for (int k = (int)(threadIdx.x >> 5); k < nk; k += (int)(blockDim.x >> 5)) {
+    double s0 = vbs[(size_t)(k * 32 + lane) * 2], s1 = vbs[(size_t)(k * 32 + lane) * 2 + 1];
     s0 = warp_sum(s0);
     s1 = warp_sum(s1);
-    if (threadIdx.x == 0) {
-      double* part = a.partials + (size_t)(slot & 3) * 2 * a.nvb;
+    if (lane == 0) {
+      const int v = gbid(a) + k * a.nblk;
       part[v] = s0;
       part[a.nvb + v] = s1;
     }
   }
-  __syncthreads();  // sm is reused by the next virtual block's call
+  __syncthreads();  // vbs is reused by the next reduction
 }
 
 // Grid totals of a slot, after a barrier; the same order in every block.
@@ -294,15 +315,17 @@ __device__ double up_tile0(const PoissonArgs& a, const float* r0, int t, bool tw
 // laid out for nvb blocks and tile t belongs to virtual block t mod nvb.
 __device__ void up_leg0_tiled(const PoissonArgs& a, const float* r0, int slot) {
   const bool two = a.nu0 == 2;
+  double* vbs = vb_scratch(a);
   if (two) {
     for (int t = gbid(a); t < a.ut_y * a.ut_x; t += a.nblk) up_tile0(a, r0, t, true);
     return;
   }
-  for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+  for (int v = gbid(a), kv = 0; v < a.nvb; v += a.nblk, ++kv) {
     double rz = 0.0;
     for (int t = v; t < a.ut_y * a.ut_x; t += a.nvb) rz += up_tile0(a, r0, t, false);
-    put_partials(a, slot, v, rz, 0.0);
+    vb_add(vbs, kv, rz, 0.0);
   }
+  vb_flush(a, vbs, slot, vb_count(a));
 }
 
 // Second fine-level pre-sweep (nu0 = 2): s = r - A (d r) on the free nodes, i.e.
@@ -339,7 +362,8 @@ __device__ void presmooth0(const PoissonArgs& a, const float* r, float* s_out, i
 __device__ void smooth0(const PoissonArgs& a, const float* r, int slot) {
   const MgLevel& F = a.lev[0];
   const int N = F.ny * F.nx, nth = a.nvb * (int)blockDim.x;
-  for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+  double* vbs = vb_scratch(a);
+  for (int v = gbid(a), kv = 0; v < a.nvb; v += a.nblk, ++kv) {
   double rz = 0.0;
   for (int i0 = vtid(a, v); i0 < N; i0 += FU * nth) {
     float zv[FU], rv[FU];
@@ -363,8 +387,9 @@ __device__ void smooth0(const PoissonArgs& a, const float* r, int slot) {
       rz += (double)rv[u] * (double)zv[u];
     }
   }
-  put_partials(a, slot, v, rz, 0.0);
+  vb_add(vbs, kv, rz, 0.0);
   }
+  vb_flush(a, vbs, slot, vb_count(a));
 }
 
 // Levels >= 1: the same transfers from the host-built stencils (R on the coarse level,
@@ -489,11 +514,13 @@ __device__ void vcycle_below(const PoissonArgs& a, float* rcs, int slot, const f
     coarse_solve(a, r0, a.z32, rcs);
     grid_barrier(a);
     const int N = a.ny * a.nx, nv = a.nvb * (int)blockDim.x;
-    for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+    double* vbs = vb_scratch(a);
+    for (int v = gbid(a), kv = 0; v < a.nvb; v += a.nblk, ++kv) {
       double rz = 0.0;
       for (int i = vtid(a, v); i < N; i += nv) rz += (double)(*(r0 + i)) * (double)(*(a.z32 + i));
-      put_partials(a, slot, v, rz, 0.0);
+      vb_add(vbs, kv, rz, 0.0);
     }
+    vb_flush(a, vbs, slot, vb_count(a));
     grid_barrier(a);
     return;
   }
@@ -523,6 +550,7 @@ __device__ void vcycle_below(const PoissonArgs& a, float* rcs, int slot, const f
 __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   extern __shared__ float4 dyn_smem[];
   float* rcs = reinterpret_cast<float*>(dyn_smem);  // nc floats: the coarsest r, gathered
+  double* vbs = vb_scratch(a);
   const int tid = gtid(a), nth = a.nblk * blockDim.x;
   const int nv = a.nvb * (int)blockDim.x;  // stride of a virtual block's nodes (reduction loops)
   const int N = a.ny * a.nx;
@@ -532,23 +560,26 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
   if (gbid(a) == 0 && threadIdx.x == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
   tmark(a, 20);
 
-  // Dirichlet-neighbour sums (V_fixed is constant during the launch)
-  for (int i = tid; i < N; i += nth) {
-    if (__ldg(a.cls + i) != NC_FREE) continue;
-    const int y = i / a.nx, x = i - y * a.nx;
-    int j[4];
-    nbrs0(a, i, y, x, j);
-    double s = 0.0;
+  // Dirichlet-neighbour sums (V_fixed is constant during the launch), with the mapping of
+  // the right-hand-side loop that reads them: each thread reads only what it wrote, so no
+  // barrier is needed between the two
+  for (int v = gbid(a); v < a.nvb; v += a.nblk)
+    for (int i = vtid(a, v); i < N; i += nv) {
+      if (__ldg(a.cls + i) != NC_FREE) continue;
+      const int y = i / a.nx, x = i - y * a.nx;
+      int j[4];
+      nbrs0(a, i, y, x, j);
+      double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (j[k] >= 0 && __ldg(a.cls + j[k]) == NC_DIR) s += __ldg(a.Vfixed + j[k]);
-    a.dirsum[i] = s;
-  }
+      for (int k = 0; k < 4; ++k)
+        if (j[k] >= 0 && __ldg(a.cls + j[k]) == NC_DIR) s += __ldg(a.Vfixed + j[k]);
+      a.dirsum[i] = s;
+    }
 
   for (int pic = 0; pic < a.iterations; ++pic) {
     const double inner_at_pic = n_inner, outer_at_pic = n_outer;
     // right-hand side from the Boltzmann electron density of the current V, residual
-    for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+    for (int v = gbid(a), kv = 0; v < a.nvb; v += a.nblk, ++kv) {
       const int t0 = vtid(a, v);
       double ff = 0.0, rr = 0.0;
       for (int i = t0; i < N; i += nv) {
@@ -568,8 +599,9 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
         __stcg(a.r32 + i, (float)res);
         rr += res * res;
       }
-      put_partials(a, slot, v, ff, rr);
+      vb_add(vbs, kv, ff, rr);
     }
+    vb_flush(a, vbs, slot, vb_count(a));
     grid_barrier(a);
     double fnorm2, rnorm2;
     get_sums(a, slot++, fnorm2, rnorm2);
@@ -598,7 +630,7 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
         const double beta = k == 0 ? 0.0 : rz / rz_old;
         // FU nodes per thread and pass: every load of the pass is issued before the first
         // store, so the loads of different nodes overlap (the sums keep the node order)
-        for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+        for (int v = gbid(a), kv = 0; v < a.nvb; v += a.nblk, ++kv) {
           double pq_p = 0.0;
           for (int i0 = vtid(a, v); i0 < N; i0 += FU * nv) {
             float pv[FU], qv[FU];
@@ -620,13 +652,14 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
               pq_p += (double)pv[u] * (double)qv[u];
             }
           }
-          put_partials(a, slot, v, pq_p, 0.0);
+          vb_add(vbs, kv, pq_p, 0.0);
         }
+        vb_flush(a, vbs, slot, vb_count(a));
         grid_barrier(a);
         double pq;
         get_sums(a, slot++, pq, dummy);
         const double alpha = pq != 0.0 ? rz / pq : 0.0;
-        for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+        for (int v = gbid(a), kv = 0; v < a.nvb; v += a.nblk, ++kv) {
           double rr_p = 0.0;
           for (int i0 = vtid(a, v); i0 < N; i0 += FU * nv) {
             float ev[FU], rv[FU];
@@ -646,8 +679,9 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
               rr_p += (double)rv[u] * (double)rv[u];
             }
           }
-          put_partials(a, slot, v, rr_p, 0.0);
+          vb_add(vbs, kv, rr_p, 0.0);
         }
+        vb_flush(a, vbs, slot, vb_count(a));
         grid_barrier(a);
         double rrk;
         get_sums(a, slot++, rrk, dummy);
@@ -664,7 +698,7 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
       for (int i = tid; i < N; i += nth)
         if (__ldg(a.cls + i) == NC_FREE) __stcg(a.x + i, (*(a.x + i)) + (double)(*(a.e32 + i)));
       grid_barrier(a);
-      for (int v = gbid(a); v < a.nvb; v += a.nblk) {
+      for (int v = gbid(a), kv = 0; v < a.nvb; v += a.nblk, ++kv) {
         double rr = 0.0;
         for (int i = vtid(a, v); i < N; i += nv) {
           if (__ldg(a.cls + i) != NC_FREE) { __stcg(a.r32 + i, 0.0f); continue; }
@@ -673,8 +707,9 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
           __stcg(a.r32 + i, (float)res);
           rr += res * res;
         }
-        put_partials(a, slot, v, rr, 0.0);
+        vb_add(vbs, kv, rr, 0.0);
       }
+      vb_flush(a, vbs, slot, vb_count(a));
       grid_barrier(a);
       get_sums(a, slot++, rnorm2, dummy);
       tmark(a, 16);

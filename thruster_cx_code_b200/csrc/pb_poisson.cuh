@@ -58,8 +58,9 @@ struct PoissonArgs {
   const float* cinv;      // coarsest inverse (nc x nc, exactly symmetric)
   // this instance's blocks in the launch and its reductions and barrier
   int blk0, nblk;         // first block and number of blocks
-  int nvb;                // virtual blocks of the reductions (the device's SM count, >= nblk):
-                          // the order of every sum, whatever nblk is
+  int nvb;                // virtual blocks of the reductions (mg_virtual_blocks): the order of
+                          // every sum, whatever nblk is
+  int vb_off;             // float4 offset of the virtual-block sums in the dynamic shared memory
   int ut_y, ut_x;         // tiles of the fine-level up leg (fine_up_tiles for nblk blocks, or
                           // for nvb when nu0 = 1: its tiles then carry the (r, z) partials)
   double* partials;       // 4 slots x 2 values x nvb doubles
@@ -72,8 +73,21 @@ struct PoissonArgs {
 };
 
 // dynamic shared memory of k_poisson: the coarsest right-hand side gathered by each block
-// (sized for the capacity of the coarsest level, which a rebuild on the device may fill)
+// (sized for the capacity of the coarsest level, which a rebuild on the device may fill),
+// then the warp sums of the virtual blocks the block runs
 inline size_t mg_coarse_smem_bytes(int nc) { return 4 * (size_t)(nc > 0 ? nc : 1); }
+inline int mg_vb_offset(int ncap) { return (int)((mg_coarse_smem_bytes(ncap) + 15) / 16); }
+inline size_t mg_solve_smem_bytes(int ncap, int nvb, int nblk) {
+  return 16 * (size_t)mg_vb_offset(ncap) + (size_t)((nvb + nblk - 1) / nblk) * 2 * 32 * sizeof(double);
+}
+// Virtual blocks of the reductions on an n-node fine level: about 2048 nodes each (two per
+// thread of a 1024-thread block), at most the device's SM count.  A function of the grid
+// alone, so every reduction of a solve has the same order on any number of blocks; with the
+// full grid of blocks no block runs more than two nodes per thread of them.
+inline int mg_virtual_blocks(long n, int num_sms) {
+  const long v = (n + 2047) / 2048;
+  return (int)std::max(1L, std::min<long>(v, num_sms));
+}
 
 // ---------------------------------------------------------------- rebuild on the device
 // Arrays of one level for k_mg_rebuild: the hierarchy the solve reads (dinv, R, U, z) and
@@ -93,6 +107,10 @@ enum : int {
   MG_CNT_FLAGS = MG_MAX_LEVELS,   // bit 0: coupling outside the 9-point pattern, bit 1: not SPD
   MG_CNT_REBUILDS,                // rebuilds completed on the device (cumulative)
   MG_CNT_DEFERRED,                // rebuilds left to the host (cumulative)
+  MG_CNT_US_LEVELS,               // microseconds (cumulative, block 0's clock) in the coarse levels,
+  MG_CNT_US_CHOLESKY,             //   the dense assembly and Cholesky factor,
+  MG_CNT_US_INVERSE,              //   the inverse factor and smoother weights,
+  MG_CNT_US_TRANSFER,             //   the transfer stencils and the dense inverse
   MG_CNT_SLOTS = 32
 };
 // MgRebuildArgs::status bit: the freed nodes change the level structure; the host rebuilds

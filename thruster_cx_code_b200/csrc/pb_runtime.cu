@@ -410,7 +410,7 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   // the coarsest level grows as cells break (more free nodes): room for a quarter more than
   // max(nc, max_coarse) nodes for the device rebuild, within the dense solve's limit
   s->ncap = std::min(MG_MAX_COARSE, std::max(s->nc, s->max_coarse) * 5 / 4);
-  s->psmem = mg_coarse_smem_bytes(s->ncap);
+  s->psmem = mg_solve_smem_bytes(s->ncap, mg_virtual_blocks((long)s->ny * s->nx, s->num_sms), 1);
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_poisson, PT, s->psmem));
   if (occ < 1) return fail(PB_ERR_ARG, "field solver: no resident block with " + std::to_string(s->psmem) +
@@ -496,7 +496,8 @@ static PoissonArgs poisson_args(Sim* s, int iterations, const pb_step_params* p)
   }
   a.nc_dev = s->nc_dev; a.cidx = s->cidx; a.cinv = s->cinv;
   a.blk0 = 0; a.nblk = s->pgrid;
-  a.nvb = s->num_sms;
+  a.nvb = mg_virtual_blocks((long)s->ny * s->nx, s->num_sms);
+  a.vb_off = mg_vb_offset(s->ncap);
   set_up_tiles(s, &a);
   a.partials = s->partials; a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
@@ -556,7 +557,7 @@ static int32_t launch_poisson(Sim* s, int iterations, const pb_step_params* p) {
   }
   PoissonArgs a = poisson_args(s, iterations, p);
   void* args[] = {&a};
-  return coop_field_launch(s, (const void*)k_poisson, args, s->psmem);
+  return coop_field_launch(s, (const void*)k_poisson, args, mg_solve_smem_bytes(s->ncap, a.nvb, a.nblk));
 }
 
 // The per-step resets in one launch instead of a dozen memsets (each of which is an
@@ -1181,7 +1182,7 @@ int32_t pb_sim_create(pb_sim** out, int32_t device) {
   // field solve: one block of PT threads per SM (cooperative launch); the little shared
   // memory it uses leaves the rest of the SM's L1 to cache the grid
   CK(cudaFuncSetAttribute((const void*)k_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)mg_coarse_smem_bytes(MG_MAX_COARSE)));
+                          (int)mg_solve_smem_bytes(MG_MAX_COARSE, s->num_sms, 1)));
   CK(cudaFuncSetAttribute((const void*)k_poisson, cudaFuncAttributePreferredSharedMemoryCarveout,
                           (int)cudaSharedmemCarveoutMaxL1));
   s->pgrid = s->num_sms;
@@ -1807,9 +1808,10 @@ int32_t pb_sim_batch_share(pb_sim* h, double* out2) {
   return PB_OK;
 }
 
-int32_t pb_sim_mg_stats(pb_sim* h, int64_t* out4) {
+int32_t pb_sim_mg_stats(pb_sim* h, int64_t* out8) {
   Sim* s = &h->s;
-  if (!out4) return fail(PB_ERR_ARG, "pb_sim_mg_stats: null output");
+  int64_t* out4 = out8;
+  if (!out8) return fail(PB_ERR_ARG, "pb_sim_mg_stats: null output");
   if (!s->domain_set) return fail(PB_ERR_STATE, "pb_sim_mg_stats: no domain");
   int c[MG_CNT_SLOTS];
   int nc = 0;
@@ -1820,6 +1822,10 @@ int32_t pb_sim_mg_stats(pb_sim* h, int64_t* out4) {
   out4[1] = c[MG_CNT_DEFERRED];
   out4[2] = s->mg_host_rebuilds;
   out4[3] = nc;
+  out8[4] = c[MG_CNT_US_LEVELS];
+  out8[5] = c[MG_CNT_US_CHOLESKY];
+  out8[6] = c[MG_CNT_US_INVERSE];
+  out8[7] = c[MG_CNT_US_TRANSFER];
   return PB_OK;
 }
 
