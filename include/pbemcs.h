@@ -341,6 +341,11 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
  * without graphs.  Steps that cannot be captured are enqueued as usual (and graphs stay
  * off for the batch until re-enabled; see pb_batch_graph_stats). */
 int32_t pb_batch_set_graphs(pb_batch* b, int32_t on);
+/* Host threads that enqueue the members' kernels in the streams form (the calling thread
+ * included; member i goes to thread i mod threads): 1 (default) enqueues from the calling
+ * thread alone, 0 picks min(8, half the host's hardware threads).  Results do not depend on
+ * it; on a 64-member sweep eight threads took more host and device time than one. */
+int32_t pb_batch_set_threads(pb_batch* b, int32_t threads);
 /* out3: captures, replays, 1 if a capture failed (pb_last_error() gives the reason). */
 int32_t pb_batch_graph_stats(pb_batch* b, int64_t* out3);
 /* out4[0] = device time (ms) of the last pb_batch_run, out4[1] = kernel launches in it,

@@ -114,6 +114,7 @@ PROTOTYPES = {
     "pb_batch_run": (i32, [vp, P(vp), i32, P(StepParams), i32, P(StepReport)]),
     "pb_batch_timing": (i32, [vp, P(f64)]),
     "pb_batch_set_graphs": (i32, [vp, i32]),
+    "pb_batch_set_threads": (i32, [vp, i32]),
     "pb_batch_graph_stats": (i32, [vp, P(C.c_int64)]),
     "pb_sim_memory": (i32, [vp, P(C.c_int64)]),
     "pb_host_seq_add_f32d": (f32, [f32, f64, u32]),

@@ -8,6 +8,62 @@
 // cooperative launch in which every instance gets a contiguous range of blocks with its
 // own grid barrier and reductions (k_poisson_batch).
 
+#include <condition_variable>
+#include <thread>
+
+// Host threads that enqueue the members' step halves in parallel (the streams form): a
+// persistent pool; run(f) calls f(w) on every worker w and on the calling thread (the last
+// index) and returns when all are done.
+struct EnqueuePool {
+  std::vector<std::thread> th;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::function<void(int)> task;
+  long long generation = 0;
+  int pending = 0;
+  bool stop = false;
+  int workers() const { return (int)th.size(); }
+  void start(int n) {
+    for (int w = 0; w < n; ++w)
+      th.emplace_back([this, w] {
+        long long seen = 0;
+        while (true) {
+          std::function<void(int)> f;
+          {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_work.wait(lk, [&] { return stop || generation != seen; });
+            if (stop) return;
+            seen = generation;
+            f = task;
+          }
+          f(w);
+          std::lock_guard<std::mutex> lk(mu);
+          if (--pending == 0) cv_done.notify_one();
+        }
+      });
+  }
+  void run(const std::function<void(int)>& f) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      task = f;
+      pending = (int)th.size();
+      ++generation;
+    }
+    cv_work.notify_all();
+    f((int)th.size());
+    std::unique_lock<std::mutex> lk(mu);
+    cv_done.wait(lk, [&] { return pending == 0; });
+  }
+  ~EnqueuePool() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+    }
+    cv_work.notify_all();
+    for (auto& t : th) t.join();
+  }
+};
+
 struct pb_batch {
   int device = 0;
   int num_sms = 0;
@@ -52,6 +108,11 @@ struct pb_batch {
   int* slot = nullptr;                // next ring row
   cudaEvent_t ev_fork = nullptr;
   long long graph_captures = 0, graph_replays = 0;
+  // host threads of the streams form (created on first use); one by default: more measured
+  // slower (64 sweep points: 3.6 ms of host time per step on one thread, 6.7 ms on eight,
+  // and 5% more device time), the driver serialises the launches anyway
+  int enqueue_threads = 1;  // total, the calling thread included (0: chosen from the host)
+  std::unique_ptr<EnqueuePool> pool;
 };
 
 namespace {
@@ -150,6 +211,7 @@ int64_t sim_device_bytes(const Sim* s) {
     b += Nl * 4 * ((s->lev[l].R ? 25 : 0) + (s->lev[l].U ? 18 : 0));
   }
   b += (int64_t)s->ncap * s->ncap * (4 + 8);  // coarsest inverse and the rebuild's dense scratch
+  b += (int64_t)s->ncap * MG_PANEL * 4 * 8;
   for (size_t l = 1; l < s->lev.size(); ++l) b += (int64_t)s->lev[l].ny * s->lev[l].nx * (1 + 9 * 4);
   b += 4LL * (int64_t)s->sort_cap * 4 + (int64_t)s->hist_cap * 4 + 2LL * (int64_t)s->tile_cap * 8;
   b += (int64_t)s->see_cap * 16 + (int64_t)s->angle_cap * 8;
@@ -634,11 +696,47 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
   for (int i = 0; i < n; ++i) CK(cudaStreamWaitEvent(sims[i]->s.stream, b->ev_solve[0], 0));
   b->launches = 0;
   size_t pi = 0;
+  // the members are split over the enqueue threads (member i on thread i mod T); each thread
+  // keeps its first error, and the run returns the first of them
+  if (!b->pool) {
+    int T = b->enqueue_threads;
+    if (T <= 0) T = std::max(1, std::min(8, (int)std::thread::hardware_concurrency() / 2));
+    b->pool.reset(new EnqueuePool());
+    b->pool->start(T - 1);
+  }
+  const int T = b->pool->workers() + 1;
+  std::vector<int32_t> wrc(T, PB_OK);
+  std::vector<std::string> werr(T);
+  auto phase = [&](auto body) -> int32_t {
+    std::fill(wrc.begin(), wrc.end(), PB_OK);
+    b->pool->run([&](int w) {
+      if (cudaSetDevice(b->device) != cudaSuccess) {
+        wrc[w] = PB_ERR_CUDA;
+        werr[w] = "cudaSetDevice on an enqueue thread failed";
+        return;
+      }
+      for (int i = w; i < n && wrc[w] == PB_OK; i += T) {
+        const int32_t r = body(i);
+        if (r) {
+          wrc[w] = r;
+          werr[w] = g_err;
+        }
+      }
+    });
+    for (int w = 0; w < T; ++w)
+      if (wrc[w]) {
+        g_err = werr[w];
+        return wrc[w];
+      }
+    return PB_OK;
+  };
   for (int k = 0; k < K; ++k) {
-    for (int i = 0; i < n; ++i) {
-      if ((rc = enqueue_step_pre(sims[i], &params[(size_t)i * K + k]))) return rc;
+    rc = phase([&](int i) -> int32_t {
+      if (int32_t r = enqueue_step_pre(sims[i], &params[(size_t)i * K + k])) return r;
       CK(cudaEventRecord(b->ev_inst[i], sims[i]->s.stream));
-    }
+      return PB_OK;
+    });
+    if (rc) return rc;
     std::vector<int> solved_by(n, -1);
     int li = 0;
     for (; pi < plan.size() && plan[pi].step == k; ++pi, ++li) {
@@ -661,14 +759,16 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       ++b->launches;
       CK(cudaEventRecord(b->ev_solve[li], b->stream));
     }
-    for (int i = 0; i < n; ++i) {
+    rc = phase([&](int i) -> int32_t {
       Sim* s = &sims[i]->s;
       if (solved_by[i] >= 0) CK(cudaStreamWaitEvent(s->stream, b->ev_solve[solved_by[i]], 0));
-      if ((rc = enqueue_step_post(sims[i], &params[(size_t)i * K + k]))) return rc;
+      if (int32_t r = enqueue_step_post(sims[i], &params[(size_t)i * K + k])) return r;
       if (reports)
         CK(cudaMemcpyAsync(&b->hrep[(size_t)i * K + k], s->rep_dev, sizeof(pb_step_report), cudaMemcpyDeviceToHost,
                            s->stream));
-    }
+      return PB_OK;
+    });
+    if (rc) return rc;
   }
   for (int i = 0; i < n; ++i) {
     CK(cudaEventRecord(b->ev_inst[i], sims[i]->s.stream));
@@ -699,6 +799,15 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       for (int k = 0; k < K; ++k)
         if ((rc = check_flags(&sims[i]->s, reports[(size_t)i * K + k].errflags))) return rc;
   }
+  return PB_OK;
+}
+
+int32_t pb_batch_set_threads(pb_batch* b, int32_t threads) {
+  if (!b || threads < 0 || threads > 64) return fail(PB_ERR_ARG, "pb_batch_set_threads: 0 to 64 threads");
+  CK(cudaSetDevice(b->device));
+  CK(cudaStreamSynchronize(b->stream));
+  b->pool.reset();
+  b->enqueue_threads = threads;
   return PB_OK;
 }
 

@@ -126,15 +126,13 @@ __device__ __forceinline__ int child_rows(int I, int nyf, int wrapC, int* ys) {
 // Four-way partial dot product of the host (dot4): sum t over terms k = t mod 4 below the
 // last multiple of four, the tail added to sum 0, then (s0 + s1) + (s2 + s3).  Lane t of a
 // four-lane group keeps sum t; every lane of the group gets the result.  ga(k), gb(k) give
-// the terms.
+// the terms.  quad_dot4_from continues chains that already hold the terms below p (p a
+// multiple of four, at most the last multiple of four below len; s is lane t's chain);
+// chain_prefix forms those first p terms of lane t's chain.  Eight terms of a chain are
+// loaded before they are added, in order, so the loads of a dot product overlap.
 template <class GA, class GB>
-__device__ __forceinline__ double quad_dot4(GA ga, GB gb, int len, int t, unsigned qmask) {
-  double s = 0.0;
-  const int m4 = len & ~3;
-  int k = t;
-  // eight terms of the lane's chain loaded before they are added (in order): the loads of a
-  // dot product overlap instead of each waiting on the L2
-  for (; k + 28 < m4; k += 32) {
+__device__ __forceinline__ double chain_run(double s, GA ga, GB gb, int k, int end) {
+  for (; k + 28 < end; k += 32) {
     double pa[8], pb[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
@@ -144,7 +142,19 @@ __device__ __forceinline__ double quad_dot4(GA ga, GB gb, int len, int t, unsign
 #pragma unroll
     for (int u = 0; u < 8; ++u) s = dadd(s, dmul(pa[u], pb[u]));
   }
-  for (; k < m4; k += 4) s = dadd(s, dmul(ga(k), gb(k)));
+  for (; k < end; k += 4) s = dadd(s, dmul(ga(k), gb(k)));
+  return s;
+}
+
+template <class GA, class GB>
+__device__ __forceinline__ double chain_prefix(GA ga, GB gb, int p, int t) {
+  return chain_run(0.0, ga, gb, t, p);
+}
+
+template <class GA, class GB>
+__device__ __forceinline__ double quad_dot4_from(double s, GA ga, GB gb, int p, int len, int t, unsigned qmask) {
+  const int m4 = len & ~3;
+  s = chain_run(s, ga, gb, p + t, m4);
   if (t == 0)
     for (int k = m4; k < len; ++k) s = dadd(s, dmul(ga(k), gb(k)));
   const double nxt = __shfl_down_sync(qmask, s, 1, 4);
@@ -152,6 +162,11 @@ __device__ __forceinline__ double quad_dot4(GA ga, GB gb, int len, int t, unsign
   const double far = __shfl_down_sync(qmask, pair, 2, 4);
   const double tot = dadd(pair, far);                   // lane 0
   return __shfl_sync(qmask, tot, 0, 4);
+}
+
+template <class GA, class GB>
+__device__ __forceinline__ double quad_dot4(GA ga, GB gb, int len, int t, unsigned qmask) {
+  return quad_dot4_from(0.0, ga, gb, 0, len, t, qmask);
 }
 
 // ---- the level structure: act and Galerkin stencils of level l + 1 from level l
@@ -411,34 +426,63 @@ __device__ void assemble_dense(const MgRebuildArgs& a, int n) {
 }
 
 // Cholesky factor of the dense operator in place (lower triangle), the host's column order:
-// L_jj = sqrt(A_jj - L_j . L_j), L_ij = (A_ij - L_i . L_j) / L_jj over the first j terms.
-// Column j is one grid-wide step; the group that forms L_{j+1,j} also forms L_{j+1,j+1}.
+// L_jj = sqrt(A_jj - L_j . L_j), L_ij = (A_ij - L_i . L_j) / L_jj, each dot product over the
+// first j terms.  Columns go in panels of MG_PANEL: (1) every pair (i >= j, j in the panel)
+// forms its four chains over the terms below the panel, in parallel; (2) block 0 finishes the
+// panel's diagonal block column by column; (3) every row below it finishes its panel entries
+// in order.  The chains continue where their prefix stopped, so each dot product adds its
+// terms in the host's order.  Three grid barriers per panel.
 __device__ void cholesky(const MgRebuildArgs& a, int n) {
   double* A = a.dense;
   const int t = threadIdx.x & 3;
   const unsigned qmask = 0xFu << (threadIdx.x & 28);
   const int q = mg_tid(a) >> 2, nq = mg_nth(a) >> 2;
-  if (mgb(a) == 0 && threadIdx.x == 0 && n > 0) {
-    const double s = A[0];
-    if (!(s > 0.0)) atomicOr(a.counts + MG_CNT_FLAGS, 2);
-    A[0] = __dsqrt_rn(s);
-  }
-  mg_sync(a);
-  for (int j = 0; j + 1 < n; ++j) {
-    const double* Lj = A + (size_t)j * n;
-    const double djj = Lj[j];
-    for (int i = j + 1 + q; i < n; i += nq) {
-      double* Li = A + (size_t)i * n;
-      const double dot = quad_dot4([&](int k) { return Li[k]; }, [&](int k) { return Lj[k]; }, j, t, qmask);
-      if (t == 0) Li[j] = __ddiv_rn(__dsub_rn(Li[j], dot), djj);
-      if (i == j + 1) {
-        __syncwarp(qmask);
-        const double dd = quad_dot4([&](int k) { return Li[k]; }, [&](int k) { return Li[k]; }, j + 1, t, qmask);
-        if (t == 0) {
-          const double s = __dsub_rn(Li[i], dd);
-          if (!(s > 0.0)) atomicOr(a.counts + MG_CNT_FLAGS, 2);
-          Li[i] = __dsqrt_rn(s);
+  const int ql = (int)threadIdx.x >> 2, nql = (int)blockDim.x >> 2;
+  for (int j0 = 0; j0 < n; j0 += MG_PANEL) {
+    const int j1 = min(j0 + MG_PANEL, n), w = j1 - j0;
+    if (j0 > 0) {
+      const long long np = (long long)(n - j0) * w;
+      for (long long pid = q; pid < np; pid += nq) {
+        const int r = (int)(pid / w), j = j0 + (int)(pid - (long long)r * w), i = j0 + r;
+        if (i < j) continue;
+        const double* Li = A + (size_t)i * n;
+        const double* Lj = A + (size_t)j * n;
+        a.pre[pid * 4 + t] = chain_prefix([&](int k) { return Li[k]; }, [&](int k) { return Lj[k]; }, j0, t);
+      }
+      mg_sync(a);
+    }
+    auto pre_of = [&](int i, int j) { return j0 > 0 ? a.pre[((size_t)(i - j0) * w + (j - j0)) * 4 + t] : 0.0; };
+    if (mgb(a) == 0) {
+      for (int j = j0; j < j1; ++j) {
+        double* Lj = A + (size_t)j * n;
+        if (ql == 0) {
+          const double dd = quad_dot4_from(pre_of(j, j), [&](int k) { return Lj[k]; }, [&](int k) { return Lj[k]; },
+                                           j0, j, t, qmask);
+          if (t == 0) {
+            const double s = __dsub_rn(Lj[j], dd);
+            if (!(s > 0.0)) atomicOr(a.counts + MG_CNT_FLAGS, 2);
+            Lj[j] = __dsqrt_rn(s);
+          }
         }
+        __syncthreads();
+        for (int i = j + 1 + ql; i < j1; i += nql) {
+          double* Li = A + (size_t)i * n;
+          const double dot = quad_dot4_from(pre_of(i, j), [&](int k) { return Li[k]; }, [&](int k) { return Lj[k]; },
+                                            j0, j, t, qmask);
+          if (t == 0) Li[j] = __ddiv_rn(__dsub_rn(Li[j], dot), Lj[j]);
+        }
+        __syncthreads();
+      }
+    }
+    mg_sync(a);
+    for (int i = j1 + q; i < n; i += nq) {
+      double* Li = A + (size_t)i * n;
+      for (int j = j0; j < j1; ++j) {
+        const double* Lj = A + (size_t)j * n;
+        const double dot = quad_dot4_from(pre_of(i, j), [&](int k) { return Li[k]; }, [&](int k) { return Lj[k]; },
+                                          j0, j, t, qmask);
+        if (t == 0) Li[j] = __ddiv_rn(__dsub_rn(Li[j], dot), Lj[j]);
+        __syncwarp(qmask);
       }
     }
     mg_sync(a);
@@ -447,23 +491,52 @@ __device__ void cholesky(const MgRebuildArgs& a, int n) {
 
 // Columns of M = L^-1 (the host's forward substitution): m_c = 1 / L_cc, then
 // m_i = -(L_i[c..i) . m[c..i)) / L_ii.  Column c is stored in row c of the upper triangle
-// (dense[c n + i], i > c) with its diagonal in mdiag[c]; one group per column.
+// (dense[c n + i], i > c) with its diagonal in mdiag[c].  Rows go in panels of MG_PANEL:
+// (1) every pair (row i of the panel, column c) forms its chains over the column's entries
+// below the panel, cut at a multiple of four, in parallel; (2) one group per column finishes
+// the panel's rows in order.  Two grid barriers per panel.
 __device__ void inverse_factor(const MgRebuildArgs& a, int n) {
   double* A = a.dense;
   const int t = threadIdx.x & 3;
   const unsigned qmask = 0xFu << (threadIdx.x & 28);
   const int q = mg_tid(a) >> 2, nq = mg_nth(a) >> 2;
-  for (int c = q; c < n; c += nq) {
-    double* Mc = A + (size_t)c * n;
-    const double mcc = __ddiv_rn(1.0, A[(size_t)c * n + c]);
-    if (t == 0) a.mdiag[c] = mcc;
-    for (int i = c + 1; i < n; ++i) {
-      const double* Li = A + (size_t)i * n + c;
-      const double dot = quad_dot4([&](int k) { return Li[k]; }, [&](int k) { return k == 0 ? mcc : Mc[c + k]; },
-                                   i - c, t, qmask);
-      if (t == 0) Mc[i] = __ddiv_rn(-dot, A[(size_t)i * n + i]);
-      __syncwarp(qmask);
+  for (int i0 = 0; i0 < n; i0 += MG_PANEL) {
+    const int i1 = min(i0 + MG_PANEL, n), w = i1 - i0;
+    if (i0 > 0) {
+      const long long np = (long long)w * i0;
+      for (long long pid = q; pid < np; pid += nq) {
+        const int r = (int)(pid / i0), c = (int)(pid - (long long)r * i0);
+        const int p = ((i0 - c) >> 2) << 2;
+        if (p == 0) continue;
+        const double* Li = A + (size_t)(i0 + r) * n + c;
+        const double* Mc = A + (size_t)c * n + c;
+        const double mcd = a.mdiag[c];
+        a.pre[pid * 4 + t] =
+            chain_prefix([&](int k) { return Li[k]; }, [&](int k) { return k == 0 ? mcd : Mc[k]; }, p, t);
+      }
+      mg_sync(a);
     }
+    for (int c = q; c < i1; c += nq) {
+      double* Mc = A + (size_t)c * n + c;  // Mc[k] = m_c[c + k], k >= 1
+      double mcd;
+      if (c >= i0) {
+        mcd = __ddiv_rn(1.0, A[(size_t)c * n + c]);
+        if (t == 0) a.mdiag[c] = mcd;
+      } else {
+        mcd = a.mdiag[c];
+      }
+      const int p = c < i0 ? ((i0 - c) >> 2) << 2 : 0;
+      for (int i = max(i0, c + 1); i < i1; ++i) {
+        const double* Li = A + (size_t)i * n + c;
+        const double s0 = p > 0 ? a.pre[((size_t)(i - i0) * i0 + c) * 4 + t] : 0.0;
+        const double dot =
+            quad_dot4_from(s0, [&](int k) { return Li[k]; }, [&](int k) { return k == 0 ? mcd : Mc[k]; }, p, i - c,
+                           t, qmask);
+        if (t == 0) Mc[i - c] = __ddiv_rn(-dot, A[(size_t)i * n + i]);
+        __syncwarp(qmask);
+      }
+    }
+    mg_sync(a);
   }
 }
 

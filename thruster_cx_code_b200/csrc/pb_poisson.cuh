@@ -115,6 +115,8 @@ enum : int {
 };
 // MgRebuildArgs::status bit: the freed nodes change the level structure; the host rebuilds
 constexpr uint32_t MG_STATUS_HOST = 1u;
+// columns (rows) per panel of the rebuild's Cholesky factor (inverse factor); a multiple of 4
+constexpr int MG_PANEL = 32;
 
 struct MgRebuildArgs {
   int nlevels, max_coarse, ncap;  // ncap: capacity of the coarsest level (cidx, cinv, dense)
@@ -126,6 +128,7 @@ struct MgRebuildArgs {
   double* dense;                  // scratch ncap^2: the coarsest operator, its Cholesky factor
                                   // (lower triangle) and the columns of its inverse (upper)
   double* mdiag;                  // scratch ncap: diagonal of the inverse factor
+  double* pre;                    // scratch ncap x MG_PANEL x 4: chain prefixes of a panel
   int* cidx_new;                  // scratch ncap
   int* pos;                       // scratch, one per node of the coarsest level
   int* counts;                    // MG_CNT_SLOTS ints: active counts per level, flags, totals

@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <functional>
@@ -96,6 +97,7 @@ struct Sim {
   // rebuild of the hierarchy on the device after cells break (k_mg_rebuild)
   double* mg_dense = nullptr;
   double* mg_mdiag = nullptr;
+  double* mg_pre = nullptr;
   int *mg_cidx_new = nullptr, *mg_pos = nullptr;
   int* mg_counts = nullptr;      // MG_CNT_SLOTS (persist across host builds)
   int* mg_dirty = nullptr;
@@ -355,6 +357,7 @@ static void free_levels(Sim* s) {
   dfree(s->cinv);
   dfree(s->mg_dense);
   dfree(s->mg_mdiag);
+  dfree(s->mg_pre);
   dfree(s->mg_cidx_new);
   dfree(s->mg_pos);
 }
@@ -422,6 +425,7 @@ static int32_t build_operator(Sim* s, const uint8_t* isBound_host) {
   CK(cudaMemcpy(s->cinv, H.cinv.data(), (size_t)s->nc * s->nc * sizeof(float), cudaMemcpyHostToDevice));
   CK(dalloc(&s->mg_dense, ncap * ncap));
   CK(dalloc(&s->mg_mdiag, ncap));
+  CK(dalloc(&s->mg_pre, ncap * MG_PANEL * 4));
   CK(dalloc(&s->mg_cidx_new, ncap));
   CK(dalloc(&s->mg_pos, (size_t)H.lev.back().ny * H.lev.back().nx));
   if (!s->nc_dev) CK(dalloc(&s->nc_dev, 1));
@@ -451,7 +455,7 @@ static MgRebuildArgs mg_rebuild_args(Sim* s) {
     B.dinv = D.dinv; B.R = D.R; B.U = D.U; B.z = D.z; B.act = D.act; B.st = D.st;
   }
   a.cidx = s->cidx; a.cinv = s->cinv; a.nc_dev = s->nc_dev;
-  a.dense = s->mg_dense; a.mdiag = s->mg_mdiag; a.cidx_new = s->mg_cidx_new; a.pos = s->mg_pos;
+  a.dense = s->mg_dense; a.mdiag = s->mg_mdiag; a.pre = s->mg_pre; a.cidx_new = s->mg_cidx_new; a.pos = s->mg_pos;
   a.counts = s->mg_counts; a.dirty = s->mg_dirty; a.status = s->mg_status;
   a.bar = s->bar;
   a.errflags = &s->rep_dev->errflags;
@@ -1039,7 +1043,7 @@ static uint64_t state_signature(const pb_sim* h) {
                         s->tile_counter, s->see_key, s->see_xy, s->see_count, s->angles, s->angle_scratch,
                         s->angle_count, s->ds_bits, s->n_sub, s->inj, s->see_spawned, s->skey[0], s->skey[1],
                         s->sval[0], s->sval[1], s->shist, s->sblk, s->rep_dev, h->cx.t, h->cx.c, h->see.t,
-                        h->see.c, s->step_dev, s->ekeep, s->nc_dev, s->mg_dense, s->mg_mdiag, s->mg_cidx_new,
+                        h->see.c, s->step_dev, s->ekeep, s->nc_dev, s->mg_dense, s->mg_mdiag, s->mg_pre, s->mg_cidx_new,
                         s->mg_pos, s->mg_counts, s->mg_dirty, s->mg_status};
   k = fnv(k, ptrs, sizeof(ptrs));
   for (const DevLevel& L : s->lev) k = fnv_v(k, L);

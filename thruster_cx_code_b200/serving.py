@@ -42,6 +42,10 @@ class SweepBatch:
         self.last_launches = 0
         self.last_host_ms = 0.0
 
+    def set_threads(self, threads):
+        """Host threads enqueuing the members' kernels (0: the library's choice)."""
+        _lib.check(self._libh.pb_batch_set_threads(self._h, int(threads)), "pb_batch_set_threads")
+
     def set_graphs(self, on):
         """Capture each batch step shape as a CUDA graph and replay it (pb_batch_set_graphs)."""
         _lib.check(self._libh.pb_batch_set_graphs(self._h, 1 if on else 0), "pb_batch_set_graphs")
