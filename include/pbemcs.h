@@ -179,8 +179,8 @@ int32_t pb_sim_set_solver(pb_sim* s, double tol, double tol_inner, int32_t max_o
 /* Launch shapes (the autotuner's knobs; the reference has no counterpart): blocks per SM
  * of the ion and electron step kernels (1-32, default 8; tiles are handed out by a counter,
  * so any grid covers every particle) and blocks of the field-solve launch (1 to the number
- * of SMs, default all). Results do not depend on either, except the field solve's
- * block-order sums, whose rounding follows the block count. */
+ * of SMs, default all). Results do not depend on either: the field solve sums over a fixed
+ * set of virtual blocks whatever its block count. */
 int32_t pb_sim_set_launch(pb_sim* s, int32_t particle_blocks_per_sm, int32_t solve_blocks);
 /* Kernel variants of the step (the autotuner's knobs; no counterpart in the reference).
  * Every combination gives bit-identical results; they differ in speed only.
@@ -355,7 +355,8 @@ int32_t pb_batch_graph_stats(pb_batch* b, int64_t* out3);
 int32_t pb_batch_timing(pb_batch* b, double* out4);
 /* A member's field-solve cost as the batch measured it (out2[0]: block-milliseconds per
  * launch in its last batch run, 0 before one) and its block share in the last launch planned
- * (out2[1]); pb_batch_run shares each launch's blocks in proportion to the first. */
+ * (out2[1]); pb_batch_run shares each launch's blocks so that the largest cost per block
+ * is as small as it can be (one block each, then each further block to the largest). */
 int32_t pb_sim_batch_share(pb_sim* s, double* out2);
 /* Device memory held by a simulator (bytes, estimated from its capacities). */
 int32_t pb_sim_memory(pb_sim* s, int64_t* bytes);

@@ -24,9 +24,10 @@ best values depend on the grid size and the particle count:
   compaction.  Every combination computes the same bits.
 
 Particle results are identical for every value of these knobs except ``sort_every``,
-which changes only the array order.  The field solve reaches the same FP64 tolerance
-whatever ``max_coarse``, ``tol_inner`` and ``solve_blocks`` are, but its rounding follows
-them.
+which changes only the array order, and the solver's ``max_coarse``, ``tol_inner`` and
+``smoother_sweeps``: the field solve reaches the same FP64 tolerance whatever they are,
+but its rounding follows them.  ``solve_blocks`` changes nothing but speed (the solve's
+sums run over a fixed set of virtual blocks).
 
 With ``horizon_steps`` set, the cost of a setting is its step time plus its multigrid
 build time (host, measured) spread over that many steps: short-lived simulators, such as

@@ -9,6 +9,7 @@
 // own grid barrier and reductions (k_poisson_batch).
 
 #include <condition_variable>
+#include <queue>
 #include <thread>
 
 // Host threads that enqueue the members' step halves in parallel (the streams form): a
@@ -122,12 +123,12 @@ struct SolveLaunch {
   std::vector<int> inst;  // instances (indices into the run's simulator list)
   size_t args_off;        // first argument block
   size_t blk_off;         // first entry of the block map
+  size_t map_len;         // entries of the block map: an offset per block, then per block its
+                          // instance count and instances
   int nblocks;
   size_t smem;
 };
 
-// Blocks of one launch shared out in proportion to each instance's node count (at least
-// one block each, at most the instance's own full-device grid).
 // After a batch run: block-ns per field-solve launch of the run's solves (their counters
 // were cleared at its start).  The estimate moves only when the run's figure is off by more
 // than 30%, so that the block shares, and the step graphs captured with them, stay put while
@@ -168,35 +169,73 @@ std::vector<long> solve_work(pb_sim* const* sims, const std::vector<int>& inst) 
   return work;
 }
 
-std::vector<int> share_blocks(const std::vector<long>& work, int total) {
+// Blocks of one launch shared out by each instance's cost (solve_work): the smallest makespan
+// T (found by bisection) for which the instances costing more than T get ceil(cost / T) blocks
+// of their own and the others fit, first fit by decreasing cost, into blocks of capacity T that
+// run them one after another; the blocks left over go one at a time to the instance, alone on
+// its blocks, with the largest cost per block.  Packing the cheap instances frees blocks that
+// one block each would tie up.  Returns per block the instances (indices into work) it runs,
+// an instance's own blocks consecutive.
+std::vector<std::vector<int>> plan_blocks(const std::vector<long>& work, int total) {
   const int m = (int)work.size();
-  std::vector<int> nb(m, 1);
-  long sum = 0;
-  for (long w : work) sum += w;
-  int left = total - m;
-  if (left > 0 && sum > 0) {
-    std::vector<std::pair<double, int>> frac;
-    int given = 0;
+  auto pack = [&](double T, std::vector<int>* own, std::vector<std::vector<int>>* bins) -> int {
+    int need = 0;
+    std::vector<int> small;
     for (int i = 0; i < m; ++i) {
-      double want = (double)left * (double)work[i] / (double)sum;
-      int add = (int)want;
-      nb[i] += add;
-      given += add;
-      frac.push_back({want - add, i});
+      if ((double)work[i] > T) {
+        const int k = (int)std::ceil((double)work[i] / T);
+        need += k;
+        if (own) (*own)[i] = k;
+      } else {
+        small.push_back(i);
+      }
     }
-    std::sort(frac.begin(), frac.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
-      return a.first > b.first || (a.first == b.first && a.second < b.second);
-    });
-    for (int k = 0; k < left - given && k < m; ++k) nb[frac[k].second] += 1;
+    std::stable_sort(small.begin(), small.end(), [&](int a, int b) { return work[a] > work[b]; });
+    std::vector<double> load;
+    std::vector<std::vector<int>> bl;
+    for (int i : small) {
+      size_t k = 0;
+      while (k < load.size() && load[k] + (double)work[i] > T) ++k;
+      if (k == load.size()) { load.push_back(0.0); bl.emplace_back(); }
+      load[k] += (double)work[i];
+      bl[k].push_back(i);
+    }
+    if (bins) *bins = bl;
+    return need + (int)bl.size();
+  };
+  double sum = 0.0, mx = 0.0;
+  for (long w : work) { sum += (double)w; mx = std::max(mx, (double)w); }
+  double lo = sum / total, hi = std::max(mx, lo);
+  for (int it = 0; it < 64 && hi > lo * (1.0 + 1e-9); ++it) {
+    const double mid = 0.5 * (lo + hi);
+    if (pack(mid, nullptr, nullptr) <= total) hi = mid; else lo = mid;
   }
-  // every block of the launch belongs to an instance
-  int sum_nb = 0, big = 0;
-  for (int i = 0; i < m; ++i) {
-    sum_nb += nb[i];
-    if (work[i] > work[big]) big = i;
+  std::vector<int> own(m, 0);
+  std::vector<std::vector<int>> bins;
+  int used = pack(hi, &own, &bins);
+  // an instance alone in its block takes further blocks like one with blocks of its own
+  std::vector<std::vector<int>> shared;
+  for (auto& b : bins) {
+    if (b.size() == 1) own[b[0]] = 1;
+    else shared.push_back(b);
   }
-  if (m > 0 && sum_nb < total) nb[big] += total - sum_nb;
-  return nb;
+  using E = std::pair<double, int>;
+  auto lower = [](const E& a, const E& b) { return a.first < b.first || (a.first == b.first && a.second > b.second); };
+  std::priority_queue<E, std::vector<E>, decltype(lower)> q(lower);
+  for (int i = 0; i < m; ++i)
+    if (own[i] > 0) q.push({(double)work[i] / own[i], i});
+  for (; used < total && !q.empty(); ++used) {
+    const int i = q.top().second;
+    q.pop();
+    own[i] += 1;
+    q.push({(double)work[i] / own[i], i});
+  }
+  std::vector<std::vector<int>> blocks;
+  for (int i = 0; i < m; ++i)
+    for (int k = 0; k < own[i]; ++k) blocks.push_back({i});
+  for (auto& b : shared) blocks.push_back(b);
+  while ((int)blocks.size() < total) blocks.emplace_back();
+  return blocks;
 }
 
 // Device memory held by one simulator (an estimate from its capacities, for admission).
@@ -358,7 +397,7 @@ static int32_t batch_run_graphs(pb_batch* b, pb_sim* const* sims, int n, const p
     for (; pi < plan.size() && plan[pi].step == k; ++pi) Ls.push_back(&plan[pi]);
     const size_t args0 = Ls.empty() ? 0 : Ls.front()->args_off, blk0 = Ls.empty() ? 0 : Ls.front()->blk_off;
     size_t nargs = 0, nblk = 0;
-    for (const SolveLaunch* L : Ls) { nargs += L->inst.size(); nblk += (size_t)L->nblocks; }
+    for (const SolveLaunch* L : Ls) { nargs += L->inst.size(); nblk += L->map_len; }
     uint64_t key = fnv_v(1469598103934665603ull, n);
     for (int i = 0; i < n; ++i) {
       key = fnv_v(key, sims[i]);
@@ -542,7 +581,8 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
       L.nblocks = b->num_sms;
       L.smem = 0;  // set with the block shares
       nargs += L.inst.size();
-      nblk += (size_t)L.nblocks;
+      L.map_len = 3 * (size_t)L.nblocks + L.inst.size();  // bound: see plan_blocks
+      nblk += L.map_len;
       plan.push_back(L);
     }
   }
@@ -571,29 +611,44 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
     b->dblk_cap = b->blk_cap;
   }
   for (SolveLaunch& L : plan) {
-    std::vector<int> nb = share_blocks(solve_work(sims, L.inst), L.nblocks);
+    const std::vector<std::vector<int>> blocks = plan_blocks(solve_work(sims, L.inst), L.nblocks);
+    if ((int)blocks.size() != L.nblocks) return fail(PB_ERR_STATE, "pb_batch_run: block plan does not cover the launch");
+    std::vector<int> first(L.inst.size(), -1), count(L.inst.size(), 0);
+    int* map = b->hblk + L.blk_off;
+    int at = L.nblocks;
+    for (int q = 0; q < L.nblocks; ++q) {
+      map[q] = at;
+      map[at++] = (int)blocks[q].size();
+      for (int j : blocks[q]) {
+        map[at++] = j;
+        if (blocks[q].size() == 1) {
+          if (first[j] < 0) first[j] = q;
+          ++count[j];
+        } else {
+          first[j] = q;
+          count[j] = 1;
+        }
+      }
+    }
     L.smem = 0;
-    int blk0 = 0;
     for (size_t j = 0; j < L.inst.size(); ++j) {
       Sim* s = &sims[L.inst[j]]->s;
       const pb_step_params& p = params[(size_t)L.inst[j] * K + L.step];
+      if (first[j] < 0 || count[j] > s->num_sms)
+        return fail(PB_ERR_STATE, "pb_batch_run: an instance without blocks in its field-solve launch");
       PoissonArgs a = poisson_args(s, p.picard_iters, &p);
-      if (nb[j] > s->num_sms) return fail(PB_ERR_STATE, "pb_batch_run: block share above the device's SM count");
-      a.blk0 = blk0;
-      a.nblk = nb[j];
+      a.blk0 = first[j];
+      a.nblk = count[j];
       set_up_tiles(s, &a);
       L.smem = std::max(L.smem, mg_solve_smem_bytes(s->ncap, a.nvb, a.nblk));
       a.trace = s->trace_on ? s->ptrace : nullptr;  // traced members run without graphs
       b->hargs[L.args_off + j] = a;
       MgRebuildArgs m = mg_rebuild_args(s);
-      m.blk0 = blk0;
-      m.nblk = nb[j];
+      m.blk0 = first[j];
+      m.nblk = count[j];
       b->hmg[L.args_off + j] = m;
-      s->batch_blocks = nb[j];
-      for (int q = 0; q < nb[j]; ++q) b->hblk[L.blk_off + blk0 + q] = (int)j;
-      blk0 += nb[j];
+      s->batch_blocks = count[j];
     }
-    if (blk0 != L.nblocks) return fail(PB_ERR_STATE, "pb_batch_run: block shares do not cover the launch");
   }
   // ---- per-instance events
   while ((int)b->ev_inst.size() < n) {

@@ -662,14 +662,18 @@ __device__ void mg_rebuild_body(const MgRebuildArgs& a) {
 __global__ void __launch_bounds__(PT, 1) k_mg_rebuild(const __grid_constant__ MgRebuildArgs a) { mg_rebuild_body(a); }
 
 __global__ void __launch_bounds__(PT, 1) k_mg_rebuild_batch(const MgRebuildArgs* __restrict__ args,
-                                                            const int* __restrict__ blk_inst) {
+                                                            const int* __restrict__ blk_map) {
   __shared__ MgRebuildArgs sa;
-  const int inst = blk_inst[blockIdx.x];
-  const int* src = reinterpret_cast<const int*>(args + inst);
-  int* dst = reinterpret_cast<int*>(&sa);
-  for (int k = threadIdx.x; k < (int)(sizeof(MgRebuildArgs) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
-  __syncthreads();
-  mg_rebuild_body(sa);
+  const int* lst = blk_map + blk_map[blockIdx.x];
+  const int cnt = lst[0];
+  for (int q = 0; q < cnt; ++q) {
+    const int* src = reinterpret_cast<const int*>(args + lst[1 + q]);
+    int* dst = reinterpret_cast<int*>(&sa);
+    for (int k = threadIdx.x; k < (int)(sizeof(MgRebuildArgs) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    __syncthreads();
+    mg_rebuild_body(sa);
+    __syncthreads();
+  }
 }
 
 }  // namespace pb

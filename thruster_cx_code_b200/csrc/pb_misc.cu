@@ -276,11 +276,11 @@ __global__ void k_erosion_break(double* damage, uint8_t* isBound, uint8_t* cls, 
   if (cntb) atomicAdd(broken, cntb);
 }
 
-// After a break the fine-level smoother weights follow the new node classes, so the
-// field solves left in a multi-step run precondition the freed nodes too; the coarse
-// levels keep the old operator until the host rebuilds the hierarchy.  The V-cycle stays
-// symmetric positive definite: its smoother part is, once every free node has its weight,
-// and the coarse part adds a semidefinite term.  The weights are the host build's,
+// After a break the fine-level smoother weights follow the new node classes, and the
+// hierarchy is marked dirty: k_mg_rebuild forms the coarse levels again before the next
+// field solve.  (Should it leave them to the host, the V-cycle with the old coarse levels
+// stays symmetric positive definite: its smoother part is, once every free node has its
+// weight, and the coarse part adds a semidefinite term.)  The weights are the host build's,
 // omega / (4 - Neumann neighbours) in double rounded to float, 0 off the free nodes.
 __global__ void k_refresh_dinv0(const uint8_t* cls, float* dinv, int ny, int nx, int periodic, const int* broken,
                                 int* mg_dirty) {

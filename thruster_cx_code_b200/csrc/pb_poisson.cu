@@ -784,14 +784,18 @@ __device__ __forceinline__ void poisson_body(const PoissonArgs& a) {
 __global__ void __launch_bounds__(PT, 1) k_poisson(const __grid_constant__ PoissonArgs a) { poisson_body(a); }
 
 __global__ void __launch_bounds__(PT, 1) k_poisson_batch(const PoissonArgs* __restrict__ args,
-                                                         const int* __restrict__ blk_inst) {
+                                                         const int* __restrict__ blk_map) {
   __shared__ PoissonArgs sa;
-  const int inst = blk_inst[blockIdx.x];
-  const int* src = reinterpret_cast<const int*>(args + inst);
-  int* dst = reinterpret_cast<int*>(&sa);
-  for (int k = threadIdx.x; k < (int)(sizeof(PoissonArgs) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
-  __syncthreads();
-  poisson_body(sa);
+  const int* lst = blk_map + blk_map[blockIdx.x];
+  const int cnt = lst[0];
+  for (int q = 0; q < cnt; ++q) {
+    const int* src = reinterpret_cast<const int*>(args + lst[1 + q]);
+    int* dst = reinterpret_cast<int*>(&sa);
+    for (int k = threadIdx.x; k < (int)(sizeof(PoissonArgs) / sizeof(int)); k += blockDim.x) dst[k] = src[k];
+    __syncthreads();
+    poisson_body(sa);
+    __syncthreads();
+  }
 }
 
 }  // namespace pb

@@ -185,13 +185,15 @@ inline void fine_up_tiles(int ny, int nx, int nblk, int* ty_out, int* tx_out) {
 // tolerance, not bit for bit, unlike the particle arithmetic.
 // One instance on every block of the launch.
 __global__ void k_poisson(const __grid_constant__ PoissonArgs a);
-// Several instances in one launch: block b solves instance blk_inst[b] together with the
-// other blocks of that instance's contiguous range (args[i].blk0, args[i].nblk).
-__global__ void k_poisson_batch(const PoissonArgs* __restrict__ args, const int* __restrict__ blk_inst);
+// Several instances in one launch: block b runs the instances listed at blk_map[blk_map[b]]
+// (a count, then indices into args) one after another, each together with the other blocks of
+// its contiguous range (args[i].blk0, args[i].nblk): an instance with blocks of its own, or
+// several one-block instances packed into one block.
+__global__ void k_poisson_batch(const PoissonArgs* __restrict__ args, const int* __restrict__ blk_map);
 // The hierarchy rebuilt from the node classes after cells broke (no-op unless *dirty), on
 // every block of the launch, or per instance as k_poisson_batch.
 __global__ void k_mg_rebuild(const __grid_constant__ MgRebuildArgs a);
-__global__ void k_mg_rebuild_batch(const MgRebuildArgs* __restrict__ args, const int* __restrict__ blk_inst);
+__global__ void k_mg_rebuild_batch(const MgRebuildArgs* __restrict__ args, const int* __restrict__ blk_map);
 #endif
 
 }  // namespace pb
