@@ -315,6 +315,12 @@ float pb_host_seq_add_f32d(float s, double c, uint32_t n);
 double pb_host_philox_uniform(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j);
 double pb_host_philox_normal(uint64_t seed, uint64_t pid, uint32_t site, uint32_t step, uint32_t j);
 float pb_host_percentile95(const float* sorted, int32_t n);
+/* The block plan of one batched field-solve launch (pb_batch_run): m members of positive cost
+ * (block-time of one launch) on total >= m blocks.  Per member: its first block, its block
+ * count, and packed = 1 when it shares its one block with other members (run one after
+ * another). */
+int32_t pb_host_plan_blocks(const int64_t* work, int32_t m, int32_t total, int32_t* first, int32_t* count,
+                            int32_t* packed);
 
 /* ---------------------------------------------------------------- batched instances
  * Several simulators advanced together on one GPU: sweep points of a perveance or

@@ -118,6 +118,7 @@ PROTOTYPES = {
     "pb_batch_graph_stats": (i32, [vp, P(C.c_int64)]),
     "pb_sim_memory": (i32, [vp, P(C.c_int64)]),
     "pb_host_seq_add_f32d": (f32, [f32, f64, u32]),
+    "pb_host_plan_blocks": (i32, [P(C.c_int64), i32, i32, P(i32), P(i32), P(i32)]),
     "pb_host_philox_uniform": (f64, [u64, u64, u32, u32, u32]),
     "pb_host_philox_normal": (f64, [u64, u64, u32, u32, u32]),
     "pb_host_percentile95": (f32, [vp, i32]),

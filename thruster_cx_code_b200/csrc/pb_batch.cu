@@ -857,6 +857,26 @@ int32_t pb_batch_run(pb_batch* b, pb_sim* const* sims, int32_t n, const pb_step_
   return PB_OK;
 }
 
+int32_t pb_host_plan_blocks(const int64_t* work, int32_t m, int32_t total, int32_t* first, int32_t* count,
+                            int32_t* packed) {
+  if (!work || !first || !count || !packed || m < 1 || total < m)
+    return fail(PB_ERR_ARG, "pb_host_plan_blocks: need work, outputs and 1 <= m <= total");
+  std::vector<long> w(m);
+  for (int i = 0; i < m; ++i) {
+    if (work[i] < 1) return fail(PB_ERR_ARG, "pb_host_plan_blocks: costs must be positive");
+    w[i] = (long)work[i];
+  }
+  const std::vector<std::vector<int>> blocks = plan_blocks(w, total);
+  for (int i = 0; i < m; ++i) { first[i] = -1; count[i] = 0; packed[i] = 0; }
+  for (int q = 0; q < (int)blocks.size(); ++q)
+    for (int j : blocks[q]) {
+      if (first[j] < 0) first[j] = q;
+      ++count[j];
+      packed[j] = blocks[q].size() > 1 ? 1 : 0;
+    }
+  return PB_OK;
+}
+
 int32_t pb_batch_set_threads(pb_batch* b, int32_t threads) {
   if (!b || threads < 0 || threads > 64) return fail(PB_ERR_ARG, "pb_batch_set_threads: 0 to 64 threads");
   CK(cudaSetDevice(b->device));
