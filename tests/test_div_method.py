@@ -6,6 +6,9 @@ q = x * inv (inv = RN(1/d)), one correction q += (x - q d) inv, accepted when
 float32 operands is emulated exactly in float64 here: a * b is exact in float64 and, for
 q within a few ulps of x / d, so is the sum, which is then rounded once to float32.  The
 full check (every float |x| < 64, ten spacings) ran on the host in C; this samples it.
+
+The second test covers the cell-index tricks the particle kernels use beside it (floor,
+fraction, rint and truncation by adding 2^23).
 """
 import numpy as np
 
@@ -46,3 +49,38 @@ def test_div_rn_checked_matches_ieee():
             assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
             # nearly every position in the grid takes the fast path
             assert accept[:pos.size].mean() > 0.999
+
+
+# The integer and fraction tricks of the particle kernels (floor_frac in csrc/pb_particles.cu,
+# rint_clip and trunc_clip in csrc/pb_common.cuh): for 0 <= q < 2^22 the float32 sum q + 2^23,
+# rounded to nearest (rint) or down (floor), is an integer in [2^23, 2^24) whose low mantissa
+# bits hold the result; q minus that integer is exact in float32.
+def _sum_bits(q, down):
+    if down:  # round down: the exact sum (float64) floored onto the integer grid of [2^23, 2^24)
+        t = np.floor(q.astype(np.float64) + 8388608.0).astype(F32)
+    else:     # float32 addition rounds to nearest, ties to even
+        t = (q + F32(8388608.0)).astype(F32)
+    return t, t.view(np.int32).astype(np.int64) - 0x4B000000
+
+
+def _samples(rng):
+    k = rng.integers(0, 4194304, 400_000).astype(F32)
+    ties = (k + F32(0.5)).astype(F32)
+    q = np.concatenate([rng.uniform(0.0, 4096.0, 1_000_000).astype(F32), k, ties,
+                        np.nextafter(ties, F32(0)), np.nextafter(ties, F32(np.inf)),
+                        rng.integers(0, 0x4A800000, 500_000, dtype=np.uint32).view(F32),
+                        np.array([0.0, 0.5, 1.5, 2.5, 4194303.5, np.nextafter(F32(4194304.0), F32(0))], F32)])
+    return q[(q >= 0) & (q < F32(4194304.0))]
+
+
+def test_floor_frac_and_rint_by_adding_2p23():
+    rng = np.random.default_rng(11)
+    q = _samples(rng)
+    t, fl = _sum_bits(q, down=True)
+    assert np.array_equal(fl, np.floor(q).astype(np.int64))
+    frac = (q - (t - F32(8388608.0)).astype(F32)).astype(F32)
+    assert np.array_equal(frac.astype(np.float64), q.astype(np.float64) - np.floor(q.astype(np.float64)))
+    _, rn = _sum_bits(q, down=False)
+    assert np.array_equal(rn, np.rint(q).astype(np.int64))
+    # trunc_clip: astype(int) of a non-negative float is its floor
+    assert np.array_equal(fl, q.astype(np.int64))

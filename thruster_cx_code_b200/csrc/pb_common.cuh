@@ -115,6 +115,21 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       : "memory");
 }
 
+// np.clip(np.rint(q).astype(int), lo, hi) for 0 <= lo <= hi < 2^22.  For 0 <= q < 2^22 the
+// float sum q + 2^23 is rint(q) + 2^23 (rounded to nearest, ties to even, as rintf rounds),
+// an integer held in the low mantissa bits: no rounding or conversion instruction.  Other q
+// (negative, large, NaN) take NumPy's cast.
+__device__ __forceinline__ int rint_clip(float q, int lo, int hi) {
+  if ((q >= 0.0f) & (q < 4194304.0f)) return min(max(__float_as_int(__fadd_rn(q, 8388608.0f)) - 0x4B000000, lo), hi);
+  return (int)clampll(np_f2i64(rintf(q)), lo, hi);
+}
+// the same for np.clip(q.astype(int), lo, hi): for q >= 0 the cast truncates, i.e. floors,
+// and q + 2^23 rounded down is floor(q) + 2^23
+__device__ __forceinline__ int trunc_clip(float q, int lo, int hi) {
+  if ((q >= 0.0f) & (q < 4194304.0f)) return min(max(__float_as_int(__fadd_rd(q, 8388608.0f)) - 0x4B000000, lo), hi);
+  return (int)clampll(np_f2i64(truncf(q)), lo, hi);
+}
+
 // cell index of np.clip(np.round(s / d).astype(int), lo, hi)   (float32 division)
 __device__ __forceinline__ int cell_round(float s, float d, int lo, int hi) {
   float q = __fdiv_rn(s, d);

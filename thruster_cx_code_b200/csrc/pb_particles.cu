@@ -77,24 +77,34 @@ __global__ void k_e_corners(const float* __restrict__ Ex, const float* __restric
 // remaining operations are kept, so signed zeros come out as in the reference.
 // floor(q) as an int and the fraction q - floor(q), exactly and without conversion
 // instructions, for 0 <= q < 2^22: adding 2^23 with rounding down leaves floor(q) in the
-// low mantissa bits of the sum, and q minus the floor is exact in float.  Returns false
-// for any other q (NaN included); the caller then takes the general path.
+// low mantissa bits of the sum, and q minus the floor is exact in float.  Returns whether
+// q is in that range (false for NaN); fl and frac are meaningful only then, and the
+// caller takes the general path otherwise.  No branch, so that the callers can test both
+// coordinates with one.
 __device__ __forceinline__ bool floor_frac(float q, int& fl, float& frac) {
-  if (!(q >= 0.0f && q < 4194304.0f)) return false;
   const float t = __fadd_rd(q, 8388608.0f);
   fl = __float_as_int(t) - 0x4B000000;
   frac = __fsub_rn(q, __fsub_rn(t, 8388608.0f));
-  return true;
+  return (q >= 0.0f) & (q < 4194304.0f);
 }
 
 // RN(x / d) without the reciprocal instruction: q = x * inv (inv = RN(1/d)) and one
 // Markstein correction q += (x - q d) inv, accepted when |x - q d| < ulp(q) |d| / 2.  The
 // residual is exact (one FMA) for q within an ulp of x / d, and a quotient of two floats
 // is never a midpoint, so the test holds exactly when q is the correctly rounded quotient.
-// Zero, powers of two (whose lower half-ulp is smaller), tiny and non-finite q fall back
-// to the division.  Checked on the host against IEEE division for every float |x| < 64
-// and ten grid spacings: no mismatch, the test accepts 84% of those inputs (nearly all
-// positions in a grid).
+// Zero, powers of two (whose lower half-ulp is smaller), tiny and non-finite q fail the
+// test.  Checked on the host against IEEE division for every float |x| < 64 and ten grid
+// spacings: no mismatch, the test accepts 84% of those inputs (nearly all positions in a
+// grid).  div_fast returns whether q is accepted, without a branch.
+__device__ __forceinline__ bool div_fast(float x, float d, float inv, float& q) {
+  q = __fmul_rn(x, inv);
+  q = __fmaf_rn(__fmaf_rn(-q, d, x), inv, q);
+  const float r = __fmaf_rn(-q, d, x);
+  const unsigned int b = __float_as_uint(q), e = b & 0x7F800000u;
+  const float h = __fmul_rn(__uint_as_float((e - (24u << 23)) & 0x7F800000u), fabsf(d));
+  return (e > (26u << 23)) & (e < 0x7F800000u) & ((b & 0x007FFFFFu) != 0u) & (fabsf(r) < h);
+}
+// The same with a branch per quotient, for callers that need one quotient at a time.
 __device__ __forceinline__ float div_rn_checked(float x, float d, float inv) {
   float q = __fmul_rn(x, inv);
   q = __fmaf_rn(__fmaf_rn(-q, d, x), inv, q);
@@ -108,24 +118,34 @@ __device__ __forceinline__ float div_rn_checked(float x, float d, float inv) {
 }
 
 // CORN: E is gathered from the corner array Ec (B = 0 only); otherwise from Ex, Ey.
-// LIGHT: the cell position from div_rn_checked and, inside the grid, the cell index and
-// fraction from floor_frac: six fewer XU-pipe instructions (reciprocal and conversions)
-// per substep.  The XU pipe limits the electron kernel (many substeps); kernels with
-// fewer substeps and more live registers run faster without it.
+// LIGHT: the cell position from div_fast and, inside the grid, the cell index and fraction
+// from floor_frac, each pair tested with one branch: six fewer XU-pipe instructions
+// (reciprocal and conversions) per substep.  The step kernels are bound by instruction
+// issue and use it (measured 7% faster for the ion step, whose 64 registers it does not
+// raise); the module-level push and the B != 0 path keep the plain division.
 // Cell and bilinear weights of a push at (x, y): float32 quotients x / dx, y / dy, the
 // clamped floor cell (ix0, iy0) and the float64 weights of the reference's gather.
 template <bool LIGHT>
 __device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, float dxf, float dyf, float inv_dx,
                                           float inv_dy, float* q_start, int& ix0, int& iy0, double& w00,
                                           double& w10, double& w01, double& w11) {
-  const float ixf = LIGHT ? div_rn_checked(x, dxf, inv_dx) : __fdiv_rn(x, dxf);
-  const float iyf = LIGHT ? div_rn_checked(y, dyf, inv_dy) : __fdiv_rn(y, dyf);
+  float ixf, iyf;
+  if (LIGHT) {
+    const bool okq = div_fast(x, dxf, inv_dx, ixf) & div_fast(y, dyf, inv_dy, iyf);
+    if (!okq) { ixf = __fdiv_rn(x, dxf); iyf = __fdiv_rn(y, dyf); }
+  } else {
+    ixf = __fdiv_rn(x, dxf);
+    iyf = __fdiv_rn(y, dyf);
+  }
   if (q_start) { q_start[0] = ixf; q_start[1] = iyf; }  // x / dx, y / dy at the start position
   double fx, fy;
   // inside the grid the clamp is a no-op and ixf - ix0 is the exact float fraction
   int fxi, fyi;
   float frx, fry;
-  if (LIGHT && floor_frac(ixf, fxi, frx) && fxi <= nx - 2 && floor_frac(iyf, fyi, fry) && fyi <= ny - 2) {
+  bool inside = false;
+  if (LIGHT)
+    inside = floor_frac(ixf, fxi, frx) & floor_frac(iyf, fyi, fry) & (fxi <= nx - 2) & (fyi <= ny - 2);
+  if (inside) {
     ix0 = fxi;
     iy0 = fyi;
     fx = (double)frx;
@@ -145,8 +165,8 @@ __device__ __forceinline__ void push_update_b0(float& x, float& y, float& vx, fl
                                                double ey, double h, float dtf) {
   const double vmx = DADD((double)vx, DMUL(h, ex));
   const double vmy = DADD((double)vy, DMUL(h, ey));
-  if (vmx != 0.0 && vmy != 0.0 && vz != 0.0f && fabs(vmx) < INFINITY && fabs(vmy) < INFINITY &&
-      fabsf(vz) < INFINITY) {
+  if ((vmx != 0.0) & (vmy != 0.0) & (vz != 0.0f) & (fabs(vmx) < INFINITY) & (fabs(vmy) < INFINITY) &
+      (fabsf(vz) < INFINITY)) {
     // every cross-product term below is a signed zero (t = s = h * (+0)), and a finite
     // nonzero value plus a zero is that value: the rotation is the identity, bit for bit
     // (vz goes to double and back unchanged, so it is left as it is)
@@ -195,7 +215,12 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
       const float4* q = eb.box + 2 * (oy * TB_W + ox);
       gather4v(q[0], q[1], w00, w10, w01, w11, ex, ey);
     } else {
-      gather4c(Ec, r0 + ix0, w00, w10, w01, w11, ex, ey);
+      if (LIGHT) {  // 32-bit cell index (a grid has fewer than 2^30 cells): fewer instructions
+        const float4* e = Ec + 2 * (iy0 * nx + ix0);
+        gather4v(__ldg(e), __ldg(e + 1), w00, w10, w01, w11, ex, ey);
+      } else {
+        gather4c(Ec, r0 + ix0, w00, w10, w01, w11, ex, ey);
+      }
     }
   } else {
     ex = gather4(Ex, r0, r1, ix0, ix1, w00, w10, w01, w11);
@@ -390,11 +415,29 @@ __device__ __forceinline__ double gather_sub(const float* __restrict__ F, size_t
 // Ec non-null: E from the corner array (same values and arithmetic as gather_sub)
 __device__ __forceinline__ double predicted_ds(float x, float y, float vx, float vy, float vz,
                                                const float* Ex, const float* Ey, const float4* Ec, int nx, int ny,
-                                               float dxf, float dyf, double qm, float dtf, double dt2) {
-  float ixf = __fdiv_rn(x, dxf), iyf = __fdiv_rn(y, dyf);
-  long long ix0 = clampll(np_f2i64(floorf(ixf)), 0, nx - 2);
-  long long iy0 = clampll(np_f2i64(floorf(iyf)), 0, ny - 2);
-  double fx = DSUB((double)ixf, (double)ix0), fy = DSUB((double)iyf, (double)iy0);
+                                               float dxf, float dyf, double qm, float dtf, double dt2,
+                                               float inv_dx = 0.0f, float inv_dy = 0.0f) {
+  // with the corner array (the step's path): the cell as in push_cell<true>
+  float ixf, iyf;
+  long long ix0, iy0;
+  double fx, fy;
+  bool inside = false;
+  int fxi = 0, fyi = 0;
+  float frx = 0.0f, fry = 0.0f;
+  if (Ec) {
+    const bool okq = div_fast(x, dxf, inv_dx, ixf) & div_fast(y, dyf, inv_dy, iyf);
+    if (!okq) { ixf = __fdiv_rn(x, dxf); iyf = __fdiv_rn(y, dyf); }
+    inside = floor_frac(ixf, fxi, frx) & floor_frac(iyf, fyi, fry) & (fxi <= nx - 2) & (fyi <= ny - 2);
+  } else {
+    ixf = __fdiv_rn(x, dxf); iyf = __fdiv_rn(y, dyf);
+  }
+  if (inside) {
+    ix0 = fxi; iy0 = fyi; fx = (double)frx; fy = (double)fry;
+  } else {
+    ix0 = clampll(np_f2i64(floorf(ixf)), 0, nx - 2);
+    iy0 = clampll(np_f2i64(floorf(iyf)), 0, ny - 2);
+    fx = DSUB((double)ixf, (double)ix0); fy = DSUB((double)iyf, (double)iy0);
+  }
   size_t r0 = (size_t)iy0 * nx, r1 = (size_t)(iy0 + 1) * nx;
   double ex, ey;
   if (Ec) {
@@ -422,6 +465,7 @@ __global__ void k_substep_reduce(const float* __restrict__ x, const float* __res
   pdl_enter();
   int n = n_dev ? *n_dev : n_host;
   unsigned long long m = 0ull;
+  const float inv_dx = __frcp_rn(dxf), inv_dy = __frcp_rn(dyf);
   // four particles per thread and pass (16-byte loads of each array), so that a thread
   // has four sets of loads and gathers in flight; the maximum does not depend on the
   // order.  Arrays that do not all start 16-byte aligned take the one-by-one loop.
@@ -436,10 +480,10 @@ __global__ void k_substep_reduce(const float* __restrict__ x, const float* __res
     const float4 U = __ldg(reinterpret_cast<const float4*>(vx) + q);
     const float4 V = __ldg(reinterpret_cast<const float4*>(vy) + q);
     const float4 W = __ldg(reinterpret_cast<const float4*>(vz) + q);
-    const double d0 = predicted_ds(X.x, Y.x, U.x, V.x, W.x, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2);
-    const double d1 = predicted_ds(X.y, Y.y, U.y, V.y, W.y, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2);
-    const double d2 = predicted_ds(X.z, Y.z, U.z, V.z, W.z, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2);
-    const double d3 = predicted_ds(X.w, Y.w, U.w, V.w, W.w, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2);
+    const double d0 = predicted_ds(X.x, Y.x, U.x, V.x, W.x, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
+    const double d1 = predicted_ds(X.y, Y.y, U.y, V.y, W.y, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
+    const double d2 = predicted_ds(X.z, Y.z, U.z, V.z, W.z, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
+    const double d3 = predicted_ds(X.w, Y.w, U.w, V.w, W.w, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
     const unsigned long long b0 = (unsigned long long)__double_as_longlong(d0);
     const unsigned long long b1 = (unsigned long long)__double_as_longlong(d1);
     const unsigned long long b2 = (unsigned long long)__double_as_longlong(d2);
@@ -449,7 +493,7 @@ __global__ void k_substep_reduce(const float* __restrict__ x, const float* __res
     m = b > m ? b : m;
   }
   for (int i = 4 * n4 + t0; i < n; i += stride) {
-    double ds = predicted_ds(x[i], y[i], vx[i], vy[i], vz[i], Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2);
+    double ds = predicted_ds(x[i], y[i], vx[i], vy[i], vz[i], Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
     unsigned long long b = (unsigned long long)__double_as_longlong(ds);
     m = b > m ? b : m;
   }
@@ -765,11 +809,11 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
         const uint32_t pid = a.src.id[i];
         const float x0 = x, y0 = y;
         float q0[2];  // x0 / dx, y0 / dy (correctly rounded), from the first substep
-        boris_push_one<HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h,
-                                      dtf, a.Ec, 0.0f, 0.0f, q0, eb);
+        boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
+                                              a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy, q0, eb);
         for (int s = 1; s < n_sub; ++s)
-          boris_push_one<HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf, a.dyf, h,
-                                        dtf, a.Ec, 0.0f, 0.0f, nullptr, eb);
+          boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
+                                                a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy, nullptr, eb);
         if (a.periodic) y = np_modf_pos(y, a.Lyf);
         // the final cell, the PPC cell and the deposit cell all round or truncate the same
         // correctly rounded quotients (what rint_div and trunc_div return)
@@ -779,11 +823,11 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
         // final-cell and path hits (:1326-1336).  The 8 path samples lie in cells at most
         // max(|di|, |dj|) + 1 (Chebyshev) from the start cell; they are examined only when
         // that reaches the distance from the start cell to the nearest bound node.
-        const int icx = (int)clampll(np_f2i64(rintf(qx)), 0, a.nx - 1);
-        const int icy = (int)clampll(np_f2i64(rintf(qy)), 0, a.ny - 1);
+        const int icx = rint_clip(qx, 0, a.nx - 1);
+        const int icy = rint_clip(qy, 0, a.ny - 1);
         const bool hit_final = __ldg(a.isBound + (size_t)icy * a.nx + icx) != 0;
-        const int sx0 = (int)clampll(np_f2i64(rintf(q0[0])), 0, a.nx - 1);
-        const int sy0 = (int)clampll(np_f2i64(rintf(q0[1])), 0, a.ny - 1);
+        const int sx0 = rint_clip(q0[0], 0, a.nx - 1);
+        const int sy0 = rint_clip(q0[1], 0, a.ny - 1);
         const int reach = max(abs(icx - sx0), abs(icy - sy0)) + 1;
         SegHit sh;
         sh.hit = false; sh.ix = icx; sh.iy = icy;
@@ -908,10 +952,8 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
             }
           }
           // PPC map with truncated cells (:1749-1757), next-step deposit cell (rounded)
-          long long tx = clampll(np_f2i64(truncf(qx)), 0, a.nx - 1);
-          long long ty = clampll(np_f2i64(truncf(qy)), 0, a.ny - 1);
-          ppc_cell = (int)(ty * a.nx + tx);
-          dep_cell = clampi(np_f2i32(rintf(qy)), 1, a.ny - 2) * a.nx + clampi(np_f2i32(rintf(qx)), 1, a.nx - 2);
+          ppc_cell = trunc_clip(qy, 0, a.ny - 1) * a.nx + trunc_clip(qx, 0, a.nx - 1);
+          dep_cell = rint_clip(qy, 1, a.ny - 2) * a.nx + rint_clip(qx, 1, a.nx - 2);
         }
         st.x[k] = x; st.y[k] = y; st.vx[k] = vx; st.vy[k] = vy; st.vz[k] = vz;
         st.cex[k] = cx; st.id[k] = pid;
@@ -1071,7 +1113,7 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
 // in order (the same single-pass look-back as the fused kernel).  The push is compute-bound
 // at many sub-steps per electron, so the extra pass over the state costs less than the
 // barriers it removes.  Same operations, same bits as k_ele_step.
-__global__ void __launch_bounds__(NT, 6) k_ele_push(EleStepArgs a, uint8_t* __restrict__ keep) {
+__global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __restrict__ keep) {
   pdl_enter();
   const int n = *a.num_src;
   const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
