@@ -78,7 +78,11 @@ int32_t pb_thermal_conduction(const float* T, float* T_new, const int32_t* mask,
                               double Fo_x, double Fo_y, void* stream);
 
 /* compute_particle_substeps (physics_engine.py:928-966): out_host[0] = n_sub,
- * out_host[1] = ds_max [m], out_host[2] = ds_lim [m]; synchronises the stream. */
+ * out_host[1] = ds_max [m], out_host[2] = ds_lim [m]; synchronises the stream.  Runs the
+ * step's reduction (E from a temporary corner array; with 16-byte aligned arrays, particles
+ * whose displacement provably stays below one already seen are passed over), so it also
+ * checks that path: the result is the full maximum, bit for bit.  Grids below 2 x 2 are
+ * refused with PB_ERR_ARG. */
 int32_t pb_compute_particle_substeps(const float* x, const float* y, const float* vx, const float* vy,
                                      const float* vz, int32_t n, const float* Ex, const float* Ey, int32_t nx,
                                      int32_t ny, double dx, double dy, double qm, double dt, double frac,

@@ -117,6 +117,66 @@ def test_substeps_exact(torch_cuda):
         assert out[1] == res[1] and out[2] == res[2]
 
 
+def test_substeps_skip_equals_full(torch_cuda):
+    """The reduction passes over particles whose displacement provably stays below one
+    already seen (16-byte aligned arrays); the same particles 4 bytes past a 16-byte
+    boundary take the full loop.  Both give the same n_sub and ds_max bits on sets built
+    against the bound: a fast particle late in the array, fields large enough that the
+    acceleration term dominates, positions outside the grid (clamped cells extrapolate the
+    field), all velocities zero, and a NaN velocity."""
+    import ctypes as C
+    import struct
+    torch = torch_cuda
+    from thruster_cx_code_b200 import _lib
+    lib = _lib.load()
+    d = load("domain_c1_half.npz")
+    nx, ny, dx, dy = int(d["nx"]), int(d["ny"]), float(d["dx"]), float(d["dy"])
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(21)
+    n = 300_000
+    Lx, Ly = (nx - 1) * dx, (ny - 1) * dy
+
+    def run(cols, ex, ey, qm):
+        Ex = torch.tensor(ex.astype(np.float32), device=dev)
+        Ey = torch.tensor(ey.astype(np.float32), device=dev)
+        res = []
+        for off in (0, 1):
+            t = [torch.zeros(n + 1, dtype=torch.float32, device=dev) for _ in cols]
+            for a, c in zip(t, cols):
+                a[off:off + n] = torch.tensor(c.astype(np.float32), device=dev)
+            out = (C.c_double * 3)()
+            _lib.check(lib.pb_compute_particle_substeps(*[a[off:].data_ptr() for a in t], n, Ex.data_ptr(),
+                                                        Ey.data_ptr(), nx, ny, dx, dy, qm, 1e-10, 0.25, out, None),
+                       "substeps")
+            res.append((out[0], struct.pack("<d", out[1])))
+        return res
+
+    x = rng.uniform(0.0, Lx, n)
+    y = rng.uniform(0.0, Ly, n)
+    Ex0, Ey0 = np.asarray(d["Ex"], np.float64), np.asarray(d["Ey"], np.float64)
+    qm_i, qm_e = 1.602e-19 / (131.29 * 1.6605e-27), -1.602e-19 / (131.29 * 1.6605e-27 / 100)
+    cases = []
+    v = rng.normal(0.0, 1e4, (3, n))
+    cases.append(("ions", [x, y, *v], Ex0, Ey0, qm_i))
+    ve = rng.normal(0.0, 5e5, (3, n))
+    ve[:, n - 5] *= 10.0
+    cases.append(("fast electron late", [x, y, *ve], Ex0, Ey0, qm_e))
+    cases.append(("acceleration dominates", [x, y, *ve], Ex0 * 1e4, Ey0 * 1e4, qm_e))
+    xo, yo = x.copy(), y.copy()
+    k = rng.choice(n, n // 100, replace=False)
+    xo[k] = rng.uniform(-Lx, 2 * Lx, k.size)
+    yo[k] = rng.uniform(-Ly, 2 * Ly, k.size)
+    cases.append(("outside the grid", [xo, yo, *ve], Ex0 * 1e3, Ey0 * 1e3, qm_e))
+    z = np.zeros(n)
+    cases.append(("no velocity", [x, y, z, z, z], Ex0, Ey0, qm_i))
+    vn = ve.copy()
+    vn[0, n - 1] = np.nan
+    cases.append(("NaN velocity", [x, y, *vn], Ex0, Ey0, qm_e))
+    for name, cols, ex, ey, qm in cases:
+        skip, full = run(cols, ex, ey, qm)
+        assert skip == full, name
+
+
 def test_segment_hits_exact(torch_cuda):
     torch = torch_cuda
     from thruster_cx_code_b200 import _lib

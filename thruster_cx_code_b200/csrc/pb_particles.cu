@@ -58,17 +58,34 @@ struct EBox {
 };
 
 // Builds the corner array from Ex and Ey (cells of the last row and column are not used:
-// the gather clamps the lower corner to ny - 2, nx - 2).
+// the gather clamps the lower corner to ny - 2, nx - 2).  With ebound, also the largest
+// |Ex| + |Ey| over the nodes (every node is a corner of some cell), as float bits through
+// an unsigned max: a NaN (0x7FC00000) or infinity wins, which disables the bound below.
 __global__ void k_e_corners(const float* __restrict__ Ex, const float* __restrict__ Ey, float4* __restrict__ Ec,
-                            int ny, int nx) {
+                            int ny, int nx, unsigned* ebound) {
   pdl_enter();
   const int N = ny * nx;
+  unsigned m = 0u;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < N; c += gridDim.x * blockDim.x) {
     const int iy = c / nx, ix = c - iy * nx;
     if (iy >= ny - 1 || ix >= nx - 1) continue;
     const int r1 = c + nx;
-    Ec[2 * c] = make_float4(__ldg(Ex + c), __ldg(Ex + c + 1), __ldg(Ex + r1), __ldg(Ex + r1 + 1));
-    Ec[2 * c + 1] = make_float4(__ldg(Ey + c), __ldg(Ey + c + 1), __ldg(Ey + r1), __ldg(Ey + r1 + 1));
+    const float4 a = make_float4(__ldg(Ex + c), __ldg(Ex + c + 1), __ldg(Ex + r1), __ldg(Ex + r1 + 1));
+    const float4 b = make_float4(__ldg(Ey + c), __ldg(Ey + c + 1), __ldg(Ey + r1), __ldg(Ey + r1 + 1));
+    Ec[2 * c] = a;
+    Ec[2 * c + 1] = b;
+    m = max(m, max(max(__float_as_uint(fabsf(a.x) + fabsf(b.x)), __float_as_uint(fabsf(a.y) + fabsf(b.y))),
+                   max(__float_as_uint(fabsf(a.z) + fabsf(b.z)), __float_as_uint(fabsf(a.w) + fabsf(b.w)))));
+  }
+  if (!ebound) return;
+  __shared__ unsigned wm[32];
+  m = __reduce_max_sync(0xFFFFFFFFu, m);
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? wm[threadIdx.x] : 0u;
+    m = __reduce_max_sync(0xFFFFFFFFu, m);
+    if (threadIdx.x == 0 && m) atomicMax(ebound, m);
   }
 }
 
@@ -143,8 +160,10 @@ __device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, floa
   int fxi, fyi;
   float frx, fry;
   bool inside = false;
-  if (LIGHT)
-    inside = floor_frac(ixf, fxi, frx) & floor_frac(iyf, fyi, fry) & (fxi <= nx - 2) & (fyi <= ny - 2);
+  if (LIGHT) {
+    const bool okx = floor_frac(ixf, fxi, frx), oky = floor_frac(iyf, fyi, fry);
+    inside = okx & oky & (fxi <= nx - 2) & (fyi <= ny - 2);
+  }
   if (inside) {
     ix0 = fxi;
     iy0 = fyi;
@@ -427,7 +446,8 @@ __device__ __forceinline__ double predicted_ds(float x, float y, float vx, float
   if (Ec) {
     const bool okq = div_fast(x, dxf, inv_dx, ixf) & div_fast(y, dyf, inv_dy, iyf);
     if (!okq) { ixf = __fdiv_rn(x, dxf); iyf = __fdiv_rn(y, dyf); }
-    inside = floor_frac(ixf, fxi, frx) & floor_frac(iyf, fyi, fry) & (fxi <= nx - 2) & (fyi <= ny - 2);
+    const bool okx = floor_frac(ixf, fxi, frx), oky = floor_frac(iyf, fyi, fry);
+    inside = okx & oky & (fxi <= nx - 2) & (fyi <= ny - 2);
   } else {
     ixf = __fdiv_rn(x, dxf); iyf = __fdiv_rn(y, dyf);
   }
@@ -457,11 +477,24 @@ __device__ __forceinline__ double predicted_ds(float x, float y, float vx, float
   return DADD((double)__fmul_rn(v_mag, dtf), DMUL(DMUL(0.5, a_mag), dt2));
 }
 
-__global__ void k_substep_reduce(const float* __restrict__ x, const float* __restrict__ y,
+// Particles that cannot raise the maximum are passed over without the gather and the
+// float64 arithmetic (ebound non-null, the corner path).  predicted_ds is monotone in the
+// float32 |v|^2 it takes the root of, and for a particle inside the grid (fractions in
+// [0, 1], so the bilinear E is a convex combination of corner values) its acceleration
+// term is at most acc = 0.5 |qm| Emax dt^2, Emax = max over nodes of |Ex| + |Ey| (the
+// bound k_e_corners leaves).  With every rounding of both terms below 1e-6 relative,
+// ds <= (sqrt(v2) dtf + acc)(1 + 1e-6).  A particle is therefore skipped when
+// v2 < ((M (1 - 2e-4) - acc (1 + 2e-4)) / dtf)^2 (1 - 2e-4), M an exact ds already seen:
+// its ds is below M, and the maximum, hence n_sub, is that of the full loop.  Positions
+// outside [0, nx - 2) x [0, ny - 2) cells, NaN and infinite values are never skipped.  The
+// warp shares its running maximum after each pass that evaluated any particle, so after
+// the first pass nearly every particle is skipped and the loop streams 20 B per particle.
+__global__ void __launch_bounds__(256, 4) k_substep_reduce(const float* __restrict__ x, const float* __restrict__ y,
                                  const float* __restrict__ vx, const float* __restrict__ vy,
                                  const float* __restrict__ vz, const int* n_dev, int n_host, const float* Ex,
                                  const float* Ey, const float4* Ec, int nx, int ny, float dxf, float dyf, double qm,
-                                 float dtf, double dt2, unsigned long long* ds_max_bits) {
+                                 float dtf, double dt2, unsigned long long* ds_max_bits,
+                                 const unsigned* ebound = nullptr) {
   pdl_enter();
   int n = n_dev ? *n_dev : n_host;
   unsigned long long m = 0ull;
@@ -474,23 +507,67 @@ __global__ void k_substep_reduce(const float* __restrict__ x, const float* __res
                      reinterpret_cast<uintptr_t>(vz)) & 15u) == 0;
   const int n4 = vec ? n >> 2 : 0;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  for (int q = t0; q < n4; q += stride) {
-    const float4 X = __ldg(reinterpret_cast<const float4*>(x) + q);
-    const float4 Y = __ldg(reinterpret_cast<const float4*>(y) + q);
-    const float4 U = __ldg(reinterpret_cast<const float4*>(vx) + q);
-    const float4 V = __ldg(reinterpret_cast<const float4*>(vy) + q);
-    const float4 W = __ldg(reinterpret_cast<const float4*>(vz) + q);
-    const double d0 = predicted_ds(X.x, Y.x, U.x, V.x, W.x, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
-    const double d1 = predicted_ds(X.y, Y.y, U.y, V.y, W.y, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
-    const double d2 = predicted_ds(X.z, Y.z, U.z, V.z, W.z, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
-    const double d3 = predicted_ds(X.w, Y.w, U.w, V.w, W.w, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
-    const unsigned long long b0 = (unsigned long long)__double_as_longlong(d0);
-    const unsigned long long b1 = (unsigned long long)__double_as_longlong(d1);
-    const unsigned long long b2 = (unsigned long long)__double_as_longlong(d2);
-    const unsigned long long b3 = (unsigned long long)__double_as_longlong(d3);
-    const unsigned long long b01 = b0 > b1 ? b0 : b1, b23 = b2 > b3 ? b2 : b3;
-    const unsigned long long b = b01 > b23 ? b01 : b23;
-    m = b > m ? b : m;
+  if (vec && Ec && ebound) {
+    const double acc = 0.5 * fabs(qm) * (double)__uint_as_float(__ldg(ebound)) * dt2;  // NaN, inf: no skips
+    const double invdt2 = 1.0 / ((double)dtf * (double)dtf);
+    const float xlim = (float)(nx - 2), ylim = (float)(ny - 2);
+    float thr = -1.0f;  // v2 < thr: below the running maximum (none yet)
+    const int lane = threadIdx.x & 31;
+    for (int qb = t0 - lane; qb < n4; qb += stride) {  // the same trip count in every lane
+      const int q = qb + lane;
+      bool did = false;
+      if (q < n4) {
+        const float4 X = __ldg(reinterpret_cast<const float4*>(x) + q);
+        const float4 Y = __ldg(reinterpret_cast<const float4*>(y) + q);
+        const float4 U = __ldg(reinterpret_cast<const float4*>(vx) + q);
+        const float4 V = __ldg(reinterpret_cast<const float4*>(vy) + q);
+        const float4 W = __ldg(reinterpret_cast<const float4*>(vz) + q);
+        const float px[4] = {X.x, X.y, X.z, X.w}, py[4] = {Y.x, Y.y, Y.z, Y.w};
+        const float pu[4] = {U.x, U.y, U.z, U.w}, pv[4] = {V.x, V.y, V.z, V.w}, pw[4] = {W.x, W.y, W.z, W.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float v2 = __fadd_rn(__fadd_rn(__fmul_rn(pu[j], pu[j]), __fmul_rn(pv[j], pv[j])),
+                                     __fmul_rn(pw[j], pw[j]));
+          const bool below = (v2 < thr) & (px[j] >= 0.0f) & (py[j] >= 0.0f) &
+                             (__fmul_rn(px[j], inv_dx) < xlim) & (__fmul_rn(py[j], inv_dy) < ylim);
+          if (!below) {
+            const double d = predicted_ds(px[j], py[j], pu[j], pv[j], pw[j], Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf,
+                                          dt2, inv_dx, inv_dy);
+            const unsigned long long b = (unsigned long long)__double_as_longlong(d);
+            m = b > m ? b : m;
+            did = true;
+          }
+        }
+      }
+      if (__any_sync(0xFFFFFFFFu, did)) {
+        for (int o = 16; o > 0; o >>= 1) {
+          const unsigned long long v = __shfl_xor_sync(0xFFFFFFFFu, m, o);
+          m = v > m ? v : m;
+        }
+        const double M = __longlong_as_double((long long)m);
+        const double R = M * (1.0 - 2e-4) - acc * (1.0 + 2e-4);
+        thr = R > 0.0 ? __double2float_rd(R * R * invdt2 * (1.0 - 2e-4)) : -1.0f;
+      }
+    }
+  } else {
+    for (int q = t0; q < n4; q += stride) {
+      const float4 X = __ldg(reinterpret_cast<const float4*>(x) + q);
+      const float4 Y = __ldg(reinterpret_cast<const float4*>(y) + q);
+      const float4 U = __ldg(reinterpret_cast<const float4*>(vx) + q);
+      const float4 V = __ldg(reinterpret_cast<const float4*>(vy) + q);
+      const float4 W = __ldg(reinterpret_cast<const float4*>(vz) + q);
+      const double d0 = predicted_ds(X.x, Y.x, U.x, V.x, W.x, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
+      const double d1 = predicted_ds(X.y, Y.y, U.y, V.y, W.y, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
+      const double d2 = predicted_ds(X.z, Y.z, U.z, V.z, W.z, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
+      const double d3 = predicted_ds(X.w, Y.w, U.w, V.w, W.w, Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);
+      const unsigned long long b0 = (unsigned long long)__double_as_longlong(d0);
+      const unsigned long long b1 = (unsigned long long)__double_as_longlong(d1);
+      const unsigned long long b2 = (unsigned long long)__double_as_longlong(d2);
+      const unsigned long long b3 = (unsigned long long)__double_as_longlong(d3);
+      const unsigned long long b01 = b0 > b1 ? b0 : b1, b23 = b2 > b3 ? b2 : b3;
+      const unsigned long long b = b01 > b23 ? b01 : b23;
+      m = b > m ? b : m;
+    }
   }
   for (int i = 4 * n4 + t0; i < n; i += stride) {
     double ds = predicted_ds(x[i], y[i], vx[i], vy[i], vz[i], Ex, Ey, Ec, nx, ny, dxf, dyf, qm, dtf, dt2, inv_dx, inv_dy);

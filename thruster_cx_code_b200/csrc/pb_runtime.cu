@@ -134,7 +134,7 @@ struct Sim {
   uint64_t* angle_scratch = nullptr;
   int angle_cap = 0;
   int* angle_count = nullptr;
-  unsigned long long* ds_bits = nullptr;  // [ion, ele]
+  unsigned long long* ds_bits = nullptr;  // [ion, ele, field bound (low word: float bits)]
   int* n_sub = nullptr;                    // [ion, ele]
   uint8_t* ekeep = nullptr;                // survivor flags of the split electron step
   size_t ekeep_cap = 0;
@@ -588,7 +588,7 @@ __global__ void k_step_reset(StepResetArgs a) {
   for (long long i = tid; i < a.ntile; i += nth) a.tile_status[i] = 0ull;
   if (tid == 0) {
     *a.angle_count = 0; *a.see_count = 0; *a.see_spawned = 0;
-    a.ds_bits[0] = 0ull; a.ds_bits[1] = 0ull;
+    a.ds_bits[0] = 0ull; a.ds_bits[1] = 0ull; a.ds_bits[2] = 0ull;
     a.tile_counter[0] = 0; a.tile_counter[1] = 0;
     *a.ni_dst = 0; *a.ne_dst = 0;
     for (int k = 0; k < 7; ++k) a.inj[k] = 0;
@@ -852,18 +852,20 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
 
   // corners of Ex, Ey for the gathers below (rebuilt every step: fields change in the
   // solve, through pb_sim_set_field or through pb_sim_field_ptr)
-  CK(launch_pdl(k_e_corners, grid_for(s, N, 256), 256, 0, st, s->Ex, s->Ey, s->ecorn, s->ny, s->nx));
+  // the field bound that lets the sub-step reductions pass over slow particles
+  unsigned* ebound = reinterpret_cast<unsigned*>(s->ds_bits + 2);
+  CK(launch_pdl(k_e_corners, grid_for(s, N, 256), 256, 0, st, s->Ex, s->Ey, s->ecorn, s->ny, s->nx, ebound));
   ++s->launches;
 
   // C. sub-step counts (:1177-1209)
   const float dtf = (float)p->dt;
   CK(launch_pdl(k_substep_reduce, grid_for(s, I.cap / 4, 256, 4), 256, 0, st, I.buf[I.cur].x, I.buf[I.cur].y,
                 I.buf[I.cur].vx, I.buf[I.cur].vy, I.buf[I.cur].vz, ni_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf,
-                dyf, p->qm_ion, dtf, p->dt2, s->ds_bits));
+                dyf, p->qm_ion, dtf, p->dt2, s->ds_bits, ebound));
   ++s->launches;
   CK(launch_pdl(k_substep_reduce, grid_for(s, E.cap / 4, 256, 4), 256, 0, st, E.buf[E.cur].x, E.buf[E.cur].y,
                 E.buf[E.cur].vx, E.buf[E.cur].vy, E.buf[E.cur].vz, ne_src, 0, s->Ex, s->Ey, s->ecorn, s->nx, s->ny, dxf,
-                dyf, p->qm_e, dtf, p->dt2, s->ds_bits + 1));
+                dyf, p->qm_e, dtf, p->dt2, s->ds_bits + 1, ebound));
   ++s->launches;
   CK(launch_pdl(k_substep_finish2, 1, 1, 0, st, (const double*)s->ds_bits, p->ds_lim, s->n_sub, ef));
   ++s->launches;
@@ -1203,7 +1205,7 @@ int32_t pb_sim_create(pb_sim** out, int32_t device) {
   CK(dalloc(&s->next_ids, 2));
   CK(cudaMemset(s->next_ids, 0, 2 * sizeof(uint32_t)));
   CK(dalloc(&s->tile_counter, 2));
-  CK(dalloc(&s->ds_bits, 2));
+  CK(dalloc(&s->ds_bits, 3));
   CK(dalloc(&s->n_sub, 2));
   CK(dalloc(&s->inj, 7));
   CK(dalloc(&s->see_count, 1));
@@ -1992,15 +1994,25 @@ int32_t pb_compute_particle_substeps(const float* x, const float* y, const float
                                      double dy, double qm, double dt, double frac, double* out_host, void* stream) {
   double ds_lim = frac * std::min(dx, dy) * 1e-3;
   if (n <= 0) { out_host[0] = 1; out_host[1] = 0.0; out_host[2] = ds_lim; return PB_OK; }
+  if (nx < 2 || ny < 2) return fail(PB_ERR_ARG, "compute_particle_substeps: grid must be at least 2 x 2");
   cudaStream_t st = (cudaStream_t)stream;
+  // the step's path: the corner array with the field bound, so that particles which cannot
+  // raise the maximum are passed over (arrays 16-byte aligned; others take the full loop)
+  const long long G = (long long)nx * ny;
   unsigned long long* bits = nullptr;
-  CK(cudaMallocAsync((void**)&bits, sizeof(unsigned long long), st));
-  CK(cudaMemsetAsync(bits, 0, sizeof(unsigned long long), st));
+  float4* ec = nullptr;
+  CK(cudaMallocAsync((void**)&bits, 2 * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(bits, 0, 2 * sizeof(unsigned long long), st));
+  CK(cudaMallocAsync((void**)&ec, (size_t)G * 2 * sizeof(float4), st));
+  unsigned* ebound = reinterpret_cast<unsigned*>(bits + 1);
+  const int gc = (int)std::min<long long>((G + 255) / 256, 148LL * 8);
+  k_e_corners<<<gc, 256, 0, st>>>(Ex, Ey, ec, ny, nx, ebound);
   int g = (int)std::min<long>((n + 255) / 256, 148L * 16);
-  k_substep_reduce<<<g, 256, 0, st>>>(x, y, vx, vy, vz, nullptr, n, Ex, Ey, nullptr, nx, ny, (float)dx, (float)dy, qm, (float)dt,
-                                      dt * dt, bits);
+  k_substep_reduce<<<g, 256, 0, st>>>(x, y, vx, vy, vz, nullptr, n, Ex, Ey, ec, nx, ny, (float)dx, (float)dy, qm,
+                                      (float)dt, dt * dt, bits, ebound);
   unsigned long long hb = 0;
   CK(cudaMemcpyAsync(&hb, bits, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  CK(cudaFreeAsync(ec, st));
   CK(cudaFreeAsync(bits, st));
   CK(cudaStreamSynchronize(st));
   double ds_max;
