@@ -7,8 +7,8 @@ float32 operands is emulated exactly in float64 here: a * b is exact in float64 
 q within a few ulps of x / d, so is the sum, which is then rounded once to float32.  The
 full check (every float |x| < 64, ten spacings) ran on the host in C; this samples it.
 
-The second test covers the cell-index tricks the particle kernels use beside it (floor,
-fraction, rint and truncation by adding 2^23).
+The other tests cover the cell-index tricks the particle kernels use beside it (floor,
+fraction, rint and truncation by adding 2^23, and the one-compare range test of the floor).
 """
 import numpy as np
 
@@ -84,3 +84,39 @@ def test_floor_frac_and_rint_by_adding_2p23():
     assert np.array_equal(rn, np.rint(q).astype(np.int64))
     # trunc_clip: astype(int) of a non-negative float is its floor
     assert np.array_equal(fl, q.astype(np.int64))
+
+
+def _rd_sum_bits(q):
+    """float32 q + 2^23 rounded down (emulated through the float64 sum), as int32 bits."""
+    with np.errstate(invalid="ignore", over="ignore"):
+        s = q.astype(np.float64) + 8388608.0
+        t = s.astype(F32)
+    with np.errstate(invalid="ignore"):
+        up = t.astype(np.float64) > s
+    t = np.where(up, np.nextafter(t, F32(-np.inf)), t)
+    # an exact zero sum rounds to -0 when rounding down
+    t = np.where(s == 0.0, F32(-0.0), t)
+    # below 2^-29 the float64 sum itself rounds; the float32 sum rounded down is then 2^23 for
+    # a positive q and the float just below 2^23 for a negative one
+    with np.errstate(invalid="ignore"):
+        t = np.where((q < 0) & (q > -2.0 ** -29), F32(8388607.5), t)
+    return t.view(np.int32).astype(np.int64)
+
+
+def test_one_unsigned_compare_bounds_the_floor():
+    """push_cell tests fl = bits(q + 2^23, rounded down) - 0x4B000000 with one unsigned compare,
+    fl <= N (N = nx - 2 < 2^22), in place of 0 <= q < 2^22 and fl <= N: any q that passes
+    (negative, huge, infinite and NaN q included) lies in [0, N + 1) and fl is its floor."""
+    rng = np.random.default_rng(17)
+    for N in (2, 255, 2047, 4194302):
+        q = np.concatenate([
+            rng.integers(0, 0xFFFFFFFF, 2_000_000, dtype=np.uint64).astype(np.uint32).view(F32),
+            rng.uniform(-3.0, N + 3.0, 1_000_000).astype(F32),
+            np.array([0.0, -0.0, -8388608.0, -8388607.5, 8388608.0, 4194304.0, N, N + 1, N + 0.5,
+                      np.nextafter(F32(N + 1), F32(0)), np.inf, -np.inf, np.nan, -1e-45, 1e-45], F32)])
+        fl = (_rd_sum_bits(q) - 0x4B000000) & 0xFFFFFFFF
+        ok = fl <= N
+        with np.errstate(invalid="ignore"):
+            inside = (q >= 0) & (q < N + 1)
+        assert np.array_equal(ok, inside)
+        assert np.array_equal(fl[ok], np.floor(q[ok]).astype(np.int64))

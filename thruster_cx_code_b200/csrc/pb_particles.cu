@@ -161,8 +161,12 @@ __device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, floa
   float frx, fry;
   bool inside = false;
   if (LIGHT) {
-    const bool okx = floor_frac(ixf, fxi, frx), oky = floor_frac(iyf, fyi, fry);
-    inside = okx & oky & (fxi <= nx - 2) & (fyi <= ny - 2);
+    // one unsigned compare per coordinate: a floor in [0, n - 2] (n - 2 < 2^22) from the
+    // rounded-down sum implies 0 <= q < n - 1, the range floor_frac needs; negative, huge,
+    // infinite and NaN q give a floor outside it (tests/test_div_method.py)
+    floor_frac(ixf, fxi, frx);
+    floor_frac(iyf, fyi, fry);
+    inside = ((unsigned)fxi <= (unsigned)(nx - 2)) & ((unsigned)fyi <= (unsigned)(ny - 2));
   }
   if (inside) {
     ix0 = fxi;
