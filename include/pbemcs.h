@@ -65,6 +65,17 @@ int32_t pb_accumulate_rho(const float* x, const float* y, float* rho, int32_t nu
 int32_t pb_accumulate_rho_noalloc(const float* x, const float* y, float* rho, int32_t num_p, double dx, double dy,
                                   int32_t nx, int32_t ny, double charge_density, void* stream);
 
+/* Exhaustive check of the division the step kernels use for x / dx and y / dy (no
+ * counterpart in the reference; a test of this library).  For the float32 spacing d, every
+ * one of the 2^32 float32 values x is divided by bracketing (x * RN(1/d), its FMA residual
+ * and two FMA corrections with the neighbours of RN(1/d); accepted when both corrections
+ * round alike) and compared with the IEEE float32 division.  out3[0]: accepted quotients
+ * that differ in any bit (0 expected for every d); out3[1]: rejected x among those a grid
+ * can hold (x >= 2^-80 and x / d < 2^22, which then take the division instruction);
+ * out3[2]: all such x.  Runs on the current device in a few milliseconds and allocates
+ * 24 bytes of device memory. */
+int32_t pb_check_division(double d, int64_t* out3);
+
 /* Bilinear E/B gather + 2D3V Boris + drift (x += vx dt 1000), in place; bit-identical
  * to push_particles_boris_cpu (physics_engine.py:188-254; Taichi form :63-144). */
 int32_t pb_push_particles_boris(float* x, float* y, float* vx, float* vy, float* vz, const float* Ex,

@@ -102,6 +102,7 @@ PROTOTYPES = {
     "pb_sim_phase_times": (i32, [vp, P(f64)]),
     "pb_sim_set_kernel_options": (i32, [vp, u32]),
     "pb_sim_get_kernel_options": (i32, [vp, P(u32)]),
+    "pb_check_division": (i32, [f64, P(C.c_int64)]),
     "pb_sim_set_tile": (i32, [vp, i32]),
     "pb_sim_set_graphs": (i32, [vp, i32]),
     "pb_sim_graph_stats": (i32, [vp, P(C.c_int64)]),

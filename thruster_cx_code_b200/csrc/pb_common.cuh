@@ -11,6 +11,7 @@
 #pragma once
 #include <cstdint>
 #include <climits>
+#include <cstring>
 #include <cuda.h>
 #include <cuda_runtime.h>
 

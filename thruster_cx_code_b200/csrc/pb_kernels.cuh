@@ -20,6 +20,31 @@ struct Spline {
   int enabled;
 };
 
+// Reciprocals of the grid spacings for the division of the particle kernels (div_bracket):
+// inv = RN(1/d) and the floats two steps below and above it, which bracket 1/d with room
+// for the residual's rounding.  NaN brackets (a spacing that is not a positive normal
+// float) make every quotient take the division instruction.
+struct Rcp {
+  float ix, ix_lo, ix_hi, iy, iy_lo, iy_hi;
+};
+
+__host__ __device__ inline void rcp_axis(float d, float& inv, float& lo, float& hi) {
+  inv = 1.0f / d;
+  unsigned b;
+  memcpy(&b, &inv, sizeof(b));
+  const bool ok = d > 0.0f && b >= 0x01000000u && b < 0x7F000000u;  // inv and its neighbours normal
+  const unsigned bl = ok ? b - 2u : 0x7FC00000u, bh = ok ? b + 2u : 0x7FC00000u;
+  memcpy(&lo, &bl, sizeof(lo));
+  memcpy(&hi, &bh, sizeof(hi));
+}
+
+__host__ __device__ inline Rcp make_rcp(float dxf, float dyf) {
+  Rcp r;
+  rcp_axis(dxf, r.ix, r.ix_lo, r.ix_hi);
+  rcp_axis(dyf, r.iy, r.iy_lo, r.iy_hi);
+  return r;
+}
+
 // Everything the ion step kernel reads besides the particles.
 // E-corner window that the ion step stages per tile with a TMA copy (PB_OPT_TMA_TILE):
 // TB_W x TB_H cells of 8 floats (8 KB)
@@ -42,6 +67,7 @@ struct IonStepArgs {
   int nx, ny;
   float dxf, dyf;
   float inv_dx, inv_dy;   // f32(1/dxf), f32(1/dyf)
+  Rcp rcp;                // the same with their brackets (the push's division)
   // push
   double dt, qm, ds_lim;
   const double *ds_max;   // device: max predicted displacement (n_sub)
@@ -107,6 +133,7 @@ struct EleStepArgs {
   int nx, ny;
   float dxf, dyf;
   float inv_dx, inv_dy;
+  Rcp rcp;
   double dt, qm, ds_lim;
   const double *ds_max;
   int *n_sub_out;

@@ -121,6 +121,56 @@ __device__ __forceinline__ bool div_fast(float x, float d, float inv, float& q) 
   const float h = __fmul_rn(__uint_as_float((e - (24u << 23)) & 0x7F800000u), fabsf(d));
   return (e > (26u << 23)) & (e < 0x7F800000u) & ((b & 0x007FFFFFu) != 0u) & (fabsf(r) < h);
 }
+// RN(x / d) by bracketing, without the division instruction.  q0 = RN(x inv) (inv =
+// RN(1/d)) is within 1.5 ulp of x / d, and r0 = RN(q0 d - x) (one FMA) is within a relative
+// 2^-24 of the exact q0 d - x when it is a normal float.  The exact quotient is
+// x / d = q0 - (q0 d - x) / d, and lo <= (1/d)(1 - 2^-24), hi >= (1/d)(1 + 2^-24) (inv moved
+// two float steps down and up), so x / d lies between q0 - r0 lo and q0 - r0 hi.  Rounding
+// is monotone: when qa = RN(q0 - r0 lo) and qb = RN(q0 - r0 hi) (one FMA each) are equal,
+// RN(x / d) is that value.  |x| >= 2^-80 keeps r0 out of the subnormal range; NaN, infinite
+// and overflowing quotients give NaN or unequal values, and NaN brackets never agree.  The
+// test fails only when x / d lies within about 2^-22 ulp of a rounding midpoint.  Returns
+// whether q is accepted, without a branch (k_div_check counts misses over every float x).
+__device__ __forceinline__ bool div_bracket(float x, float d, float inv, float lo, float hi, float& q) {
+  const float q0 = __fmul_rn(x, inv);
+  const float r0 = __fmaf_rn(q0, d, -x);
+  q = __fmaf_rn(-r0, lo, q0);
+  const float qb = __fmaf_rn(-r0, hi, q0);
+  return (q == qb) & (fabsf(x) >= 0x1p-80f);
+}
+
+// Checks div_bracket for one spacing over all 2^32 bit patterns of x: out[0] counts the
+// accepted quotients that differ in any bit from __fdiv_rn(x, d); out[1] the rejected x
+// among those a grid's cells can hold (x >= 2^-80, x / d < 2^22); out[2] all such x.
+__global__ void k_div_check(float d, unsigned long long* out) {
+  float inv, lo, hi;
+  rcp_axis(d, inv, lo, hi);
+  unsigned long long miss = 0, rej = 0, cand = 0;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < (1ull << 32);
+       k += stride) {
+    const float x = __uint_as_float((unsigned)k);
+    const float qd = __fdiv_rn(x, d);
+    float q;
+    const bool ok = div_bracket(x, d, inv, lo, hi, q);
+    if (ok && __float_as_uint(q) != __float_as_uint(qd)) ++miss;
+    if (x >= 0x1p-80f && qd < 4194304.0f) {
+      ++cand;
+      if (!ok) ++rej;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    miss += __shfl_xor_sync(0xFFFFFFFFu, miss, o);
+    rej += __shfl_xor_sync(0xFFFFFFFFu, rej, o);
+    cand += __shfl_xor_sync(0xFFFFFFFFu, cand, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (miss) atomicAdd(out, miss);
+    if (rej) atomicAdd(out + 1, rej);
+    if (cand) atomicAdd(out + 2, cand);
+  }
+}
+
 // The same with a branch per quotient, for callers that need one quotient at a time.
 __device__ __forceinline__ float div_rn_checked(float x, float d, float inv) {
   float q = __fmul_rn(x, inv);
@@ -143,18 +193,18 @@ __device__ __forceinline__ float div_rn_checked(float x, float d, float inv) {
 // Cell and bilinear weights of a push at (x, y): float32 quotients x / dx, y / dy, the
 // clamped floor cell (ix0, iy0) and the float64 weights of the reference's gather.
 template <bool LIGHT>
-__device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, float dxf, float dyf, float inv_dx,
-                                          float inv_dy, float* q_start, int& ix0, int& iy0, double& w00,
-                                          double& w10, double& w01, double& w11) {
+__device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, float dxf, float dyf, const Rcp& rc,
+                                          float* q_start, int& ix0, int& iy0, double& w00, double& w10,
+                                          double& w01, double& w11) {
   float ixf, iyf;
   if (LIGHT) {
-    const bool okq = div_fast(x, dxf, inv_dx, ixf) & div_fast(y, dyf, inv_dy, iyf);
+    const bool okq = div_bracket(x, dxf, rc.ix, rc.ix_lo, rc.ix_hi, ixf) &
+                     div_bracket(y, dyf, rc.iy, rc.iy_lo, rc.iy_hi, iyf);
     if (!okq) { ixf = __fdiv_rn(x, dxf); iyf = __fdiv_rn(y, dyf); }
   } else {
     ixf = __fdiv_rn(x, dxf);
     iyf = __fdiv_rn(y, dyf);
   }
-  if (q_start) { q_start[0] = ixf; q_start[1] = iyf; }  // x / dx, y / dy at the start position
   double fx, fy;
   // inside the grid the clamp is a no-op and ixf - ix0 is the exact float fraction
   int fxi, fyi;
@@ -179,6 +229,7 @@ __device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, floa
     fx = DSUB((double)ixf, (double)ix0);
     fy = DSUB((double)iyf, (double)iy0);
   }
+  if (q_start) { q_start[0] = ixf; q_start[1] = iyf; }  // x / dx, y / dy at the start position
   const double gx = DSUB(1.0, fx), gy = DSUB(1.0, fy);
   w00 = DMUL(gx, gy); w10 = DMUL(fx, gy); w01 = DMUL(gx, fy); w11 = DMUL(fx, fy);
 }
@@ -221,13 +272,13 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
                                                const float* __restrict__ Bx, const float* __restrict__ By,
                                                const float* __restrict__ Bz, int nx, int ny,
                                                float dxf, float dyf, double h, float dtf,
-                                               const float4* __restrict__ Ec = nullptr, float inv_dx = 0.0f,
-                                               float inv_dy = 0.0f, float* q_start = nullptr,
+                                               const float4* __restrict__ Ec = nullptr, Rcp rc = Rcp{},
+                                               float* q_start = nullptr,
                                                EBox eb = EBox{nullptr, 0, 0}) {
   static_assert(!(HAS_B && CORN), "the corner gather has no B field");
   int ix0, iy0;
   double w00, w10, w01, w11;
-  push_cell<LIGHT>(x, y, nx, ny, dxf, dyf, inv_dx, inv_dy, q_start, ix0, iy0, w00, w10, w01, w11);
+  push_cell<LIGHT>(x, y, nx, ny, dxf, dyf, rc, q_start, ix0, iy0, w00, w10, w01, w11);
   int ix1 = min(ix0 + 1, nx - 1);
   int iy1 = min(iy0 + 1, ny - 1);
   size_t r0 = (size_t)iy0 * nx, r1 = (size_t)iy1 * nx;
@@ -281,15 +332,14 @@ __device__ __forceinline__ void boris_push_one(float& x, float& y, float& vx, fl
 // latency overlaps the other's.  Each particle's operations are those of boris_push_one.
 __device__ __forceinline__ void push_pair_b0(float (&x)[2], float (&y)[2], float (&vx)[2], float (&vy)[2],
                                              float (&vz)[2], int n_sub, const float4* __restrict__ Ec, int nx,
-                                             int ny, float dxf, float dyf, float inv_dx, float inv_dy, double h,
-                                             float dtf) {
+                                             int ny, float dxf, float dyf, const Rcp& rc, double h, float dtf) {
   for (int s = 0; s < n_sub; ++s) {
     int ix0[2], iy0[2];
     double w[2][4];
     float4 A[2], B[2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-      push_cell<true>(x[q], y[q], nx, ny, dxf, dyf, inv_dx, inv_dy, nullptr, ix0[q], iy0[q], w[q][0], w[q][1],
+      push_cell<true>(x[q], y[q], nx, ny, dxf, dyf, rc, nullptr, ix0[q], iy0[q], w[q][0], w[q][1],
                       w[q][2], w[q][3]);
       const size_t c = (size_t)iy0[q] * nx + ix0[q];
       A[q] = __ldg(Ec + 2 * c);
@@ -891,10 +941,10 @@ __global__ void __launch_bounds__(NT, 4) k_ion_step(const __grid_constant__ IonS
         const float x0 = x, y0 = y;
         float q0[2];  // x0 / dx, y0 / dy (correctly rounded), from the first substep
         boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
-                                              a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy, q0, eb);
+                                              a.dyf, h, dtf, a.Ec, a.rcp, q0, eb);
         for (int s = 1; s < n_sub; ++s)
           boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
-                                                a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy, nullptr, eb);
+                                                a.dyf, h, dtf, a.Ec, a.rcp, nullptr, eb);
         if (a.periodic) y = np_modf_pos(y, a.Lyf);
         // the final cell, the PPC cell and the deposit cell all round or truncate the same
         // correctly rounded quotients (what rint_div and trunc_div return)
@@ -1142,7 +1192,7 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
           const int j = i < n ? i : t0;
           x[q] = a.src.x[j]; y[q] = a.src.y[j]; vx[q] = a.src.vx[j]; vy[q] = a.src.vy[j]; vz[q] = a.src.vz[j];
         }
-        push_pair_b0(x, y, vx, vy, vz, n_sub, a.Ec, a.nx, a.ny, a.dxf, a.dyf, a.inv_dx, a.inv_dy, h, dtf);
+        push_pair_b0(x, y, vx, vy, vz, n_sub, a.Ec, a.nx, a.ny, a.dxf, a.dyf, a.rcp, h, dtf);
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
           const int kk = k + q * NT, i = t0 + kk;
@@ -1164,7 +1214,7 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
           float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
           for (int s = 0; s < n_sub; ++s)
             boris_push_one<HAS_B, !HAS_B, !HAS_B>(x, y, vx, vy, vz, a.Ex, a.Ey, a.Bx, a.By, a.Bz, a.nx, a.ny, a.dxf,
-                                                  a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy);
+                                                  a.dyf, h, dtf, a.Ec, a.rcp);
           ele_finish(a, st, k, i, x, y, vx, vy, vz, kp, dep_cell);
         }
         st.keep[k] = kp;
@@ -1214,7 +1264,7 @@ __global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __re
 #pragma unroll 2
       for (int s = 0; s < n_sub; ++s)
         boris_push_one<false, true, true>(x, y, vx, vy, vz, a.Ex, a.Ey, nullptr, nullptr, nullptr, a.nx, a.ny, a.dxf,
-                                          a.dyf, h, dtf, a.Ec, a.inv_dx, a.inv_dy);
+                                          a.dyf, h, dtf, a.Ec, a.rcp);
       if (a.periodic) y = np_modf_pos(y, a.Lyf);
       const int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1);
       const int icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);

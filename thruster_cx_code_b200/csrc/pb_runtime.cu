@@ -876,7 +876,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   a.src = I.buf[I.cur]; a.dst = I.buf[1 - I.cur]; a.num_src = ni_src; a.num_dst = ni_dst;
   a.Ex = s->Ex; a.Ey = s->Ey; a.Ec = s->ecorn; a.Bx = a.By = a.Bz = nullptr; a.has_B = 0;
   a.isBound = s->isBound; a.bdist = s->bdist; a.nx = s->nx; a.ny = s->ny; a.dxf = dxf; a.dyf = dyf;
-  a.inv_dx = 1.0f / dxf; a.inv_dy = 1.0f / dyf;
+  a.inv_dx = 1.0f / dxf; a.inv_dy = 1.0f / dyf; a.rcp = make_rcp(dxf, dyf);
   a.dt = p->dt; a.qm = p->qm_ion; a.ds_lim = p->ds_lim; a.ds_max = (const double*)s->ds_bits; a.n_sub_out = s->n_sub;
   a.periodic = s->periodic; a.Lyf = (float)p->Ly; a.Lxf = (float)p->Lx;
   a.x_entry = (float)p->x_entry; a.x_exit = (float)p->x_exit; a.x_plume = (float)p->x_plume;
@@ -931,7 +931,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.src = E.buf[E.cur]; b.dst = E.buf[1 - E.cur]; b.num_src = ne_src; b.num_dst = ne_dst;
   b.Ex = s->Ex; b.Ey = s->Ey; b.Ec = s->ecorn; b.Bx = b.By = b.Bz = nullptr; b.has_B = 0;
   b.isBound = s->isBound; b.nx = s->nx; b.ny = s->ny; b.dxf = dxf; b.dyf = dyf;
-  b.inv_dx = 1.0f / dxf; b.inv_dy = 1.0f / dyf;
+  b.inv_dx = 1.0f / dxf; b.inv_dy = 1.0f / dyf; b.rcp = make_rcp(dxf, dyf);
   b.dt = p->dt; b.qm = p->qm_e; b.ds_lim = p->ds_lim; b.ds_max = (const double*)(s->ds_bits + 1);
   b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
@@ -1890,6 +1890,26 @@ int32_t pb_sim_set_profiling(pb_sim* h, int32_t on) {
 }
 
 // ------------------------------------------------------------------ kernel-level entry points
+int32_t pb_check_division(double d, int64_t* out3) {
+  if (!out3) return fail(PB_ERR_ARG, "pb_check_division: null output");
+  unsigned long long* dev = nullptr;
+  CK(cudaMalloc((void**)&dev, 3 * sizeof(unsigned long long)));
+  unsigned long long h[3] = {0, 0, 0};
+  cudaError_t e = cudaMemset(dev, 0, sizeof(h));
+  int sms = 148, dv = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dv);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dv);
+  if (e == cudaSuccess) {
+    k_div_check<<<sms * 8, 256>>>((float)d, dev);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(h, dev, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaFree(dev);
+  CK(e);
+  for (int k = 0; k < 3; ++k) out3[k] = (int64_t)h[k];
+  return PB_OK;
+}
+
 int32_t pb_push_particles_boris(float* x, float* y, float* vx, float* vy, float* vz, const float* Ex, const float* Ey,
                                 const float* Bx, const float* By, const float* Bz, int32_t num_p, double dx, double dy,
                                 int32_t nx, int32_t ny, double dt, double q_m, void* stream) {
