@@ -134,6 +134,7 @@ struct EleStepArgs {
   float dxf, dyf;
   float inv_dx, inv_dy;
   Rcp rcp;
+  const unsigned *ebound;  // float bits of max |Ex| + |Ey| over the corners (k_e_corners), or nullptr
   double dt, qm, ds_lim;
   const double *ds_max;
   int *n_sub_out;

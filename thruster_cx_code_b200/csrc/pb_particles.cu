@@ -234,6 +234,15 @@ __device__ __forceinline__ void push_cell(float x, float y, int nx, int ny, floa
   w00 = DMUL(gx, gy); w10 = DMUL(fx, gy); w01 = DMUL(gx, fy); w11 = DMUL(fx, fy);
 }
 
+// A float as a double scaled by 2^-896, from its bits (sign, then the 8 exponent bits as the
+// low bits of the 11-bit exponent, then the mantissa): exact for every finite float, zero
+// and subnormals included, with integer instructions instead of the conversion unit.
+// Infinities and NaN come out finite, so it is used only on values known to be finite.
+__device__ __forceinline__ double f2d_scaled(float f) {
+  const int b = __float_as_int(f);
+  return __hiloint2double((b >> 3) & (int)0x8FFFFFFF, (int)((unsigned)b << 29));
+}
+
 // Half kick, rotation (B = 0: t = s = h * (+0)), half kick and drift from the gathered E.
 __device__ __forceinline__ void push_update_b0(float& x, float& y, float& vx, float& vy, float& vz, double ex,
                                                double ey, double h, float dtf) {
@@ -1244,14 +1253,48 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
 // in order (the same single-pass look-back as the fused kernel).  The push is compute-bound
 // at many sub-steps per electron, so the extra pass over the state costs less than the
 // barriers it removes.  Same operations, same bits as k_ele_step.
-__global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __restrict__ keep) {
-  pdl_enter();
-  const int n = *a.num_src;
-  const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
-  const double dt_sub = DDIV(a.dt, (double)n_sub);
-  const double h = DMUL(DMUL(0.5, a.qm), dt_sub);
-  const float dtf = __double2float_rn(dt_sub);
-  if (blockIdx.x == 0 && threadIdx.x == 0) *a.n_sub_out = n_sub;
+// One electron sub-step of k_ele_push.  EFIN (every corner value finite, from the bound
+// k_e_corners leaves): a position inside the grid has weights in [0, 1], and the Ex and Ey
+// values of the cell's lower-left corner are made doubles by their bits (f2d_scaled) and
+// multiplied by w00 2^896 (exact), which rounds a.x w00 exactly as the converted product
+// does, with two fewer conversion-unit instructions.  Other positions take boris_push_one.
+template <bool EFIN>
+__device__ __forceinline__ void ele_substep(float& x, float& y, float& vx, float& vy, float& vz,
+                                            const EleStepArgs& a, double h, float dtf) {
+  if (!EFIN) {
+    boris_push_one<false, true, true>(x, y, vx, vy, vz, a.Ex, a.Ey, nullptr, nullptr, nullptr, a.nx, a.ny, a.dxf,
+                                      a.dyf, h, dtf, a.Ec, a.rcp);
+    return;
+  }
+  float ixf, iyf;
+  const bool okq = div_bracket(x, a.dxf, a.rcp.ix, a.rcp.ix_lo, a.rcp.ix_hi, ixf) &
+                   div_bracket(y, a.dyf, a.rcp.iy, a.rcp.iy_lo, a.rcp.iy_hi, iyf);
+  int fxi, fyi;
+  float frx, fry;
+  floor_frac(ixf, fxi, frx);
+  floor_frac(iyf, fyi, fry);
+  const bool inside = okq & ((unsigned)fxi <= (unsigned)(a.nx - 2)) & ((unsigned)fyi <= (unsigned)(a.ny - 2));
+  if (!inside) {
+    boris_push_one<false, true, true>(x, y, vx, vy, vz, a.Ex, a.Ey, nullptr, nullptr, nullptr, a.nx, a.ny, a.dxf,
+                                      a.dyf, h, dtf, a.Ec, a.rcp);
+    return;
+  }
+  const double fx = (double)frx, fy = (double)fry;
+  const double gx = DSUB(1.0, fx), gy = DSUB(1.0, fy);
+  const double w00 = DMUL(gx, gy), w10 = DMUL(fx, gy), w01 = DMUL(gx, fy), w11 = DMUL(fx, fy);
+  const double w00s = DMUL(w00, 0x1p896);
+  const float4* e = a.Ec + 2 * (fyi * a.nx + fxi);
+  const float4 A = __ldg(e), B = __ldg(e + 1);
+  const double ex = DADD(DADD(DADD(DMUL(f2d_scaled(A.x), w00s), DMUL((double)A.y, w10)), DMUL((double)A.z, w01)),
+                         DMUL((double)A.w, w11));
+  const double ey = DADD(DADD(DADD(DMUL(f2d_scaled(B.x), w00s), DMUL((double)B.y, w10)), DMUL((double)B.z, w01)),
+                         DMUL((double)B.w, w11));
+  push_update_b0(x, y, vx, vy, vz, ex, ey, h, dtf);
+}
+
+template <bool EFIN>
+__device__ __forceinline__ void ele_push_range(const EleStepArgs& a, uint8_t* __restrict__ keep, int n, int n_sub,
+                                               double h, float dtf) {
   const int stride = gridDim.x * blockDim.x;
   // trip count uniform across a warp (the deposit count is a warp-wide vote)
   const int n_pad = (n + 31) & ~31;
@@ -1260,11 +1303,9 @@ __global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __re
     bool kp = false;
     if (i < n) {
       float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
-      // two sub-steps per loop pass: no spills at 32 registers (20 bytes without), 1.3% faster
-#pragma unroll 2
-      for (int s = 0; s < n_sub; ++s)
-        boris_push_one<false, true, true>(x, y, vx, vy, vz, a.Ex, a.Ey, nullptr, nullptr, nullptr, a.nx, a.ny, a.dxf,
-                                          a.dyf, h, dtf, a.Ec, a.rcp);
+      // plain path: two sub-steps per loop pass (no spills at 32 registers, 1.3% faster)
+#pragma unroll (EFIN ? 1 : 2)
+      for (int s = 0; s < n_sub; ++s) ele_substep<EFIN>(x, y, vx, vy, vz, a, h, dtf);
       if (a.periodic) y = np_modf_pos(y, a.Lyf);
       const int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1);
       const int icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
@@ -1279,6 +1320,20 @@ __global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __re
     }
     warp_count_add(a.cnt, dep_cell, kp);
   }
+}
+
+__global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __restrict__ keep) {
+  pdl_enter();
+  const int n = *a.num_src;
+  const int n_sub = substep_count(*a.ds_max, a.ds_lim, nullptr);
+  const double dt_sub = DDIV(a.dt, (double)n_sub);
+  const double h = DMUL(DMUL(0.5, a.qm), dt_sub);
+  const float dtf = __double2float_rn(dt_sub);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.n_sub_out = n_sub;
+  // every corner value finite (and |Ex| + |Ey| below the float range): the bound's bits
+  const bool efin = a.ebound && *a.ebound < 0x7F800000u;
+  if (efin) ele_push_range<true>(a, keep, n, n_sub, h, dtf);
+  else ele_push_range<false>(a, keep, n, n_sub, h, dtf);
 }
 
 struct EleCompactStage {

@@ -932,6 +932,7 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
   b.Ex = s->Ex; b.Ey = s->Ey; b.Ec = s->ecorn; b.Bx = b.By = b.Bz = nullptr; b.has_B = 0;
   b.isBound = s->isBound; b.nx = s->nx; b.ny = s->ny; b.dxf = dxf; b.dyf = dyf;
   b.inv_dx = 1.0f / dxf; b.inv_dy = 1.0f / dyf; b.rcp = make_rcp(dxf, dyf);
+  b.ebound = ebound;
   b.dt = p->dt; b.qm = p->qm_e; b.ds_lim = p->ds_lim; b.ds_max = (const double*)(s->ds_bits + 1);
   b.n_sub_out = s->n_sub + 1; b.periodic = s->periodic; b.Lyf = (float)p->Ly; b.Lxf = (float)p->Lx;
   b.cnt = s->cnt_e; b.tile_status = s->tile_status + s->tile_cap; b.tile_counter = s->tile_counter + 1;
