@@ -244,10 +244,13 @@ __device__ __forceinline__ double f2d_scaled(float f) {
 }
 
 // Half kick, rotation (B = 0: t = s = h * (+0)), half kick and drift from the gathered E.
+// VBITS (callers know vx, vy finite): vx and vy become doubles by their bits, and
+// RN(vx 2^-896 * 2^896 + h ex) in one FMA is the rounded sum of the converted value.
+template <bool VBITS = false>
 __device__ __forceinline__ void push_update_b0(float& x, float& y, float& vx, float& vy, float& vz, double ex,
                                                double ey, double h, float dtf) {
-  const double vmx = DADD((double)vx, DMUL(h, ex));
-  const double vmy = DADD((double)vy, DMUL(h, ey));
+  const double vmx = VBITS ? __fma_rn(f2d_scaled(vx), 0x1p896, DMUL(h, ex)) : DADD((double)vx, DMUL(h, ex));
+  const double vmy = VBITS ? __fma_rn(f2d_scaled(vy), 0x1p896, DMUL(h, ey)) : DADD((double)vy, DMUL(h, ey));
   if ((vmx != 0.0) & (vmy != 0.0) & (vz != 0.0f) & (fabs(vmx) < INFINITY) & (fabs(vmy) < INFINITY) &
       (fabsf(vz) < INFINITY)) {
     // every cross-product term below is a signed zero (t = s = h * (+0)), and a finite
@@ -1246,19 +1249,16 @@ __global__ void __launch_bounds__(NT) k_ele_step(EleStepArgs a) {
   }
 }
 
-// ------------------------------------------------------------------ split electron step
-// PB_OPT_ELE_SPLIT: the electron step as two kernels.  k_ele_push advances every electron
-// independently (no shared-memory staging, no block barriers), writes it back in place and
-// records whether it survives; k_ele_compact then moves the survivors to the other buffer
-// in order (the same single-pass look-back as the fused kernel).  The push is compute-bound
-// at many sub-steps per electron, so the extra pass over the state costs less than the
-// barriers it removes.  Same operations, same bits as k_ele_step.
 // One electron sub-step of k_ele_push.  EFIN (every corner value finite, from the bound
 // k_e_corners leaves): a position inside the grid has weights in [0, 1], and the Ex and Ey
 // values of the cell's lower-left corner are made doubles by their bits (f2d_scaled) and
 // multiplied by w00 2^896 (exact), which rounds a.x w00 exactly as the converted product
 // does, with two fewer conversion-unit instructions.  Other positions take boris_push_one.
-template <bool EFIN>
+// VFIN (every electron's velocity finite at the start of the step, from the sub-step
+// reduction's maximum): on that path vx and vy are finite too, since a sub-step that makes
+// a velocity non-finite makes the position non-finite, which never lies inside the grid
+// again; they become doubles by their bits (push_update_b0<true>).
+template <bool EFIN, bool VFIN>
 __device__ __forceinline__ void ele_substep(float& x, float& y, float& vx, float& vy, float& vz,
                                             const EleStepArgs& a, double h, float dtf) {
   if (!EFIN) {
@@ -1289,10 +1289,10 @@ __device__ __forceinline__ void ele_substep(float& x, float& y, float& vx, float
                          DMUL((double)A.w, w11));
   const double ey = DADD(DADD(DADD(DMUL(f2d_scaled(B.x), w00s), DMUL((double)B.y, w10)), DMUL((double)B.z, w01)),
                          DMUL((double)B.w, w11));
-  push_update_b0(x, y, vx, vy, vz, ex, ey, h, dtf);
+  push_update_b0<VFIN>(x, y, vx, vy, vz, ex, ey, h, dtf);
 }
 
-template <bool EFIN>
+template <bool EFIN, bool VFIN>
 __device__ __forceinline__ void ele_push_range(const EleStepArgs& a, uint8_t* __restrict__ keep, int n, int n_sub,
                                                double h, float dtf) {
   const int stride = gridDim.x * blockDim.x;
@@ -1305,7 +1305,7 @@ __device__ __forceinline__ void ele_push_range(const EleStepArgs& a, uint8_t* __
       float x = a.src.x[i], y = a.src.y[i], vx = a.src.vx[i], vy = a.src.vy[i], vz = a.src.vz[i];
       // plain path: two sub-steps per loop pass (no spills at 32 registers, 1.3% faster)
 #pragma unroll (EFIN ? 1 : 2)
-      for (int s = 0; s < n_sub; ++s) ele_substep<EFIN>(x, y, vx, vy, vz, a, h, dtf);
+      for (int s = 0; s < n_sub; ++s) ele_substep<EFIN, VFIN>(x, y, vx, vy, vz, a, h, dtf);
       if (a.periodic) y = np_modf_pos(y, a.Lyf);
       const int icx = cell_round_f(x, a.dxf, a.inv_dx, 0, a.nx - 1);
       const int icy = cell_round_f(y, a.dyf, a.inv_dy, 0, a.ny - 1);
@@ -1322,6 +1322,13 @@ __device__ __forceinline__ void ele_push_range(const EleStepArgs& a, uint8_t* __
   }
 }
 
+// ------------------------------------------------------------------ split electron step
+// PB_OPT_ELE_SPLIT: the electron step as two kernels.  k_ele_push advances every electron
+// independently (no shared-memory staging, no block barriers), writes it back in place and
+// records whether it survives; k_ele_compact then moves the survivors to the other buffer
+// in order (the same single-pass look-back as the fused kernel).  The push is compute-bound
+// at many sub-steps per electron, so the extra pass over the state costs less than the
+// barriers it removes.  Same operations, same bits as k_ele_step.
 __global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __restrict__ keep) {
   pdl_enter();
   const int n = *a.num_src;
@@ -1332,8 +1339,12 @@ __global__ void __launch_bounds__(NT, 8) k_ele_push(EleStepArgs a, uint8_t* __re
   if (blockIdx.x == 0 && threadIdx.x == 0) *a.n_sub_out = n_sub;
   // every corner value finite (and |Ex| + |Ey| below the float range): the bound's bits
   const bool efin = a.ebound && *a.ebound < 0x7F800000u;
-  if (efin) ele_push_range<true>(a, keep, n, n_sub, h, dtf);
-  else ele_push_range<false>(a, keep, n, n_sub, h, dtf);
+  // every electron's |v| finite: the sub-step reduction's maximum is finite (a NaN or
+  // infinite velocity gives a NaN or infinite predicted displacement, never passed over)
+  const bool vfin = *a.ds_max < INFINITY;
+  if (efin && vfin) ele_push_range<true, true>(a, keep, n, n_sub, h, dtf);
+  else if (efin) ele_push_range<true, false>(a, keep, n, n_sub, h, dtf);
+  else ele_push_range<false, false>(a, keep, n, n_sub, h, dtf);
 }
 
 struct EleCompactStage {
