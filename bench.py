@@ -43,6 +43,11 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# The batched sweep enqueues its members' kernels on one stream each; with the default 8
+# hardware queues, streams share queues and the host blocks on full ones.  32 queues (the
+# most CUDA allows, for this process only, read when the context is created) measured 1.5%
+# less device time for the 64-point batch and half the host enqueue time.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 import numpy as np  # noqa: E402
 
