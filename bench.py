@@ -456,11 +456,15 @@ def poisson_section(sim, stats_before, reports, field_ms, peak):
 
 
 # ----------------------------------------------------------------------------- sweeps
-SWEEP_WARMUP, SWEEP_STEPS, SWEEP_REF_STEPS = 3, 40, 3000
-# warm-up of each batched form: 20 steps hold every step shape (field solve or not, buffer
-# parity, the sort step), so the graph form captures before the timed steps, and the block
-# shares come from a measured run
-SWEEP_WARMUP_BATCH = 20
+SWEEP_STEPS, SWEEP_REF_STEPS = 40, 3000
+# Each form (plain, batched on streams, batched as step graphs) runs its own copy of the same
+# points, built from the same seeds, and times the same steps: two warm-up runs of 20 and 40
+# steps, then 40 timed steps (steps 61-100 of every point).  The first warm-up run measures
+# each point's field-solve cost for the batch's block plan; the second grows the particle
+# buffers to what 40-step runs reserve and, as graphs, captures every step shape (field solve
+# or not, buffer parity, the sort step) under that plan.  A point's results are the same bits
+# in every form, so the three timed regions do the same work.
+SWEEP_WARMUP_RUNS = (20, 40)
 # a request retires when the 500-step means of its saddle potential and beamlet current
 # change by less than 0.5% from one 500 steps to the next
 SERVE_RATE_HZ, SERVE_WINDOW, SERVE_TOL, SERVE_CHUNK = 20.0, 1000, 5e-3, 50
@@ -490,17 +494,16 @@ def _build_all(specs, device, solver=None, workers=8):
 
 
 def sweep_section(device, args):
-    """Sweep points per hour, plain against batched, on one set of C3 perveance-sweep
-    points: screen 600-1800 V, accel -300..-100 V, plasma density log-uniform
-    3e16-3e17 m^-3, grids drawn from {64x256, 128x512, 256x1024} cells and 0.2M-4M
-    macro-particles log-uniform.  Plain: each point alone through pb_sim_run (3 warm-up
-    steps, then 40 timed).  Batched: all points together through pb_batch_run, from the
-    state the plain steps left (20 warm-up steps, then 40 timed), first with every member's
-    kernels enqueued on its own stream, then with each batch step shape captured as one CUDA
-    graph and replayed (the warm-up steps capture); the faster form is the one reported as
-    batched, both are listed.  Rates use device time, scaled to 3000
-    steps per point; setup is excluded.  The particle-pushes of each part are reported, so
-    their workloads can be compared.  Then the C4 served run."""
+    """Sweep points per hour, plain against batched, on C3 perveance-sweep points: screen
+    600-1800 V, accel -300..-100 V, plasma density log-uniform 3e16-3e17 m^-3, grids drawn
+    from {64x256, 128x512, 256x1024} cells and 0.2M-4M macro-particles log-uniform.  Plain:
+    each point alone through pb_sim_run.  Batched: all points together through pb_batch_run,
+    with every member's kernels enqueued on its own stream, and with each batch step shape
+    captured as one CUDA graph and replayed; the faster form is the one reported as batched,
+    both are listed.  Each form runs its own copy of the same points and times the same steps
+    (SWEEP_WARMUP_RUNS), so the three timed regions do the same work (``same_work`` checks
+    the pushes).  Rates use device time, scaled to 3000 steps per point; setup is excluded.
+    Then the C4 served run."""
     from thruster_cx_code_b200 import serving as SV
     from thruster_cx_code_b200 import workloads as W
     rng = np.random.default_rng(7)
@@ -509,33 +512,42 @@ def sweep_section(device, args):
     t_setup = time.perf_counter()
     built = _build_all(specs, device)
     t_setup = time.perf_counter() - t_setup
-    sims, prm = [s for s, _ in built], [p for _, p in built]
     for s, p in built:
-        _run_plain(s, p, SWEEP_WARMUP)
+        for k in SWEEP_WARMUP_RUNS:
+            _run_plain(s, p, k)
     plain_pushes, plain_solve = [], []
     plain_ms = sum(_run_plain(s, p, SWEEP_STEPS, plain_pushes, plain_solve) for s, p in built)
+    for s, _ in built:
+        s.close()
+
+    batch = SV.SweepBatch(device)
+
     def batched(graphs):
+        """One batched form on a fresh copy of the points; returns device ms, host enqueue ms,
+        pushes, field-solve ms and the graph captures that fell in the timed steps."""
+        sb = _build_all(specs, device)
+        sims, prm = [s for s, _ in sb], [p for _, p in sb]
+        # the batched points' coarsest level (default: the plain points' own; 256 measured slower)
+        if args.batch_max_coarse != 1536:
+            from thruster_cx_code_b200 import autotune as AT
+            for s in sims:
+                AT.apply(s, {"max_coarse": args.batch_max_coarse})
         batch.set_graphs(graphs)
-        batch.run(sims, prm, SWEEP_WARMUP_BATCH)
+        for k in SWEEP_WARMUP_RUNS:
+            batch.run(sims, prm, k)
         n0 = [(s.num_p, s.num_e) for s in sims]
         g0 = batch.graph_stats()
         res = batch.run(sims, prm, SWEEP_STEPS)
-        batched.timed_captures = batch.graph_stats()[0] - g0[0]
+        captures = batch.graph_stats()[0] - g0[0]
         pushes = sum(SV.pushes_of([rep for _, rep in r], a, b) for r, (a, b) in zip(res, n0))
-        batched.solve_ms = batch.last_solve_ms
-        return batch.last_ms, batch.last_host_ms, pushes
-
-    # the batched points' coarsest level (default: the plain points' own; 256 measured slower)
-    if args.batch_max_coarse != 1536:
-        from thruster_cx_code_b200 import autotune as AT
+        out = (batch.last_ms, batch.last_host_ms, pushes, batch.last_solve_ms, captures)
+        batch.set_graphs(False)
         for s in sims:
-            AT.apply(s, {"max_coarse": args.batch_max_coarse})
-    batch = SV.SweepBatch(device)
-    streams_ms, streams_host_ms, streams_pushes = batched(False)
-    streams_solve_ms = batched.solve_ms
-    graph_ms, graph_host_ms, graph_pushes = batched(True)
-    graph_solve_ms = batched.solve_ms
-    graph_timed_captures = batched.timed_captures
+            s.close()
+        return out
+
+    streams_ms, streams_host_ms, streams_pushes, streams_solve_ms, _ = batched(False)
+    graph_ms, graph_host_ms, graph_pushes, graph_solve_ms, graph_timed_captures = batched(True)
     g_stats = batch.graph_stats()
     # the batched form reported: the faster of the two (graphs only when no capture failed)
     use_graphs = not g_stats[2] and graph_ms < streams_ms
@@ -543,9 +555,6 @@ def sweep_section(device, args):
         batched_ms, batched_host_ms, batched_pushes = graph_ms, graph_host_ms, graph_pushes
     else:
         batched_ms, batched_host_ms, batched_pushes = streams_ms, streams_host_ms, streams_pushes
-    batch.set_graphs(False)
-    for s in sims:
-        s.close()
     per_point_plain_s = plain_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts
     per_point_batched_s = batched_ms / SWEEP_STEPS * SWEEP_REF_STEPS / 1e3 / npts
     peak, _ = measured_peak_gbs()
@@ -571,7 +580,10 @@ def sweep_section(device, args):
                       "device_ms": graph_ms, "host_enqueue_ms": graph_host_ms,
                       "field_solve_ms": graph_solve_ms if graph_solve_ms >= 0 else None,
                       "over_plain": plain_ms / graph_ms},
-           "setup": f"excluded ({t_setup:.1f} s of host geometry, multigrid build and pre-load on 8 threads)"}
+           "steps": f"each form on its own copy of the points: warm-up runs of {SWEEP_WARMUP_RUNS} steps, "
+                    f"then steps {sum(SWEEP_WARMUP_RUNS) + 1}-{sum(SWEEP_WARMUP_RUNS) + SWEEP_STEPS} timed",
+           "same_work": float(sum(plain_pushes)) == float(streams_pushes) == float(graph_pushes),
+           "setup": f"excluded ({t_setup:.1f} s per copy of host geometry, multigrid build and pre-load on 8 threads)"}
     for name, pushes, ms in (("plain", float(sum(plain_pushes)), plain_ms),
                              ("batched", float(batched_pushes), batched_ms)):
         rate = pushes / (ms * 1e-3)
