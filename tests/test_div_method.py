@@ -1,5 +1,7 @@
-"""The electron push's division without the reciprocal instruction (div_rn_checked in
-csrc/pb_particles.cu), restated in NumPy and checked against IEEE float32 division.
+"""The particle kernels' divisions without the division instruction, restated on the host and
+checked against IEEE float32 division: div_rn_checked (csrc/pb_particles.cu; the ion step's
+final cells and the sub-step reduction) and div_bracket (the push of both step kernels), and
+the electron push's float-to-double conversion by bits (f2d_scaled).
 
 q = x * inv (inv = RN(1/d)), one correction q += (x - q d) inv, accepted when
 |x - q d| < ulp(q) |d| / 2; anything else falls back to the division.  fmaf(a, b, c) of
@@ -120,3 +122,103 @@ def test_one_unsigned_compare_bounds_the_floor():
             inside = (q >= 0) & (q < N + 1)
         assert np.array_equal(ok, inside)
         assert np.array_equal(fl[ok], np.floor(q[ok]).astype(np.int64))
+
+
+# ---------------------------------------------------------------- bracketed division
+# div_bracket (csrc/pb_particles.cu), the division of the step kernels' push: q0 = RN(x inv),
+# r0 = RN(q0 d - x), qa = RN(q0 - r0 lo), qb = RN(q0 - r0 hi) with lo and hi the floats two
+# steps below and above inv = RN(1/d); accepted when qa == qb and |x| >= 2^-80.  Every
+# fused multiply-add is emulated exactly here (rational arithmetic, one rounding to float32,
+# ties to even); pb_check_division runs the same test on the GPU over all 2^32 x.
+from fractions import Fraction  # noqa: E402
+
+
+def _rn32(v):
+    """Fraction -> nearest float32 (ties to even), finite inputs whose result is finite."""
+    if v == 0:
+        return F32(0.0)
+    s = -1 if v < 0 else 1
+    a = abs(v)
+    e = a.numerator.bit_length() - a.denominator.bit_length()
+    if Fraction(2) ** e > a:
+        e -= 1
+    e = max(e, -126)                    # below 2^-126: subnormal spacing 2^-149
+    scale = Fraction(2) ** (23 - e)     # a * scale in [2^23, 2^24) for normal results
+    m = a * scale
+    q, r = divmod(m.numerator, m.denominator)
+    rem = Fraction(r, m.denominator)
+    if rem > Fraction(1, 2) or (rem == Fraction(1, 2) and q % 2 == 1):
+        q += 1
+    return F32(s * float(Fraction(q) / scale))
+
+
+def _fma32_exact(a, b, c):
+    return _rn32(Fraction(float(a)) * Fraction(float(b)) + Fraction(float(c)))
+
+
+def div_bracket(x, d):
+    x, d = F32(x), F32(d)
+    inv = F32(1.0) / d
+    b = np.array([inv], dtype=F32).view(np.uint32)[0]
+    lo = np.array([b - 2], dtype=np.uint32).view(F32)[0]
+    hi = np.array([b + 2], dtype=np.uint32).view(F32)[0]
+    q0 = F32(x * inv)
+    r0 = _fma32_exact(q0, d, -x)
+    qa = _fma32_exact(-r0, lo, q0)
+    qb = _fma32_exact(-r0, hi, q0)
+    return qa, bool(qa == qb and abs(float(x)) >= 2.0 ** -80)
+
+
+def test_div_bracket_accepts_only_the_division():
+    rng = np.random.default_rng(11)
+    spacings = [F32(v) for v in (0.025, 0.00625, 0.003125, 0.011, 0.3)] + \
+        [F32(v) for v in rng.uniform(1e-3, 1.0, 3)]
+    n_acc = n = 0
+    with np.errstate(over="ignore", invalid="ignore", under="ignore"):
+        for d in spacings:
+            xs = list(rng.uniform(0.0, 2048 * float(d), 400).astype(F32))                  # in the grid
+            k = rng.integers(1, 2048, 300)
+            xs += list((k * d).astype(F32))                                                  # cell boundaries
+            xs += list(np.nextafter((k * d).astype(F32), F32(np.inf)))
+            n_grid = len(xs)
+            bits = rng.integers(0x0C000000, 0x4B000000, 300, dtype=np.int64).astype(np.uint32)
+            xs += list(bits.view(F32))                                                       # random patterns
+            for j, x in enumerate(xs):
+                q, ok = div_bracket(x, d)
+                if ok:
+                    assert q == F32(x) / d, (float(x), float(d))
+                if j < n_grid:
+                    n += 1
+                    n_acc += ok
+    assert n_acc >= 0.999 * n  # in-grid positions: nearly all take the bracketed quotient
+
+
+def test_div_bracket_zero_and_tiny_fall_back():
+    for x in (0.0, -0.0, 1e-30, -1e-30):
+        assert not div_bracket(x, 0.025)[1]
+
+
+# ---------------------------------------------------------------- float -> double by bits
+# f2d_scaled (csrc/pb_particles.cu): hi = (bits >> 3, arithmetic) & 0x8FFFFFFF, lo = bits << 29
+# is the double f 2^-896 for every finite float f; the electron push multiplies it by a weight
+# scaled by 2^896 (or adds it times 2^896 in an FMA), which rounds as the converted value does.
+def _f2d_scaled(f):
+    b = np.asarray(f, dtype=F32).view(np.int32).astype(np.int64)
+    hi = ((b >> 3) & 0x8FFFFFFF) & 0xFFFFFFFF
+    lo = (b << 29) & 0xFFFFFFFF
+    return ((hi << 32) | lo).astype(np.uint64).view(np.float64)
+
+
+def test_f2d_scaled_is_exact_for_finite_floats():
+    rng = np.random.default_rng(3)
+    bits = rng.integers(0, 1 << 32, 200000, dtype=np.int64).astype(np.uint32)
+    bits = np.concatenate([bits, np.array([0, 0x80000000, 1, 0x80000001, 0x007FFFFF, 0x00800000, 0x7F7FFFFF,
+                                           0xFF7FFFFF, 0x3F800000], dtype=np.uint32)])
+    f = bits.view(F32)
+    f = f[np.isfinite(f)]
+    got = _f2d_scaled(f) * 2.0 ** 896
+    want = f.astype(np.float64)
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+    # the product with a scaled weight equals the product with the converted value, bit for bit
+    w = rng.uniform(0.0, 1.0, f.size)
+    assert np.array_equal((_f2d_scaled(f) * (w * 2.0 ** 896)).view(np.uint64), (want * w).view(np.uint64))
