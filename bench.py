@@ -55,7 +55,10 @@ DEFAULT_WORKLOAD = "long_erosion_3grid"
 SECOND_WORKLOAD = "large_aperture_3grid"
 ALG_BYTES_PUSH = 41     # per particle and fused step-kernel launch
 ALG_BYTES_DEPOSIT = 8   # per particle deposited (x, y)
-TRAFFIC_PROFILE = os.path.join(ROOT, "profiles", "dram_traffic_large_aperture_3grid.md")
+# ncu summaries of the DRAM bytes per particle of the step kernels, one per workload: the
+# 513 x 2049 particle state exceeds L2 and moves more bytes per particle than 257 x 1025's
+TRAFFIC_PROFILES = {name: os.path.join(ROOT, "profiles", f"dram_traffic_{name}.md")
+                    for name in ("long_erosion_3grid", "large_aperture_3grid")}
 KERNEL_SOURCES = ("pb_particles.cu", "pb_common.cuh", "pb_kernels.cuh")
 # fine phases of pb_sim_phase_times
 PHASES = ("inject_deposit", "field_solve", "corners_substeps", "ion_step", "sputter_break", "electron_step",
@@ -168,15 +171,16 @@ def kernel_source_sha():
     return h.hexdigest()[:16]
 
 
-def traffic_table():
-    """DRAM bytes per particle of each step kernel from the committed ncu summary:
-    ({kernel: bytes per particle}, note).  Empty when the summary was taken on kernel
-    sources other than the current ones (its 'kernel_source_sha:' line)."""
+def traffic_table(workload):
+    """DRAM bytes per particle of each step kernel from the committed ncu summary of the
+    workload: ({kernel: bytes per particle}, note).  Empty when there is none, or when it was
+    taken on kernel sources other than the current ones (its 'kernel_source_sha:' line)."""
+    path = TRAFFIC_PROFILES.get(workload)
     try:
-        with open(TRAFFIC_PROFILE) as f:
+        with open(path) as f:
             lines = f.read().splitlines()
-    except OSError:
-        return {}, "no ncu traffic summary"
+    except (OSError, TypeError):
+        return {}, f"no ncu traffic summary for {workload}"
     sha, table = None, {}
     for ln in lines:
         s = ln.strip()
@@ -189,7 +193,7 @@ def traffic_table():
     cur = kernel_source_sha()
     if sha != cur:
         return {}, f"stale: ncu summary taken on kernel sources {sha}, current {cur}"
-    return table, f"ncu summary on kernel sources {cur}"
+    return table, f"ncu summary {os.path.basename(path)} on kernel sources {cur}"
 
 
 # ----------------------------------------------------------------------------- GPU arm
@@ -346,7 +350,7 @@ def gpu_arm(args):
         e2e = {"value": pe2e / wall, "unit": "particle-pushes/s", "h2d_bytes_per_step": C.sizeof(_lib.StepParams),
                "d2h_bytes_per_step": C.sizeof(_lib.StepReport), "same_steps_as_value": pe2e == pushes_all}
     peak, peak_kind = measured_peak_gbs()
-    traffic, traffic_note = traffic_table()
+    traffic, traffic_note = traffic_table(args.workload)
     kr = kernel_rooflines(run, K, peak, traffic)
     # the dominant kernel of the step: the electron step (many sub-steps per launch)
     dom = "k_ele_step" if kr["k_ele_step"]["launch_ms"] >= kr["k_ion_step"]["launch_ms"] else "k_ion_step"
@@ -372,7 +376,7 @@ def gpu_arm(args):
     sim.close()
     del sim
     if rank == 0 and world == 1 and not args.no_second and args.workload != SECOND_WORKLOAD:
-        line["workloads"] = {SECOND_WORKLOAD: second_workload(args, local, peak, traffic)}
+        line["workloads"] = {SECOND_WORKLOAD: second_workload(args, local, peak, traffic_table(SECOND_WORKLOAD)[0])}
     if rank == 0 and world == 1 and not args.no_sweep:
         line["sweep"] = sweep_section(local, args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
