@@ -57,3 +57,22 @@ def test_reference_arm_prints_its_line():
     assert line["metric"] == "particle-pushes/s" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_traffic_summaries_parse_per_workload():
+    """Each headline workload has its own ncu traffic summary with a kernel-source hash and the
+    DRAM bytes per particle of both step kernels; bench.traffic_table reads it (or reports it
+    stale when the kernel sources changed since the capture)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    for name in ("long_erosion_3grid", "large_aperture_3grid"):
+        with open(bench.TRAFFIC_PROFILES[name]) as f:
+            text = f.read()
+        assert "kernel_source_sha:" in text
+        assert text.count("dram_bytes_per_particle:") == 2
+        table, note = bench.traffic_table(name)
+        if note.startswith("stale"):
+            assert table == {}
+        else:
+            assert set(table) == {"k_ion_step", "k_ele_step"} and all(v >= 41.0 for v in table.values())
+    assert bench.traffic_table("no_such_workload") == ({}, "no ncu traffic summary for no_such_workload")
