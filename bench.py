@@ -726,8 +726,8 @@ _REF_DOMAIN = None
 
 
 def reference_arm(args):
-    """The reference's CPU path (the oracle port: /root/reference is not on the bench
-    host) on all host cores.  One domain build, then one forked worker per core, each a
+    """The reference's CPU path (the oracle port: the reference's own source tree is not on
+    the bench host) on all host cores.  One domain build, then one forked worker per core, each a
     replica of the workload run on a particle sample; each replica's step time is its
     particle time scaled to the workload's particle count plus its full-grid field-solve
     time.  value = replicas x pushes per full step / the slowest replica's step time."""

@@ -988,7 +988,8 @@ static int32_t enqueue_step_post(pb_sim* h, const pb_step_params* p) {
                 (unsigned long long*)&rep->ppc_active));
   ++s->launches;
 
-  // periodic re-sort by cell (north-star (a)); the permutation equals a stable argsort
+  // periodic re-sort by cell key (locality of the gathers and deposits); the permutation
+  // equals a stable argsort
   if (p->sort_now) {
     int bits = 1;
     while ((1L << bits) < (long)N) ++bits;
